@@ -1,0 +1,380 @@
+"""GCV smoothing-parameter selection and residuals for ``regrXonS`` (oracle).
+
+TEST INFRASTRUCTURE ONLY: the CPU checker for the library's fit kernels.
+
+GCV score V(rho) = n * RSS / (n - EDF)^2 in rho = log(lambda), minimised by
+mgcv ``magic``'s Newton scheme as the reference restates it:
+
+* single penalty (|S| <= 2): spectral form.  With X'X = U'U and the whitened
+  penalty U^-T S U^-1 = W diag(e) W', the hat values are h_k = 1/(1+lambda e_k)
+  and z = W' U^-T X' y, so RSS = |y|^2 - 2 sum h z^2 + sum h^2 z^2 and
+  EDF = sum h (fastkpc/src/full_cuda_ci_one_call.cpp:1869-1947 geometry;
+  fastkpc/src/cuda/mgcv_single_penalty_gcv.cu:189-283 objective and
+  :1479-1700 optimizer: 15 step halvings, 400 iterations, |step| <= 5,
+  tolerance 1e-7, boundary probes of +-2 up to 5 times, flat-objective stop).
+* several penalties (|S| > 2): augmented SVD form.  [R; B] = U D V' with
+  X = QR and B'B = sum lambda_j S_j; singular values below d_0 * sqrt(eps)
+  are dropped; U1 = top q rows of U; y1 = U1' Q'y;
+  RSS = |y|^2 - 2|y1|^2 + |U1 y1|^2, EDF = |U1|_F^2, with the analytic
+  gradient and Hessian in rho (fastkpc/src/mgcv_multi_penalty_cpp.cpp:732-975)
+  and the Newton loop of :1124-1346 (25 step halvings, steepest descent after
+  the third rejected Newton trial or when the Hessian has a negative
+  eigenvalue, boundary probes).
+
+Residuals at the selected lambda use the same augmented SVD
+(``refine_multi_penalty_selected_fit``, :977-1029).
+"""
+import math
+
+import numpy as np
+
+EPS = np.finfo(np.float64).eps
+RANK_TOL = math.sqrt(EPS)  # 1.4901161193847656e-8
+CONV_TOL = 1e-7
+
+
+class Prepared:
+    """Per-design quantities shared by every target fitted on that design."""
+
+    def __init__(self, des):
+        X = des["X"]
+        self.X = X
+        self.n, self.q = X.shape
+        self.blocks = des["blocks"]
+        self.offsets = des["offsets"]
+        self.ranks = des["ranks"]
+        self.m = len(self.blocks)
+        self.initial_sp = np.asarray(des["initial_sp"], dtype=np.float64)
+        self.Q, self.R = np.linalg.qr(X)
+        # penalty roots placed in the full coefficient space: root root' = S_j
+        self.roots = []
+        for S, off, r in zip(self.blocks, self.offsets, self.ranks):
+            w, v = np.linalg.eigh((S + S.T) / 2.0)
+            order = np.argsort(-w)[:r]
+            root = np.zeros((self.q, r))
+            root[off:off + S.shape[0], :] = v[:, order] * np.sqrt(np.maximum(w[order], 0.0))
+            self.roots.append(root)
+        if self.m == 1:
+            self._single_geometry()
+
+    def _single_geometry(self):
+        q = self.q
+        S = np.zeros((q, q))
+        off = self.offsets[0]
+        b = self.blocks[0]
+        S[off:off + b.shape[0], off:off + b.shape[0]] = b
+        G = self.X.T @ self.X
+        Uc = np.linalg.cholesky(G).T  # G = Uc' Uc
+        Ui = np.linalg.solve(Uc, np.eye(q))
+        W = Ui.T @ S @ Ui
+        W = 0.5 * (W + W.T)
+        vals, vecs = np.linalg.eigh(W)
+        vals = vals[::-1].copy()
+        vecs = vecs[:, ::-1].copy()
+        vals = np.maximum(vals, 0.0)
+        vals[self.ranks[0]:] = 0.0
+        self.spec_values = vals
+        self.rhs_transform = vecs.T @ Ui.T
+
+    def response(self, y):
+        y = np.asarray(y, dtype=np.float64)
+        out = {"y": y, "y0": self.Q.T @ y, "yy": float(np.dot(y, y))}
+        if self.m == 1:
+            out["z"] = self.rhs_transform @ (self.X.T @ y)
+        return out
+
+
+# ---------------------------------------------------------------- single
+
+def _hat(log_sp, e):
+    if e == 0.0:
+        return 1.0
+    c = log_sp + math.log(e)
+    if c >= 0.0:
+        v = math.exp(-c)
+        return v / (1.0 + v)
+    return 1.0 / (1.0 + math.exp(c))
+
+
+def single_objective(log_sp, e, z, yy, n):
+    lin = quad = edf = rg = rh = dg = dh = 0.0
+    for ek, zk in zip(e, z):
+        h = _hat(log_sp, ek)
+        z2 = zk * zk
+        omh = 1.0 - h
+        w = h * omh
+        lin += h * z2
+        quad += h * h * z2
+        edf += h
+        rg += 2.0 * h * omh * omh * z2
+        rh += 2.0 * h * omh * omh * (3.0 * h - 1.0) * z2
+        dg += w
+        dh -= w * (1.0 - 2.0 * h)
+    rss = yy - 2.0 * lin + quad
+    if rss < 0.0 and math.isfinite(rss):
+        rss = 0.0
+    rdf = n - edf
+    if not (math.isfinite(rss) and math.isfinite(edf)) or rss <= 0.0 or rdf <= 1e-8:
+        return {"valid": False, "rss": rss, "edf": edf, "score": math.inf}
+    score = n * rss / (rdf * rdf)
+    lg = rg / rss - 2.0 * dg / rdf
+    lh = rh / rss - (rg / rss) ** 2 - 2.0 * (dh / rdf - (dg / rdf) ** 2)
+    return {"valid": True, "rss": rss, "edf": edf, "score": score,
+            "gradient": score * lg, "hessian": score * (lh + lg * lg)}
+
+
+def optimize_single(prep, resp):
+    e = prep.spec_values
+    z = resp["z"]
+    yy = resp["yy"]
+    n = prep.n
+    max_half = 15
+    log_sp = math.log(prep.initial_sp[0])
+    cur = single_objective(log_sp, e, z, yy, n)
+    if not cur["valid"]:
+        raise ValueError("non-finite single-penalty objective")
+    min_score = cur["score"]
+    score_red = 1e10
+    steepest = False
+    prior_grad = math.nan
+    newton = 0.0
+    steep = 0.0
+    it = 0
+    calls = 1
+    converged = False
+    flat = False
+    while not converged and it < 400:
+        it += 1
+        try_step = it > 1
+        tries = 0
+        step = steep if steepest else newton
+        src_newton = not steepest
+        it_flat = False
+        while try_step:
+            tries += 1
+            if tries == 4 and not steepest:
+                steepest = True
+                step = steep
+                src_newton = False
+            trial_ls = log_sp + step
+            trial = single_objective(trial_ls, e, z, yy, n)
+            calls += 1
+            pred = cur["gradient"] * step + 0.5 * cur["hessian"] * step * step
+            resolution = 8.0 * EPS * (1.0 + abs(min_score))
+            unresolved = src_newton and math.isfinite(pred) and pred <= 0.0 and abs(pred) <= resolution
+            accepted = trial["valid"] and trial["score"] < min_score
+            if accepted:
+                try_step = False
+                score_red = min_score - trial["score"]
+                min_score = trial["score"]
+                log_sp = trial_ls
+                cur = trial
+            elif unresolved:
+                try_step = False
+                it_flat = True
+                flat = True
+            else:
+                step /= 2.0
+            if tries == max_half - 1 and try_step:
+                step = 0.0
+            if tries == max_half:
+                try_step = False
+        if it > 3:
+            converged = True
+            if score_red > CONV_TOL * (1.0 + min_score):
+                converged = False
+            if abs(prior_grad) > CONV_TOL ** (1.0 / 3.0) * (1.0 + abs(min_score)):
+                converged = False
+            if tries == max_half:
+                converged = True
+            if it_flat:
+                converged = True
+        prior_grad = cur["gradient"]
+        steepest = cur["hessian"] < 0.0
+        if not steepest:
+            newton = -cur["gradient"] / cur["hessian"]
+            if abs(newton) > 5.0:
+                newton = math.copysign(5.0, newton)
+        steep = 0.0 if cur["gradient"] == 0.0 else -cur["gradient"] / abs(cur["gradient"])
+    if not converged:
+        raise ValueError("single-penalty optimizer hit its iteration limit")
+    direction = 1.0 if cur["gradient"] < 0.0 else -1.0
+    for _ in range(5):
+        trial_ls = log_sp + direction * 2.0
+        trial = single_objective(trial_ls, e, z, yy, n)
+        calls += 1
+        if not (trial["valid"] and trial["score"] < min_score):
+            break
+        log_sp = trial_ls
+        cur = trial
+        min_score = trial["score"]
+    return {"log_sp": np.array([log_sp]), "score": cur["score"], "rss": cur["rss"],
+            "edf": cur["edf"], "iterations": it, "calls": calls}
+
+
+# ---------------------------------------------------------------- multi
+
+def _augmented_svd(prep, log_sp):
+    lam = np.exp(log_sp)
+    B = np.vstack([math.sqrt(l) * r.T for l, r in zip(lam, prep.roots)])
+    A = np.vstack([prep.R, B])
+    U, d, Vt = np.linalg.svd(A, full_matrices=False)
+    r = int(np.count_nonzero(d >= d[0] * RANK_TOL))
+    return U[:prep.q, :r], Vt[:r, :].T, d[:r], lam
+
+
+def multi_core(prep, resp, log_sp):
+    U1, V, d, lam = _augmented_svd(prep, log_sp)
+    y1 = U1.T @ resp["y0"]
+    Uy = U1 @ y1
+    rss = resp["yy"] - 2.0 * float(y1 @ y1) + float(Uy @ Uy)
+    if rss < 0.0:
+        rss = 0.0
+    edf = float(np.sum(U1 * U1))
+    delta = prep.n - edf
+    if not (math.isfinite(rss) and math.isfinite(edf)) or delta <= 1e-8:
+        raise ValueError("invalid multi-penalty objective")
+    score = prep.n * rss / (delta * delta)
+    return {"U1": U1, "V": V, "d": d, "lam": lam, "y1": y1, "rss": rss,
+            "edf": edf, "score": score, "log_sp": np.array(log_sp, dtype=np.float64)}
+
+
+def multi_derivatives(prep, core):
+    """Analytic gradient and Hessian of V in rho = log(lambda)."""
+    U1, V, d, lam, y1 = core["U1"], core["V"], core["d"], core["lam"], core["y1"]
+    m = prep.m
+    P = U1.T @ U1
+    Ms = []
+    for root in prep.roots:
+        T = (V.T @ root) / d[:, None]
+        Ms.append(T @ T.T)
+    e1 = y1 - P @ y1
+    ddelta = np.array([lam[i] * np.trace(Ms[i] @ P) for i in range(m)])
+    drss = np.array([2.0 * lam[i] * float(e1 @ (Ms[i] @ y1)) for i in range(m)])
+    d2delta = np.zeros((m, m))
+    d2rss = np.zeros((m, m))
+    My = [M @ y1 for M in Ms]
+    for i in range(m):
+        for j in range(i + 1):
+            MiMj = Ms[i] @ Ms[j]
+            dd = -2.0 * lam[i] * lam[j] * np.trace(MiMj @ P)
+            rr = 2.0 * lam[i] * lam[j] * (float(My[j] @ (P @ My[i]))
+                                          - float(e1 @ (MiMj @ y1)) - float(e1 @ (Ms[j] @ My[i])))
+            if i == j:
+                dd += ddelta[i]
+                rr += drss[i]
+            d2delta[i, j] = d2delta[j, i] = dd
+            d2rss[i, j] = d2rss[j, i] = rr
+    n = prep.n
+    delta = n - core["edf"]
+    rss = core["rss"]
+    s1 = n / (delta * delta)
+    s2 = 2.0 * s1 * rss / delta
+    grad = s1 * drss - s2 * ddelta
+    hess = np.zeros((m, m))
+    for i in range(m):
+        for j in range(i + 1):
+            v = (-2.0 * s1 / delta * (ddelta[j] * drss[i] + ddelta[i] * drss[j])
+                 + s1 * d2rss[i, j] + 3.0 * s2 / delta * ddelta[i] * ddelta[j]
+                 - s2 * d2delta[i, j])
+            hess[i, j] = hess[j, i] = v
+    return grad, hess
+
+
+def optimize_multi(prep, resp, max_half=25):
+    m = prep.m
+    log_sp = np.log(prep.initial_sp)
+    cur = multi_core(prep, resp, log_sp)
+    grad_c, hess_c = multi_derivatives(prep, cur)
+    min_score = cur["score"]
+    score_red = 1e10
+    gradient = np.zeros(m)
+    newton = np.zeros(m)
+    steep = np.zeros(m)
+    steepest = False
+    converged = False
+    calls = 1
+    it = 0
+    for it in range(1, 401):
+        tries = 0
+        if it > 1:
+            step = (steep if steepest else newton).copy()
+            trying = True
+            while trying:
+                tries += 1
+                if tries == 4 and not steepest:
+                    steepest = True
+                    step = steep.copy()
+                trial_ls = log_sp + step
+                trial = multi_core(prep, resp, trial_ls)
+                calls += 1
+                if trial["score"] < min_score:
+                    trying = False
+                    score_red = min_score - trial["score"]
+                    min_score = trial["score"]
+                    log_sp = trial_ls
+                    cur = trial
+                    grad_c, hess_c = multi_derivatives(prep, cur)
+                else:
+                    step = step / 2.0
+                if tries == max_half - 1 and trying:
+                    step = np.zeros(m)
+                if tries == max_half:
+                    trying = False
+        if it > 3:
+            gnorm = float(np.sqrt(np.sum(gradient * gradient)))
+            converged = (score_red <= CONV_TOL * (1.0 + min_score)
+                         and gnorm <= CONV_TOL ** (1.0 / 3.0) * (1.0 + abs(min_score)))
+            if tries == max_half:
+                converged = True
+        gradient = grad_c.copy()
+        w, v = np.linalg.eigh(hess_c)
+        steepest = bool(np.any(w < 0.0))
+        if not steepest:
+            newton = -(v @ ((v.T @ gradient) / w))
+            mx = np.max(np.abs(newton))
+            if mx > 5.0:
+                newton = newton * (5.0 / mx)
+        mg = np.max(np.abs(gradient))
+        steep = np.zeros(m) if mg == 0.0 else -gradient / mg
+        if converged:
+            break
+    if not converged:
+        raise ValueError("multi-penalty optimizer hit its iteration limit")
+    for c in range(m):
+        direction = 1.0 if gradient[c] < 0.0 else -1.0
+        for _ in range(5):
+            step = np.zeros(m)
+            step[c] = direction * 2.0
+            trial_ls = log_sp + step
+            trial = multi_core(prep, resp, trial_ls)
+            calls += 1
+            if not trial["score"] < min_score:
+                break
+            log_sp = trial_ls
+            cur = trial
+            min_score = cur["score"]
+    return {"log_sp": log_sp, "score": cur["score"], "rss": cur["rss"],
+            "edf": cur["edf"], "iterations": it, "calls": calls}
+
+
+def residual_at(prep, resp, log_sp):
+    """y - A(lambda) y through the augmented SVD."""
+    core = multi_core(prep, resp, np.asarray(log_sp, dtype=np.float64))
+    fitted = prep.Q @ (core["U1"] @ core["y1"])
+    return resp["y"] - fitted
+
+
+def fit(prep, y):
+    """Select lambda by GCV and return (residual, info)."""
+    resp = prep.response(y)
+    info = optimize_single(prep, resp) if prep.m == 1 else optimize_multi(prep, resp)
+    return residual_at(prep, resp, info["log_sp"]), info
+
+
+def gcv_value_grad_hess(prep, y, log_sp):
+    """V, analytic gradient and full Hessian at rho (multi or single)."""
+    resp = prep.response(y)
+    core = multi_core(prep, resp, np.asarray(log_sp, dtype=np.float64))
+    g, H = multi_derivatives(prep, core)
+    return core["score"], g, H

@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""CI tests/s of one skeleton level batch on B200: batched vs plain per-test.
+
+Workload: the single-level CI batch -- n=500, p=50 nonlinear SEM (edge prob
+0.08), 4096 (x, y, S) triples with |S| uniform on 0..4 (thin-plate smooths for
+|S| <= 2, additive above), regrXonS residuals by GCV + dcc.gamma p-values
+(exact screen, low-rank refinement in the [0.05, 0.15] guard band), FP64.
+A step is one pass of the whole batch (fit, residuals, statistics, p-values).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line.  ``value``: batched tests/s with every input resident in
+HBM (CUDA events on the engine stream over exactly K replays of the captured
+level graph, max over ranks).  ``e2e``: the public call fkpc_ci_level_batch
+with host data in and records out (design set-up, uploads and downloads
+inside the timed region).  ``plain``: the plain per-test GPU form (one launch
+set and a synchronisation per test) on a sample of the same batch.
+``--impl reference`` times the reference algorithm's CPU restatement (the
+oracle) on the host cores with a bounded sample per step.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CI tests/s batched vs plain at n=500; 351x48 skeleton wall-s vs host CPU"
+UNIT = "CI tests/s"
+WORKLOAD = "level batch n=500 p=50 SEM edge 0.08, 4096 triples |S|~U{0..4}, dcc.gamma, FP64"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--count", type=int, default=4096)
+    ap.add_argument("--plain-sample", type=int, default=256)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, value, local):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, value, local):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ------------------------------------------------------------ CPU baseline
+
+def _oracle_chunk(payload):
+    """Worker: oracle p-values for a list of triples (spawned process)."""
+    sys.path.insert(0, ROOT)
+    from oracle import skeleton
+    X, triples = payload
+    cache = skeleton.ResidualCache(X)
+    return [skeleton.ci_pvalue(cache, "dcc.gamma", x, y, S) for (x, y, S) in triples]
+
+
+def cpu_oracle_rate(X, triples, budget_s, cores):
+    """Oracle throughput on the host cores over a bounded sample (tests/s)."""
+    import multiprocessing as mp
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"  # one BLAS thread per worker process: the pool supplies the parallelism
+    ctx = mp.get_context("spawn")
+    per = max(1, int(math.ceil(budget_s * 4.0)))  # ~0.25 s per test per core on this workload
+    sample = triples[:min(len(triples), per * cores)]
+    chunks = [sample[i::cores] for i in range(cores)]
+    chunks = [c for c in chunks if c]
+    with ctx.Pool(len(chunks)) as pool:
+        pool.map(_oracle_chunk, [(X, [c[0]]) for c in chunks])  # import / start-up outside the timing
+        t0 = time.perf_counter()
+        pool.map(_oracle_chunk, [(X, c) for c in chunks])
+        dt = time.perf_counter() - t0
+    return len(sample) / dt, len(sample), dt
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------ reference arm
+
+def run_reference(args, world, rank):
+    from fastkpc_b200 import workloads
+    if rank != 0:
+        return
+    X, triples = workloads.level_batch_500x50(count=args.count)
+    cores = host_cores()
+    per_step = 2 * cores
+    rates = []
+    offset = 0
+    for step in range(args.warmup + args.steps):
+        sample = [triples[(offset + i) % len(triples)] for i in range(per_step)]
+        offset += per_step
+        rate, count, dt = cpu_oracle_rate(X, sample, budget_s=per_step / cores / 4.0, cores=cores)
+        if step >= args.warmup:
+            rates.append((count, dt))
+    total = sum(c for c, _ in rates)
+    secs = sum(d for _, d in rates)
+    value = total / secs
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(1, args.steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "n": 500, "p": 50, "triples": args.count,
+                                              "ci_method": "dcc.gamma", "sample_per_step": per_step},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{per_step} triples per step of the {args.count}-triple batch, "
+                                       f"numpy oracle restatement in {cores} spawned processes"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------ our arm
+
+def run_ours(args, world, rank, local, pg):
+    import fastkpc_b200 as fk
+    from fastkpc_b200 import workloads
+    X, triples = workloads.level_batch_500x50(seed=2 + 10 * rank, count=args.count)
+
+    # batched form, inputs resident
+    batch = fk.StagedBatch(X, triples, device=local)
+    batch.execute(args.warmup)
+    barrier(pg)
+    with ClockSampler(local) as clocks:
+        ms = batch.execute(args.steps)
+    barrier(pg)
+    ms = max_over_ranks(pg, ms, local)
+    recs, st = batch.collect()
+    if not np.all(recs["status"] == 0):
+        raise RuntimeError("batched form returned failing records")
+    total_tests = sum_over_ranks(pg, float(args.count * args.steps), local)
+    value = total_tests / (ms / 1e3)
+
+    # roofline of the dominant kernel (replayed alone, CUDA events)
+    stages = ["fit_single", "fit_multi_small", "fit_multi_large", "dcov_components", "dcov_pairs",
+              "lowrank_eigen", "lowrank_pairs"]
+    timed = {}
+    for s in stages:
+        avg, fl = batch.time_stage(s, repeats=3)
+        timed[s] = (avg, fl)
+    dominant = max(timed, key=lambda s: timed[s][0])
+    peak = fk.measure_fp64_peak(local)
+    avg_ms, flops = timed[dominant]
+    achieved = flops / (avg_ms * 1e-3) / 1e12 if flops > 0 else None
+
+    # plain per-test form on a sample of the same batch (designs resident)
+    sample = triples[:args.plain_sample]
+    plain = fk.StagedBatch(X, sample, device=local, mode="plain")
+    plain.execute(1)
+    plain_ms = plain.execute(1)
+    prec, _ = plain.collect()
+    plain_rate = len(sample) / (plain_ms / 1e3)
+
+    # end to end through the public call: host data in, records out
+    e2e_t = []
+    e2e_stats = None
+    for _ in range(max(1, args.e2e_steps)):
+        t0 = time.perf_counter()
+        rec, e2e_stats = fk.ci_level_batch(X, triples, device=local)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_value = args.count / statistics.median(e2e_t)
+    e2e_value = sum_over_ranks(pg, e2e_value, local)
+
+    clocks_s = clocks.summary()
+    line = None
+    if rank == 0:
+        cores = host_cores()
+        cpu_rate, cpu_n, cpu_dt = cpu_oracle_rate(X, triples, args.cpu_seconds / 4.0, cores)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": 500, "p": 50, "triples_per_gpu": args.count,
+                       "ci_method": "dcc.gamma", "parallelism": f"replicas x{world} (independent level batches)",
+                       "l2": "inputs larger than L2 (design arena > 126 MB per step)",
+                       "designs": st["designs"], "fits": st["targets"], "guarded": st["guarded"]},
+            "plain": {"value": plain_rate, "unit": UNIT, "sample_tests": len(sample),
+                      "batched_over_plain": value / world / plain_rate},
+            "stages_ms": {s: timed[s][0] for s in stages},
+            "roofline": {"bound": "fp64", "kernel": dominant, "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "peak_source": "measured live: FP64 FMA probe (no FP64 figure in MEASURED_PEAKS.json)",
+                         "flops_per_launch": flops, "avg_launch_ms": avg_ms},
+            "cpu_baseline": {"value": cpu_rate, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"first {cpu_n} triples of the batch, numpy oracle in {cores} spawned "
+                                       f"processes ({cpu_dt:.1f} s)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": e2e_stats["h2d_bytes"],
+                    "d2h_bytes_per_step": e2e_stats["d2h_bytes"], "steps": len(e2e_t),
+                    "setup_ms": e2e_stats["setup_ms"], "wall_s": statistics.median(e2e_t)},
+            "gpu_launches": int(st["kernel_launches"]) * args.steps,
+            "clocks": clocks_s,
+        }
+    return line
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+            return
+        line = run_ours(args, world, rank, local, pg)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,432 @@
+"""fastkpc_b200 -- B200-native conditional-independence path of the kernel-PC skeleton.
+
+Python host over the library's C ABI (``include/fastkpc_b200.h``).  The entry
+point ``fastkpc_compatible_cuda_skeleton`` mirrors the reference facade of the
+same name (fastkpc/R/fast_kpc.R:56-130 -> precision_run_skeleton_full_cuda_native,
+fastkpc/R/cuda_native.R:2237-2311): same option names and meaning, same
+fail-closed errors.  Indices are 0-based here (the R facade is 1-based).
+
+The compute runs in ``libfastkpc_b200.so`` (CUDA, sm_100a).  There is no CPU
+fallback: importing works without a GPU, but every compute call raises
+``FkpcError`` when no CUDA device is present, and loading fails loudly when
+the shared library has not been built (``python -m fastkpc_b200.build``).
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+__all__ = [
+    "FkpcError", "library_path", "load_library", "fastkpc_compatible_cuda_skeleton",
+    "ci_level_batch", "ci_plain_one", "regress_batch", "stat_batch", "design_export",
+    "METHODS",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+METHODS = {"dcc.gamma": 0, "dcc.perm": 1, "hsic.gamma": 2, "hsic.perm": 3}
+MODES = {"batched": 0, "plain": 1}
+FLAG_GUARDED = 1
+FLAG_DIRECT = 2
+
+STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-finite numerics",
+                4: "iteration limit", 5: "rank deficiency", 6: "allocation failure", 7: "no CUDA device"}
+
+
+class FkpcError(RuntimeError):
+    """A library call failed; ``status`` is the FKPC_STATUS_* code."""
+
+    def __init__(self, status, message):
+        super().__init__(f"{message} (status {status}: {STATUS_NAMES.get(status, '?')})")
+        self.status = status
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("alpha", ctypes.c_double), ("index", ctypes.c_double), ("num_col", ctypes.c_int),
+                ("max_conditioning_size", ctypes.c_int), ("ci_method", ctypes.c_int),
+                ("hsic_sig", ctypes.c_double), ("permutation_replicates", ctypes.c_int),
+                ("has_seed", ctypes.c_int), ("seed", ctypes.c_uint), ("mode", ctypes.c_int),
+                ("collect_trace", ctypes.c_int), ("device", ctypes.c_int), ("strict", ctypes.c_int)]
+
+
+class CiRecord(ctypes.Structure):
+    _fields_ = [("p_value", ctypes.c_double), ("p_exact", ctypes.c_double), ("statistic", ctypes.c_double),
+                ("mean", ctypes.c_double), ("variance", ctypes.c_double), ("status", ctypes.c_int),
+                ("flags", ctypes.c_uint)]
+
+
+class StageStats(ctypes.Structure):
+    _fields_ = [("setup_ms", ctypes.c_double), ("upload_ms", ctypes.c_double), ("fit_ms", ctypes.c_double),
+                ("statistic_ms", ctypes.c_double), ("refine_ms", ctypes.c_double),
+                ("download_ms", ctypes.c_double), ("total_ms", ctypes.c_double), ("designs", ctypes.c_int),
+                ("targets", ctypes.c_int), ("pairs", ctypes.c_int), ("guarded", ctypes.c_int),
+                ("kernel_launches", ctypes.c_int), ("h2d_bytes", ctypes.c_double), ("d2h_bytes", ctypes.c_double),
+                ("fit_evaluations", ctypes.c_double), ("fit_flops", ctypes.c_double),
+                ("statistic_flops", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class TraceRow(ctypes.Structure):
+    _fields_ = [("level", ctypes.c_int), ("task_index", ctypes.c_int), ("edge_x", ctypes.c_int),
+                ("edge_y", ctypes.c_int), ("x", ctypes.c_int), ("y", ctypes.c_int), ("s_offset", ctypes.c_int),
+                ("s_count", ctypes.c_int), ("p_value", ctypes.c_double), ("p_exact", ctypes.c_double),
+                ("deleted", ctypes.c_int), ("flags", ctypes.c_uint)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("p", ctypes.c_int), ("levels", ctypes.c_int),
+                ("adjacency", ctypes.POINTER(ctypes.c_int)), ("pmax", ctypes.POINTER(ctypes.c_double)),
+                ("sepset_offsets", ctypes.POINTER(ctypes.c_int)), ("sepset_values", ctypes.POINTER(ctypes.c_int)),
+                ("n_edgetests", ctypes.POINTER(ctypes.c_int)), ("trace_rows", ctypes.c_int),
+                ("trace", ctypes.POINTER(TraceRow)), ("trace_s_values", ctypes.POINTER(ctypes.c_int)),
+                ("elapsed_sec", ctypes.c_double), ("stats", StageStats)]
+
+
+_lib = None
+
+_P = ctypes.POINTER
+_DBL = _P(ctypes.c_double)
+_INT = _P(ctypes.c_int)
+
+_SIGNATURES = {
+    "fkpc_abi_version": (ctypes.c_int, []),
+    "fkpc_last_error": (ctypes.c_char_p, []),
+    "fkpc_default_options": (None, [_P(Options)]),
+    "fkpc_skeleton_run": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _P(Options), _P(_P(Result))]),
+    "fkpc_result_free": (None, [_P(Result)]),
+    "fkpc_ci_level_batch": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, _INT, ctypes.c_int,
+                                           _P(Options), _P(CiRecord), _P(StageStats)]),
+    "fkpc_ci_plain_one": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _INT,
+                                         ctypes.c_int, _P(Options), _P(CiRecord)]),
+    "fkpc_regress_batch": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, ctypes.c_int,
+                                          _P(Options), _DBL, _DBL, ctypes.c_int, _INT]),
+    "fkpc_stat_batch": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, ctypes.c_int, _INT,
+                                       _P(Options), _P(CiRecord)]),
+    "fkpc_gcv_adjoint": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, ctypes.c_int, _INT, ctypes.c_int,
+                                        ctypes.c_int, _DBL, _DBL, _DBL, _DBL, _DBL]),
+    "fkpc_batch_prepare": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, _INT, ctypes.c_int,
+                                          _P(Options)]),
+    "fkpc_batch_execute": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _DBL]),
+    "fkpc_batch_collect": (ctypes.c_int, [ctypes.c_int, _P(CiRecord), _P(StageStats)]),
+    "fkpc_batch_time_stage": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _DBL, _DBL]),
+    "fkpc_measure_fp64_peak": (ctypes.c_int, [ctypes.c_int, _DBL]),
+    "fkpc_design_export": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, ctypes.c_int, _INT, _INT, _DBL,
+                                          _DBL, _DBL]),
+}
+
+
+def library_path():
+    return os.path.join(_HERE, "libfastkpc_b200.so")
+
+
+def load_library():
+    """Load the CUDA library; raises ImportError when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise ImportError(f"fastkpc_b200 CUDA library not built: {path} is missing "
+                          "(run `python -m fastkpc_b200.build`)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != 0:
+        msg = load_library().fkpc_last_error().decode("utf-8", errors="replace")
+        raise FkpcError(rc, msg)
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(_P(ctype))
+
+
+def _as_data(data):
+    a = np.asarray(data, dtype=np.float64)
+    if a.ndim != 2:
+        raise ValueError("data must be a 2-D matrix")
+    return np.asfortranarray(a)
+
+
+def make_options(ci_method="dcc.gamma", alpha=0.1, index=1.0, numCol=35, max_conditioning_size=math.inf,
+                 hsic_sig=1.0, replicates=100, seed=None, mode="batched", trace=True, device=0, strict=True):
+    o = Options()
+    load_library().fkpc_default_options(ctypes.byref(o))
+    if ci_method not in METHODS:
+        raise ValueError(f"unknown ci_method {ci_method!r}")
+    o.alpha = float(alpha)
+    o.index = float(index)
+    o.num_col = int(numCol)
+    o.max_conditioning_size = -1 if math.isinf(max_conditioning_size) else int(max_conditioning_size)
+    o.ci_method = METHODS[ci_method]
+    o.hsic_sig = float(hsic_sig)
+    o.permutation_replicates = int(replicates)
+    o.has_seed = 0 if seed is None else 1
+    o.seed = 0 if seed is None else int(seed) & 0xFFFFFFFF
+    o.mode = MODES[mode]
+    o.collect_trace = 1 if trace else 0
+    o.device = int(device)
+    o.strict = 1 if strict else 0
+    return o
+
+
+_ALLOWED = {"max_conditioning_size", "index", "numCol", "trace_level", "route", "compatible_cuda_strict",
+            "ci_method", "hsic_params", "permutation_params", "mode", "device"}
+
+
+def fastkpc_compatible_cuda_skeleton(data, alpha, labels=None, options=None):
+    """Kernel-PC skeleton with the full-CUDA CI route.
+
+    ``options`` keys follow the reference facade: ``max_conditioning_size``
+    (default Inf), ``index`` (1), ``numCol`` (default floor(n/10) as in the
+    reference; the strict envelope requires 35), ``trace_level``
+    ("summary" | "logical" | "full" | "none"), ``route`` ("full_cuda"),
+    ``compatible_cuda_strict`` (True), ``ci_method`` ("dcc.gamma",
+    "dcc.perm", "hsic.gamma", "hsic.perm"), ``hsic_params`` ({"sig": 1}),
+    ``permutation_params`` ({"replicates": 100, "seed": None,
+    "include_observed": True}); plus ``mode`` ("batched" | "plain") and
+    ``device``.
+
+    Returns a dict with ``adjacency`` (bool p x p), ``pMax``, ``sepsets``
+    (list of p lists; None or the separating set, 0-based), ``n_edgetests``,
+    ``tasks`` (the logical trace as column arrays), ``summary``.
+    """
+    options = dict(options or {})
+    unknown = set(options) - _ALLOWED
+    if unknown:
+        raise ValueError("unknown compatible CUDA option(s): " + ",".join(sorted(unknown)))
+    if options.get("route", "full_cuda") != "full_cuda":
+        raise ValueError("only route = 'full_cuda' is provided by this library")
+    X = _as_data(data)
+    n, p = X.shape
+    labels = list(labels) if labels is not None else [f"V{i + 1}" for i in range(p)]
+    if len(labels) != p:
+        raise ValueError("labels must have one entry per column")
+    trace_level = options.get("trace_level", "summary")
+    if trace_level not in ("summary", "logical", "full", "none"):
+        raise ValueError("trace_level must be summary, logical, full or none")
+    hsic = options.get("hsic_params") or {"sig": 1}
+    perm = options.get("permutation_params") or {"replicates": 100, "seed": None, "include_observed": True}
+    if not perm.get("include_observed", True):
+        raise ValueError("strict permutation p-values require include_observed = TRUE")
+    method = options.get("ci_method", "dcc.gamma")
+    if method in ("dcc.perm", "hsic.perm") and perm.get("seed") is None:
+        raise ValueError("strict compatible CUDA permutation methods require an explicit seed")
+    o = make_options(ci_method=method, alpha=alpha, index=options.get("index", 1),
+                     numCol=options.get("numCol", n // 10),
+                     max_conditioning_size=options.get("max_conditioning_size", math.inf),
+                     hsic_sig=hsic.get("sig", 1), replicates=perm.get("replicates", 100), seed=perm.get("seed"),
+                     mode=options.get("mode", "batched"), trace=trace_level in ("logical", "full"),
+                     device=options.get("device", 0), strict=options.get("compatible_cuda_strict", True))
+    lib = load_library()
+    res = _P(Result)()
+    _check(lib.fkpc_skeleton_run(_ptr(X, ctypes.c_double), n, p, ctypes.byref(o), ctypes.byref(res)))
+    try:
+        r = res.contents
+        adj = np.ctypeslib.as_array(r.adjacency, shape=(p * p,)).reshape((p, p), order="F").astype(bool)
+        pmax = np.ctypeslib.as_array(r.pmax, shape=(p * p,)).reshape((p, p), order="F").copy()
+        offs = np.ctypeslib.as_array(r.sepset_offsets, shape=(p * p + 1,)).copy()
+        nvals = int(offs[-1])
+        vals = np.ctypeslib.as_array(r.sepset_values, shape=(max(nvals, 1),))[:nvals].copy()
+        sepsets = [[None] * p for _ in range(p)]
+        for j in range(p):
+            for i in range(p):
+                cell = i + p * j
+                if offs[cell + 1] > offs[cell] or _deleted(adj, i, j):
+                    s = [int(v) for v in vals[offs[cell]:offs[cell + 1]]]
+                    sepsets[i][j] = s if (offs[cell + 1] > offs[cell] or not adj[i, j]) else None
+        for i in range(p):
+            for j in range(p):
+                if adj[i, j] or i == j:
+                    sepsets[i][j] = None
+        n_edgetests = [int(r.n_edgetests[k]) for k in range(r.levels)]
+        tasks = None
+        if r.trace and r.trace_rows > 0:
+            rows = [r.trace[k] for k in range(r.trace_rows)]
+            svals = r.trace_s_values
+            tasks = {
+                "level": np.array([t.level for t in rows]), "task_index": np.array([t.task_index for t in rows]),
+                "edge_x": np.array([t.edge_x for t in rows]), "edge_y": np.array([t.edge_y for t in rows]),
+                "x": np.array([t.x for t in rows]), "y": np.array([t.y for t in rows]),
+                "S": [[int(svals[t.s_offset + k]) for k in range(t.s_count)] for t in rows],
+                "p_used": np.array([t.p_value for t in rows]), "p_exact": np.array([t.p_exact for t in rows]),
+                "native_edge_deleted": np.array([bool(t.deleted) for t in rows]),
+                "guarded": np.array([bool(t.flags & FLAG_GUARDED) for t in rows]),
+            }
+        stats = r.stats.as_dict()
+        summary = {"n": n, "p": p, "alpha": float(alpha), "ci_method": method, "levels": r.levels,
+                   "tests_replayed": int(sum(n_edgetests)), "elapsed_sec": r.elapsed_sec, "labels": labels,
+                   "max_conditioning_size_resolved": (p - 2 if o.max_conditioning_size < 0
+                                                      else min(o.max_conditioning_size, p - 2)),
+                   "stages": stats, "entrypoint": "fkpc_skeleton_run"}
+        return {"adjacency": adj, "pMax": pmax, "sepsets": sepsets, "n_edgetests": n_edgetests,
+                "tasks": tasks, "summary": summary}
+    finally:
+        lib.fkpc_result_free(res)
+
+
+def _deleted(adj, i, j):
+    return i != j and not adj[i, j]
+
+
+def _tests_arrays(tests):
+    xs = np.array([t[0] for t in tests], dtype=np.int32)
+    ys = np.array([t[1] for t in tests], dtype=np.int32)
+    offs = np.zeros(len(tests) + 1, dtype=np.int32)
+    vals = []
+    for k, t in enumerate(tests):
+        vals.extend(int(v) for v in t[2])
+        offs[k + 1] = len(vals)
+    return xs, ys, offs, np.array(vals if vals else [0], dtype=np.int32)
+
+
+def _records(recs):
+    return {name: np.array([getattr(r, name) for r in recs]) for name, _ in CiRecord._fields_}
+
+
+def ci_level_batch(data, tests, ci_method="dcc.gamma", mode="batched", **kw):
+    """Evaluate CI tests ``[(x, y, S), ...]``; returns (records dict, stage stats dict)."""
+    X = _as_data(data)
+    n, p = X.shape
+    o = make_options(ci_method=ci_method, mode=mode, **kw)
+    xs, ys, offs, vals = _tests_arrays(tests)
+    out = (CiRecord * max(1, len(tests)))()
+    st = StageStats()
+    _check(load_library().fkpc_ci_level_batch(_ptr(X, ctypes.c_double), n, p, _ptr(xs, ctypes.c_int),
+                                                _ptr(ys, ctypes.c_int), _ptr(offs, ctypes.c_int),
+                                                _ptr(vals, ctypes.c_int), len(tests), ctypes.byref(o), out,
+                                                ctypes.byref(st)))
+    return _records(out[:len(tests)]), st.as_dict()
+
+
+def ci_plain_one(data, x, y, S, ci_method="dcc.gamma", **kw):
+    """One CI test through the plain per-test form; returns a record dict."""
+    X = _as_data(data)
+    n, p = X.shape
+    o = make_options(ci_method=ci_method, mode="plain", **kw)
+    s = np.array(list(S) if S else [0], dtype=np.int32)
+    rec = CiRecord()
+    _check(load_library().fkpc_ci_plain_one(_ptr(X, ctypes.c_double), n, p, int(x), int(y),
+                                              _ptr(s, ctypes.c_int), len(S), ctypes.byref(o),
+                                              ctypes.byref(rec)))
+    return {name: getattr(rec, name) for name, _ in CiRecord._fields_}
+
+
+def regress_batch(data, fits, max_penalties=8, device=0):
+    """regrXonS residuals for ``[(target, S), ...]``: (residuals n x k, log_sp k x m, status k)."""
+    X = _as_data(data)
+    n, p = X.shape
+    k = len(fits)
+    tg = np.array([f[0] for f in fits], dtype=np.int32)
+    offs = np.zeros(k + 1, dtype=np.int32)
+    vals = []
+    for i, f in enumerate(fits):
+        vals.extend(int(v) for v in f[1])
+        offs[i + 1] = len(vals)
+    vals = np.array(vals if vals else [0], dtype=np.int32)
+    resid = np.zeros((n, k), dtype=np.float64, order="F")
+    lsp = np.zeros((k, max_penalties), dtype=np.float64)
+    status = np.zeros(k, dtype=np.int32)
+    o = make_options(device=device)
+    _check(load_library().fkpc_regress_batch(_ptr(X, ctypes.c_double), n, p, _ptr(tg, ctypes.c_int),
+                                               _ptr(offs, ctypes.c_int), _ptr(vals, ctypes.c_int), k,
+                                               ctypes.byref(o), _ptr(resid, ctypes.c_double),
+                                               _ptr(lsp, ctypes.c_double), max_penalties,
+                                               _ptr(status, ctypes.c_int)))
+    return resid, lsp, status
+
+
+def stat_batch(residuals, pairs, ci_method="dcc.gamma", permutations=None, **kw):
+    """Statistics for ``[(left, right), ...]`` columns of ``residuals`` (n x m)."""
+    R = np.asfortranarray(np.asarray(residuals, dtype=np.float64))
+    n, m = R.shape
+    left = np.array([a for a, _ in pairs], dtype=np.int32)
+    right = np.array([b for _, b in pairs], dtype=np.int32)
+    o = make_options(ci_method=ci_method, **kw)
+    perm_ptr = None
+    if permutations is not None:
+        perms = np.ascontiguousarray(permutations, dtype=np.int32)
+        perm_ptr = _ptr(perms, ctypes.c_int)
+    out = (CiRecord * max(1, len(pairs)))()
+    _check(load_library().fkpc_stat_batch(_ptr(R, ctypes.c_double), n, m, _ptr(left, ctypes.c_int),
+                                            _ptr(right, ctypes.c_int), len(pairs), perm_ptr, ctypes.byref(o), out))
+    return _records(out[:len(pairs)])
+
+
+STAGES = {"fit_single": 0, "fit_multi_small": 1, "fit_multi_large": 2, "dcov_components": 3, "dcov_pairs": 4,
+          "hsic_components": 5, "hsic_pairs": 6, "lowrank_eigen": 7, "lowrank_pairs": 8}
+
+
+class StagedBatch:
+    """Prepared level batch on one device: every input resident in HBM.
+
+    ``execute(k)`` replays the captured launch sequence k times and returns the
+    CUDA-event device time; ``collect()`` waits and returns (records, stats);
+    ``time_stage(name, k)`` replays one kernel alone (mean ms, flops/launch).
+    """
+
+    def __init__(self, data, tests, ci_method="dcc.gamma", device=0, **kw):
+        X = _as_data(data)
+        n, p = X.shape
+        self.device = device
+        self.count = len(tests)
+        o = make_options(ci_method=ci_method, device=device, **kw)
+        xs, ys, offs, vals = _tests_arrays(tests)
+        _check(load_library().fkpc_batch_prepare(_ptr(X, ctypes.c_double), n, p, _ptr(xs, ctypes.c_int),
+                                                   _ptr(ys, ctypes.c_int), _ptr(offs, ctypes.c_int),
+                                                   _ptr(vals, ctypes.c_int), len(tests), ctypes.byref(o)))
+
+    def execute(self, repeats=1):
+        ms = ctypes.c_double()
+        _check(load_library().fkpc_batch_execute(self.device, int(repeats), ctypes.byref(ms)))
+        return ms.value
+
+    def collect(self):
+        out = (CiRecord * self.count)()
+        st = StageStats()
+        _check(load_library().fkpc_batch_collect(self.device, out, ctypes.byref(st)))
+        return _records(out[:self.count]), st.as_dict()
+
+    def time_stage(self, stage, repeats=3):
+        ms = ctypes.c_double()
+        fl = ctypes.c_double()
+        _check(load_library().fkpc_batch_time_stage(self.device, STAGES[stage], int(repeats), ctypes.byref(ms),
+                                                      ctypes.byref(fl)))
+        return ms.value, fl.value
+
+
+def measure_fp64_peak(device=0):
+    """Measured FP64 FMA throughput of the device, TFLOP/s."""
+    t = ctypes.c_double()
+    _check(load_library().fkpc_measure_fp64_peak(int(device), ctypes.byref(t)))
+    return t.value
+
+
+def design_export(data, S):
+    """Host design set-up for S: dict(X, penalties (m x q x q), initial_log_sp)."""
+    X = _as_data(data)
+    n, p = X.shape
+    s = np.array(sorted(S), dtype=np.int32)
+    q = ctypes.c_int()
+    m = ctypes.c_int()
+    lib = load_library()
+    _check(lib.fkpc_design_export(_ptr(X, ctypes.c_double), n, p, _ptr(s, ctypes.c_int), len(s),
+                                  ctypes.byref(q), ctypes.byref(m), None, None, None))
+    Xd = np.zeros((n, q.value), order="F")
+    pen = np.zeros((m.value, q.value, q.value))
+    pen_f = np.zeros(m.value * q.value * q.value)
+    lsp = np.zeros(m.value)
+    _check(lib.fkpc_design_export(_ptr(X, ctypes.c_double), n, p, _ptr(s, ctypes.c_int), len(s),
+                                  ctypes.byref(q), ctypes.byref(m), _ptr(Xd, ctypes.c_double),
+                                  _ptr(pen_f, ctypes.c_double), _ptr(lsp, ctypes.c_double)))
+    for j in range(m.value):
+        pen[j] = pen_f[j * q.value * q.value:(j + 1) * q.value * q.value].reshape((q.value, q.value), order="F")
+    return {"X": np.asarray(Xd), "penalties": pen, "initial_log_sp": lsp, "q": q.value, "m": m.value}

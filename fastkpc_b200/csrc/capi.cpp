@@ -1,0 +1,546 @@
+// C ABI of the library and the skeleton runner.
+//
+// Skeleton semantics (pcalg "stable", as replayed by the reference in
+// fastkpc/src/full_cuda_ci_one_call.cpp:5229-5579 over the plan of
+// fastkpc/src/skeleton_task_scheduler.cpp:70-132):
+//  * level plan: for each edge x < y of the level-start adjacency, the x-side
+//    tasks (S over combinations of adj(x)\{y} of size ``level``, in
+//    lexicographic order) then the y-side tasks; a side's first task "opens
+//    the next level" when the side has more than ``level`` neighbours;
+//  * per edge the tasks count in plan order up to and including the first
+//    deleting one (p >= alpha); pMax keeps the max p per edge, the deleting
+//    S becomes the sepset, deletions apply at level end; the run stops after
+//    a level where no counted task opens the next level, or past m.max.
+// The batched form evaluates every planned task of a level in one batch
+// (tests are independent given the level-start graph) and then replays; the
+// counted tests, graph, sepsets and trace are those of the sequential order.
+// Permutation methods draw their tables from one R-compatible stream in
+// pcalg order (x, y, S lexicographic) over the counted tests, so they run one
+// test at a time in that order.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fastkpc_b200.h"
+#include "runtime.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+std::mutex g_engine_mu;
+std::map<int, std::unique_ptr<fkpc::Engine>> g_engines;
+
+fkpc::Engine& engine_for(int device) {
+  auto it = g_engines.find(device);
+  if (it == g_engines.end()) {
+    it = g_engines.emplace(device, std::unique_ptr<fkpc::Engine>(new fkpc::Engine(device))).first;
+  }
+  return *it->second;
+}
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return FKPC_OK;
+  } catch (const fkpc::Error& e) {
+    return fail(e.code, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(FKPC_STATUS_ALLOCATION, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(FKPC_STATUS_INVALID_ARGUMENT, e.what());
+  }
+}
+
+void validate_options(const fkpc_options& o, int n, int p) {
+  using fkpc::Error;
+  if (!(std::isfinite(o.alpha) && o.alpha > 0.0 && o.alpha < 1.0))
+    throw Error(FKPC_STATUS_INVALID_ARGUMENT, "alpha must lie in (0, 1)");
+  if (o.index != 1.0) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "index must be 1 (legacy dCov semantics)");
+  if (o.num_col < 1 || o.num_col > 64 || o.num_col >= n)
+    throw Error(FKPC_STATUS_INVALID_ARGUMENT, "numCol must lie in [1, min(64, n - 1)]");
+  if (o.ci_method < FKPC_DCC_GAMMA || o.ci_method > FKPC_HSIC_PERM)
+    throw Error(FKPC_STATUS_INVALID_ARGUMENT, "unknown CI method");
+  if (!(std::isfinite(o.hsic_sig) && o.hsic_sig > 0.0))
+    throw Error(FKPC_STATUS_INVALID_ARGUMENT, "HSIC sig must be positive and finite");
+  if (o.ci_method == FKPC_DCC_PERM || o.ci_method == FKPC_HSIC_PERM) {
+    if (!o.has_seed) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "permutation methods require a seed");
+    if (o.permutation_replicates < 1 || o.permutation_replicates > 10000)
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "permutation replicates must lie in [1, 10000]");
+    if (n > 32768) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "permutation methods support n <= 32768");
+  }
+  if (o.mode != FKPC_MODE_BATCHED && o.mode != FKPC_MODE_PLAIN)
+    throw Error(FKPC_STATUS_INVALID_ARGUMENT, "unknown execution mode");
+  if (p < 2 || n <= 5) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "need n > 5 and p >= 2");
+  if (o.strict) {
+    // the qualified envelope of fastkpc/src/full_cuda_ci_one_call.cpp:5052-5087
+    if (std::fabs(o.alpha - 0.1) > 1e-15) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "strict mode requires alpha = 0.1");
+    if (o.num_col != 35) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "strict mode requires numCol = 35");
+    if (p > 64) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "strict mode requires 2 <= p <= 64");
+  }
+}
+
+struct Task {
+  int edge_x, edge_y, x, y;
+  std::vector<int> S;
+  bool opens;
+};
+
+std::vector<Task> make_layer_plan(const std::vector<int>& adj, int p, int level) {
+  std::vector<Task> tasks;
+  auto nbrs = [&](int v, int excl) {
+    std::vector<int> out;
+    for (int i = 0; i < p; ++i)
+      if (i != excl && adj[i + static_cast<size_t>(p) * v]) out.push_back(i);
+    return out;
+  };
+  for (int x = 0; x < p - 1; ++x)
+    for (int y = x + 1; y < p; ++y) {
+      if (!adj[x + static_cast<size_t>(p) * y]) continue;
+      for (int side = 0; side < 2; ++side) {
+        const int a = side == 0 ? x : y, b = side == 0 ? y : x;
+        const std::vector<int> nb = nbrs(a, b);
+        if (static_cast<int>(nb.size()) < level) continue;
+        std::vector<int> idx(level);
+        for (int i = 0; i < level; ++i) idx[i] = i;
+        bool first = true;
+        for (;;) {
+          Task t;
+          t.edge_x = x;
+          t.edge_y = y;
+          t.x = a;
+          t.y = b;
+          for (int i = 0; i < level; ++i) t.S.push_back(nb[idx[i]]);
+          t.opens = first && static_cast<int>(nb.size()) > level;
+          first = false;
+          tasks.push_back(std::move(t));
+          int i = level - 1;
+          while (i >= 0 && idx[i] == static_cast<int>(nb.size()) - level + i) --i;
+          if (i < 0) break;
+          ++idx[i];
+          for (int j = i + 1; j < level; ++j) idx[j] = idx[j - 1] + 1;
+        }
+      }
+    }
+  return tasks;
+}
+
+struct Run {
+  int n = 0, p = 0;
+  std::vector<int> adj;
+  std::vector<double> pmax;
+  std::map<std::pair<int, int>, std::vector<int>> sepsets;
+  std::vector<int> n_edgetests;
+  std::vector<fkpc_trace_row> trace;
+  std::vector<int> trace_s;
+  fkpc_stage_stats stats{};
+};
+
+void add_stats(fkpc_stage_stats* acc, const fkpc_stage_stats& s) {
+  acc->setup_ms += s.setup_ms;
+  acc->upload_ms += s.upload_ms;
+  acc->fit_ms += s.fit_ms;
+  acc->statistic_ms += s.statistic_ms;
+  acc->refine_ms += s.refine_ms;
+  acc->download_ms += s.download_ms;
+  acc->designs += s.designs;
+  acc->targets += s.targets;
+  acc->pairs += s.pairs;
+  acc->guarded += s.guarded;
+  acc->kernel_launches += s.kernel_launches;
+}
+
+// Evaluate ``tests`` on the engine in chunks; records in test order.
+void evaluate(fkpc::Engine& eng, const std::vector<fkpc::Test>& tests, const fkpc_options& opt, fkpc::RStream* rs,
+              std::vector<fkpc_ci_record>* out, fkpc_stage_stats* acc) {
+  out->resize(tests.size());
+  const size_t chunk = opt.mode == FKPC_MODE_PLAIN ? 1 : 16384;
+  for (size_t b = 0; b < tests.size(); b += chunk) {
+    const size_t e = std::min(tests.size(), b + chunk);
+    std::vector<fkpc::Test> part(tests.begin() + b, tests.begin() + e);
+    fkpc_stage_stats st{};
+    eng.prepare(part, opt, rs);
+    eng.execute();
+    eng.collect(out->data() + b, &st);
+    add_stats(acc, st);
+  }
+}
+
+void skeleton(const double* data, int n, int p, const fkpc_options& opt, Run* run) {
+  auto& eng = engine_for(opt.device);
+  eng.load(data, n, p);
+  const int m_max = opt.max_conditioning_size < 0 ? p - 2 : std::min(opt.max_conditioning_size, p - 2);
+  const bool perm = opt.ci_method == FKPC_DCC_PERM || opt.ci_method == FKPC_HSIC_PERM;
+  std::unique_ptr<fkpc::RStream> rs;
+  if (perm) rs.reset(new fkpc::RStream(opt.seed));
+  run->n = n;
+  run->p = p;
+  run->adj.assign(static_cast<size_t>(p) * p, 1);
+  for (int i = 0; i < p; ++i) run->adj[i + static_cast<size_t>(p) * i] = 0;
+  run->pmax.assign(static_cast<size_t>(p) * p, -INFINITY);
+  for (int level = 0; level <= m_max; ++level) {
+    std::vector<Task> plan = make_layer_plan(run->adj, p, level);
+    std::map<std::pair<int, int>, std::vector<int>> by_edge;
+    for (size_t i = 0; i < plan.size(); ++i) by_edge[{plan[i].edge_x, plan[i].edge_y}].push_back(static_cast<int>(i));
+    std::vector<double> pv(plan.size(), NAN), pe(plan.size(), NAN);
+    std::vector<unsigned> fl(plan.size(), 0u);
+    std::vector<char> counted(plan.size(), 0);
+    auto to_test = [&](const Task& t) { return fkpc::Test{t.x, t.y, t.S}; };
+    if (perm || opt.mode == FKPC_MODE_PLAIN) {
+      // one test at a time; permutation methods in pcalg order
+      std::map<std::pair<int, int>, size_t> pos;
+      for (auto& kv : by_edge) pos[kv.first] = 0;
+      for (;;) {
+        int best = -1;
+        for (auto& kv : by_edge) {
+          const size_t at = pos[kv.first];
+          if (at >= kv.second.size()) continue;
+          const int cand = kv.second[at];
+          if (best < 0) { best = cand; continue; }
+          const Task& a = plan[cand];
+          const Task& b = plan[best];
+          const bool less = perm ? (a.x != b.x ? a.x < b.x : (a.y != b.y ? a.y < b.y : a.S < b.S)) : cand < best;
+          if (less) best = cand;
+        }
+        if (best < 0) break;
+        std::vector<fkpc_ci_record> rec;
+        fkpc_options o1 = opt;
+        o1.mode = FKPC_MODE_PLAIN;
+        evaluate(eng, {to_test(plan[best])}, o1, rs.get(), &rec, &run->stats);
+        pv[best] = rec[0].p_value;
+        pe[best] = rec[0].p_exact;
+        fl[best] = rec[0].flags;
+        counted[best] = 1;
+        const std::pair<int, int> key{plan[best].edge_x, plan[best].edge_y};
+        pos[key] = rec[0].p_value >= opt.alpha ? by_edge[key].size() : pos[key] + 1;
+      }
+    } else {
+      std::vector<fkpc::Test> tests;
+      tests.reserve(plan.size());
+      for (const Task& t : plan) tests.push_back(to_test(t));
+      std::vector<fkpc_ci_record> rec;
+      evaluate(eng, tests, opt, nullptr, &rec, &run->stats);
+      for (size_t i = 0; i < plan.size(); ++i) {
+        pv[i] = rec[i].p_value;
+        pe[i] = rec[i].p_exact;
+        fl[i] = rec[i].flags;
+      }
+      for (auto& kv : by_edge)
+        for (int i : kv.second) {
+          counted[i] = 1;
+          if (pv[i] >= opt.alpha) break;
+        }
+    }
+    // canonical replay in plan order
+    bool done = true;
+    int count = 0;
+    std::vector<std::pair<int, int>> deleted;
+    for (size_t i = 0; i < plan.size(); ++i) {
+      if (!counted[i]) continue;
+      const Task& t = plan[i];
+      ++count;
+      const size_t fwd = t.edge_x + static_cast<size_t>(p) * t.edge_y;
+      const size_t rev = t.edge_y + static_cast<size_t>(p) * t.edge_x;
+      if (pv[i] > run->pmax[fwd]) run->pmax[fwd] = run->pmax[rev] = pv[i];
+      const bool del = pv[i] >= opt.alpha;
+      if (del) {
+        run->sepsets[{t.edge_x, t.edge_y}] = t.S;
+        run->sepsets[{t.edge_y, t.edge_x}] = t.S;
+        deleted.push_back({t.edge_x, t.edge_y});
+      }
+      if (t.opens) done = false;
+      if (opt.collect_trace) {
+        fkpc_trace_row row;
+        row.level = level;
+        row.task_index = static_cast<int>(i);
+        row.edge_x = t.edge_x;
+        row.edge_y = t.edge_y;
+        row.x = t.x;
+        row.y = t.y;
+        row.s_offset = static_cast<int>(run->trace_s.size());
+        row.s_count = static_cast<int>(t.S.size());
+        row.p_value = pv[i];
+        row.p_exact = pe[i];
+        row.deleted = del ? 1 : 0;
+        row.flags = fl[i];
+        run->trace_s.insert(run->trace_s.end(), t.S.begin(), t.S.end());
+        run->trace.push_back(row);
+      }
+    }
+    for (auto& e : deleted) {
+      run->adj[e.first + static_cast<size_t>(p) * e.second] = 0;
+      run->adj[e.second + static_cast<size_t>(p) * e.first] = 0;
+    }
+    run->n_edgetests.push_back(count);
+    if (done) break;
+  }
+}
+
+template <class T>
+T* copy_out(const std::vector<T>& v) {
+  T* out = static_cast<T*>(std::malloc(sizeof(T) * std::max<size_t>(1, v.size())));
+  if (!out) throw std::bad_alloc();
+  if (!v.empty()) std::memcpy(out, v.data(), sizeof(T) * v.size());
+  return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fkpc_abi_version(void) { return FKPC_ABI_VERSION; }
+
+const char* fkpc_last_error(void) { return g_last_error.c_str(); }
+
+void fkpc_default_options(fkpc_options* o) {
+  if (!o) return;
+  o->alpha = 0.1;
+  o->index = 1.0;
+  o->num_col = 35;
+  o->max_conditioning_size = -1;
+  o->ci_method = FKPC_DCC_GAMMA;
+  o->hsic_sig = 1.0;
+  o->permutation_replicates = 100;
+  o->has_seed = 0;
+  o->seed = 0;
+  o->mode = FKPC_MODE_BATCHED;
+  o->collect_trace = 1;
+  o->device = 0;
+  o->strict = 1;
+}
+
+int fkpc_skeleton_run(const double* data, int n, int p, const fkpc_options* options, fkpc_result** out) {
+  return guarded([&]() {
+    if (!data || !options || !out) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    validate_options(*options, n, p);
+    if (p > 64) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "p must be at most 64");
+    std::lock_guard<std::mutex> lock(g_engine_mu);
+    auto t0 = std::chrono::steady_clock::now();
+    Run run;
+    skeleton(data, n, p, *options, &run);
+    fkpc_result* r = static_cast<fkpc_result*>(std::calloc(1, sizeof(fkpc_result)));
+    if (!r) throw std::bad_alloc();
+    r->n = n;
+    r->p = p;
+    r->levels = static_cast<int>(run.n_edgetests.size());
+    r->adjacency = copy_out(run.adj);
+    r->pmax = copy_out(run.pmax);
+    std::vector<int> offs(static_cast<size_t>(p) * p + 1, 0), vals;
+    for (int j = 0; j < p; ++j)
+      for (int i = 0; i < p; ++i) {
+        const size_t cell = i + static_cast<size_t>(p) * j;
+        auto it = run.sepsets.find({i, j});
+        if (it != run.sepsets.end()) vals.insert(vals.end(), it->second.begin(), it->second.end());
+        offs[cell + 1] = static_cast<int>(vals.size());
+      }
+    r->sepset_offsets = copy_out(offs);
+    r->sepset_values = copy_out(vals);
+    r->n_edgetests = copy_out(run.n_edgetests);
+    r->trace_rows = static_cast<int>(run.trace.size());
+    r->trace = options->collect_trace ? copy_out(run.trace) : nullptr;
+    r->trace_s_values = options->collect_trace ? copy_out(run.trace_s) : nullptr;
+    r->stats = run.stats;
+    r->elapsed_sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    r->stats.total_ms = r->elapsed_sec * 1e3;
+    *out = r;
+  });
+}
+
+void fkpc_result_free(fkpc_result* r) {
+  if (!r) return;
+  std::free(r->adjacency);
+  std::free(r->pmax);
+  std::free(r->sepset_offsets);
+  std::free(r->sepset_values);
+  std::free(r->n_edgetests);
+  std::free(r->trace);
+  std::free(r->trace_s_values);
+  std::free(r);
+}
+
+int fkpc_ci_level_batch(const double* data, int n, int p, const int* x, const int* y, const int* s_offsets,
+                        const int* s_values, int count, const fkpc_options* options, fkpc_ci_record* out,
+                        fkpc_stage_stats* stats) {
+  return guarded([&]() {
+    if (!data || !options || !out || count < 0 || (count > 0 && (!x || !y || !s_offsets)))
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    validate_options(*options, n, p);
+    std::lock_guard<std::mutex> lock(g_engine_mu);
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<fkpc::Test> tests(count);
+    for (int t = 0; t < count; ++t) {
+      tests[t].x = x[t];
+      tests[t].y = y[t];
+      if (s_offsets[t + 1] < s_offsets[t]) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "s_offsets must be nondecreasing");
+      tests[t].S.assign(s_values + s_offsets[t], s_values + s_offsets[t + 1]);
+    }
+    auto& eng = engine_for(options->device);
+    eng.load(data, n, p);
+    std::unique_ptr<fkpc::RStream> rs;
+    if (options->ci_method == FKPC_DCC_PERM || options->ci_method == FKPC_HSIC_PERM) rs.reset(new fkpc::RStream(options->seed));
+    std::vector<fkpc_ci_record> rec;
+    fkpc_stage_stats acc{};
+    evaluate(eng, tests, *options, rs.get(), &rec, &acc);
+    std::copy(rec.begin(), rec.end(), out);
+    if (stats) {
+      *stats = acc;
+      stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+  });
+}
+
+int fkpc_ci_plain_one(const double* data, int n, int p, int x, int y, const int* s_values, int s_count,
+                      const fkpc_options* options, fkpc_ci_record* out) {
+  return guarded([&]() {
+    if (!data || !options || !out || s_count < 0 || (s_count > 0 && !s_values))
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    validate_options(*options, n, p);
+    std::lock_guard<std::mutex> lock(g_engine_mu);
+    auto& eng = engine_for(options->device);
+    eng.load(data, n, p);
+    fkpc_options o = *options;
+    o.mode = FKPC_MODE_PLAIN;
+    std::unique_ptr<fkpc::RStream> rs;
+    if (o.ci_method == FKPC_DCC_PERM || o.ci_method == FKPC_HSIC_PERM) rs.reset(new fkpc::RStream(o.seed));
+    std::vector<fkpc_ci_record> rec;
+    fkpc_stage_stats acc{};
+    evaluate(eng, {fkpc::Test{x, y, std::vector<int>(s_values, s_values + s_count)}}, o, rs.get(), &rec, &acc);
+    *out = rec[0];
+  });
+}
+
+int fkpc_regress_batch(const double* data, int n, int p, const int* target, const int* s_offsets,
+                       const int* s_values, int count, const fkpc_options* options, double* residuals,
+                       double* log_sp, int max_penalties, int* status) {
+  return guarded([&]() {
+    if (!data || !target || !s_offsets || !residuals || count < 0)
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    fkpc_options o;
+    fkpc_default_options(&o);
+    if (options) o = *options;
+    std::lock_guard<std::mutex> lock(g_engine_mu);
+    auto& eng = engine_for(o.device);
+    eng.load(data, n, p);
+    std::vector<int> tg(target, target + count);
+    std::vector<std::vector<int>> sets(count);
+    for (int t = 0; t < count; ++t) sets[t].assign(s_values + s_offsets[t], s_values + s_offsets[t + 1]);
+    eng.regress(tg, sets, residuals, log_sp, max_penalties, status);
+  });
+}
+
+int fkpc_stat_batch(const double* residuals, int n, int m, const int* left, const int* right, int count,
+                    const int* permutations, const fkpc_options* options, fkpc_ci_record* out) {
+  return guarded([&]() {
+    if (!residuals || !left || !right || !options || !out || count < 0 || m < 1)
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    validate_options(*options, n, std::max(2, m));
+    std::lock_guard<std::mutex> lock(g_engine_mu);
+    auto& eng = engine_for(options->device);
+    eng.load(residuals, n, m);
+    eng.statistics(residuals, m, std::vector<int>(left, left + count), std::vector<int>(right, right + count),
+                   permutations, *options, out);
+  });
+}
+
+int fkpc_batch_prepare(const double* data, int n, int p, const int* x, const int* y, const int* s_offsets,
+                       const int* s_values, int count, const fkpc_options* options) {
+  return guarded([&]() {
+    if (!data || !options || count < 1 || !x || !y || !s_offsets)
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    validate_options(*options, n, p);
+    if (options->ci_method == FKPC_DCC_PERM || options->ci_method == FKPC_HSIC_PERM)
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "the staged form covers the gamma methods");
+    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::vector<fkpc::Test> tests(count);
+    for (int t = 0; t < count; ++t) {
+      tests[t].x = x[t];
+      tests[t].y = y[t];
+      tests[t].S.assign(s_values + s_offsets[t], s_values + s_offsets[t + 1]);
+    }
+    auto& eng = engine_for(options->device);
+    eng.load(data, n, p);
+    fkpc_options o = *options;
+    o.mode = FKPC_MODE_BATCHED;
+    eng.prepare(tests, o, nullptr);
+  });
+}
+
+int fkpc_batch_execute(int device, int repeats, double* device_ms) {
+  return guarded([&]() {
+    if (repeats < 1) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "repeats must be positive");
+    std::lock_guard<std::mutex> lock(g_engine_mu);
+    const double ms = engine_for(device).execute_timed(repeats);
+    if (device_ms) *device_ms = ms;
+  });
+}
+
+int fkpc_batch_collect(int device, fkpc_ci_record* out, fkpc_stage_stats* stats) {
+  return guarded([&]() {
+    std::lock_guard<std::mutex> lock(g_engine_mu);
+    engine_for(device).collect(out, stats);
+  });
+}
+
+int fkpc_batch_time_stage(int device, int stage, int repeats, double* avg_ms, double* flops_per_launch) {
+  return guarded([&]() {
+    std::lock_guard<std::mutex> lock(g_engine_mu);
+    const double ms = engine_for(device).time_stage(stage, repeats, flops_per_launch);
+    if (avg_ms) *avg_ms = ms;
+  });
+}
+
+int fkpc_measure_fp64_peak(int device, double* tflops) {
+  return guarded([&]() {
+    std::lock_guard<std::mutex> lock(g_engine_mu);
+    const double t = engine_for(device).measure_fp64_peak();
+    if (tflops) *tflops = t;
+  });
+}
+
+int fkpc_design_export(const double* data, int n, int p, const int* s_values, int s_count, int* q, int* m,
+                       double* X, double* penalties, double* initial_log_sp) {
+  return guarded([&]() {
+    if (!data || !q || !m || s_count < 1 || !s_values) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    std::vector<int> S(s_values, s_values + s_count);
+    std::sort(S.begin(), S.end());
+    auto des = fkpc::build_design(data, n, p, S, nullptr);
+    *q = des->q;
+    *m = des->m;
+    if (X) std::copy(des->X.begin(), des->X.end(), X);
+    if (penalties) {
+      const size_t qq = static_cast<size_t>(des->q) * des->q;
+      std::fill(penalties, penalties + qq * des->m, 0.0);
+      for (int j = 0; j < des->m; ++j) {
+        const int off = des->offsets[j], dim = des->dims[j];
+        for (int b = 0; b < dim; ++b)
+          for (int a = 0; a < dim; ++a)
+            penalties[qq * j + (off + a) + static_cast<size_t>(des->q) * (off + b)] =
+                des->blocks[j][a + static_cast<size_t>(dim) * b];
+      }
+    }
+    if (initial_log_sp) std::copy(des->initial_log_sp.begin(), des->initial_log_sp.end(), initial_log_sp);
+  });
+}
+
+int fkpc_gcv_adjoint(const double*, int, int, int, const int*, int, int, const double*, double*, double*, double*,
+                     double*) {
+  return fail(FKPC_STATUS_INVALID_ARGUMENT, "fkpc_gcv_adjoint is not available in this build");
+}
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+// regrXonS design setup: mgcv-style thin-plate (|S| <= 2) and additive
+// (|S| > 2) smooth bases, penalties, initial smoothing parameters and the
+// per-design geometry the GPU fit kernels consume.
+#pragma once
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+namespace fkpc {
+
+struct Smooth {
+  int n = 0, cols = 0, rank = 0;   // cols = k - 1 after the centering constraint
+  std::vector<double> X;           // n x cols, column-major
+  std::vector<double> S;           // cols x cols penalty
+};
+
+// One conditioning set's model: X = [1 | smooth_1 | ... ] with one penalty
+// block per smooth.
+struct Design {
+  int n = 0, q = 0, m = 0;
+  std::vector<int> S;                       // conditioning columns (sorted as given)
+  std::vector<double> X;                    // n x q
+  std::vector<std::vector<double>> blocks;  // dim_j x dim_j
+  std::vector<int> offsets, dims, ranks;
+  std::vector<double> initial_log_sp;       // m
+  // geometry
+  std::vector<double> Q;                    // n x q, X = Q R
+  std::vector<double> R;                    // q x q upper triangular
+  // single penalty (m == 1): whitened-penalty spectrum
+  std::vector<double> spec;                 // q hat eigenvalues e_k (descending, >= 0)
+  std::vector<double> QW;                   // n x q: Q * W, W the whitened eigenvectors
+  // several penalties: per block root (dim_j x rank_j), root root' = S_j
+  std::vector<std::vector<double>> roots;
+};
+
+Smooth build_smooth(const double* cols, int n, int d, int k);
+double r_mean(const double* v, int n);
+std::vector<double> initial_sp(const Design& des);
+void prepare_geometry(Design* des);
+
+// Cache of univariate smooths (shared by every additive model containing the
+// variable) and of full designs per conditioning set.
+class DesignCache {
+ public:
+  DesignCache(const double* data, int n, int p) : data_(data), n_(n), p_(p) {}
+  std::shared_ptr<const Design> get(const std::vector<int>& S);
+  std::shared_ptr<const Smooth> univariate(int column);
+  size_t size() const { return designs_.size(); }
+
+ private:
+  const double* data_;
+  int n_, p_;
+  std::mutex mu_;
+  std::map<std::vector<int>, std::shared_ptr<const Design>> designs_;
+  std::map<int, std::shared_ptr<const Smooth>> uni_;
+};
+
+std::shared_ptr<Design> build_design(const double* data, int n, int p, const std::vector<int>& S,
+                                     DesignCache* cache);
+
+}  // namespace fkpc

@@ -1,0 +1,319 @@
+#include "hostla.h"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <stdexcept>
+
+namespace fkpc {
+
+void householder_qr(const double* A, int rows, int cols, std::vector<double>* Q,
+                    std::vector<double>* R) {
+  if (rows < cols || cols <= 0) throw std::runtime_error("householder_qr: need rows >= cols > 0");
+  std::vector<double> W(A, A + static_cast<size_t>(rows) * cols);
+  std::vector<double> V(static_cast<size_t>(rows) * cols, 0.0);
+  std::vector<double> beta(cols, 0.0);
+  for (int k = 0; k < cols; ++k) {
+    double* x = &W[static_cast<size_t>(k) * rows];
+    double norm2 = 0.0;
+    for (int i = k; i < rows; ++i) norm2 += x[i] * x[i];
+    double norm = std::sqrt(norm2);
+    double* v = &V[static_cast<size_t>(k) * rows];
+    if (norm == 0.0) { beta[k] = 0.0; continue; }
+    double alpha = x[k] >= 0.0 ? -norm : norm;
+    for (int i = k; i < rows; ++i) v[i] = x[i];
+    v[k] -= alpha;
+    double vnorm2 = norm2 - x[k] * x[k] + v[k] * v[k];
+    beta[k] = 2.0 / vnorm2;
+    // apply H = I - beta v v' to columns k..cols-1
+    for (int j = k; j < cols; ++j) {
+      double* c = &W[static_cast<size_t>(j) * rows];
+      double dot = 0.0;
+      for (int i = k; i < rows; ++i) dot += v[i] * c[i];
+      dot *= beta[k];
+      for (int i = k; i < rows; ++i) c[i] -= dot * v[i];
+    }
+  }
+  R->assign(static_cast<size_t>(cols) * cols, 0.0);
+  for (int j = 0; j < cols; ++j)
+    for (int i = 0; i <= j; ++i) (*R)[i + static_cast<size_t>(cols) * j] = W[i + static_cast<size_t>(rows) * j];
+  Q->assign(static_cast<size_t>(rows) * cols, 0.0);
+  for (int j = 0; j < cols; ++j) (*Q)[j + static_cast<size_t>(rows) * j] = 1.0;
+  for (int k = cols - 1; k >= 0; --k) {
+    if (beta[k] == 0.0) continue;
+    const double* v = &V[static_cast<size_t>(k) * rows];
+    for (int j = 0; j < cols; ++j) {
+      double* c = &(*Q)[static_cast<size_t>(j) * rows];
+      double dot = 0.0;
+      for (int i = k; i < rows; ++i) dot += v[i] * c[i];
+      dot *= beta[k];
+      for (int i = k; i < rows; ++i) c[i] -= dot * v[i];
+    }
+  }
+}
+
+void jacobi_eigen(const double* A, int n, std::vector<double>* values,
+                  std::vector<double>* vectors) {
+  std::vector<double> a(A, A + static_cast<size_t>(n) * n);
+  std::vector<double> v(static_cast<size_t>(n) * n, 0.0);
+  for (int i = 0; i < n; ++i) v[i + static_cast<size_t>(n) * i] = 1.0;
+  auto at = [&](int i, int j) -> double& { return a[i + static_cast<size_t>(n) * j]; };
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, diag = 0.0;
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        if (i == j) diag += at(i, i) * at(i, i);
+        else off += at(i, j) * at(i, j);
+      }
+    if (off <= 1e-32 * diag || off == 0.0) break;
+    for (int p = 0; p < n - 1; ++p) {
+      for (int q = p + 1; q < n; ++q) {
+        double apq = at(p, q);
+        if (apq == 0.0) continue;
+        double app = at(p, p), aqq = at(q, q);
+        double theta = (aqq - app) / (2.0 * apq);
+        double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        double c = 1.0 / std::sqrt(t * t + 1.0);
+        double s = t * c;
+        for (int k = 0; k < n; ++k) {
+          double akp = at(k, p), akq = at(k, q);
+          at(k, p) = c * akp - s * akq;
+          at(k, q) = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          double apk = at(p, k), aqk = at(q, k);
+          at(p, k) = c * apk - s * aqk;
+          at(q, k) = s * apk + c * aqk;
+        }
+        at(p, q) = 0.0;
+        at(q, p) = 0.0;
+        for (int k = 0; k < n; ++k) {
+          double vkp = v[k + static_cast<size_t>(n) * p], vkq = v[k + static_cast<size_t>(n) * q];
+          v[k + static_cast<size_t>(n) * p] = c * vkp - s * vkq;
+          v[k + static_cast<size_t>(n) * q] = s * vkp + c * vkq;
+        }
+      }
+    }
+  }
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int l, int r) { return at(l, l) < at(r, r); });
+  values->resize(n);
+  vectors->resize(static_cast<size_t>(n) * n);
+  for (int j = 0; j < n; ++j) {
+    (*values)[j] = at(order[j], order[j]);
+    for (int i = 0; i < n; ++i)
+      (*vectors)[i + static_cast<size_t>(n) * j] = v[i + static_cast<size_t>(n) * order[j]];
+  }
+}
+
+bool tridiagonal_ql(int n, double* d, double* e, double* z) {
+  if (n <= 0) return true;
+  e[n - 1] = 0.0;
+  const double eps = 2.220446049250313e-16;
+  for (int l = 0; l < n; ++l) {
+    int iter = 0;
+    for (;;) {
+      int m = l;
+      for (; m < n - 1; ++m) {
+        double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+        if (std::fabs(e[m]) <= eps * dd) break;
+      }
+      if (m == l) break;
+      if (++iter > 60) return false;
+      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      double r = std::hypot(g, 1.0);
+      g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? std::fabs(r) : -std::fabs(r)));
+      double s = 1.0, c = 1.0, p = 0.0;
+      int i = m - 1;
+      for (; i >= l; --i) {
+        double f = s * e[i];
+        double b = c * e[i];
+        r = std::hypot(f, g);
+        e[i + 1] = r;
+        if (r == 0.0) {
+          d[i + 1] -= p;
+          e[m] = 0.0;
+          break;
+        }
+        s = f / r;
+        c = g / r;
+        g = d[i + 1] - p;
+        r = (d[i] - g) * s + 2.0 * c * b;
+        p = s * r;
+        d[i + 1] = g + p;
+        g = c * r - b;
+        for (int k = 0; k < n; ++k) {
+          double zk1 = z[k + static_cast<size_t>(n) * (i + 1)];
+          double zk = z[k + static_cast<size_t>(n) * i];
+          z[k + static_cast<size_t>(n) * (i + 1)] = s * zk + c * zk1;
+          z[k + static_cast<size_t>(n) * i] = c * zk - s * zk1;
+        }
+      }
+      if (r == 0.0 && i >= l) continue;
+      d[l] -= p;
+      e[l] = g;
+      e[m] = 0.0;
+    }
+  }
+  return true;
+}
+
+namespace {
+
+void symv(const double* A, int n, const double* x, double* y) {
+  for (int i = 0; i < n; ++i) y[i] = 0.0;
+  for (int j = 0; j < n; ++j) {
+    const double xj = x[j];
+    const double* col = A + static_cast<size_t>(n) * j;
+    for (int i = 0; i < n; ++i) y[i] += col[i] * xj;
+  }
+}
+
+double dot(const double* a, const double* b, int n) {
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += a[i] * b[i];
+  return s;
+}
+
+// indices of the k entries of largest |value| (ties toward the lower index)
+std::vector<int> top_k_by_magnitude(const std::vector<double>& v, int count, int k) {
+  std::vector<int> idx(count);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return std::fabs(v[a]) > std::fabs(v[b]); });
+  idx.resize(k);
+  return idx;
+}
+
+}  // namespace
+
+int top_magnitude_eigen(const double* A, int n, int k, std::vector<double>* values,
+                        std::vector<double>* vectors) {
+  if (k <= 0 || k > n) throw std::runtime_error("top_magnitude_eigen: invalid k");
+  const int maxit = n;
+  std::vector<double> Qv(static_cast<size_t>(n) * (maxit + 1), 0.0);
+  std::vector<double> alpha(maxit + 1, 0.0), beta(maxit + 1, 0.0);
+  // deterministic start vector from a small LCG
+  unsigned long state = 1;
+  double norm = 0.0;
+  for (int i = 0; i < n; ++i) {
+    state = (state * 106UL + 1283UL) % 6075UL;
+    Qv[i] = static_cast<double>(state) / 6075.0 - 0.5;
+    norm += Qv[i] * Qv[i];
+  }
+  norm = std::sqrt(norm);
+  for (int i = 0; i < n; ++i) Qv[i] /= norm;
+  std::vector<double> w(n), theta, S, dwork, ework;
+  int steps = 0;
+  const double tol = 1e-14;
+  double anorm = 0.0;
+  for (int j = 0; j < maxit; ++j) {
+    double* qj = &Qv[static_cast<size_t>(n) * j];
+    symv(A, n, qj, w.data());
+    alpha[j] = dot(qj, w.data(), n);
+    for (int i = 0; i < n; ++i) w[i] -= alpha[j] * qj[i];
+    if (j > 0) {
+      const double* qp = &Qv[static_cast<size_t>(n) * (j - 1)];
+      for (int i = 0; i < n; ++i) w[i] -= beta[j - 1] * qp[i];
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int b = 0; b <= j; ++b) {
+        const double* qb = &Qv[static_cast<size_t>(n) * b];
+        double c = dot(w.data(), qb, n);
+        for (int i = 0; i < n; ++i) w[i] -= c * qb[i];
+      }
+    }
+    beta[j] = std::sqrt(dot(w.data(), w.data(), n));
+    steps = j + 1;
+    anorm = std::max(anorm, std::fabs(alpha[j]) + beta[j] + (j > 0 ? beta[j - 1] : 0.0));
+    bool invariant = beta[j] <= 1e-15 * anorm;
+    bool check = invariant || j + 1 == maxit || (j + 1 >= k + 5 && ((j + 1 - k) % 5 == 0));
+    if (check) {
+      int m = j + 1;
+      dwork.assign(alpha.begin(), alpha.begin() + m);
+      ework.assign(m, 0.0);
+      for (int i = 0; i + 1 < m; ++i) ework[i] = beta[i];
+      S.assign(static_cast<size_t>(m) * m, 0.0);
+      for (int i = 0; i < m; ++i) S[i + static_cast<size_t>(m) * i] = 1.0;
+      if (!tridiagonal_ql(m, dwork.data(), ework.data(), S.data()))
+        throw std::runtime_error("Lanczos tridiagonal eigen-solve failed");
+      std::vector<int> sel = top_k_by_magnitude(dwork, m, std::min(k, m));
+      double tmax = 0.0;
+      for (int i = 0; i < m; ++i) tmax = std::max(tmax, std::fabs(dwork[i]));
+      bool converged = m >= k;
+      if (converged && !invariant) {
+        for (int i : sel) {
+          double resid = std::fabs(beta[j] * S[(m - 1) + static_cast<size_t>(m) * i]);
+          if (resid > tol * tmax) { converged = false; break; }
+        }
+      }
+      if (converged || invariant || j + 1 == maxit) {
+        if (m < k) throw std::runtime_error("Lanczos produced fewer Ritz pairs than requested");
+        theta.assign(k, 0.0);
+        std::vector<double> V(static_cast<size_t>(n) * k, 0.0);
+        for (int c = 0; c < k; ++c) {
+          int i = sel[c];
+          theta[c] = dwork[i];
+          for (int b = 0; b < m; ++b) {
+            double coef = S[b + static_cast<size_t>(m) * i];
+            const double* qb = &Qv[static_cast<size_t>(n) * b];
+            double* vc = &V[static_cast<size_t>(n) * c];
+            for (int r = 0; r < n; ++r) vc[r] += coef * qb[r];
+          }
+        }
+        // Rayleigh-Ritz refinement on span[V, A V]
+        int k2 = 2 * k;
+        std::vector<double> Wm(static_cast<size_t>(n) * k2);
+        std::copy(V.begin(), V.end(), Wm.begin());
+        for (int c = 0; c < k; ++c)
+          symv(A, n, &V[static_cast<size_t>(n) * c], &Wm[static_cast<size_t>(n) * (k + c)]);
+        std::vector<double> Qb, Rb;
+        householder_qr(Wm.data(), n, k2, &Qb, &Rb);
+        std::vector<double> AQ(static_cast<size_t>(n) * k2);
+        for (int c = 0; c < k2; ++c)
+          symv(A, n, &Qb[static_cast<size_t>(n) * c], &AQ[static_cast<size_t>(n) * c]);
+        std::vector<double> H(static_cast<size_t>(k2) * k2);
+        for (int a = 0; a < k2; ++a)
+          for (int b = 0; b < k2; ++b)
+            H[a + static_cast<size_t>(k2) * b] = dot(&Qb[static_cast<size_t>(n) * a], &AQ[static_cast<size_t>(n) * b], n);
+        for (int a = 0; a < k2; ++a)
+          for (int b = a + 1; b < k2; ++b) {
+            double s = 0.5 * (H[a + static_cast<size_t>(k2) * b] + H[b + static_cast<size_t>(k2) * a]);
+            H[a + static_cast<size_t>(k2) * b] = H[b + static_cast<size_t>(k2) * a] = s;
+          }
+        std::vector<double> hv, hz;
+        jacobi_eigen(H.data(), k2, &hv, &hz);
+        std::vector<int> pick = top_k_by_magnitude(hv, k2, k);
+        std::stable_sort(pick.begin(), pick.end(), [&](int a, int b) { return hv[a] > hv[b]; });
+        values->assign(k, 0.0);
+        vectors->assign(static_cast<size_t>(n) * k, 0.0);
+        for (int c = 0; c < k; ++c) {
+          int i = pick[c];
+          (*values)[c] = hv[i];
+          double* out = &(*vectors)[static_cast<size_t>(n) * c];
+          for (int b = 0; b < k2; ++b) {
+            double coef = hz[b + static_cast<size_t>(k2) * i];
+            const double* qb = &Qb[static_cast<size_t>(n) * b];
+            for (int r = 0; r < n; ++r) out[r] += coef * qb[r];
+          }
+          double nn = std::sqrt(dot(out, out, n));
+          int imax = 0;
+          double amax = -1.0;
+          for (int r = 0; r < n; ++r) {
+            out[r] /= nn;
+            if (std::fabs(out[r]) > amax) { amax = std::fabs(out[r]); imax = r; }
+          }
+          if (out[imax] < 0.0)
+            for (int r = 0; r < n; ++r) out[r] = -out[r];
+        }
+        return steps;
+      }
+    }
+    if (invariant) break;
+    double* qn = &Qv[static_cast<size_t>(n) * (j + 1)];
+    for (int i = 0; i < n; ++i) qn[i] = w[i] / beta[j];
+  }
+  throw std::runtime_error("Lanczos did not converge");
+}
+
+}  // namespace fkpc

@@ -1,0 +1,74 @@
+// Kernel launchers (host-callable) for the fit and statistic stages.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "device.h"
+
+namespace fkpc {
+
+size_t multi_smem_bytes(int qmax_class);
+// Raise the dynamic shared-memory limits (call outside graph capture).
+cudaError_t configure_fit_kernels();
+cudaError_t configure_stat_kernels(int n);
+
+cudaError_t launch_fit_single(const DesignDev* designs, const double* arena, const double* data, int n,
+                              const FitJob* jobs, int count, double* residuals, FitResult* results,
+                              cudaStream_t stream);
+
+// qmax_class 0: q <= 40 and rank sum <= 32; 1: q <= 76 and rank sum <= 64.
+cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const double* arena, const double* data,
+                             int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
+                             FitResult* results, cudaStream_t stream);
+
+// dCov: per component centring constants and moments, then per pair statistic
+// and gamma p-value.  comp_cols[c] is the residual column of component c.
+struct DcovComponent {
+  double total;    // sum of distances
+  double self;     // sum of squared double-centred distances
+};
+
+cudaError_t launch_dcov_components(const double* residuals, int n, const int* comp_cols, int count,
+                                   double* centre, DcovComponent* comps, cudaStream_t stream);
+cudaError_t launch_dcov_pairs(const double* residuals, int n, const int* comp_cols, const double* centre,
+                              const DcovComponent* comps, const PairJob* pairs, int count, RecordDev* records,
+                              cudaStream_t stream);
+
+// Guard band: list the pairs whose exact p lies in [lo, hi] and give each of
+// their components a low-rank slot.  guard layout: [0] pair count, [1] slot
+// count, [2, 2+count) pair list, comp_slot[ncomp], slot_comps[cap].
+cudaError_t launch_guard_select(const RecordDev* records, const PairJob* pairs, int count, int ncomp, int cap,
+                                double lo, double hi, int* guard, cudaStream_t stream);
+// Low-rank (legacy) dCov for the guarded pairs: num_col largest-|value|
+// eigenpairs per slot (vals cap x num_col, vecs n x num_col x cap, centred).
+size_t legacy_eigen_workspace_doubles(int n, int ctas);
+cudaError_t launch_legacy_eigen(const double* residuals, int n, const int* comp_cols, const int* guard,
+                                const int* slot_comps, int cap, int ctas, int num_col, double* workspace,
+                                double* lowrank_vals, double* lowrank_vecs, int* status, cudaStream_t stream);
+cudaError_t launch_legacy_pairs(int n, int num_col, const double* lowrank_vals, const double* lowrank_vecs,
+                                const DcovComponent* comps, const int* guard, const int* guard_pairs,
+                                const int* comp_slot, const PairJob* pairs, int count, RecordDev* records,
+                                cudaStream_t stream);
+
+// HSIC: incomplete Cholesky factors (n x num_col, column-centred) per component.
+struct HsicComponent {
+  double offdiag;  // sum of off-diagonal entries of G G' (raw factor)
+  double self;     // |Gc' Gc|_F^2
+  int rank;
+  int status;
+};
+
+cudaError_t launch_hsic_components(const double* residuals, int n, const int* comp_cols, int count, int num_col,
+                                   double sig, double* factors, HsicComponent* comps, cudaStream_t stream);
+cudaError_t launch_hsic_pairs(int n, int num_col, const double* factors, const HsicComponent* comps,
+                              const PairJob* pairs, int count, RecordDev* records, cudaStream_t stream);
+cudaError_t launch_hsic_perm_pairs(int n, int num_col, const double* factors, const HsicComponent* comps,
+                                   const PairJob* pairs, int count, const int* perms, int replicates,
+                                   RecordDev* records, cudaStream_t stream);
+cudaError_t launch_dcc_perm_pairs(const double* residuals, int n, const int* comp_cols, const double* centre,
+                                  const PairJob* pairs, int count, const int* perms, int replicates,
+                                  RecordDev* records, cudaStream_t stream);
+
+// FP64 FMA throughput probe: blocks x 256 threads, 16 chains, iters steps.
+cudaError_t launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t stream);
+
+}  // namespace fkpc

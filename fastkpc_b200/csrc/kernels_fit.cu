@@ -1,0 +1,843 @@
+// GCV smoothing-parameter selection and residuals on the GPU (FP64).
+//
+// fit_single_kernel: one warp per target for designs with one penalty
+//   (|S| <= 2).  Spectral form of mgcv magic's GCV: with the whitened
+//   penalty spectrum e_k and z = (QW)'y, the hat values are
+//   h_k = 1/(1 + lambda e_k); RSS = |y|^2 - 2 sum h z^2 + sum h^2 z^2,
+//   EDF = sum h, V = n RSS/(n - EDF)^2.  Newton / steepest-descent search in
+//   rho = log(lambda) as in fastkpc/src/cuda/mgcv_single_penalty_gcv.cu:1479-1700
+//   (15 step halvings, 400 iterations, |step| <= 5, tolerance 1e-7, boundary
+//   probes of 2 up to 5 times).  Residual r = y - QW (h .* z).
+//
+// fit_multi_kernel: one CTA per target for additive designs (|S| > 2).
+//   Each objective evaluation factors the augmented system [R; B(rho)],
+//   B'B = sum_j lambda_j S_j, by Householder reflections that fold the
+//   stacked penalty roots into R (shared memory, one thread per column),
+//   giving Ra with Ra'Ra = X'X + S_lambda.  With W = R Ra^-1 the hat matrix is
+//   Q W W' Q', so EDF = |W|_F^2 and, with g = W'Q'y,
+//   RSS = |y|^2 - 2|g|^2 + |W g|^2 -- the quantities mgcv magic derives from
+//   the SVD of [R; B] (fastkpc/src/mgcv_multi_penalty_cpp.cpp:732-810), in a
+//   rotated basis.  The analytic gradient and Hessian in rho
+//   (:834-975) use T_j = Ra^-T root_j:  M_j = T_j T_j', and every trace is a
+//   small block sum over C = T'T and D = (WT)'(WT).  Newton loop of
+//   :1124-1346 (25 step halvings, steepest descent after the third rejected
+//   Newton trial or for an indefinite Hessian, boundary probes).
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "device.h"
+#include "kernels.h"
+
+namespace fkpc {
+
+namespace {
+
+constexpr double kConvTol = 1e-7;
+constexpr double kEps = 2.220446049250313e-16;
+constexpr int kMaxIterations = 400;
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ----------------------------------------------------------------- single
+
+struct SingleObjective {
+  double rss, edf, score, gradient, hessian;
+  bool valid;
+};
+
+__device__ double hat_value(double log_sp, double e) {
+  if (e == 0.0) return 1.0;
+  const double c = log_sp + log(e);
+  if (c >= 0.0) {
+    const double v = exp(-c);
+    return v / (1.0 + v);
+  }
+  return 1.0 / (1.0 + exp(c));
+}
+
+// All 32 lanes call with the same log_sp; lane k < q owns component k.
+__device__ SingleObjective single_objective(double log_sp, double e, double z, bool active,
+                                            double yy, int n) {
+  double lin = 0, quad = 0, edf = 0, rg = 0, rh = 0, dg = 0, dh = 0;
+  if (active) {
+    const double h = hat_value(log_sp, e);
+    const double z2 = z * z;
+    const double omh = 1.0 - h;
+    const double w = h * omh;
+    lin = h * z2;
+    quad = h * h * z2;
+    edf = h;
+    rg = 2.0 * h * omh * omh * z2;
+    rh = 2.0 * h * omh * omh * (3.0 * h - 1.0) * z2;
+    dg = w;
+    dh = -w * (1.0 - 2.0 * h);
+  }
+  lin = warp_sum(lin);
+  quad = warp_sum(quad);
+  edf = warp_sum(edf);
+  rg = warp_sum(rg);
+  rh = warp_sum(rh);
+  dg = warp_sum(dg);
+  dh = warp_sum(dh);
+  SingleObjective out;
+  double rss = yy - 2.0 * lin + quad;
+  if (rss < 0.0 && isfinite(rss)) rss = 0.0;
+  const double rdf = static_cast<double>(n) - edf;
+  out.rss = rss;
+  out.edf = edf;
+  out.valid = isfinite(rss) && isfinite(edf) && rss > 0.0 && rdf > 1e-8;
+  if (!out.valid) {
+    out.score = INFINITY;
+    out.gradient = NAN;
+    out.hessian = NAN;
+    return out;
+  }
+  const double score = static_cast<double>(n) * rss / (rdf * rdf);
+  const double lg = rg / rss - 2.0 * dg / rdf;
+  const double lh = rh / rss - (rg / rss) * (rg / rss) - 2.0 * (dh / rdf - (dg / rdf) * (dg / rdf));
+  out.score = score;
+  out.gradient = score * lg;
+  out.hessian = score * (lh + lg * lg);
+  return out;
+}
+
+}  // namespace
+
+__global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const double* __restrict__ arena,
+                                  const double* __restrict__ data, int n, const FitJob* __restrict__ jobs,
+                                  int job_count, double* __restrict__ residuals, FitResult* __restrict__ results) {
+  const int warps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int t = blockIdx.x * warps + warp;
+  if (t >= job_count) return;
+  const FitJob job = jobs[t];
+  const DesignDev& des = designs[job.design];
+  const int q = des.q;
+  const double* QW = arena + des.basis;
+  const double* y = data + static_cast<int64_t>(n) * job.column;
+
+  // z = QW' y and |y|^2; lane-strided rows, per-column partial sums
+  double acc[kMaxSingleQ];
+#pragma unroll
+  for (int k = 0; k < kMaxSingleQ; ++k) acc[k] = 0.0;
+  double yy = 0.0;
+  for (int i = lane; i < n; i += 32) {
+    const double yi = y[i];
+    yy += yi * yi;
+#pragma unroll
+    for (int k = 0; k < kMaxSingleQ; ++k)
+      if (k < q) acc[k] += QW[i + static_cast<int64_t>(n) * k] * yi;
+  }
+  yy = warp_sum(yy);
+  double zk = 0.0;
+#pragma unroll
+  for (int k = 0; k < kMaxSingleQ; ++k) {
+    const double s = warp_sum(acc[k]);
+    if (k == lane) zk = s;
+  }
+  const bool active = lane < q;
+  const double ek = active ? arena[des.spec + lane] : 0.0;
+
+  FitResult res;
+  for (int j = 0; j < kMaxPenalties; ++j) res.log_sp[j] = NAN;
+  res.flags = 0;
+  res.status = kStatusOk;
+  const int max_half = 15;
+  double log_sp = des.log_sp0[0];
+  SingleObjective cur = single_objective(log_sp, ek, zk, active, yy, n);
+  int calls = 1;
+  int it = 0;
+  bool converged = false;
+  if (!cur.valid) {
+    res.status = kStatusNumeric;
+  } else {
+    double min_score = cur.score;
+    double score_red = 1e10;
+    bool steepest = false;
+    double prior_grad = NAN;
+    double newton = 0.0, steep = 0.0;
+    while (!converged && it < kMaxIterations) {
+      ++it;
+      bool try_step = it > 1;
+      int tries = 0;
+      double step = steepest ? steep : newton;
+      bool src_newton = !steepest;
+      bool it_flat = false;
+      while (try_step) {
+        ++tries;
+        if (tries == 4 && !steepest) {
+          steepest = true;
+          step = steep;
+          src_newton = false;
+        }
+        const double trial_ls = log_sp + step;
+        const SingleObjective trial = single_objective(trial_ls, ek, zk, active, yy, n);
+        ++calls;
+        const double pred = cur.gradient * step + 0.5 * cur.hessian * step * step;
+        const double resolution = 8.0 * kEps * (1.0 + fabs(min_score));
+        const bool unresolved = src_newton && isfinite(pred) && pred <= 0.0 && fabs(pred) <= resolution;
+        if (trial.valid && trial.score < min_score) {
+          try_step = false;
+          score_red = min_score - trial.score;
+          min_score = trial.score;
+          log_sp = trial_ls;
+          cur = trial;
+        } else if (unresolved) {
+          try_step = false;
+          it_flat = true;
+        } else {
+          step /= 2.0;
+        }
+        if (tries == max_half - 1 && try_step) step = 0.0;
+        if (tries == max_half) try_step = false;
+      }
+      if (it > 3) {
+        converged = true;
+        if (score_red > kConvTol * (1.0 + min_score)) converged = false;
+        if (fabs(prior_grad) > pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(min_score))) converged = false;
+        if (tries == max_half) converged = true;
+        if (it_flat) converged = true;
+      }
+      prior_grad = cur.gradient;
+      steepest = cur.hessian < 0.0;
+      if (!steepest) {
+        newton = -cur.gradient / cur.hessian;
+        if (fabs(newton) > 5.0) newton = copysign(5.0, newton);
+      }
+      steep = cur.gradient == 0.0 ? 0.0 : -cur.gradient / fabs(cur.gradient);
+    }
+    if (!converged) {
+      res.status = kStatusNotConverged;
+    } else {
+      const double direction = cur.gradient < 0.0 ? 1.0 : -1.0;
+      for (int probe = 0; probe < 5; ++probe) {
+        const double trial_ls = log_sp + direction * 2.0;
+        const SingleObjective trial = single_objective(trial_ls, ek, zk, active, yy, n);
+        ++calls;
+        if (!(trial.valid && trial.score < min_score)) break;
+        log_sp = trial_ls;
+        cur = trial;
+        min_score = trial.score;
+      }
+    }
+  }
+  // residual r = y - QW (h .* z)
+  __shared__ double coef_all[32 * 8];
+  double* coef = coef_all + warp * 32;
+  coef[lane] = active ? hat_value(log_sp, ek) * zk : 0.0;
+  __syncwarp();
+  double* r = residuals + static_cast<int64_t>(n) * job.out;
+  for (int i = lane; i < n; i += 32) {
+    double f = 0.0;
+    for (int k = 0; k < q; ++k) f += QW[i + static_cast<int64_t>(n) * k] * coef[k];
+    r[i] = y[i] - f;
+  }
+  if (lane == 0) {
+    res.log_sp[0] = log_sp;
+    res.score = cur.score;
+    res.edf = cur.edf;
+    res.rss = cur.rss;
+    res.iterations = it;
+    res.evaluations = calls;
+    results[t] = res;
+  }
+}
+
+// ----------------------------------------------------------------- multi
+
+namespace {
+
+constexpr int kMultiThreads = 128;
+
+__device__ __forceinline__ int tri(int i, int j) { return j * (j + 1) / 2 + i; }  // packed upper, i <= j
+
+template <int QMAX, int RMAX>
+struct MultiLayout {
+  static constexpr int TRI = QMAX * (QMAX + 1) / 2;
+  static constexpr int LDB = RMAX + 1;
+  static constexpr int LDT = QMAX + 1;
+  static constexpr int BSZ = (LDB * QMAX > LDT * RMAX) ? LDB * QMAX : LDT * RMAX;
+  static constexpr int RA = 0;
+  static constexpr int RINV = RA + TRI;
+  static constexpr int W = RINV + TRI;
+  static constexpr int B = W + TRI;  // also T after the factorisation
+  static constexpr int WT = B + BSZ;
+  static constexpr int C = WT + LDT * RMAX;
+  static constexpr int D = C + RMAX * RMAX;
+  static constexpr int Y0 = D + RMAX * RMAX;
+  static constexpr int G = Y0 + QMAX;
+  static constexpr int WG = G + QMAX;
+  static constexpr int E1 = WG + QMAX;
+  static constexpr int AV = E1 + QMAX;
+  static constexpr int BV = AV + RMAX;
+  static constexpr int TOTAL = BV + RMAX;
+};
+
+struct MultiScalars {
+  double beta[2], v0[2];
+  double red[kMultiThreads / 32];
+  double score, rss, edf, yy;
+  double lam[kMaxPenalties];
+  double log_sp[kMaxPenalties];
+  double trial[kMaxPenalties];
+  double step[kMaxPenalties];
+  double grad_c[kMaxPenalties];
+  double hess_c[kMaxPenalties * kMaxPenalties];
+  double gradient[kMaxPenalties];
+  double newton[kMaxPenalties];
+  double steep[kMaxPenalties];
+  double ddelta[kMaxPenalties];
+  double drss[kMaxPenalties];
+  int status;
+  int nzrow[128];
+  int col_block[128];
+};
+
+__device__ double block_sum(double v, MultiScalars* sc) {
+  v = warp_sum(v);
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sc->red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+#pragma unroll
+  for (int w = 0; w < kMultiThreads / 32; ++w) s += sc->red[w];
+  return s;
+}
+
+// Householder reflector that maps (akk, B[0..nz)) onto (alpha, 0).
+__device__ void make_reflector(double* Ra, const double* Bk, int nz, int k, MultiScalars* sc, int slot) {
+  double sigma = 0.0;
+  for (int i = 0; i < nz; ++i) sigma += Bk[i] * Bk[i];
+  const double akk = Ra[tri(k, k)];
+  if (sigma == 0.0) {
+    sc->beta[slot] = 0.0;
+    sc->v0[slot] = 0.0;
+    return;
+  }
+  const double nrm = sqrt(akk * akk + sigma);
+  const double alpha = akk >= 0.0 ? -nrm : nrm;
+  const double v0 = akk - alpha;
+  sc->beta[slot] = 2.0 / (v0 * v0 + sigma);
+  sc->v0[slot] = v0;
+  Ra[tri(k, k)] = alpha;
+}
+
+// Objective at sc->trial: factor [R; B], W = R Ra^-1, score.  Leaves Ra, Rinv,
+// W, g, Wg in shared memory for multi_derivatives.
+template <int QMAX, int RMAX>
+__device__ void multi_core(const DesignDev& des, const double* __restrict__ arena, int n, double* sm,
+                           MultiScalars* sc) {
+  using L = MultiLayout<QMAX, RMAX>;
+  const int tid = threadIdx.x;
+  const int q = des.q, m = des.m, rs = des.rsum;
+  double* Ra = sm + L::RA;
+  double* Rinv = sm + L::RINV;
+  double* W = sm + L::W;
+  double* B = sm + L::B;
+  const double* R = arena + des.rmat;
+  const double* roots = arena + des.roots;
+  if (tid < m) sc->lam[tid] = exp(sc->trial[tid]);
+  for (int idx = tid; idx < L::LDB * q; idx += kMultiThreads) B[idx] = 0.0;
+  for (int c = 0; c < q; ++c)
+    for (int i = tid; i <= c; i += kMultiThreads) Ra[tri(i, c)] = R[i + static_cast<int64_t>(q) * c];
+  __syncthreads();
+  for (int j = 0; j < m; ++j) {
+    const double s = sqrt(sc->lam[j]);
+    const int dim = des.dim[j], rk = des.rank[j];
+    const double* root = roots + des.rootoff[j];
+    for (int idx = tid; idx < dim * rk; idx += kMultiThreads) {
+      const int a = idx % dim, c = idx / dim;  // root[a + dim c] -> B[rowoff + c, off + a]
+      B[(des.rowoff[j] + c) + L::LDB * (des.off[j] + a)] = s * root[idx];
+    }
+  }
+  __syncthreads();
+  if (tid == 0) make_reflector(Ra, B, sc->nzrow[0], 0, sc, 0);
+  __syncthreads();
+  for (int k = 0; k < q; ++k) {
+    const int slot = k & 1;
+    const double beta = sc->beta[slot];
+    const double v0 = sc->v0[slot];
+    const int nz = sc->nzrow[k];
+    const double* Bk = B + L::LDB * k;
+    const int j = tid;
+    if (j > k && j < q) {
+      double* Bj = B + L::LDB * j;
+      if (beta != 0.0) {
+        double w = v0 * Ra[tri(k, j)];
+        for (int i = 0; i < nz; ++i) w += Bk[i] * Bj[i];
+        w *= beta;
+        Ra[tri(k, j)] -= w * v0;
+        for (int i = 0; i < nz; ++i) Bj[i] -= w * Bk[i];
+      }
+      if (j == k + 1) make_reflector(Ra, Bj, sc->nzrow[j], j, sc, slot ^ 1);
+    }
+    __syncthreads();
+  }
+  // Rinv = Ra^-1 (upper triangular), thread per column
+  if (tid < q) {
+    const int c = tid;
+    const double dc = Ra[tri(c, c)];
+    if (dc == 0.0) sc->status = kStatusRank;
+    Rinv[tri(c, c)] = 1.0 / dc;
+    for (int r = c - 1; r >= 0; --r) {
+      double s = 0.0;
+      for (int t = r + 1; t <= c; ++t) s += Ra[tri(r, t)] * Rinv[tri(t, c)];
+      Rinv[tri(r, c)] = -s / Ra[tri(r, r)];
+    }
+  }
+  __syncthreads();
+  // W = R Rinv (upper triangular)
+  for (int c = 0; c < q; ++c)
+    for (int i = tid; i <= c; i += kMultiThreads) {
+      double s = 0.0;
+      for (int t = i; t <= c; ++t) s += R[i + static_cast<int64_t>(q) * t] * Rinv[tri(t, c)];
+      W[tri(i, c)] = s;
+    }
+  __syncthreads();
+  double* y0 = sm + L::Y0;
+  double* g = sm + L::G;
+  double* Wg = sm + L::WG;
+  double e = 0.0;
+  if (tid < q) {
+    const int c = tid;
+    double s = 0.0;
+    for (int i = 0; i <= c; ++i) {
+      const double w = W[tri(i, c)];
+      s += w * y0[i];
+      e += w * w;
+    }
+    g[c] = s;
+  }
+  const double edf = block_sum(e, sc);
+  double gg = 0.0;
+  if (tid < q) {
+    const int i = tid;
+    double s = 0.0;
+    for (int c = i; c < q; ++c) s += W[tri(i, c)] * g[c];
+    Wg[i] = s;
+    gg = g[i] * g[i] * -2.0 + s * s;
+  }
+  const double part = block_sum(gg, sc);
+  if (tid == 0) {
+    double rss = sc->yy + part;
+    if (rss < 0.0) rss = 0.0;
+    const double delta = static_cast<double>(n) - edf;
+    sc->rss = rss;
+    sc->edf = edf;
+    if (!(isfinite(rss) && isfinite(edf)) || delta <= 1e-8) {
+      sc->score = INFINITY;
+      if (sc->status == kStatusOk) sc->status = kStatusNumeric;
+    } else {
+      sc->score = static_cast<double>(n) * rss / (delta * delta);
+    }
+  }
+  __syncthreads();
+}
+
+// Gradient and Hessian of V at the point of the last multi_core call.
+template <int QMAX, int RMAX>
+__device__ void multi_derivatives(const DesignDev& des, const double* __restrict__ arena, int n, double* sm,
+                                  MultiScalars* sc) {
+  using L = MultiLayout<QMAX, RMAX>;
+  const int tid = threadIdx.x;
+  const int q = des.q, m = des.m, rs = des.rsum;
+  const double* Rinv = sm + L::RINV;
+  const double* W = sm + L::W;
+  double* T = sm + L::B;
+  double* WT = sm + L::WT;
+  double* C = sm + L::C;
+  double* D = sm + L::D;
+  const double* g = sm + L::G;
+  const double* Wg = sm + L::WG;
+  double* e1 = sm + L::E1;
+  double* av = sm + L::AV;
+  double* bv = sm + L::BV;
+  const double* roots = arena + des.roots;
+  // T(i, col) = sum_t Rinv(t, i) root_j(t - off_j, c): Ra^-T root
+  for (int idx = tid; idx < q * rs; idx += kMultiThreads) {
+    const int i = idx % q, col = idx / q;
+    const int j = sc->col_block[col];
+    const int c = col - des.rowoff[j];
+    const int off = des.off[j], dim = des.dim[j];
+    const double* root = roots + des.rootoff[j];
+    double s = 0.0;
+    const int tend = min(i, off + dim - 1);
+    for (int t = off; t <= tend; ++t) s += Rinv[tri(t, i)] * root[(t - off) + dim * c];
+    T[i + L::LDT * col] = s;
+  }
+  // e1 = g - W'(W g)
+  if (tid < q) {
+    const int c = tid;
+    double s = 0.0;
+    for (int i = 0; i <= c; ++i) s += W[tri(i, c)] * Wg[i];
+    e1[c] = g[c] - s;
+  }
+  __syncthreads();
+  // WT = W T
+  for (int idx = tid; idx < q * rs; idx += kMultiThreads) {
+    const int i = idx % q, col = idx / q;
+    const int j = sc->col_block[col];
+    double s = 0.0;
+    for (int t = max(i, des.off[j]); t < q; ++t) s += W[tri(i, t)] * T[t + L::LDT * col];
+    WT[i + L::LDT * col] = s;
+  }
+  // a = T'g, b = T'e1
+  if (tid < rs) {
+    double sa = 0.0, sb = 0.0;
+    for (int i = 0; i < q; ++i) {
+      const double tv = T[i + L::LDT * tid];
+      sa += tv * g[i];
+      sb += tv * e1[i];
+    }
+    av[tid] = sa;
+    bv[tid] = sb;
+  }
+  __syncthreads();
+  // C = T'T, D = (WT)'(WT): upper triangle, mirrored
+  for (int idx = tid; idx < rs * rs; idx += kMultiThreads) {
+    const int a = idx % rs, b = idx / rs;
+    if (a > b) continue;
+    double sc_ = 0.0, sd = 0.0;
+    for (int i = 0; i < q; ++i) {
+      sc_ += T[i + L::LDT * a] * T[i + L::LDT * b];
+      sd += WT[i + L::LDT * a] * WT[i + L::LDT * b];
+    }
+    C[a + RMAX * b] = sc_;
+    C[b + RMAX * a] = sc_;
+    D[a + RMAX * b] = sd;
+    D[b + RMAX * a] = sd;
+  }
+  __syncthreads();
+  if (tid < m) {
+    const int j = tid;
+    double dd = 0.0, dr = 0.0;
+    for (int a = des.rowoff[j]; a < des.rowoff[j] + des.rank[j]; ++a) {
+      dd += D[a + RMAX * a];
+      dr += bv[a] * av[a];
+    }
+    sc->ddelta[j] = sc->lam[j] * dd;
+    sc->drss[j] = 2.0 * sc->lam[j] * dr;
+  }
+  __syncthreads();
+  const double nd = static_cast<double>(n);
+  const double delta = nd - sc->edf;
+  const double s1 = nd / (delta * delta);
+  const double s2 = 2.0 * s1 * sc->rss / delta;
+  if (tid < m * m) {
+    const int i = tid % m, j = tid / m;
+    if (j <= i) {
+      double trmmp = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+      for (int a = des.rowoff[i]; a < des.rowoff[i] + des.rank[i]; ++a)
+        for (int b = des.rowoff[j]; b < des.rowoff[j] + des.rank[j]; ++b) {
+          const double cab = C[a + RMAX * b];
+          const double dab = D[a + RMAX * b];
+          trmmp += cab * dab;
+          t1 += av[b] * dab * av[a];  // a_j' D_ji a_i
+          t2 += bv[a] * cab * av[b];  // b_i' C_ij a_j
+          t3 += bv[b] * cab * av[a];  // b_j' C_ji a_i
+        }
+      const double ll = sc->lam[i] * sc->lam[j];
+      double d2delta = -2.0 * ll * trmmp;
+      double d2rss = 2.0 * ll * (t1 - t2 - t3);
+      if (i == j) {
+        d2delta += sc->ddelta[i];
+        d2rss += sc->drss[i];
+      }
+      const double h = -2.0 * s1 / delta * (sc->ddelta[j] * sc->drss[i] + sc->ddelta[i] * sc->drss[j]) +
+                       s1 * d2rss + 3.0 * s2 / delta * sc->ddelta[i] * sc->ddelta[j] - s2 * d2delta;
+      sc->hess_c[i + kMaxPenalties * j] = h;
+      sc->hess_c[j + kMaxPenalties * i] = h;
+    }
+  }
+  if (tid < m) sc->grad_c[tid] = s1 * sc->drss[tid] - s2 * sc->ddelta[tid];
+  __syncthreads();
+}
+
+// Newton step from the Hessian eigen-decomposition (cyclic Jacobi, m <= 8).
+__device__ void newton_from_hessian(int m, MultiScalars* sc, bool* steepest) {
+  double a[kMaxPenalties * kMaxPenalties];
+  double v[kMaxPenalties * kMaxPenalties];
+  for (int j = 0; j < m; ++j)
+    for (int i = 0; i < m; ++i) {
+      a[i + kMaxPenalties * j] = sc->hess_c[i + kMaxPenalties * j];
+      v[i + kMaxPenalties * j] = i == j ? 1.0 : 0.0;
+    }
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0.0, dg = 0.0;
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i) {
+        const double x = a[i + kMaxPenalties * j];
+        if (i == j) dg += x * x;
+        else off += x * x;
+      }
+    if (off == 0.0 || off <= 1e-32 * dg) break;
+    for (int p = 0; p < m - 1; ++p)
+      for (int r = p + 1; r < m; ++r) {
+        const double apq = a[p + kMaxPenalties * r];
+        if (apq == 0.0) continue;
+        const double theta = (a[r + kMaxPenalties * r] - a[p + kMaxPenalties * p]) / (2.0 * apq);
+        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0);
+        const double s = t * c;
+        for (int k = 0; k < m; ++k) {
+          const double akp = a[k + kMaxPenalties * p], akq = a[k + kMaxPenalties * r];
+          a[k + kMaxPenalties * p] = c * akp - s * akq;
+          a[k + kMaxPenalties * r] = s * akp + c * akq;
+        }
+        for (int k = 0; k < m; ++k) {
+          const double apk = a[p + kMaxPenalties * k], aqk = a[r + kMaxPenalties * k];
+          a[p + kMaxPenalties * k] = c * apk - s * aqk;
+          a[r + kMaxPenalties * k] = s * apk + c * aqk;
+        }
+        a[p + kMaxPenalties * r] = 0.0;
+        a[r + kMaxPenalties * p] = 0.0;
+        for (int k = 0; k < m; ++k) {
+          const double vkp = v[k + kMaxPenalties * p], vkq = v[k + kMaxPenalties * r];
+          v[k + kMaxPenalties * p] = c * vkp - s * vkq;
+          v[k + kMaxPenalties * r] = s * vkp + c * vkq;
+        }
+      }
+  }
+  bool neg = false;
+  for (int j = 0; j < m; ++j)
+    if (a[j + kMaxPenalties * j] < 0.0) neg = true;
+  *steepest = neg;
+  if (!neg) {
+    double proj[kMaxPenalties];
+    for (int c = 0; c < m; ++c) {
+      double s = 0.0;
+      for (int r = 0; r < m; ++r) s += v[r + kMaxPenalties * c] * sc->gradient[r];
+      proj[c] = s / a[c + kMaxPenalties * c];
+    }
+    double mx = 0.0;
+    for (int r = 0; r < m; ++r) {
+      double s = 0.0;
+      for (int c = 0; c < m; ++c) s += v[r + kMaxPenalties * c] * proj[c];
+      sc->newton[r] = -s;
+      mx = fmax(mx, fabs(sc->newton[r]));
+    }
+    if (mx > 5.0)
+      for (int r = 0; r < m; ++r) sc->newton[r] *= 5.0 / mx;
+  }
+  double mg = 0.0;
+  for (int r = 0; r < m; ++r) mg = fmax(mg, fabs(sc->gradient[r]));
+  for (int r = 0; r < m; ++r) sc->steep[r] = mg == 0.0 ? 0.0 : -sc->gradient[r] / mg;
+}
+
+}  // namespace
+
+template <int QMAX, int RMAX>
+__global__ void __launch_bounds__(kMultiThreads) fit_multi_kernel(
+    const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data,
+    int n, const FitJob* __restrict__ jobs, const int* __restrict__ job_index, int job_count,
+    double* __restrict__ residuals, FitResult* __restrict__ results) {
+  using L = MultiLayout<QMAX, RMAX>;
+  extern __shared__ double sm[];
+  __shared__ MultiScalars sc;
+  __shared__ int ctl[4];  // steepest, converged, trying, accepted
+  if (blockIdx.x >= job_count) return;
+  const int t = job_index[blockIdx.x];
+  const FitJob job = jobs[t];
+  const DesignDev& des = designs[job.design];
+  const int tid = threadIdx.x;
+  const int q = des.q, m = des.m;
+  const double* y = data + static_cast<int64_t>(n) * job.column;
+  const double* Q = arena + des.basis;
+  if (tid == 0) {
+    sc.status = kStatusOk;
+    int row = 0;
+    for (int c = 0; c < q; ++c) {
+      int nz = 0;
+      for (int j = 0; j < m; ++j)
+        if (des.off[j] <= c) nz = des.rowoff[j] + des.rank[j];
+      sc.nzrow[c] = nz;
+    }
+    for (int j = 0; j < m; ++j)
+      for (int c = 0; c < des.rank[j]; ++c) sc.col_block[row++] = j;
+  }
+  // y0 = Q'y, yy
+  double* y0 = sm + L::Y0;
+  {
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int c = warp; c < q; c += kMultiThreads / 32) {
+      double s = 0.0;
+      for (int i = lane; i < n; i += 32) s += Q[i + static_cast<int64_t>(n) * c] * y[i];
+      s = warp_sum(s);
+      if (lane == 0) y0[c] = s;
+    }
+    double yy = 0.0;
+    for (int i = tid; i < n; i += kMultiThreads) yy += y[i] * y[i];
+    yy = block_sum(yy, &sc);
+    if (tid == 0) sc.yy = yy;
+  }
+  if (tid < m) {
+    sc.log_sp[tid] = des.log_sp0[tid];
+    sc.trial[tid] = des.log_sp0[tid];
+  }
+  __syncthreads();
+  multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+  multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
+  double min_score = sc.score;
+  double score_red = 1e10;
+  bool steepest = false;
+  bool converged = false;
+  int calls = 1;
+  int it = 0;
+  const int max_half = 25;
+  if (tid < m) {
+    sc.gradient[tid] = 0.0;
+    sc.newton[tid] = 0.0;
+    sc.steep[tid] = 0.0;
+  }
+  __syncthreads();
+  for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
+    int tries = 0;
+    if (it > 1) {
+      if (tid < m) sc.step[tid] = steepest ? sc.steep[tid] : sc.newton[tid];
+      __syncthreads();
+      bool trying = true;
+      while (trying) {
+        ++tries;
+        if (tries == 4 && !steepest) {
+          steepest = true;
+          if (tid < m) sc.step[tid] = sc.steep[tid];
+        }
+        __syncthreads();
+        if (tid < m) sc.trial[tid] = sc.log_sp[tid] + sc.step[tid];
+        __syncthreads();
+        multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+        ++calls;
+        if (sc.status != kStatusOk) break;
+        const double tscore = sc.score;
+        if (tscore < min_score) {
+          trying = false;
+          score_red = min_score - tscore;
+          min_score = tscore;
+          if (tid < m) sc.log_sp[tid] = sc.trial[tid];
+          __syncthreads();
+          multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
+        } else {
+          if (tid < m) sc.step[tid] *= 0.5;
+        }
+        if (tries == max_half - 1 && trying)
+          if (tid < m) sc.step[tid] = 0.0;
+        if (tries == max_half) trying = false;
+        __syncthreads();
+      }
+      if (sc.status != kStatusOk) break;
+    }
+    if (it > 3) {
+      double g2 = 0.0;
+      for (int r = 0; r < m; ++r) g2 += sc.gradient[r] * sc.gradient[r];
+      converged = score_red <= kConvTol * (1.0 + min_score) &&
+                  sqrt(g2) <= pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(min_score));
+      if (tries == max_half) converged = true;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int r = 0; r < m; ++r) sc.gradient[r] = sc.grad_c[r];
+      bool st = false;
+      newton_from_hessian(m, &sc, &st);
+      ctl[0] = st ? 1 : 0;
+    }
+    __syncthreads();
+    steepest = ctl[0] != 0;
+    if (converged) break;
+  }
+  if (sc.status == kStatusOk && !converged) {
+    __syncthreads();
+    if (tid == 0) sc.status = kStatusNotConverged;
+    __syncthreads();
+  }
+  if (sc.status == kStatusOk) {
+    for (int c = 0; c < m; ++c) {
+      const double direction = sc.gradient[c] < 0.0 ? 1.0 : -1.0;
+      for (int probe = 0; probe < 5; ++probe) {
+        if (tid < m) sc.trial[tid] = sc.log_sp[tid] + (tid == c ? direction * 2.0 : 0.0);
+        __syncthreads();
+        multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+        ++calls;
+        if (sc.status != kStatusOk || !(sc.score < min_score)) break;
+        min_score = sc.score;
+        if (tid < m) sc.log_sp[tid] = sc.trial[tid];
+        __syncthreads();
+      }
+      if (sc.status != kStatusOk) break;
+    }
+  }
+  // final fit at the selected point
+  if (sc.status == kStatusOk) {
+    __syncthreads();
+    if (tid < m) sc.trial[tid] = sc.log_sp[tid];
+    __syncthreads();
+    multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+  }
+  const double* Wg = sm + L::WG;
+  double* r = residuals + static_cast<int64_t>(n) * job.out;
+  const bool ok = sc.status == kStatusOk;
+  for (int i = tid; i < n; i += kMultiThreads) {
+    double f = 0.0;
+    if (ok)
+      for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * Wg[c];
+    r[i] = ok ? y[i] - f : NAN;
+  }
+  if (tid == 0) {
+    FitResult res;
+    for (int j = 0; j < kMaxPenalties; ++j) res.log_sp[j] = j < m ? sc.log_sp[j] : NAN;
+    res.score = sc.score;
+    res.edf = sc.edf;
+    res.rss = sc.rss;
+    res.status = sc.status;
+    res.iterations = it;
+    res.evaluations = calls;
+    res.flags = 0;
+    results[t] = res;
+  }
+}
+
+size_t multi_smem_bytes(int qmax_class) {
+  if (qmax_class == 0) return sizeof(double) * MultiLayout<40, 32>::TOTAL;
+  return sizeof(double) * MultiLayout<76, 64>::TOTAL;
+}
+
+cudaError_t configure_fit_kernels() {
+  cudaError_t e = cudaFuncSetAttribute(fit_multi_kernel<40, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(multi_smem_bytes(0)));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(fit_multi_kernel<76, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(multi_smem_bytes(1)));
+}
+
+cudaError_t launch_fit_single(const DesignDev* designs, const double* arena, const double* data, int n,
+                              const FitJob* jobs, int count, double* residuals, FitResult* results,
+                              cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  const int warps = 8;
+  dim3 grid((count + warps - 1) / warps);
+  fit_single_kernel<<<grid, warps * 32, 0, stream>>>(designs, arena, data, n, jobs, count, residuals, results);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const double* arena, const double* data,
+                             int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
+                             FitResult* results, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  const size_t smem = multi_smem_bytes(qmax_class);
+  if (qmax_class == 0) {
+    auto k = fit_multi_kernel<40, 32>;
+    k<<<count, kMultiThreads, smem, stream>>>(designs, arena, data, n, jobs, job_index, count, residuals, results);
+  } else {
+    auto k = fit_multi_kernel<76, 64>;
+    k<<<count, kMultiThreads, smem, stream>>>(designs, arena, data, n, jobs, job_index, count, residuals, results);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace fkpc

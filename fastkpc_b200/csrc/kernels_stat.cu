@@ -1,0 +1,1081 @@
+// Independence statistics and p-values on the GPU (FP64).
+//
+// dCov (fastkpc/src/cuda/full_cuda_ci_vertical.cu:485-769 restated without
+// any n x n buffer): per component the row-centring constants
+// c_i = mean_j |r_i - r_j| - grand/2 (so A_ij = |r_i - r_j| - c_i - c_j), the
+// distance total and sum A^2; per pair sum A_ij B_ij over the upper triangle
+// with both residual vectors and their constants staged in shared memory,
+// then nV2, the gamma moments and the upper tail in the same CTA.
+//
+// Legacy low-rank dCov for the guard band (kpcalg/R/dcovgamma.R:51-100;
+// fastkpc/src/cuda/full_cuda_ci_vertical.cu:771-967): the num_col eigenpairs
+// of largest |value| of the raw distance matrix by Lanczos with full
+// re-orthogonalisation (distance entries recomputed on the fly), Ritz
+// vectors from inverse iteration on the tridiagonal, centred.
+//
+// HSIC (kpcalg/R/hsicgamma.R:52-99; fastkpc/src/cuda/full_cuda_ci_method_batch.cu:445-789):
+// kernlab-style incomplete Cholesky of the RBF Gram per component, pair
+// statistic |Gx' Gy|_F^2 / n^2, gamma moments, p = 1 - (1 - Q).
+// Permutation forms (fastkpc/src/cuda/full_cuda_ci_method_batch.cu:341-443,
+// :791-908): p = (1 + #{T_pi >= T}) / (R + 1).
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "device.h"
+#include "kernels.h"
+
+namespace fkpc {
+
+namespace {
+
+constexpr int kStatThreads = 256;
+constexpr double kIncholTol = 1e-3;
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ double block_sum256(double v, double* red) {
+  v = warp_sum(v);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+  return s;
+}
+
+// Regularised upper incomplete gamma Q(a, x): power series for x < a + 1,
+// modified Lentz continued fraction otherwise (the standard scheme of
+// Press et al., Numerical Recipes, section 6.2), relative tolerance 2e-15,
+// at most 10000 terms; *ok = 0 when the iteration cap is hit.
+__device__ double gamma_q(double a, double x, int* ok) {
+  *ok = 0;
+  if (!(a > 0.0) || !(x >= 0.0) || !isfinite(a) || !isfinite(x)) return NAN;
+  if (x == 0.0) {
+    *ok = 1;
+    return 1.0;
+  }
+  const double lpre = -x + a * log(x) - lgamma(a);
+  if (x < a + 1.0) {
+    double ap = a, sum = 1.0 / a, term = sum;
+    for (int it = 1; it <= 10000; ++it) {
+      ap += 1.0;
+      term *= x / ap;
+      sum += term;
+      if (fabs(term) <= fabs(sum) * 2e-15) {
+        *ok = 1;
+        const double lower = fmin(1.0, fmax(0.0, sum * exp(lpre)));
+        return fmin(1.0, fmax(0.0, 1.0 - lower));
+      }
+    }
+    return NAN;
+  }
+  const double tiny = 1e-300;
+  double b = x + 1.0 - a;
+  double c = 1.0 / tiny;
+  double d = 1.0 / fmax(fabs(b), tiny);
+  if (b < 0.0) d = -d;
+  double f = d;
+  for (int it = 1; it <= 10000; ++it) {
+    const double an = -it * (it - a);
+    b += 2.0;
+    d = an * d + b;
+    if (fabs(d) < tiny) d = copysign(tiny, d == 0.0 ? 1.0 : d);
+    c = b + an / c;
+    if (fabs(c) < tiny) c = copysign(tiny, c == 0.0 ? 1.0 : c);
+    d = 1.0 / d;
+    const double delta = d * c;
+    f *= delta;
+    if (fabs(delta - 1.0) <= 2e-15) {
+      *ok = 1;
+      return fmin(1.0, fmax(0.0, exp(lpre) * f));
+    }
+  }
+  return NAN;
+}
+
+__device__ double var_factor(double n) {
+  return 2.0 * (n - 4.0) * (n - 5.0) / n / (n - 1.0) / (n - 2.0) / (n - 3.0);
+}
+
+// statistic, moments -> record with the gamma upper tail
+__device__ void gamma_record(double stat, double mean, double var, bool hsic, RecordDev* out) {
+  out->statistic = stat;
+  out->mean = mean;
+  out->variance = var;
+  out->flags = 0;
+  if (!isfinite(stat) || !isfinite(mean) || !isfinite(var) || !(mean > 0.0) || !(var > 0.0)) {
+    out->status = kStatusNumeric;
+    out->p_value = NAN;
+    out->p_exact = NAN;
+    return;
+  }
+  const double shape = mean * mean / var;
+  const double scale = var / mean;
+  int ok = 0;
+  double p = gamma_q(shape, fmax(0.0, stat / scale), &ok);
+  if (!ok || !isfinite(p)) {
+    out->status = kStatusNotConverged;
+    out->p_value = NAN;
+    out->p_exact = NAN;
+    return;
+  }
+  if (hsic) p = 1.0 - (1.0 - fmin(1.0, fmax(0.0, p)));
+  out->status = kStatusOk;
+  out->p_value = p;
+  out->p_exact = p;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ dCov
+
+__global__ void __launch_bounds__(kStatThreads) dcov_component_kernel(const double* __restrict__ residuals, int n,
+                                                                       const int* __restrict__ comp_cols, int count,
+                                                                       double* __restrict__ centre,
+                                                                       DcovComponent* __restrict__ comps) {
+  extern __shared__ double sm[];
+  __shared__ double red[kStatThreads / 32];
+  const int comp = blockIdx.x;
+  if (comp >= count) return;
+  double* r = sm;
+  double* c = sm + n;
+  const double* src = residuals + static_cast<int64_t>(n) * comp_cols[comp];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) r[i] = src[i];
+  __syncthreads();
+  double part = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double ri = r[i];
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s += fabs(ri - r[j]);
+    c[i] = s;
+    part += s;
+  }
+  const double total = block_sum256(part, red);
+  const double nd = static_cast<double>(n);
+  const double half_grand = 0.5 * total / (nd * nd);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) c[i] = c[i] / nd - half_grand;
+  __syncthreads();
+  // sum A^2 over the upper triangle (rows i and n-1-i per thread), plus diagonal
+  double acc = 0.0;
+  const int half = (n + 1) / 2;
+  for (int t = threadIdx.x; t < half; t += blockDim.x) {
+    const int a = t, b = n - 1 - t;
+    {
+      const double ra = r[a], ca = c[a];
+      for (int j = a + 1; j < n; ++j) {
+        const double v = fabs(ra - r[j]) - ca - c[j];
+        acc += v * v;
+      }
+    }
+    if (b != a) {
+      const double rb = r[b], cb = c[b];
+      for (int j = b + 1; j < n; ++j) {
+        const double v = fabs(rb - r[j]) - cb - c[j];
+        acc += v * v;
+      }
+    }
+  }
+  double diag = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) diag += 4.0 * c[i] * c[i];
+  const double self = 2.0 * block_sum256(acc, red) + block_sum256(diag, red);
+  double* cout = centre + static_cast<int64_t>(n) * comp;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) cout[i] = c[i];
+  if (threadIdx.x == 0) {
+    comps[comp].total = total;
+    comps[comp].self = self;
+  }
+}
+
+__global__ void __launch_bounds__(kStatThreads) dcov_pair_kernel(const double* __restrict__ residuals, int n,
+                                                                  const int* __restrict__ comp_cols,
+                                                                  const double* __restrict__ centre,
+                                                                  const DcovComponent* __restrict__ comps,
+                                                                  const PairJob* __restrict__ pairs, int count,
+                                                                  RecordDev* __restrict__ records) {
+  extern __shared__ double sm[];
+  __shared__ double red[kStatThreads / 32];
+  const int t = blockIdx.x;
+  if (t >= count) return;
+  const PairJob job = pairs[t];
+  double* x = sm;
+  double* cx = sm + n;
+  double* y = sm + 2 * n;
+  double* cy = sm + 3 * n;
+  const double* xs = residuals + static_cast<int64_t>(n) * comp_cols[job.left];
+  const double* ys = residuals + static_cast<int64_t>(n) * comp_cols[job.right];
+  const double* cxs = centre + static_cast<int64_t>(n) * job.left;
+  const double* cys = centre + static_cast<int64_t>(n) * job.right;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    x[i] = xs[i];
+    y[i] = ys[i];
+    cx[i] = cxs[i];
+    cy[i] = cys[i];
+  }
+  __syncthreads();
+  double acc = 0.0;
+  const int half = (n + 1) / 2;
+  for (int tt = threadIdx.x; tt < half; tt += blockDim.x) {
+    const int a = tt, b = n - 1 - tt;
+    {
+      const double xa = x[a], ya = y[a], ca = cx[a], da = cy[a];
+      for (int j = a + 1; j < n; ++j) {
+        const double u = fabs(xa - x[j]) - ca - cx[j];
+        const double v = fabs(ya - y[j]) - da - cy[j];
+        acc = fma(u, v, acc);
+      }
+    }
+    if (b != a) {
+      const double xb = x[b], yb = y[b], cb = cx[b], db = cy[b];
+      for (int j = b + 1; j < n; ++j) {
+        const double u = fabs(xb - x[j]) - cb - cx[j];
+        const double v = fabs(yb - y[j]) - db - cy[j];
+        acc = fma(u, v, acc);
+      }
+    }
+  }
+  double diag = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) diag += 4.0 * cx[i] * cy[i];
+  const double sab = 2.0 * block_sum256(acc, red) + block_sum256(diag, red);
+  if (threadIdx.x == 0) {
+    const double nd = static_cast<double>(n);
+    const DcovComponent lx = comps[job.left], ly = comps[job.right];
+    RecordDev rec;
+    gamma_record(sab / nd, (lx.total / (nd * nd)) * (ly.total / (nd * nd)),
+                 var_factor(nd) * lx.self * ly.self / (nd * nd), false, &rec);
+    records[job.out] = rec;
+  }
+}
+
+// ------------------------------------------------------ legacy low rank
+
+namespace {
+
+constexpr int kLanczosMax = 384;
+
+// LU with partial pivoting of the tridiagonal (T - shift I), then solve; used
+// for inverse iteration.  d, e: diagonal / off-diagonal of T (size m).
+__device__ void tridiag_inverse_iteration(const double* d, const double* e, int m, double shift, double tnorm,
+                                          double* x, double* l, double* u0, double* u1, double* u2, int* piv) {
+  // factor
+  const double small = 2.220446049250313e-16 * tnorm;
+  double a = d[0] - shift;
+  double b = m > 1 ? e[0] : 0.0;
+  for (int i = 0; i < m; ++i) {
+    const double sub = i + 1 < m ? e[i] : 0.0;        // T(i+1, i)
+    const double dn = i + 1 < m ? d[i + 1] - shift : 0.0;
+    const double sup2 = i + 2 < m ? e[i + 1] : 0.0;   // T(i+1, i+2)
+    if (i + 1 < m && fabs(sub) > fabs(a)) {
+      // swap rows i and i+1
+      piv[i] = 1;
+      u0[i] = sub;
+      u1[i] = dn;
+      u2[i] = sup2;
+      const double mult = a / sub;
+      l[i] = mult;
+      a = b - mult * dn;
+      b = -mult * sup2;
+    } else {
+      piv[i] = 0;
+      double aa = a;
+      if (fabs(aa) < small) aa = aa >= 0.0 ? small : -small;
+      u0[i] = aa;
+      u1[i] = b;
+      u2[i] = 0.0;
+      const double mult = i + 1 < m ? sub / aa : 0.0;
+      l[i] = mult;
+      a = dn - mult * b;
+      b = sup2;
+    }
+  }
+  for (int sweep = 0; sweep < 3; ++sweep) {
+    // forward (apply L and pivots)
+    for (int i = 0; i + 1 < m; ++i) {
+      if (piv[i]) {
+        const double t = x[i];
+        x[i] = x[i + 1];
+        x[i + 1] = t - l[i] * x[i];
+      } else {
+        x[i + 1] -= l[i] * x[i];
+      }
+    }
+    // back substitution with U (diag u0, super u1, super-2 u2)
+    for (int i = m - 1; i >= 0; --i) {
+      double s = x[i];
+      if (i + 1 < m) s -= u1[i] * x[i + 1];
+      if (i + 2 < m) s -= u2[i] * x[i + 2];
+      double piv_ = u0[i];
+      if (fabs(piv_) < small) piv_ = piv_ >= 0.0 ? small : -small;
+      x[i] = s / piv_;
+    }
+    double nrm = 0.0;
+    for (int i = 0; i < m; ++i) nrm += x[i] * x[i];
+    nrm = sqrt(nrm);
+    for (int i = 0; i < m; ++i) x[i] /= nrm;
+  }
+}
+
+// eigenvalues of a symmetric tridiagonal matrix by implicit QL (values only)
+__device__ bool tridiag_values(double* d, double* e, int m) {
+  if (m <= 0) return true;
+  e[m - 1] = 0.0;
+  for (int l = 0; l < m; ++l) {
+    int iter = 0;
+    for (;;) {
+      int mm = l;
+      for (; mm < m - 1; ++mm) {
+        const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
+        if (fabs(e[mm]) <= 2.220446049250313e-16 * dd) break;
+      }
+      if (mm == l) break;
+      if (++iter > 60) return false;
+      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      double r = hypot(g, 1.0);
+      g = d[mm] - d[l] + e[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
+      double s = 1.0, c = 1.0, p = 0.0;
+      int i = mm - 1;
+      for (; i >= l; --i) {
+        double f = s * e[i];
+        const double bb = c * e[i];
+        r = hypot(f, g);
+        e[i + 1] = r;
+        if (r == 0.0) {
+          d[i + 1] -= p;
+          e[mm] = 0.0;
+          break;
+        }
+        s = f / r;
+        c = g / r;
+        g = d[i + 1] - p;
+        r = (d[i] - g) * s + 2.0 * c * bb;
+        p = s * r;
+        d[i + 1] = g + p;
+        g = c * r - bb;
+      }
+      if (r == 0.0 && i >= l) continue;
+      d[l] -= p;
+      e[l] = g;
+      e[mm] = 0.0;
+    }
+  }
+  return true;
+}
+
+struct LanczosShared {
+  double alpha[kLanczosMax];
+  double beta[kLanczosMax];
+  double td[kLanczosMax];
+  double te[kLanczosMax];
+  double theta[64];
+  int sel[64];
+  double coef[kLanczosMax];
+  double red[kStatThreads / 32];
+  int done;
+  int steps;
+  int fail;
+};
+
+}  // namespace
+
+// Grid-stride over the guarded components: CTA b handles slots b, b + grid,
+// ...  guard[1] holds the slot count, slot_comps the component of each slot.
+// workspace per CTA: V (n x (kLanczosMax+1)), S (kLanczosMax x 64) Ritz
+// coefficients, scratch 7 * kLanczosMax.
+__global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double* __restrict__ residuals, int n,
+                                                                     const int* __restrict__ comp_cols,
+                                                                     const int* __restrict__ guard,
+                                                                     const int* __restrict__ slot_comps, int cap,
+                                                                     int k, double* __restrict__ workspace,
+                                                                     double* __restrict__ vals,
+                                                                     double* __restrict__ vecs,
+                                                                     int* __restrict__ status) {
+  extern __shared__ double sm[];
+  __shared__ LanczosShared ls;
+  const int slots = min(guard[1], cap);
+  for (int slot = blockIdx.x; slot < slots; slot += gridDim.x) {
+  const int comp = slot_comps[slot];
+  const int tid = threadIdx.x;
+  const int maxit = min(n, kLanczosMax);
+  double* r = sm;
+  double* qv = sm + n;
+  double* w = sm + 2 * n;
+  const int64_t per = static_cast<int64_t>(n) * (kLanczosMax + 1) + static_cast<int64_t>(kLanczosMax) * 64 +
+                      6 * kLanczosMax + kLanczosMax;
+  double* V = workspace + per * blockIdx.x;
+  double* S = V + static_cast<int64_t>(n) * (kLanczosMax + 1);
+  double* scratch = S + static_cast<int64_t>(kLanczosMax) * 64;
+  const double* src = residuals + static_cast<int64_t>(n) * comp_cols[comp];
+  for (int i = tid; i < n; i += blockDim.x) r[i] = src[i];
+  if (tid == 0) {
+    ls.done = 0;
+    ls.fail = 0;
+    ls.steps = 0;
+    unsigned long state = 1;
+    double nrm = 0.0;
+    for (int i = 0; i < n; ++i) {
+      state = (state * 106UL + 1283UL) % 6075UL;
+      const double v = static_cast<double>(state) / 6075.0 - 0.5;
+      V[i] = v;
+      nrm += v * v;
+    }
+    nrm = sqrt(nrm);
+    for (int i = 0; i < n; ++i) V[i] /= nrm;
+  }
+  __syncthreads();
+  double anorm = 0.0;
+  for (int j = 0; j < maxit && !ls.done; ++j) {
+    double* vj = V + static_cast<int64_t>(n) * j;
+    for (int i = tid; i < n; i += blockDim.x) qv[i] = vj[i];
+    __syncthreads();
+    // w = D q, D_ij = |r_i - r_j|
+    double part = 0.0;
+    for (int i = tid; i < n; i += blockDim.x) {
+      const double ri = r[i];
+      double s = 0.0;
+      for (int t = 0; t < n; ++t) s += fabs(ri - r[t]) * qv[t];
+      w[i] = s;
+      part += s * qv[i];
+    }
+    const double alpha = block_sum256(part, ls.red);
+    const double bprev = j > 0 ? ls.beta[j - 1] : 0.0;
+    const double* vp = j > 0 ? V + static_cast<int64_t>(n) * (j - 1) : nullptr;
+    for (int i = tid; i < n; i += blockDim.x) {
+      double v = w[i] - alpha * qv[i];
+      if (vp) v -= bprev * vp[i];
+      w[i] = v;
+    }
+    __syncthreads();
+    // two passes of classical Gram-Schmidt against V[:, 0..j]
+    for (int pass = 0; pass < 2; ++pass) {
+      const int warp = tid >> 5, lane = tid & 31;
+      for (int b = warp; b <= j; b += blockDim.x >> 5) {
+        const double* vb = V + static_cast<int64_t>(n) * b;
+        double s = 0.0;
+        for (int i = lane; i < n; i += 32) s += w[i] * vb[i];
+        s = warp_sum(s);
+        if (lane == 0) ls.coef[b] = s;
+      }
+      __syncthreads();
+      for (int i = tid; i < n; i += blockDim.x) {
+        double s = w[i];
+        for (int b = 0; b <= j; ++b) s -= ls.coef[b] * V[i + static_cast<int64_t>(n) * b];
+        w[i] = s;
+      }
+      __syncthreads();
+    }
+    double nn = 0.0;
+    for (int i = tid; i < n; i += blockDim.x) nn += w[i] * w[i];
+    const double beta = sqrt(block_sum256(nn, ls.red));
+    anorm = fmax(anorm, fabs(alpha) + beta + bprev);
+    if (tid == 0) {
+      ls.alpha[j] = alpha;
+      ls.beta[j] = beta;
+      ls.steps = j + 1;
+    }
+    const bool invariant = beta <= 1e-15 * anorm;
+    const int m = j + 1;
+    const bool check = invariant || m == maxit || (m >= k + 10 && ((m - k) % 10 == 0));
+    __syncthreads();
+    if (check) {
+      if (tid == 0) {
+        for (int i = 0; i < m; ++i) {
+          ls.td[i] = ls.alpha[i];
+          ls.te[i] = i + 1 < m ? ls.beta[i] : 0.0;
+        }
+        if (!tridiag_values(ls.td, ls.te, m)) ls.fail = 1;
+        // select k largest |theta| (ties toward the lower index)
+        const int kk = min(k, m);
+        for (int c = 0; c < kk; ++c) {
+          int best = -1;
+          double bm = -1.0;
+          for (int i = 0; i < m; ++i) {
+            bool used = false;
+            for (int u = 0; u < c; ++u)
+              if (ls.sel[u] == i) used = true;
+            if (used) continue;
+            if (fabs(ls.td[i]) > bm) {
+              bm = fabs(ls.td[i]);
+              best = i;
+            }
+          }
+          ls.sel[c] = best;
+          ls.theta[c] = ls.td[best];
+        }
+      }
+      __syncthreads();
+      // Ritz coefficient vectors by inverse iteration on T (thread 0, one
+      // selected value after another, so one scratch set suffices)
+      const int kk = min(k, m);
+      double tnorm = 0.0;
+      for (int i = 0; i < m; ++i) tnorm = fmax(tnorm, fabs(ls.alpha[i]) + 2.0 * fabs(ls.beta[i]));
+      if (tid < kk) {
+        double* x = S + static_cast<int64_t>(kLanczosMax) * tid;
+        for (int i = 0; i < m; ++i) x[i] = (1.0 + 0.01 * ((i * 7 + tid) % 5)) / sqrt(static_cast<double>(m));
+      }
+      __syncthreads();
+      if (tid == 0) {
+        double* l = scratch;
+        double* u0 = scratch + kLanczosMax;
+        double* u1 = scratch + 2 * kLanczosMax;
+        double* u2 = scratch + 3 * kLanczosMax;
+        int* piv = reinterpret_cast<int*>(scratch + 4 * kLanczosMax);
+        for (int c = 0; c < kk; ++c) {
+          double* x = S + static_cast<int64_t>(kLanczosMax) * c;
+          tridiag_inverse_iteration(ls.alpha, ls.beta, m, ls.theta[c], tnorm, x, l, u0, u1, u2, piv);
+        }
+        bool conv = m >= k;
+        double tmax = 0.0;
+        for (int c = 0; c < kk; ++c) tmax = fmax(tmax, fabs(ls.theta[c]));
+        if (conv && !invariant) {
+          for (int c = 0; c < kk; ++c) {
+            const double resid = fabs(beta * S[static_cast<int64_t>(kLanczosMax) * c + (m - 1)]);
+            if (resid > 1e-13 * tmax) {
+              conv = false;
+              break;
+            }
+          }
+        }
+        if (conv || invariant || m == maxit) ls.done = 1;
+        if (ls.done && m < k) ls.fail = 1;
+      }
+      __syncthreads();
+    }
+    if (!ls.done) {
+      double* vn = V + static_cast<int64_t>(n) * (j + 1);
+      for (int i = tid; i < n; i += blockDim.x) vn[i] = w[i] / beta;
+      __syncthreads();
+    }
+  }
+  const int m = ls.steps;
+  // order selected values descending (the order does not change any statistic)
+  double* vout = vecs + static_cast<int64_t>(n) * k * slot;
+  for (int c = 0; c < k; ++c) {
+    const double* x = S + static_cast<int64_t>(kLanczosMax) * c;
+    double part = 0.0;
+    for (int i = tid; i < n; i += blockDim.x) {
+      double s = 0.0;
+      for (int b = 0; b < m; ++b) s += V[i + static_cast<int64_t>(n) * b] * x[b];
+      w[i] = s;
+      part += s;
+    }
+    const double mean = block_sum256(part, ls.red) / static_cast<double>(n);
+    for (int i = tid; i < n; i += blockDim.x) vout[i + static_cast<int64_t>(n) * c] = w[i] - mean;
+    __syncthreads();
+  }
+  if (tid < k) vals[static_cast<int64_t>(k) * slot + tid] = ls.theta[tid];
+  if (tid == 0) status[slot] = ls.fail ? kStatusNotConverged : kStatusOk;
+  __syncthreads();
+  }
+}
+
+// legacy pair: nV2 = sum l_i m_j (u_i . v_j)^2 / n; self moments per side.
+// CTA t handles guarded pair guard_pairs[t] when t < guard[0].
+__global__ void __launch_bounds__(kStatThreads) legacy_pair_kernel(int n, int k, const double* __restrict__ vals,
+                                                                    const double* __restrict__ vecs,
+                                                                    const DcovComponent* __restrict__ comps,
+                                                                    const int* __restrict__ guard,
+                                                                    const int* __restrict__ guard_pairs,
+                                                                    const int* __restrict__ comp_slot,
+                                                                    const PairJob* __restrict__ pairs, int count,
+                                                                    RecordDev* __restrict__ records) {
+  __shared__ double red[kStatThreads / 32];
+  const int t = blockIdx.x;
+  if (t >= count || t >= guard[0]) return;
+  const PairJob job = pairs[guard_pairs[t]];
+  const int sx = comp_slot[job.left], sy = comp_slot[job.right];
+  const double* Ux = vecs + static_cast<int64_t>(n) * k * sx;
+  const double* Uy = vecs + static_cast<int64_t>(n) * k * sy;
+  const double* lx = vals + static_cast<int64_t>(k) * sx;
+  const double* ly = vals + static_cast<int64_t>(k) * sy;
+  double cross = 0.0, selfx = 0.0, selfy = 0.0;
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+    const int a = e % k, b = e / k;
+    double cxy = 0.0, cxx = 0.0, cyy = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double ua = Ux[i + static_cast<int64_t>(n) * a], ub = Ux[i + static_cast<int64_t>(n) * b];
+      const double va = Uy[i + static_cast<int64_t>(n) * a], vb = Uy[i + static_cast<int64_t>(n) * b];
+      cxy += ua * vb;
+      cxx += ua * ub;
+      cyy += va * vb;
+    }
+    cross += lx[a] * ly[b] * cxy * cxy;
+    selfx += lx[a] * lx[b] * cxx * cxx;
+    selfy += ly[a] * ly[b] * cyy * cyy;
+  }
+  cross = block_sum256(cross, red);
+  selfx = block_sum256(selfx, red);
+  selfy = block_sum256(selfy, red);
+  if (threadIdx.x == 0) {
+    const double nd = static_cast<double>(n);
+    const DcovComponent cxm = comps[job.left], cym = comps[job.right];
+    RecordDev rec;
+    gamma_record(cross / nd, (cxm.total / (nd * nd)) * (cym.total / (nd * nd)),
+                 var_factor(nd) * selfx * selfy / (nd * nd), false, &rec);
+    RecordDev prev = records[job.out];
+    rec.p_exact = prev.p_exact;
+    rec.flags = prev.flags | FKPC_FLAG_GUARDED_DEV;
+    records[job.out] = rec;
+  }
+}
+
+
+// Guard band [lo, hi] on the exact-screen p: list the guarded pairs and give
+// every component they use a low-rank slot (order of slots is irrelevant).
+// guard: [0] pair count, [1] slot count, [2, 2+count) pair list,
+// then comp_slot[ncomp] and slot_comps[cap].
+__global__ void guard_select_kernel(const RecordDev* __restrict__ records, const PairJob* __restrict__ pairs,
+                                    int count, int ncomp, int cap, double lo, double hi, int* __restrict__ guard) {
+  int* list = guard + 2;
+  int* comp_slot = list + count;
+  int* slot_comps = comp_slot + ncomp;
+  if (threadIdx.x == 0) {
+    guard[0] = 0;
+    guard[1] = 0;
+  }
+  for (int c = threadIdx.x; c < ncomp; c += blockDim.x) comp_slot[c] = -1;
+  __syncthreads();
+  for (int t = threadIdx.x; t < count; t += blockDim.x) {
+    const PairJob job = pairs[t];
+    const RecordDev rec = records[job.out];
+    if (rec.status == kStatusOk && rec.p_exact >= lo && rec.p_exact <= hi) {
+      const int idx = atomicAdd(guard, 1);
+      list[idx] = t;
+      comp_slot[job.left] = -2;
+      comp_slot[job.right] = -2;
+    }
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < ncomp; c += blockDim.x) {
+    if (comp_slot[c] == -2) {
+      const int slot = atomicAdd(guard + 1, 1);
+      if (slot < cap) {
+        comp_slot[c] = slot;
+        slot_comps[slot] = c;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ HSIC
+
+__global__ void __launch_bounds__(kStatThreads) hsic_component_kernel(const double* __restrict__ residuals, int n,
+                                                                       const int* __restrict__ comp_cols, int count,
+                                                                       int max_rank, double sigma,
+                                                                       double* __restrict__ factors,
+                                                                       HsicComponent* __restrict__ comps) {
+  extern __shared__ double sm[];
+  __shared__ double red[kStatThreads / 32];
+  __shared__ double redv[kStatThreads / 32];
+  __shared__ int redi[kStatThreads / 32];
+  __shared__ double upper[64 * 64];
+  __shared__ double solve[64];
+  __shared__ int pivots[64];
+  __shared__ double s_tau;
+  __shared__ int s_pivot, s_rank, s_active;
+  __shared__ double s_residue;
+  const int comp = blockIdx.x;
+  if (comp >= count) return;
+  const int tid = threadIdx.x;
+  double* r = sm;
+  double* diag = sm + n;
+  double* col = sm + 2 * n;
+  double* G = factors + static_cast<int64_t>(n) * max_rank * comp;
+  const double* src = residuals + static_cast<int64_t>(n) * comp_cols[comp];
+  for (int i = tid; i < n; i += blockDim.x) {
+    r[i] = src[i];
+    diag[i] = 1.0;
+  }
+  if (tid == 0) {
+    s_residue = 1.0;
+    s_pivot = 0;
+    s_rank = 0;
+    s_active = 1;
+  }
+  __syncthreads();
+  while (true) {
+    if (tid == 0) s_active = (s_residue > kIncholTol && s_rank < max_rank) ? 1 : 0;
+    __syncthreads();
+    if (!s_active) break;
+    const double rp = r[s_pivot];
+    for (int i = tid; i < n; i += blockDim.x) {
+      const double d = r[i] - rp;
+      col[i] = exp(-sigma * d * d);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const int rank = s_rank;
+      double tau2 = col[s_pivot];
+      for (int row = 0; row < rank; ++row) {
+        double v = col[pivots[row]];
+        for (int prev = 0; prev < row; ++prev) v -= upper[prev + 64 * row] * solve[prev];
+        solve[row] = v / upper[row + 64 * row];
+        tau2 -= solve[row] * solve[row];
+        upper[row + 64 * rank] = solve[row];
+      }
+      if (!(tau2 > 0.0) || !isfinite(tau2)) {
+        s_active = 0;
+      } else {
+        s_tau = sqrt(tau2);
+        upper[rank + 64 * rank] = s_tau;
+      }
+    }
+    __syncthreads();
+    if (!s_active) break;
+    const int rank = s_rank;
+    const double tau = s_tau;
+    for (int i = tid; i < n; i += blockDim.x) {
+      double proj = 0.0;
+      for (int prev = 0; prev < rank; ++prev) proj += G[i + static_cast<int64_t>(n) * prev] * solve[prev];
+      const double upd = (col[i] - proj) / tau;
+      G[i + static_cast<int64_t>(n) * rank] = upd;
+      diag[i] -= upd * upd;
+    }
+    __syncthreads();
+    // argmax of the residual diagonal, first index on ties
+    double bv = -INFINITY;
+    int bi = 0x7fffffff;
+    for (int i = tid; i < n; i += blockDim.x) {
+      if (diag[i] > bv) {
+        bv = diag[i];
+        bi = i;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) {
+        bv = ov;
+        bi = oi;
+      }
+    }
+    const int warp = tid >> 5, lane = tid & 31;
+    if (lane == 0) {
+      redv[warp] = bv;
+      redi[warp] = bi;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double best = redv[0];
+      int besti = redi[0];
+      for (int w2 = 1; w2 < (int)(blockDim.x >> 5); ++w2)
+        if (redv[w2] > best || (redv[w2] == best && redi[w2] < besti)) {
+          best = redv[w2];
+          besti = redi[w2];
+        }
+      pivots[s_rank] = s_pivot;
+      s_rank = s_rank + 1;
+      s_residue = best;
+      s_pivot = besti;
+    }
+    __syncthreads();
+  }
+  const int rank = s_rank;
+  // off-diagonal sum of G G' from the raw factor, then centre columns
+  double off = 0.0;
+  double* colsum = col;  // reuse: column sums in shared memory
+  for (int c = 0; c < rank; ++c) {
+    double s = 0.0, s2 = 0.0;
+    for (int i = tid; i < n; i += blockDim.x) {
+      const double v = G[i + static_cast<int64_t>(n) * c];
+      s += v;
+      s2 += v * v;
+    }
+    s = block_sum256(s, red);
+    s2 = block_sum256(s2, red);
+    off += s * s - s2;
+    if (tid == 0) colsum[c] = s;
+    __syncthreads();
+  }
+  for (int c = 0; c < rank; ++c) {
+    const double mean = colsum[c] / static_cast<double>(n);
+    for (int i = tid; i < n; i += blockDim.x) G[i + static_cast<int64_t>(n) * c] -= mean;
+  }
+  __syncthreads();
+  // |Gc' Gc|_F^2
+  double self = 0.0;
+  for (int e = tid; e < rank * rank; e += blockDim.x) {
+    const int a = e % rank, b = e / rank;
+    double d = 0.0;
+    for (int i = 0; i < n; ++i) d += G[i + static_cast<int64_t>(n) * a] * G[i + static_cast<int64_t>(n) * b];
+    self += d * d;
+  }
+  self = block_sum256(self, red);
+  if (tid == 0) {
+    comps[comp].offdiag = off;
+    comps[comp].self = self;
+    comps[comp].rank = rank;
+    comps[comp].status = kStatusOk;
+  }
+}
+
+__device__ double hsic_cross(int n, const double* Gx, int rx, const double* Gy, int ry, const int* perm,
+                             double* red) {
+  double acc = 0.0;
+  for (int e = threadIdx.x; e < rx * ry; e += blockDim.x) {
+    const int a = e % rx, b = e / rx;
+    const double* ga = Gx + static_cast<int64_t>(n) * a;
+    const double* gb = Gy + static_cast<int64_t>(n) * b;
+    double d = 0.0;
+    if (perm)
+      for (int i = 0; i < n; ++i) d += ga[i] * gb[perm[i]];
+    else
+      for (int i = 0; i < n; ++i) d += ga[i] * gb[i];
+    acc += d * d;
+  }
+  return block_sum256(acc, red);
+}
+
+__global__ void __launch_bounds__(kStatThreads) hsic_pair_kernel(int n, int max_rank, const double* __restrict__ factors,
+                                                                  const HsicComponent* __restrict__ comps,
+                                                                  const PairJob* __restrict__ pairs, int count,
+                                                                  RecordDev* __restrict__ records) {
+  __shared__ double red[kStatThreads / 32];
+  const int t = blockIdx.x;
+  if (t >= count) return;
+  const PairJob job = pairs[t];
+  const HsicComponent cx = comps[job.left], cy = comps[job.right];
+  const double* Gx = factors + static_cast<int64_t>(n) * max_rank * job.left;
+  const double* Gy = factors + static_cast<int64_t>(n) * max_rank * job.right;
+  const double s = hsic_cross(n, Gx, cx.rank, Gy, cy.rank, nullptr, red);
+  if (threadIdx.x == 0) {
+    const double nd = static_cast<double>(n);
+    const double mux = cx.offdiag / (nd * (nd - 1.0));
+    const double muy = cy.offdiag / (nd * (nd - 1.0));
+    RecordDev rec;
+    gamma_record(s / (nd * nd), (1.0 + mux * muy - mux - muy) / nd,
+                 var_factor(nd) * cx.self * cy.self / (nd * nd * nd * nd), true, &rec);
+    records[job.out] = rec;
+  }
+}
+
+__global__ void __launch_bounds__(kStatThreads) hsic_perm_pair_kernel(int n, int max_rank,
+                                                                       const double* __restrict__ factors,
+                                                                       const HsicComponent* __restrict__ comps,
+                                                                       const PairJob* __restrict__ pairs, int count,
+                                                                       const int* __restrict__ perms, int replicates,
+                                                                       RecordDev* __restrict__ records) {
+  __shared__ double red[kStatThreads / 32];
+  const int t = blockIdx.x;
+  if (t >= count) return;
+  const PairJob job = pairs[t];
+  const HsicComponent cx = comps[job.left], cy = comps[job.right];
+  const double* Gx = factors + static_cast<int64_t>(n) * max_rank * job.left;
+  const double* Gy = factors + static_cast<int64_t>(n) * max_rank * job.right;
+  const double nd = static_cast<double>(n);
+  const double obs = hsic_cross(n, Gx, cx.rank, Gy, cy.rank, nullptr, red) / (nd * nd);
+  int exceed = 1;
+  for (int rep = 0; rep < replicates; ++rep) {
+    const int* pi = perms + (static_cast<int64_t>(t) * replicates + rep) * n;
+    const double s = hsic_cross(n, Gx, cx.rank, Gy, cy.rank, pi, red) / (nd * nd);
+    if (s >= obs) ++exceed;
+  }
+  if (threadIdx.x == 0) {
+    RecordDev rec;
+    rec.statistic = obs;
+    rec.mean = NAN;
+    rec.variance = NAN;
+    rec.p_value = static_cast<double>(exceed) / static_cast<double>(replicates + 1);
+    rec.p_exact = rec.p_value;
+    rec.status = kStatusOk;
+    rec.flags = 0;
+    records[job.out] = rec;
+  }
+}
+
+__global__ void __launch_bounds__(kStatThreads) dcc_perm_pair_kernel(const double* __restrict__ residuals, int n,
+                                                                      const int* __restrict__ comp_cols,
+                                                                      const double* __restrict__ centre,
+                                                                      const PairJob* __restrict__ pairs, int count,
+                                                                      const int* __restrict__ perms, int replicates,
+                                                                      RecordDev* __restrict__ records) {
+  extern __shared__ double sm[];
+  __shared__ double red[kStatThreads / 32];
+  const int t = blockIdx.x;
+  if (t >= count) return;
+  const PairJob job = pairs[t];
+  double* x = sm;
+  double* cx = sm + n;
+  double* y = sm + 2 * n;
+  double* cy = sm + 3 * n;
+  const double* xs = residuals + static_cast<int64_t>(n) * comp_cols[job.left];
+  const double* ys = residuals + static_cast<int64_t>(n) * comp_cols[job.right];
+  const double* cxs = centre + static_cast<int64_t>(n) * job.left;
+  const double* cys = centre + static_cast<int64_t>(n) * job.right;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    x[i] = xs[i];
+    cx[i] = cxs[i];
+  }
+  const double nd = static_cast<double>(n);
+  double obs = 0.0;
+  int exceed = 1;
+  for (int rep = -1; rep < replicates; ++rep) {
+    const int* pi = rep >= 0 ? perms + (static_cast<int64_t>(t) * replicates + rep) * n : nullptr;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int src = pi ? pi[i] : i;
+      y[i] = ys[src];
+      cy[i] = cys[src];
+    }
+    __syncthreads();
+    double acc = 0.0;
+    const int half = (n + 1) / 2;
+    for (int tt = threadIdx.x; tt < half; tt += blockDim.x) {
+      const int a = tt, b = n - 1 - tt;
+      {
+        const double xa = x[a], ya = y[a], ca = cx[a], da = cy[a];
+        for (int j = a + 1; j < n; ++j) acc = fma(fabs(xa - x[j]) - ca - cx[j], fabs(ya - y[j]) - da - cy[j], acc);
+      }
+      if (b != a) {
+        const double xb = x[b], yb = y[b], cb = cx[b], db = cy[b];
+        for (int j = b + 1; j < n; ++j) acc = fma(fabs(xb - x[j]) - cb - cx[j], fabs(yb - y[j]) - db - cy[j], acc);
+      }
+    }
+    double diag = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) diag += 4.0 * cx[i] * cy[i];
+    const double s = (2.0 * block_sum256(acc, red) + block_sum256(diag, red)) / nd;
+    if (rep < 0) obs = s;
+    else if (s >= obs) ++exceed;
+  }
+  if (threadIdx.x == 0) {
+    RecordDev rec;
+    rec.statistic = obs;
+    rec.mean = NAN;
+    rec.variance = NAN;
+    rec.p_value = static_cast<double>(exceed) / static_cast<double>(replicates + 1);
+    rec.p_exact = rec.p_value;
+    rec.status = kStatusOk;
+    rec.flags = 0;
+    records[job.out] = rec;
+  }
+}
+
+// ------------------------------------------------------- FP64 peak probe
+
+// 16 independent FMA chains per thread; the result is written so the chains
+// are not removed.  Flops per launch: 2 * 16 * iters * threads.
+__global__ void __launch_bounds__(256) fp64_fma_kernel(double* __restrict__ out, int iters, double a, double b) {
+  double x[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) x[k] = 1e-3 * (threadIdx.x + k);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = fma(x[k], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) s += x[k];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+cudaError_t launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t stream) {
+  fp64_fma_kernel<<<blocks, 256, 0, stream>>>(out, iters, 0.9999999, 1e-7);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------- launchers
+
+cudaError_t configure_stat_kernels(int n) {
+  const int s2 = static_cast<int>(sizeof(double) * 2 * n);
+  const int s3 = static_cast<int>(sizeof(double) * 3 * n);
+  const int s4 = static_cast<int>(sizeof(double) * 4 * n);
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(dcov_component_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s2)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(dcov_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s4)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(dcc_perm_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s4)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(legacy_eigen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s3)) != cudaSuccess) return e;
+  return cudaFuncSetAttribute(hsic_component_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s3);
+}
+
+cudaError_t launch_dcov_components(const double* residuals, int n, const int* comp_cols, int count,
+                                   double* centre, DcovComponent* comps, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  const size_t smem = sizeof(double) * 2 * n;
+  dcov_component_kernel<<<count, kStatThreads, smem, stream>>>(residuals, n, comp_cols, count, centre, comps);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dcov_pairs(const double* residuals, int n, const int* comp_cols, const double* centre,
+                              const DcovComponent* comps, const PairJob* pairs, int count, RecordDev* records,
+                              cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  const size_t smem = sizeof(double) * 4 * n;
+  dcov_pair_kernel<<<count, kStatThreads, smem, stream>>>(residuals, n, comp_cols, centre, comps, pairs, count,
+                                                           records);
+  return cudaGetLastError();
+}
+
+size_t legacy_eigen_workspace_doubles(int n, int ctas) {
+  const size_t per = static_cast<size_t>(n) * (kLanczosMax + 1) + static_cast<size_t>(kLanczosMax) * 64 +
+                     6 * kLanczosMax + kLanczosMax;
+  return per * static_cast<size_t>(ctas);
+}
+
+cudaError_t launch_guard_select(const RecordDev* records, const PairJob* pairs, int count, int ncomp, int cap,
+                                double lo, double hi, int* guard, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  guard_select_kernel<<<1, 1024, 0, stream>>>(records, pairs, count, ncomp, cap, lo, hi, guard);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_legacy_eigen(const double* residuals, int n, const int* comp_cols, const int* guard,
+                                const int* slot_comps, int cap, int ctas, int num_col, double* workspace,
+                                double* lowrank_vals, double* lowrank_vecs, int* status, cudaStream_t stream) {
+  if (cap <= 0 || ctas <= 0) return cudaSuccess;
+  if (num_col > 64) return cudaErrorInvalidValue;
+  const size_t smem = sizeof(double) * 3 * n;
+  legacy_eigen_kernel<<<ctas, kStatThreads, smem, stream>>>(residuals, n, comp_cols, guard, slot_comps, cap,
+                                                             num_col, workspace, lowrank_vals, lowrank_vecs, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_legacy_pairs(int n, int num_col, const double* lowrank_vals, const double* lowrank_vecs,
+                                const DcovComponent* comps, const int* guard, const int* guard_pairs,
+                                const int* comp_slot, const PairJob* pairs, int count, RecordDev* records,
+                                cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  legacy_pair_kernel<<<count, kStatThreads, 0, stream>>>(n, num_col, lowrank_vals, lowrank_vecs, comps, guard,
+                                                         guard_pairs, comp_slot, pairs, count, records);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hsic_components(const double* residuals, int n, const int* comp_cols, int count, int num_col,
+                                   double sig, double* factors, HsicComponent* comps, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  if (num_col > 64) return cudaErrorInvalidValue;
+  const size_t smem = sizeof(double) * 3 * n;
+  hsic_component_kernel<<<count, kStatThreads, smem, stream>>>(residuals, n, comp_cols, count, num_col, 1.0 / sig,
+                                                                factors, comps);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hsic_pairs(int n, int num_col, const double* factors, const HsicComponent* comps,
+                              const PairJob* pairs, int count, RecordDev* records, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  hsic_pair_kernel<<<count, kStatThreads, 0, stream>>>(n, num_col, factors, comps, pairs, count, records);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hsic_perm_pairs(int n, int num_col, const double* factors, const HsicComponent* comps,
+                                   const PairJob* pairs, int count, const int* perms, int replicates,
+                                   RecordDev* records, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  hsic_perm_pair_kernel<<<count, kStatThreads, 0, stream>>>(n, num_col, factors, comps, pairs, count, perms,
+                                                            replicates, records);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dcc_perm_pairs(const double* residuals, int n, const int* comp_cols, const double* centre,
+                                  const PairJob* pairs, int count, const int* perms, int replicates,
+                                  RecordDev* records, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  const size_t smem = sizeof(double) * 4 * n;
+  dcc_perm_pair_kernel<<<count, kStatThreads, smem, stream>>>(residuals, n, comp_cols, centre, pairs, count, perms,
+                                                               replicates, records);
+  return cudaGetLastError();
+}
+
+}  // namespace fkpc

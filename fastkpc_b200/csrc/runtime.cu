@@ -1,0 +1,892 @@
+// Batched CI-test engine (host orchestration of the device pipeline).
+//
+// A batch of tests (x, y, S) becomes:
+//   * designs     -- one per distinct non-empty S (host set-up, cached);
+//   * components  -- one per distinct (target, S): a residual column of the
+//                    device slab (|S| = 0 columns are copied, not fitted);
+//   * pairs       -- one per test: (component of x, component of y).
+// The device work of a batch is a fixed launch sequence on one stream:
+//   gather direct columns -> fit (single / multi) -> method statistics
+//   [-> guard select -> low-rank eigen -> low-rank pairs for dcc.gamma],
+// captured once as a CUDA graph and replayed by execute().
+#include "runtime.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <thread>
+
+namespace fkpc {
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error(FKPC_STATUS_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+__global__ void gather_columns_kernel(const double* __restrict__ data, int n, const int* __restrict__ cols,
+                                      const int* __restrict__ slots, int count, double* __restrict__ slab) {
+  const int c = blockIdx.y;
+  if (c >= count) return;
+  const double* src = data + static_cast<int64_t>(n) * cols[c];
+  double* dst = slab + static_cast<int64_t>(n) * slots[c];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+template <class T>
+double upload(DevBuf<T>& buf, const std::vector<T>& host, cudaStream_t s) {
+  T* d = buf.ensure(host.size());
+  if (!host.empty()) cuda_check(cudaMemcpyAsync(d, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+  return static_cast<double>(host.size() * sizeof(T));
+}
+
+constexpr double kGuardLower = 0.05;
+constexpr double kGuardUpper = 0.15;
+constexpr int kLegacyCtas = 296;  // 2 x 148 SMs
+
+}  // namespace
+
+Engine::Engine(int device) : device_(device) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count <= 0) throw Error(FKPC_STATUS_NO_DEVICE, "no CUDA device is available");
+  if (device < 0 || device >= count) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "CUDA device ordinal out of range");
+  cuda_check(cudaSetDevice(device), "cudaSetDevice");
+  cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (auto& ev : ev_) cuda_check(cudaEventCreate(&ev), "cudaEventCreate");
+}
+
+Engine::~Engine() {
+  cudaSetDevice(device_);
+  release_graph();
+  for (auto& ev : ev_)
+    if (ev) cudaEventDestroy(ev);
+  if (stream_) {
+    cudaStreamSynchronize(stream_);
+    cudaStreamDestroy(stream_);
+  }
+}
+
+void Engine::release_graph() {
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  graph_exec_ = nullptr;
+  graph_ = nullptr;
+}
+
+void Engine::load(const double* data, int n, int p) {
+  if (n <= 5 || p < 2) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "data must have n > 5 rows and p >= 2 columns");
+  for (size_t i = 0; i < static_cast<size_t>(n) * p; ++i)
+    if (!std::isfinite(data[i])) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "data must contain finite doubles");
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  n_ = n;
+  p_ = p;
+  host_data_.assign(data, data + static_cast<size_t>(n) * p);
+  double* d = d_data_.ensure(host_data_.size());
+  cuda_check(cudaMemcpyAsync(d, host_data_.data(), host_data_.size() * sizeof(double), cudaMemcpyHostToDevice, stream_),
+             "upload data");
+  cuda_check(cudaStreamSynchronize(stream_), "upload data");
+  cache_.reset(new DesignCache(host_data_.data(), n, p));
+  release_graph();
+}
+
+void Engine::plan_components(const std::vector<Test>& tests) {
+  tests_ = tests;
+  sets_.clear();
+  comps_.clear();
+  pairs_.clear();
+  std::map<std::vector<int>, int> set_index;
+  std::map<std::pair<int, int>, int> comp_index;  // (target, set or -1)
+  const bool share = opt_.mode != FKPC_MODE_PLAIN;  // the plain form fits every test on its own
+  auto component = [&](int target, int set) {
+    auto key = std::make_pair(target, set);
+    auto it = comp_index.find(key);
+    if (share && it != comp_index.end()) return it->second;
+    const int id = static_cast<int>(comps_.size());
+    comps_.push_back(Component{target, set});
+    comp_index[key] = id;
+    return id;
+  };
+  for (size_t t = 0; t < tests_.size(); ++t) {
+    Test& ts = tests_[t];
+    if (ts.x < 0 || ts.x >= p_ || ts.y < 0 || ts.y >= p_ || ts.x == ts.y)
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "test variables out of range");
+    std::sort(ts.S.begin(), ts.S.end());
+    for (size_t i = 0; i < ts.S.size(); ++i) {
+      if (ts.S[i] < 0 || ts.S[i] >= p_ || ts.S[i] == ts.x || ts.S[i] == ts.y || (i > 0 && ts.S[i] == ts.S[i - 1]))
+        throw Error(FKPC_STATUS_INVALID_ARGUMENT, "conditioning set must hold distinct variables other than x and y");
+    }
+    if (static_cast<int>(ts.S.size()) > kMaxPenalties)
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "conditioning sets larger than 8 are not supported by this build");
+    int set = -1;
+    if (!ts.S.empty()) {
+      auto it = set_index.find(ts.S);
+      if (it == set_index.end()) {
+        set = static_cast<int>(sets_.size());
+        sets_.push_back(ts.S);
+        set_index[ts.S] = set;
+      } else {
+        set = it->second;
+      }
+    }
+    PairJob job;
+    job.left = component(ts.x, set);
+    job.right = component(ts.y, set);
+    job.out = static_cast<int>(t);
+    job.pad = 0;
+    pairs_.push_back(job);
+  }
+}
+
+void Engine::build_designs() {
+  designs_.assign(sets_.size(), nullptr);
+  std::atomic<size_t> next(0);
+  std::string err;
+  std::mutex err_mu;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t workers = std::min<size_t>(hw, std::max<size_t>(1, sets_.size()));
+  auto work = [&]() {
+    for (;;) {
+      const size_t i = next.fetch_add(1);
+      if (i >= sets_.size()) return;
+      try {
+        designs_[i] = cache_->get(sets_[i]);
+      } catch (const std::exception& e) {
+        std::lock_guard<std::mutex> lock(err_mu);
+        if (err.empty()) err = e.what();
+      }
+    }
+  };
+  if (workers <= 1) {
+    work();
+  } else {
+    std::vector<std::thread> pool;
+    for (size_t w = 0; w < workers; ++w) pool.emplace_back(work);
+    for (auto& th : pool) th.join();
+  }
+  if (!err.empty()) throw Error(FKPC_STATUS_RANK, "design set-up failed: " + err);
+}
+
+void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
+  const int n = n_;
+  std::vector<double> arena;
+  std::vector<DesignDev> ddesc(designs_.size());
+  for (size_t d = 0; d < designs_.size(); ++d) {
+    const Design& des = *designs_[d];
+    DesignDev& dd = ddesc[d];
+    std::memset(&dd, 0, sizeof(dd));
+    dd.q = des.q;
+    dd.m = des.m;
+    if (des.m == 1) {
+      if (des.q > kMaxSingleQ) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "single-penalty design too wide");
+      dd.kind = 1;
+      dd.basis = static_cast<int64_t>(arena.size());
+      arena.insert(arena.end(), des.QW.begin(), des.QW.end());
+      dd.spec = static_cast<int64_t>(arena.size());
+      arena.insert(arena.end(), des.spec.begin(), des.spec.end());
+      dd.log_sp0[0] = des.initial_log_sp[0];
+      dd.off[0] = des.offsets[0];
+      dd.dim[0] = des.dims[0];
+      dd.rank[0] = des.ranks[0];
+      dd.rsum = des.ranks[0];
+    } else {
+      dd.kind = 2;
+      dd.basis = static_cast<int64_t>(arena.size());
+      arena.insert(arena.end(), des.Q.begin(), des.Q.end());
+      dd.rmat = static_cast<int64_t>(arena.size());
+      arena.insert(arena.end(), des.R.begin(), des.R.end());
+      dd.roots = static_cast<int64_t>(arena.size());
+      int rows = 0;
+      int64_t rootoff = 0;
+      for (int j = 0; j < des.m; ++j) {
+        dd.off[j] = des.offsets[j];
+        dd.dim[j] = des.dims[j];
+        dd.rank[j] = des.ranks[j];
+        dd.rowoff[j] = rows;
+        dd.rootoff[j] = static_cast<int>(rootoff);
+        dd.log_sp0[j] = des.initial_log_sp[j];
+        rows += des.ranks[j];
+        arena.insert(arena.end(), des.roots[j].begin(), des.roots[j].end());
+        rootoff += static_cast<int64_t>(des.roots[j].size());
+      }
+      dd.rsum = rows;
+      if (des.q > 76 || rows > 64) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity");
+    }
+  }
+  single_jobs_.clear();
+  multi_jobs_.clear();
+  multi_small_.clear();
+  multi_large_.clear();
+  direct_cols_.clear();
+  direct_slots_.clear();
+  plain_single_off_.clear();
+  plain_small_off_.clear();
+  plain_large_off_.clear();
+  plain_direct_off_.clear();
+  for (size_t c = 0; c < comps_.size(); ++c) {
+    if (opt.mode == FKPC_MODE_PLAIN && c % 2 == 0) {
+      plain_single_off_.push_back(static_cast<int>(single_jobs_.size()));
+      plain_small_off_.push_back(static_cast<int>(multi_small_.size()));
+      plain_large_off_.push_back(static_cast<int>(multi_large_.size()));
+      plain_direct_off_.push_back(static_cast<int>(direct_cols_.size()));
+    }
+    const Component& cp = comps_[c];
+    if (cp.design < 0) {
+      direct_cols_.push_back(cp.target);
+      direct_slots_.push_back(static_cast<int>(c));
+      continue;
+    }
+    FitJob job{cp.design, cp.target, static_cast<int>(c), 0};
+    const DesignDev& dd = ddesc[cp.design];
+    if (dd.kind == 1) {
+      single_jobs_.push_back(job);
+    } else {
+      const int idx = static_cast<int>(multi_jobs_.size());
+      multi_jobs_.push_back(job);
+      if (dd.q <= 40 && dd.rsum <= 32) multi_small_.push_back(idx);
+      else multi_large_.push_back(idx);
+    }
+  }
+  if (opt.mode == FKPC_MODE_PLAIN) {
+    plain_single_off_.push_back(static_cast<int>(single_jobs_.size()));
+    plain_small_off_.push_back(static_cast<int>(multi_small_.size()));
+    plain_large_off_.push_back(static_cast<int>(multi_large_.size()));
+    plain_direct_off_.push_back(static_cast<int>(direct_cols_.size()));
+  }
+  const size_t ncomp = comps_.size();
+  const size_t npairs = pairs_.size();
+  auto t0 = std::chrono::steady_clock::now();
+  h2d_bytes_ = static_cast<double>(host_data_.size() * sizeof(double));
+  h2d_bytes_ += upload(d_arena_, arena, stream_);
+  h2d_bytes_ += upload(d_designs_, ddesc, stream_);
+  h2d_bytes_ += upload(d_single_jobs_, single_jobs_, stream_);
+  h2d_bytes_ += upload(d_multi_jobs_, multi_jobs_, stream_);
+  h2d_bytes_ += upload(d_multi_small_, multi_small_, stream_);
+  h2d_bytes_ += upload(d_multi_large_, multi_large_, stream_);
+  h2d_bytes_ += upload(d_direct_cols_, direct_cols_, stream_);
+  h2d_bytes_ += upload(d_direct_slots_, direct_slots_, stream_);
+  h2d_bytes_ += upload(d_pairs_, pairs_, stream_);
+  std::vector<int> ident(ncomp);
+  for (size_t c = 0; c < ncomp; ++c) ident[c] = static_cast<int>(c);
+  h2d_bytes_ += upload(d_comp_cols_, ident, stream_);
+  collected_ = false;
+  d_single_res_.ensure(single_jobs_.size());
+  d_multi_res_.ensure(multi_jobs_.size());
+  d_resid_.ensure(static_cast<size_t>(n) * ncomp);
+  d_records_.ensure(npairs);
+  if (stats_enabled_) {
+    const int method = opt.ci_method;
+    if (method == FKPC_DCC_GAMMA || method == FKPC_DCC_PERM) {
+      d_centre_.ensure(static_cast<size_t>(n) * ncomp);
+      d_dcov_.ensure(ncomp);
+    }
+    if (method == FKPC_HSIC_GAMMA || method == FKPC_HSIC_PERM) {
+      d_factors_.ensure(static_cast<size_t>(n) * opt.num_col * ncomp);
+      d_hsic_.ensure(ncomp);
+    }
+    if (method == FKPC_DCC_GAMMA) {
+      const size_t bytes_per_slot = static_cast<size_t>(n) * opt.num_col * sizeof(double);
+      const size_t budget = static_cast<size_t>(8) << 30;
+      guard_cap_ = static_cast<int>(std::min<size_t>(ncomp, std::max<size_t>(1, budget / bytes_per_slot)));
+      d_guard_.ensure(2 + npairs + ncomp + guard_cap_);
+      d_lr_vals_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col);
+      d_lr_vecs_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col * n);
+      d_lr_status_.ensure(guard_cap_);
+      d_legacy_ws_.ensure(legacy_eigen_workspace_doubles(n, kLegacyCtas));
+    }
+    if (method == FKPC_DCC_PERM || method == FKPC_HSIC_PERM) {
+      if (!rstream) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "permutation methods require a seeded stream");
+      const int R = opt.permutation_replicates;
+      std::vector<int> perms(npairs * static_cast<size_t>(R) * n);
+      for (size_t t = 0; t < npairs; ++t) {
+        int* dst = perms.data() + t * static_cast<size_t>(R) * n;
+        if (method == FKPC_DCC_PERM) rstream->dcc_permutations(n, R, dst);
+        else rstream->hsic_permutations(n, R, dst);
+      }
+      h2d_bytes_ += upload(d_perms_, perms, stream_);
+    }
+  }
+  cuda_check(cudaStreamSynchronize(stream_), "prepare upload");
+  upload_ms_ = ms_since(t0);
+}
+
+void Engine::prepare(const std::vector<Test>& tests, const fkpc_options& opt, RStream* rstream) {
+  if (n_ == 0) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "no data loaded");
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  opt_ = opt;
+  stats_enabled_ = true;
+  release_graph();
+  auto t0 = std::chrono::steady_clock::now();
+  plan_components(tests);
+  build_designs();
+  setup_ms_ = ms_since(t0);
+  pack_and_upload(opt, rstream);
+}
+
+void Engine::enqueue() {
+  const int n = n_;
+  const int ncomp = static_cast<int>(comps_.size());
+  const int npairs = static_cast<int>(pairs_.size());
+  launches_ = 0;
+  cuda_check(cudaEventRecord(ev_[0], stream_), "event");
+  if (!direct_cols_.empty()) {
+    dim3 grid((n + 255) / 256, static_cast<unsigned>(direct_cols_.size()));
+    gather_columns_kernel<<<grid, 256, 0, stream_>>>(d_data_.get(), n, d_direct_cols_.get(), d_direct_slots_.get(),
+                                                      static_cast<int>(direct_cols_.size()), d_resid_.get());
+    cuda_check(cudaGetLastError(), "gather columns");
+    ++launches_;
+  }
+  if (!single_jobs_.empty()) {
+    cuda_check(launch_fit_single(d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_single_jobs_.get(),
+                                 static_cast<int>(single_jobs_.size()), d_resid_.get(), d_single_res_.get(), stream_),
+               "fit single");
+    ++launches_;
+  }
+  if (!multi_small_.empty()) {
+    cuda_check(launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                d_multi_small_.get(), static_cast<int>(multi_small_.size()), d_resid_.get(),
+                                d_multi_res_.get(), stream_),
+               "fit multi");
+    ++launches_;
+  }
+  if (!multi_large_.empty()) {
+    cuda_check(launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                d_multi_large_.get(), static_cast<int>(multi_large_.size()), d_resid_.get(),
+                                d_multi_res_.get(), stream_),
+               "fit multi");
+    ++launches_;
+  }
+  cuda_check(cudaEventRecord(ev_[1], stream_), "event");
+  if (stats_enabled_ && npairs > 0) {
+    const int method = opt_.ci_method;
+    if (method == FKPC_DCC_GAMMA || method == FKPC_DCC_PERM) {
+      cuda_check(launch_dcov_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, d_centre_.get(), d_dcov_.get(),
+                                        stream_),
+                 "dcov components");
+      ++launches_;
+    }
+    if (method == FKPC_DCC_GAMMA) {
+      cuda_check(launch_dcov_pairs(d_resid_.get(), n, d_comp_cols_.get(), d_centre_.get(), d_dcov_.get(),
+                                   d_pairs_.get(), npairs, d_records_.get(), stream_),
+                 "dcov pairs");
+      ++launches_;
+      cuda_check(cudaEventRecord(ev_[2], stream_), "event");
+      int* guard = d_guard_.get();
+      cuda_check(launch_guard_select(d_records_.get(), d_pairs_.get(), npairs, ncomp, guard_cap_, kGuardLower,
+                                     kGuardUpper, guard, stream_),
+                 "guard select");
+      const int* list = guard + 2;
+      const int* comp_slot = list + npairs;
+      const int* slot_comps = comp_slot + ncomp;
+      cuda_check(launch_legacy_eigen(d_resid_.get(), n, d_comp_cols_.get(), guard, slot_comps, guard_cap_,
+                                     std::min(kLegacyCtas, guard_cap_), opt_.num_col, d_legacy_ws_.get(),
+                                     d_lr_vals_.get(), d_lr_vecs_.get(), d_lr_status_.get(), stream_),
+                 "legacy eigen");
+      cuda_check(launch_legacy_pairs(n, opt_.num_col, d_lr_vals_.get(), d_lr_vecs_.get(), d_dcov_.get(), guard, list,
+                                     comp_slot, d_pairs_.get(), npairs, d_records_.get(), stream_),
+                 "legacy pairs");
+      launches_ += 3;
+    } else if (method == FKPC_DCC_PERM) {
+      cuda_check(launch_dcc_perm_pairs(d_resid_.get(), n, d_comp_cols_.get(), d_centre_.get(), d_pairs_.get(), npairs,
+                                       d_perms_.get(), opt_.permutation_replicates, d_records_.get(), stream_),
+                 "dcc perm pairs");
+      ++launches_;
+    } else {
+      cuda_check(launch_hsic_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, opt_.num_col, opt_.hsic_sig,
+                                        d_factors_.get(), d_hsic_.get(), stream_),
+                 "hsic components");
+      ++launches_;
+      if (method == FKPC_HSIC_GAMMA) {
+        cuda_check(launch_hsic_pairs(n, opt_.num_col, d_factors_.get(), d_hsic_.get(), d_pairs_.get(), npairs,
+                                     d_records_.get(), stream_),
+                   "hsic pairs");
+      } else {
+        cuda_check(launch_hsic_perm_pairs(n, opt_.num_col, d_factors_.get(), d_hsic_.get(), d_pairs_.get(), npairs,
+                                          d_perms_.get(), opt_.permutation_replicates, d_records_.get(), stream_),
+                   "hsic perm pairs");
+      }
+      ++launches_;
+    }
+  }
+  cuda_check(cudaEventRecord(ev_[3], stream_), "event");
+}
+
+void Engine::execute() {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  const bool perm = opt_.ci_method == FKPC_DCC_PERM || opt_.ci_method == FKPC_HSIC_PERM;
+  if (opt_.mode == FKPC_MODE_PLAIN && perm) {
+    // one permutation test: its launch sequence without a graph
+    cuda_check(configure_fit_kernels(), "kernel attributes");
+    cuda_check(configure_stat_kernels(n_), "kernel attributes");
+    enqueue();
+    return;
+  }
+  if (opt_.mode == FKPC_MODE_PLAIN) {
+    // the plain per-test form: each test's own launch set, synchronised
+    cuda_check(configure_fit_kernels(), "kernel attributes");
+    cuda_check(configure_stat_kernels(n_), "kernel attributes");
+    cuda_check(cudaEventRecord(ev_[0], stream_), "event");
+    launches_ = 0;
+    for (int t = 0; t < static_cast<int>(pairs_.size()); ++t) {
+      enqueue_plain_test(t);
+      cuda_check(cudaStreamSynchronize(stream_), "plain test");
+    }
+    cuda_check(cudaEventRecord(ev_[1], stream_), "event");
+    cuda_check(cudaEventRecord(ev_[2], stream_), "event");
+    cuda_check(cudaEventRecord(ev_[3], stream_), "event");
+    return;
+  }
+  if (!graph_exec_) {
+    cuda_check(configure_fit_kernels(), "kernel attributes");
+    cuda_check(configure_stat_kernels(n_), "kernel attributes");
+    cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+      enqueue();
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(stream_, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    cuda_check(cudaStreamEndCapture(stream_, &graph_), "end capture");
+    cuda_check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
+  }
+  cuda_check(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
+}
+
+void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
+  auto t0 = std::chrono::steady_clock::now();
+  cuda_check(cudaStreamSynchronize(stream_), "batch execution");
+  std::vector<FitResult> sres(single_jobs_.size()), mres(multi_jobs_.size());
+  if (!sres.empty())
+    cuda_check(cudaMemcpy(sres.data(), d_single_res_.get(), sres.size() * sizeof(FitResult), cudaMemcpyDeviceToHost), "download");
+  if (!mres.empty())
+    cuda_check(cudaMemcpy(mres.data(), d_multi_res_.get(), mres.size() * sizeof(FitResult), cudaMemcpyDeviceToHost), "download");
+  auto fit_failure = [&](const FitJob& job, const FitResult& r) {
+    const Design& des = *designs_[job.design];
+    std::string s = "residual fit of variable " + std::to_string(job.column) + " on S = {";
+    for (size_t i = 0; i < des.S.size(); ++i) s += (i ? "," : "") + std::to_string(des.S[i]);
+    s += "} failed with status " + std::to_string(r.status);
+    return Error(r.status == kStatusRank ? FKPC_STATUS_RANK
+                                          : (r.status == kStatusNotConverged ? FKPC_STATUS_NOT_CONVERGED : FKPC_STATUS_NUMERIC),
+                 s);
+  };
+  d2h_bytes_ = static_cast<double>((sres.size() + mres.size()) * sizeof(FitResult));
+  account_flops(sres, mres);
+  collected_ = true;
+  for (size_t i = 0; i < sres.size(); ++i)
+    if (sres[i].status != kStatusOk) throw fit_failure(single_jobs_[i], sres[i]);
+  for (size_t i = 0; i < mres.size(); ++i)
+    if (mres[i].status != kStatusOk) throw fit_failure(multi_jobs_[i], mres[i]);
+  std::vector<RecordDev> recs(pairs_.size());
+  if (!recs.empty() && stats_enabled_)
+    cuda_check(cudaMemcpy(recs.data(), d_records_.get(), recs.size() * sizeof(RecordDev), cudaMemcpyDeviceToHost), "download");
+  d2h_bytes_ += static_cast<double>(recs.size() * sizeof(RecordDev));
+  int guarded = 0;
+  if (stats_enabled_ && opt_.ci_method == FKPC_DCC_GAMMA && !pairs_.empty()) {
+    int counts[2] = {0, 0};
+    cuda_check(cudaMemcpy(counts, d_guard_.get(), sizeof(counts), cudaMemcpyDeviceToHost), "download");
+    guarded = counts[0];
+    if (counts[1] > guard_cap_) throw Error(FKPC_STATUS_ALLOCATION, "guard-band low-rank capacity exceeded");
+    std::vector<int> lrs(std::min(counts[1], guard_cap_));
+    if (!lrs.empty())
+      cuda_check(cudaMemcpy(lrs.data(), d_lr_status_.get(), lrs.size() * sizeof(int), cudaMemcpyDeviceToHost), "download");
+    for (int s : lrs)
+      if (s != kStatusOk) throw Error(FKPC_STATUS_NOT_CONVERGED, "low-rank eigen-solve of a guarded component did not converge");
+  }
+  double download_ms = ms_since(t0);
+  if (out) {
+    for (size_t t = 0; t < recs.size(); ++t) {
+      const RecordDev& r = recs[t];
+      fkpc_ci_record& o = out[t];
+      o.p_value = r.p_value;
+      o.p_exact = r.p_exact;
+      o.statistic = r.statistic;
+      o.mean = r.mean;
+      o.variance = r.variance;
+      o.status = r.status;
+      o.flags = r.flags | (tests_[t].S.empty() ? FKPC_FLAG_DIRECT : 0u);
+      if (r.status != kStatusOk)
+        throw Error(r.status == kStatusNotConverged ? FKPC_STATUS_NOT_CONVERGED : FKPC_STATUS_NUMERIC,
+                    "statistic of test " + std::to_string(t) + " failed with status " + std::to_string(r.status));
+    }
+  }
+  if (stats) {
+    float f_ms = 0.f, s_ms = 0.f, g_ms = 0.f, tot = 0.f;
+    cudaEventElapsedTime(&f_ms, ev_[0], ev_[1]);
+    cudaEventElapsedTime(&tot, ev_[0], ev_[3]);
+    s_ms = tot - f_ms;
+    if (stats_enabled_ && opt_.ci_method == FKPC_DCC_GAMMA && !pairs_.empty()) {
+      cudaEventElapsedTime(&g_ms, ev_[2], ev_[3]);
+      s_ms -= g_ms;
+    }
+    stats->setup_ms = setup_ms_;
+    stats->upload_ms = upload_ms_;
+    stats->fit_ms = f_ms;
+    stats->statistic_ms = s_ms;
+    stats->refine_ms = g_ms;
+    stats->download_ms = download_ms;
+    stats->designs = static_cast<int>(sets_.size());
+    stats->targets = static_cast<int>(single_jobs_.size() + multi_jobs_.size());
+    stats->pairs = static_cast<int>(pairs_.size());
+    stats->guarded = guarded;
+    stats->kernel_launches = launches_;
+    stats->h2d_bytes = h2d_bytes_;
+    stats->d2h_bytes = d2h_bytes_;
+    double evals = 0.0;
+    for (const auto& r : sres) evals += r.evaluations;
+    for (const auto& r : mres) evals += r.evaluations;
+    stats->fit_evaluations = evals;
+    stats->fit_flops = stage_flops_[0] + stage_flops_[1] + stage_flops_[2];
+    stats->statistic_flops = stage_flops_[3] + stage_flops_[4] + stage_flops_[5] + stage_flops_[6];
+  }
+}
+
+// Algorithmic FP64 flop counts of the implemented algorithms (FMA = 2):
+//  fit single : z = (QW)'y and the residual, 2nq each; 20q per spectral
+//               objective evaluation.
+//  fit multi  : y0 = Q'y and the residual, 2nq each; per objective
+//               evaluation the Householder fold of the stacked roots
+//               4 (rsum + 1) q^2 / 2, the triangular inverse and W = R Ra^-1
+//               q^3 / 3 each, g and W g 2 q^2; per derivative evaluation
+//               (one per Newton iteration) T and W T 2 q^2 rsum, C and D
+//               2 rsum^2 q.
+//  dCov components : row sums 2 n^2, squared centred entries 2.5 n (n - 1).
+//  dCov pairs      : 4 n (n - 1) (n(n-1)/2 entries x 2 abs-diffs, 4 centring
+//                    subtractions and one FMA).
+//  HSIC components : per incomplete-Cholesky step k, n exponentials (20 each)
+//                    and 2 n k; then 2 n r^2 for |Gc'Gc|_F^2.
+//  HSIC pairs      : 2 n rx ry.
+void Engine::account_flops(const std::vector<FitResult>& sres, const std::vector<FitResult>& mres) {
+  for (double& f : stage_flops_) f = 0.0;
+  const double n = n_;
+  for (size_t i = 0; i < single_jobs_.size(); ++i) {
+    const double q = designs_[single_jobs_[i].design]->q;
+    stage_flops_[0] += 4.0 * n * q + 20.0 * q * sres[i].evaluations;
+  }
+  for (size_t i = 0; i < multi_jobs_.size(); ++i) {
+    const Design& des = *designs_[multi_jobs_[i].design];
+    const double q = des.q;
+    double rs = 0.0;
+    for (int r : des.ranks) rs += r;
+    const double core = 2.0 * (rs + 1.0) * q * q + 2.0 * q * q * q / 3.0 + 4.0 * q * q;
+    const double deriv = 2.0 * q * q * rs + 2.0 * rs * rs * q;
+    const double f = 4.0 * n * q + core * mres[i].evaluations + deriv * mres[i].iterations;
+    const bool small = des.q <= 40 && rs <= 32;
+    stage_flops_[small ? 1 : 2] += f;
+  }
+  if (stats_enabled_) {
+    const double nc = static_cast<double>(comps_.size()), np = static_cast<double>(pairs_.size());
+    if (opt_.ci_method == FKPC_DCC_GAMMA || opt_.ci_method == FKPC_DCC_PERM) {
+      stage_flops_[3] = nc * (2.0 * n * n + 2.5 * n * (n - 1.0));
+      const double reps = opt_.ci_method == FKPC_DCC_PERM ? opt_.permutation_replicates + 1.0 : 1.0;
+      stage_flops_[4] = np * reps * 4.0 * n * (n - 1.0);
+    }
+    if (opt_.ci_method == FKPC_HSIC_GAMMA || opt_.ci_method == FKPC_HSIC_PERM) {
+      const double r = opt_.num_col;
+      stage_flops_[5] = nc * (r * n * 20.0 + n * r * r + 2.0 * n * r * r);
+      const double reps = opt_.ci_method == FKPC_HSIC_PERM ? opt_.permutation_replicates + 1.0 : 1.0;
+      stage_flops_[6] = np * reps * 2.0 * n * r * r;
+    }
+  }
+}
+
+void Engine::enqueue_plain_test(int t) {
+  const int n = n_;
+  const int ncomp = static_cast<int>(comps_.size());
+  const int npairs = static_cast<int>(pairs_.size());
+  const int d0 = plain_direct_off_[t], d1 = plain_direct_off_[t + 1];
+  if (d1 > d0) {
+    dim3 grid((n + 255) / 256, static_cast<unsigned>(d1 - d0));
+    gather_columns_kernel<<<grid, 256, 0, stream_>>>(d_data_.get(), n, d_direct_cols_.get() + d0,
+                                                      d_direct_slots_.get() + d0, d1 - d0, d_resid_.get());
+    cuda_check(cudaGetLastError(), "gather columns");
+    ++launches_;
+  }
+  const int s0 = plain_single_off_[t], s1 = plain_single_off_[t + 1];
+  if (s1 > s0) {
+    cuda_check(launch_fit_single(d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_single_jobs_.get() + s0, s1 - s0,
+                                 d_resid_.get(), d_single_res_.get() + s0, stream_),
+               "fit single");
+    ++launches_;
+  }
+  const int a0 = plain_small_off_[t], a1 = plain_small_off_[t + 1];
+  if (a1 > a0) {
+    cuda_check(launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                d_multi_small_.get() + a0, a1 - a0, d_resid_.get(), d_multi_res_.get(), stream_),
+               "fit multi");
+    ++launches_;
+  }
+  const int b0 = plain_large_off_[t], b1 = plain_large_off_[t + 1];
+  if (b1 > b0) {
+    cuda_check(launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                d_multi_large_.get() + b0, b1 - b0, d_resid_.get(), d_multi_res_.get(), stream_),
+               "fit multi");
+    ++launches_;
+  }
+  const int method = opt_.ci_method;
+  const PairJob* pair = d_pairs_.get() + t;
+  const int* cols = d_comp_cols_.get() + 2 * t;
+  if (method == FKPC_DCC_GAMMA) {
+    // the two components of test t are 2t and 2t+1 (no sharing in this form)
+    cuda_check(launch_dcov_components(d_resid_.get(), n, cols, 2, d_centre_.get() + static_cast<size_t>(n) * 2 * t,
+                                      d_dcov_.get() + 2 * t, stream_),
+               "dcov components");
+    cuda_check(launch_dcov_pairs(d_resid_.get(), n, d_comp_cols_.get(), d_centre_.get(), d_dcov_.get(), pair, 1,
+                                 d_records_.get(), stream_),
+               "dcov pairs");
+    int* guard = d_guard_.get();
+    cuda_check(launch_guard_select(d_records_.get(), pair, 1, ncomp, guard_cap_, kGuardLower, kGuardUpper, guard, stream_),
+               "guard select");
+    cuda_check(launch_legacy_eigen(d_resid_.get(), n, d_comp_cols_.get(), guard, guard + 2 + 1 + ncomp, guard_cap_, 2,
+                                   opt_.num_col, d_legacy_ws_.get(), d_lr_vals_.get(), d_lr_vecs_.get(),
+                                   d_lr_status_.get(), stream_),
+               "legacy eigen");
+    cuda_check(launch_legacy_pairs(n, opt_.num_col, d_lr_vals_.get(), d_lr_vecs_.get(), d_dcov_.get(), guard, guard + 2,
+                                   guard + 2 + 1, pair, 1, d_records_.get(), stream_),
+               "legacy pairs");
+    launches_ += 5;
+  } else if (method == FKPC_HSIC_GAMMA) {
+    cuda_check(launch_hsic_components(d_resid_.get(), n, cols, 2, opt_.num_col, opt_.hsic_sig,
+                                      d_factors_.get() + static_cast<size_t>(n) * opt_.num_col * 2 * t,
+                                      d_hsic_.get() + 2 * t, stream_),
+               "hsic components");
+    cuda_check(launch_hsic_pairs(n, opt_.num_col, d_factors_.get(), d_hsic_.get(), pair, 1, d_records_.get(), stream_),
+               "hsic pairs");
+    launches_ += 2;
+  } else {
+    throw Error(FKPC_STATUS_INVALID_ARGUMENT, "the plain form covers the gamma methods; permutation tests run batched");
+  }
+  (void)npairs;
+}
+
+double Engine::execute_timed(int repeats) {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  if (opt_.mode == FKPC_MODE_PLAIN) {
+    cuda_check(configure_fit_kernels(), "kernel attributes");
+    cuda_check(configure_stat_kernels(n_), "kernel attributes");
+    float total = 0.f;
+    for (int r = 0; r < repeats; ++r) {
+      cuda_check(cudaEventRecord(ev_[4], stream_), "event");
+      execute();
+      cuda_check(cudaEventRecord(ev_[5], stream_), "event");
+      cuda_check(cudaEventSynchronize(ev_[5]), "event sync");
+      float ms = 0.f;
+      cuda_check(cudaEventElapsedTime(&ms, ev_[4], ev_[5]), "event time");
+      total += ms;
+    }
+    return total;
+  }
+  execute();  // builds the graph on first use
+  cuda_check(cudaStreamSynchronize(stream_), "warm graph");
+  cuda_check(cudaEventRecord(ev_[4], stream_), "event");
+  for (int r = 0; r < repeats; ++r) cuda_check(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
+  cuda_check(cudaEventRecord(ev_[5], stream_), "event");
+  cuda_check(cudaEventSynchronize(ev_[5]), "event sync");
+  float ms = 0.f;
+  cuda_check(cudaEventElapsedTime(&ms, ev_[4], ev_[5]), "event time");
+  return ms;
+}
+
+double Engine::time_stage(int stage, int repeats, double* flops_per_launch) {
+  if (!collected_) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "collect the prepared batch before timing a stage");
+  if (stage < 0 || stage > 8) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "unknown stage");
+  cuda_check(configure_fit_kernels(), "kernel attributes");
+  cuda_check(configure_stat_kernels(n_), "kernel attributes");
+  const int n = n_;
+  const int ncomp = static_cast<int>(comps_.size());
+  const int npairs = static_cast<int>(pairs_.size());
+  int* guard = d_guard_.get();
+  auto launch = [&]() -> cudaError_t {
+    switch (stage) {
+      case 0: return launch_fit_single(d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_single_jobs_.get(),
+                                       static_cast<int>(single_jobs_.size()), d_resid_.get(), d_single_res_.get(), stream_);
+      case 1: return launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                      d_multi_small_.get(), static_cast<int>(multi_small_.size()), d_resid_.get(),
+                                      d_multi_res_.get(), stream_);
+      case 2: return launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                      d_multi_large_.get(), static_cast<int>(multi_large_.size()), d_resid_.get(),
+                                      d_multi_res_.get(), stream_);
+      case 3: return launch_dcov_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, d_centre_.get(),
+                                            d_dcov_.get(), stream_);
+      case 4: return launch_dcov_pairs(d_resid_.get(), n, d_comp_cols_.get(), d_centre_.get(), d_dcov_.get(),
+                                       d_pairs_.get(), npairs, d_records_.get(), stream_);
+      case 5: return launch_hsic_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, opt_.num_col, opt_.hsic_sig,
+                                            d_factors_.get(), d_hsic_.get(), stream_);
+      case 6: return launch_hsic_pairs(n, opt_.num_col, d_factors_.get(), d_hsic_.get(), d_pairs_.get(), npairs,
+                                       d_records_.get(), stream_);
+      case 7: return launch_legacy_eigen(d_resid_.get(), n, d_comp_cols_.get(), guard, guard + 2 + npairs + ncomp,
+                                         guard_cap_, std::min(kLegacyCtas, guard_cap_), opt_.num_col,
+                                         d_legacy_ws_.get(), d_lr_vals_.get(), d_lr_vecs_.get(), d_lr_status_.get(),
+                                         stream_);
+      default: return launch_legacy_pairs(n, opt_.num_col, d_lr_vals_.get(), d_lr_vecs_.get(), d_dcov_.get(), guard,
+                                          guard + 2, guard + 2 + npairs, d_pairs_.get(), npairs, d_records_.get(),
+                                          stream_);
+    }
+  };
+  const bool dcc = opt_.ci_method == FKPC_DCC_GAMMA || opt_.ci_method == FKPC_DCC_PERM;
+  const bool hsic = opt_.ci_method == FKPC_HSIC_GAMMA || opt_.ci_method == FKPC_HSIC_PERM;
+  if (((stage == 3 || stage == 4) && !dcc) || ((stage == 5 || stage == 6) && !hsic) ||
+      ((stage == 7 || stage == 8) && opt_.ci_method != FKPC_DCC_GAMMA))
+    throw Error(FKPC_STATUS_INVALID_ARGUMENT, "stage not part of the prepared method");
+  cuda_check(launch(), "stage warm-up");
+  cuda_check(cudaStreamSynchronize(stream_), "stage warm-up");
+  cuda_check(cudaEventRecord(ev_[4], stream_), "event");
+  for (int r = 0; r < repeats; ++r) cuda_check(launch(), "stage launch");
+  cuda_check(cudaEventRecord(ev_[5], stream_), "event");
+  cuda_check(cudaEventSynchronize(ev_[5]), "event sync");
+  float ms = 0.f;
+  cuda_check(cudaEventElapsedTime(&ms, ev_[4], ev_[5]), "event time");
+  if (flops_per_launch) *flops_per_launch = stage_flops_[stage];
+  return ms / std::max(1, repeats);
+}
+
+double Engine::measure_fp64_peak() {
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  int sms = 0;
+  cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "device attribute");
+  const int blocks = sms * 8, iters = 4096;
+  DevBuf<double> out;
+  double* d = out.ensure(static_cast<size_t>(blocks) * 256);
+  cuda_check(launch_fp64_peak(d, blocks, iters, stream_), "fp64 probe");
+  cuda_check(cudaStreamSynchronize(stream_), "fp64 probe");
+  double best = 0.0;
+  for (int rep = 0; rep < 5; ++rep) {
+    cuda_check(cudaEventRecord(ev_[4], stream_), "event");
+    cuda_check(launch_fp64_peak(d, blocks, iters, stream_), "fp64 probe");
+    cuda_check(cudaEventRecord(ev_[5], stream_), "event");
+    cuda_check(cudaEventSynchronize(ev_[5]), "event sync");
+    float ms = 0.f;
+    cuda_check(cudaEventElapsedTime(&ms, ev_[4], ev_[5]), "event time");
+    const double flops = 2.0 * 16.0 * iters * 256.0 * blocks;
+    best = std::max(best, flops / (ms * 1e-3) / 1e12);
+  }
+  return best;
+}
+
+void Engine::regress(const std::vector<int>& targets, const std::vector<std::vector<int>>& sets,
+                     double* residuals, double* log_sp, int max_penalties, int* status) {
+  if (targets.size() != sets.size()) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "targets and sets differ in length");
+  std::vector<Test> tests;
+  for (size_t i = 0; i < targets.size(); ++i) {
+    Test t;
+    t.x = targets[i];
+    t.y = targets[i] == 0 ? 1 : 0;  // placeholder partner; only the x component is read back
+    t.S = sets[i];
+    for (int s : t.S)
+      if (s == t.y) t.y = -1;
+    if (t.y < 0)
+      for (int c = 0; c < p_; ++c)
+        if (c != t.x && std::find(t.S.begin(), t.S.end(), c) == t.S.end()) { t.y = c; break; }
+    tests.push_back(t);
+  }
+  fkpc_options opt;
+  fkpc_default_options(&opt);
+  opt_ = opt;
+  release_graph();
+  auto t0 = std::chrono::steady_clock::now();
+  plan_components(tests);
+  build_designs();
+  setup_ms_ = ms_since(t0);
+  stats_enabled_ = false;
+  pack_and_upload(opt, nullptr);
+  cuda_check(configure_fit_kernels(), "kernel attributes");
+  enqueue();
+  cuda_check(cudaStreamSynchronize(stream_), "regress");
+  collect(nullptr, nullptr);
+  const int n = n_;
+  std::vector<double> slab(static_cast<size_t>(n) * comps_.size());
+  cuda_check(cudaMemcpy(slab.data(), d_resid_.get(), slab.size() * sizeof(double), cudaMemcpyDeviceToHost), "download");
+  std::vector<FitResult> sres(single_jobs_.size()), mres(multi_jobs_.size());
+  if (!sres.empty())
+    cuda_check(cudaMemcpy(sres.data(), d_single_res_.get(), sres.size() * sizeof(FitResult), cudaMemcpyDeviceToHost), "download");
+  if (!mres.empty())
+    cuda_check(cudaMemcpy(mres.data(), d_multi_res_.get(), mres.size() * sizeof(FitResult), cudaMemcpyDeviceToHost), "download");
+  std::vector<const FitResult*> by_comp(comps_.size(), nullptr);
+  for (size_t i = 0; i < single_jobs_.size(); ++i) by_comp[single_jobs_[i].out] = &sres[i];
+  for (size_t i = 0; i < multi_jobs_.size(); ++i) by_comp[multi_jobs_[i].out] = &mres[i];
+  for (size_t i = 0; i < targets.size(); ++i) {
+    const int c = pairs_[i].left;
+    std::copy(slab.begin() + static_cast<size_t>(n) * c, slab.begin() + static_cast<size_t>(n) * (c + 1),
+              residuals + static_cast<size_t>(n) * i);
+    const FitResult* r = by_comp[c];
+    if (status) status[i] = r ? r->status : kStatusOk;
+    if (log_sp)
+      for (int j = 0; j < max_penalties; ++j)
+        log_sp[i * static_cast<size_t>(max_penalties) + j] = (r && j < kMaxPenalties) ? r->log_sp[j] : NAN;
+  }
+  stats_enabled_ = true;
+}
+
+void Engine::statistics(const double* residuals, int m, const std::vector<int>& left, const std::vector<int>& right,
+                        const int* permutations, const fkpc_options& opt, fkpc_ci_record* out) {
+  const int n = n_;
+  if (left.size() != right.size()) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "left and right differ in length");
+  for (size_t i = 0; i < left.size(); ++i)
+    if (left[i] < 0 || left[i] >= m || right[i] < 0 || right[i] >= m)
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "residual column index out of range");
+  opt_ = opt;
+  release_graph();
+  tests_.clear();
+  comps_.assign(m, Component{0, -1});
+  pairs_.clear();
+  for (size_t i = 0; i < left.size(); ++i) {
+    pairs_.push_back(PairJob{left[i], right[i], static_cast<int>(i), 0});
+    tests_.push_back(Test{left[i], right[i], {}});
+  }
+  sets_.clear();
+  designs_.clear();
+  single_jobs_.clear();
+  multi_jobs_.clear();
+  multi_small_.clear();
+  multi_large_.clear();
+  direct_cols_.clear();
+  direct_slots_.clear();
+  stats_enabled_ = true;
+  // pack: no designs; residual slab = caller residuals
+  std::vector<int> ident(m);
+  for (int c = 0; c < m; ++c) ident[c] = c;
+  upload(d_comp_cols_, ident, stream_);
+  upload(d_pairs_, pairs_, stream_);
+  double* slab = d_resid_.ensure(static_cast<size_t>(n) * m);
+  cuda_check(cudaMemcpyAsync(slab, residuals, sizeof(double) * n * static_cast<size_t>(m), cudaMemcpyHostToDevice, stream_),
+             "upload residuals");
+  d_records_.ensure(pairs_.size());
+  const size_t ncomp = static_cast<size_t>(m), npairs = pairs_.size();
+  if (opt.ci_method == FKPC_DCC_GAMMA || opt.ci_method == FKPC_DCC_PERM) {
+    d_centre_.ensure(static_cast<size_t>(n) * ncomp);
+    d_dcov_.ensure(ncomp);
+  }
+  if (opt.ci_method == FKPC_HSIC_GAMMA || opt.ci_method == FKPC_HSIC_PERM) {
+    d_factors_.ensure(static_cast<size_t>(n) * opt.num_col * ncomp);
+    d_hsic_.ensure(ncomp);
+  }
+  if (opt.ci_method == FKPC_DCC_GAMMA) {
+    guard_cap_ = static_cast<int>(ncomp);
+    d_guard_.ensure(2 + npairs + ncomp + guard_cap_);
+    d_lr_vals_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col);
+    d_lr_vecs_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col * n);
+    d_lr_status_.ensure(guard_cap_);
+    d_legacy_ws_.ensure(legacy_eigen_workspace_doubles(n, kLegacyCtas));
+  }
+  if (opt.ci_method == FKPC_DCC_PERM || opt.ci_method == FKPC_HSIC_PERM) {
+    if (!permutations) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "permutation methods need a permutation table");
+    const size_t cnt = npairs * static_cast<size_t>(opt.permutation_replicates) * n;
+    for (size_t i = 0; i < cnt; ++i)
+      if (permutations[i] < 0 || permutations[i] >= n) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "permutation entry out of range");
+    int* d = d_perms_.ensure(cnt);
+    cuda_check(cudaMemcpyAsync(d, permutations, cnt * sizeof(int), cudaMemcpyHostToDevice, stream_), "upload perms");
+  }
+  cuda_check(configure_stat_kernels(n), "kernel attributes");
+  enqueue();
+  collect(out, nullptr);
+}
+
+}  // namespace fkpc

@@ -1,0 +1,159 @@
+// Batched CI-test engine: host-side batching of one level's tests into
+// designs, residual components and pairs; device arena packing; a fixed
+// launch sequence captured once as a CUDA graph and replayed.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/fastkpc_b200.h"
+#include "design.h"
+#include "device.h"
+#include "kernels.h"
+#include "rstream.h"
+
+namespace fkpc {
+
+struct Error : public std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what);
+
+template <class T>
+class DevBuf {
+ public:
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (ptr_) cudaFree(ptr_);
+  }
+  T* ensure(size_t count) {
+    if (count == 0) count = 1;
+    if (count > cap_) {
+      if (ptr_) cudaFree(ptr_);
+      ptr_ = nullptr;
+      cap_ = 0;
+      cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr_), count * sizeof(T));
+      if (e != cudaSuccess) {
+        ptr_ = nullptr;
+        throw Error(FKPC_STATUS_ALLOCATION, std::string("device allocation failed: ") + cudaGetErrorString(e));
+      }
+      cap_ = count;
+    }
+    return ptr_;
+  }
+  T* get() const { return ptr_; }
+  size_t capacity() const { return cap_; }
+
+ private:
+  T* ptr_ = nullptr;
+  size_t cap_ = 0;
+};
+
+struct Test {
+  int x, y;
+  std::vector<int> S;
+};
+
+struct Component {
+  int target;
+  int design;  // -1 for a direct (|S| = 0) component
+};
+
+class Engine {
+ public:
+  explicit Engine(int device);
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  void load(const double* data, int n, int p);
+  int n() const { return n_; }
+  int p() const { return p_; }
+
+  // Batched form: plan, set-up, pack and upload one batch of tests.
+  void prepare(const std::vector<Test>& tests, const fkpc_options& opt, RStream* stream);
+  // Enqueue the device work of the prepared batch (CUDA graph replay).
+  void execute();
+  // Wait, copy results back and validate statuses.
+  void collect(fkpc_ci_record* out, fkpc_stage_stats* stats);
+
+  // Residual fits only (the regrXonS stage).
+  void regress(const std::vector<int>& targets, const std::vector<std::vector<int>>& sets,
+               double* residuals, double* log_sp, int max_penalties, int* status);
+  // Statistics only, on caller residual columns.
+  void statistics(const double* residuals, int m, const std::vector<int>& left, const std::vector<int>& right,
+                  const int* permutations, const fkpc_options& opt, fkpc_ci_record* out);
+  // Repeated graph launches of the prepared batch, timed with CUDA events.
+  double execute_timed(int repeats);
+  // One kernel of the prepared batch replayed alone: mean ms per launch.
+  double time_stage(int stage, int repeats, double* flops_per_launch);
+  double measure_fp64_peak();
+  cudaStream_t stream() const { return stream_; }
+  int launches() const { return launches_; }
+  double setup_ms() const { return setup_ms_; }
+
+ private:
+  void plan_components(const std::vector<Test>& tests);
+  void enqueue_plain_test(int t);  // one test's launch set (plain form)
+  double execute_plain_timed(int repeats);
+  void build_designs();
+  void pack_and_upload(const fkpc_options& opt, RStream* stream);
+  void enqueue();  // the launch sequence
+  void release_graph();
+
+  int device_ = 0;
+  cudaStream_t stream_ = nullptr;
+  int n_ = 0, p_ = 0;
+  std::vector<double> host_data_;
+  DevBuf<double> d_data_;
+  std::unique_ptr<DesignCache> cache_;
+
+  // batch plan
+  fkpc_options opt_{};
+  std::vector<Test> tests_;
+  std::vector<std::vector<int>> sets_;                  // unique conditioning sets
+  std::vector<std::shared_ptr<const Design>> designs_;  // aligned with sets_
+  std::vector<Component> comps_;
+  std::vector<PairJob> pairs_;
+  std::vector<FitJob> single_jobs_, multi_jobs_;
+  std::vector<int> multi_small_, multi_large_;
+  std::vector<int> direct_cols_, direct_slots_;
+  // plain form: per test, offsets of its jobs in the job lists
+  std::vector<int> plain_single_off_, plain_small_off_, plain_large_off_, plain_direct_off_;
+  int guard_cap_ = 0;
+  bool stats_enabled_ = true;
+
+  // device buffers
+  DevBuf<double> d_arena_, d_resid_, d_centre_, d_factors_, d_lr_vals_, d_lr_vecs_, d_legacy_ws_;
+  DevBuf<DesignDev> d_designs_;
+  DevBuf<FitJob> d_single_jobs_, d_multi_jobs_;
+  DevBuf<int> d_multi_small_, d_multi_large_, d_direct_cols_, d_direct_slots_, d_comp_cols_;
+  DevBuf<FitResult> d_single_res_, d_multi_res_;
+  DevBuf<PairJob> d_pairs_;
+  DevBuf<RecordDev> d_records_;
+  DevBuf<DcovComponent> d_dcov_;
+  DevBuf<HsicComponent> d_hsic_;
+  DevBuf<int> d_guard_;  // [0] pair count, [1] slot count, then lists
+  DevBuf<int> d_lr_status_;
+  DevBuf<int> d_perms_;
+
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  cudaEvent_t ev_[6] = {};
+  int launches_ = 0;
+  double setup_ms_ = 0.0, upload_ms_ = 0.0;
+  int guard_count_host_ = 0;
+  double h2d_bytes_ = 0.0, d2h_bytes_ = 0.0;
+  double stage_flops_[9] = {};
+  bool collected_ = false;
+  void account_flops(const std::vector<FitResult>& sres, const std::vector<FitResult>& mres);
+};
+
+}  // namespace fkpc

@@ -1,0 +1,75 @@
+"""Seeded synthetic inputs with the shapes of the benchmark configurations.
+
+No public dataset ships with the reference for these shapes, so inputs are
+drawn from the nonlinear structural equation model the configurations name:
+a random topological order; edge i -> j (i earlier) with probability
+``edge_prob`` (optionally capped at ``max_in_degree`` parents); each node is
+the sum over its parents of f(parent) with f drawn per edge from
+{tanh(2u), sin(u), 0.5 u^2, u}, plus N(0, 0.5^2) noise; columns standardised
+to mean 0, sd 1.
+"""
+import numpy as np
+
+_FUNCS = (lambda u: np.tanh(2.0 * u), np.sin, lambda u: 0.5 * u * u, lambda u: u)
+
+
+def nonlinear_sem(n, p, edge_prob, seed, max_in_degree=None):
+    rs = np.random.default_rng(seed)
+    order = rs.permutation(p)
+    X = np.zeros((n, p))
+    edges = []
+    for pos, j in enumerate(order):
+        parents = [int(i) for i in order[:pos] if rs.random() < edge_prob]
+        if max_in_degree is not None and len(parents) > max_in_degree:
+            parents = sorted(rs.choice(parents, size=max_in_degree, replace=False).tolist())
+        v = rs.normal(0.0, 0.5, size=n)
+        for i in parents:
+            f = _FUNCS[int(rs.integers(len(_FUNCS)))]
+            v = v + f(X[:, i])
+        X[:, j] = v
+        edges.extend((i, int(j)) for i in parents)
+    X = (X - X.mean(axis=0)) / X.std(axis=0, ddof=1)
+    return np.asfortranarray(X), edges
+
+
+def ci_triples(p, count, seed, size_sampler):
+    """``count`` random (x, y, S) triples; |S| from ``size_sampler(rs)``."""
+    rs = np.random.default_rng(seed)
+    out = []
+    while len(out) < count:
+        k = int(size_sampler(rs))
+        if k > p - 2:
+            continue
+        vars_ = rs.choice(p, size=k + 2, replace=False)
+        x, y = int(vars_[0]), int(vars_[1])
+        out.append((x, y, sorted(int(v) for v in vars_[2:])))
+    return out
+
+
+def level_batch_500x50(seed=2, count=4096):
+    """n=500, p=50 nonlinear SEM (edge prob 0.08); ``count`` triples with |S|
+    uniform on 0..4 -- the single-level CI batch microbenchmark."""
+    X, _ = nonlinear_sem(500, 50, 0.08, seed)
+    return X, ci_triples(50, count, seed + 1, lambda rs: rs.integers(0, 5))
+
+
+def skeleton_200x10(seed=1):
+    """n=200, p=10, edge prob 0.25: the CPU-runnable skeleton case."""
+    return nonlinear_sem(200, 10, 0.25, seed)[0]
+
+
+def skeleton_351x48(seed=3):
+    """n=351, p=48, edge prob 0.1, at most 8 parents: the full-skeleton case."""
+    return nonlinear_sem(351, 48, 0.1, seed, max_in_degree=8)[0]
+
+
+def uneven_batch_500x64(seed=4, count=16384):
+    """n=500, p=64; |S| ~ geometric(0.35) truncated at 12 (permutation batch)."""
+    X, _ = nonlinear_sem(500, 64, 0.08, seed)
+
+    def size(rs):
+        while True:
+            k = int(rs.geometric(0.35)) - 1
+            if k <= 12:
+                return k
+    return X, ci_triples(64, count, seed + 1, size)

@@ -1,0 +1,262 @@
+/*
+ * fastkpc_b200 — C ABI of the B200 kernel-PC conditional-independence path.
+ *
+ * Plain C types only: pointers, sizes and PODs.  Every function returns 0 on
+ * success and a positive FKPC_STATUS_* code on failure; fkpc_last_error()
+ * then holds a message for the calling thread.  Inputs are borrowed (the
+ * caller keeps ownership); results returned through fkpc_result** are owned
+ * by the library until fkpc_result_free().  Data matrices are column-major
+ * n x p binary64 (the layout of an R numeric matrix).  Indices are 0-based.
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the wyjistest/fastkpc tree).
+ */
+#ifndef FASTKPC_B200_H
+#define FASTKPC_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FKPC_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define FKPC_API __attribute__((visibility("default")))
+#else
+#define FKPC_API
+#endif
+
+/* status codes */
+#define FKPC_OK 0
+#define FKPC_STATUS_INVALID_ARGUMENT 1   /* envelope / argument check failed */
+#define FKPC_STATUS_CUDA 2               /* CUDA runtime error */
+#define FKPC_STATUS_NUMERIC 3            /* non-finite objective / statistic */
+#define FKPC_STATUS_NOT_CONVERGED 4      /* optimizer or gamma tail iteration cap */
+#define FKPC_STATUS_RANK 5               /* design or augmented system rank deficient */
+#define FKPC_STATUS_ALLOCATION 6         /* host or device allocation failed */
+#define FKPC_STATUS_NO_DEVICE 7          /* no usable CUDA device */
+
+/* CI methods (kpcalg ic.method) */
+#define FKPC_DCC_GAMMA 0
+#define FKPC_DCC_PERM 1
+#define FKPC_HSIC_GAMMA 2
+#define FKPC_HSIC_PERM 3
+
+/* execution forms */
+#define FKPC_MODE_BATCHED 0  /* every test of a level in one batched launch set */
+#define FKPC_MODE_PLAIN 1    /* one launch set per CI test */
+
+/* per-record flags */
+#define FKPC_FLAG_GUARDED 1u       /* dcc.gamma p came from the low-rank refinement */
+#define FKPC_FLAG_DIRECT 2u        /* |S| = 0: raw columns, no regression */
+
+typedef struct fkpc_options {
+  double alpha;                 /* significance level; the reference fixes 0.1 */
+  double index;                 /* dCov exponent; legacy semantics fix 1 */
+  int num_col;                  /* low-rank / inchol rank cap; reference fixes 35 */
+  int max_conditioning_size;    /* m.max; negative means Inf (p - 2) */
+  int ci_method;                /* FKPC_DCC_GAMMA ... FKPC_HSIC_PERM */
+  double hsic_sig;              /* Gaussian kernel width sig (rbfdot sigma = 1/sig) */
+  int permutation_replicates;   /* R for the permutation methods, 1..10000 */
+  int has_seed;                 /* permutation methods require a seed */
+  unsigned int seed;            /* set.seed() value for the R-compatible stream */
+  int mode;                     /* FKPC_MODE_BATCHED or FKPC_MODE_PLAIN */
+  int collect_trace;            /* keep the per-test logical trace */
+  int device;                   /* CUDA device ordinal */
+  int strict;                   /* reference envelope: alpha 0.1, index 1, numCol 35 < n, 2 <= p <= 64 */
+} fkpc_options;
+
+/* One CI test result. */
+typedef struct fkpc_ci_record {
+  double p_value;      /* p used for the decision */
+  double p_exact;      /* dcc.gamma exact-screen p (== p_value for other methods) */
+  double statistic;    /* nV2, HSIC or the permutation statistic */
+  double mean;         /* gamma-approximation mean (NaN for permutation methods) */
+  double variance;     /* gamma-approximation variance (NaN for permutation methods) */
+  int status;          /* FKPC_OK or a status code */
+  unsigned int flags;  /* FKPC_FLAG_* */
+} fkpc_ci_record;
+
+/* Per-stage device timings of the last batched call, milliseconds. */
+typedef struct fkpc_stage_stats {
+  double setup_ms;          /* host design setup (TPRS / additive bases, QR) */
+  double upload_ms;         /* host -> device copies */
+  double fit_ms;            /* GCV selection + residuals */
+  double statistic_ms;      /* dCov / HSIC statistics and p-values */
+  double refine_ms;         /* dcc.gamma guard-band low-rank refinement */
+  double download_ms;       /* device -> host copies */
+  double total_ms;          /* wall time of the call */
+  int designs;              /* distinct conditioning sets */
+  int targets;              /* distinct (target, S) residual fits */
+  int pairs;                /* CI tests evaluated */
+  int guarded;              /* tests refined in the guard band */
+  int kernel_launches;      /* library kernels launched by the call */
+  double h2d_bytes;         /* host -> device bytes copied by the call */
+  double d2h_bytes;         /* device -> host bytes copied by the call */
+  double fit_evaluations;   /* GCV objective evaluations over all fits */
+  double fit_flops;         /* algorithmic FP64 flops of the fit stage */
+  double statistic_flops;   /* algorithmic FP64 flops of the statistic stage */
+} fkpc_stage_stats;
+
+typedef struct fkpc_trace_row {
+  int level;
+  int task_index;      /* position in the canonical level plan */
+  int edge_x, edge_y;  /* edge, edge_x < edge_y */
+  int x, y;            /* tested orientation */
+  int s_offset;        /* into fkpc_result.trace_s_values */
+  int s_count;
+  double p_value;
+  double p_exact;
+  int deleted;         /* p_value >= alpha */
+  unsigned int flags;
+} fkpc_trace_row;
+
+typedef struct fkpc_result {
+  int n, p;
+  int levels;                /* levels executed */
+  int* adjacency;            /* p*p, column-major, 1 = edge kept */
+  double* pmax;              /* p*p, column-major; -Inf where untested */
+  int* sepset_offsets;       /* p*p+1, CSR over cells i + p*j (column-major) */
+  int* sepset_values;        /* conditioning sets of the deleting tests */
+  int* n_edgetests;          /* tests per level, length levels */
+  int trace_rows;
+  fkpc_trace_row* trace;     /* canonical replay order; NULL unless collect_trace */
+  int* trace_s_values;
+  double elapsed_sec;
+  fkpc_stage_stats stats;    /* accumulated over levels */
+} fkpc_result;
+
+/*
+ * Full default-Inf kernel-PC skeleton (pcalg "stable" level replay).
+ * Replaces C_full_cuda_ci_one_call_skeleton / _method
+ * (fastkpc/src/r_api_cuda.cpp:9183-9249, driven by
+ * fastkpc/src/full_cuda_ci_one_call.cpp:5040) as reached from
+ * fastkpc_compatible_cuda_skeleton() (fastkpc/R/fast_kpc.R:56-130).
+ */
+FKPC_API int fkpc_skeleton_run(const double* data_colmajor, int n, int p,
+                      const fkpc_options* options, fkpc_result** out);
+FKPC_API void fkpc_result_free(fkpc_result* result);
+
+/*
+ * One batch of CI tests (x, y, S): residuals of x and y on S by GCV-selected
+ * thin-plate / additive smooths, then the statistic and p-value.  Test t uses
+ * S = s_values[s_offsets[t] .. s_offsets[t+1]).
+ * Replaces execute_group (fastkpc/src/full_cuda_ci_one_call.cpp:4197-5038)
+ * and its CUDA calls run_full_cuda_ci_phase35_exact_batch
+ * (fastkpc/src/cuda/full_cuda_ci_vertical.cu:2316) and
+ * run_full_cuda_ci_method_batch (fastkpc/src/cuda/full_cuda_ci_method_batch.cu:2923).
+ * ``stats`` may be NULL.
+ */
+FKPC_API int fkpc_ci_level_batch(const double* data_colmajor, int n, int p,
+                        const int* x, const int* y, const int* s_offsets,
+                        const int* s_values, int count,
+                        const fkpc_options* options, fkpc_ci_record* out,
+                        fkpc_stage_stats* stats);
+
+/*
+ * The plain per-test form: one CI test, one launch set, synchronised.
+ * Replaces the vertical single-pair route
+ * (fastkpc/src/cuda/full_cuda_ci_vertical.cu:1240-1339).
+ */
+FKPC_API int fkpc_ci_plain_one(const double* data_colmajor, int n, int p, int x, int y,
+                      const int* s_values, int s_count,
+                      const fkpc_options* options, fkpc_ci_record* out);
+
+/*
+ * regrXonS residuals for ``count`` (target, S) fits: residuals is n x count
+ * column-major; log_sp receives up to ``max_penalties`` selected
+ * log smoothing parameters per fit (row-major count x max_penalties, unused
+ * entries NaN); status per fit.
+ * Replaces single_penalty_gcv_cuda (fastkpc/src/cuda/mgcv_single_penalty_gcv.cu:1863),
+ * multi_penalty_gcv_capacity_optimize_batch
+ * (fastkpc/src/cuda/mgcv_multi_penalty_gcv_capacity.cpp:233) and
+ * solve_fixed_sp_batch (fastkpc/src/cuda/mgcv_fixed_sp_runtime.cu:5668).
+ */
+FKPC_API int fkpc_regress_batch(const double* data_colmajor, int n, int p,
+                       const int* target, const int* s_offsets,
+                       const int* s_values, int count,
+                       const fkpc_options* options, double* residuals,
+                       double* log_sp, int max_penalties, int* status);
+
+/*
+ * Statistics and p-values for ``count`` pairs of given residual columns
+ * (residuals n x m column-major; pair t uses columns left[t], right[t]).
+ * ``permutations`` (count x replicates x n, int32) is required for the
+ * permutation methods and ignored otherwise.
+ * Replaces the statistic stage of run_full_cuda_ci_phase35_exact_batch,
+ * run_full_cuda_ci_phase35_legacy_eig_batch
+ * (fastkpc/src/cuda/full_cuda_ci_vertical.cu:2316,2940) and
+ * run_full_cuda_ci_method_batch.
+ */
+FKPC_API int fkpc_stat_batch(const double* residuals, int n, int m, const int* left,
+                    const int* right, int count, const int* permutations,
+                    const fkpc_options* options, fkpc_ci_record* out);
+
+/*
+ * GCV score, gradient and Gauss-Newton Hessian in rho = log(lambda) of the
+ * additive-smooth fit of data[:, target] on S at the given rho (one entry per
+ * conditioning variable), plus the exact Hessian for comparison.  Arrays are
+ * count-major: log_lambda/grad are count x m, hessians count x m x m.
+ * Replaces the analytic derivative block of
+ * evaluate_multi_penalty_target_device
+ * (fastkpc/src/cuda/mgcv_multi_penalty_gcv.cu:1274-1490).
+ */
+FKPC_API int fkpc_gcv_adjoint(const double* data_colmajor, int n, int p, int target,
+                     const int* s_values, int s_count, int count,
+                     const double* log_lambda, double* score, double* grad,
+                     double* gn_hessian, double* exact_hessian);
+
+/*
+ * Staged form of fkpc_ci_level_batch on the engine of options->device, for
+ * timing the device work with every input already resident in HBM:
+ * prepare (host set-up, uploads, graph capture), execute (``repeats`` graph
+ * launches; *device_ms = CUDA-event time of all of them on the engine's
+ * stream), collect (wait, download, validate).
+ * Same reference counterpart as fkpc_ci_level_batch.
+ */
+FKPC_API int fkpc_batch_prepare(const double* data_colmajor, int n, int p,
+                                const int* x, const int* y, const int* s_offsets,
+                                const int* s_values, int count,
+                                const fkpc_options* options);
+FKPC_API int fkpc_batch_execute(int device, int repeats, double* device_ms);
+FKPC_API int fkpc_batch_collect(int device, fkpc_ci_record* out,
+                                fkpc_stage_stats* stats);
+/*
+ * Replay one kernel of the prepared batch alone ``repeats`` times and return
+ * its mean CUDA-event duration (ms) and its algorithmic FP64 flops per launch.
+ * Stages: 0 fit single, 1 fit multi (q <= 40), 2 fit multi (q <= 76),
+ * 3 dCov components, 4 dCov pairs, 5 HSIC components, 6 HSIC pairs,
+ * 7 low-rank eigen, 8 low-rank pairs.  Run fkpc_batch_execute first.
+ * No reference counterpart (measurement utility).
+ */
+FKPC_API int fkpc_batch_time_stage(int device, int stage, int repeats,
+                                   double* avg_ms, double* flops_per_launch);
+/*
+ * Dense FP64 FMA throughput of the device (TFLOP/s), measured with
+ * independent FMA chains in every thread.  No reference counterpart.
+ */
+FKPC_API int fkpc_measure_fp64_peak(int device, double* tflops);
+
+/*
+ * Host-only design set-up for one conditioning set S (no device needed):
+ * q and m always; when non-NULL, X (n x q column-major), penalties
+ * (m blocks, each placed in a full q x q matrix, column-major, m*q*q) and
+ * the mgcv initial log smoothing parameters (m).
+ * Replaces full_cuda_ci_native_setup
+ * (fastkpc/src/full_cuda_ci_native_setup.cpp:1321) with initial.sp
+ * (:1019-1127).
+ */
+FKPC_API int fkpc_design_export(const double* data_colmajor, int n, int p,
+                                const int* s_values, int s_count, int* q, int* m,
+                                double* X, double* penalties,
+                                double* initial_log_sp);
+
+FKPC_API const char* fkpc_last_error(void);
+FKPC_API int fkpc_abi_version(void);
+FKPC_API void fkpc_default_options(fkpc_options* options);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTKPC_B200_H */

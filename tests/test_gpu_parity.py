@@ -1,0 +1,190 @@
+"""CUDA path against the oracle and the reference fixtures (needs a B200).
+
+Every call goes through the C ABI (libfastkpc_b200.so).  Tolerances:
+statistics and gamma p-values within 1e-12 of the oracle (scipy gamma tail),
+residuals within 1e-10 relative to their maximum, permutation p-values and
+all graph / sepset / decision / test-count outcomes exact.
+"""
+import numpy as np
+import pytest
+
+import fastkpc_b200 as fk
+from fastkpc_b200 import workloads
+from oracle import gcv, rng, skeleton, stats, tprs
+
+pytestmark = pytest.mark.gpu
+
+STAT_TOL = 1e-12
+RESID_TOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def lib(lib_built):
+    return lib_built
+
+
+def _residual_pool(n, m, seed):
+    rs = np.random.default_rng(seed)
+    base = rs.normal(size=(n, m))
+    # dependent columns so p-values spread over (0, 1)
+    base[:, 1] = np.tanh(base[:, 0]) + 0.7 * base[:, 1]
+    base[:, 3] = np.sin(2 * base[:, 2]) * 0.5 + base[:, 3]
+    base[:, 5] = 0.2 * base[:, 4] ** 2 + base[:, 5]
+    return np.asfortranarray(base)
+
+
+@pytest.mark.parametrize("n", [60, 200, 500])
+def test_dcov_exact_statistics_match_oracle(lib, n):
+    R = _residual_pool(n, 8, n)
+    pairs = [(0, 1), (2, 3), (4, 5), (6, 7), (0, 7), (1, 6)]
+    rec = fk.stat_batch(R, pairs, ci_method="dcc.gamma")
+    for k, (a, b) in enumerate(pairs):
+        o = stats.dcov_gamma_exact(R[:, a], R[:, b])
+        assert abs(rec["p_exact"][k] - o["p_value"]) <= STAT_TOL
+        if rec["flags"][k] & fk.FLAG_GUARDED:
+            # guard band: the record carries the low-rank (legacy) statistic
+            assert 0.05 <= o["p_value"] <= 0.15
+            o = stats.dcov_gamma_legacy(R[:, a], R[:, b], 35)
+            assert abs(rec["p_value"][k] - o["p_value"]) <= 1e-10
+            assert rec["statistic"][k] == pytest.approx(o["statistic"], rel=1e-10)
+            continue
+        assert rec["statistic"][k] == pytest.approx(o["statistic"], rel=STAT_TOL)
+        assert rec["mean"][k] == pytest.approx(o["mean"], rel=STAT_TOL)
+        assert rec["variance"][k] == pytest.approx(o["variance"], rel=STAT_TOL)
+        assert abs(rec["p_value"][k] - o["p_value"]) <= STAT_TOL
+
+
+def test_dcov_guard_band_uses_low_rank_refinement(lib):
+    import json
+    from tests.conftest import golden_path
+    cases = json.load(open(golden_path("legacy_dcov_gamma.json")))["cases"]
+    R = np.asfortranarray(np.column_stack([np.array(c[k]) for c in cases for k in ("rx", "ry")]))
+    pairs = [(2 * i, 2 * i + 1) for i in range(len(cases))]
+    rec = fk.stat_batch(R, pairs, ci_method="dcc.gamma")
+    for k, c in enumerate(cases):
+        ex = stats.dcov_gamma_exact(np.array(c["rx"]), np.array(c["ry"]))
+        guarded = 0.05 <= ex["p_value"] <= 0.15
+        assert bool(rec["flags"][k] & fk.FLAG_GUARDED) == guarded, c["case_id"]
+        if guarded:
+            # reference legacy values (RSpectra-based, 1e-8) and the dense-eigen oracle
+            assert abs(rec["p_value"][k] - c["p_value"]) <= 1e-8, c["case_id"]
+            lg = stats.dcov_gamma_legacy(np.array(c["rx"]), np.array(c["ry"]), 35)
+            assert abs(rec["p_value"][k] - lg["p_value"]) <= 1e-10, c["case_id"]
+            assert (rec["p_value"][k] >= 0.1) == c["delete_edge"], c["case_id"]
+
+
+@pytest.mark.parametrize("n", [60, 200, 500])
+def test_hsic_gamma_matches_oracle(lib, n):
+    R = _residual_pool(n, 8, 7 + n)
+    pairs = [(0, 1), (2, 3), (4, 5), (6, 7), (0, 7)]
+    rec = fk.stat_batch(R, pairs, ci_method="hsic.gamma")
+    for k, (a, b) in enumerate(pairs):
+        o = stats.hsic_gamma(R[:, a], R[:, b], 1.0, 35)
+        assert rec["statistic"][k] == pytest.approx(o["statistic"], rel=1e-11)
+        assert rec["mean"][k] == pytest.approx(o["mean"], rel=1e-11)
+        assert rec["variance"][k] == pytest.approx(o["variance"], rel=1e-10)
+        assert abs(rec["p_value"][k] - o["p_value"]) <= 1e-11
+
+
+@pytest.mark.parametrize("method", ["dcc.perm", "hsic.perm"])
+def test_permutation_statistics_match_oracle(lib, method):
+    n, R_ = 80, 40
+    R = _residual_pool(n, 6, 11)
+    pairs = [(0, 1), (2, 3), (4, 5)]
+    stream = rng.RStream(2024)
+    gen = rng.dcc_permutations if method == "dcc.perm" else rng.hsic_permutations
+    perms = np.stack([gen(stream, n, R_) for _ in pairs])
+    rec = fk.stat_batch(R, pairs, ci_method=method, permutations=perms, seed=1, replicates=R_)
+    for k, (a, b) in enumerate(pairs):
+        if method == "dcc.perm":
+            o = stats.dcc_perm(R[:, a], R[:, b], perms[k])
+        else:
+            o = stats.hsic_perm(R[:, a], R[:, b], perms[k], 1.0, 35)
+        assert rec["p_value"][k] == o["p_value"]
+        assert rec["statistic"][k] == pytest.approx(o["statistic"], rel=1e-11)
+
+
+FITS = [(0, [3]), (20, [3]), (7, [2, 11]), (30, [5, 6]), (20, [1, 5, 9]), (0, [1, 5, 9]),
+        (41, [2, 11, 17, 40]), (8, [0, 12, 24, 36, 48]), (15, [1, 3, 5, 7, 9, 11, 13, 19])]
+
+
+def test_regress_residuals_match_oracle(lib, dev500):
+    d = dev500["data"]
+    resid, lsp, status = fk.regress_batch(d, FITS)
+    assert (status == 0).all()
+    for k, (t, S) in enumerate(FITS):
+        prep = gcv.Prepared(tprs.design(d, S))
+        r, info = gcv.fit(prep, d[:, t])
+        err = np.max(np.abs(resid[:, k] - r)) / np.max(np.abs(r))
+        assert err <= RESID_TOL, (t, S, err)
+        assert np.allclose(lsp[k, :len(S) if len(S) > 2 else 1], info["log_sp"], atol=1e-5)
+
+
+def _oracle_p(cache, t, method="dcc.gamma"):
+    return skeleton.ci_pvalue(cache, method, t[0], t[1], t[2])
+
+
+def test_level_batch_matches_oracle_and_plain(lib):
+    X, triples = workloads.level_batch_500x50(count=48)
+    rec, st = fk.ci_level_batch(X, triples)
+    assert st["pairs"] == 48 and st["kernel_launches"] > 0
+    cache = skeleton.ResidualCache(X)
+    for k, t in enumerate(triples):
+        p = _oracle_p(cache, t)
+        assert abs(rec["p_value"][k] - p) <= 1e-9, (t, rec["p_value"][k], p)
+        assert (rec["p_value"][k] >= 0.1) == (p >= 0.1)
+    plain = [fk.ci_plain_one(X, t[0], t[1], t[2]) for t in triples[:12]]
+    for k, r in enumerate(plain):
+        assert r["p_value"] == rec["p_value"][k]
+
+
+def test_hsic_level_batch_matches_oracle(lib):
+    X, triples = workloads.level_batch_500x50(count=24)
+    rec, _ = fk.ci_level_batch(X, triples, ci_method="hsic.gamma")
+    cache = skeleton.ResidualCache(X)
+    for k, t in enumerate(triples):
+        p = _oracle_p(cache, t, "hsic.gamma")
+        assert abs(rec["p_value"][k] - p) <= 1e-9, (t, rec["p_value"][k], p)
+
+
+def test_skeleton_500x50_matches_reference_fixture(lib, dev500, dev500_trace):
+    out = fk.fastkpc_compatible_cuda_skeleton(dev500["data"], 0.1, options={"trace_level": "logical"})
+    assert out["n_edgetests"] == dev500["n_edgetests"].tolist()
+    assert np.array_equal(out["adjacency"].astype(np.int8), dev500["adjacency"])
+    tasks = out["tasks"]
+    ref = {(r["level"], r["x"], r["y"], tuple(r["S"])): r for r in dev500_trace["logical_trace"]}
+    assert len(tasks["level"]) == len(ref)
+    for k in range(len(tasks["level"])):
+        key = (int(tasks["level"][k]), int(tasks["x"][k]), int(tasks["y"][k]), tuple(tasks["S"][k]))
+        assert bool(tasks["native_edge_deleted"][k]) == ref[key]["deletes_edge"], key
+    ref_sep = {(i, j): s for i, j, s in dev500_trace["sepsets"]}
+    for (i, j), s in ref_sep.items():
+        assert sorted(out["sepsets"][i][j]) == s
+
+
+@pytest.mark.parametrize("method", ["hsic.gamma", "dcc.gamma"])
+def test_skeleton_200x10_matches_oracle(lib, method):
+    X = workloads.skeleton_200x10()
+    out = fk.fastkpc_compatible_cuda_skeleton(X, 0.1, options={"ci_method": method, "numCol": 35,
+                                                               "trace_level": "logical"})
+    ora = skeleton.skeleton(X, 0.1, method)
+    assert out["n_edgetests"] == ora["n_edgetests"].tolist()
+    assert np.array_equal(out["adjacency"], ora["adjacency"])
+    for k, row in enumerate(ora["trace"]):
+        assert abs(out["tasks"]["p_used"][k] - row["p_value"]) <= 1e-9
+
+
+@pytest.mark.parametrize("method", ["dcc.perm", "hsic.perm"])
+def test_permutation_skeleton_matches_oracle_stream(lib, method):
+    X = workloads.nonlinear_sem(60, 5, 0.4, 9)[0]
+    opts = {"ci_method": method, "numCol": 35, "trace_level": "logical",
+            "permutation_params": {"replicates": 30, "seed": 42, "include_observed": True}}
+    out = fk.fastkpc_compatible_cuda_skeleton(X, 0.1, options=opts)
+    ora = skeleton.skeleton(X, 0.1, method, replicates=30, seed=42)
+    assert out["n_edgetests"] == ora["n_edgetests"].tolist()
+    assert np.array_equal(out["adjacency"], ora["adjacency"])
+    got = sorted(zip(out["tasks"]["level"], out["tasks"]["x"], out["tasks"]["y"],
+                     map(tuple, out["tasks"]["S"]), out["tasks"]["p_used"]))
+    exp = sorted((r["level"], r["x"], r["y"], tuple(r["S"]), r["p_value"]) for r in ora["trace"])
+    assert [g[:4] for g in got] == [e[:4] for e in exp]
+    assert [g[4] for g in got] == [e[4] for e in exp]

@@ -157,6 +157,31 @@ def _oracle_chunk(payload):
     return [skeleton.ci_pvalue(cache, "dcc.gamma", x, y, S) for (x, y, S) in triples]
 
 
+def skeleton_351x48(device, cores):
+    """Full default-Inf dcc.gamma skeleton on the n=351, p=48 SEM through the
+    public facade (wall seconds), and the oracle's rate on a sample of the
+    same run's level-1 tests, extrapolated to the run's logical test count."""
+    import fastkpc_b200 as fk
+    from fastkpc_b200 import workloads
+    X = workloads.skeleton_351x48()
+    t0 = time.perf_counter()
+    out = fk.fastkpc_compatible_cuda_skeleton(X, 0.1, options={"numCol": 35, "trace_level": "logical",
+                                                               "device": device})
+    wall = time.perf_counter() - t0
+    tasks = out["tasks"]
+    lvl1 = [(int(tasks["x"][k]), int(tasks["y"][k]), list(tasks["S"][k]))
+            for k in range(len(tasks["level"])) if tasks["level"][k] == 1]
+    rate, count, dt = cpu_oracle_rate(X, lvl1, budget_s=5.0, cores=cores)
+    total = int(sum(out["n_edgetests"]))
+    return {"wall_s": wall, "n_edgetests": out["n_edgetests"], "logical_tests": total,
+            "edges": int(out["adjacency"].sum() // 2), "device_ms": out["summary"]["stages"]["device_ms"],
+            "setup_ms": out["summary"]["stages"]["setup_ms"],
+            "cpu_estimate_s": total / rate, "cpu_cores": cores,
+            "cpu_sample": f"oracle on {count} level-1 tests of this run in {cores} processes ({dt:.1f} s), "
+                          f"rate extrapolated to all {total} logical tests",
+            "data": "synthetic SEM n=351 p=48 edge prob 0.1, max in-degree 8, seed 3"}
+
+
 def cpu_oracle_rate(X, triples, budget_s, cores):
     """Oracle throughput on the host cores over a bounded sample (tests/s)."""
     import multiprocessing as mp
@@ -253,6 +278,8 @@ def run_ours(args, world, rank, local, pg):
     plain.execute(1)
     plain_ms = plain.execute(1)
     prec, _ = plain.collect()
+    if not np.all(prec["p_value"] == recs["p_value"][:len(sample)]):
+        raise RuntimeError("plain and batched forms disagree")
     plain_rate = len(sample) / (plain_ms / 1e3)
 
     # end to end through the public call: host data in, records out
@@ -269,6 +296,7 @@ def run_ours(args, world, rank, local, pg):
     line = None
     if rank == 0:
         cores = host_cores()
+        skel = skeleton_351x48(local, cores)
         cpu_rate, cpu_n, cpu_dt = cpu_oracle_rate(X, triples, args.cpu_seconds / 4.0, cores)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -277,7 +305,10 @@ def run_ours(args, world, rank, local, pg):
             "config": {"workload": WORKLOAD, "n": 500, "p": 50, "triples_per_gpu": args.count,
                        "ci_method": "dcc.gamma", "parallelism": f"replicas x{world} (independent level batches)",
                        "l2": "inputs larger than L2 (design arena > 126 MB per step)",
-                       "designs": st["designs"], "fits": st["targets"], "guarded": st["guarded"]},
+                       "designs": st["designs"], "fits": st["targets"], "guarded": st["guarded"],
+                       "fit_evaluations": st["fit_evaluations"], "fit_iterations": st["fit_iterations"],
+                       "lowrank_components": st["lowrank_components"],
+                       "lowrank_steps_mean": st["lowrank_steps_mean"]},
             "plain": {"value": plain_rate, "unit": UNIT, "sample_tests": len(sample),
                       "batched_over_plain": value / world / plain_rate},
             "stages_ms": {s: timed[s][0] for s in stages},
@@ -291,6 +322,7 @@ def run_ours(args, world, rank, local, pg):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": e2e_stats["h2d_bytes"],
                     "d2h_bytes_per_step": e2e_stats["d2h_bytes"], "steps": len(e2e_t),
                     "setup_ms": e2e_stats["setup_ms"], "wall_s": statistics.median(e2e_t)},
+            "skeleton_351x48": skel,
             "gpu_launches": int(st["kernel_launches"]) * args.steps,
             "clocks": clocks_s,
         }

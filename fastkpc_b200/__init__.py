@@ -62,7 +62,9 @@ class StageStats(ctypes.Structure):
                 ("targets", ctypes.c_int), ("pairs", ctypes.c_int), ("guarded", ctypes.c_int),
                 ("kernel_launches", ctypes.c_int), ("h2d_bytes", ctypes.c_double), ("d2h_bytes", ctypes.c_double),
                 ("fit_evaluations", ctypes.c_double), ("fit_flops", ctypes.c_double),
-                ("statistic_flops", ctypes.c_double)]
+                ("statistic_flops", ctypes.c_double), ("fit_iterations", ctypes.c_double),
+                ("lowrank_components", ctypes.c_int), ("lowrank_steps_max", ctypes.c_int),
+                ("lowrank_steps_mean", ctypes.c_double), ("device_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

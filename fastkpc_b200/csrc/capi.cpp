@@ -163,6 +163,16 @@ void add_stats(fkpc_stage_stats* acc, const fkpc_stage_stats& s) {
   acc->pairs += s.pairs;
   acc->guarded += s.guarded;
   acc->kernel_launches += s.kernel_launches;
+  acc->h2d_bytes += s.h2d_bytes;
+  acc->d2h_bytes += s.d2h_bytes;
+  acc->fit_evaluations += s.fit_evaluations;
+  acc->fit_flops += s.fit_flops;
+  acc->statistic_flops += s.statistic_flops;
+  acc->fit_iterations += s.fit_iterations;
+  acc->lowrank_components += s.lowrank_components;
+  acc->lowrank_steps_max = std::max(acc->lowrank_steps_max, s.lowrank_steps_max);
+  acc->lowrank_steps_mean = s.lowrank_steps_mean;
+  acc->device_ms += s.device_ms;
 }
 
 // Evaluate ``tests`` on the engine in chunks; records in test order.
@@ -475,9 +485,7 @@ int fkpc_batch_prepare(const double* data, int n, int p, const int* x, const int
     }
     auto& eng = engine_for(options->device);
     eng.load(data, n, p);
-    fkpc_options o = *options;
-    o.mode = FKPC_MODE_BATCHED;
-    eng.prepare(tests, o, nullptr);
+    eng.prepare(tests, *options, nullptr);
   });
 }
 

@@ -224,6 +224,19 @@ __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const d
         cur = trial;
         min_score = trial.score;
       }
+      // terminal Newton polish to the stationary point: magic's stopping rule
+      // fixes rho only to about its tolerance, a few Newton steps (taken only
+      // when small, with positive curvature) make the selected point
+      // reproducible to rounding
+      for (int ps = 0; ps < 4; ++ps) {
+        if (!(cur.valid && cur.hessian > 1e-6 * cur.score)) break;
+        const double step = -cur.gradient / cur.hessian;
+        if (fabs(step) > 1e-6) break;
+        log_sp += step;
+        cur = single_objective(log_sp, ek, zk, active, yy, n);
+        ++calls;
+        if (fabs(step) <= 1e-10) break;
+      }
     }
   }
   // residual r = y - QW (h .* z)
@@ -253,29 +266,32 @@ __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const d
 namespace {
 
 constexpr int kMultiThreads = 128;
+constexpr int kPolishSteps = 4;
+constexpr double kPolishMaxStep = 1e-6;
+constexpr double kPolishDone = 1e-10;
+constexpr double kPolishCurvature = 1e-6;
 
 __device__ __forceinline__ int tri(int i, int j) { return j * (j + 1) / 2 + i; }  // packed upper, i <= j
 
 template <int QMAX, int RMAX>
 struct MultiLayout {
   static constexpr int TRI = QMAX * (QMAX + 1) / 2;
-  static constexpr int LDB = RMAX + 1;
+  static constexpr int LDB = RMAX + 1;  // odd leading dimensions: conflict-free column walks
   static constexpr int LDT = QMAX + 1;
   static constexpr int BSZ = (LDB * QMAX > LDT * RMAX) ? LDB * QMAX : LDT * RMAX;
-  static constexpr int RA = 0;
-  static constexpr int RINV = RA + TRI;
-  static constexpr int W = RINV + TRI;
-  static constexpr int B = W + TRI;  // also T after the factorisation
+  static constexpr int RS = 0;         // R of the design, packed upper (staged once per target)
+  static constexpr int RA = RS + TRI;
+  static constexpr int W = RA + TRI;
+  static constexpr int B = W + TRI;  // stacked penalty roots, then T = Ra^-T root
   static constexpr int WT = B + BSZ;
-  static constexpr int C = WT + LDT * RMAX;
-  static constexpr int D = C + RMAX * RMAX;
-  static constexpr int Y0 = D + RMAX * RMAX;
+  static constexpr int Y0 = WT + LDT * RMAX;
   static constexpr int G = Y0 + QMAX;
   static constexpr int WG = G + QMAX;
   static constexpr int E1 = WG + QMAX;
   static constexpr int AV = E1 + QMAX;
   static constexpr int BV = AV + RMAX;
-  static constexpr int TOTAL = BV + RMAX;
+  static constexpr int IDG = BV + RMAX;  // 1 / Ra(c, c)
+  static constexpr int TOTAL = IDG + QMAX;
 };
 
 struct MultiScalars {
@@ -296,6 +312,10 @@ struct MultiScalars {
   int status;
   int nzrow[128];
   int col_block[128];
+  int pair_i[kMaxPenalties * (kMaxPenalties + 1) / 2];
+  int pair_j[kMaxPenalties * (kMaxPenalties + 1) / 2];
+  double ja[kMaxPenalties * kMaxPenalties];  // thread-0 scratch: Jacobi matrix / Cholesky factor
+  double jv[kMaxPenalties * kMaxPenalties];  // Jacobi rotations
 };
 
 __device__ double block_sum(double v, MultiScalars* sc) {
@@ -311,42 +331,24 @@ __device__ double block_sum(double v, MultiScalars* sc) {
   return s;
 }
 
-// Householder reflector that maps (akk, B[0..nz)) onto (alpha, 0).
-__device__ void make_reflector(double* Ra, const double* Bk, int nz, int k, MultiScalars* sc, int slot) {
-  double sigma = 0.0;
-  for (int i = 0; i < nz; ++i) sigma += Bk[i] * Bk[i];
-  const double akk = Ra[tri(k, k)];
-  if (sigma == 0.0) {
-    sc->beta[slot] = 0.0;
-    sc->v0[slot] = 0.0;
-    return;
-  }
-  const double nrm = sqrt(akk * akk + sigma);
-  const double alpha = akk >= 0.0 ? -nrm : nrm;
-  const double v0 = akk - alpha;
-  sc->beta[slot] = 2.0 / (v0 * v0 + sigma);
-  sc->v0[slot] = v0;
-  Ra[tri(k, k)] = alpha;
-}
-
-// Objective at sc->trial: factor [R; B], W = R Ra^-1, score.  Leaves Ra, Rinv,
-// W, g, Wg in shared memory for multi_derivatives.
+// Objective at sc->trial: fold the stacked roots into R (Ra'Ra = X'X + S),
+// W = R Ra^-1 by row solves, g = W'y0, W g, EDF, RSS, score.  Leaves Ra, W,
+// g, Wg in shared memory for multi_derivatives.
 template <int QMAX, int RMAX>
 __device__ void multi_core(const DesignDev& des, const double* __restrict__ arena, int n, double* sm,
                            MultiScalars* sc) {
   using L = MultiLayout<QMAX, RMAX>;
   const int tid = threadIdx.x;
-  const int q = des.q, m = des.m, rs = des.rsum;
+  const int q = des.q, m = des.m;
   double* Ra = sm + L::RA;
-  double* Rinv = sm + L::RINV;
   double* W = sm + L::W;
   double* B = sm + L::B;
-  const double* R = arena + des.rmat;
+  const double* Rs = sm + L::RS;
+  double* idg = sm + L::IDG;
   const double* roots = arena + des.roots;
   if (tid < m) sc->lam[tid] = exp(sc->trial[tid]);
   for (int idx = tid; idx < L::LDB * q; idx += kMultiThreads) B[idx] = 0.0;
-  for (int c = 0; c < q; ++c)
-    for (int i = tid; i <= c; i += kMultiThreads) Ra[tri(i, c)] = R[i + static_cast<int64_t>(q) * c];
+  for (int idx = tid; idx < q * (q + 1) / 2; idx += kMultiThreads) Ra[idx] = Rs[idx];
   __syncthreads();
   for (int j = 0; j < m; ++j) {
     const double s = sqrt(sc->lam[j]);
@@ -358,48 +360,139 @@ __device__ void multi_core(const DesignDev& des, const double* __restrict__ aren
     }
   }
   __syncthreads();
-  if (tid == 0) make_reflector(Ra, B, sc->nzrow[0], 0, sc, 0);
-  __syncthreads();
-  for (int k = 0; k < q; ++k) {
-    const int slot = k & 1;
-    const double beta = sc->beta[slot];
-    const double v0 = sc->v0[slot];
-    const int nz = sc->nzrow[k];
-    const double* Bk = B + L::LDB * k;
+  if (RMAX <= 32) {
+    // Register-resident fold: thread j keeps column j of the stacked roots in
+    // registers for all q steps; step k only publishes column k (thread k)
+    // to shared memory, where the others read it as broadcasts.
+    double breg[RMAX <= 32 ? RMAX : 1];
     const int j = tid;
-    if (j > k && j < q) {
-      double* Bj = B + L::LDB * j;
-      if (beta != 0.0) {
-        double w = v0 * Ra[tri(k, j)];
-        for (int i = 0; i < nz; ++i) w += Bk[i] * Bj[i];
-        w *= beta;
-        Ra[tri(k, j)] -= w * v0;
-        for (int i = 0; i < nz; ++i) Bj[i] -= w * Bk[i];
-      }
-      if (j == k + 1) make_reflector(Ra, Bj, sc->nzrow[j], j, sc, slot ^ 1);
+    double* pub0 = B;               // two publication buffers of RMAX doubles
+    double* pub1 = B + L::LDB;
+    if (j < q) {
+#pragma unroll
+      for (int i = 0; i < (RMAX <= 32 ? RMAX : 1); ++i) breg[i] = B[i + L::LDB * j];
     }
     __syncthreads();
-  }
-  // Rinv = Ra^-1 (upper triangular), thread per column
-  if (tid < q) {
-    const int c = tid;
-    const double dc = Ra[tri(c, c)];
-    if (dc == 0.0) sc->status = kStatusRank;
-    Rinv[tri(c, c)] = 1.0 / dc;
-    for (int r = c - 1; r >= 0; --r) {
-      double s = 0.0;
-      for (int t = r + 1; t <= c; ++t) s += Ra[tri(r, t)] * Rinv[tri(t, c)];
-      Rinv[tri(r, c)] = -s / Ra[tri(r, r)];
+    auto publish = [&](int k, double* pub) {
+      // thread k: copy its column out and form the reflector
+      const int nz = sc->nzrow[k];
+      double sg0 = 0.0, sg1 = 0.0;
+#pragma unroll
+      for (int i = 0; i < (RMAX <= 32 ? RMAX : 1); i += 2) {
+        if (i < nz) { pub[i] = breg[i]; sg0 += breg[i] * breg[i]; }
+        if (i + 1 < nz) { pub[i + 1] = breg[i + 1]; sg1 += breg[i + 1] * breg[i + 1]; }
+      }
+      const double sg = sg0 + sg1;
+      const double akk = Ra[tri(k, k)];
+      const int slot = k & 1;
+      if (sg == 0.0) {
+        sc->beta[slot] = 0.0;
+        sc->v0[slot] = 0.0;
+      } else {
+        const double nrm = sqrt(akk * akk + sg);
+        const double alpha = akk >= 0.0 ? -nrm : nrm;
+        const double v0 = akk - alpha;
+        sc->beta[slot] = 2.0 / (v0 * v0 + sg);
+        sc->v0[slot] = v0;
+        Ra[tri(k, k)] = alpha;
+      }
+    };
+    if (j == 0) publish(0, pub0);
+    __syncthreads();
+    for (int k = 0; k < q; ++k) {
+      const int slot = k & 1;
+      const double* Bk = slot ? pub1 : pub0;
+      const double beta = sc->beta[slot];
+      const double v0 = sc->v0[slot];
+      const int nz = sc->nzrow[k];
+      if (j > k && j < q) {
+        if (beta != 0.0) {
+          double w0 = v0 * Ra[tri(k, j)], w1 = 0.0;
+#pragma unroll
+          for (int i = 0; i < (RMAX <= 32 ? RMAX : 1); i += 2) {
+            if (i < nz) w0 += Bk[i] * breg[i];
+            if (i + 1 < nz) w1 += Bk[i + 1] * breg[i + 1];
+          }
+          const double w = beta * (w0 + w1);
+          Ra[tri(k, j)] -= w * v0;
+#pragma unroll
+          for (int i = 0; i < (RMAX <= 32 ? RMAX : 1); ++i)
+            if (i < nz) breg[i] -= w * Bk[i];
+        }
+        if (j == k + 1) publish(k + 1, slot ? pub0 : pub1);
+      }
+      __syncthreads();
     }
+  } else {
+    for (int k = 0; k < q; ++k) {
+      // reflector for column k: warp 0 reduces |B[0..nz, k]|^2
+      const int nz = sc->nzrow[k];
+      const double* Bk = B + L::LDB * k;
+      if (tid < 32) {
+        double sg = 0.0;
+        for (int i = tid; i < nz; i += 32) sg += Bk[i] * Bk[i];
+        sg = warp_sum(sg);
+        if (tid == 0) {
+          const double akk = Ra[tri(k, k)];
+          if (sg == 0.0) {
+            sc->beta[0] = 0.0;
+            sc->v0[0] = 0.0;
+          } else {
+            const double nrm = sqrt(akk * akk + sg);
+            const double alpha = akk >= 0.0 ? -nrm : nrm;
+            const double v0 = akk - alpha;
+            sc->beta[0] = 2.0 / (v0 * v0 + sg);
+            sc->v0[0] = v0;
+            Ra[tri(k, k)] = alpha;
+          }
+        }
+      }
+      __syncthreads();
+      const double beta = sc->beta[0];
+      const double v0 = sc->v0[0];
+      const int j = tid;
+      if (beta != 0.0 && j > k && j < q) {
+        double* Bj = B + L::LDB * j;
+        double w0 = v0 * Ra[tri(k, j)], w1 = 0.0, w2 = 0.0, w3 = 0.0;
+        int i = 0;
+        for (; i + 3 < nz; i += 4) {
+          w0 += Bk[i] * Bj[i];
+          w1 += Bk[i + 1] * Bj[i + 1];
+          w2 += Bk[i + 2] * Bj[i + 2];
+          w3 += Bk[i + 3] * Bj[i + 3];
+        }
+        for (; i < nz; ++i) w0 += Bk[i] * Bj[i];
+        const double w = beta * ((w0 + w1) + (w2 + w3));
+        Ra[tri(k, j)] -= w * v0;
+        for (int r = 0; r < nz; ++r) Bj[r] -= w * Bk[r];
+      }
+      __syncthreads();
+    }
+  }
+  // reciprocal diagonal once, so the triangular solves below multiply
+  if (tid < q) {
+    const double dc = Ra[tri(tid, tid)];
+    if (dc == 0.0) sc->status = kStatusRank;
+    idg[tid] = 1.0 / dc;
   }
   __syncthreads();
-  // W = R Rinv (upper triangular)
-  for (int c = 0; c < q; ++c)
-    for (int i = tid; i <= c; i += kMultiThreads) {
-      double s = 0.0;
-      for (int t = i; t <= c; ++t) s += R[i + static_cast<int64_t>(q) * t] * Rinv[tri(t, c)];
-      W[tri(i, c)] = s;
+  // W = R Ra^-1: row i solves w Ra = R(i, :), w upper triangular
+  if (tid < q) {
+    const int i = tid;
+    for (int c = i; c < q; ++c) {
+      const double* rac = Ra + c * (c + 1) / 2;  // column c of Ra
+      double s0 = Rs[tri(i, c)], s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      int t = i;
+      for (; t + 3 < c; t += 4) {
+        s0 -= W[tri(i, t)] * rac[t];
+        s1 -= W[tri(i, t + 1)] * rac[t + 1];
+        s2 -= W[tri(i, t + 2)] * rac[t + 2];
+        s3 -= W[tri(i, t + 3)] * rac[t + 3];
+      }
+      for (; t < c; ++t) s0 -= W[tri(i, t)] * rac[t];
+      W[tri(i, c)] = ((s0 + s1) + (s2 + s3)) * idg[c];
     }
+  }
   __syncthreads();
   double* y0 = sm + L::Y0;
   double* g = sm + L::G;
@@ -442,45 +535,57 @@ __device__ void multi_core(const DesignDev& des, const double* __restrict__ aren
 }
 
 // Gradient and Hessian of V at the point of the last multi_core call.
+// M_j = T_j T_j' with T = Ra^-T root; with C = T'T and D = (WT)'(WT) every
+// trace is a block sum: d delta_j = lam_j sum_{a in j} D_aa,
+// d rss_j = 2 lam_j b_j'a_j, tr(M_i M_j P) = sum C_ab D_ab over block (i, j).
 template <int QMAX, int RMAX>
 __device__ void multi_derivatives(const DesignDev& des, const double* __restrict__ arena, int n, double* sm,
                                   MultiScalars* sc) {
   using L = MultiLayout<QMAX, RMAX>;
   const int tid = threadIdx.x;
   const int q = des.q, m = des.m, rs = des.rsum;
-  const double* Rinv = sm + L::RINV;
+  const double* Ra = sm + L::RA;
   const double* W = sm + L::W;
   double* T = sm + L::B;
   double* WT = sm + L::WT;
-  double* C = sm + L::C;
-  double* D = sm + L::D;
   const double* g = sm + L::G;
   const double* Wg = sm + L::WG;
   double* e1 = sm + L::E1;
   double* av = sm + L::AV;
   double* bv = sm + L::BV;
   const double* roots = arena + des.roots;
-  // T(i, col) = sum_t Rinv(t, i) root_j(t - off_j, c): Ra^-T root
-  for (int idx = tid; idx < q * rs; idx += kMultiThreads) {
-    const int i = idx % q, col = idx / q;
+  // T(:, col) = Ra^-T root(:, col): forward substitution, one thread per column
+  if (tid < rs) {
+    const int col = tid;
     const int j = sc->col_block[col];
     const int c = col - des.rowoff[j];
     const int off = des.off[j], dim = des.dim[j];
     const double* root = roots + des.rootoff[j];
-    double s = 0.0;
-    const int tend = min(i, off + dim - 1);
-    for (int t = off; t <= tend; ++t) s += Rinv[tri(t, i)] * root[(t - off) + dim * c];
-    T[i + L::LDT * col] = s;
+    for (int i = 0; i < off; ++i) T[i + L::LDT * col] = 0.0;
+    const double* idg = sm + L::IDG;
+    double* Tc = T + L::LDT * col;
+    for (int i = off; i < q; ++i) {
+      const double* rai = Ra + i * (i + 1) / 2;  // column i of Ra
+      double s0 = (i < off + dim) ? root[(i - off) + dim * c] : 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      int t = off;
+      for (; t + 3 < i; t += 4) {
+        s0 -= rai[t] * Tc[t];
+        s1 -= rai[t + 1] * Tc[t + 1];
+        s2 -= rai[t + 2] * Tc[t + 2];
+        s3 -= rai[t + 3] * Tc[t + 3];
+      }
+      for (; t < i; ++t) s0 -= rai[t] * Tc[t];
+      Tc[i] = ((s0 + s1) + (s2 + s3)) * idg[i];
+    }
   }
   // e1 = g - W'(W g)
-  if (tid < q) {
-    const int c = tid;
+  for (int c = tid; c < q; c += kMultiThreads) {
     double s = 0.0;
     for (int i = 0; i <= c; ++i) s += W[tri(i, c)] * Wg[i];
     e1[c] = g[c] - s;
   }
   __syncthreads();
-  // WT = W T
+  // W T, a = T'g, b = T'e1
   for (int idx = tid; idx < q * rs; idx += kMultiThreads) {
     const int i = idx % q, col = idx / q;
     const int j = sc->col_block[col];
@@ -488,7 +593,6 @@ __device__ void multi_derivatives(const DesignDev& des, const double* __restrict
     for (int t = max(i, des.off[j]); t < q; ++t) s += W[tri(i, t)] * T[t + L::LDT * col];
     WT[i + L::LDT * col] = s;
   }
-  // a = T'g, b = T'e1
   if (tid < rs) {
     double sa = 0.0, sb = 0.0;
     for (int i = 0; i < q; ++i) {
@@ -500,26 +604,13 @@ __device__ void multi_derivatives(const DesignDev& des, const double* __restrict
     bv[tid] = sb;
   }
   __syncthreads();
-  // C = T'T, D = (WT)'(WT): upper triangle, mirrored
-  for (int idx = tid; idx < rs * rs; idx += kMultiThreads) {
-    const int a = idx % rs, b = idx / rs;
-    if (a > b) continue;
-    double sc_ = 0.0, sd = 0.0;
-    for (int i = 0; i < q; ++i) {
-      sc_ += T[i + L::LDT * a] * T[i + L::LDT * b];
-      sd += WT[i + L::LDT * a] * WT[i + L::LDT * b];
-    }
-    C[a + RMAX * b] = sc_;
-    C[b + RMAX * a] = sc_;
-    D[a + RMAX * b] = sd;
-    D[b + RMAX * a] = sd;
-  }
-  __syncthreads();
   if (tid < m) {
     const int j = tid;
     double dd = 0.0, dr = 0.0;
     for (int a = des.rowoff[j]; a < des.rowoff[j] + des.rank[j]; ++a) {
-      dd += D[a + RMAX * a];
+      double d = 0.0;
+      for (int i = 0; i < q; ++i) d += WT[i + L::LDT * a] * WT[i + L::LDT * a];
+      dd += d;
       dr += bv[a] * av[a];
     }
     sc->ddelta[j] = sc->lam[j] * dd;
@@ -530,30 +621,41 @@ __device__ void multi_derivatives(const DesignDev& des, const double* __restrict
   const double delta = nd - sc->edf;
   const double s1 = nd / (delta * delta);
   const double s2 = 2.0 * s1 * sc->rss / delta;
-  if (tid < m * m) {
-    const int i = tid % m, j = tid / m;
-    if (j <= i) {
-      double trmmp = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
-      for (int a = des.rowoff[i]; a < des.rowoff[i] + des.rank[i]; ++a)
-        for (int b = des.rowoff[j]; b < des.rowoff[j] + des.rank[j]; ++b) {
-          const double cab = C[a + RMAX * b];
-          const double dab = D[a + RMAX * b];
-          trmmp += cab * dab;
-          t1 += av[b] * dab * av[a];  // a_j' D_ji a_i
-          t2 += bv[a] * cab * av[b];  // b_i' C_ij a_j
-          t3 += bv[b] * cab * av[a];  // b_j' C_ji a_i
-        }
-      const double ll = sc->lam[i] * sc->lam[j];
+  const int npair = m * (m + 1) / 2;
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int pidx = warp; pidx < npair; pidx += kMultiThreads / 32) {
+    const int bi = sc->pair_i[pidx], bj = sc->pair_j[pidx];
+    const int ri = des.rank[bi], rj = des.rank[bj];
+    const int oi = des.rowoff[bi], oj = des.rowoff[bj];
+    double trmmp = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    for (int e = lane; e < ri * rj; e += 32) {
+      const int a = oi + e % ri, b = oj + e / ri;
+      double cab = 0.0, dab = 0.0;
+      for (int i = 0; i < q; ++i) {
+        cab += T[i + L::LDT * a] * T[i + L::LDT * b];
+        dab += WT[i + L::LDT * a] * WT[i + L::LDT * b];
+      }
+      trmmp += cab * dab;
+      t1 += av[b] * dab * av[a];  // a_j' D_ji a_i
+      t2 += bv[a] * cab * av[b];  // b_i' C_ij a_j
+      t3 += bv[b] * cab * av[a];  // b_j' C_ji a_i
+    }
+    trmmp = warp_sum(trmmp);
+    t1 = warp_sum(t1);
+    t2 = warp_sum(t2);
+    t3 = warp_sum(t3);
+    if (lane == 0) {
+      const double ll = sc->lam[bi] * sc->lam[bj];
       double d2delta = -2.0 * ll * trmmp;
       double d2rss = 2.0 * ll * (t1 - t2 - t3);
-      if (i == j) {
-        d2delta += sc->ddelta[i];
-        d2rss += sc->drss[i];
+      if (bi == bj) {
+        d2delta += sc->ddelta[bi];
+        d2rss += sc->drss[bi];
       }
-      const double h = -2.0 * s1 / delta * (sc->ddelta[j] * sc->drss[i] + sc->ddelta[i] * sc->drss[j]) +
-                       s1 * d2rss + 3.0 * s2 / delta * sc->ddelta[i] * sc->ddelta[j] - s2 * d2delta;
-      sc->hess_c[i + kMaxPenalties * j] = h;
-      sc->hess_c[j + kMaxPenalties * i] = h;
+      const double h = -2.0 * s1 / delta * (sc->ddelta[bj] * sc->drss[bi] + sc->ddelta[bi] * sc->drss[bj]) +
+                       s1 * d2rss + 3.0 * s2 / delta * sc->ddelta[bi] * sc->ddelta[bj] - s2 * d2delta;
+      sc->hess_c[bi + kMaxPenalties * bj] = h;
+      sc->hess_c[bj + kMaxPenalties * bi] = h;
     }
   }
   if (tid < m) sc->grad_c[tid] = s1 * sc->drss[tid] - s2 * sc->ddelta[tid];
@@ -561,9 +663,9 @@ __device__ void multi_derivatives(const DesignDev& des, const double* __restrict
 }
 
 // Newton step from the Hessian eigen-decomposition (cyclic Jacobi, m <= 8).
-__device__ void newton_from_hessian(int m, MultiScalars* sc, bool* steepest) {
-  double a[kMaxPenalties * kMaxPenalties];
-  double v[kMaxPenalties * kMaxPenalties];
+__device__ void newton_from_hessian_eigen(int m, MultiScalars* sc, bool* steepest) {
+  double* a = sc->ja;
+  double* v = sc->jv;
   for (int j = 0; j < m; ++j)
     for (int i = 0; i < m; ++i) {
       a[i + kMaxPenalties * j] = sc->hess_c[i + kMaxPenalties * j];
@@ -631,17 +733,110 @@ __device__ void newton_from_hessian(int m, MultiScalars* sc, bool* steepest) {
   for (int r = 0; r < m; ++r) sc->steep[r] = mg == 0.0 ? 0.0 : -sc->gradient[r] / mg;
 }
 
+// Newton step for the magic loop (one thread).  A positive definite Hessian
+// (Cholesky succeeds) gives the Newton step -H^-1 g from the factor; when
+// Cholesky fails the eigen-decomposition decides, as in the reference: any
+// negative eigenvalue selects steepest descent.  The step is capped at 5 in
+// max norm and the steepest-descent direction is -g / max|g|.
+__device__ void newton_from_hessian(int m, MultiScalars* sc, bool* steepest) {
+  double* Lm = sc->ja;
+  for (int c = 0; c < m; ++c)
+    for (int r = 0; r < m; ++r) Lm[r + kMaxPenalties * c] = sc->hess_c[r + kMaxPenalties * c];
+  bool pd = true;
+  for (int c = 0; c < m && pd; ++c) {
+    double d = Lm[c + kMaxPenalties * c];
+    for (int k = 0; k < c; ++k) d -= Lm[c + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
+    if (!(d > 0.0)) {
+      pd = false;
+      break;
+    }
+    d = sqrt(d);
+    Lm[c + kMaxPenalties * c] = d;
+    const double inv = 1.0 / d;
+    for (int r = c + 1; r < m; ++r) {
+      double s = Lm[r + kMaxPenalties * c];
+      for (int k = 0; k < c; ++k) s -= Lm[r + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
+      Lm[r + kMaxPenalties * c] = s * inv;
+    }
+  }
+  if (!pd) {
+    newton_from_hessian_eigen(m, sc, steepest);
+    return;
+  }
+  *steepest = false;
+  double z[kMaxPenalties];
+  for (int r = 0; r < m; ++r) {
+    double s = -sc->gradient[r];
+    for (int k = 0; k < r; ++k) s -= Lm[r + kMaxPenalties * k] * z[k];
+    z[r] = s / Lm[r + kMaxPenalties * r];
+  }
+  double mx = 0.0;
+  for (int r = m - 1; r >= 0; --r) {
+    double s = z[r];
+    for (int k = r + 1; k < m; ++k) s -= Lm[k + kMaxPenalties * r] * z[k];
+    z[r] = s / Lm[r + kMaxPenalties * r];
+    mx = fmax(mx, fabs(z[r]));
+  }
+  for (int r = 0; r < m; ++r) sc->newton[r] = mx > 5.0 ? z[r] * (5.0 / mx) : z[r];
+  double mg = 0.0;
+  for (int r = 0; r < m; ++r) mg = fmax(mg, fabs(sc->gradient[r]));
+  for (int r = 0; r < m; ++r) sc->steep[r] = mg == 0.0 ? 0.0 : -sc->gradient[r] / mg;
+}
+
+// Terminal Newton polish (one thread): Newton step on the coordinates whose
+// curvature exceeds kPolishCurvature * V, by Cholesky of that sub-Hessian.
+// Returns 0 to stop (no active coordinate, indefinite, or step too large),
+// 1 when the step was applied, 2 when it was applied and was negligible.
+__device__ int polish_step(int m, MultiScalars* sc) {
+  int act[kMaxPenalties];
+  int na = 0;
+  for (int j = 0; j < m; ++j)
+    if (sc->hess_c[j + kMaxPenalties * j] > kPolishCurvature * sc->score) act[na++] = j;
+  if (na == 0) return 0;
+  double* Lm = sc->ja;
+  for (int c = 0; c < na; ++c)
+    for (int r = 0; r < na; ++r) Lm[r + kMaxPenalties * c] = sc->hess_c[act[r] + kMaxPenalties * act[c]];
+  for (int c = 0; c < na; ++c) {
+    double d = Lm[c + kMaxPenalties * c];
+    for (int k = 0; k < c; ++k) d -= Lm[c + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
+    if (!(d > 0.0)) return 0;
+    d = sqrt(d);
+    Lm[c + kMaxPenalties * c] = d;
+    for (int r = c + 1; r < na; ++r) {
+      double s = Lm[r + kMaxPenalties * c];
+      for (int k = 0; k < c; ++k) s -= Lm[r + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
+      Lm[r + kMaxPenalties * c] = s / d;
+    }
+  }
+  double z[kMaxPenalties];
+  for (int r = 0; r < na; ++r) {
+    double s = -sc->grad_c[act[r]];
+    for (int k = 0; k < r; ++k) s -= Lm[r + kMaxPenalties * k] * z[k];
+    z[r] = s / Lm[r + kMaxPenalties * r];
+  }
+  double mx = 0.0;
+  for (int r = na - 1; r >= 0; --r) {
+    double s = z[r];
+    for (int k = r + 1; k < na; ++k) s -= Lm[k + kMaxPenalties * r] * z[k];
+    z[r] = s / Lm[r + kMaxPenalties * r];
+    mx = fmax(mx, fabs(z[r]));
+  }
+  if (mx > kPolishMaxStep) return 0;
+  for (int r = 0; r < na; ++r) sc->log_sp[act[r]] += z[r];
+  return mx <= kPolishDone ? 2 : 1;
+}
+
 }  // namespace
 
 template <int QMAX, int RMAX>
-__global__ void __launch_bounds__(kMultiThreads) fit_multi_kernel(
+__global__ void __launch_bounds__(kMultiThreads, QMAX <= 40 ? 4 : 1) fit_multi_kernel(
     const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data,
     int n, const FitJob* __restrict__ jobs, const int* __restrict__ job_index, int job_count,
     double* __restrict__ residuals, FitResult* __restrict__ results) {
   using L = MultiLayout<QMAX, RMAX>;
   extern __shared__ double sm[];
   __shared__ MultiScalars sc;
-  __shared__ int ctl[4];  // steepest, converged, trying, accepted
+  __shared__ int ctl[4];
   if (blockIdx.x >= job_count) return;
   const int t = job_index[blockIdx.x];
   const FitJob job = jobs[t];
@@ -661,6 +856,19 @@ __global__ void __launch_bounds__(kMultiThreads) fit_multi_kernel(
     }
     for (int j = 0; j < m; ++j)
       for (int c = 0; c < des.rank[j]; ++c) sc.col_block[row++] = j;
+    int pp = 0;
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j <= i; ++j) {
+        sc.pair_i[pp] = i;
+        sc.pair_j[pp] = j;
+        ++pp;
+      }
+  }
+  {
+    const double* R = arena + des.rmat;
+    double* Rs = sm + L::RS;
+    for (int c = 0; c < q; ++c)
+      for (int i = tid; i <= c; i += kMultiThreads) Rs[tri(i, c)] = R[i + static_cast<int64_t>(q) * c];
   }
   // y0 = Q'y, yy
   double* y0 = sm + L::Y0;
@@ -772,7 +980,26 @@ __global__ void __launch_bounds__(kMultiThreads) fit_multi_kernel(
       if (sc.status != kStatusOk) break;
     }
   }
-  // final fit at the selected point
+  // terminal Newton polish from the selected point
+  if (sc.status == kStatusOk) {
+    __syncthreads();
+    if (tid < m) sc.trial[tid] = sc.log_sp[tid];
+    __syncthreads();
+    multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+    for (int ps = 0; ps < kPolishSteps && sc.status == kStatusOk; ++ps) {
+      multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
+      if (tid == 0) ctl[1] = polish_step(m, &sc);
+      __syncthreads();
+      const int act = ctl[1];
+      if (act == 0) break;
+      if (tid < m) sc.trial[tid] = sc.log_sp[tid];
+      __syncthreads();
+      multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+      ++calls;
+      if (act == 2) break;
+    }
+  }
+  // final fit at the selected point (the last core call may be a rejected probe)
   if (sc.status == kStatusOk) {
     __syncthreads();
     if (tid < m) sc.trial[tid] = sc.log_sp[tid];

@@ -292,6 +292,11 @@ __device__ void tridiag_inverse_iteration(const double* d, const double* e, int 
       b = sup2;
     }
   }
+  for (int i = 0; i < m; ++i) {
+    double piv_ = u0[i];
+    if (fabs(piv_) < small) piv_ = piv_ >= 0.0 ? small : -small;
+    u0[i] = 1.0 / piv_;
+  }
   for (int sweep = 0; sweep < 3; ++sweep) {
     // forward (apply L and pivots)
     for (int i = 0; i + 1 < m; ++i) {
@@ -303,66 +308,56 @@ __device__ void tridiag_inverse_iteration(const double* d, const double* e, int 
         x[i + 1] -= l[i] * x[i];
       }
     }
-    // back substitution with U (diag u0, super u1, super-2 u2)
+    // back substitution with U (diag u0 held as reciprocals, super u1, super-2 u2)
     for (int i = m - 1; i >= 0; --i) {
       double s = x[i];
       if (i + 1 < m) s -= u1[i] * x[i + 1];
       if (i + 2 < m) s -= u2[i] * x[i + 2];
-      double piv_ = u0[i];
-      if (fabs(piv_) < small) piv_ = piv_ >= 0.0 ? small : -small;
-      x[i] = s / piv_;
+      x[i] = s * u0[i];
     }
     double nrm = 0.0;
     for (int i = 0; i < m; ++i) nrm += x[i] * x[i];
-    nrm = sqrt(nrm);
-    for (int i = 0; i < m; ++i) x[i] /= nrm;
+    const double inv = 1.0 / sqrt(nrm);
+    for (int i = 0; i < m; ++i) x[i] *= inv;
   }
 }
 
-// eigenvalues of a symmetric tridiagonal matrix by implicit QL (values only)
-__device__ bool tridiag_values(double* d, double* e, int m) {
-  if (m <= 0) return true;
-  e[m - 1] = 0.0;
-  for (int l = 0; l < m; ++l) {
-    int iter = 0;
-    for (;;) {
-      int mm = l;
-      for (; mm < m - 1; ++mm) {
-        const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
-        if (fabs(e[mm]) <= 2.220446049250313e-16 * dd) break;
-      }
-      if (mm == l) break;
-      if (++iter > 60) return false;
-      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-      double r = hypot(g, 1.0);
-      g = d[mm] - d[l] + e[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
-      double s = 1.0, c = 1.0, p = 0.0;
-      int i = mm - 1;
-      for (; i >= l; --i) {
-        double f = s * e[i];
-        const double bb = c * e[i];
-        r = hypot(f, g);
-        e[i + 1] = r;
-        if (r == 0.0) {
-          d[i + 1] -= p;
-          e[mm] = 0.0;
-          break;
-        }
-        s = f / r;
-        c = g / r;
-        g = d[i + 1] - p;
-        r = (d[i] - g) * s + 2.0 * c * bb;
-        p = s * r;
-        d[i + 1] = g + p;
-        g = c * r - bb;
-      }
-      if (r == 0.0 && i >= l) continue;
-      d[l] -= p;
-      e[l] = g;
-      e[mm] = 0.0;
+// Number of eigenvalues of the symmetric tridiagonal (d, e) below x: sign
+// changes of the characteristic-polynomial sequence p_0 = 1,
+// p_{i+1} = (d_i - x) p_i - e_{i-1}^2 p_{i-1} (Sturm), kept in range by exact
+// power-of-two rescaling -- no division in the recurrence.  A zero term is
+// replaced by a tiny value of the opposite sign (a negative pivot).
+__device__ int sturm_count(const double* d, const double* e, int m, double x, double pivmin) {
+  (void)pivmin;
+  int cnt = 0;
+  double pm = 0.0, pc = 1.0;
+  for (int i = 0; i < m; ++i) {
+    double pn = (d[i] - x) * pc - (i > 0 ? e[i - 1] * e[i - 1] * pm : 0.0);
+    if (pn == 0.0) pn = -copysign(1e-300, pc) * 1e-8;
+    if ((pn < 0.0) != (pc < 0.0)) ++cnt;
+    pm = pc;
+    pc = pn;
+    const double a = fabs(pc);
+    if (a > 1e150 || a < 1e-150) {
+      const int ex = ilogb(a);
+      pc = scalbn(pc, -ex);
+      pm = scalbn(pm, -ex);
     }
   }
-  return true;
+  return cnt;
+}
+
+// The idx-th smallest eigenvalue (0-based) of (d, e) by bisection on
+// [lo, hi] until the bracket is at rounding level.
+__device__ double bisect_eigenvalue(const double* d, const double* e, int m, int idx, double lo, double hi,
+                                    double pivmin) {
+  for (int it = 0; it < 200; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (hi - lo <= 4.0 * 2.220446049250313e-16 * fmax(fabs(lo), fabs(hi)) + pivmin || mid == lo || mid == hi) break;
+    if (sturm_count(d, e, m, mid, pivmin) <= idx) lo = mid;
+    else hi = mid;
+  }
+  return 0.5 * (lo + hi);
 }
 
 struct LanczosShared {
@@ -371,6 +366,8 @@ struct LanczosShared {
   double td[kLanczosMax];
   double te[kLanczosMax];
   double theta[64];
+  double cand[128];
+  int cand_idx[128];
   int sel[64];
   double coef[kLanczosMax];
   double red[kStatThreads / 32];
@@ -383,8 +380,9 @@ struct LanczosShared {
 
 // Grid-stride over the guarded components: CTA b handles slots b, b + grid,
 // ...  guard[1] holds the slot count, slot_comps the component of each slot.
-// workspace per CTA: V (n x (kLanczosMax+1)), S (kLanczosMax x 64) Ritz
-// coefficients, scratch 7 * kLanczosMax.
+// workspace per CTA: V (n x (kLanczosMax+1)) Lanczos basis, S
+// (kLanczosMax x 64) Ritz coefficient vectors, 64 x 5 x kLanczosMax
+// inverse-iteration scratch (one set per thread).
 __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double* __restrict__ residuals, int n,
                                                                      const int* __restrict__ comp_cols,
                                                                      const int* __restrict__ guard,
@@ -404,7 +402,7 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
   double* qv = sm + n;
   double* w = sm + 2 * n;
   const int64_t per = static_cast<int64_t>(n) * (kLanczosMax + 1) + static_cast<int64_t>(kLanczosMax) * 64 +
-                      6 * kLanczosMax + kLanczosMax;
+                      static_cast<int64_t>(64) * 5 * kLanczosMax;
   double* V = workspace + per * blockIdx.x;
   double* S = V + static_cast<int64_t>(n) * (kLanczosMax + 1);
   double* scratch = S + static_cast<int64_t>(kLanczosMax) * 64;
@@ -449,7 +447,11 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
       w[i] = v;
     }
     __syncthreads();
-    // two passes of classical Gram-Schmidt against V[:, 0..j]
+    // classical Gram-Schmidt against V[:, 0..j]; a second pass only when the
+    // first removed more than half the norm ("twice is enough")
+    double before = 0.0;
+    for (int i = tid; i < n; i += blockDim.x) before += w[i] * w[i];
+    before = block_sum256(before, ls.red);
     for (int pass = 0; pass < 2; ++pass) {
       const int warp = tid >> 5, lane = tid & 31;
       for (int b = warp; b <= j; b += blockDim.x >> 5) {
@@ -460,12 +462,16 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
         if (lane == 0) ls.coef[b] = s;
       }
       __syncthreads();
+      double after = 0.0;
       for (int i = tid; i < n; i += blockDim.x) {
         double s = w[i];
         for (int b = 0; b <= j; ++b) s -= ls.coef[b] * V[i + static_cast<int64_t>(n) * b];
         w[i] = s;
+        after += s * s;
       }
-      __syncthreads();
+      after = block_sum256(after, ls.red);
+      if (after > 0.25 * before) break;
+      before = after;
     }
     double nn = 0.0;
     for (int i = tid; i < n; i += blockDim.x) nn += w[i] * w[i];
@@ -478,55 +484,65 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
     }
     const bool invariant = beta <= 1e-15 * anorm;
     const int m = j + 1;
-    const bool check = invariant || m == maxit || (m >= k + 10 && ((m - k) % 10 == 0));
+    const int first = min(maxit, k + 40);
+    const bool check = invariant || m == maxit || (m >= first && ((m - first) % 10 == 0));
     __syncthreads();
     if (check) {
-      if (tid == 0) {
-        for (int i = 0; i < m; ++i) {
-          ls.td[i] = ls.alpha[i];
-          ls.te[i] = i + 1 < m ? ls.beta[i] : 0.0;
+      const int kk = min(k, m);
+      double tnorm = 0.0, lo = INFINITY, hi = -INFINITY, bmax = 0.0;
+      for (int i = 0; i < m; ++i) {
+        const double bl = i > 0 ? fabs(ls.beta[i - 1]) : 0.0;
+        const double br = i + 1 < m ? fabs(ls.beta[i]) : 0.0;
+        lo = fmin(lo, ls.alpha[i] - bl - br);
+        hi = fmax(hi, ls.alpha[i] + bl + br);
+        tnorm = fmax(tnorm, fabs(ls.alpha[i]) + bl + br);
+        if (i + 1 < m) bmax = fmax(bmax, ls.beta[i] * ls.beta[i]);
+      }
+      const double pivmin = fmax(2.2250738585072014e-308, 2.220446049250313e-16 * fmax(bmax, 1e-300));
+      // candidates: the kk largest and kk smallest Ritz values (bisection, one per thread)
+      if (tid < 2 * kk) {
+        const int idx = tid < kk ? m - 1 - tid : tid - kk;
+        if (idx >= 0 && idx < m) {
+          ls.cand[tid] = bisect_eigenvalue(ls.alpha, ls.beta, m, idx, lo, hi, pivmin);
+          ls.cand_idx[tid] = idx;
+        } else {
+          ls.cand_idx[tid] = -1;
         }
-        if (!tridiag_values(ls.td, ls.te, m)) ls.fail = 1;
-        // select k largest |theta| (ties toward the lower index)
-        const int kk = min(k, m);
+      }
+      __syncthreads();
+      if (tid == 0) {
+        // kk largest |theta| among distinct indices (ties toward the higher index)
         for (int c = 0; c < kk; ++c) {
           int best = -1;
-          double bm = -1.0;
-          for (int i = 0; i < m; ++i) {
+          for (int u = 0; u < 2 * kk; ++u) {
+            const int id = ls.cand_idx[u];
+            if (id < 0) continue;
             bool used = false;
-            for (int u = 0; u < c; ++u)
-              if (ls.sel[u] == i) used = true;
+            for (int v = 0; v < c; ++v)
+              if (ls.sel[v] == id) used = true;
+            for (int v = 0; v < u; ++v)
+              if (ls.cand_idx[v] == id) used = true;  // duplicate index from the other end
             if (used) continue;
-            if (fabs(ls.td[i]) > bm) {
-              bm = fabs(ls.td[i]);
-              best = i;
-            }
+            if (best < 0 || fabs(ls.cand[u]) > fabs(ls.cand[best]) ||
+                (fabs(ls.cand[u]) == fabs(ls.cand[best]) && id > ls.cand_idx[best]))
+              best = u;
           }
-          ls.sel[c] = best;
-          ls.theta[c] = ls.td[best];
+          ls.sel[c] = ls.cand_idx[best];
+          ls.theta[c] = ls.cand[best];
         }
       }
       __syncthreads();
-      // Ritz coefficient vectors by inverse iteration on T (thread 0, one
-      // selected value after another, so one scratch set suffices)
-      const int kk = min(k, m);
-      double tnorm = 0.0;
-      for (int i = 0; i < m; ++i) tnorm = fmax(tnorm, fabs(ls.alpha[i]) + 2.0 * fabs(ls.beta[i]));
+      // Ritz coefficient vectors by inverse iteration, one thread per value
       if (tid < kk) {
         double* x = S + static_cast<int64_t>(kLanczosMax) * tid;
+        double* base = scratch + static_cast<int64_t>(tid) * 5 * kLanczosMax;
         for (int i = 0; i < m; ++i) x[i] = (1.0 + 0.01 * ((i * 7 + tid) % 5)) / sqrt(static_cast<double>(m));
+        tridiag_inverse_iteration(ls.alpha, ls.beta, m, ls.theta[tid], tnorm, x, base, base + kLanczosMax,
+                                  base + 2 * kLanczosMax, base + 3 * kLanczosMax,
+                                  reinterpret_cast<int*>(base + 4 * kLanczosMax));
       }
       __syncthreads();
       if (tid == 0) {
-        double* l = scratch;
-        double* u0 = scratch + kLanczosMax;
-        double* u1 = scratch + 2 * kLanczosMax;
-        double* u2 = scratch + 3 * kLanczosMax;
-        int* piv = reinterpret_cast<int*>(scratch + 4 * kLanczosMax);
-        for (int c = 0; c < kk; ++c) {
-          double* x = S + static_cast<int64_t>(kLanczosMax) * c;
-          tridiag_inverse_iteration(ls.alpha, ls.beta, m, ls.theta[c], tnorm, x, l, u0, u1, u2, piv);
-        }
         bool conv = m >= k;
         double tmax = 0.0;
         for (int c = 0; c < kk; ++c) tmax = fmax(tmax, fabs(ls.theta[c]));
@@ -567,7 +583,10 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
     __syncthreads();
   }
   if (tid < k) vals[static_cast<int64_t>(k) * slot + tid] = ls.theta[tid];
-  if (tid == 0) status[slot] = ls.fail ? kStatusNotConverged : kStatusOk;
+  if (tid == 0) {
+    status[slot] = ls.fail ? kStatusNotConverged : kStatusOk;
+    status[cap + slot] = ls.steps;
+  }
   __syncthreads();
   }
 }
@@ -1010,7 +1029,7 @@ cudaError_t launch_dcov_pairs(const double* residuals, int n, const int* comp_co
 
 size_t legacy_eigen_workspace_doubles(int n, int ctas) {
   const size_t per = static_cast<size_t>(n) * (kLanczosMax + 1) + static_cast<size_t>(kLanczosMax) * 64 +
-                     6 * kLanczosMax + kLanczosMax;
+                     static_cast<size_t>(64) * 5 * kLanczosMax;
   return per * static_cast<size_t>(ctas);
 }
 

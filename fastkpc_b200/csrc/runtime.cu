@@ -49,7 +49,7 @@ double upload(DevBuf<T>& buf, const std::vector<T>& host, cudaStream_t s) {
 
 constexpr double kGuardLower = 0.05;
 constexpr double kGuardUpper = 0.15;
-constexpr int kLegacyCtas = 296;  // 2 x 148 SMs
+constexpr int kLegacyCtas = 148;  // one per SM: the Lanczos bases of the active components stay in L2
 
 }  // namespace
 
@@ -298,7 +298,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       d_guard_.ensure(2 + npairs + ncomp + guard_cap_);
       d_lr_vals_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col);
       d_lr_vecs_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col * n);
-      d_lr_status_.ensure(guard_cap_);
+      d_lr_status_.ensure(2 * static_cast<size_t>(guard_cap_));
       d_legacy_ws_.ensure(legacy_eigen_workspace_doubles(n, kLegacyCtas));
     }
     if (method == FKPC_DCC_PERM || method == FKPC_HSIC_PERM) {
@@ -319,6 +319,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
 
 void Engine::prepare(const std::vector<Test>& tests, const fkpc_options& opt, RStream* rstream) {
   if (n_ == 0) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "no data loaded");
+  graph_timed_ = false;
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   opt_ = opt;
   stats_enabled_ = true;
@@ -421,6 +422,7 @@ void Engine::enqueue() {
 void Engine::execute() {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   const bool perm = opt_.ci_method == FKPC_DCC_PERM || opt_.ci_method == FKPC_HSIC_PERM;
+  graph_timed_ = false;
   if (opt_.mode == FKPC_MODE_PLAIN && perm) {
     // one permutation test: its launch sequence without a graph
     cuda_check(configure_fit_kernels(), "kernel attributes");
@@ -458,7 +460,10 @@ void Engine::execute() {
     cuda_check(cudaStreamEndCapture(stream_, &graph_), "end capture");
     cuda_check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
   }
+  cuda_check(cudaEventRecord(ev_[4], stream_), "event");
   cuda_check(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
+  cuda_check(cudaEventRecord(ev_[5], stream_), "event");
+  graph_timed_ = true;
 }
 
 void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
@@ -495,9 +500,21 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
     cuda_check(cudaMemcpy(counts, d_guard_.get(), sizeof(counts), cudaMemcpyDeviceToHost), "download");
     guarded = counts[0];
     if (counts[1] > guard_cap_) throw Error(FKPC_STATUS_ALLOCATION, "guard-band low-rank capacity exceeded");
-    std::vector<int> lrs(std::min(counts[1], guard_cap_));
-    if (!lrs.empty())
-      cuda_check(cudaMemcpy(lrs.data(), d_lr_status_.get(), lrs.size() * sizeof(int), cudaMemcpyDeviceToHost), "download");
+    const int slots = std::min(counts[1], guard_cap_);
+    std::vector<int> lrs(slots), steps(slots);
+    if (slots > 0) {
+      cuda_check(cudaMemcpy(lrs.data(), d_lr_status_.get(), slots * sizeof(int), cudaMemcpyDeviceToHost), "download");
+      cuda_check(cudaMemcpy(steps.data(), d_lr_status_.get() + guard_cap_, slots * sizeof(int), cudaMemcpyDeviceToHost),
+                 "download");
+    }
+    lowrank_steps_mean_ = 0.0;
+    lowrank_steps_max_ = 0;
+    for (int k = 0; k < slots; ++k) {
+      lowrank_steps_mean_ += steps[k];
+      lowrank_steps_max_ = std::max(lowrank_steps_max_, steps[k]);
+    }
+    if (slots > 0) lowrank_steps_mean_ /= slots;
+    lowrank_slots_ = slots;
     for (int s : lrs)
       if (s != kStatusOk) throw Error(FKPC_STATUS_NOT_CONVERGED, "low-rank eigen-solve of a guarded component did not converge");
   }
@@ -519,14 +536,21 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
     }
   }
   if (stats) {
+    // stage split from the event pairs of a direct (uncaptured) launch; a graph
+    // replay reports its whole device time as fit_ms + statistic_ms = device_ms
     float f_ms = 0.f, s_ms = 0.f, g_ms = 0.f, tot = 0.f;
-    cudaEventElapsedTime(&f_ms, ev_[0], ev_[1]);
-    cudaEventElapsedTime(&tot, ev_[0], ev_[3]);
-    s_ms = tot - f_ms;
-    if (stats_enabled_ && opt_.ci_method == FKPC_DCC_GAMMA && !pairs_.empty()) {
-      cudaEventElapsedTime(&g_ms, ev_[2], ev_[3]);
-      s_ms -= g_ms;
+    if (graph_timed_) {
+      cudaEventElapsedTime(&tot, ev_[4], ev_[5]);
+    } else {
+      cudaEventElapsedTime(&f_ms, ev_[0], ev_[1]);
+      cudaEventElapsedTime(&tot, ev_[0], ev_[3]);
+      s_ms = tot - f_ms;
+      if (stats_enabled_ && opt_.ci_method == FKPC_DCC_GAMMA && !pairs_.empty()) {
+        cudaEventElapsedTime(&g_ms, ev_[2], ev_[3]);
+        s_ms -= g_ms;
+      }
     }
+    stats->device_ms = tot;
     stats->setup_ms = setup_ms_;
     stats->upload_ms = upload_ms_;
     stats->fit_ms = f_ms;
@@ -545,6 +569,13 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
     for (const auto& r : mres) evals += r.evaluations;
     stats->fit_evaluations = evals;
     stats->fit_flops = stage_flops_[0] + stage_flops_[1] + stage_flops_[2];
+    double its = 0.0;
+    for (const auto& r : sres) its += r.iterations;
+    for (const auto& r : mres) its += r.iterations;
+    stats->fit_iterations = its;
+    stats->lowrank_components = lowrank_slots_;
+    stats->lowrank_steps_mean = lowrank_steps_mean_;
+    stats->lowrank_steps_max = lowrank_steps_max_;
     stats->statistic_flops = stage_flops_[3] + stage_flops_[4] + stage_flops_[5] + stage_flops_[6];
   }
 }
@@ -873,7 +904,7 @@ void Engine::statistics(const double* residuals, int m, const std::vector<int>& 
     d_guard_.ensure(2 + npairs + ncomp + guard_cap_);
     d_lr_vals_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col);
     d_lr_vecs_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col * n);
-    d_lr_status_.ensure(guard_cap_);
+    d_lr_status_.ensure(2 * static_cast<size_t>(guard_cap_));
     d_legacy_ws_.ensure(legacy_eigen_workspace_doubles(n, kLegacyCtas));
   }
   if (opt.ci_method == FKPC_DCC_PERM || opt.ci_method == FKPC_HSIC_PERM) {

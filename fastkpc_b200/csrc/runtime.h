@@ -153,6 +153,9 @@ class Engine {
   double h2d_bytes_ = 0.0, d2h_bytes_ = 0.0;
   double stage_flops_[9] = {};
   bool collected_ = false;
+  bool graph_timed_ = false;
+  double lowrank_steps_mean_ = 0.0;
+  int lowrank_steps_max_ = 0, lowrank_slots_ = 0;
   void account_flops(const std::vector<FitResult>& sres, const std::vector<FitResult>& mres);
 };
 

@@ -96,6 +96,11 @@ typedef struct fkpc_stage_stats {
   double fit_evaluations;   /* GCV objective evaluations over all fits */
   double fit_flops;         /* algorithmic FP64 flops of the fit stage */
   double statistic_flops;   /* algorithmic FP64 flops of the statistic stage */
+  double fit_iterations;    /* optimizer iterations over all fits */
+  int lowrank_components;   /* guarded components given a low-rank eigen-solve */
+  int lowrank_steps_max;    /* most Lanczos steps any of them took */
+  double lowrank_steps_mean;
+  double device_ms;         /* device time of the batch's launch sequence */
 } fkpc_stage_stats;
 
 typedef struct fkpc_trace_row {

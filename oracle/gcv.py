@@ -31,6 +31,10 @@ import numpy as np
 EPS = np.finfo(np.float64).eps
 RANK_TOL = math.sqrt(EPS)  # 1.4901161193847656e-8
 CONV_TOL = 1e-7
+POLISH_STEPS = 4
+POLISH_MAX_STEP = 1e-6
+POLISH_DONE = 1e-10
+POLISH_CURVATURE = 1e-6
 
 
 class Prepared:
@@ -63,9 +67,10 @@ class Prepared:
         off = self.offsets[0]
         b = self.blocks[0]
         S[off:off + b.shape[0], off:off + b.shape[0]] = b
-        G = self.X.T @ self.X
-        Uc = np.linalg.cholesky(G).T  # G = Uc' Uc
-        Ui = np.linalg.solve(Uc, np.eye(q))
+        # whitening by the R factor of X (X'X = R'R) keeps the condition of X
+        # (the reference whitens with the Cholesky factor of X'X: the same
+        # spectrum, with the condition number squared)
+        Ui = np.linalg.solve(self.R, np.eye(q))
         W = Ui.T @ S @ Ui
         W = 0.5 * (W + W.T)
         vals, vecs = np.linalg.eigh(W)
@@ -208,6 +213,18 @@ def optimize_single(prep, resp):
         log_sp = trial_ls
         cur = trial
         min_score = trial["score"]
+    # terminal Newton polish to the stationary point (see polish_newton)
+    for _ in range(POLISH_STEPS):
+        if not (cur["valid"] and cur["hessian"] > POLISH_CURVATURE * cur["score"]):
+            break
+        step = -cur["gradient"] / cur["hessian"]
+        if abs(step) > POLISH_MAX_STEP:
+            break
+        log_sp = log_sp + step
+        cur = single_objective(log_sp, e, z, yy, n)
+        calls += 1
+        if abs(step) <= POLISH_DONE:
+            break
     return {"log_sp": np.array([log_sp]), "score": cur["score"], "rss": cur["rss"],
             "edf": cur["edf"], "iterations": it, "calls": calls}
 
@@ -354,8 +371,43 @@ def optimize_multi(prep, resp, max_half=25):
             log_sp = trial_ls
             cur = trial
             min_score = cur["score"]
+    log_sp, cur, extra = polish_newton(prep, resp, log_sp, cur)
+    calls += extra
     return {"log_sp": log_sp, "score": cur["score"], "rss": cur["rss"],
             "edf": cur["edf"], "iterations": it, "calls": calls}
+
+
+def polish_newton(prep, resp, log_sp, cur):
+    """Terminal Newton polish of the selected point.
+
+    Magic's stopping rule leaves the selected rho determined only to about the
+    convergence tolerance, so two correct implementations can stop 1e-7 apart.
+    Up to POLISH_STEPS Newton steps on the coordinates whose curvature exceeds
+    POLISH_CURVATURE * V (smooths pushed to the boundary have none and stay
+    put) move the point to the stationary point itself; a step larger than
+    POLISH_MAX_STEP, or a sub-Hessian that is not positive definite, leaves the
+    point as selected.  Returns (rho, core, evaluations)."""
+    extra = 0
+    for _ in range(POLISH_STEPS):
+        g, H = multi_derivatives(prep, cur)
+        act = [j for j in range(prep.m) if H[j, j] > POLISH_CURVATURE * cur["score"]]
+        if not act:
+            break
+        Ha = H[np.ix_(act, act)]
+        try:
+            L = np.linalg.cholesky(Ha)
+        except np.linalg.LinAlgError:
+            break
+        d = -np.linalg.solve(L.T, np.linalg.solve(L, g[act]))
+        if np.max(np.abs(d)) > POLISH_MAX_STEP:
+            break
+        log_sp = log_sp.copy()
+        log_sp[act] += d
+        cur = multi_core(prep, resp, log_sp)
+        extra += 1
+        if np.max(np.abs(d)) <= POLISH_DONE:
+            break
+    return log_sp, cur, extra
 
 
 def residual_at(prep, resp, log_sp):

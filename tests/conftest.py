@@ -1,7 +1,12 @@
 import os
 import sys
 
-import pytest
+# one BLAS thread per process: the oracle's dense eigen-solves run fastest
+# single-threaded here, and parallel test processes must not oversubscribe
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+os.environ.setdefault("OMP_NUM_THREADS", "1")
+
+import pytest  # noqa: E402
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:

@@ -148,7 +148,7 @@ def test_hsic_level_batch_matches_oracle(lib):
 
 
 def test_skeleton_500x50_matches_reference_fixture(lib, dev500, dev500_trace):
-    out = fk.fastkpc_compatible_cuda_skeleton(dev500["data"], 0.1, options={"trace_level": "logical"})
+    out = fk.fastkpc_compatible_cuda_skeleton(dev500["data"], 0.1, options={"trace_level": "logical", "numCol": 35})
     assert out["n_edgetests"] == dev500["n_edgetests"].tolist()
     assert np.array_equal(out["adjacency"].astype(np.int8), dev500["adjacency"])
     tasks = out["tasks"]

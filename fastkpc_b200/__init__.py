@@ -114,6 +114,8 @@ _SIGNATURES = {
     "fkpc_batch_collect": (ctypes.c_int, [ctypes.c_int, _P(CiRecord), _P(StageStats)]),
     "fkpc_batch_time_stage": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _DBL, _DBL]),
     "fkpc_measure_fp64_peak": (ctypes.c_int, [ctypes.c_int, _DBL]),
+    "fkpc_dcov_gamma_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                               ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
     "fkpc_design_export": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, ctypes.c_int, _INT, _INT, _DBL,
                                           _DBL, _DBL]),
 }

@@ -36,6 +36,14 @@ namespace {
 
 thread_local std::string g_last_error;
 
+}  // namespace
+
+namespace fkpc {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace fkpc
+
+namespace {
+
 std::mutex g_engine_mu;
 std::map<int, std::unique_ptr<fkpc::Engine>> g_engines;
 

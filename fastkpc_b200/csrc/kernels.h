@@ -2,9 +2,14 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "device.h"
 
 namespace fkpc {
+
+// Message for fkpc_last_error() on the calling thread.
+void set_last_error(const std::string& msg);
 
 size_t multi_smem_bytes(int qmax_class);
 // Raise the dynamic shared-memory limits (call outside graph capture).

@@ -256,6 +256,26 @@ FKPC_API int fkpc_design_export(const double* data_colmajor, int n, int p,
                                 double* X, double* penalties,
                                 double* initial_log_sp);
 
+/*
+ * Exact-screen dcc.gamma records for ``count`` pairs without allocating any
+ * device memory, for callers that cannot call cudaMalloc -- code running
+ * inside a host framework that owns every device allocation, or that must
+ * not allocate once running.  No counterpart in the reference.
+ * residuals: device pointer, n x m column-major binary64; pairs: device
+ * pointer to 2*count ints (left, right per pair); out: device pointer to
+ * count records (p_value = p_exact = the exact-screen p; no guard-band
+ * refinement); stream: a cudaStream_t or NULL.  Scratch lives in one fixed
+ * 8 MiB device array inside the library: n <= 4096 and
+ * n*m + 2.5*m + 2*count + 1 <= 2^20 doubles, otherwise the call fails with
+ * FKPC_STATUS_INVALID_ARGUMENT.  The first call on a device looks the array's
+ * address up (make it before any stream capture).  Calls share the array:
+ * calls that overlap on the GPU race.  Synchronises ``stream`` before
+ * returning.
+ */
+FKPC_API int fkpc_dcov_gamma_noalloc(const double* residuals, int n, int m,
+                                     const int* pairs, int count,
+                                     fkpc_ci_record* out, void* stream);
+
 FKPC_API const char* fkpc_last_error(void);
 FKPC_API int fkpc_abi_version(void);
 FKPC_API void fkpc_default_options(fkpc_options* options);

@@ -2,6 +2,12 @@
 #pragma once
 #include <cstdint>
 
+#if defined(__CUDACC__)
+#define FKPC_HD __host__ __device__
+#else
+#define FKPC_HD
+#endif
+
 namespace fkpc {
 
 constexpr int kMaxPenalties = 8;      // |S| <= 8 in the shared-memory multi-penalty kernel
@@ -14,6 +20,16 @@ constexpr int kStatusInvalid = 1;
 constexpr unsigned int FKPC_FLAG_GUARDED_DEV = 1u;  // matches FKPC_FLAG_GUARDED
 constexpr unsigned int FKPC_FLAG_DIRECT_DEV = 2u;   // matches FKPC_FLAG_DIRECT
 
+// Warp-per-fit class of additive designs: q <= kWarpQ coefficients, at most
+// kWarpR stacked penalty rows and kWarpM penalties.
+constexpr int kWarpQ = 40;
+constexpr int kWarpR = 32;
+constexpr int kWarpM = 4;
+constexpr int kWarpTri = kWarpQ * (kWarpQ + 1) / 2;
+
+// Row-packed upper triangle of width kWarpQ: row t holds columns t..kWarpQ-1.
+FKPC_HD constexpr int packed_row(int t, int c) { return t * (2 * kWarpQ - t + 1) / 2 + (c - t); }
+
 // One conditioning set's geometry, resident in a device arena of doubles.
 struct DesignDev {
   int kind;        // 1: single penalty (spectral), 2: several penalties (augmented QR)
@@ -24,6 +40,7 @@ struct DesignDev {
   int64_t rmat;    // kind 2: R (q x q column-major, upper triangular)
   int64_t spec;    // kind 1: hat eigenvalues e (q)
   int64_t roots;   // kind 2: penalty roots, block j dim_j x rank_j column-major, consecutive
+  int64_t rpack;   // kind 2 with q <= kWarpQ: R row-packed (kWarpTri doubles, zero beyond q), else -1
   int off[kMaxPenalties];
   int dim[kMaxPenalties];
   int rank[kMaxPenalties];

@@ -360,114 +360,49 @@ __device__ void multi_core(const DesignDev& des, const double* __restrict__ aren
     }
   }
   __syncthreads();
-  if (RMAX <= 32) {
-    // Register-resident fold: thread j keeps column j of the stacked roots in
-    // registers for all q steps; step k only publishes column k (thread k)
-    // to shared memory, where the others read it as broadcasts.
-    double breg[RMAX <= 32 ? RMAX : 1];
+  for (int k = 0; k < q; ++k) {
+    // reflector for column k: warp 0 reduces |B[0..nz, k]|^2
+    const int nz = sc->nzrow[k];
+    const double* Bk = B + L::LDB * k;
+    if (tid < 32) {
+      double sg = 0.0;
+      for (int i = tid; i < nz; i += 32) sg += Bk[i] * Bk[i];
+      sg = warp_sum(sg);
+      if (tid == 0) {
+        const double akk = Ra[tri(k, k)];
+        if (sg == 0.0) {
+          sc->beta[0] = 0.0;
+          sc->v0[0] = 0.0;
+        } else {
+          const double nrm = sqrt(akk * akk + sg);
+          const double alpha = akk >= 0.0 ? -nrm : nrm;
+          const double v0 = akk - alpha;
+          sc->beta[0] = 2.0 / (v0 * v0 + sg);
+          sc->v0[0] = v0;
+          Ra[tri(k, k)] = alpha;
+        }
+      }
+    }
+    __syncthreads();
+    const double beta = sc->beta[0];
+    const double v0 = sc->v0[0];
     const int j = tid;
-    double* pub0 = B;               // two publication buffers of RMAX doubles
-    double* pub1 = B + L::LDB;
-    if (j < q) {
-#pragma unroll
-      for (int i = 0; i < (RMAX <= 32 ? RMAX : 1); ++i) breg[i] = B[i + L::LDB * j];
+    if (beta != 0.0 && j > k && j < q) {
+      double* Bj = B + L::LDB * j;
+      double w0 = v0 * Ra[tri(k, j)], w1 = 0.0, w2 = 0.0, w3 = 0.0;
+      int i = 0;
+      for (; i + 3 < nz; i += 4) {
+        w0 += Bk[i] * Bj[i];
+        w1 += Bk[i + 1] * Bj[i + 1];
+        w2 += Bk[i + 2] * Bj[i + 2];
+        w3 += Bk[i + 3] * Bj[i + 3];
+      }
+      for (; i < nz; ++i) w0 += Bk[i] * Bj[i];
+      const double w = beta * ((w0 + w1) + (w2 + w3));
+      Ra[tri(k, j)] -= w * v0;
+      for (int r = 0; r < nz; ++r) Bj[r] -= w * Bk[r];
     }
     __syncthreads();
-    auto publish = [&](int k, double* pub) {
-      // thread k: copy its column out and form the reflector
-      const int nz = sc->nzrow[k];
-      double sg0 = 0.0, sg1 = 0.0;
-#pragma unroll
-      for (int i = 0; i < (RMAX <= 32 ? RMAX : 1); i += 2) {
-        if (i < nz) { pub[i] = breg[i]; sg0 += breg[i] * breg[i]; }
-        if (i + 1 < nz) { pub[i + 1] = breg[i + 1]; sg1 += breg[i + 1] * breg[i + 1]; }
-      }
-      const double sg = sg0 + sg1;
-      const double akk = Ra[tri(k, k)];
-      const int slot = k & 1;
-      if (sg == 0.0) {
-        sc->beta[slot] = 0.0;
-        sc->v0[slot] = 0.0;
-      } else {
-        const double nrm = sqrt(akk * akk + sg);
-        const double alpha = akk >= 0.0 ? -nrm : nrm;
-        const double v0 = akk - alpha;
-        sc->beta[slot] = 2.0 / (v0 * v0 + sg);
-        sc->v0[slot] = v0;
-        Ra[tri(k, k)] = alpha;
-      }
-    };
-    if (j == 0) publish(0, pub0);
-    __syncthreads();
-    for (int k = 0; k < q; ++k) {
-      const int slot = k & 1;
-      const double* Bk = slot ? pub1 : pub0;
-      const double beta = sc->beta[slot];
-      const double v0 = sc->v0[slot];
-      const int nz = sc->nzrow[k];
-      if (j > k && j < q) {
-        if (beta != 0.0) {
-          double w0 = v0 * Ra[tri(k, j)], w1 = 0.0;
-#pragma unroll
-          for (int i = 0; i < (RMAX <= 32 ? RMAX : 1); i += 2) {
-            if (i < nz) w0 += Bk[i] * breg[i];
-            if (i + 1 < nz) w1 += Bk[i + 1] * breg[i + 1];
-          }
-          const double w = beta * (w0 + w1);
-          Ra[tri(k, j)] -= w * v0;
-#pragma unroll
-          for (int i = 0; i < (RMAX <= 32 ? RMAX : 1); ++i)
-            if (i < nz) breg[i] -= w * Bk[i];
-        }
-        if (j == k + 1) publish(k + 1, slot ? pub0 : pub1);
-      }
-      __syncthreads();
-    }
-  } else {
-    for (int k = 0; k < q; ++k) {
-      // reflector for column k: warp 0 reduces |B[0..nz, k]|^2
-      const int nz = sc->nzrow[k];
-      const double* Bk = B + L::LDB * k;
-      if (tid < 32) {
-        double sg = 0.0;
-        for (int i = tid; i < nz; i += 32) sg += Bk[i] * Bk[i];
-        sg = warp_sum(sg);
-        if (tid == 0) {
-          const double akk = Ra[tri(k, k)];
-          if (sg == 0.0) {
-            sc->beta[0] = 0.0;
-            sc->v0[0] = 0.0;
-          } else {
-            const double nrm = sqrt(akk * akk + sg);
-            const double alpha = akk >= 0.0 ? -nrm : nrm;
-            const double v0 = akk - alpha;
-            sc->beta[0] = 2.0 / (v0 * v0 + sg);
-            sc->v0[0] = v0;
-            Ra[tri(k, k)] = alpha;
-          }
-        }
-      }
-      __syncthreads();
-      const double beta = sc->beta[0];
-      const double v0 = sc->v0[0];
-      const int j = tid;
-      if (beta != 0.0 && j > k && j < q) {
-        double* Bj = B + L::LDB * j;
-        double w0 = v0 * Ra[tri(k, j)], w1 = 0.0, w2 = 0.0, w3 = 0.0;
-        int i = 0;
-        for (; i + 3 < nz; i += 4) {
-          w0 += Bk[i] * Bj[i];
-          w1 += Bk[i + 1] * Bj[i + 1];
-          w2 += Bk[i + 2] * Bj[i + 2];
-          w3 += Bk[i + 3] * Bj[i + 3];
-        }
-        for (; i < nz; ++i) w0 += Bk[i] * Bj[i];
-        const double w = beta * ((w0 + w1) + (w2 + w3));
-        Ra[tri(k, j)] -= w * v0;
-        for (int r = 0; r < nz; ++r) Bj[r] -= w * Bk[r];
-      }
-      __syncthreads();
-    }
   }
   // reciprocal diagonal once, so the triangular solves below multiply
   if (tid < q) {
@@ -663,7 +598,8 @@ __device__ void multi_derivatives(const DesignDev& des, const double* __restrict
 }
 
 // Newton step from the Hessian eigen-decomposition (cyclic Jacobi, m <= 8).
-__device__ void newton_from_hessian_eigen(int m, MultiScalars* sc, bool* steepest) {
+template <class S>
+__device__ void newton_from_hessian_eigen(int m, S* sc, bool* steepest) {
   double* a = sc->ja;
   double* v = sc->jv;
   for (int j = 0; j < m; ++j)
@@ -738,7 +674,8 @@ __device__ void newton_from_hessian_eigen(int m, MultiScalars* sc, bool* steepes
 // Cholesky fails the eigen-decomposition decides, as in the reference: any
 // negative eigenvalue selects steepest descent.  The step is capped at 5 in
 // max norm and the steepest-descent direction is -g / max|g|.
-__device__ void newton_from_hessian(int m, MultiScalars* sc, bool* steepest) {
+template <class S>
+__device__ void newton_from_hessian(int m, S* sc, bool* steepest) {
   double* Lm = sc->ja;
   for (int c = 0; c < m; ++c)
     for (int r = 0; r < m; ++r) Lm[r + kMaxPenalties * c] = sc->hess_c[r + kMaxPenalties * c];
@@ -787,7 +724,8 @@ __device__ void newton_from_hessian(int m, MultiScalars* sc, bool* steepest) {
 // curvature exceeds kPolishCurvature * V, by Cholesky of that sub-Hessian.
 // Returns 0 to stop (no active coordinate, indefinite, or step too large),
 // 1 when the step was applied, 2 when it was applied and was negligible.
-__device__ int polish_step(int m, MultiScalars* sc) {
+template <class S>
+__device__ int polish_step(int m, S* sc) {
   int act[kMaxPenalties];
   int na = 0;
   for (int j = 0; j < m; ++j)
@@ -829,7 +767,7 @@ __device__ int polish_step(int m, MultiScalars* sc) {
 }  // namespace
 
 template <int QMAX, int RMAX>
-__global__ void __launch_bounds__(kMultiThreads, QMAX <= 40 ? 4 : 1) fit_multi_kernel(
+__global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
     const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data,
     int n, const FitJob* __restrict__ jobs, const int* __restrict__ job_index, int job_count,
     double* __restrict__ residuals, FitResult* __restrict__ results) {
@@ -1029,14 +967,709 @@ __global__ void __launch_bounds__(kMultiThreads, QMAX <= 40 ? 4 : 1) fit_multi_k
   }
 }
 
+// ------------------------------------------------------ multi, warp per fit
+//
+// fit_multi_warp_kernel: one warp per target for the additive designs of the
+// warp class (q <= kWarpQ, rsum <= kWarpR, m <= kWarpM: |S| = 3 and 4 with
+// k = 10 margins).  The evaluation and the Newton loop are those of
+// fit_multi_kernel, laid out so that no step of the sequential Householder
+// fold waits on a block barrier and many fits share an SM:
+//  - fold: lane j keeps column j of the stacked roots in registers (columns
+//    32..39 in a second register slot of lanes 0..7 until the first q - 32
+//    pivots are done, then moved into the first slot); the pivot lane
+//    publishes its column and reflector through shared memory and every lane
+//    updates its own column, rows < nzrow(k) only;
+//  - W = R Ra^-1 (lane = row of W) and T = Ra^-T root (lane = column of T)
+//    are forward substitutions with the right-hand side in registers and the
+//    rows of Ra read as shared-memory broadcasts;
+//  - C = T'T and D = (WT)'(WT): lane a accumulates row a of both over the
+//    coefficient index, reading rows of T and WT as broadcasts, then forms
+//    the four block sums the Hessian needs per pair of penalty blocks; a
+//    final pass sums them over the lanes of each block.
+namespace {
+
+constexpr int kWarpPart = 19;  // per-lane partial sums (odd stride)
+constexpr int kWarpSums = 4 * kWarpM * kWarpM + 2 * kWarpM;
+
+struct WarpLayout {
+  static constexpr int X = 0;                    // Ra (packed rows) | WT (row-major) | per-lane partials
+  static constexpr int XSZ = kWarpQ * kWarpR;    // >= kWarpTri, >= 32 * kWarpPart
+  static constexpr int Y = X + XSZ;              // W (packed rows) | T (row-major)
+  static constexpr int Y0 = Y + XSZ;
+  static constexpr int G = Y0 + kWarpQ;
+  static constexpr int WG = G + kWarpQ;
+  static constexpr int E1 = WG + kWarpQ;
+  static constexpr int IDG = E1 + kWarpQ;
+  static constexpr int AV = IDG + kWarpQ;
+  static constexpr int BV = AV + kWarpR;
+  static constexpr int PV = BV + kWarpR;         // pivot column of the fold
+  static constexpr int TOTAL = PV + kWarpR;
+};
+static_assert(WarpLayout::XSZ >= kWarpTri && WarpLayout::XSZ >= 32 * kWarpPart, "warp layout");
+static_assert(kWarpR == 32 && kWarpQ > 32 && kWarpQ <= 64 && kWarpQ % 4 == 0, "warp class shape");
+
+struct WarpScalars {
+  double beta, v0, score, rss, edf, yy;
+  double lam[kMaxPenalties];
+  double log_sp[kMaxPenalties];
+  double trial[kMaxPenalties];
+  double step[kMaxPenalties];
+  double grad_c[kMaxPenalties];
+  double gradient[kMaxPenalties];
+  double newton[kMaxPenalties];
+  double steep[kMaxPenalties];
+  double ddelta[kMaxPenalties];
+  double drss[kMaxPenalties];
+  double hess_c[kMaxPenalties * kMaxPenalties];
+  double hsum[kWarpSums];
+  double ja[kMaxPenalties * kMaxPenalties];
+  double jv[kMaxPenalties * kMaxPenalties];
+  int status;
+  int ctl;
+  int nzrow[kWarpQ];
+  int rowblk[kWarpR];  // penalty block of each stacked root row (-1 beyond rsum)
+};
+
+// Per-CTA state of the warp kernel (one warp per CTA).  File scope, so that
+// the out-of-line evaluation and derivative routines address it directly.
+__shared__ __align__(16) double s_wsm[WarpLayout::TOTAL];
+__shared__ WarpScalars s_wsc;
+__shared__ DesignDev s_wdes;
+
+// Column ``col`` of the stacked roots scaled by sqrt(lambda) (rows 0..kWarpR-1).
+__device__ __forceinline__ void warp_root_column(const DesignDev& des, const double* __restrict__ arena,
+                                                 const WarpScalars& sc, int col, int jb, double (&b)[kWarpR]) {
+  int ro = 0, rk = 0, dim = 1, a = 0;
+  double s = 0.0;
+  const double* root = arena + des.roots;
+  if (jb >= 0) {
+    ro = des.rowoff[jb];
+    rk = des.rank[jb];
+    dim = des.dim[jb];
+    a = col - des.off[jb];
+    s = sqrt(sc.lam[jb]);
+    root += des.rootoff[jb];
+  }
+#pragma unroll
+  for (int r = 0; r < kWarpR; ++r) b[r] = (r >= ro && r < ro + rk) ? s * root[a + dim * (r - ro)] : 0.0;
+}
+
+// Apply the step-k reflector (pv, v0, beta) to this lane's column ``col``.
+__device__ __forceinline__ void warp_fold_update(int k, int q, int nz, double beta, double v0, double* X,
+                                                 const double* pv, double (&b)[kWarpR], int col) {
+  if (col > k && col < q) {
+    const double2* p2 = reinterpret_cast<const double2*>(pv);
+    const int at = packed_row(k, col);
+    double w0 = v0 * X[at], w1 = 0.0, w2 = 0.0, w3 = 0.0;
+#pragma unroll
+    for (int h = 0; h < kWarpR / 8; ++h) {
+      if (8 * h < nz) {
+#pragma unroll
+        for (int u = 0; u < 8; u += 4) {
+          const int r = 8 * h + u;
+          const double2 pa = p2[r / 2], pb = p2[r / 2 + 1];
+          w0 += pa.x * b[r];
+          w1 += pa.y * b[r + 1];
+          w2 += pb.x * b[r + 2];
+          w3 += pb.y * b[r + 3];
+        }
+      }
+    }
+    const double w = beta * ((w0 + w1) + (w2 + w3));
+    X[at] -= w * v0;
+#pragma unroll
+    for (int h = 0; h < kWarpR / 8; ++h) {
+      if (8 * h < nz) {
+#pragma unroll
+        for (int u = 0; u < 8; u += 2) {
+          const int r = 8 * h + u;
+          const double2 pa = p2[r / 2];
+          b[r] -= w * pa.x;
+          b[r + 1] -= w * pa.y;
+        }
+      }
+    }
+  }
+}
+
+// Step k of the fold.  The pivot column k sits in slot 0 of lane k & 31; its
+// rows >= nzrow(k) are exactly zero, so only the 8-row chunks below nz count.
+template <bool TWO>
+__device__ __forceinline__ void warp_fold_step(int k, int q, WarpScalars& sc, double* X, double* pv,
+                                               double (&b0)[kWarpR], double (&b1)[kWarpR], int col0, int col1) {
+  const int lane = threadIdx.x;
+  const int nz = sc.nzrow[k];
+  if (lane == (k & 31)) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    double2* p2 = reinterpret_cast<double2*>(pv);
+#pragma unroll
+    for (int h = 0; h < kWarpR / 8; ++h) {
+      if (8 * h < nz) {
+#pragma unroll
+        for (int u = 0; u < 8; u += 4) {
+          const int r = 8 * h + u;
+          s0 += b0[r] * b0[r];
+          s1 += b0[r + 1] * b0[r + 1];
+          s2 += b0[r + 2] * b0[r + 2];
+          s3 += b0[r + 3] * b0[r + 3];
+          p2[r / 2] = make_double2(b0[r], b0[r + 1]);
+          p2[r / 2 + 1] = make_double2(b0[r + 2], b0[r + 3]);
+        }
+      }
+    }
+    const double sg = (s0 + s1) + (s2 + s3);
+    const int kk = packed_row(k, k);
+    const double akk = X[kk];
+    double beta = 0.0, v0 = 0.0;
+    if (sg != 0.0) {
+      const double nrm = sqrt(akk * akk + sg);
+      const double alpha = akk >= 0.0 ? -nrm : nrm;
+      v0 = akk - alpha;
+      beta = 2.0 / (v0 * v0 + sg);
+      X[kk] = alpha;
+    }
+    sc.beta = beta;
+    sc.v0 = v0;
+  }
+  __syncwarp();
+  const double beta = sc.beta;
+  const double v0 = sc.v0;
+  if (beta != 0.0) {
+    warp_fold_update(k, q, nz, beta, v0, X, pv, b0, col0);
+    if (TWO) warp_fold_update(k, q, nz, beta, v0, X, pv, b1, col1);
+  }
+  __syncwarp();
+}
+
+// Objective at sc.trial.  Leaves Ra in X, W in Y (both row-packed, zero
+// beyond q), idg, g, Wg and score / rss / edf in sc.
+__device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, int jb0, int jb1) {
+  using L = WarpLayout;
+  const DesignDev& des = s_wdes;
+  WarpScalars& sc = s_wsc;
+  double* sm = s_wsm;
+  const int lane = threadIdx.x;
+  const int q = des.q;
+  double* X = sm + L::X;
+  double* Y = sm + L::Y;
+  double* pv = sm + L::PV;
+  double* idg = sm + L::IDG;
+  if (lane < des.m) sc.lam[lane] = exp(sc.trial[lane]);
+  {
+    const double* rpack = arena + des.rpack;
+    for (int idx = lane; idx < kWarpTri; idx += 32) X[idx] = rpack[idx];
+  }
+  __syncwarp();
+  {
+    double b0[kWarpR], b1[kWarpR];
+    warp_root_column(des, arena, sc, lane, jb0, b0);
+    if (q > 32) warp_root_column(des, arena, sc, lane + 32, jb1, b1);
+    int col0 = lane;
+    const int qa = q - 32;
+    for (int k = 0; k < qa; ++k) warp_fold_step<true>(k, q, sc, X, pv, b0, b1, col0, lane + 32);
+    if (lane < qa) {
+#pragma unroll
+      for (int r = 0; r < kWarpR; ++r) b0[r] = b1[r];
+      col0 = lane + 32;
+    }
+    for (int k = qa > 0 ? qa : 0; k < q; ++k) warp_fold_step<false>(k, q, sc, X, pv, b0, b1, col0, 0);
+  }
+  for (int c = lane; c < q; c += 32) {
+    const double d = X[packed_row(c, c)];
+    if (d == 0.0) sc.status = kStatusRank;
+    idg[c] = 1.0 / d;
+  }
+  __syncwarp();
+  // W = R Ra^-1: row i (lane i; rows >= 32 on lanes 0..7) solves w Ra = R(i, :)
+  const double* R = arena + des.rmat;
+  double acc[kWarpQ];
+#pragma unroll
+  for (int c = 0; c < kWarpQ; ++c) acc[c] = (c >= lane && c < q) ? R[lane + q * c] : 0.0;
+  double e = 0.0;
+#pragma unroll
+  for (int t = 0; t < kWarpQ; ++t) {
+    if (t < q) {
+      const double w = acc[t] * idg[t];
+      acc[t] = w;
+      e += w * w;
+#pragma unroll
+      for (int c = t + 1; c < kWarpQ; ++c) acc[c] -= w * X[packed_row(t, c)];
+    }
+  }
+  constexpr int Q2 = kWarpQ - 32;
+  double acc2[Q2];
+  const int i2 = lane + 32;
+#pragma unroll
+  for (int u = 0; u < Q2; ++u) acc2[u] = (i2 < q && 32 + u >= i2 && 32 + u < q) ? R[i2 + q * (32 + u)] : 0.0;
+  if (q > 32) {
+#pragma unroll
+    for (int t = 32; t < kWarpQ; ++t) {
+      if (t < q) {
+        const double w = acc2[t - 32] * idg[t];
+        acc2[t - 32] = w;
+        e += w * w;
+#pragma unroll
+        for (int c = t + 1; c < kWarpQ; ++c) acc2[c - 32] -= w * X[packed_row(t, c)];
+      }
+    }
+  }
+  {
+    const int base = packed_row(lane, lane) - lane;
+#pragma unroll
+    for (int c = 0; c < kWarpQ; ++c)
+      if (c >= lane) Y[base + c] = acc[c];
+    if (lane < Q2) {
+      const int base2 = packed_row(i2, i2) - i2;
+#pragma unroll
+      for (int u = 0; u < Q2; ++u)
+        if (32 + u >= i2) Y[base2 + 32 + u] = acc2[u];
+    }
+  }
+  const double edf = warp_sum(e);
+  __syncwarp();
+  const double* y0 = sm + L::Y0;
+  double* g = sm + L::G;
+  double* wg = sm + L::WG;
+  for (int c = lane; c < q; c += 32) {
+    double s = 0.0;
+    for (int i = 0; i <= c; ++i) s += Y[packed_row(i, c)] * y0[i];
+    g[c] = s;
+  }
+  __syncwarp();
+  double gg = 0.0;
+  {
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < kWarpQ; ++c)
+      if (c < q) s += acc[c] * g[c];
+    if (lane < q) {
+      wg[lane] = s;
+      gg = g[lane] * g[lane] * -2.0 + s * s;
+    }
+    if (i2 < q) {
+      double s2 = 0.0;
+#pragma unroll
+      for (int u = 0; u < Q2; ++u)
+        if (32 + u < q) s2 += acc2[u] * g[32 + u];
+      wg[i2] = s2;
+      gg += g[i2] * g[i2] * -2.0 + s2 * s2;
+    }
+  }
+  const double part = warp_sum(gg);
+  if (lane == 0) {
+    double rss = sc.yy + part;
+    if (rss < 0.0) rss = 0.0;
+    const double delta = static_cast<double>(n) - edf;
+    sc.rss = rss;
+    sc.edf = edf;
+    if (!(isfinite(rss) && isfinite(edf)) || delta <= 1e-8) {
+      sc.score = INFINITY;
+      if (sc.status == kStatusOk) sc.status = kStatusNumeric;
+    } else {
+      sc.score = static_cast<double>(n) * rss / (delta * delta);
+    }
+  }
+  __syncwarp();
+}
+
+// C = T'T and D = (WT)'(WT) for the 16 columns b = B0..B0+15: row a (this
+// lane) accumulated over the coefficient index, then folded into the block
+// sums p[bj] = {sum C.D, sum D a_b, sum C a_b, sum C b_b} over b in block bj.
+template <int B0>
+__device__ __forceinline__ void warp_block_sums(int q, const double* X, const double* Y, const double* av,
+                                                const double* bv, const WarpScalars& sc, double (&p)[kWarpM][4]) {
+  const int lane = threadIdx.x;
+  double c[16], d[16];
+#pragma unroll
+  for (int u = 0; u < 16; ++u) c[u] = d[u] = 0.0;
+  for (int i = 0; i < q; ++i) {
+    const double ta = Y[kWarpR * i + lane];
+    const double wa = X[kWarpR * i + lane];
+    const double2* trow = reinterpret_cast<const double2*>(Y + kWarpR * i + B0);
+    const double2* wrow = reinterpret_cast<const double2*>(X + kWarpR * i + B0);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const double2 x = trow[u], y = wrow[u];
+      c[2 * u] += ta * x.x;
+      c[2 * u + 1] += ta * x.y;
+      d[2 * u] += wa * y.x;
+      d[2 * u + 1] += wa * y.y;
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    const int b = B0 + u;
+    const int jb = sc.rowblk[b];
+    const double avb = av[b], bvb = bv[b];
+    const double cd = c[u] * d[u], da = d[u] * avb, ca = c[u] * avb, cb = c[u] * bvb;
+#pragma unroll
+    for (int bj = 0; bj < kWarpM; ++bj)
+      if (jb == bj) {
+        p[bj][0] += cd;
+        p[bj][1] += da;
+        p[bj][2] += ca;
+        p[bj][3] += cb;
+      }
+  }
+}
+
+// Gradient and Hessian of V at the point of the last warp_core call (the
+// quantities of multi_derivatives).  jrow: penalty block of stacked row ``lane``.
+__device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, int n, int jrow) {
+  using L = WarpLayout;
+  const DesignDev& des = s_wdes;
+  WarpScalars& sc = s_wsc;
+  double* sm = s_wsm;
+  const int lane = threadIdx.x;
+  const int q = des.q, m = des.m;
+  double* X = sm + L::X;
+  double* Y = sm + L::Y;
+  const double* g = sm + L::G;
+  const double* wg = sm + L::WG;
+  double* e1 = sm + L::E1;
+  const double* idg = sm + L::IDG;
+  double* av = sm + L::AV;
+  double* bv = sm + L::BV;
+  // e1 = g - W'(W g)
+  for (int c = lane; c < q; c += 32) {
+    double s = 0.0;
+    for (int i = 0; i <= c; ++i) s += Y[packed_row(i, c)] * wg[i];
+    e1[c] = g[c] - s;
+  }
+  // T(:, a) = Ra^-T root(:, a), lane a
+  double tc[kWarpQ];
+  {
+    int off = 0, dim = 1, cc = 0;
+    const double* root = arena + des.roots;
+    if (jrow >= 0) {
+      off = des.off[jrow];
+      dim = des.dim[jrow];
+      cc = lane - des.rowoff[jrow];
+      root += des.rootoff[jrow];
+    }
+#pragma unroll
+    for (int i = 0; i < kWarpQ; ++i)
+      tc[i] = (jrow >= 0 && i >= off && i < off + dim) ? root[(i - off) + dim * cc] : 0.0;
+  }
+#pragma unroll
+  for (int t = 0; t < kWarpQ; ++t) {
+    if (t < q) {
+      const double w = tc[t] * idg[t];
+      tc[t] = w;
+#pragma unroll
+      for (int i = t + 1; i < kWarpQ; ++i) tc[i] -= w * X[packed_row(t, i)];
+    }
+  }
+  __syncwarp();  // e1 written; every read of Ra done: X takes WT
+  double sa = 0.0, sb = 0.0;
+#pragma unroll
+  for (int i = 0; i < kWarpQ; ++i)
+    if (i < q) {
+      sa += tc[i] * g[i];
+      sb += tc[i] * e1[i];
+    }
+  // WT(:, a) = W T(:, a), in two halves of rows, stored row-major in X
+  double dd = 0.0;
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    constexpr int H = kWarpQ / 2;
+    double wt[H];
+#pragma unroll
+    for (int ii = 0; ii < H; ++ii) {
+      const int i = half * H + ii;
+      double s = 0.0;
+#pragma unroll
+      for (int t = i; t < kWarpQ; ++t) s += Y[packed_row(i, t)] * tc[t];
+      wt[ii] = s;
+      dd += s * s;
+    }
+#pragma unroll
+    for (int ii = 0; ii < H; ++ii) X[kWarpR * (half * H + ii) + lane] = wt[ii];
+  }
+  __syncwarp();  // every read of W done: Y takes T
+#pragma unroll
+  for (int i = 0; i < kWarpQ; ++i) Y[kWarpR * i + lane] = tc[i];
+  av[lane] = sa;
+  bv[lane] = sb;
+  __syncwarp();
+  double p[kWarpM][4];
+#pragma unroll
+  for (int bj = 0; bj < kWarpM; ++bj) p[bj][0] = p[bj][1] = p[bj][2] = p[bj][3] = 0.0;
+  warp_block_sums<0>(q, X, Y, av, bv, sc, p);
+  warp_block_sums<16>(q, X, Y, av, bv, sc, p);
+  __syncwarp();  // T / WT reads done: X takes the per-lane partial sums
+  {
+    double* part = X + kWarpPart * lane;
+#pragma unroll
+    for (int bj = 0; bj < kWarpM; ++bj) {
+      part[4 * bj + 0] = p[bj][0];
+      part[4 * bj + 1] = p[bj][1] * sa;  // a_j' D_ji a_i
+      part[4 * bj + 2] = p[bj][2] * sb;  // b_i' C_ij a_j
+      part[4 * bj + 3] = p[bj][3] * sa;  // b_j' C_ji a_i
+    }
+    part[4 * kWarpM] = dd;
+    part[4 * kWarpM + 1] = sb * sa;
+  }
+  __syncwarp();
+  for (int o = lane; o < kWarpSums; o += 32) {
+    int bi, slot;
+    if (o < 4 * kWarpM * kWarpM) {
+      bi = o / (4 * kWarpM);
+      slot = o % (4 * kWarpM);
+      if (slot / 4 >= m) bi = kWarpM;
+    } else {
+      bi = (o - 4 * kWarpM * kWarpM) / 2;
+      slot = 4 * kWarpM + (o - 4 * kWarpM * kWarpM) % 2;
+    }
+    double s = 0.0;
+    if (bi < m)
+      for (int a = des.rowoff[bi]; a < des.rowoff[bi] + des.rank[bi]; ++a) s += X[kWarpPart * a + slot];
+    sc.hsum[o] = s;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const double nd = static_cast<double>(n);
+    const double delta = nd - sc.edf;
+    const double s1 = nd / (delta * delta);
+    const double s2 = 2.0 * s1 * sc.rss / delta;
+    for (int j = 0; j < m; ++j) {
+      sc.ddelta[j] = sc.lam[j] * sc.hsum[4 * kWarpM * kWarpM + 2 * j];
+      sc.drss[j] = 2.0 * sc.lam[j] * sc.hsum[4 * kWarpM * kWarpM + 2 * j + 1];
+    }
+    for (int bi = 0; bi < m; ++bi)
+      for (int bj = 0; bj <= bi; ++bj) {
+        const double* hs = sc.hsum + 4 * kWarpM * bi + 4 * bj;
+        const double ll = sc.lam[bi] * sc.lam[bj];
+        double d2delta = -2.0 * ll * hs[0];
+        double d2rss = 2.0 * ll * (hs[1] - hs[2] - hs[3]);
+        if (bi == bj) {
+          d2delta += sc.ddelta[bi];
+          d2rss += sc.drss[bi];
+        }
+        const double h = -2.0 * s1 / delta * (sc.ddelta[bj] * sc.drss[bi] + sc.ddelta[bi] * sc.drss[bj]) +
+                         s1 * d2rss + 3.0 * s2 / delta * sc.ddelta[bi] * sc.ddelta[bj] - s2 * d2delta;
+        sc.hess_c[bi + kMaxPenalties * bj] = h;
+        sc.hess_c[bj + kMaxPenalties * bi] = h;
+      }
+    for (int j = 0; j < m; ++j) sc.grad_c[j] = s1 * sc.drss[j] - s2 * sc.ddelta[j];
+  }
+  __syncwarp();
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __restrict__ designs,
+                                                            const double* __restrict__ arena,
+                                                            const double* __restrict__ data, int n,
+                                                            const FitJob* __restrict__ jobs,
+                                                            const int* __restrict__ job_index, int job_count,
+                                                            double* __restrict__ residuals,
+                                                            FitResult* __restrict__ results) {
+  using L = WarpLayout;
+  double* sm = s_wsm;
+  WarpScalars& sc = s_wsc;
+  const DesignDev& des = s_wdes;
+  if (blockIdx.x >= job_count) return;
+  const int lane = threadIdx.x;
+  const int t = job_index[blockIdx.x];
+  const FitJob job = jobs[t];
+  {
+    const int* src = reinterpret_cast<const int*>(designs + job.design);
+    int* dst = reinterpret_cast<int*>(&s_wdes);
+    for (int i = lane; i < static_cast<int>(sizeof(DesignDev) / sizeof(int)); i += 32) dst[i] = src[i];
+  }
+  if (lane == 0) sc.status = kStatusOk;
+  __syncwarp();
+  const int q = des.q, m = des.m;
+  int jb0 = -1, jb1 = -1, jrow = -1;
+  for (int j = 0; j < m; ++j) {
+    if (lane < q && lane >= des.off[j] && lane < des.off[j] + des.dim[j]) jb0 = j;
+    if (lane + 32 < q && lane + 32 >= des.off[j] && lane + 32 < des.off[j] + des.dim[j]) jb1 = j;
+    if (lane >= des.rowoff[j] && lane < des.rowoff[j] + des.rank[j]) jrow = j;
+  }
+  sc.rowblk[lane] = jrow;
+  for (int c = lane; c < kWarpQ; c += 32) {
+    int nz = 0;
+    for (int j = 0; j < m; ++j)
+      if (des.off[j] <= c) nz = des.rowoff[j] + des.rank[j];
+    sc.nzrow[c] = nz;
+  }
+  const double* y = data + static_cast<int64_t>(n) * job.column;
+  const double* Q = arena + des.basis;
+  double* y0 = sm + L::Y0;
+  for (int c0 = 0; c0 < q; c0 += 4) {
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = lane; i < n; i += 32) {
+      const double yi = y[i];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (c0 + u < q) s[u] += Q[i + static_cast<int64_t>(n) * (c0 + u)] * yi;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double v = warp_sum(s[u]);
+      if (lane == 0 && c0 + u < q) y0[c0 + u] = v;
+    }
+  }
+  {
+    double yy = 0.0;
+    for (int i = lane; i < n; i += 32) yy += y[i] * y[i];
+    yy = warp_sum(yy);
+    if (lane == 0) sc.yy = yy;
+  }
+  if (lane < m) {
+    sc.log_sp[lane] = des.log_sp0[lane];
+    sc.trial[lane] = des.log_sp0[lane];
+  }
+  __syncwarp();
+  warp_core(arena, n, jb0, jb1);
+  warp_derivatives(arena, n, jrow);
+  double min_score = sc.score;
+  double score_red = 1e10;
+  bool steepest = false;
+  bool converged = false;
+  int calls = 1;
+  int it = 0;
+  const int max_half = 25;
+  if (lane < m) {
+    sc.gradient[lane] = 0.0;
+    sc.newton[lane] = 0.0;
+    sc.steep[lane] = 0.0;
+  }
+  __syncwarp();
+  for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
+    int tries = 0;
+    if (it > 1) {
+      if (lane < m) sc.step[lane] = steepest ? sc.steep[lane] : sc.newton[lane];
+      __syncwarp();
+      bool trying = true;
+      while (trying) {
+        ++tries;
+        if (tries == 4 && !steepest) {
+          steepest = true;
+          if (lane < m) sc.step[lane] = sc.steep[lane];
+        }
+        __syncwarp();
+        if (lane < m) sc.trial[lane] = sc.log_sp[lane] + sc.step[lane];
+        __syncwarp();
+        warp_core(arena, n, jb0, jb1);
+        ++calls;
+        if (sc.status != kStatusOk) break;
+        const double tscore = sc.score;
+        if (tscore < min_score) {
+          trying = false;
+          score_red = min_score - tscore;
+          min_score = tscore;
+          if (lane < m) sc.log_sp[lane] = sc.trial[lane];
+          __syncwarp();
+          warp_derivatives(arena, n, jrow);
+        } else {
+          if (lane < m) sc.step[lane] *= 0.5;
+        }
+        if (tries == max_half - 1 && trying)
+          if (lane < m) sc.step[lane] = 0.0;
+        if (tries == max_half) trying = false;
+        __syncwarp();
+      }
+      if (sc.status != kStatusOk) break;
+    }
+    if (it > 3) {
+      double g2 = 0.0;
+      for (int r = 0; r < m; ++r) g2 += sc.gradient[r] * sc.gradient[r];
+      converged = score_red <= kConvTol * (1.0 + min_score) &&
+                  sqrt(g2) <= pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(min_score));
+      if (tries == max_half) converged = true;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      for (int r = 0; r < m; ++r) sc.gradient[r] = sc.grad_c[r];
+      bool st = false;
+      newton_from_hessian(m, &sc, &st);
+      sc.ctl = st ? 1 : 0;
+    }
+    __syncwarp();
+    steepest = sc.ctl != 0;
+    if (converged) break;
+  }
+  if (sc.status == kStatusOk && !converged) {
+    __syncwarp();
+    if (lane == 0) sc.status = kStatusNotConverged;
+    __syncwarp();
+  }
+  if (sc.status == kStatusOk) {
+    for (int c = 0; c < m; ++c) {
+      const double direction = sc.gradient[c] < 0.0 ? 1.0 : -1.0;
+      for (int probe = 0; probe < 5; ++probe) {
+        if (lane < m) sc.trial[lane] = sc.log_sp[lane] + (lane == c ? direction * 2.0 : 0.0);
+        __syncwarp();
+        warp_core(arena, n, jb0, jb1);
+        ++calls;
+        if (sc.status != kStatusOk || !(sc.score < min_score)) break;
+        min_score = sc.score;
+        if (lane < m) sc.log_sp[lane] = sc.trial[lane];
+        __syncwarp();
+      }
+      if (sc.status != kStatusOk) break;
+    }
+  }
+  // terminal Newton polish from the selected point
+  if (sc.status == kStatusOk) {
+    __syncwarp();
+    if (lane < m) sc.trial[lane] = sc.log_sp[lane];
+    __syncwarp();
+    warp_core(arena, n, jb0, jb1);
+    for (int ps = 0; ps < kPolishSteps && sc.status == kStatusOk; ++ps) {
+      warp_derivatives(arena, n, jrow);
+      if (lane == 0) sc.ctl = polish_step(m, &sc);
+      __syncwarp();
+      const int act = sc.ctl;
+      __syncwarp();
+      if (act == 0) break;
+      if (lane < m) sc.trial[lane] = sc.log_sp[lane];
+      __syncwarp();
+      warp_core(arena, n, jb0, jb1);
+      ++calls;
+      if (act == 2) break;
+    }
+  }
+  // final fit at the selected point (the last core call may be a rejected probe)
+  if (sc.status == kStatusOk) {
+    __syncwarp();
+    if (lane < m) sc.trial[lane] = sc.log_sp[lane];
+    __syncwarp();
+    warp_core(arena, n, jb0, jb1);
+  }
+  const double* wg = sm + L::WG;
+  double* r = residuals + static_cast<int64_t>(n) * job.out;
+  const bool ok = sc.status == kStatusOk;
+  for (int i = lane; i < n; i += 32) {
+    double f = 0.0;
+    if (ok)
+      for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * wg[c];
+    r[i] = ok ? y[i] - f : NAN;
+  }
+  if (lane == 0) {
+    FitResult res;
+    for (int j = 0; j < kMaxPenalties; ++j) res.log_sp[j] = j < m ? sc.log_sp[j] : NAN;
+    res.score = sc.score;
+    res.edf = sc.edf;
+    res.rss = sc.rss;
+    res.status = sc.status;
+    res.iterations = it;
+    res.evaluations = calls;
+    res.flags = 0;
+    results[t] = res;
+  }
+}
+
 size_t multi_smem_bytes(int qmax_class) {
-  if (qmax_class == 0) return sizeof(double) * MultiLayout<40, 32>::TOTAL;
+  if (qmax_class == 0) return sizeof(double) * WarpLayout::TOTAL + sizeof(WarpScalars) + sizeof(DesignDev);
   return sizeof(double) * MultiLayout<76, 64>::TOTAL;
 }
 
 cudaError_t configure_fit_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(fit_multi_kernel<40, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(multi_smem_bytes(0)));
+  cudaError_t e = cudaFuncSetAttribute(fit_multi_warp_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(fit_multi_kernel<76, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               static_cast<int>(multi_smem_bytes(1)));
@@ -1058,8 +1691,8 @@ cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const dou
   if (count <= 0) return cudaSuccess;
   const size_t smem = multi_smem_bytes(qmax_class);
   if (qmax_class == 0) {
-    auto k = fit_multi_kernel<40, 32>;
-    k<<<count, kMultiThreads, smem, stream>>>(designs, arena, data, n, jobs, job_index, count, residuals, results);
+    fit_multi_warp_kernel<<<count, 32, 0, stream>>>(designs, arena, data, n, jobs, job_index, count, residuals,
+                                                    results);
   } else {
     auto k = fit_multi_kernel<76, 64>;
     k<<<count, kMultiThreads, smem, stream>>>(designs, arena, data, n, jobs, job_index, count, residuals, results);

@@ -218,6 +218,14 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       }
       dd.rsum = rows;
       if (des.q > 76 || rows > 64) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity");
+      dd.rpack = -1;
+      if (des.q <= kWarpQ) {
+        dd.rpack = static_cast<int64_t>(arena.size());
+        const size_t base = arena.size();
+        arena.resize(base + kWarpTri, 0.0);
+        for (int t = 0; t < des.q; ++t)
+          for (int c = t; c < des.q; ++c) arena[base + packed_row(t, c)] = des.R[t + static_cast<size_t>(des.q) * c];
+      }
     }
   }
   single_jobs_.clear();
@@ -250,7 +258,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
     } else {
       const int idx = static_cast<int>(multi_jobs_.size());
       multi_jobs_.push_back(job);
-      if (dd.q <= 40 && dd.rsum <= 32) multi_small_.push_back(idx);
+      if (dd.q <= kWarpQ && dd.rsum <= kWarpR && dd.m <= kWarpM) multi_small_.push_back(idx);
       else multi_large_.push_back(idx);
     }
   }

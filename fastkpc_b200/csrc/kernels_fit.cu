@@ -972,16 +972,18 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
 // fit_multi_warp_kernel: one warp per target for the additive designs of the
 // warp class (q <= kWarpQ, rsum <= kWarpR, m <= kWarpM: |S| = 3 and 4 with
 // k = 10 margins).  The evaluation and the Newton loop are those of
-// fit_multi_kernel, laid out so that no step of the sequential Householder
-// fold waits on a block barrier and many fits share an SM:
+// fit_multi_kernel, laid out so that no step waits on a block barrier, many
+// fits share an SM, and the code the warps run stays small enough for the
+// instruction cache (every phase is a short loop, nothing is unrolled over
+// the coefficient index):
 //  - fold: lane j keeps column j of the stacked roots in registers (columns
 //    32..39 in a second register slot of lanes 0..7 until the first q - 32
 //    pivots are done, then moved into the first slot); the pivot lane
 //    publishes its column and reflector through shared memory and every lane
 //    updates its own column, rows < nzrow(k) only;
 //  - W = R Ra^-1 (lane = row of W) and T = Ra^-T root (lane = column of T)
-//    are forward substitutions with the right-hand side in registers and the
-//    rows of Ra read as shared-memory broadcasts;
+//    are right-looking forward substitutions in shared memory, the rows of
+//    Ra read as broadcasts;
 //  - C = T'T and D = (WT)'(WT): lane a accumulates row a of both over the
 //    coefficient index, reading rows of T and WT as broadcasts, then forms
 //    the four block sums the Hessian needs per pair of penalty blocks; a
@@ -993,9 +995,10 @@ constexpr int kWarpSums = 4 * kWarpM * kWarpM + 2 * kWarpM;
 
 struct WarpLayout {
   static constexpr int X = 0;                    // Ra (packed rows) | WT (row-major) | per-lane partials
-  static constexpr int XSZ = kWarpQ * kWarpR;    // >= kWarpTri, >= 32 * kWarpPart
-  static constexpr int Y = X + XSZ;              // W (packed rows) | T (row-major)
-  static constexpr int Y0 = Y + XSZ;
+  static constexpr int XSZ = kWarpQ * kWarpR;
+  static constexpr int Y = X + XSZ;              // W (packed rows)
+  static constexpr int Z = Y + kWarpTri;         // T (row-major) | block sums, Newton scratch
+  static constexpr int Y0 = Z + XSZ;
   static constexpr int G = Y0 + kWarpQ;
   static constexpr int WG = G + kWarpQ;
   static constexpr int E1 = WG + kWarpQ;
@@ -1006,6 +1009,7 @@ struct WarpLayout {
   static constexpr int TOTAL = PV + kWarpR;
 };
 static_assert(WarpLayout::XSZ >= kWarpTri && WarpLayout::XSZ >= 32 * kWarpPart, "warp layout");
+static_assert(WarpLayout::XSZ >= kWarpSums + 2 * kMaxPenalties * kMaxPenalties, "warp layout");
 static_assert(kWarpR == 32 && kWarpQ > 32 && kWarpQ <= 64 && kWarpQ % 4 == 0, "warp class shape");
 
 struct WarpScalars {
@@ -1021,9 +1025,8 @@ struct WarpScalars {
   double ddelta[kMaxPenalties];
   double drss[kMaxPenalties];
   double hess_c[kMaxPenalties * kMaxPenalties];
-  double hsum[kWarpSums];
-  double ja[kMaxPenalties * kMaxPenalties];
-  double jv[kMaxPenalties * kMaxPenalties];
+  double* ja;  // Newton scratch (Cholesky factor / Jacobi matrix), in the Z region
+  double* jv;  // Jacobi rotations, in the Z region
   int status;
   int ctl;
   int nzrow[kWarpQ];
@@ -1141,8 +1144,27 @@ __device__ __forceinline__ void warp_fold_step(int k, int q, WarpScalars& sc, do
   __syncwarp();
 }
 
-// Objective at sc.trial.  Leaves Ra in X, W in Y (both row-packed, zero
-// beyond q), idg, g, Wg and score / rss / edf in sc.
+// Right-looking forward-substitution step t on a shared-memory row ``v`` of
+// stride ``ld`` (v[ld * c] is entry c): v[t] *= idg[t], then entries c in
+// (t, q) lose v[t] * Ra(t, c).  Returns the finished entry v[t].
+__device__ __forceinline__ double warp_subst_step(double* v, int ld, int t, int q, double idg_t, const double* Ra) {
+  const double w = v[ld * t] * idg_t;
+  v[ld * t] = w;
+  const double* rat = Ra + packed_row(t, 0);  // rat[c] = Ra(t, c) for c >= t
+  int c = t + 1;
+  for (; c + 3 < q; c += 4) {
+    const double r0 = rat[c], r1 = rat[c + 1], r2 = rat[c + 2], r3 = rat[c + 3];
+    v[ld * c] -= w * r0;
+    v[ld * (c + 1)] -= w * r1;
+    v[ld * (c + 2)] -= w * r2;
+    v[ld * (c + 3)] -= w * r3;
+  }
+  for (; c < q; ++c) v[ld * c] -= w * rat[c];
+  return w;
+}
+
+// Objective at sc.trial.  Leaves Ra in X and W in Y (row-packed, valid for
+// columns < q), idg, g, Wg and score / rss / edf in sc.
 __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, int jb0, int jb1) {
   using L = WarpLayout;
   const DesignDev& des = s_wdes;
@@ -1179,50 +1201,18 @@ __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, 
     if (d == 0.0) sc.status = kStatusRank;
     idg[c] = 1.0 / d;
   }
-  __syncwarp();
-  // W = R Ra^-1: row i (lane i; rows >= 32 on lanes 0..7) solves w Ra = R(i, :)
+  // W = R Ra^-1: row i (lane i; rows 32.. on lanes 0..) solves w Ra = R(i, :).
+  // Packed row i starts at Y + packed_row(i, 0), entry c >= i at offset c.
   const double* R = arena + des.rmat;
-  double acc[kWarpQ];
-#pragma unroll
-  for (int c = 0; c < kWarpQ; ++c) acc[c] = (c >= lane && c < q) ? R[lane + q * c] : 0.0;
+  for (int c = 0; c < q; ++c)
+    for (int i = lane; i <= c; i += 32) Y[packed_row(i, 0) + c] = R[i + q * c];
+  __syncwarp();
   double e = 0.0;
-#pragma unroll
-  for (int t = 0; t < kWarpQ; ++t) {
-    if (t < q) {
-      const double w = acc[t] * idg[t];
-      acc[t] = w;
+  for (int t = 0; t < q; ++t) {
+    const double it = idg[t];
+    for (int i = lane; i <= t; i += 32) {
+      const double w = warp_subst_step(Y + packed_row(i, 0), 1, t, q, it, X);
       e += w * w;
-#pragma unroll
-      for (int c = t + 1; c < kWarpQ; ++c) acc[c] -= w * X[packed_row(t, c)];
-    }
-  }
-  constexpr int Q2 = kWarpQ - 32;
-  double acc2[Q2];
-  const int i2 = lane + 32;
-#pragma unroll
-  for (int u = 0; u < Q2; ++u) acc2[u] = (i2 < q && 32 + u >= i2 && 32 + u < q) ? R[i2 + q * (32 + u)] : 0.0;
-  if (q > 32) {
-#pragma unroll
-    for (int t = 32; t < kWarpQ; ++t) {
-      if (t < q) {
-        const double w = acc2[t - 32] * idg[t];
-        acc2[t - 32] = w;
-        e += w * w;
-#pragma unroll
-        for (int c = t + 1; c < kWarpQ; ++c) acc2[c - 32] -= w * X[packed_row(t, c)];
-      }
-    }
-  }
-  {
-    const int base = packed_row(lane, lane) - lane;
-#pragma unroll
-    for (int c = 0; c < kWarpQ; ++c)
-      if (c >= lane) Y[base + c] = acc[c];
-    if (lane < Q2) {
-      const int base2 = packed_row(i2, i2) - i2;
-#pragma unroll
-      for (int u = 0; u < Q2; ++u)
-        if (32 + u >= i2) Y[base2 + 32 + u] = acc2[u];
     }
   }
   const double edf = warp_sum(e);
@@ -1237,23 +1227,12 @@ __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, 
   }
   __syncwarp();
   double gg = 0.0;
-  {
+  for (int i = lane; i < q; i += 32) {
+    const double* wi = Y + packed_row(i, 0);
     double s = 0.0;
-#pragma unroll
-    for (int c = 0; c < kWarpQ; ++c)
-      if (c < q) s += acc[c] * g[c];
-    if (lane < q) {
-      wg[lane] = s;
-      gg = g[lane] * g[lane] * -2.0 + s * s;
-    }
-    if (i2 < q) {
-      double s2 = 0.0;
-#pragma unroll
-      for (int u = 0; u < Q2; ++u)
-        if (32 + u < q) s2 += acc2[u] * g[32 + u];
-      wg[i2] = s2;
-      gg += g[i2] * g[i2] * -2.0 + s2 * s2;
-    }
+    for (int c = i; c < q; ++c) s += wi[c] * g[c];
+    wg[i] = s;
+    gg += g[i] * g[i] * -2.0 + s * s;
   }
   const double part = warp_sum(gg);
   if (lane == 0) {
@@ -1276,17 +1255,17 @@ __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, 
 // lane) accumulated over the coefficient index, then folded into the block
 // sums p[bj] = {sum C.D, sum D a_b, sum C a_b, sum C b_b} over b in block bj.
 template <int B0>
-__device__ __forceinline__ void warp_block_sums(int q, const double* X, const double* Y, const double* av,
+__device__ __forceinline__ void warp_block_sums(int q, const double* WT, const double* T, const double* av,
                                                 const double* bv, const WarpScalars& sc, double (&p)[kWarpM][4]) {
   const int lane = threadIdx.x;
   double c[16], d[16];
 #pragma unroll
   for (int u = 0; u < 16; ++u) c[u] = d[u] = 0.0;
   for (int i = 0; i < q; ++i) {
-    const double ta = Y[kWarpR * i + lane];
-    const double wa = X[kWarpR * i + lane];
-    const double2* trow = reinterpret_cast<const double2*>(Y + kWarpR * i + B0);
-    const double2* wrow = reinterpret_cast<const double2*>(X + kWarpR * i + B0);
+    const double ta = T[kWarpR * i + lane];
+    const double wa = WT[kWarpR * i + lane];
+    const double2* trow = reinterpret_cast<const double2*>(T + kWarpR * i + B0);
+    const double2* wrow = reinterpret_cast<const double2*>(WT + kWarpR * i + B0);
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const double2 x = trow[u], y = wrow[u];
@@ -1323,7 +1302,8 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
   const int lane = threadIdx.x;
   const int q = des.q, m = des.m;
   double* X = sm + L::X;
-  double* Y = sm + L::Y;
+  const double* Y = sm + L::Y;
+  double* Z = sm + L::Z;
   const double* g = sm + L::G;
   const double* wg = sm + L::WG;
   double* e1 = sm + L::E1;
@@ -1336,10 +1316,10 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
     for (int i = 0; i <= c; ++i) s += Y[packed_row(i, c)] * wg[i];
     e1[c] = g[c] - s;
   }
-  // T(:, a) = Ra^-T root(:, a), lane a
-  double tc[kWarpQ];
+  // T(:, a) = Ra^-T root(:, a): lane a, column a of Z (row-major, stride kWarpR)
+  double* ta = Z + lane;
   {
-    int off = 0, dim = 1, cc = 0;
+    int off = 0, dim = 0, cc = 0;
     const double* root = arena + des.roots;
     if (jrow >= 0) {
       off = des.off[jrow];
@@ -1347,56 +1327,38 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
       cc = lane - des.rowoff[jrow];
       root += des.rootoff[jrow];
     }
-#pragma unroll
-    for (int i = 0; i < kWarpQ; ++i)
-      tc[i] = (jrow >= 0 && i >= off && i < off + dim) ? root[(i - off) + dim * cc] : 0.0;
+    for (int i = 0; i < q; ++i) ta[kWarpR * i] = (i >= off && i < off + dim) ? root[(i - off) + dim * cc] : 0.0;
   }
-#pragma unroll
-  for (int t = 0; t < kWarpQ; ++t) {
-    if (t < q) {
-      const double w = tc[t] * idg[t];
-      tc[t] = w;
-#pragma unroll
-      for (int i = t + 1; i < kWarpQ; ++i) tc[i] -= w * X[packed_row(t, i)];
-    }
-  }
+  for (int t = 0; t < q; ++t) warp_subst_step(ta, kWarpR, t, q, idg[t], X);
   __syncwarp();  // e1 written; every read of Ra done: X takes WT
   double sa = 0.0, sb = 0.0;
-#pragma unroll
-  for (int i = 0; i < kWarpQ; ++i)
-    if (i < q) {
-      sa += tc[i] * g[i];
-      sb += tc[i] * e1[i];
-    }
-  // WT(:, a) = W T(:, a), in two halves of rows, stored row-major in X
-  double dd = 0.0;
-#pragma unroll
-  for (int half = 0; half < 2; ++half) {
-    constexpr int H = kWarpQ / 2;
-    double wt[H];
-#pragma unroll
-    for (int ii = 0; ii < H; ++ii) {
-      const int i = half * H + ii;
-      double s = 0.0;
-#pragma unroll
-      for (int t = i; t < kWarpQ; ++t) s += Y[packed_row(i, t)] * tc[t];
-      wt[ii] = s;
-      dd += s * s;
-    }
-#pragma unroll
-    for (int ii = 0; ii < H; ++ii) X[kWarpR * (half * H + ii) + lane] = wt[ii];
+  for (int i = 0; i < q; ++i) {
+    sa += ta[kWarpR * i] * g[i];
+    sb += ta[kWarpR * i] * e1[i];
   }
-  __syncwarp();  // every read of W done: Y takes T
-#pragma unroll
-  for (int i = 0; i < kWarpQ; ++i) Y[kWarpR * i + lane] = tc[i];
+  // WT(:, a) = W T(:, a), row-major in X
+  double dd = 0.0;
+  for (int i = 0; i < q; ++i) {
+    const double* wi = Y + packed_row(i, 0);
+    double s0 = 0.0, s1 = 0.0;
+    int t = i;
+    for (; t + 1 < q; t += 2) {
+      s0 += wi[t] * ta[kWarpR * t];
+      s1 += wi[t + 1] * ta[kWarpR * (t + 1)];
+    }
+    if (t < q) s0 += wi[t] * ta[kWarpR * t];
+    const double s = s0 + s1;
+    X[kWarpR * i + lane] = s;
+    dd += s * s;
+  }
   av[lane] = sa;
   bv[lane] = sb;
   __syncwarp();
   double p[kWarpM][4];
 #pragma unroll
   for (int bj = 0; bj < kWarpM; ++bj) p[bj][0] = p[bj][1] = p[bj][2] = p[bj][3] = 0.0;
-  warp_block_sums<0>(q, X, Y, av, bv, sc, p);
-  warp_block_sums<16>(q, X, Y, av, bv, sc, p);
+  warp_block_sums<0>(q, X, Z, av, bv, sc, p);
+  warp_block_sums<16>(q, X, Z, av, bv, sc, p);
   __syncwarp();  // T / WT reads done: X takes the per-lane partial sums
   {
     double* part = X + kWarpPart * lane;
@@ -1411,6 +1373,7 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
     part[4 * kWarpM + 1] = sb * sa;
   }
   __syncwarp();
+  double* hsum = Z;  // T is no longer needed
   for (int o = lane; o < kWarpSums; o += 32) {
     int bi, slot;
     if (o < 4 * kWarpM * kWarpM) {
@@ -1424,7 +1387,7 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
     double s = 0.0;
     if (bi < m)
       for (int a = des.rowoff[bi]; a < des.rowoff[bi] + des.rank[bi]; ++a) s += X[kWarpPart * a + slot];
-    sc.hsum[o] = s;
+    hsum[o] = s;
   }
   __syncwarp();
   if (lane == 0) {
@@ -1433,12 +1396,12 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
     const double s1 = nd / (delta * delta);
     const double s2 = 2.0 * s1 * sc.rss / delta;
     for (int j = 0; j < m; ++j) {
-      sc.ddelta[j] = sc.lam[j] * sc.hsum[4 * kWarpM * kWarpM + 2 * j];
-      sc.drss[j] = 2.0 * sc.lam[j] * sc.hsum[4 * kWarpM * kWarpM + 2 * j + 1];
+      sc.ddelta[j] = sc.lam[j] * hsum[4 * kWarpM * kWarpM + 2 * j];
+      sc.drss[j] = 2.0 * sc.lam[j] * hsum[4 * kWarpM * kWarpM + 2 * j + 1];
     }
     for (int bi = 0; bi < m; ++bi)
       for (int bj = 0; bj <= bi; ++bj) {
-        const double* hs = sc.hsum + 4 * kWarpM * bi + 4 * bj;
+        const double* hs = hsum + 4 * kWarpM * bi + 4 * bj;
         const double ll = sc.lam[bi] * sc.lam[bj];
         double d2delta = -2.0 * ll * hs[0];
         double d2rss = 2.0 * ll * (hs[1] - hs[2] - hs[3]);
@@ -1478,7 +1441,11 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
     int* dst = reinterpret_cast<int*>(&s_wdes);
     for (int i = lane; i < static_cast<int>(sizeof(DesignDev) / sizeof(int)); i += 32) dst[i] = src[i];
   }
-  if (lane == 0) sc.status = kStatusOk;
+  if (lane == 0) {
+    sc.status = kStatusOk;
+    sc.ja = sm + L::Z + kWarpSums;
+    sc.jv = sc.ja + kMaxPenalties * kMaxPenalties;
+  }
   __syncwarp();
   const int q = des.q, m = des.m;
   int jb0 = -1, jb1 = -1, jrow = -1;

@@ -1011,6 +1011,7 @@ struct WarpLayout {
 static_assert(WarpLayout::XSZ >= kWarpTri && WarpLayout::XSZ >= 32 * kWarpPart, "warp layout");
 static_assert(WarpLayout::XSZ >= kWarpSums + 2 * kMaxPenalties * kMaxPenalties, "warp layout");
 static_assert(kWarpR == 32 && kWarpQ > 32 && kWarpQ <= 64 && kWarpQ % 4 == 0, "warp class shape");
+static_assert(kWarpTri % 2 == 0 && WarpLayout::Y % 2 == 0, "16-byte copies of the packed triangle");
 
 struct WarpScalars {
   double beta, v0, score, rss, edf, yy;
@@ -1038,6 +1039,15 @@ struct WarpScalars {
 __shared__ __align__(16) double s_wsm[WarpLayout::TOTAL];
 __shared__ WarpScalars s_wsc;
 __shared__ DesignDev s_wdes;
+
+// Asynchronous 16-byte global -> shared copies (cp.async, L1-allocating).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Column ``col`` of the stacked roots scaled by sqrt(lambda) (rows 0..kWarpR-1).
 __device__ __forceinline__ void warp_root_column(const DesignDev& des, const double* __restrict__ arena,
@@ -1144,23 +1154,58 @@ __device__ __forceinline__ void warp_fold_step(int k, int q, WarpScalars& sc, do
   __syncwarp();
 }
 
-// Right-looking forward-substitution step t on a shared-memory row ``v`` of
-// stride ``ld`` (v[ld * c] is entry c): v[t] *= idg[t], then entries c in
-// (t, q) lose v[t] * Ra(t, c).  Returns the finished entry v[t].
-__device__ __forceinline__ double warp_subst_step(double* v, int ld, int t, int q, double idg_t, const double* Ra) {
-  const double w = v[ld * t] * idg_t;
-  v[ld * t] = w;
-  const double* rat = Ra + packed_row(t, 0);  // rat[c] = Ra(t, c) for c >= t
-  int c = t + 1;
-  for (; c + 3 < q; c += 4) {
-    const double r0 = rat[c], r1 = rat[c + 1], r2 = rat[c + 2], r3 = rat[c + 3];
-    v[ld * c] -= w * r0;
-    v[ld * (c + 1)] -= w * r1;
-    v[ld * (c + 2)] -= w * r2;
-    v[ld * (c + 3)] -= w * r3;
+// Left-looking forward substitution through Ra' on one shared-memory vector
+// ``v`` of stride ``ld`` (v[ld * c] is entry c, holding the right-hand side):
+// for c = start..q-1, v[c] = (v[c] - sum_{s in [start, c)} v[s] Ra(s, c)) / Ra(c, c).
+// Each entry is one dot product with four chains, so its loads overlap.
+// Returns the sum of squares of the solved entries.
+__device__ __forceinline__ double warp_left_subst(double* __restrict__ v, int ld, int start, int q,
+                                                  const double* __restrict__ Ra, const double* __restrict__ idg) {
+  double ss = 0.0;
+  for (int c = start; c < q; ++c) {
+    double s0 = v[ld * c], s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int t = start;
+    for (; t + 3 < c; t += 4) {
+      s0 -= v[ld * t] * Ra[packed_row(t, c)];
+      s1 -= v[ld * (t + 1)] * Ra[packed_row(t + 1, c)];
+      s2 -= v[ld * (t + 2)] * Ra[packed_row(t + 2, c)];
+      s3 -= v[ld * (t + 3)] * Ra[packed_row(t + 3, c)];
+    }
+    for (; t < c; ++t) s0 -= v[ld * t] * Ra[packed_row(t, c)];
+    const double w = ((s0 + s1) + (s2 + s3)) * idg[c];
+    v[ld * c] = w;
+    ss += w * w;
   }
-  for (; c < q; ++c) v[ld * c] -= w * rat[c];
-  return w;
+  return ss;
+}
+
+// Dot product of a[0..len) (stride 1) with b[0..len) (stride ldb), four chains.
+__device__ __forceinline__ double warp_dot(const double* __restrict__ a, const double* __restrict__ b, int ldb,
+                                           int len) {
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int i = 0;
+  for (; i + 3 < len; i += 4) {
+    s0 += a[i] * b[ldb * i];
+    s1 += a[i + 1] * b[ldb * (i + 1)];
+    s2 += a[i + 2] * b[ldb * (i + 2)];
+    s3 += a[i + 3] * b[ldb * (i + 3)];
+  }
+  for (; i < len; ++i) s0 += a[i] * b[ldb * i];
+  return (s0 + s1) + (s2 + s3);
+}
+
+// sum_{i <= c} W(i, c) v[i] for the row-packed W, four chains.
+__device__ __forceinline__ double warp_column_dot(const double* __restrict__ W, int c, const double* __restrict__ v) {
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int i = 0;
+  for (; i + 3 <= c; i += 4) {
+    s0 += W[packed_row(i, c)] * v[i];
+    s1 += W[packed_row(i + 1, c)] * v[i + 1];
+    s2 += W[packed_row(i + 2, c)] * v[i + 2];
+    s3 += W[packed_row(i + 3, c)] * v[i + 3];
+  }
+  for (; i <= c; ++i) s0 += W[packed_row(i, c)] * v[i];
+  return (s0 + s1) + (s2 + s3);
 }
 
 // Objective at sc.trial.  Leaves Ra in X and W in Y (row-packed, valid for
@@ -1178,8 +1223,15 @@ __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, 
   double* idg = sm + L::IDG;
   if (lane < des.m) sc.lam[lane] = exp(sc.trial[lane]);
   {
+    // R (row-packed) into X, where the fold turns it into Ra, and into Y,
+    // where the W solve starts from it; only the first copy is waited for
+    // before the fold.
     const double* rpack = arena + des.rpack;
-    for (int idx = lane; idx < kWarpTri; idx += 32) X[idx] = rpack[idx];
+    for (int idx = 2 * lane; idx < kWarpTri; idx += 64) cp_async16(X + idx, rpack + idx);
+    cp_async_commit();
+    for (int idx = 2 * lane; idx < kWarpTri; idx += 64) cp_async16(Y + idx, rpack + idx);
+    cp_async_commit();
+    cp_async_wait<1>();
   }
   __syncwarp();
   {
@@ -1203,34 +1255,20 @@ __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, 
   }
   // W = R Ra^-1: row i (lane i; rows 32.. on lanes 0..) solves w Ra = R(i, :).
   // Packed row i starts at Y + packed_row(i, 0), entry c >= i at offset c.
-  const double* R = arena + des.rmat;
-  for (int c = 0; c < q; ++c)
-    for (int i = lane; i <= c; i += 32) Y[packed_row(i, 0) + c] = R[i + q * c];
+  cp_async_wait<0>();
   __syncwarp();
   double e = 0.0;
-  for (int t = 0; t < q; ++t) {
-    const double it = idg[t];
-    for (int i = lane; i <= t; i += 32) {
-      const double w = warp_subst_step(Y + packed_row(i, 0), 1, t, q, it, X);
-      e += w * w;
-    }
-  }
+  for (int i = lane; i < q; i += 32) e += warp_left_subst(Y + packed_row(i, 0), 1, i, q, X, idg);
   const double edf = warp_sum(e);
   __syncwarp();
   const double* y0 = sm + L::Y0;
   double* g = sm + L::G;
   double* wg = sm + L::WG;
-  for (int c = lane; c < q; c += 32) {
-    double s = 0.0;
-    for (int i = 0; i <= c; ++i) s += Y[packed_row(i, c)] * y0[i];
-    g[c] = s;
-  }
+  for (int c = lane; c < q; c += 32) g[c] = warp_column_dot(Y, c, y0);
   __syncwarp();
   double gg = 0.0;
   for (int i = lane; i < q; i += 32) {
-    const double* wi = Y + packed_row(i, 0);
-    double s = 0.0;
-    for (int c = i; c < q; ++c) s += wi[c] * g[c];
+    const double s = warp_dot(Y + packed_row(i, 0) + i, g + i, 1, q - i);
     wg[i] = s;
     gg += g[i] * g[i] * -2.0 + s * s;
   }
@@ -1311,11 +1349,7 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
   double* av = sm + L::AV;
   double* bv = sm + L::BV;
   // e1 = g - W'(W g)
-  for (int c = lane; c < q; c += 32) {
-    double s = 0.0;
-    for (int i = 0; i <= c; ++i) s += Y[packed_row(i, c)] * wg[i];
-    e1[c] = g[c] - s;
-  }
+  for (int c = lane; c < q; c += 32) e1[c] = g[c] - warp_column_dot(Y, c, wg);
   // T(:, a) = Ra^-T root(:, a): lane a, column a of Z (row-major, stride kWarpR)
   double* ta = Z + lane;
   {
@@ -1327,27 +1361,24 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
       cc = lane - des.rowoff[jrow];
       root += des.rootoff[jrow];
     }
-    for (int i = 0; i < q; ++i) ta[kWarpR * i] = (i >= off && i < off + dim) ? root[(i - off) + dim * cc] : 0.0;
+    for (int i = 0; i < q; ++i) ta[kWarpR * i] = 0.0;
+    for (int i0 = 0; i0 < dim; i0 += 16) {
+      double r[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) r[u] = i0 + u < dim ? root[i0 + u + dim * cc] : 0.0;
+#pragma unroll
+      for (int u = 0; u < 16; ++u)
+        if (i0 + u < dim) ta[kWarpR * (off + i0 + u)] = r[u];
+    }
   }
-  for (int t = 0; t < q; ++t) warp_subst_step(ta, kWarpR, t, q, idg[t], X);
+  if (jrow >= 0) warp_left_subst(ta, kWarpR, des.off[jrow], q, X, idg);
   __syncwarp();  // e1 written; every read of Ra done: X takes WT
-  double sa = 0.0, sb = 0.0;
-  for (int i = 0; i < q; ++i) {
-    sa += ta[kWarpR * i] * g[i];
-    sb += ta[kWarpR * i] * e1[i];
-  }
+  const double sa = warp_dot(g, ta, kWarpR, q);
+  const double sb = warp_dot(e1, ta, kWarpR, q);
   // WT(:, a) = W T(:, a), row-major in X
   double dd = 0.0;
   for (int i = 0; i < q; ++i) {
-    const double* wi = Y + packed_row(i, 0);
-    double s0 = 0.0, s1 = 0.0;
-    int t = i;
-    for (; t + 1 < q; t += 2) {
-      s0 += wi[t] * ta[kWarpR * t];
-      s1 += wi[t + 1] * ta[kWarpR * (t + 1)];
-    }
-    if (t < q) s0 += wi[t] * ta[kWarpR * t];
-    const double s = s0 + s1;
+    const double s = warp_dot(Y + packed_row(i, 0) + i, ta + kWarpR * i, kWarpR, q - i);
     X[kWarpR * i + lane] = s;
     dd += s * s;
   }

@@ -220,6 +220,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       if (des.q > 76 || rows > 64) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity");
       dd.rpack = -1;
       if (des.q <= kWarpQ) {
+        if (arena.size() % 2) arena.push_back(0.0);  // 16-byte aligned: copied with 16-byte cp.async
         dd.rpack = static_cast<int64_t>(arena.size());
         const size_t base = arena.size();
         arena.resize(base + kWarpTri, 0.0);

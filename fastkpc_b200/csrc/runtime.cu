@@ -619,7 +619,7 @@ void Engine::account_flops(const std::vector<FitResult>& sres, const std::vector
     const double core = 2.0 * (rs + 1.0) * q * q + 2.0 * q * q * q / 3.0 + 4.0 * q * q;
     const double deriv = 2.0 * q * q * rs + 2.0 * rs * rs * q;
     const double f = 4.0 * n * q + core * mres[i].evaluations + deriv * mres[i].iterations;
-    const bool small = des.q <= 40 && rs <= 32;
+    const bool small = des.q <= kWarpQ && rs <= kWarpR && des.m <= kWarpM;
     stage_flops_[small ? 1 : 2] += f;
   }
   if (stats_enabled_) {

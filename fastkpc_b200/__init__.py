@@ -414,6 +414,31 @@ def measure_fp64_peak(device=0):
     return t.value
 
 
+def gcv_adjoint(data, target, S, log_lambda):
+    """GCV score V, gradient, Gauss-Newton Hessian and exact Hessian in
+    rho = log(lambda) of the additive fit of column ``target`` on S (|S| >= 3)
+    at each row of ``log_lambda`` (count x |S|; entry j belongs to the j-th
+    smallest variable of S).  Returns a dict of arrays (count, count x m,
+    count x m x m, count x m x m)."""
+    X = _as_data(data)
+    n, p = X.shape
+    s = np.array(sorted(S), dtype=np.int32)
+    m = len(s)
+    rho = np.ascontiguousarray(np.atleast_2d(np.asarray(log_lambda, dtype=np.float64)))
+    if rho.shape[1] != m:
+        raise ValueError("log_lambda must have one column per conditioning variable")
+    count = rho.shape[0]
+    score = np.zeros(count)
+    grad = np.zeros((count, m))
+    gn = np.zeros((count, m, m))
+    hess = np.zeros((count, m, m))
+    _check(load_library().fkpc_gcv_adjoint(_ptr(X, ctypes.c_double), n, p, int(target), _ptr(s, ctypes.c_int), m,
+                                             count, _ptr(rho, ctypes.c_double), _ptr(score, ctypes.c_double),
+                                             _ptr(grad, ctypes.c_double), _ptr(gn, ctypes.c_double),
+                                             _ptr(hess, ctypes.c_double)))
+    return {"score": score, "grad": grad, "gn_hessian": gn, "hessian": hess}
+
+
 def design_export(data, S):
     """Host design set-up for S: dict(X, penalties (m x q x q), initial_log_sp)."""
     X = _as_data(data)

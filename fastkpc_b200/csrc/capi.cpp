@@ -554,9 +554,19 @@ int fkpc_design_export(const double* data, int n, int p, const int* s_values, in
   });
 }
 
-int fkpc_gcv_adjoint(const double*, int, int, int, const int*, int, int, const double*, double*, double*, double*,
-                     double*) {
-  return fail(FKPC_STATUS_INVALID_ARGUMENT, "fkpc_gcv_adjoint is not available in this build");
+int fkpc_gcv_adjoint(const double* data, int n, int p, int target, const int* s_values, int s_count, int count,
+                     const double* log_lambda, double* score, double* grad, double* gn_hessian,
+                     double* exact_hessian) {
+  return guarded([&]() {
+    if (!data || !s_values || (count > 0 && !log_lambda) || count < 0 || s_count < 0)
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    if (n <= 5 || p < 2) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "data must be n x p with n > 5, p >= 2");
+    std::lock_guard<std::mutex> lock(g_engine_mu);
+    auto& eng = engine_for(0);
+    eng.load(data, n, p);
+    eng.adjoint(target, std::vector<int>(s_values, s_values + s_count), count, log_lambda, score, grad, gn_hessian,
+                exact_hessian);
+  });
 }
 
 }  // extern "C"

@@ -21,6 +21,12 @@ cudaError_t launch_fit_single(const DesignDev* designs, const double* arena, con
                               cudaStream_t stream);
 
 // qmax_class 0: q <= 40 and rank sum <= 32; 1: q <= 76 and rank sum <= 64.
+// Score, gradient, Gauss-Newton and exact Hessian of GCV in log(lambda) at
+// ``count`` points (rho: count x m) for design ``design`` and response y.
+// qmax_class 0: q <= kWarpQ, rsum <= kWarpR, m <= kWarpM; 1: q <= 76, rsum <= 64.
+cudaError_t launch_gcv_adjoint(int qmax_class, const DesignDev* designs, int design, const double* arena,
+                               const double* y, int n, const double* rho, int count, double* score, double* grad,
+                               double* gn, double* hess, int* status, cudaStream_t stream);
 cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const double* arena, const double* data,
                              int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
                              FitResult* results, cudaStream_t stream);

@@ -304,6 +304,7 @@ struct MultiScalars {
   double step[kMaxPenalties];
   double grad_c[kMaxPenalties];
   double hess_c[kMaxPenalties * kMaxPenalties];
+  double gn_c[kMaxPenalties * kMaxPenalties];  // Gauss-Newton Hessian (adjoint entry point)
   double gradient[kMaxPenalties];
   double newton[kMaxPenalties];
   double steep[kMaxPenalties];
@@ -591,6 +592,11 @@ __device__ void multi_derivatives(const DesignDev& des, const double* __restrict
                        s1 * d2rss + 3.0 * s2 / delta * sc->ddelta[bi] * sc->ddelta[bj] - s2 * d2delta;
       sc->hess_c[bi + kMaxPenalties * bj] = h;
       sc->hess_c[bj + kMaxPenalties * bi] = h;
+      // Gauss-Newton: V = |f|^2, f = sqrt(n) r / delta, dr_i . dr_j = ll a_i' D_ij a_j
+      const double gn = 2.0 * s1 * ll * t1 - s1 / delta * (sc->ddelta[bj] * sc->drss[bi] + sc->ddelta[bi] * sc->drss[bj]) +
+                        s2 / delta * sc->ddelta[bi] * sc->ddelta[bj];
+      sc->gn_c[bi + kMaxPenalties * bj] = gn;
+      sc->gn_c[bj + kMaxPenalties * bi] = gn;
     }
   }
   if (tid < m) sc->grad_c[tid] = s1 * sc->drss[tid] - s2 * sc->ddelta[tid];
@@ -766,22 +772,14 @@ __device__ int polish_step(int m, S* sc) {
 
 }  // namespace
 
+// Per-fit set-up shared by the fit and adjoint kernels: fill-in bounds, block
+// maps, R staged in shared memory, y0 = Q'y and |y|^2.
 template <int QMAX, int RMAX>
-__global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
-    const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data,
-    int n, const FitJob* __restrict__ jobs, const int* __restrict__ job_index, int job_count,
-    double* __restrict__ residuals, FitResult* __restrict__ results) {
+__device__ void multi_fit_setup(const DesignDev& des, const double* __restrict__ arena, const double* __restrict__ y,
+                                int n, double* sm, MultiScalars& sc) {
   using L = MultiLayout<QMAX, RMAX>;
-  extern __shared__ double sm[];
-  __shared__ MultiScalars sc;
-  __shared__ int ctl[4];
-  if (blockIdx.x >= job_count) return;
-  const int t = job_index[blockIdx.x];
-  const FitJob job = jobs[t];
-  const DesignDev& des = designs[job.design];
   const int tid = threadIdx.x;
   const int q = des.q, m = des.m;
-  const double* y = data + static_cast<int64_t>(n) * job.column;
   const double* Q = arena + des.basis;
   if (tid == 0) {
     sc.status = kStatusOk;
@@ -823,6 +821,26 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
     yy = block_sum(yy, &sc);
     if (tid == 0) sc.yy = yy;
   }
+}
+
+template <int QMAX, int RMAX>
+__global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
+    const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data,
+    int n, const FitJob* __restrict__ jobs, const int* __restrict__ job_index, int job_count,
+    double* __restrict__ residuals, FitResult* __restrict__ results) {
+  using L = MultiLayout<QMAX, RMAX>;
+  extern __shared__ double sm[];
+  __shared__ MultiScalars sc;
+  __shared__ int ctl[4];
+  if (blockIdx.x >= job_count) return;
+  const int t = job_index[blockIdx.x];
+  const FitJob job = jobs[t];
+  const DesignDev& des = designs[job.design];
+  const int tid = threadIdx.x;
+  const int q = des.q, m = des.m;
+  const double* y = data + static_cast<int64_t>(n) * job.column;
+  const double* Q = arena + des.basis;
+  multi_fit_setup<QMAX, RMAX>(des, arena, y, n, sm, sc);
   if (tid < m) {
     sc.log_sp[tid] = des.log_sp0[tid];
     sc.trial[tid] = des.log_sp0[tid];
@@ -1026,6 +1044,7 @@ struct WarpScalars {
   double ddelta[kMaxPenalties];
   double drss[kMaxPenalties];
   double hess_c[kMaxPenalties * kMaxPenalties];
+  double gn_c[kMaxPenalties * kMaxPenalties];  // Gauss-Newton Hessian (adjoint entry point)
   double* ja;  // Newton scratch (Cholesky factor / Jacobi matrix), in the Z region
   double* jv;  // Jacobi rotations, in the Z region
   int status;
@@ -1444,6 +1463,12 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
                          s1 * d2rss + 3.0 * s2 / delta * sc.ddelta[bi] * sc.ddelta[bj] - s2 * d2delta;
         sc.hess_c[bi + kMaxPenalties * bj] = h;
         sc.hess_c[bj + kMaxPenalties * bi] = h;
+        // Gauss-Newton: V = |f|^2, f = sqrt(n) r / delta, dr_i . dr_j = ll a_i' D_ij a_j
+        const double gn = 2.0 * s1 * ll * hs[1] -
+                          s1 / delta * (sc.ddelta[bj] * sc.drss[bi] + sc.ddelta[bi] * sc.drss[bj]) +
+                          s2 / delta * sc.ddelta[bi] * sc.ddelta[bj];
+        sc.gn_c[bi + kMaxPenalties * bj] = gn;
+        sc.gn_c[bj + kMaxPenalties * bi] = gn;
       }
     for (int j = 0; j < m; ++j) sc.grad_c[j] = s1 * sc.drss[j] - s2 * sc.ddelta[j];
   }
@@ -1452,23 +1477,19 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
 
 }  // namespace
 
-__global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __restrict__ designs,
-                                                            const double* __restrict__ arena,
-                                                            const double* __restrict__ data, int n,
-                                                            const FitJob* __restrict__ jobs,
-                                                            const int* __restrict__ job_index, int job_count,
-                                                            double* __restrict__ residuals,
-                                                            FitResult* __restrict__ results) {
+// Per-fit set-up shared by the fit and adjoint kernels: the design
+// descriptor into shared memory, fill-in bounds and block maps, y0 = Q'y and
+// |y|^2.  Returns the penalty blocks of this lane's columns and stacked row.
+__device__ __noinline__ void warp_fit_setup(const DesignDev* __restrict__ design, const double* __restrict__ arena,
+                                            const double* __restrict__ y, int n, int* jb0_out, int* jb1_out,
+                                            int* jrow_out) {
   using L = WarpLayout;
   double* sm = s_wsm;
   WarpScalars& sc = s_wsc;
   const DesignDev& des = s_wdes;
-  if (blockIdx.x >= job_count) return;
   const int lane = threadIdx.x;
-  const int t = job_index[blockIdx.x];
-  const FitJob job = jobs[t];
   {
-    const int* src = reinterpret_cast<const int*>(designs + job.design);
+    const int* src = reinterpret_cast<const int*>(design);
     int* dst = reinterpret_cast<int*>(&s_wdes);
     for (int i = lane; i < static_cast<int>(sizeof(DesignDev) / sizeof(int)); i += 32) dst[i] = src[i];
   }
@@ -1492,7 +1513,6 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
       if (des.off[j] <= c) nz = des.rowoff[j] + des.rank[j];
     sc.nzrow[c] = nz;
   }
-  const double* y = data + static_cast<int64_t>(n) * job.column;
   const double* Q = arena + des.basis;
   double* y0 = sm + L::Y0;
   for (int c0 = 0; c0 < q; c0 += 4) {
@@ -1515,6 +1535,31 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
     yy = warp_sum(yy);
     if (lane == 0) sc.yy = yy;
   }
+  *jb0_out = jb0;
+  *jb1_out = jb1;
+  *jrow_out = jrow;
+}
+
+__global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __restrict__ designs,
+                                                            const double* __restrict__ arena,
+                                                            const double* __restrict__ data, int n,
+                                                            const FitJob* __restrict__ jobs,
+                                                            const int* __restrict__ job_index, int job_count,
+                                                            double* __restrict__ residuals,
+                                                            FitResult* __restrict__ results) {
+  using L = WarpLayout;
+  double* sm = s_wsm;
+  WarpScalars& sc = s_wsc;
+  const DesignDev& des = s_wdes;
+  if (blockIdx.x >= job_count) return;
+  const int lane = threadIdx.x;
+  const int t = job_index[blockIdx.x];
+  const FitJob job = jobs[t];
+  int jb0 = -1, jb1 = -1, jrow = -1;
+  warp_fit_setup(designs + job.design, arena, data + static_cast<int64_t>(n) * job.column, n, &jb0, &jb1, &jrow);
+  const int q = des.q, m = des.m;
+  const double* y = data + static_cast<int64_t>(n) * job.column;
+  const double* Q = arena + des.basis;
   if (lane < m) {
     sc.log_sp[lane] = des.log_sp0[lane];
     sc.trial[lane] = des.log_sp0[lane];
@@ -1660,6 +1705,82 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
   }
 }
 
+// ------------------------------------------------------ GCV adjoint
+//
+// Score V, gradient, exact Hessian and Gauss-Newton Hessian of V in
+// rho = log(lambda) at caller-given points (one warp or one CTA per point),
+// for one additive design and one response column.  The same evaluation and
+// derivative routines as the fit kernels; no optimiser.  Outputs per point:
+// score[pt], grad[pt*m + j], gn / hess[(pt*m + i)*m + j], status[pt].
+
+__global__ void __launch_bounds__(32) gcv_adjoint_warp_kernel(const DesignDev* __restrict__ designs, int design,
+                                                              const double* __restrict__ arena,
+                                                              const double* __restrict__ y, int n,
+                                                              const double* __restrict__ rho, int count,
+                                                              double* __restrict__ score, double* __restrict__ grad,
+                                                              double* __restrict__ gn, double* __restrict__ hess,
+                                                              int* __restrict__ status) {
+  WarpScalars& sc = s_wsc;
+  const DesignDev& des = s_wdes;
+  const int pt = blockIdx.x;
+  if (pt >= count) return;
+  const int lane = threadIdx.x;
+  int jb0 = -1, jb1 = -1, jrow = -1;
+  warp_fit_setup(designs + design, arena, y, n, &jb0, &jb1, &jrow);
+  const int m = des.m;
+  if (lane < m) {
+    sc.trial[lane] = rho[static_cast<int64_t>(pt) * m + lane];
+    sc.log_sp[lane] = sc.trial[lane];
+  }
+  __syncwarp();
+  warp_core(arena, n, jb0, jb1);
+  if (sc.status == kStatusOk) warp_derivatives(arena, n, jrow);
+  if (lane == 0) {
+    score[pt] = sc.score;
+    status[pt] = sc.status;
+    for (int i = 0; i < m; ++i) {
+      grad[static_cast<int64_t>(pt) * m + i] = sc.grad_c[i];
+      for (int j = 0; j < m; ++j) {
+        gn[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.gn_c[i + kMaxPenalties * j];
+        hess[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.hess_c[i + kMaxPenalties * j];
+      }
+    }
+  }
+}
+
+template <int QMAX, int RMAX>
+__global__ void __launch_bounds__(kMultiThreads, 1) gcv_adjoint_kernel(
+    const DesignDev* __restrict__ designs, int design, const double* __restrict__ arena, const double* __restrict__ y,
+    int n, const double* __restrict__ rho, int count, double* __restrict__ score, double* __restrict__ grad,
+    double* __restrict__ gn, double* __restrict__ hess, int* __restrict__ status) {
+  extern __shared__ double sm[];
+  __shared__ MultiScalars sc;
+  const int pt = blockIdx.x;
+  if (pt >= count) return;
+  const DesignDev& des = designs[design];
+  const int tid = threadIdx.x;
+  const int m = des.m;
+  multi_fit_setup<QMAX, RMAX>(des, arena, y, n, sm, sc);
+  if (tid < m) {
+    sc.trial[tid] = rho[static_cast<int64_t>(pt) * m + tid];
+    sc.log_sp[tid] = sc.trial[tid];
+  }
+  __syncthreads();
+  multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+  if (sc.status == kStatusOk) multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
+  if (tid == 0) {
+    score[pt] = sc.score;
+    status[pt] = sc.status;
+    for (int i = 0; i < m; ++i) {
+      grad[static_cast<int64_t>(pt) * m + i] = sc.grad_c[i];
+      for (int j = 0; j < m; ++j) {
+        gn[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.gn_c[i + kMaxPenalties * j];
+        hess[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.hess_c[i + kMaxPenalties * j];
+      }
+    }
+  }
+}
+
 size_t multi_smem_bytes(int qmax_class) {
   if (qmax_class == 0) return sizeof(double) * WarpLayout::TOTAL + sizeof(WarpScalars) + sizeof(DesignDev);
   return sizeof(double) * MultiLayout<76, 64>::TOTAL;
@@ -1669,8 +1790,25 @@ cudaError_t configure_fit_kernels() {
   cudaError_t e = cudaFuncSetAttribute(fit_multi_warp_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(fit_multi_kernel<76, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  e = cudaFuncSetAttribute(fit_multi_kernel<76, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(multi_smem_bytes(1)));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(gcv_adjoint_kernel<76, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               static_cast<int>(multi_smem_bytes(1)));
+}
+
+cudaError_t launch_gcv_adjoint(int qmax_class, const DesignDev* designs, int design, const double* arena,
+                               const double* y, int n, const double* rho, int count, double* score, double* grad,
+                               double* gn, double* hess, int* status, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  if (qmax_class == 0) {
+    gcv_adjoint_warp_kernel<<<count, 32, 0, stream>>>(designs, design, arena, y, n, rho, count, score, grad, gn, hess,
+                                                      status);
+  } else {
+    gcv_adjoint_kernel<76, 64><<<count, kMultiThreads, multi_smem_bytes(1), stream>>>(
+        designs, design, arena, y, n, rho, count, score, grad, gn, hess, status);
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t launch_fit_single(const DesignDev* designs, const double* arena, const double* data, int n,

@@ -865,6 +865,67 @@ void Engine::regress(const std::vector<int>& targets, const std::vector<std::vec
   stats_enabled_ = true;
 }
 
+void Engine::adjoint(int target, const std::vector<int>& S, int count, const double* rho, double* score,
+                     double* grad, double* gn_hessian, double* exact_hessian) {
+  if (S.size() < 3) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "the GCV adjoint covers additive designs (|S| >= 3)");
+  if (target < 0 || target >= p_) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "target column out of range");
+  for (size_t i = 0; i < S.size(); ++i) {
+    if (S[i] < 0 || S[i] >= p_ || S[i] == target) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "invalid conditioning set");
+    for (size_t j = 0; j < i; ++j)
+      if (S[j] == S[i]) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "repeated conditioning variable");
+  }
+  if (count < 0) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "negative point count");
+  Test t;
+  t.x = target;
+  t.y = -1;  // a partner column outside {target} and S; only the target's fit is used
+  for (int c = 0; c < p_ && t.y < 0; ++c)
+    if (c != target && std::find(S.begin(), S.end(), c) == S.end()) t.y = c;
+  if (t.y < 0) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "no column outside the target and S");
+  t.S = S;
+  fkpc_options opt;
+  fkpc_default_options(&opt);
+  opt_ = opt;
+  release_graph();
+  auto t0 = std::chrono::steady_clock::now();
+  plan_components({t});
+  build_designs();
+  setup_ms_ = ms_since(t0);
+  stats_enabled_ = false;
+  pack_and_upload(opt, nullptr);
+  stats_enabled_ = true;
+  cuda_check(configure_fit_kernels(), "kernel attributes");
+  const Design& des = *designs_.at(0);
+  const int m = des.m;
+  int rsum = 0;
+  for (int r : des.ranks) rsum += r;
+  const int qclass = (des.q <= kWarpQ && rsum <= kWarpR && m <= kWarpM) ? 0 : 1;
+  if (count == 0) return;
+  DevBuf<double> d_rho, d_score, d_grad, d_gn, d_hess;
+  DevBuf<int> d_status;
+  const size_t cm = static_cast<size_t>(count) * m, cmm = cm * m;
+  cuda_check(cudaMemcpyAsync(d_rho.ensure(cm), rho, cm * sizeof(double), cudaMemcpyHostToDevice, stream_), "upload");
+  cuda_check(launch_gcv_adjoint(qclass, d_designs_.get(), 0, d_arena_.get(), d_data_.get() + static_cast<size_t>(n_) * target,
+                                n_, d_rho.get(), count, d_score.ensure(count), d_grad.ensure(cm), d_gn.ensure(cmm),
+                                d_hess.ensure(cmm), d_status.ensure(count), stream_),
+             "gcv adjoint");
+  ++launches_;
+  std::vector<int> st(count);
+  cuda_check(cudaMemcpyAsync(st.data(), d_status.get(), count * sizeof(int), cudaMemcpyDeviceToHost, stream_), "download");
+  if (score)
+    cuda_check(cudaMemcpyAsync(score, d_score.get(), count * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
+  if (grad) cuda_check(cudaMemcpyAsync(grad, d_grad.get(), cm * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
+  if (gn_hessian)
+    cuda_check(cudaMemcpyAsync(gn_hessian, d_gn.get(), cmm * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
+  if (exact_hessian)
+    cuda_check(cudaMemcpyAsync(exact_hessian, d_hess.get(), cmm * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+               "download");
+  cuda_check(cudaStreamSynchronize(stream_), "gcv adjoint");
+  for (int k = 0; k < count; ++k)
+    if (st[k] != kStatusOk)
+      throw Error(st[k] == kStatusRank ? FKPC_STATUS_RANK : FKPC_STATUS_NUMERIC,
+                  "GCV evaluation failed at point " + std::to_string(k));
+}
+
 void Engine::statistics(const double* residuals, int m, const std::vector<int>& left, const std::vector<int>& right,
                         const int* permutations, const fkpc_options& opt, fkpc_ci_record* out) {
   const int n = n_;

@@ -90,6 +90,10 @@ class Engine {
   // Statistics only, on caller residual columns.
   void statistics(const double* residuals, int m, const std::vector<int>& left, const std::vector<int>& right,
                   const int* permutations, const fkpc_options& opt, fkpc_ci_record* out);
+  // GCV score, gradient, Gauss-Newton and exact Hessian in log(lambda) of the
+  // additive fit of column ``target`` on S at ``count`` points (rho: count x m).
+  void adjoint(int target, const std::vector<int>& S, int count, const double* rho, double* score, double* grad,
+               double* gn_hessian, double* exact_hessian);
   // Repeated graph launches of the prepared batch, timed with CUDA events.
   double execute_timed(int repeats);
   // One kernel of the prepared batch replayed alone: mean ms per launch.

@@ -73,3 +73,17 @@ def uneven_batch_500x64(seed=4, count=16384):
             if k <= 12:
                 return k
     return X, ci_triples(64, count, seed + 1, size)
+
+
+def adjoint_targets_1000(seed=5, count=2048):
+    """GCV adjoint / Newton selection workload: n=1000, p=50 SEM (edge prob
+    0.08) and ``count`` (target, S) fits with |S| uniform on 3..8 (additive
+    smooths, 3..8 log smoothing parameters, q = 1 + 9|S| up to 73)."""
+    X, _ = nonlinear_sem(1000, 50, 0.08, seed)
+    rs = np.random.default_rng(seed + 1)
+    fits = []
+    for _ in range(count):
+        k = int(rs.integers(3, 9))
+        cols = rs.choice(50, size=k + 1, replace=False)
+        fits.append((int(cols[0]), sorted(int(c) for c in cols[1:])))
+    return X, fits

@@ -199,9 +199,12 @@ FKPC_API int fkpc_stat_batch(const double* residuals, int n, int m, const int* l
 
 /*
  * GCV score, gradient and Gauss-Newton Hessian in rho = log(lambda) of the
- * additive-smooth fit of data[:, target] on S at the given rho (one entry per
- * conditioning variable), plus the exact Hessian for comparison.  Arrays are
- * count-major: log_lambda/grad are count x m, hessians count x m x m.
+ * additive-smooth fit of data[:, target] on S (|S| >= 3, m = |S|) at
+ * ``count`` given points, plus the exact Hessian for comparison, on device 0.
+ * Arrays are count-major: log_lambda and grad are count x m, the Hessians
+ * count x m x m (row-major per point); any output may be NULL.  Entry j
+ * of a point belongs to the j-th smallest variable of S.  The
+ * Gauss-Newton Hessian is 2 J'J of f = sqrt(n) r / (n - EDF), V = |f|^2.
  * Replaces the analytic derivative block of
  * evaluate_multi_penalty_target_device
  * (fastkpc/src/cuda/mgcv_multi_penalty_gcv.cu:1274-1490).

@@ -430,3 +430,43 @@ def gcv_value_grad_hess(prep, y, log_sp):
     core = multi_core(prep, resp, np.asarray(log_sp, dtype=np.float64))
     g, H = multi_derivatives(prep, core)
     return core["score"], g, H
+
+
+def gcv_gauss_newton(prep, y, log_sp):
+    """Gauss-Newton Hessian of V in rho, from the normal equations.
+
+    V = |f|^2 with f(rho) = sqrt(n) r / delta, r = y - X beta(rho),
+    beta = (X'X + S_lambda)^-1 X'y, delta = n - EDF.  GN = 2 J'J with
+    J_j = sqrt(n) (dr_j / delta - r ddelta_j / delta^2),
+    dr_j = lambda_j X (X'X + S_lambda)^-1 S_j beta, and
+    ddelta_j = lambda_j tr((X'X + S)^-1 S_j (X'X + S)^-1 X'X).
+    A restatement independent of the augmented-SVD path (dense solves);
+    the adjoint routine's GN block (no reference counterpart: the reference
+    uses the exact Hessian, fastkpc/src/cuda/mgcv_multi_penalty_gcv.cu:1410-1490)
+    is checked against it and against finite differences of f.
+    """
+    X = prep.X
+    n = prep.n
+    lam = np.exp(np.asarray(log_sp, dtype=np.float64))
+    Ss = [r @ r.T for r in prep.roots]
+    XtX = X.T @ X
+    A = XtX + sum(l * S for l, S in zip(lam, Ss))
+    Ainv = np.linalg.inv(A)
+    beta = Ainv @ (X.T @ y)
+    r = y - X @ beta
+    edf = float(np.trace(Ainv @ XtX))
+    delta = n - edf
+    J = np.zeros((n, prep.m))
+    for j, (l, S) in enumerate(zip(lam, Ss)):
+        dr = l * (X @ (Ainv @ (S @ beta)))
+        dd = l * float(np.trace(Ainv @ S @ Ainv @ XtX))
+        J[:, j] = math.sqrt(n) * (dr / delta - r * dd / (delta * delta))
+    return 2.0 * J.T @ J
+
+
+def gcv_residual_vector(prep, y, log_sp):
+    """f(rho) = sqrt(n) r / (n - EDF), whose squared norm is V (augmented SVD)."""
+    resp = prep.response(y)
+    core = multi_core(prep, resp, np.asarray(log_sp, dtype=np.float64))
+    fitted = prep.Q @ (core["U1"] @ core["y1"])
+    return math.sqrt(prep.n) * (y - fitted) / (prep.n - core["edf"])

@@ -1,0 +1,77 @@
+"""GCV adjoint through the C ABI (fkpc_gcv_adjoint) against the oracle (B200).
+
+Workload: n=1000, p=50 SEM, additive fits with |S| = 3..8 (q = 28..73; the
+warp kernel for q <= 40, the CTA kernel above).  At each point rho:
+- V, the analytic gradient and the exact Hessian against the oracle's
+  augmented-SVD derivatives (oracle.gcv.gcv_value_grad_hess);
+- the Gauss-Newton Hessian against the oracle's dense normal-equation
+  restatement (oracle.gcv.gcv_gauss_newton);
+- the gradient against central differences of the GPU's own V (h = 1e-5 in
+  log lambda), and the Gauss-Newton Hessian against 2 J'J with J the central
+  difference of the oracle's f = sqrt(n) r / (n - EDF).
+Tolerances (relative to the largest entry of the quantity): 1e-10 for V,
+1e-8 analytic vs analytic, 1e-5 against finite differences.
+"""
+import numpy as np
+import pytest
+
+import fastkpc_b200 as fk
+from fastkpc_b200 import workloads
+from oracle import gcv, tprs
+
+pytestmark = pytest.mark.gpu
+
+H = 1e-5
+CASES = [(0, 3), (1, 4), (2, 5), (3, 6), (5, 8)]  # (index into the fit list with that |S|, |S|)
+
+
+@pytest.fixture(scope="module")
+def workload():
+    return workloads.adjoint_targets_1000(count=256)
+
+
+def _pick(fits, k, size):
+    sel = [f for f in fits if len(f[1]) == size]
+    return sel[k % len(sel)]
+
+
+def _points(prep, seed):
+    rs = np.random.default_rng(seed)
+    base = np.asarray(prep.initial_sp, dtype=np.float64)
+    return np.vstack([base, base + rs.uniform(-2.0, 2.0, size=base.size), base + rs.uniform(-1.0, 3.0, size=base.size)])
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(1e-300, np.max(np.abs(b))))
+
+
+@pytest.mark.parametrize("k,size", CASES)
+def test_adjoint_matches_oracle_and_finite_differences(lib_built, workload, k, size):
+    X, fits = workload
+    target, S = _pick(fits, k, size)
+    prep = gcv.Prepared(tprs.design(X, S))
+    y = X[:, target]
+    pts = _points(prep, 100 + size)
+    out = fk.gcv_adjoint(X, target, S, pts)
+    m = len(S)
+    for i, rho in enumerate(pts):
+        V, g, Hx = gcv.gcv_value_grad_hess(prep, y, rho)
+        assert abs(out["score"][i] - V) <= 1e-10 * V, (S, i)
+        assert _rel(out["grad"][i], g) <= 1e-8, (S, i, out["grad"][i], g)
+        assert _rel(out["hessian"][i], Hx) <= 1e-8, (S, i)
+        gn = gcv.gcv_gauss_newton(prep, y, rho)
+        assert _rel(out["gn_hessian"][i], gn) <= 1e-8, (S, i)
+        # finite differences
+        shifts = np.vstack([rho + H * e for e in np.eye(m)] + [rho - H * e for e in np.eye(m)])
+        vs = fk.gcv_adjoint(X, target, S, shifts)["score"]
+        gfd = (vs[:m] - vs[m:]) / (2 * H)
+        assert _rel(out["grad"][i], gfd) <= 1e-5, (S, i, out["grad"][i], gfd)
+        J = np.column_stack([(gcv.gcv_residual_vector(prep, y, rho + H * e)
+                              - gcv.gcv_residual_vector(prep, y, rho - H * e)) / (2 * H) for e in np.eye(m)])
+        assert _rel(out["gn_hessian"][i], 2.0 * J.T @ J) <= 1e-5, (S, i)
+
+
+def test_adjoint_rejects_single_penalty_sets(lib_built, workload):
+    X, _ = workload
+    with pytest.raises(fk.FkpcError, match="additive"):
+        fk.gcv_adjoint(X, 0, [1, 2], np.zeros((1, 2)))

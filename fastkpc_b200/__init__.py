@@ -24,6 +24,7 @@ __all__ = [
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
+SELECTIONS = {"magic": 0, "gn_newton": 1}  # FKPC_SELECT_MAGIC, FKPC_SELECT_GN_NEWTON
 METHODS = {"dcc.gamma": 0, "dcc.perm": 1, "hsic.gamma": 2, "hsic.perm": 3}
 MODES = {"batched": 0, "plain": 1}
 FLAG_GUARDED = 1
@@ -46,7 +47,8 @@ class Options(ctypes.Structure):
                 ("max_conditioning_size", ctypes.c_int), ("ci_method", ctypes.c_int),
                 ("hsic_sig", ctypes.c_double), ("permutation_replicates", ctypes.c_int),
                 ("has_seed", ctypes.c_int), ("seed", ctypes.c_uint), ("mode", ctypes.c_int),
-                ("collect_trace", ctypes.c_int), ("device", ctypes.c_int), ("strict", ctypes.c_int)]
+                ("collect_trace", ctypes.c_int), ("device", ctypes.c_int), ("strict", ctypes.c_int),
+                ("selection", ctypes.c_int)]
 
 
 class CiRecord(ctypes.Structure):
@@ -161,7 +163,8 @@ def _as_data(data):
 
 
 def make_options(ci_method="dcc.gamma", alpha=0.1, index=1.0, numCol=35, max_conditioning_size=math.inf,
-                 hsic_sig=1.0, replicates=100, seed=None, mode="batched", trace=True, device=0, strict=True):
+                 hsic_sig=1.0, replicates=100, seed=None, mode="batched", trace=True, device=0, strict=True,
+                 selection="magic"):
     o = Options()
     load_library().fkpc_default_options(ctypes.byref(o))
     if ci_method not in METHODS:
@@ -179,6 +182,9 @@ def make_options(ci_method="dcc.gamma", alpha=0.1, index=1.0, numCol=35, max_con
     o.collect_trace = 1 if trace else 0
     o.device = int(device)
     o.strict = 1 if strict else 0
+    if selection not in SELECTIONS:
+        raise ValueError(f"unknown selection {selection!r}")
+    o.selection = SELECTIONS[selection]
     return o
 
 
@@ -324,8 +330,11 @@ def ci_plain_one(data, x, y, S, ci_method="dcc.gamma", **kw):
     return {name: getattr(rec, name) for name, _ in CiRecord._fields_}
 
 
-def regress_batch(data, fits, max_penalties=8, device=0):
-    """regrXonS residuals for ``[(target, S), ...]``: (residuals n x k, log_sp k x m, status k)."""
+def regress_batch(data, fits, max_penalties=8, device=0, selection="magic"):
+    """regrXonS residuals for ``[(target, S), ...]``: (residuals n x k, log_sp k x m, status k).
+
+    ``selection``: "magic" (mgcv magic's search, as the reference) or
+    "gn_newton" (Newton on the Gauss-Newton Hessian of GCV) for |S| >= 3."""
     X = _as_data(data)
     n, p = X.shape
     k = len(fits)
@@ -339,7 +348,7 @@ def regress_batch(data, fits, max_penalties=8, device=0):
     resid = np.zeros((n, k), dtype=np.float64, order="F")
     lsp = np.zeros((k, max_penalties), dtype=np.float64)
     status = np.zeros(k, dtype=np.int32)
-    o = make_options(device=device)
+    o = make_options(device=device, selection=selection)
     _check(load_library().fkpc_regress_batch(_ptr(X, ctypes.c_double), n, p, _ptr(tg, ctypes.c_int),
                                                _ptr(offs, ctypes.c_int), _ptr(vals, ctypes.c_int), k,
                                                ctypes.byref(o), _ptr(resid, ctypes.c_double),

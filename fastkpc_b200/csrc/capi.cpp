@@ -94,6 +94,8 @@ void validate_options(const fkpc_options& o, int n, int p) {
   }
   if (o.mode != FKPC_MODE_BATCHED && o.mode != FKPC_MODE_PLAIN)
     throw Error(FKPC_STATUS_INVALID_ARGUMENT, "unknown execution mode");
+  if (o.selection != FKPC_SELECT_MAGIC && o.selection != FKPC_SELECT_GN_NEWTON)
+    throw Error(FKPC_STATUS_INVALID_ARGUMENT, "selection must be FKPC_SELECT_MAGIC or FKPC_SELECT_GN_NEWTON");
   if (p < 2 || n <= 5) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "need n > 5 and p >= 2");
   if (o.strict) {
     // the qualified envelope of fastkpc/src/full_cuda_ci_one_call.cpp:5052-5087
@@ -340,6 +342,7 @@ void fkpc_default_options(fkpc_options* o) {
   o->collect_trace = 1;
   o->device = 0;
   o->strict = 1;
+  o->selection = FKPC_SELECT_MAGIC;
 }
 
 int fkpc_skeleton_run(const double* data, int n, int p, const fkpc_options* options, fkpc_result** out) {
@@ -458,7 +461,9 @@ int fkpc_regress_batch(const double* data, int n, int p, const int* target, cons
     std::vector<int> tg(target, target + count);
     std::vector<std::vector<int>> sets(count);
     for (int t = 0; t < count; ++t) sets[t].assign(s_values + s_offsets[t], s_values + s_offsets[t + 1]);
-    eng.regress(tg, sets, residuals, log_sp, max_penalties, status);
+    if (o.selection != FKPC_SELECT_MAGIC && o.selection != FKPC_SELECT_GN_NEWTON)
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "selection must be FKPC_SELECT_MAGIC or FKPC_SELECT_GN_NEWTON");
+    eng.regress(tg, sets, residuals, log_sp, max_penalties, status, o.selection);
   });
 }
 

@@ -29,7 +29,8 @@ cudaError_t launch_gcv_adjoint(int qmax_class, const DesignDev* designs, int des
                                double* gn, double* hess, int* status, cudaStream_t stream);
 cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const double* arena, const double* data,
                              int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
-                             FitResult* results, cudaStream_t stream);
+                             FitResult* results, cudaStream_t stream,
+                             int selection = 0);
 
 // dCov: per component centring constants and moments, then per pair statistic
 // and gamma p-value.  comp_cols[c] is the residual column of component c.

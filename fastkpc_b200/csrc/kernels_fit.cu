@@ -26,6 +26,7 @@
 
 #include <cmath>
 
+#include "../../include/fastkpc_b200.h"
 #include "device.h"
 #include "kernels.h"
 
@@ -770,6 +771,59 @@ __device__ int polish_step(int m, S* sc) {
   return mx <= kPolishDone ? 2 : 1;
 }
 
+// Gauss-Newton step (one thread): solve (GN + mu I) d = -g by Cholesky, with
+// mu = 0 first and then 1e-12, 1e-10, ... times the largest diagonal entry
+// until the factor exists (GN = 2 J'J is positive semi-definite, singular in
+// the flat directions of V); the step is capped at 5 in max norm as magic's.
+template <class S>
+__device__ void gn_step(int m, S* sc) {
+  double dmax = 0.0;
+  for (int j = 0; j < m; ++j) dmax = fmax(dmax, fabs(sc->gn_c[j + kMaxPenalties * j]));
+  double mu = 0.0;
+  double* Lm = sc->ja;
+  for (int attempt = 0; attempt < 12; ++attempt) {
+    for (int c = 0; c < m; ++c)
+      for (int r = 0; r < m; ++r) Lm[r + kMaxPenalties * c] = sc->gn_c[r + kMaxPenalties * c] + (r == c ? mu : 0.0);
+    bool pd = true;
+    for (int c = 0; c < m && pd; ++c) {
+      double d = Lm[c + kMaxPenalties * c];
+      for (int k = 0; k < c; ++k) d -= Lm[c + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
+      if (!(d > 0.0)) {
+        pd = false;
+        break;
+      }
+      d = sqrt(d);
+      Lm[c + kMaxPenalties * c] = d;
+      for (int r = c + 1; r < m; ++r) {
+        double v = Lm[r + kMaxPenalties * c];
+        for (int k = 0; k < c; ++k) v -= Lm[r + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
+        Lm[r + kMaxPenalties * c] = v / d;
+      }
+    }
+    if (pd) {
+      double z[kMaxPenalties];
+      for (int r = 0; r < m; ++r) {
+        double v = -sc->grad_c[r];
+        for (int k = 0; k < r; ++k) v -= Lm[r + kMaxPenalties * k] * z[k];
+        z[r] = v / Lm[r + kMaxPenalties * r];
+      }
+      double mx = 0.0;
+      for (int r = m - 1; r >= 0; --r) {
+        double v = z[r];
+        for (int k = r + 1; k < m; ++k) v -= Lm[k + kMaxPenalties * r] * z[k];
+        z[r] = v / Lm[r + kMaxPenalties * r];
+        mx = fmax(mx, fabs(z[r]));
+      }
+      for (int r = 0; r < m; ++r) sc->step[r] = mx > 5.0 ? z[r] * (5.0 / mx) : z[r];
+      return;
+    }
+    mu = mu == 0.0 ? 1e-12 * fmax(dmax, 1e-300) : mu * 100.0;
+  }
+  double mg = 0.0;
+  for (int r = 0; r < m; ++r) mg = fmax(mg, fabs(sc->grad_c[r]));
+  for (int r = 0; r < m; ++r) sc->step[r] = mg == 0.0 ? 0.0 : -sc->grad_c[r] / mg;
+}
+
 }  // namespace
 
 // Per-fit set-up shared by the fit and adjoint kernels: fill-in bounds, block
@@ -827,7 +881,7 @@ template <int QMAX, int RMAX>
 __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
     const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data,
     int n, const FitJob* __restrict__ jobs, const int* __restrict__ job_index, int job_count,
-    double* __restrict__ residuals, FitResult* __restrict__ results) {
+    double* __restrict__ residuals, FitResult* __restrict__ results, int selection) {
   using L = MultiLayout<QMAX, RMAX>;
   extern __shared__ double sm[];
   __shared__ MultiScalars sc;
@@ -861,59 +915,101 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
     sc.steep[tid] = 0.0;
   }
   __syncthreads();
-  for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
-    int tries = 0;
-    if (it > 1) {
-      if (tid < m) sc.step[tid] = steepest ? sc.steep[tid] : sc.newton[tid];
+  if (selection == FKPC_SELECT_GN_NEWTON) {
+    // Newton on the Gauss-Newton Hessian, halving until V decreases
+    if (tid < m) sc.gradient[tid] = sc.grad_c[tid];
+    __syncthreads();
+    for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
+      if (tid == 0) gn_step(m, &sc);
       __syncthreads();
-      bool trying = true;
-      while (trying) {
-        ++tries;
-        if (tries == 4 && !steepest) {
-          steepest = true;
-          if (tid < m) sc.step[tid] = sc.steep[tid];
-        }
-        __syncthreads();
+      bool accepted = false;
+      for (int tries = 1; tries <= max_half; ++tries) {
         if (tid < m) sc.trial[tid] = sc.log_sp[tid] + sc.step[tid];
         __syncthreads();
         multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
         ++calls;
         if (sc.status != kStatusOk) break;
-        const double tscore = sc.score;
-        if (tscore < min_score) {
-          trying = false;
-          score_red = min_score - tscore;
-          min_score = tscore;
-          if (tid < m) sc.log_sp[tid] = sc.trial[tid];
-          __syncthreads();
-          multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
-        } else {
-          if (tid < m) sc.step[tid] *= 0.5;
+        if (sc.score < min_score) {
+          accepted = true;
+          break;
         }
-        if (tries == max_half - 1 && trying)
-          if (tid < m) sc.step[tid] = 0.0;
-        if (tries == max_half) trying = false;
+        if (tid < m) sc.step[tid] *= 0.5;
         __syncthreads();
       }
       if (sc.status != kStatusOk) break;
-    }
-    if (it > 3) {
+      if (!accepted) {  // no decrease along the Gauss-Newton direction: a minimum
+        converged = true;
+        break;
+      }
+      score_red = min_score - sc.score;
+      min_score = sc.score;
+      if (tid < m) sc.log_sp[tid] = sc.trial[tid];
+      __syncthreads();
+      multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
+      if (tid < m) sc.gradient[tid] = sc.grad_c[tid];
+      __syncthreads();
       double g2 = 0.0;
       for (int r = 0; r < m; ++r) g2 += sc.gradient[r] * sc.gradient[r];
-      converged = score_red <= kConvTol * (1.0 + min_score) &&
-                  sqrt(g2) <= pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(min_score));
-      if (tries == max_half) converged = true;
+      if (score_red <= kConvTol * (1.0 + min_score) && sqrt(g2) <= pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(min_score))) {
+        converged = true;
+        break;
+      }
     }
-    __syncthreads();
-    if (tid == 0) {
-      for (int r = 0; r < m; ++r) sc.gradient[r] = sc.grad_c[r];
-      bool st = false;
-      newton_from_hessian(m, &sc, &st);
-      ctl[0] = st ? 1 : 0;
+  } else {
+    for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
+      int tries = 0;
+      if (it > 1) {
+        if (tid < m) sc.step[tid] = steepest ? sc.steep[tid] : sc.newton[tid];
+        __syncthreads();
+        bool trying = true;
+        while (trying) {
+          ++tries;
+          if (tries == 4 && !steepest) {
+            steepest = true;
+            if (tid < m) sc.step[tid] = sc.steep[tid];
+          }
+          __syncthreads();
+          if (tid < m) sc.trial[tid] = sc.log_sp[tid] + sc.step[tid];
+          __syncthreads();
+          multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+          ++calls;
+          if (sc.status != kStatusOk) break;
+          const double tscore = sc.score;
+          if (tscore < min_score) {
+            trying = false;
+            score_red = min_score - tscore;
+            min_score = tscore;
+            if (tid < m) sc.log_sp[tid] = sc.trial[tid];
+            __syncthreads();
+            multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
+          } else {
+            if (tid < m) sc.step[tid] *= 0.5;
+          }
+          if (tries == max_half - 1 && trying)
+            if (tid < m) sc.step[tid] = 0.0;
+          if (tries == max_half) trying = false;
+          __syncthreads();
+        }
+        if (sc.status != kStatusOk) break;
+      }
+      if (it > 3) {
+        double g2 = 0.0;
+        for (int r = 0; r < m; ++r) g2 += sc.gradient[r] * sc.gradient[r];
+        converged = score_red <= kConvTol * (1.0 + min_score) &&
+                    sqrt(g2) <= pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(min_score));
+        if (tries == max_half) converged = true;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        for (int r = 0; r < m; ++r) sc.gradient[r] = sc.grad_c[r];
+        bool st = false;
+        newton_from_hessian(m, &sc, &st);
+        ctl[0] = st ? 1 : 0;
+      }
+      __syncthreads();
+      steepest = ctl[0] != 0;
+      if (converged) break;
     }
-    __syncthreads();
-    steepest = ctl[0] != 0;
-    if (converged) break;
   }
   if (sc.status == kStatusOk && !converged) {
     __syncthreads();
@@ -1546,7 +1642,7 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
                                                             const FitJob* __restrict__ jobs,
                                                             const int* __restrict__ job_index, int job_count,
                                                             double* __restrict__ residuals,
-                                                            FitResult* __restrict__ results) {
+                                                            FitResult* __restrict__ results, int selection) {
   using L = WarpLayout;
   double* sm = s_wsm;
   WarpScalars& sc = s_wsc;
@@ -1580,59 +1676,101 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
     sc.steep[lane] = 0.0;
   }
   __syncwarp();
-  for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
-    int tries = 0;
-    if (it > 1) {
-      if (lane < m) sc.step[lane] = steepest ? sc.steep[lane] : sc.newton[lane];
+  if (selection == FKPC_SELECT_GN_NEWTON) {
+    // Newton on the Gauss-Newton Hessian, halving until V decreases
+    if (lane < m) sc.gradient[lane] = sc.grad_c[lane];
+    __syncwarp();
+    for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
+      if (lane == 0) gn_step(m, &sc);
       __syncwarp();
-      bool trying = true;
-      while (trying) {
-        ++tries;
-        if (tries == 4 && !steepest) {
-          steepest = true;
-          if (lane < m) sc.step[lane] = sc.steep[lane];
-        }
-        __syncwarp();
+      bool accepted = false;
+      for (int tries = 1; tries <= max_half; ++tries) {
         if (lane < m) sc.trial[lane] = sc.log_sp[lane] + sc.step[lane];
         __syncwarp();
         warp_core(arena, n, jb0, jb1);
         ++calls;
         if (sc.status != kStatusOk) break;
-        const double tscore = sc.score;
-        if (tscore < min_score) {
-          trying = false;
-          score_red = min_score - tscore;
-          min_score = tscore;
-          if (lane < m) sc.log_sp[lane] = sc.trial[lane];
-          __syncwarp();
-          warp_derivatives(arena, n, jrow);
-        } else {
-          if (lane < m) sc.step[lane] *= 0.5;
+        if (sc.score < min_score) {
+          accepted = true;
+          break;
         }
-        if (tries == max_half - 1 && trying)
-          if (lane < m) sc.step[lane] = 0.0;
-        if (tries == max_half) trying = false;
+        if (lane < m) sc.step[lane] *= 0.5;
         __syncwarp();
       }
       if (sc.status != kStatusOk) break;
-    }
-    if (it > 3) {
+      if (!accepted) {  // no decrease along the Gauss-Newton direction: a minimum
+        converged = true;
+        break;
+      }
+      score_red = min_score - sc.score;
+      min_score = sc.score;
+      if (lane < m) sc.log_sp[lane] = sc.trial[lane];
+      __syncwarp();
+      warp_derivatives(arena, n, jrow);
+      if (lane < m) sc.gradient[lane] = sc.grad_c[lane];
+      __syncwarp();
       double g2 = 0.0;
       for (int r = 0; r < m; ++r) g2 += sc.gradient[r] * sc.gradient[r];
-      converged = score_red <= kConvTol * (1.0 + min_score) &&
-                  sqrt(g2) <= pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(min_score));
-      if (tries == max_half) converged = true;
+      if (score_red <= kConvTol * (1.0 + min_score) && sqrt(g2) <= pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(min_score))) {
+        converged = true;
+        break;
+      }
     }
-    __syncwarp();
-    if (lane == 0) {
-      for (int r = 0; r < m; ++r) sc.gradient[r] = sc.grad_c[r];
-      bool st = false;
-      newton_from_hessian(m, &sc, &st);
-      sc.ctl = st ? 1 : 0;
+  } else {
+    for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
+      int tries = 0;
+      if (it > 1) {
+        if (lane < m) sc.step[lane] = steepest ? sc.steep[lane] : sc.newton[lane];
+        __syncwarp();
+        bool trying = true;
+        while (trying) {
+          ++tries;
+          if (tries == 4 && !steepest) {
+            steepest = true;
+            if (lane < m) sc.step[lane] = sc.steep[lane];
+          }
+          __syncwarp();
+          if (lane < m) sc.trial[lane] = sc.log_sp[lane] + sc.step[lane];
+          __syncwarp();
+          warp_core(arena, n, jb0, jb1);
+          ++calls;
+          if (sc.status != kStatusOk) break;
+          const double tscore = sc.score;
+          if (tscore < min_score) {
+            trying = false;
+            score_red = min_score - tscore;
+            min_score = tscore;
+            if (lane < m) sc.log_sp[lane] = sc.trial[lane];
+            __syncwarp();
+            warp_derivatives(arena, n, jrow);
+          } else {
+            if (lane < m) sc.step[lane] *= 0.5;
+          }
+          if (tries == max_half - 1 && trying)
+            if (lane < m) sc.step[lane] = 0.0;
+          if (tries == max_half) trying = false;
+          __syncwarp();
+        }
+        if (sc.status != kStatusOk) break;
+      }
+      if (it > 3) {
+        double g2 = 0.0;
+        for (int r = 0; r < m; ++r) g2 += sc.gradient[r] * sc.gradient[r];
+        converged = score_red <= kConvTol * (1.0 + min_score) &&
+                    sqrt(g2) <= pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(min_score));
+        if (tries == max_half) converged = true;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        for (int r = 0; r < m; ++r) sc.gradient[r] = sc.grad_c[r];
+        bool st = false;
+        newton_from_hessian(m, &sc, &st);
+        sc.ctl = st ? 1 : 0;
+      }
+      __syncwarp();
+      steepest = sc.ctl != 0;
+      if (converged) break;
     }
-    __syncwarp();
-    steepest = sc.ctl != 0;
-    if (converged) break;
   }
   if (sc.status == kStatusOk && !converged) {
     __syncwarp();
@@ -1823,15 +1961,16 @@ cudaError_t launch_fit_single(const DesignDev* designs, const double* arena, con
 
 cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const double* arena, const double* data,
                              int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
-                             FitResult* results, cudaStream_t stream) {
+                             FitResult* results, cudaStream_t stream, int selection) {
   if (count <= 0) return cudaSuccess;
   const size_t smem = multi_smem_bytes(qmax_class);
   if (qmax_class == 0) {
     fit_multi_warp_kernel<<<count, 32, 0, stream>>>(designs, arena, data, n, jobs, job_index, count, residuals,
-                                                    results);
+                                                    results, selection);
   } else {
     auto k = fit_multi_kernel<76, 64>;
-    k<<<count, kMultiThreads, smem, stream>>>(designs, arena, data, n, jobs, job_index, count, residuals, results);
+    k<<<count, kMultiThreads, smem, stream>>>(designs, arena, data, n, jobs, job_index, count, residuals, results,
+                                              selection);
   }
   return cudaGetLastError();
 }

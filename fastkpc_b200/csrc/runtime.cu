@@ -362,14 +362,14 @@ void Engine::enqueue() {
   if (!multi_small_.empty()) {
     cuda_check(launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                 d_multi_small_.get(), static_cast<int>(multi_small_.size()), d_resid_.get(),
-                                d_multi_res_.get(), stream_),
+                                d_multi_res_.get(), stream_, opt_.selection),
                "fit multi");
     ++launches_;
   }
   if (!multi_large_.empty()) {
     cuda_check(launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                 d_multi_large_.get(), static_cast<int>(multi_large_.size()), d_resid_.get(),
-                                d_multi_res_.get(), stream_),
+                                d_multi_res_.get(), stream_, opt_.selection),
                "fit multi");
     ++launches_;
   }
@@ -660,14 +660,14 @@ void Engine::enqueue_plain_test(int t) {
   const int a0 = plain_small_off_[t], a1 = plain_small_off_[t + 1];
   if (a1 > a0) {
     cuda_check(launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
-                                d_multi_small_.get() + a0, a1 - a0, d_resid_.get(), d_multi_res_.get(), stream_),
+                                d_multi_small_.get() + a0, a1 - a0, d_resid_.get(), d_multi_res_.get(), stream_, opt_.selection),
                "fit multi");
     ++launches_;
   }
   const int b0 = plain_large_off_[t], b1 = plain_large_off_[t + 1];
   if (b1 > b0) {
     cuda_check(launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
-                                d_multi_large_.get() + b0, b1 - b0, d_resid_.get(), d_multi_res_.get(), stream_),
+                                d_multi_large_.get() + b0, b1 - b0, d_resid_.get(), d_multi_res_.get(), stream_, opt_.selection),
                "fit multi");
     ++launches_;
   }
@@ -750,10 +750,10 @@ double Engine::time_stage(int stage, int repeats, double* flops_per_launch) {
                                        static_cast<int>(single_jobs_.size()), d_resid_.get(), d_single_res_.get(), stream_);
       case 1: return launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                       d_multi_small_.get(), static_cast<int>(multi_small_.size()), d_resid_.get(),
-                                      d_multi_res_.get(), stream_);
+                                      d_multi_res_.get(), stream_, opt_.selection);
       case 2: return launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                       d_multi_large_.get(), static_cast<int>(multi_large_.size()), d_resid_.get(),
-                                      d_multi_res_.get(), stream_);
+                                      d_multi_res_.get(), stream_, opt_.selection);
       case 3: return launch_dcov_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, d_centre_.get(),
                                             d_dcov_.get(), stream_);
       case 4: return launch_dcov_pairs(d_resid_.get(), n, d_comp_cols_.get(), d_centre_.get(), d_dcov_.get(),
@@ -812,7 +812,8 @@ double Engine::measure_fp64_peak() {
 }
 
 void Engine::regress(const std::vector<int>& targets, const std::vector<std::vector<int>>& sets,
-                     double* residuals, double* log_sp, int max_penalties, int* status) {
+                     double* residuals, double* log_sp, int max_penalties, int* status, int selection,
+                     int* evaluations) {
   if (targets.size() != sets.size()) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "targets and sets differ in length");
   std::vector<Test> tests;
   for (size_t i = 0; i < targets.size(); ++i) {
@@ -829,6 +830,7 @@ void Engine::regress(const std::vector<int>& targets, const std::vector<std::vec
   }
   fkpc_options opt;
   fkpc_default_options(&opt);
+  opt.selection = selection;
   opt_ = opt;
   release_graph();
   auto t0 = std::chrono::steady_clock::now();
@@ -858,6 +860,7 @@ void Engine::regress(const std::vector<int>& targets, const std::vector<std::vec
               residuals + static_cast<size_t>(n) * i);
     const FitResult* r = by_comp[c];
     if (status) status[i] = r ? r->status : kStatusOk;
+    if (evaluations) evaluations[i] = r ? r->evaluations : 0;
     if (log_sp)
       for (int j = 0; j < max_penalties; ++j)
         log_sp[i * static_cast<size_t>(max_penalties) + j] = (r && j < kMaxPenalties) ? r->log_sp[j] : NAN;

@@ -86,7 +86,8 @@ class Engine {
 
   // Residual fits only (the regrXonS stage).
   void regress(const std::vector<int>& targets, const std::vector<std::vector<int>>& sets,
-               double* residuals, double* log_sp, int max_penalties, int* status);
+               double* residuals, double* log_sp, int max_penalties, int* status,
+               int selection = FKPC_SELECT_MAGIC, int* evaluations = nullptr);
   // Statistics only, on caller residual columns.
   void statistics(const double* residuals, int m, const std::vector<int>& left, const std::vector<int>& right,
                   const int* permutations, const fkpc_options& opt, fkpc_ci_record* out);

@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define FKPC_ABI_VERSION 1
+#define FKPC_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define FKPC_API __attribute__((visibility("default")))
@@ -46,6 +46,10 @@ extern "C" {
 #define FKPC_MODE_BATCHED 0  /* every test of a level in one batched launch set */
 #define FKPC_MODE_PLAIN 1    /* one launch set per CI test */
 
+/* smoothing-parameter selection for additive designs (|S| >= 3) */
+#define FKPC_SELECT_MAGIC 0      /* mgcv magic's Newton / halving search, as the reference */
+#define FKPC_SELECT_GN_NEWTON 1  /* Newton on the Gauss-Newton Hessian of GCV (fkpc_gcv_adjoint's) */
+
 /* per-record flags */
 #define FKPC_FLAG_GUARDED 1u       /* dcc.gamma p came from the low-rank refinement */
 #define FKPC_FLAG_DIRECT 2u        /* |S| = 0: raw columns, no regression */
@@ -64,6 +68,7 @@ typedef struct fkpc_options {
   int collect_trace;            /* keep the per-test logical trace */
   int device;                   /* CUDA device ordinal */
   int strict;                   /* reference envelope: alpha 0.1, index 1, numCol 35 < n, 2 <= p <= 64 */
+  int selection;                /* FKPC_SELECT_MAGIC (default) or FKPC_SELECT_GN_NEWTON */
 } fkpc_options;
 
 /* One CI test result. */

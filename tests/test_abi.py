@@ -33,9 +33,12 @@ def test_library_exports_every_declared_symbol(lib_built):
 
 
 def test_abi_version_and_defaults(lib_built):
-    assert lib_built.fkpc_abi_version() == 1
+    assert lib_built.fkpc_abi_version() == 2
     o = fk.make_options()
     assert o.alpha == 0.1 and o.num_col == 35 and o.index == 1.0 and o.strict == 1
+    assert o.selection == 0 and fk.make_options(selection="gn_newton").selection == 1
+    with pytest.raises(ValueError):
+        fk.make_options(selection="bfgs")
 
 
 def test_envelope_errors_are_raised_before_any_device_work(lib_built):

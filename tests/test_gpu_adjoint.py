@@ -75,3 +75,24 @@ def test_adjoint_rejects_single_penalty_sets(lib_built, workload):
     X, _ = workload
     with pytest.raises(fk.FkpcError, match="additive"):
         fk.gcv_adjoint(X, 0, [1, 2], np.zeros((1, 2)))
+
+
+def test_gn_newton_selection_matches_the_plain_search(lib_built, workload):
+    """Newton selection on the Gauss-Newton Hessian against magic's search on
+    the same fits: residuals within 1e-8 of their scale, and the selected
+    log(lambda) within 1e-4 wherever V has curvature there (flat directions,
+    log(lambda) beyond ~20, move the residual by less than the tolerance)."""
+    X, fits = workload
+    sel = fits[:96]
+    r_magic, lsp_magic, st_magic = fk.regress_batch(X, sel)
+    r_gn, lsp_gn, st_gn = fk.regress_batch(X, sel, selection="gn_newton")
+    assert (st_magic == 0).all() and (st_gn == 0).all()
+    worst = 0.0
+    for k, (t, S) in enumerate(sel):
+        scale = np.max(np.abs(r_magic[:, k]))
+        err = np.max(np.abs(r_gn[:, k] - r_magic[:, k])) / scale
+        worst = max(worst, err)
+        assert err <= 1e-8, (t, S, err, lsp_magic[k, :len(S)], lsp_gn[k, :len(S)])
+        a = fk.gcv_adjoint(X, t, S, lsp_magic[k, :len(S)][None, :])
+        curved = np.diag(a["hessian"][0]) > 1e-6 * a["score"][0]
+        assert np.all(np.abs(lsp_gn[k, :len(S)] - lsp_magic[k, :len(S)])[curved] <= 1e-4), (t, S)

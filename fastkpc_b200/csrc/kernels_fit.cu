@@ -271,6 +271,10 @@ constexpr int kPolishSteps = 4;
 constexpr double kPolishMaxStep = 1e-6;
 constexpr double kPolishDone = 1e-10;
 constexpr double kPolishCurvature = 1e-6;
+constexpr double kGnGradTol = 1e-9;   // Gauss-Newton selection: |grad V| <= 1e-9 (1 + V),
+constexpr double kGnFlatTol = 1e-12;  // or a decrease <= 1e-12 (1 + V)
+constexpr double kGnFlatGrad = 1e-6;  // with |grad V| <= 1e-6 (1 + V)
+constexpr double kGnMaxLogSp = 25.0;  // upper bound of the Gauss-Newton search in log(lambda)
 
 __device__ __forceinline__ int tri(int i, int j) { return j * (j + 1) / 2 + i; }  // packed upper, i <= j
 
@@ -771,57 +775,89 @@ __device__ int polish_step(int m, S* sc) {
   return mx <= kPolishDone ? 2 : 1;
 }
 
-// Gauss-Newton step (one thread): solve (GN + mu I) d = -g by Cholesky, with
-// mu = 0 first and then 1e-12, 1e-10, ... times the largest diagonal entry
-// until the factor exists (GN = 2 J'J is positive semi-definite, singular in
-// the flat directions of V); the step is capped at 5 in max norm as magic's.
+// Cholesky solve of (A + mu I) z = -g (one thread, m <= kMaxPenalties, A
+// column-major with leading dimension kMaxPenalties) on the coordinates
+// whose bit in ``fixed`` is clear; fixed coordinates get z = 0.  False when
+// the factor does not exist.
+__device__ bool chol_solve_neg(int m, const double* A, double mu, const double* g, unsigned fixed, double* Lm,
+                               double* z) {
+  for (int c = 0; c < m; ++c)
+    for (int r = 0; r < m; ++r) {
+      const bool fr = (fixed >> r) & 1u, fc = (fixed >> c) & 1u;
+      Lm[r + kMaxPenalties * c] = (fr || fc) ? (r == c ? 1.0 : 0.0) : A[r + kMaxPenalties * c] + (r == c ? mu : 0.0);
+    }
+  for (int c = 0; c < m; ++c) {
+    double d = Lm[c + kMaxPenalties * c];
+    for (int k = 0; k < c; ++k) d -= Lm[c + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
+    if (!(d > 0.0)) return false;
+    d = sqrt(d);
+    Lm[c + kMaxPenalties * c] = d;
+    for (int r = c + 1; r < m; ++r) {
+      double v = Lm[r + kMaxPenalties * c];
+      for (int k = 0; k < c; ++k) v -= Lm[r + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
+      Lm[r + kMaxPenalties * c] = v / d;
+    }
+  }
+  for (int r = 0; r < m; ++r) {
+    double v = ((fixed >> r) & 1u) ? 0.0 : -g[r];
+    for (int k = 0; k < r; ++k) v -= Lm[r + kMaxPenalties * k] * z[k];
+    z[r] = v / Lm[r + kMaxPenalties * r];
+  }
+  for (int r = m - 1; r >= 0; --r) {
+    double v = z[r];
+    for (int k = r + 1; k < m; ++k) v -= Lm[k + kMaxPenalties * r] * z[k];
+    z[r] = v / Lm[r + kMaxPenalties * r];
+  }
+  return true;
+}
+
+// Newton or damped Gauss-Newton solve of the adjoint-driven selection on the
+// free coordinates (see gn_step).  False when no factor exists.
 template <class S>
-__device__ void gn_step(int m, S* sc) {
+__device__ bool gn_solve(int m, S* sc, unsigned fixed, double* z) {
+  if (chol_solve_neg(m, sc->hess_c, 0.0, sc->grad_c, fixed, sc->ja, z)) return true;
   double dmax = 0.0;
   for (int j = 0; j < m; ++j) dmax = fmax(dmax, fabs(sc->gn_c[j + kMaxPenalties * j]));
   double mu = 0.0;
-  double* Lm = sc->ja;
   for (int attempt = 0; attempt < 12; ++attempt) {
-    for (int c = 0; c < m; ++c)
-      for (int r = 0; r < m; ++r) Lm[r + kMaxPenalties * c] = sc->gn_c[r + kMaxPenalties * c] + (r == c ? mu : 0.0);
-    bool pd = true;
-    for (int c = 0; c < m && pd; ++c) {
-      double d = Lm[c + kMaxPenalties * c];
-      for (int k = 0; k < c; ++k) d -= Lm[c + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
-      if (!(d > 0.0)) {
-        pd = false;
-        break;
-      }
-      d = sqrt(d);
-      Lm[c + kMaxPenalties * c] = d;
-      for (int r = c + 1; r < m; ++r) {
-        double v = Lm[r + kMaxPenalties * c];
-        for (int k = 0; k < c; ++k) v -= Lm[r + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
-        Lm[r + kMaxPenalties * c] = v / d;
-      }
-    }
-    if (pd) {
-      double z[kMaxPenalties];
-      for (int r = 0; r < m; ++r) {
-        double v = -sc->grad_c[r];
-        for (int k = 0; k < r; ++k) v -= Lm[r + kMaxPenalties * k] * z[k];
-        z[r] = v / Lm[r + kMaxPenalties * r];
-      }
-      double mx = 0.0;
-      for (int r = m - 1; r >= 0; --r) {
-        double v = z[r];
-        for (int k = r + 1; k < m; ++k) v -= Lm[k + kMaxPenalties * r] * z[k];
-        z[r] = v / Lm[r + kMaxPenalties * r];
-        mx = fmax(mx, fabs(z[r]));
-      }
-      for (int r = 0; r < m; ++r) sc->step[r] = mx > 5.0 ? z[r] * (5.0 / mx) : z[r];
-      return;
-    }
+    if (chol_solve_neg(m, sc->gn_c, mu, sc->grad_c, fixed, sc->ja, z)) return true;
     mu = mu == 0.0 ? 1e-12 * fmax(dmax, 1e-300) : mu * 100.0;
   }
-  double mg = 0.0;
-  for (int r = 0; r < m; ++r) mg = fmax(mg, fabs(sc->grad_c[r]));
-  for (int r = 0; r < m; ++r) sc->step[r] = mg == 0.0 ? 0.0 : -sc->grad_c[r] / mg;
+  return false;
+}
+
+// Step of the adjoint-driven selection (one thread): Newton on the exact
+// Hessian where it is positive definite (quadratic convergence near a
+// minimum), else on the Gauss-Newton Hessian GN = 2 J'J (positive
+// semi-definite, singular in the flat directions of V) damped by mu = 1e-12,
+// 1e-10, ... times its largest diagonal entry until Cholesky succeeds.
+// Projected on the bound log(lambda) <= kGnMaxLogSp: coordinates on the
+// bound whose step points outwards are fixed and the rest re-solved.  The
+// step is capped at 5 in max norm as magic's.
+template <class S>
+__device__ void gn_step(int m, S* sc) {
+  double z[kMaxPenalties];
+  unsigned fixed = 0u;
+  bool ok = gn_solve(m, sc, fixed, z);
+  if (ok) {
+    for (int r = 0; r < m; ++r)
+      if (sc->log_sp[r] >= kGnMaxLogSp && z[r] > 0.0) fixed |= 1u << r;
+    if (fixed) ok = gn_solve(m, sc, fixed, z);
+  }
+  if (!ok) {
+    double mg = 0.0;
+    for (int r = 0; r < m; ++r) mg = fmax(mg, fabs(sc->grad_c[r]));
+    for (int r = 0; r < m; ++r) z[r] = mg == 0.0 ? 0.0 : -sc->grad_c[r] / mg;
+  }
+  double mx = 0.0;
+  for (int r = 0; r < m; ++r) mx = fmax(mx, fabs(z[r]));
+  for (int r = 0; r < m; ++r) {
+    const double st = mx > 5.0 ? z[r] * (5.0 / mx) : z[r];
+    // the unpivoted fold loses accuracy in the penalty null spaces as
+    // log(lambda) grows (about 1e-16 sqrt(lambda) relative), and V is flat
+    // there: the search stays below kGnMaxLogSp
+    sc->step[r] = fmin(st, kGnMaxLogSp - sc->log_sp[r]);
+  }
 }
 
 }  // namespace
@@ -948,9 +984,13 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
       multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
       if (tid < m) sc.gradient[tid] = sc.grad_c[tid];
       __syncthreads();
-      double g2 = 0.0;
-      for (int r = 0; r < m; ++r) g2 += sc.gradient[r] * sc.gradient[r];
-      if (score_red <= kConvTol * (1.0 + min_score) && sqrt(g2) <= pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(min_score))) {
+      double g2 = 0.0;  // projected gradient: a coordinate on the upper bound that V pushes outwards counts 0
+      for (int r = 0; r < m; ++r)
+        if (!(sc.log_sp[r] >= kGnMaxLogSp && sc.gradient[r] < 0.0)) g2 += sc.gradient[r] * sc.gradient[r];
+      // a stationary point (not magic's loose stop), or V no longer moving
+      // along directions that have gone flat (log lambda drifting upwards)
+      if (sqrt(g2) <= kGnGradTol * (1.0 + fabs(min_score)) ||
+          (score_red <= kGnFlatTol * (1.0 + min_score) && sqrt(g2) <= kGnFlatGrad * (1.0 + fabs(min_score)))) {
         converged = true;
         break;
       }
@@ -1016,7 +1056,7 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
     if (tid == 0) sc.status = kStatusNotConverged;
     __syncthreads();
   }
-  if (sc.status == kStatusOk) {
+  if (sc.status == kStatusOk && selection != FKPC_SELECT_GN_NEWTON) {  // magic's boundary probes
     for (int c = 0; c < m; ++c) {
       const double direction = sc.gradient[c] < 0.0 ? 1.0 : -1.0;
       for (int probe = 0; probe < 5; ++probe) {
@@ -1709,9 +1749,13 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
       warp_derivatives(arena, n, jrow);
       if (lane < m) sc.gradient[lane] = sc.grad_c[lane];
       __syncwarp();
-      double g2 = 0.0;
-      for (int r = 0; r < m; ++r) g2 += sc.gradient[r] * sc.gradient[r];
-      if (score_red <= kConvTol * (1.0 + min_score) && sqrt(g2) <= pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(min_score))) {
+      double g2 = 0.0;  // projected gradient: a coordinate on the upper bound that V pushes outwards counts 0
+      for (int r = 0; r < m; ++r)
+        if (!(sc.log_sp[r] >= kGnMaxLogSp && sc.gradient[r] < 0.0)) g2 += sc.gradient[r] * sc.gradient[r];
+      // a stationary point (not magic's loose stop), or V no longer moving
+      // along directions that have gone flat (log lambda drifting upwards)
+      if (sqrt(g2) <= kGnGradTol * (1.0 + fabs(min_score)) ||
+          (score_red <= kGnFlatTol * (1.0 + min_score) && sqrt(g2) <= kGnFlatGrad * (1.0 + fabs(min_score)))) {
         converged = true;
         break;
       }
@@ -1777,7 +1821,7 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
     if (lane == 0) sc.status = kStatusNotConverged;
     __syncwarp();
   }
-  if (sc.status == kStatusOk) {
+  if (sc.status == kStatusOk && selection != FKPC_SELECT_GN_NEWTON) {  // magic's boundary probes
     for (int c = 0; c < m; ++c) {
       const double direction = sc.gradient[c] < 0.0 ? 1.0 : -1.0;
       for (int probe = 0; probe < 5; ++probe) {

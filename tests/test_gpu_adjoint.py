@@ -77,22 +77,24 @@ def test_adjoint_rejects_single_penalty_sets(lib_built, workload):
         fk.gcv_adjoint(X, 0, [1, 2], np.zeros((1, 2)))
 
 
-def test_gn_newton_selection_matches_the_plain_search(lib_built, workload):
-    """Newton selection on the Gauss-Newton Hessian against magic's search on
-    the same fits: residuals within 1e-8 of their scale, and the selected
-    log(lambda) within 1e-4 wherever V has curvature there (flat directions,
-    log(lambda) beyond ~20, move the residual by less than the tolerance)."""
+def test_gn_newton_selection_matches_the_oracle(lib_built, workload):
+    """FKPC_SELECT_GN_NEWTON (exact-Hessian Newton where that Hessian is
+    positive definite, damped Gauss-Newton elsewhere, then magic's probes and
+    polish) against its oracle restatement oracle.gcv.optimize_gn: residuals
+    within 1e-10 of their scale on |S| = 3..8.  (Against magic's selection it
+    agrees where both reach the same local minimum of GCV; it can settle in a
+    different one, so that is not asserted.)"""
     X, fits = workload
-    sel = fits[:96]
-    r_magic, lsp_magic, st_magic = fk.regress_batch(X, sel)
+    sel = [next(f for f in fits if len(f[1]) == k) for k in range(3, 9)]
+    sel += [f for f in fits if len(f[1]) in (3, 4)][1:7]
     r_gn, lsp_gn, st_gn = fk.regress_batch(X, sel, selection="gn_newton")
-    assert (st_magic == 0).all() and (st_gn == 0).all()
-    worst = 0.0
+    assert (st_gn == 0).all()
     for k, (t, S) in enumerate(sel):
-        scale = np.max(np.abs(r_magic[:, k]))
-        err = np.max(np.abs(r_gn[:, k] - r_magic[:, k])) / scale
-        worst = max(worst, err)
-        assert err <= 1e-8, (t, S, err, lsp_magic[k, :len(S)], lsp_gn[k, :len(S)])
-        a = fk.gcv_adjoint(X, t, S, lsp_magic[k, :len(S)][None, :])
-        curved = np.diag(a["hessian"][0]) > 1e-6 * a["score"][0]
-        assert np.all(np.abs(lsp_gn[k, :len(S)] - lsp_magic[k, :len(S)])[curved] <= 1e-4), (t, S)
+        prep = gcv.Prepared(tprs.design(X, S))
+        o = gcv.optimize_gn(prep, X[:, t])
+        r = gcv.residual_at(prep, prep.response(X[:, t]), o["log_sp"])
+        err = np.max(np.abs(r_gn[:, k] - r)) / np.max(np.abs(r))
+        # beyond log(lambda) = 25 the oracle's rank-truncated SVD and the
+        # kernels' Householder fold evaluate V differently at the 1e-10 level
+        extreme = max(np.max(lsp_gn[k, :len(S)]), np.max(o["log_sp"])) > 25.0
+        assert err <= (1e-6 if extreme else 1e-10), (t, S, err, lsp_gn[k, :len(S)], o["log_sp"])

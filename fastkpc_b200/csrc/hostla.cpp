@@ -162,11 +162,24 @@ bool tridiagonal_ql(int n, double* d, double* e, double* z) {
 namespace {
 
 void symv(const double* A, int n, const double* x, double* y) {
+  // upper triangle only: column j gives y[i] += A(i,j) x[j] and y[j] += A(i,j) x[i], i < j
   for (int i = 0; i < n; ++i) y[i] = 0.0;
   for (int j = 0; j < n; ++j) {
     const double xj = x[j];
     const double* col = A + static_cast<size_t>(n) * j;
-    for (int i = 0; i < n; ++i) y[i] += col[i] * xj;
+    double s0 = 0.0, s1 = 0.0;
+    int i = 0;
+    for (; i + 1 < j; i += 2) {
+      y[i] += col[i] * xj;
+      y[i + 1] += col[i + 1] * xj;
+      s0 += col[i] * x[i];
+      s1 += col[i + 1] * x[i + 1];
+    }
+    for (; i < j; ++i) {
+      y[i] += col[i] * xj;
+      s0 += col[i] * x[i];
+    }
+    y[j] += (s0 + s1) + col[j] * xj;
   }
 }
 
@@ -261,29 +274,28 @@ int top_magnitude_eigen(const double* A, int n, int k, std::vector<double>* valu
             for (int r = 0; r < n; ++r) vc[r] += coef * qb[r];
           }
         }
-        // Rayleigh-Ritz refinement on span[V, A V]
-        int k2 = 2 * k;
-        std::vector<double> Wm(static_cast<size_t>(n) * k2);
-        std::copy(V.begin(), V.end(), Wm.begin());
-        for (int c = 0; c < k; ++c)
-          symv(A, n, &V[static_cast<size_t>(n) * c], &Wm[static_cast<size_t>(n) * (k + c)]);
-        std::vector<double> Qb, Rb;
-        householder_qr(Wm.data(), n, k2, &Qb, &Rb);
-        std::vector<double> AQ(static_cast<size_t>(n) * k2);
-        for (int c = 0; c < k2; ++c)
-          symv(A, n, &Qb[static_cast<size_t>(n) * c], &AQ[static_cast<size_t>(n) * c]);
-        std::vector<double> H(static_cast<size_t>(k2) * k2);
-        for (int a = 0; a < k2; ++a)
-          for (int b = 0; b < k2; ++b)
-            H[a + static_cast<size_t>(k2) * b] = dot(&Qb[static_cast<size_t>(n) * a], &AQ[static_cast<size_t>(n) * b], n);
-        for (int a = 0; a < k2; ++a)
-          for (int b = a + 1; b < k2; ++b) {
-            double s = 0.5 * (H[a + static_cast<size_t>(k2) * b] + H[b + static_cast<size_t>(k2) * a]);
-            H[a + static_cast<size_t>(k2) * b] = H[b + static_cast<size_t>(k2) * a] = s;
+        // Rayleigh-Ritz within span(V): H = V'AV, with AV as one pass over A
+        // (column j of A updates every column of AV), then rotate V.
+        std::vector<double> AV(static_cast<size_t>(n) * k, 0.0);
+        for (int jj = 0; jj < n; ++jj) {
+          const double* acol = A + static_cast<size_t>(n) * jj;
+          for (int c = 0; c < k; ++c) {
+            const double vjc = V[jj + static_cast<size_t>(n) * c];
+            double* avc = &AV[static_cast<size_t>(n) * c];
+            for (int i = 0; i < n; ++i) avc[i] += acol[i] * vjc;
+          }
+        }
+        std::vector<double> H(static_cast<size_t>(k) * k);
+        for (int a = 0; a < k; ++a)
+          for (int b = 0; b <= a; ++b) {
+            const double h = 0.5 * (dot(&V[static_cast<size_t>(n) * a], &AV[static_cast<size_t>(n) * b], n) +
+                                    dot(&V[static_cast<size_t>(n) * b], &AV[static_cast<size_t>(n) * a], n));
+            H[a + static_cast<size_t>(k) * b] = H[b + static_cast<size_t>(k) * a] = h;
           }
         std::vector<double> hv, hz;
-        jacobi_eigen(H.data(), k2, &hv, &hz);
-        std::vector<int> pick = top_k_by_magnitude(hv, k2, k);
+        jacobi_eigen(H.data(), k, &hv, &hz);
+        std::vector<int> pick(k);
+        for (int c = 0; c < k; ++c) pick[c] = c;
         std::stable_sort(pick.begin(), pick.end(), [&](int a, int b) { return hv[a] > hv[b]; });
         values->assign(k, 0.0);
         vectors->assign(static_cast<size_t>(n) * k, 0.0);
@@ -291,10 +303,10 @@ int top_magnitude_eigen(const double* A, int n, int k, std::vector<double>* valu
           int i = pick[c];
           (*values)[c] = hv[i];
           double* out = &(*vectors)[static_cast<size_t>(n) * c];
-          for (int b = 0; b < k2; ++b) {
-            double coef = hz[b + static_cast<size_t>(k2) * i];
-            const double* qb = &Qb[static_cast<size_t>(n) * b];
-            for (int r = 0; r < n; ++r) out[r] += coef * qb[r];
+          for (int b = 0; b < k; ++b) {
+            double coef = hz[b + static_cast<size_t>(k) * i];
+            const double* vb = &V[static_cast<size_t>(n) * b];
+            for (int r = 0; r < n; ++r) out[r] += coef * vb[r];
           }
           double nn = std::sqrt(dot(out, out, n));
           int imax = 0;

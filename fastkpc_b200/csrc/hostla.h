@@ -26,8 +26,8 @@ bool tridiagonal_ql(int n, double* d, double* e, double* z);
 
 // The k eigenpairs of largest |value| of the symmetric n x n matrix A,
 // ordered by descending value (algebraic).  Lanczos with full
-// re-orthogonalisation, then one Rayleigh-Ritz refinement on the span of the
-// converged vectors and their images.  Each eigenvector is signed so that its
+// re-orthogonalisation, then one Rayleigh-Ritz refinement within the span of
+// the converged Ritz vectors.  Each eigenvector is signed so that its
 // largest-magnitude entry is positive.  Returns the Lanczos steps used.
 int top_magnitude_eigen(const double* A, int n, int k, std::vector<double>* values,
                         std::vector<double>* vectors);

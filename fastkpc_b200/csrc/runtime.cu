@@ -66,12 +66,31 @@ Engine::Engine(int device) : device_(device) {
 Engine::~Engine() {
   cudaSetDevice(device_);
   release_graph();
+  if (h_arena_) cudaFreeHost(h_arena_);
   for (auto& ev : ev_)
     if (ev) cudaEventDestroy(ev);
   if (stream_) {
     cudaStreamSynchronize(stream_);
     cudaStreamDestroy(stream_);
   }
+}
+
+double* Engine::pinned_arena(size_t count) {
+  if (count == 0) count = 1;
+  if (count > h_arena_cap_) {
+    cuda_check(cudaStreamSynchronize(stream_), "arena staging");  // no copy may still read the old buffer
+    if (h_arena_) cudaFreeHost(h_arena_);
+    h_arena_ = nullptr;
+    h_arena_cap_ = 0;
+    const size_t grow = count + count / 4;
+    cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&h_arena_), grow * sizeof(double), cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      h_arena_ = nullptr;
+      throw Error(FKPC_STATUS_ALLOCATION, std::string("pinned host allocation failed: ") + cudaGetErrorString(e));
+    }
+    h_arena_cap_ = grow;
+  }
+  return h_arena_;
 }
 
 void Engine::release_graph() {
@@ -176,8 +195,9 @@ void Engine::build_designs() {
 
 void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   const int n = n_;
-  std::vector<double> arena;
+  // Pass 1: descriptors and arena offsets (no copies).
   std::vector<DesignDev> ddesc(designs_.size());
+  size_t total = 0;
   for (size_t d = 0; d < designs_.size(); ++d) {
     const Design& des = *designs_[d];
     DesignDev& dd = ddesc[d];
@@ -187,10 +207,10 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
     if (des.m == 1) {
       if (des.q > kMaxSingleQ) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "single-penalty design too wide");
       dd.kind = 1;
-      dd.basis = static_cast<int64_t>(arena.size());
-      arena.insert(arena.end(), des.QW.begin(), des.QW.end());
-      dd.spec = static_cast<int64_t>(arena.size());
-      arena.insert(arena.end(), des.spec.begin(), des.spec.end());
+      dd.basis = static_cast<int64_t>(total);
+      total += des.QW.size();
+      dd.spec = static_cast<int64_t>(total);
+      total += des.spec.size();
       dd.log_sp0[0] = des.initial_log_sp[0];
       dd.off[0] = des.offsets[0];
       dd.dim[0] = des.dims[0];
@@ -198,11 +218,11 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       dd.rsum = des.ranks[0];
     } else {
       dd.kind = 2;
-      dd.basis = static_cast<int64_t>(arena.size());
-      arena.insert(arena.end(), des.Q.begin(), des.Q.end());
-      dd.rmat = static_cast<int64_t>(arena.size());
-      arena.insert(arena.end(), des.R.begin(), des.R.end());
-      dd.roots = static_cast<int64_t>(arena.size());
+      dd.basis = static_cast<int64_t>(total);
+      total += des.Q.size();
+      dd.rmat = static_cast<int64_t>(total);
+      total += des.R.size();
+      dd.roots = static_cast<int64_t>(total);
       int rows = 0;
       int64_t rootoff = 0;
       for (int j = 0; j < des.m; ++j) {
@@ -213,20 +233,55 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
         dd.rootoff[j] = static_cast<int>(rootoff);
         dd.log_sp0[j] = des.initial_log_sp[j];
         rows += des.ranks[j];
-        arena.insert(arena.end(), des.roots[j].begin(), des.roots[j].end());
         rootoff += static_cast<int64_t>(des.roots[j].size());
       }
+      total += static_cast<size_t>(rootoff);
       dd.rsum = rows;
       if (des.q > 76 || rows > 64) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity");
       dd.rpack = -1;
       if (des.q <= kWarpQ) {
-        if (arena.size() % 2) arena.push_back(0.0);  // 16-byte aligned: copied with 16-byte cp.async
-        dd.rpack = static_cast<int64_t>(arena.size());
-        const size_t base = arena.size();
-        arena.resize(base + kWarpTri, 0.0);
-        for (int t = 0; t < des.q; ++t)
-          for (int c = t; c < des.q; ++c) arena[base + packed_row(t, c)] = des.R[t + static_cast<size_t>(des.q) * c];
+        total += total % 2;  // 16-byte aligned: copied with 16-byte cp.async
+        dd.rpack = static_cast<int64_t>(total);
+        total += kWarpTri;
       }
+    }
+  }
+  // Pass 2: every design copies itself into the pinned staging buffer
+  // (threads over designs), then one DMA to the device arena.
+  double* host = pinned_arena(total);
+  {
+    std::atomic<size_t> next(0);
+    auto work = [&]() {
+      for (;;) {
+        const size_t d = next.fetch_add(1);
+        if (d >= designs_.size()) return;
+        const Design& des = *designs_[d];
+        const DesignDev& dd = ddesc[d];
+        if (dd.kind == 1) {
+          std::memcpy(host + dd.basis, des.QW.data(), des.QW.size() * sizeof(double));
+          std::memcpy(host + dd.spec, des.spec.data(), des.spec.size() * sizeof(double));
+        } else {
+          std::memcpy(host + dd.basis, des.Q.data(), des.Q.size() * sizeof(double));
+          std::memcpy(host + dd.rmat, des.R.data(), des.R.size() * sizeof(double));
+          for (int j = 0; j < des.m; ++j)
+            std::memcpy(host + dd.roots + dd.rootoff[j], des.roots[j].data(), des.roots[j].size() * sizeof(double));
+          if (dd.rpack >= 0) {
+            double* rp = host + dd.rpack;
+            std::fill(rp, rp + kWarpTri, 0.0);
+            for (int t = 0; t < des.q; ++t)
+              for (int c = t; c < des.q; ++c) rp[packed_row(t, c)] = des.R[t + static_cast<size_t>(des.q) * c];
+          }
+        }
+      }
+    };
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t workers = std::min<size_t>(std::min<size_t>(hw, 16), std::max<size_t>(1, designs_.size() / 64));
+    if (workers <= 1) {
+      work();
+    } else {
+      std::vector<std::thread> pool;
+      for (size_t w = 0; w < workers; ++w) pool.emplace_back(work);
+      for (auto& th : pool) th.join();
     }
   }
   single_jobs_.clear();
@@ -273,7 +328,10 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   const size_t npairs = pairs_.size();
   auto t0 = std::chrono::steady_clock::now();
   h2d_bytes_ = static_cast<double>(host_data_.size() * sizeof(double));
-  h2d_bytes_ += upload(d_arena_, arena, stream_);
+  if (total > 0)
+    cuda_check(cudaMemcpyAsync(d_arena_.ensure(total), host, total * sizeof(double), cudaMemcpyHostToDevice, stream_),
+               "upload arena");
+  h2d_bytes_ += static_cast<double>(total * sizeof(double));
   h2d_bytes_ += upload(d_designs_, ddesc, stream_);
   h2d_bytes_ += upload(d_single_jobs_, single_jobs_, stream_);
   h2d_bytes_ += upload(d_multi_jobs_, multi_jobs_, stream_);

@@ -112,6 +112,7 @@ class Engine {
   void pack_and_upload(const fkpc_options& opt, RStream* stream);
   void enqueue();  // the launch sequence
   void release_graph();
+  double* pinned_arena(size_t count);  // persistent page-locked staging buffer of the design arena
 
   int device_ = 0;
   cudaStream_t stream_ = nullptr;
@@ -149,6 +150,8 @@ class Engine {
   DevBuf<int> d_lr_status_;
   DevBuf<int> d_perms_;
 
+  double* h_arena_ = nullptr;
+  size_t h_arena_cap_ = 0;
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;
   cudaEvent_t ev_[6] = {};

@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--count", type=int, default=4096)
     ap.add_argument("--plain-sample", type=int, default=256)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -282,7 +282,10 @@ def run_ours(args, world, rank, local, pg):
         raise RuntimeError("plain and batched forms disagree")
     plain_rate = len(sample) / (plain_ms / 1e3)
 
-    # end to end through the public call: host data in, records out
+    # end to end through the public call: host data in, records out.  One
+    # untimed call first: it creates the engine's device buffers and pinned
+    # staging (one-time per process), like CUDA context creation.
+    fk.ci_level_batch(X, triples, device=local)
     e2e_t = []
     e2e_stats = None
     for _ in range(max(1, args.e2e_steps)):
@@ -320,7 +323,7 @@ def run_ours(args, world, rank, local, pg):
                              "sample": f"first {cpu_n} triples of the batch, numpy oracle in {cores} spawned "
                                        f"processes ({cpu_dt:.1f} s)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": e2e_stats["h2d_bytes"],
-                    "d2h_bytes_per_step": e2e_stats["d2h_bytes"], "steps": len(e2e_t),
+                    "d2h_bytes_per_step": e2e_stats["d2h_bytes"], "steps": len(e2e_t), "warmup_calls": 1,
                     "setup_ms": e2e_stats["setup_ms"], "wall_s": statistics.median(e2e_t)},
             "skeleton_351x48": skel,
             "gpu_launches": int(st["kernel_launches"]) * args.steps,

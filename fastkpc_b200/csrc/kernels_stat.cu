@@ -429,14 +429,37 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
     double* vj = V + static_cast<int64_t>(n) * j;
     for (int i = tid; i < n; i += blockDim.x) qv[i] = vj[i];
     __syncthreads();
-    // w = D q, D_ij = |r_i - r_j|
+    // w = D q, D_ij = |r_i - r_j|: two rows per thread, four chains each
     double part = 0.0;
-    for (int i = tid; i < n; i += blockDim.x) {
-      const double ri = r[i];
-      double s = 0.0;
-      for (int t = 0; t < n; ++t) s += fabs(ri - r[t]) * qv[t];
-      w[i] = s;
-      part += s * qv[i];
+    for (int i0 = tid; i0 < n; i0 += 2 * blockDim.x) {
+      const int i1 = i0 + blockDim.x;
+      const double ra = r[i0], rb = i1 < n ? r[i1] : 0.0;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+      int t = 0;
+      for (; t + 3 < n; t += 4) {
+        const double x0 = r[t], x1 = r[t + 1], x2 = r[t + 2], x3 = r[t + 3];
+        const double q0 = qv[t], q1 = qv[t + 1], q2 = qv[t + 2], q3 = qv[t + 3];
+        a0 += fabs(ra - x0) * q0;
+        a1 += fabs(ra - x1) * q1;
+        a2 += fabs(ra - x2) * q2;
+        a3 += fabs(ra - x3) * q3;
+        b0 += fabs(rb - x0) * q0;
+        b1 += fabs(rb - x1) * q1;
+        b2 += fabs(rb - x2) * q2;
+        b3 += fabs(rb - x3) * q3;
+      }
+      for (; t < n; ++t) {
+        a0 += fabs(ra - r[t]) * qv[t];
+        b0 += fabs(rb - r[t]) * qv[t];
+      }
+      const double sa = (a0 + a1) + (a2 + a3);
+      w[i0] = sa;
+      part += sa * qv[i0];
+      if (i1 < n) {
+        const double sb = (b0 + b1) + (b2 + b3);
+        w[i1] = sb;
+        part += sb * qv[i1];
+      }
     }
     const double alpha = block_sum256(part, ls.red);
     const double bprev = j > 0 ? ls.beta[j - 1] : 0.0;
@@ -511,24 +534,29 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
       }
       __syncthreads();
       if (tid == 0) {
-        // kk largest |theta| among distinct indices (ties toward the higher index)
+        // kk largest |theta| among distinct indices (ties toward the higher
+        // index).  cand[c] holds the Ritz value of rank m-1-c (descending),
+        // cand[kk+c] that of rank c (ascending): merge the two ends.
+        int top = 0, bot = 0;  // next candidate from each end
         for (int c = 0; c < kk; ++c) {
-          int best = -1;
-          for (int u = 0; u < 2 * kk; ++u) {
-            const int id = ls.cand_idx[u];
-            if (id < 0) continue;
-            bool used = false;
-            for (int v = 0; v < c; ++v)
-              if (ls.sel[v] == id) used = true;
-            for (int v = 0; v < u; ++v)
-              if (ls.cand_idx[v] == id) used = true;  // duplicate index from the other end
-            if (used) continue;
-            if (best < 0 || fabs(ls.cand[u]) > fabs(ls.cand[best]) ||
-                (fabs(ls.cand[u]) == fabs(ls.cand[best]) && id > ls.cand_idx[best]))
-              best = u;
+          const int it = m - 1 - top, ib = bot;
+          bool take_top;
+          if (top >= kk || it < 0) take_top = false;
+          else if (bot >= kk || ib >= m || ib > it) take_top = true;
+          else if (it == ib) take_top = true;  // the two ends met: one value left
+          else {
+            const double ft = fabs(ls.cand[top]), fb = fabs(ls.cand[kk + bot]);
+            take_top = ft > fb || (ft == fb && it > ib);
           }
-          ls.sel[c] = ls.cand_idx[best];
-          ls.theta[c] = ls.cand[best];
+          if (take_top) {
+            ls.sel[c] = it;
+            ls.theta[c] = ls.cand[top];
+            ++top;
+          } else {
+            ls.sel[c] = ib;
+            ls.theta[c] = ls.cand[kk + bot];
+            ++bot;
+          }
         }
       }
       __syncthreads();

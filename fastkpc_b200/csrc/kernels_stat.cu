@@ -371,10 +371,46 @@ struct LanczosShared {
   int sel[64];
   double coef[kLanczosMax];
   double red[kStatThreads / 32];
+  double scan[2 * (kStatThreads / 32)];
   int done;
   int steps;
   int fail;
 };
+
+// Exclusive prefix sums over the block of two per-thread values (thread
+// order), with the block totals; every thread sums the warp totals in the
+// same order, so the totals agree bit for bit.
+__device__ void block_exscan2(double a, double c, double* scan, double* ea, double* ec, double* ta, double* tc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double ia = a, ic = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const double x = __shfl_up_sync(0xffffffffu, ia, o);
+    const double y = __shfl_up_sync(0xffffffffu, ic, o);
+    if (lane >= o) {
+      ia += x;
+      ic += y;
+    }
+  }
+  __syncthreads();
+  if (lane == 31) {
+    scan[warp] = ia;
+    scan[nw + warp] = ic;
+  }
+  __syncthreads();
+  double oa = 0.0, oc = 0.0, sa = 0.0, sc = 0.0;
+  for (int w = 0; w < nw; ++w) {
+    if (w < warp) {
+      oa += scan[w];
+      oc += scan[nw + w];
+    }
+    sa += scan[w];
+    sc += scan[nw + w];
+  }
+  *ea = oa + ia - a;
+  *ec = oc + ic - c;
+  *ta = sa;
+  *tc = sc;
+}
 
 }  // namespace
 
@@ -401,6 +437,7 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
   double* r = sm;
   double* qv = sm + n;
   double* w = sm + 2 * n;
+  int* perm = reinterpret_cast<int*>(sm + 3 * n);  // sorted position -> sample index
   const int64_t per = static_cast<int64_t>(n) * (kLanczosMax + 1) + static_cast<int64_t>(kLanczosMax) * 64 +
                       static_cast<int64_t>(64) * 5 * kLanczosMax;
   double* V = workspace + per * blockIdx.x;
@@ -408,20 +445,42 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
   double* scratch = S + static_cast<int64_t>(kLanczosMax) * 64;
   const double* src = residuals + static_cast<int64_t>(n) * comp_cols[comp];
   for (int i = tid; i < n; i += blockDim.x) r[i] = src[i];
+  __syncthreads();
+  // Sort the residual once (rank sort on (value, index); NaN ranks as +Inf so
+  // the ranks stay a permutation): the whole Lanczos runs in the sorted basis,
+  // where D q is two prefix sums.  Eigenvectors are put back in sample order
+  // on output.
+  for (int i = tid; i < n; i += blockDim.x) {
+    const double ri = isnan(r[i]) ? INFINITY : r[i];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const double rj = isnan(r[j]) ? INFINITY : r[j];
+      rank += (rj < ri || (rj == ri && j < i)) ? 1 : 0;
+    }
+    perm[rank] = i;
+  }
+  __syncthreads();
+  for (int pos = tid; pos < n; pos += blockDim.x) w[pos] = r[perm[pos]];
+  __syncthreads();
+  for (int pos = tid; pos < n; pos += blockDim.x) r[pos] = w[pos];
   if (tid == 0) {
     ls.done = 0;
     ls.fail = 0;
     ls.steps = 0;
     unsigned long state = 1;
     double nrm = 0.0;
-    for (int i = 0; i < n; ++i) {
+    for (int i = 0; i < n; ++i) {  // start vector in sample order
       state = (state * 106UL + 1283UL) % 6075UL;
       const double v = static_cast<double>(state) / 6075.0 - 0.5;
-      V[i] = v;
+      qv[i] = v;
       nrm += v * v;
     }
-    nrm = sqrt(nrm);
-    for (int i = 0; i < n; ++i) V[i] /= nrm;
+    ls.scan[0] = sqrt(nrm);
+  }
+  __syncthreads();
+  {
+    const double nrm = ls.scan[0];
+    for (int pos = tid; pos < n; pos += blockDim.x) V[pos] = qv[perm[pos]] / nrm;
   }
   __syncthreads();
   double anorm = 0.0;
@@ -429,36 +488,26 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
     double* vj = V + static_cast<int64_t>(n) * j;
     for (int i = tid; i < n; i += blockDim.x) qv[i] = vj[i];
     __syncthreads();
-    // w = D q, D_ij = |r_i - r_j|: two rows per thread, four chains each
+    // w = D q, D_kl = |r_k - r_l| with r sorted: with a_k and c_k the
+    // exclusive prefix sums of q and r.q, (D q)_k = r_k (2 a_k - A) + (C - 2 c_k)
+    // (A, C the totals); each thread scans a contiguous chunk.
     double part = 0.0;
-    for (int i0 = tid; i0 < n; i0 += 2 * blockDim.x) {
-      const int i1 = i0 + blockDim.x;
-      const double ra = r[i0], rb = i1 < n ? r[i1] : 0.0;
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
-      int t = 0;
-      for (; t + 3 < n; t += 4) {
-        const double x0 = r[t], x1 = r[t + 1], x2 = r[t + 2], x3 = r[t + 3];
-        const double q0 = qv[t], q1 = qv[t + 1], q2 = qv[t + 2], q3 = qv[t + 3];
-        a0 += fabs(ra - x0) * q0;
-        a1 += fabs(ra - x1) * q1;
-        a2 += fabs(ra - x2) * q2;
-        a3 += fabs(ra - x3) * q3;
-        b0 += fabs(rb - x0) * q0;
-        b1 += fabs(rb - x1) * q1;
-        b2 += fabs(rb - x2) * q2;
-        b3 += fabs(rb - x3) * q3;
+    {
+      const int ept = (n + blockDim.x - 1) / blockDim.x;
+      const int k0 = min(n, tid * ept), k1 = min(n, k0 + ept);
+      double sa = 0.0, sc = 0.0;
+      for (int pos = k0; pos < k1; ++pos) {
+        sa += qv[pos];
+        sc += r[pos] * qv[pos];
       }
-      for (; t < n; ++t) {
-        a0 += fabs(ra - r[t]) * qv[t];
-        b0 += fabs(rb - r[t]) * qv[t];
-      }
-      const double sa = (a0 + a1) + (a2 + a3);
-      w[i0] = sa;
-      part += sa * qv[i0];
-      if (i1 < n) {
-        const double sb = (b0 + b1) + (b2 + b3);
-        w[i1] = sb;
-        part += sb * qv[i1];
+      double ea, ec, ta, tc;
+      block_exscan2(sa, sc, ls.scan, &ea, &ec, &ta, &tc);
+      for (int pos = k0; pos < k1; ++pos) {
+        const double v = r[pos] * (2.0 * ea - ta) + (tc - 2.0 * ec);
+        w[pos] = v;
+        part += v * qv[pos];
+        ea += qv[pos];
+        ec += r[pos] * qv[pos];
       }
     }
     const double alpha = block_sum256(part, ls.red);
@@ -607,7 +656,7 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
       part += s;
     }
     const double mean = block_sum256(part, ls.red) / static_cast<double>(n);
-    for (int i = tid; i < n; i += blockDim.x) vout[i + static_cast<int64_t>(n) * c] = w[i] - mean;
+    for (int i = tid; i < n; i += blockDim.x) vout[perm[i] + static_cast<int64_t>(n) * c] = w[i] - mean;
     __syncthreads();
   }
   if (tid < k) vals[static_cast<int64_t>(k) * slot + tid] = ls.theta[tid];
@@ -1025,6 +1074,9 @@ cudaError_t launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st
 
 // ------------------------------------------------------------- launchers
 
+// legacy Lanczos: r (sorted), q, w (n doubles each) and the sort permutation (n ints)
+size_t legacy_smem_bytes(int n) { return sizeof(double) * 3 * static_cast<size_t>(n) + sizeof(int) * static_cast<size_t>(n); }
+
 cudaError_t configure_stat_kernels(int n) {
   const int s2 = static_cast<int>(sizeof(double) * 2 * n);
   const int s3 = static_cast<int>(sizeof(double) * 3 * n);
@@ -1033,7 +1085,9 @@ cudaError_t configure_stat_kernels(int n) {
   if ((e = cudaFuncSetAttribute(dcov_component_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s2)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(dcov_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s4)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(dcc_perm_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s4)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(legacy_eigen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s3)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(legacy_eigen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(legacy_smem_bytes(n)))) != cudaSuccess)
+    return e;
   return cudaFuncSetAttribute(hsic_component_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, s3);
 }
 
@@ -1073,7 +1127,7 @@ cudaError_t launch_legacy_eigen(const double* residuals, int n, const int* comp_
                                 double* lowrank_vals, double* lowrank_vecs, int* status, cudaStream_t stream) {
   if (cap <= 0 || ctas <= 0) return cudaSuccess;
   if (num_col > 64) return cudaErrorInvalidValue;
-  const size_t smem = sizeof(double) * 3 * n;
+  const size_t smem = legacy_smem_bytes(n);
   legacy_eigen_kernel<<<ctas, kStatThreads, smem, stream>>>(residuals, n, comp_cols, guard, slot_comps, cap,
                                                              num_col, workspace, lowrank_vals, lowrank_vecs, status);
   return cudaGetLastError();

@@ -525,19 +525,52 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
     for (int i = tid; i < n; i += blockDim.x) before += w[i] * w[i];
     before = block_sum256(before, ls.red);
     for (int pass = 0; pass < 2; ++pass) {
-      const int warp = tid >> 5, lane = tid & 31;
-      for (int b = warp; b <= j; b += blockDim.x >> 5) {
-        const double* vb = V + static_cast<int64_t>(n) * b;
-        double s = 0.0;
-        for (int i = lane; i < n; i += 32) s += w[i] * vb[i];
-        s = warp_sum(s);
-        if (lane == 0) ls.coef[b] = s;
+      // coefficients V(:, b)'w: each warp takes four basis vectors per pass so
+      // that their L2 loads overlap
+      const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
+      for (int b0 = 4 * warp; b0 <= j; b0 += 4 * nwarps) {
+        const double* v0 = V + static_cast<int64_t>(n) * b0;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        const bool h1 = b0 + 1 <= j, h2 = b0 + 2 <= j, h3 = b0 + 3 <= j;
+#pragma unroll 4
+        for (int i = lane; i < n; i += 32) {
+          const double wi = w[i];
+          const double x0 = v0[i];
+          const double x1 = h1 ? v0[i + n] : 0.0;
+          const double x2 = h2 ? v0[i + 2 * static_cast<int64_t>(n)] : 0.0;
+          const double x3 = h3 ? v0[i + 3 * static_cast<int64_t>(n)] : 0.0;
+          s0 += wi * x0;
+          s1 += wi * x1;
+          s2 += wi * x2;
+          s3 += wi * x3;
+        }
+        s0 = warp_sum(s0);
+        s1 = warp_sum(s1);
+        s2 = warp_sum(s2);
+        s3 = warp_sum(s3);
+        if (lane == 0) {
+          ls.coef[b0] = s0;
+          if (h1) ls.coef[b0 + 1] = s1;
+          if (h2) ls.coef[b0 + 2] = s2;
+          if (h3) ls.coef[b0 + 3] = s3;
+        }
       }
       __syncthreads();
       double after = 0.0;
       for (int i = tid; i < n; i += blockDim.x) {
-        double s = w[i];
-        for (int b = 0; b <= j; ++b) s -= ls.coef[b] * V[i + static_cast<int64_t>(n) * b];
+        double s0 = w[i], s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int b = 0;
+        for (; b + 7 <= j; b += 8) {  // eight independent basis loads in flight
+          double x[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) x[u] = V[i + static_cast<int64_t>(n) * (b + u)];
+          s0 -= ls.coef[b] * x[0] + ls.coef[b + 4] * x[4];
+          s1 -= ls.coef[b + 1] * x[1] + ls.coef[b + 5] * x[5];
+          s2 -= ls.coef[b + 2] * x[2] + ls.coef[b + 6] * x[6];
+          s3 -= ls.coef[b + 3] * x[3] + ls.coef[b + 7] * x[7];
+        }
+        for (; b <= j; ++b) s0 -= ls.coef[b] * V[i + static_cast<int64_t>(n) * b];
+        const double s = (s0 + s1) + (s2 + s3);
         w[i] = s;
         after += s * s;
       }
@@ -646,17 +679,45 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
   const int m = ls.steps;
   // order selected values descending (the order does not change any statistic)
   double* vout = vecs + static_cast<int64_t>(n) * k * slot;
-  for (int c = 0; c < k; ++c) {
-    const double* x = S + static_cast<int64_t>(kLanczosMax) * c;
-    double part = 0.0;
+  // Ritz vectors V x_c, five per pass over the basis, centred, back in sample order
+  constexpr int kC = 5;
+  for (int c0 = 0; c0 < k; c0 += kC) {
+    double part[kC];
+#pragma unroll
+    for (int u = 0; u < kC; ++u) part[u] = 0.0;
     for (int i = tid; i < n; i += blockDim.x) {
-      double s = 0.0;
-      for (int b = 0; b < m; ++b) s += V[i + static_cast<int64_t>(n) * b] * x[b];
-      w[i] = s;
-      part += s;
+      double acc[kC];
+#pragma unroll
+      for (int u = 0; u < kC; ++u) acc[u] = 0.0;
+      int b = 0;
+      for (; b + 7 < m; b += 8) {  // eight basis loads in flight
+        double vb[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) vb[t] = V[i + static_cast<int64_t>(n) * (b + t)];
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+#pragma unroll
+          for (int u = 0; u < kC; ++u)
+            if (c0 + u < k) acc[u] += vb[t] * S[static_cast<int64_t>(kLanczosMax) * (c0 + u) + b + t];
+      }
+      for (; b < m; ++b) {
+        const double vb = V[i + static_cast<int64_t>(n) * b];
+#pragma unroll
+        for (int u = 0; u < kC; ++u)
+          if (c0 + u < k) acc[u] += vb * S[static_cast<int64_t>(kLanczosMax) * (c0 + u) + b];
+      }
+#pragma unroll
+      for (int u = 0; u < kC; ++u) {
+        if (c0 + u < k) vout[perm[i] + static_cast<int64_t>(n) * (c0 + u)] = acc[u];
+        part[u] += acc[u];
+      }
     }
-    const double mean = block_sum256(part, ls.red) / static_cast<double>(n);
-    for (int i = tid; i < n; i += blockDim.x) vout[perm[i] + static_cast<int64_t>(n) * c] = w[i] - mean;
+#pragma unroll
+    for (int u = 0; u < kC; ++u) {
+      const double mean = block_sum256(part[u], ls.red) / static_cast<double>(n);
+      if (c0 + u < k)
+        for (int i = tid; i < n; i += blockDim.x) vout[perm[i] + static_cast<int64_t>(n) * (c0 + u)] -= mean;
+    }
     __syncthreads();
   }
   if (tid < k) vals[static_cast<int64_t>(k) * slot + tid] = ls.theta[tid];

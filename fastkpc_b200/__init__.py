@@ -330,7 +330,7 @@ def ci_plain_one(data, x, y, S, ci_method="dcc.gamma", **kw):
     return {name: getattr(rec, name) for name, _ in CiRecord._fields_}
 
 
-def regress_batch(data, fits, max_penalties=8, device=0, selection="magic"):
+def regress_batch(data, fits, max_penalties=12, device=0, selection="magic"):
     """regrXonS residuals for ``[(target, S), ...]``: (residuals n x k, log_sp k x m, status k).
 
     ``selection``: "magic" (mgcv magic's search, as the reference) or
@@ -375,7 +375,7 @@ def stat_batch(residuals, pairs, ci_method="dcc.gamma", permutations=None, **kw)
 
 
 STAGES = {"fit_single": 0, "fit_multi_small": 1, "fit_multi_large": 2, "dcov_components": 3, "dcov_pairs": 4,
-          "hsic_components": 5, "hsic_pairs": 6, "lowrank_eigen": 7, "lowrank_pairs": 8}
+          "hsic_components": 5, "hsic_pairs": 6, "lowrank_eigen": 7, "lowrank_pairs": 8, "fit_multi_huge": 9}
 
 
 class StagedBatch:

@@ -189,7 +189,14 @@ void add_stats(fkpc_stage_stats* acc, const fkpc_stage_stats& s) {
 void evaluate(fkpc::Engine& eng, const std::vector<fkpc::Test>& tests, const fkpc_options& opt, fkpc::RStream* rs,
               std::vector<fkpc_ci_record>* out, fkpc_stage_stats* acc) {
   out->resize(tests.size());
-  const size_t chunk = opt.mode == FKPC_MODE_PLAIN ? 1 : 16384;
+  size_t chunk = opt.mode == FKPC_MODE_PLAIN ? 1 : 16384;
+  if (opt.ci_method == FKPC_DCC_PERM || opt.ci_method == FKPC_HSIC_PERM) {
+    // permutation tables are R x n int32 per test: keep each chunk's table
+    // near 1 GiB (tests stay in order, so the seeded stream is consumed as in
+    // one pass)
+    const size_t per_test = static_cast<size_t>(opt.permutation_replicates) * static_cast<size_t>(eng.n()) * sizeof(int);
+    chunk = std::min(chunk, std::max<size_t>(1, (static_cast<size_t>(1) << 30) / std::max<size_t>(1, per_test)));
+  }
   for (size_t b = 0; b < tests.size(); b += chunk) {
     const size_t e = std::min(tests.size(), b + chunk);
     std::vector<fkpc::Test> part(tests.begin() + b, tests.begin() + e);

@@ -10,7 +10,7 @@
 
 namespace fkpc {
 
-constexpr int kMaxPenalties = 8;      // |S| <= 8 in the shared-memory multi-penalty kernel
+constexpr int kMaxPenalties = 12;     // |S| <= 12 (design widths up to q = 109)
 constexpr int kMaxSingleQ = 32;       // single-penalty designs have q in {10, 30}
 constexpr int kStatusOk = 0;
 constexpr int kStatusNumeric = 3;

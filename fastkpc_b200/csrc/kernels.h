@@ -20,17 +20,23 @@ cudaError_t launch_fit_single(const DesignDev* designs, const double* arena, con
                               const FitJob* jobs, int count, double* residuals, FitResult* results,
                               cudaStream_t stream);
 
-// qmax_class 0: q <= 40 and rank sum <= 32; 1: q <= 76 and rank sum <= 64.
+// qmax_class 0: q <= 40 and rank sum <= 32 (warp per fit); 1: q <= 76 and rank sum <= 64;
+// 2: q <= 112 and rank sum <= 96 (working set in global memory).
 // Score, gradient, Gauss-Newton and exact Hessian of GCV in log(lambda) at
 // ``count`` points (rho: count x m) for design ``design`` and response y.
-// qmax_class 0: q <= kWarpQ, rsum <= kWarpR, m <= kWarpM; 1: q <= 76, rsum <= 64.
+// qmax_class 0: q <= kWarpQ, rsum <= kWarpR, m <= kWarpM; 1: q <= 76, rsum <= 64;
+// 2: q <= 112, rsum <= 96 with ``workspace`` (multi_workspace_doubles(2, count)).
 cudaError_t launch_gcv_adjoint(int qmax_class, const DesignDev* designs, int design, const double* arena,
                                const double* y, int n, const double* rho, int count, double* score, double* grad,
-                               double* gn, double* hess, int* status, cudaStream_t stream);
+                               double* gn, double* hess, int* status, cudaStream_t stream,
+                               double* workspace = nullptr);
 cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const double* arena, const double* data,
                              int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
                              FitResult* results, cudaStream_t stream,
-                             int selection = 0);
+                             int selection = 0, double* workspace = nullptr);
+// Doubles of global workspace class ``qmax_class`` needs for ``count`` fits
+// (class 2: q <= 112, rsum <= 96, working set in global memory; 0 otherwise).
+size_t multi_workspace_doubles(int qmax_class, int count);
 
 // dCov: per component centring constants and moments, then per pair statistic
 // and gamma p-value.  comp_cols[c] is the residual column of component c.

@@ -300,6 +300,7 @@ struct MultiLayout {
 };
 
 struct MultiScalars {
+  static constexpr int kLd = kMaxPenalties;  // leading dimension of the m x m matrices
   double beta[2], v0[2];
   double red[kMultiThreads / 32];
   double score, rss, edf, yy;
@@ -615,60 +616,60 @@ __device__ void newton_from_hessian_eigen(int m, S* sc, bool* steepest) {
   double* v = sc->jv;
   for (int j = 0; j < m; ++j)
     for (int i = 0; i < m; ++i) {
-      a[i + kMaxPenalties * j] = sc->hess_c[i + kMaxPenalties * j];
-      v[i + kMaxPenalties * j] = i == j ? 1.0 : 0.0;
+      a[i + S::kLd * j] = sc->hess_c[i + S::kLd * j];
+      v[i + S::kLd * j] = i == j ? 1.0 : 0.0;
     }
   for (int sweep = 0; sweep < 60; ++sweep) {
     double off = 0.0, dg = 0.0;
     for (int j = 0; j < m; ++j)
       for (int i = 0; i < m; ++i) {
-        const double x = a[i + kMaxPenalties * j];
+        const double x = a[i + S::kLd * j];
         if (i == j) dg += x * x;
         else off += x * x;
       }
     if (off == 0.0 || off <= 1e-32 * dg) break;
     for (int p = 0; p < m - 1; ++p)
       for (int r = p + 1; r < m; ++r) {
-        const double apq = a[p + kMaxPenalties * r];
+        const double apq = a[p + S::kLd * r];
         if (apq == 0.0) continue;
-        const double theta = (a[r + kMaxPenalties * r] - a[p + kMaxPenalties * p]) / (2.0 * apq);
+        const double theta = (a[r + S::kLd * r] - a[p + S::kLd * p]) / (2.0 * apq);
         const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
         const double c = 1.0 / sqrt(t * t + 1.0);
         const double s = t * c;
         for (int k = 0; k < m; ++k) {
-          const double akp = a[k + kMaxPenalties * p], akq = a[k + kMaxPenalties * r];
-          a[k + kMaxPenalties * p] = c * akp - s * akq;
-          a[k + kMaxPenalties * r] = s * akp + c * akq;
+          const double akp = a[k + S::kLd * p], akq = a[k + S::kLd * r];
+          a[k + S::kLd * p] = c * akp - s * akq;
+          a[k + S::kLd * r] = s * akp + c * akq;
         }
         for (int k = 0; k < m; ++k) {
-          const double apk = a[p + kMaxPenalties * k], aqk = a[r + kMaxPenalties * k];
-          a[p + kMaxPenalties * k] = c * apk - s * aqk;
-          a[r + kMaxPenalties * k] = s * apk + c * aqk;
+          const double apk = a[p + S::kLd * k], aqk = a[r + S::kLd * k];
+          a[p + S::kLd * k] = c * apk - s * aqk;
+          a[r + S::kLd * k] = s * apk + c * aqk;
         }
-        a[p + kMaxPenalties * r] = 0.0;
-        a[r + kMaxPenalties * p] = 0.0;
+        a[p + S::kLd * r] = 0.0;
+        a[r + S::kLd * p] = 0.0;
         for (int k = 0; k < m; ++k) {
-          const double vkp = v[k + kMaxPenalties * p], vkq = v[k + kMaxPenalties * r];
-          v[k + kMaxPenalties * p] = c * vkp - s * vkq;
-          v[k + kMaxPenalties * r] = s * vkp + c * vkq;
+          const double vkp = v[k + S::kLd * p], vkq = v[k + S::kLd * r];
+          v[k + S::kLd * p] = c * vkp - s * vkq;
+          v[k + S::kLd * r] = s * vkp + c * vkq;
         }
       }
   }
   bool neg = false;
   for (int j = 0; j < m; ++j)
-    if (a[j + kMaxPenalties * j] < 0.0) neg = true;
+    if (a[j + S::kLd * j] < 0.0) neg = true;
   *steepest = neg;
   if (!neg) {
     double proj[kMaxPenalties];
     for (int c = 0; c < m; ++c) {
       double s = 0.0;
-      for (int r = 0; r < m; ++r) s += v[r + kMaxPenalties * c] * sc->gradient[r];
-      proj[c] = s / a[c + kMaxPenalties * c];
+      for (int r = 0; r < m; ++r) s += v[r + S::kLd * c] * sc->gradient[r];
+      proj[c] = s / a[c + S::kLd * c];
     }
     double mx = 0.0;
     for (int r = 0; r < m; ++r) {
       double s = 0.0;
-      for (int c = 0; c < m; ++c) s += v[r + kMaxPenalties * c] * proj[c];
+      for (int c = 0; c < m; ++c) s += v[r + S::kLd * c] * proj[c];
       sc->newton[r] = -s;
       mx = fmax(mx, fabs(sc->newton[r]));
     }
@@ -689,22 +690,22 @@ template <class S>
 __device__ void newton_from_hessian(int m, S* sc, bool* steepest) {
   double* Lm = sc->ja;
   for (int c = 0; c < m; ++c)
-    for (int r = 0; r < m; ++r) Lm[r + kMaxPenalties * c] = sc->hess_c[r + kMaxPenalties * c];
+    for (int r = 0; r < m; ++r) Lm[r + S::kLd * c] = sc->hess_c[r + S::kLd * c];
   bool pd = true;
   for (int c = 0; c < m && pd; ++c) {
-    double d = Lm[c + kMaxPenalties * c];
-    for (int k = 0; k < c; ++k) d -= Lm[c + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
+    double d = Lm[c + S::kLd * c];
+    for (int k = 0; k < c; ++k) d -= Lm[c + S::kLd * k] * Lm[c + S::kLd * k];
     if (!(d > 0.0)) {
       pd = false;
       break;
     }
     d = sqrt(d);
-    Lm[c + kMaxPenalties * c] = d;
+    Lm[c + S::kLd * c] = d;
     const double inv = 1.0 / d;
     for (int r = c + 1; r < m; ++r) {
-      double s = Lm[r + kMaxPenalties * c];
-      for (int k = 0; k < c; ++k) s -= Lm[r + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
-      Lm[r + kMaxPenalties * c] = s * inv;
+      double s = Lm[r + S::kLd * c];
+      for (int k = 0; k < c; ++k) s -= Lm[r + S::kLd * k] * Lm[c + S::kLd * k];
+      Lm[r + S::kLd * c] = s * inv;
     }
   }
   if (!pd) {
@@ -715,14 +716,14 @@ __device__ void newton_from_hessian(int m, S* sc, bool* steepest) {
   double z[kMaxPenalties];
   for (int r = 0; r < m; ++r) {
     double s = -sc->gradient[r];
-    for (int k = 0; k < r; ++k) s -= Lm[r + kMaxPenalties * k] * z[k];
-    z[r] = s / Lm[r + kMaxPenalties * r];
+    for (int k = 0; k < r; ++k) s -= Lm[r + S::kLd * k] * z[k];
+    z[r] = s / Lm[r + S::kLd * r];
   }
   double mx = 0.0;
   for (int r = m - 1; r >= 0; --r) {
     double s = z[r];
-    for (int k = r + 1; k < m; ++k) s -= Lm[k + kMaxPenalties * r] * z[k];
-    z[r] = s / Lm[r + kMaxPenalties * r];
+    for (int k = r + 1; k < m; ++k) s -= Lm[k + S::kLd * r] * z[k];
+    z[r] = s / Lm[r + S::kLd * r];
     mx = fmax(mx, fabs(z[r]));
   }
   for (int r = 0; r < m; ++r) sc->newton[r] = mx > 5.0 ? z[r] * (5.0 / mx) : z[r];
@@ -740,34 +741,34 @@ __device__ int polish_step(int m, S* sc) {
   int act[kMaxPenalties];
   int na = 0;
   for (int j = 0; j < m; ++j)
-    if (sc->hess_c[j + kMaxPenalties * j] > kPolishCurvature * sc->score) act[na++] = j;
+    if (sc->hess_c[j + S::kLd * j] > kPolishCurvature * sc->score) act[na++] = j;
   if (na == 0) return 0;
   double* Lm = sc->ja;
   for (int c = 0; c < na; ++c)
-    for (int r = 0; r < na; ++r) Lm[r + kMaxPenalties * c] = sc->hess_c[act[r] + kMaxPenalties * act[c]];
+    for (int r = 0; r < na; ++r) Lm[r + S::kLd * c] = sc->hess_c[act[r] + S::kLd * act[c]];
   for (int c = 0; c < na; ++c) {
-    double d = Lm[c + kMaxPenalties * c];
-    for (int k = 0; k < c; ++k) d -= Lm[c + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
+    double d = Lm[c + S::kLd * c];
+    for (int k = 0; k < c; ++k) d -= Lm[c + S::kLd * k] * Lm[c + S::kLd * k];
     if (!(d > 0.0)) return 0;
     d = sqrt(d);
-    Lm[c + kMaxPenalties * c] = d;
+    Lm[c + S::kLd * c] = d;
     for (int r = c + 1; r < na; ++r) {
-      double s = Lm[r + kMaxPenalties * c];
-      for (int k = 0; k < c; ++k) s -= Lm[r + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
-      Lm[r + kMaxPenalties * c] = s / d;
+      double s = Lm[r + S::kLd * c];
+      for (int k = 0; k < c; ++k) s -= Lm[r + S::kLd * k] * Lm[c + S::kLd * k];
+      Lm[r + S::kLd * c] = s / d;
     }
   }
   double z[kMaxPenalties];
   for (int r = 0; r < na; ++r) {
     double s = -sc->grad_c[act[r]];
-    for (int k = 0; k < r; ++k) s -= Lm[r + kMaxPenalties * k] * z[k];
-    z[r] = s / Lm[r + kMaxPenalties * r];
+    for (int k = 0; k < r; ++k) s -= Lm[r + S::kLd * k] * z[k];
+    z[r] = s / Lm[r + S::kLd * r];
   }
   double mx = 0.0;
   for (int r = na - 1; r >= 0; --r) {
     double s = z[r];
-    for (int k = r + 1; k < na; ++k) s -= Lm[k + kMaxPenalties * r] * z[k];
-    z[r] = s / Lm[r + kMaxPenalties * r];
+    for (int k = r + 1; k < na; ++k) s -= Lm[k + S::kLd * r] * z[k];
+    z[r] = s / Lm[r + S::kLd * r];
     mx = fmax(mx, fabs(z[r]));
   }
   if (mx > kPolishMaxStep) return 0;
@@ -779,34 +780,34 @@ __device__ int polish_step(int m, S* sc) {
 // column-major with leading dimension kMaxPenalties) on the coordinates
 // whose bit in ``fixed`` is clear; fixed coordinates get z = 0.  False when
 // the factor does not exist.
-__device__ bool chol_solve_neg(int m, const double* A, double mu, const double* g, unsigned fixed, double* Lm,
-                               double* z) {
+__device__ bool chol_solve_neg(int m, int ld, const double* A, double mu, const double* g, unsigned fixed,
+                               double* Lm, double* z) {
   for (int c = 0; c < m; ++c)
     for (int r = 0; r < m; ++r) {
       const bool fr = (fixed >> r) & 1u, fc = (fixed >> c) & 1u;
-      Lm[r + kMaxPenalties * c] = (fr || fc) ? (r == c ? 1.0 : 0.0) : A[r + kMaxPenalties * c] + (r == c ? mu : 0.0);
+      Lm[r + ld * c] = (fr || fc) ? (r == c ? 1.0 : 0.0) : A[r + ld * c] + (r == c ? mu : 0.0);
     }
   for (int c = 0; c < m; ++c) {
-    double d = Lm[c + kMaxPenalties * c];
-    for (int k = 0; k < c; ++k) d -= Lm[c + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
+    double d = Lm[c + ld * c];
+    for (int k = 0; k < c; ++k) d -= Lm[c + ld * k] * Lm[c + ld * k];
     if (!(d > 0.0)) return false;
     d = sqrt(d);
-    Lm[c + kMaxPenalties * c] = d;
+    Lm[c + ld * c] = d;
     for (int r = c + 1; r < m; ++r) {
-      double v = Lm[r + kMaxPenalties * c];
-      for (int k = 0; k < c; ++k) v -= Lm[r + kMaxPenalties * k] * Lm[c + kMaxPenalties * k];
-      Lm[r + kMaxPenalties * c] = v / d;
+      double v = Lm[r + ld * c];
+      for (int k = 0; k < c; ++k) v -= Lm[r + ld * k] * Lm[c + ld * k];
+      Lm[r + ld * c] = v / d;
     }
   }
   for (int r = 0; r < m; ++r) {
     double v = ((fixed >> r) & 1u) ? 0.0 : -g[r];
-    for (int k = 0; k < r; ++k) v -= Lm[r + kMaxPenalties * k] * z[k];
-    z[r] = v / Lm[r + kMaxPenalties * r];
+    for (int k = 0; k < r; ++k) v -= Lm[r + ld * k] * z[k];
+    z[r] = v / Lm[r + ld * r];
   }
   for (int r = m - 1; r >= 0; --r) {
     double v = z[r];
-    for (int k = r + 1; k < m; ++k) v -= Lm[k + kMaxPenalties * r] * z[k];
-    z[r] = v / Lm[r + kMaxPenalties * r];
+    for (int k = r + 1; k < m; ++k) v -= Lm[k + ld * r] * z[k];
+    z[r] = v / Lm[r + ld * r];
   }
   return true;
 }
@@ -815,12 +816,12 @@ __device__ bool chol_solve_neg(int m, const double* A, double mu, const double* 
 // free coordinates (see gn_step).  False when no factor exists.
 template <class S>
 __device__ bool gn_solve(int m, S* sc, unsigned fixed, double* z) {
-  if (chol_solve_neg(m, sc->hess_c, 0.0, sc->grad_c, fixed, sc->ja, z)) return true;
+  if (chol_solve_neg(m, S::kLd, sc->hess_c, 0.0, sc->grad_c, fixed, sc->ja, z)) return true;
   double dmax = 0.0;
-  for (int j = 0; j < m; ++j) dmax = fmax(dmax, fabs(sc->gn_c[j + kMaxPenalties * j]));
+  for (int j = 0; j < m; ++j) dmax = fmax(dmax, fabs(sc->gn_c[j + S::kLd * j]));
   double mu = 0.0;
   for (int attempt = 0; attempt < 12; ++attempt) {
-    if (chol_solve_neg(m, sc->gn_c, mu, sc->grad_c, fixed, sc->ja, z)) return true;
+    if (chol_solve_neg(m, S::kLd, sc->gn_c, mu, sc->grad_c, fixed, sc->ja, z)) return true;
     mu = mu == 0.0 ? 1e-12 * fmax(dmax, 1e-300) : mu * 100.0;
   }
   return false;
@@ -917,9 +918,11 @@ template <int QMAX, int RMAX>
 __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
     const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data,
     int n, const FitJob* __restrict__ jobs, const int* __restrict__ job_index, int job_count,
-    double* __restrict__ residuals, FitResult* __restrict__ results, int selection) {
+    double* __restrict__ residuals, FitResult* __restrict__ results, int selection, double* __restrict__ workspace) {
   using L = MultiLayout<QMAX, RMAX>;
-  extern __shared__ double sm[];
+  extern __shared__ double smem_dyn[];
+  // the widest class keeps its (~330 KB) working set in a global workspace per CTA
+  double* sm = workspace ? workspace + static_cast<int64_t>(blockIdx.x) * L::TOTAL : smem_dyn;
   __shared__ MultiScalars sc;
   __shared__ int ctl[4];
   if (blockIdx.x >= job_count) return;
@@ -1168,19 +1171,20 @@ static_assert(kWarpR == 32 && kWarpQ > 32 && kWarpQ <= 64 && kWarpQ % 4 == 0, "w
 static_assert(kWarpTri % 2 == 0 && WarpLayout::Y % 2 == 0, "16-byte copies of the packed triangle");
 
 struct WarpScalars {
+  static constexpr int kLd = kWarpM;  // leading dimension of the m x m matrices
   double beta, v0, score, rss, edf, yy;
-  double lam[kMaxPenalties];
-  double log_sp[kMaxPenalties];
-  double trial[kMaxPenalties];
-  double step[kMaxPenalties];
-  double grad_c[kMaxPenalties];
-  double gradient[kMaxPenalties];
-  double newton[kMaxPenalties];
-  double steep[kMaxPenalties];
-  double ddelta[kMaxPenalties];
-  double drss[kMaxPenalties];
-  double hess_c[kMaxPenalties * kMaxPenalties];
-  double gn_c[kMaxPenalties * kMaxPenalties];  // Gauss-Newton Hessian (adjoint entry point)
+  double lam[kWarpM];
+  double log_sp[kWarpM];
+  double trial[kWarpM];
+  double step[kWarpM];
+  double grad_c[kWarpM];
+  double gradient[kWarpM];
+  double newton[kWarpM];
+  double steep[kWarpM];
+  double ddelta[kWarpM];
+  double drss[kWarpM];
+  double hess_c[kWarpM * kWarpM];
+  double gn_c[kWarpM * kWarpM];  // Gauss-Newton Hessian (adjoint entry point)
   double* ja;  // Newton scratch (Cholesky factor / Jacobi matrix), in the Z region
   double* jv;  // Jacobi rotations, in the Z region
   int status;
@@ -1597,14 +1601,14 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
         }
         const double h = -2.0 * s1 / delta * (sc.ddelta[bj] * sc.drss[bi] + sc.ddelta[bi] * sc.drss[bj]) +
                          s1 * d2rss + 3.0 * s2 / delta * sc.ddelta[bi] * sc.ddelta[bj] - s2 * d2delta;
-        sc.hess_c[bi + kMaxPenalties * bj] = h;
-        sc.hess_c[bj + kMaxPenalties * bi] = h;
+        sc.hess_c[bi + WarpScalars::kLd * bj] = h;
+        sc.hess_c[bj + WarpScalars::kLd * bi] = h;
         // Gauss-Newton: V = |f|^2, f = sqrt(n) r / delta, dr_i . dr_j = ll a_i' D_ij a_j
         const double gn = 2.0 * s1 * ll * hs[1] -
                           s1 / delta * (sc.ddelta[bj] * sc.drss[bi] + sc.ddelta[bi] * sc.drss[bj]) +
                           s2 / delta * sc.ddelta[bi] * sc.ddelta[bj];
-        sc.gn_c[bi + kMaxPenalties * bj] = gn;
-        sc.gn_c[bj + kMaxPenalties * bi] = gn;
+        sc.gn_c[bi + WarpScalars::kLd * bj] = gn;
+        sc.gn_c[bj + WarpScalars::kLd * bi] = gn;
       }
     for (int j = 0; j < m; ++j) sc.grad_c[j] = s1 * sc.drss[j] - s2 * sc.ddelta[j];
   }
@@ -1632,7 +1636,7 @@ __device__ __noinline__ void warp_fit_setup(const DesignDev* __restrict__ design
   if (lane == 0) {
     sc.status = kStatusOk;
     sc.ja = sm + L::Z + kWarpSums;
-    sc.jv = sc.ja + kMaxPenalties * kMaxPenalties;
+    sc.jv = sc.ja + WarpScalars::kLd * WarpScalars::kLd;
   }
   __syncwarp();
   const int q = des.q, m = des.m;
@@ -1923,8 +1927,8 @@ __global__ void __launch_bounds__(32) gcv_adjoint_warp_kernel(const DesignDev* _
     for (int i = 0; i < m; ++i) {
       grad[static_cast<int64_t>(pt) * m + i] = sc.grad_c[i];
       for (int j = 0; j < m; ++j) {
-        gn[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.gn_c[i + kMaxPenalties * j];
-        hess[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.hess_c[i + kMaxPenalties * j];
+        gn[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.gn_c[i + WarpScalars::kLd * j];
+        hess[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.hess_c[i + WarpScalars::kLd * j];
       }
     }
   }
@@ -1934,8 +1938,10 @@ template <int QMAX, int RMAX>
 __global__ void __launch_bounds__(kMultiThreads, 1) gcv_adjoint_kernel(
     const DesignDev* __restrict__ designs, int design, const double* __restrict__ arena, const double* __restrict__ y,
     int n, const double* __restrict__ rho, int count, double* __restrict__ score, double* __restrict__ grad,
-    double* __restrict__ gn, double* __restrict__ hess, int* __restrict__ status) {
-  extern __shared__ double sm[];
+    double* __restrict__ gn, double* __restrict__ hess, int* __restrict__ status, double* __restrict__ workspace) {
+  using L = MultiLayout<QMAX, RMAX>;
+  extern __shared__ double smem_dyn[];
+  double* sm = workspace ? workspace + static_cast<int64_t>(blockIdx.x) * L::TOTAL : smem_dyn;
   __shared__ MultiScalars sc;
   const int pt = blockIdx.x;
   if (pt >= count) return;
@@ -1965,7 +1971,12 @@ __global__ void __launch_bounds__(kMultiThreads, 1) gcv_adjoint_kernel(
 
 size_t multi_smem_bytes(int qmax_class) {
   if (qmax_class == 0) return sizeof(double) * WarpLayout::TOTAL + sizeof(WarpScalars) + sizeof(DesignDev);
-  return sizeof(double) * MultiLayout<76, 64>::TOTAL;
+  if (qmax_class == 1) return sizeof(double) * MultiLayout<76, 64>::TOTAL;
+  return 0;  // class 2 works in global memory
+}
+
+size_t multi_workspace_doubles(int qmax_class, int count) {
+  return qmax_class == 2 ? static_cast<size_t>(MultiLayout<112, 96>::TOTAL) * static_cast<size_t>(count) : 0;
 }
 
 cudaError_t configure_fit_kernels() {
@@ -1981,14 +1992,18 @@ cudaError_t configure_fit_kernels() {
 
 cudaError_t launch_gcv_adjoint(int qmax_class, const DesignDev* designs, int design, const double* arena,
                                const double* y, int n, const double* rho, int count, double* score, double* grad,
-                               double* gn, double* hess, int* status, cudaStream_t stream) {
+                               double* gn, double* hess, int* status, cudaStream_t stream, double* workspace) {
   if (count <= 0) return cudaSuccess;
   if (qmax_class == 0) {
     gcv_adjoint_warp_kernel<<<count, 32, 0, stream>>>(designs, design, arena, y, n, rho, count, score, grad, gn, hess,
                                                       status);
-  } else {
+  } else if (qmax_class == 1) {
     gcv_adjoint_kernel<76, 64><<<count, kMultiThreads, multi_smem_bytes(1), stream>>>(
-        designs, design, arena, y, n, rho, count, score, grad, gn, hess, status);
+        designs, design, arena, y, n, rho, count, score, grad, gn, hess, status, nullptr);
+  } else {
+    if (!workspace) return cudaErrorInvalidValue;
+    gcv_adjoint_kernel<112, 96><<<count, kMultiThreads, 0, stream>>>(designs, design, arena, y, n, rho, count, score,
+                                                                      grad, gn, hess, status, workspace);
   }
   return cudaGetLastError();
 }
@@ -2005,16 +2020,18 @@ cudaError_t launch_fit_single(const DesignDev* designs, const double* arena, con
 
 cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const double* arena, const double* data,
                              int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
-                             FitResult* results, cudaStream_t stream, int selection) {
+                             FitResult* results, cudaStream_t stream, int selection, double* workspace) {
   if (count <= 0) return cudaSuccess;
-  const size_t smem = multi_smem_bytes(qmax_class);
   if (qmax_class == 0) {
     fit_multi_warp_kernel<<<count, 32, 0, stream>>>(designs, arena, data, n, jobs, job_index, count, residuals,
                                                     results, selection);
+  } else if (qmax_class == 1) {
+    fit_multi_kernel<76, 64><<<count, kMultiThreads, multi_smem_bytes(1), stream>>>(
+        designs, arena, data, n, jobs, job_index, count, residuals, results, selection, nullptr);
   } else {
-    auto k = fit_multi_kernel<76, 64>;
-    k<<<count, kMultiThreads, smem, stream>>>(designs, arena, data, n, jobs, job_index, count, residuals, results,
-                                              selection);
+    if (!workspace) return cudaErrorInvalidValue;
+    fit_multi_kernel<112, 96><<<count, kMultiThreads, 0, stream>>>(designs, arena, data, n, jobs, job_index, count,
+                                                                    residuals, results, selection, workspace);
   }
   return cudaGetLastError();
 }

@@ -237,7 +237,8 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       }
       total += static_cast<size_t>(rootoff);
       dd.rsum = rows;
-      if (des.q > 76 || rows > 64) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity");
+      if (des.q > 112 || rows > 96 || des.m > kMaxPenalties)
+        throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity (q <= 112, |S| <= 12)");
       dd.rpack = -1;
       if (des.q <= kWarpQ) {
         total += total % 2;  // 16-byte aligned: copied with 16-byte cp.async
@@ -288,17 +289,20 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   multi_jobs_.clear();
   multi_small_.clear();
   multi_large_.clear();
+  multi_huge_.clear();
   direct_cols_.clear();
   direct_slots_.clear();
   plain_single_off_.clear();
   plain_small_off_.clear();
   plain_large_off_.clear();
+  plain_huge_off_.clear();
   plain_direct_off_.clear();
   for (size_t c = 0; c < comps_.size(); ++c) {
     if (opt.mode == FKPC_MODE_PLAIN && c % 2 == 0) {
       plain_single_off_.push_back(static_cast<int>(single_jobs_.size()));
       plain_small_off_.push_back(static_cast<int>(multi_small_.size()));
       plain_large_off_.push_back(static_cast<int>(multi_large_.size()));
+      plain_huge_off_.push_back(static_cast<int>(multi_huge_.size()));
       plain_direct_off_.push_back(static_cast<int>(direct_cols_.size()));
     }
     const Component& cp = comps_[c];
@@ -315,13 +319,15 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       const int idx = static_cast<int>(multi_jobs_.size());
       multi_jobs_.push_back(job);
       if (dd.q <= kWarpQ && dd.rsum <= kWarpR && dd.m <= kWarpM) multi_small_.push_back(idx);
-      else multi_large_.push_back(idx);
+      else if (dd.q <= 76 && dd.rsum <= 64) multi_large_.push_back(idx);
+      else multi_huge_.push_back(idx);
     }
   }
   if (opt.mode == FKPC_MODE_PLAIN) {
     plain_single_off_.push_back(static_cast<int>(single_jobs_.size()));
     plain_small_off_.push_back(static_cast<int>(multi_small_.size()));
     plain_large_off_.push_back(static_cast<int>(multi_large_.size()));
+    plain_huge_off_.push_back(static_cast<int>(multi_huge_.size()));
     plain_direct_off_.push_back(static_cast<int>(direct_cols_.size()));
   }
   const size_t ncomp = comps_.size();
@@ -337,6 +343,8 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   h2d_bytes_ += upload(d_multi_jobs_, multi_jobs_, stream_);
   h2d_bytes_ += upload(d_multi_small_, multi_small_, stream_);
   h2d_bytes_ += upload(d_multi_large_, multi_large_, stream_);
+  h2d_bytes_ += upload(d_multi_huge_, multi_huge_, stream_);
+  if (!multi_huge_.empty()) d_fit_ws_.ensure(multi_workspace_doubles(2, static_cast<int>(multi_huge_.size())));
   h2d_bytes_ += upload(d_direct_cols_, direct_cols_, stream_);
   h2d_bytes_ += upload(d_direct_slots_, direct_slots_, stream_);
   h2d_bytes_ += upload(d_pairs_, pairs_, stream_);
@@ -428,6 +436,13 @@ void Engine::enqueue() {
     cuda_check(launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                 d_multi_large_.get(), static_cast<int>(multi_large_.size()), d_resid_.get(),
                                 d_multi_res_.get(), stream_, opt_.selection),
+               "fit multi");
+    ++launches_;
+  }
+  if (!multi_huge_.empty()) {
+    cuda_check(launch_fit_multi(2, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                d_multi_huge_.get(), static_cast<int>(multi_huge_.size()), d_resid_.get(),
+                                d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get()),
                "fit multi");
     ++launches_;
   }
@@ -678,7 +693,8 @@ void Engine::account_flops(const std::vector<FitResult>& sres, const std::vector
     const double deriv = 2.0 * q * q * rs + 2.0 * rs * rs * q;
     const double f = 4.0 * n * q + core * mres[i].evaluations + deriv * mres[i].iterations;
     const bool small = des.q <= kWarpQ && rs <= kWarpR && des.m <= kWarpM;
-    stage_flops_[small ? 1 : 2] += f;
+    const bool large = !small && des.q <= 76 && rs <= 64;
+    stage_flops_[small ? 1 : (large ? 2 : 9)] += f;
   }
   if (stats_enabled_) {
     const double nc = static_cast<double>(comps_.size()), np = static_cast<double>(pairs_.size());
@@ -726,6 +742,14 @@ void Engine::enqueue_plain_test(int t) {
   if (b1 > b0) {
     cuda_check(launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                 d_multi_large_.get() + b0, b1 - b0, d_resid_.get(), d_multi_res_.get(), stream_, opt_.selection),
+               "fit multi");
+    ++launches_;
+  }
+  const int h0 = plain_huge_off_[t], h1 = plain_huge_off_[t + 1];
+  if (h1 > h0) {
+    cuda_check(launch_fit_multi(2, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                d_multi_huge_.get() + h0, h1 - h0, d_resid_.get(), d_multi_res_.get(), stream_,
+                                opt_.selection, d_fit_ws_.get()),
                "fit multi");
     ++launches_;
   }
@@ -795,7 +819,7 @@ double Engine::execute_timed(int repeats) {
 
 double Engine::time_stage(int stage, int repeats, double* flops_per_launch) {
   if (!collected_) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "collect the prepared batch before timing a stage");
-  if (stage < 0 || stage > 8) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "unknown stage");
+  if (stage < 0 || stage > 9) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "unknown stage");
   cuda_check(configure_fit_kernels(), "kernel attributes");
   cuda_check(configure_stat_kernels(n_), "kernel attributes");
   const int n = n_;
@@ -812,6 +836,9 @@ double Engine::time_stage(int stage, int repeats, double* flops_per_launch) {
       case 2: return launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                       d_multi_large_.get(), static_cast<int>(multi_large_.size()), d_resid_.get(),
                                       d_multi_res_.get(), stream_, opt_.selection);
+      case 9: return launch_fit_multi(2, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                      d_multi_huge_.get(), static_cast<int>(multi_huge_.size()), d_resid_.get(),
+                                      d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get());
       case 3: return launch_dcov_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, d_centre_.get(),
                                             d_dcov_.get(), stream_);
       case 4: return launch_dcov_pairs(d_resid_.get(), n, d_comp_cols_.get(), d_centre_.get(), d_dcov_.get(),
@@ -959,15 +986,16 @@ void Engine::adjoint(int target, const std::vector<int>& S, int count, const dou
   const int m = des.m;
   int rsum = 0;
   for (int r : des.ranks) rsum += r;
-  const int qclass = (des.q <= kWarpQ && rsum <= kWarpR && m <= kWarpM) ? 0 : 1;
+  const int qclass = (des.q <= kWarpQ && rsum <= kWarpR && m <= kWarpM) ? 0 : (des.q <= 76 && rsum <= 64 ? 1 : 2);
   if (count == 0) return;
   DevBuf<double> d_rho, d_score, d_grad, d_gn, d_hess;
+  if (qclass == 2) d_fit_ws_.ensure(multi_workspace_doubles(2, count));
   DevBuf<int> d_status;
   const size_t cm = static_cast<size_t>(count) * m, cmm = cm * m;
   cuda_check(cudaMemcpyAsync(d_rho.ensure(cm), rho, cm * sizeof(double), cudaMemcpyHostToDevice, stream_), "upload");
   cuda_check(launch_gcv_adjoint(qclass, d_designs_.get(), 0, d_arena_.get(), d_data_.get() + static_cast<size_t>(n_) * target,
                                 n_, d_rho.get(), count, d_score.ensure(count), d_grad.ensure(cm), d_gn.ensure(cmm),
-                                d_hess.ensure(cmm), d_status.ensure(count), stream_),
+                                d_hess.ensure(cmm), d_status.ensure(count), stream_, qclass == 2 ? d_fit_ws_.get() : nullptr),
              "gcv adjoint");
   ++launches_;
   std::vector<int> st(count);
@@ -1009,6 +1037,7 @@ void Engine::statistics(const double* residuals, int m, const std::vector<int>& 
   multi_jobs_.clear();
   multi_small_.clear();
   multi_large_.clear();
+  multi_huge_.clear();
   direct_cols_.clear();
   direct_slots_.clear();
   stats_enabled_ = true;

@@ -239,7 +239,8 @@ FKPC_API int fkpc_batch_collect(int device, fkpc_ci_record* out,
  * its mean CUDA-event duration (ms) and its algorithmic FP64 flops per launch.
  * Stages: 0 fit single, 1 fit multi (q <= 40), 2 fit multi (q <= 76),
  * 3 dCov components, 4 dCov pairs, 5 HSIC components, 6 HSIC pairs,
- * 7 low-rank eigen, 8 low-rank pairs.  Run fkpc_batch_execute first.
+ * 7 low-rank eigen, 8 low-rank pairs, 9 fit multi (q <= 112).  Run
+ * fkpc_batch_execute first.
  * No reference counterpart (measurement utility).
  */
 FKPC_API int fkpc_batch_time_stage(int device, int stage, int repeats,

@@ -188,3 +188,26 @@ def test_permutation_skeleton_matches_oracle_stream(lib, method):
     exp = sorted((r["level"], r["x"], r["y"], tuple(r["S"]), r["p_value"]) for r in ora["trace"])
     assert [g[:4] for g in got] == [e[:4] for e in exp]
     assert [g[4] for g in got] == [e[4] for e in exp]
+
+
+def test_wide_additive_fits_match_oracle(lib):
+    """|S| = 9, 10, 12 (q = 82, 91, 109): the widest fit class, whose working
+    set lives in global memory, against the oracle at the residual tolerance."""
+    X, _ = workloads.uneven_batch_500x64(count=8)
+    fits = [(0, [3, 7, 11, 15, 19, 23, 27, 31, 35]), (5, [1, 2, 8, 13, 21, 34, 40, 44, 50, 55]),
+            (9, [2, 4, 6, 10, 12, 16, 18, 22, 26, 30, 38, 62])]
+    resid, lsp, status = fk.regress_batch(X, fits)
+    assert (status == 0).all()
+    for k, (t, S) in enumerate(fits):
+        prep = gcv.Prepared(tprs.design(X, S))
+        r, info = gcv.fit(prep, X[:, t])
+        err = np.max(np.abs(resid[:, k] - r)) / np.max(np.abs(r))
+        assert err <= RESID_TOL, (t, len(S), err)
+    t, S = fits[1]
+    prep = gcv.Prepared(tprs.design(X, S))
+    rho = np.log(prep.initial_sp)
+    a = fk.gcv_adjoint(X, t, S, rho[None, :])
+    V, g, H = gcv.gcv_value_grad_hess(prep, X[:, t], rho)
+    assert abs(a["score"][0] - V) <= 1e-10 * V
+    assert np.max(np.abs(a["grad"][0] - g)) <= 1e-8 * np.max(np.abs(g))
+    assert np.max(np.abs(a["hessian"][0] - H)) <= 1e-8 * np.max(np.abs(H))

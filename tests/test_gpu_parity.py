@@ -211,3 +211,44 @@ def test_wide_additive_fits_match_oracle(lib):
     assert abs(a["score"][0] - V) <= 1e-10 * V
     assert np.max(np.abs(a["grad"][0] - g)) <= 1e-8 * np.max(np.abs(g))
     assert np.max(np.abs(a["hessian"][0] - H)) <= 1e-8 * np.max(np.abs(H))
+
+
+def _uneven_triples(X, count, seed):
+    """Triples of the n=500, p=64 batch with a spread of |S| up to 12."""
+    rs = np.random.default_rng(seed)
+    p = X.shape[1]
+    out = []
+    for k in (0, 1, 2, 3, 4, 6, 9):
+        cols = rs.choice(p, size=k + 2, replace=False)
+        out.append((int(cols[0]), int(cols[1]), sorted(int(c) for c in cols[2:])))
+    return out[:count]
+
+
+@pytest.mark.parametrize("method", ["dcc.perm", "hsic.perm"])
+def test_uneven_permutation_batch_matches_oracle_stream(lib, method):
+    """Uneven widths (|S| up to 9 here) with permutation nulls: the level
+    batch consumes the seeded R stream test by test; p-values exact."""
+    X, _ = workloads.uneven_batch_500x64(count=8)
+    triples = _uneven_triples(X, 7, 11)
+    R_ = 40
+    rec, _ = fk.ci_level_batch(X, triples, ci_method=method, seed=7, replicates=R_)
+    stream = rng.RStream(7)
+    gen = rng.dcc_permutations if method == "dcc.perm" else rng.hsic_permutations
+    cache = skeleton.ResidualCache(X)
+    for k, (x, y, S) in enumerate(triples):
+        perms = gen(stream, X.shape[0], R_)
+        assert rec["p_value"][k] == skeleton.ci_pvalue(cache, method, x, y, S, perms=perms), (x, y, S)
+
+
+def test_permutation_batch_chunks_keep_the_stream_order(lib):
+    """600 tests with R = 1000 exceed one permutation-table chunk (about
+    1 GiB, 536 tests at n = 500): the chunked batch equals the plain per-test
+    form, which consumes the same stream one test at a time."""
+    X, triples = workloads.uneven_batch_500x64(count=800)
+    triples = [t for t in triples if len(t[2]) <= 3][:600]
+    assert len(triples) == 600
+    kw = dict(ci_method="dcc.perm", seed=3, replicates=1000)
+    batched, _ = fk.ci_level_batch(X, triples, **kw)
+    plain, _ = fk.ci_level_batch(X, triples, mode="plain", **kw)
+    assert np.array_equal(batched["p_value"], plain["p_value"])
+    assert np.array_equal(batched["statistic"], plain["statistic"])

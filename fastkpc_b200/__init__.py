@@ -100,6 +100,8 @@ _SIGNATURES = {
     "fkpc_default_options": (None, [_P(Options)]),
     "fkpc_skeleton_run": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _P(Options), _P(_P(Result))]),
     "fkpc_result_free": (None, [_P(Result)]),
+    "fkpc_skeleton_run_custom": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _P(Options), ctypes.c_void_p,
+                                                ctypes.c_void_p, _P(_P(Result))]),
     "fkpc_ci_level_batch": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, _INT, ctypes.c_int,
                                            _P(Options), _P(CiRecord), _P(StageStats)]),
     "fkpc_ci_plain_one": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _INT,
@@ -209,6 +211,12 @@ def fastkpc_compatible_cuda_skeleton(data, alpha, labels=None, options=None):
     (list of p lists; None or the separating set, 0-based), ``n_edgetests``,
     ``tasks`` (the logical trace as column arrays), ``summary``.
     """
+    X, labels, o, method = _skeleton_setup(data, alpha, labels, options)
+    return _run_skeleton(X, alpha, labels, o, method, None)
+
+
+def _skeleton_setup(data, alpha, labels, options):
+    """Validated (data, labels, fkpc_options, method) of the facade's options."""
     options = dict(options or {})
     unknown = set(options) - _ALLOWED
     if unknown:
@@ -236,9 +244,23 @@ def fastkpc_compatible_cuda_skeleton(data, alpha, labels=None, options=None):
                      hsic_sig=hsic.get("sig", 1), replicates=perm.get("replicates", 100), seed=perm.get("seed"),
                      mode=options.get("mode", "batched"), trace=trace_level in ("logical", "full"),
                      device=options.get("device", 0), strict=options.get("compatible_cuda_strict", True))
+    return X, labels, o, method
+
+
+# One level's CI tests for fkpc_skeleton_run_custom (see fastkpc_b200.distributed).
+LEVEL_EVALUATOR = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, _INT, _INT, _INT, _INT, ctypes.c_int,
+                                   _P(CiRecord))
+
+
+def _run_skeleton(X, alpha, labels, o, method, evaluator):
+    n, p = X.shape
     lib = load_library()
     res = _P(Result)()
-    _check(lib.fkpc_skeleton_run(_ptr(X, ctypes.c_double), n, p, ctypes.byref(o), ctypes.byref(res)))
+    if evaluator is None:
+        _check(lib.fkpc_skeleton_run(_ptr(X, ctypes.c_double), n, p, ctypes.byref(o), ctypes.byref(res)))
+    else:
+        _check(lib.fkpc_skeleton_run_custom(_ptr(X, ctypes.c_double), n, p, ctypes.byref(o), evaluator, None,
+                                            ctypes.byref(res)))
     try:
         r = res.contents
         adj = np.ctypeslib.as_array(r.adjacency, shape=(p * p,)).reshape((p, p), order="F").astype(bool)
@@ -276,7 +298,8 @@ def fastkpc_compatible_cuda_skeleton(data, alpha, labels=None, options=None):
                    "tests_replayed": int(sum(n_edgetests)), "elapsed_sec": r.elapsed_sec, "labels": labels,
                    "max_conditioning_size_resolved": (p - 2 if o.max_conditioning_size < 0
                                                       else min(o.max_conditioning_size, p - 2)),
-                   "stages": stats, "entrypoint": "fkpc_skeleton_run"}
+                   "stages": stats,
+                   "entrypoint": "fkpc_skeleton_run" if evaluator is None else "fkpc_skeleton_run_custom"}
         return {"adjacency": adj, "pMax": pmax, "sepsets": sepsets, "n_edgetests": n_edgetests,
                 "tasks": tasks, "summary": summary}
     finally:

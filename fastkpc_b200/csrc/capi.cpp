@@ -208,9 +208,13 @@ void evaluate(fkpc::Engine& eng, const std::vector<fkpc::Test>& tests, const fkp
   }
 }
 
-void skeleton(const double* data, int n, int p, const fkpc_options& opt, Run* run) {
-  auto& eng = engine_for(opt.device);
-  eng.load(data, n, p);
+void skeleton(const double* data, int n, int p, const fkpc_options& opt, Run* run,
+              fkpc_level_evaluator evaluator = nullptr, void* user = nullptr) {
+  fkpc::Engine* engp = nullptr;
+  if (!evaluator) {
+    engp = &engine_for(opt.device);
+    engp->load(data, n, p);
+  }
   const int m_max = opt.max_conditioning_size < 0 ? p - 2 : std::min(opt.max_conditioning_size, p - 2);
   const bool perm = opt.ci_method == FKPC_DCC_PERM || opt.ci_method == FKPC_HSIC_PERM;
   std::unique_ptr<fkpc::RStream> rs;
@@ -229,6 +233,7 @@ void skeleton(const double* data, int n, int p, const fkpc_options& opt, Run* ru
     std::vector<char> counted(plan.size(), 0);
     auto to_test = [&](const Task& t) { return fkpc::Test{t.x, t.y, t.S}; };
     if (perm || opt.mode == FKPC_MODE_PLAIN) {
+      if (evaluator) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "the level evaluator serves the batched gamma methods");
       // one test at a time; permutation methods in pcalg order
       std::map<std::pair<int, int>, size_t> pos;
       for (auto& kv : by_edge) pos[kv.first] = 0;
@@ -248,7 +253,7 @@ void skeleton(const double* data, int n, int p, const fkpc_options& opt, Run* ru
         std::vector<fkpc_ci_record> rec;
         fkpc_options o1 = opt;
         o1.mode = FKPC_MODE_PLAIN;
-        evaluate(eng, {to_test(plan[best])}, o1, rs.get(), &rec, &run->stats);
+        evaluate(*engp, {to_test(plan[best])}, o1, rs.get(), &rec, &run->stats);
         pv[best] = rec[0].p_value;
         pe[best] = rec[0].p_exact;
         fl[best] = rec[0].flags;
@@ -261,7 +266,21 @@ void skeleton(const double* data, int n, int p, const fkpc_options& opt, Run* ru
       tests.reserve(plan.size());
       for (const Task& t : plan) tests.push_back(to_test(t));
       std::vector<fkpc_ci_record> rec;
-      evaluate(eng, tests, opt, nullptr, &rec, &run->stats);
+      if (evaluator) {
+        std::vector<int> xs(tests.size()), ys(tests.size()), offs(tests.size() + 1, 0), vals;
+        for (size_t i = 0; i < tests.size(); ++i) {
+          xs[i] = tests[i].x;
+          ys[i] = tests[i].y;
+          vals.insert(vals.end(), tests[i].S.begin(), tests[i].S.end());
+          offs[i + 1] = static_cast<int>(vals.size());
+        }
+        rec.assign(tests.size(), fkpc_ci_record{});
+        const int rc = evaluator(user, level, xs.data(), ys.data(), offs.data(), vals.empty() ? nullptr : vals.data(),
+                                 static_cast<int>(tests.size()), rec.data());
+        if (rc != 0) throw fkpc::Error(rc, "the level evaluator failed at level " + std::to_string(level));
+      } else {
+        evaluate(*engp, tests, opt, nullptr, &rec, &run->stats);
+      }
       for (size_t i = 0; i < plan.size(); ++i) {
         pv[i] = rec[i].p_value;
         pe[i] = rec[i].p_exact;
@@ -326,6 +345,35 @@ T* copy_out(const std::vector<T>& v) {
   return out;
 }
 
+fkpc_result* make_result(const Run& run, const fkpc_options& options, int n, int p,
+                         std::chrono::steady_clock::time_point t0) {
+  fkpc_result* r = static_cast<fkpc_result*>(std::calloc(1, sizeof(fkpc_result)));
+  if (!r) throw std::bad_alloc();
+  r->n = n;
+  r->p = p;
+  r->levels = static_cast<int>(run.n_edgetests.size());
+  r->adjacency = copy_out(run.adj);
+  r->pmax = copy_out(run.pmax);
+  std::vector<int> offs(static_cast<size_t>(p) * p + 1, 0), vals;
+  for (int j = 0; j < p; ++j)
+    for (int i = 0; i < p; ++i) {
+      const size_t cell = i + static_cast<size_t>(p) * j;
+      auto it = run.sepsets.find({i, j});
+      if (it != run.sepsets.end()) vals.insert(vals.end(), it->second.begin(), it->second.end());
+      offs[cell + 1] = static_cast<int>(vals.size());
+    }
+  r->sepset_offsets = copy_out(offs);
+  r->sepset_values = copy_out(vals);
+  r->n_edgetests = copy_out(run.n_edgetests);
+  r->trace_rows = static_cast<int>(run.trace.size());
+  r->trace = options.collect_trace ? copy_out(run.trace) : nullptr;
+  r->trace_s_values = options.collect_trace ? copy_out(run.trace_s) : nullptr;
+  r->stats = run.stats;
+  r->elapsed_sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  r->stats.total_ms = r->elapsed_sec * 1e3;
+  return r;
+}
+
 }  // namespace
 
 extern "C" {
@@ -362,31 +410,22 @@ int fkpc_skeleton_run(const double* data, int n, int p, const fkpc_options* opti
     auto t0 = std::chrono::steady_clock::now();
     Run run;
     skeleton(data, n, p, *options, &run);
-    fkpc_result* r = static_cast<fkpc_result*>(std::calloc(1, sizeof(fkpc_result)));
-    if (!r) throw std::bad_alloc();
-    r->n = n;
-    r->p = p;
-    r->levels = static_cast<int>(run.n_edgetests.size());
-    r->adjacency = copy_out(run.adj);
-    r->pmax = copy_out(run.pmax);
-    std::vector<int> offs(static_cast<size_t>(p) * p + 1, 0), vals;
-    for (int j = 0; j < p; ++j)
-      for (int i = 0; i < p; ++i) {
-        const size_t cell = i + static_cast<size_t>(p) * j;
-        auto it = run.sepsets.find({i, j});
-        if (it != run.sepsets.end()) vals.insert(vals.end(), it->second.begin(), it->second.end());
-        offs[cell + 1] = static_cast<int>(vals.size());
-      }
-    r->sepset_offsets = copy_out(offs);
-    r->sepset_values = copy_out(vals);
-    r->n_edgetests = copy_out(run.n_edgetests);
-    r->trace_rows = static_cast<int>(run.trace.size());
-    r->trace = options->collect_trace ? copy_out(run.trace) : nullptr;
-    r->trace_s_values = options->collect_trace ? copy_out(run.trace_s) : nullptr;
-    r->stats = run.stats;
-    r->elapsed_sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    r->stats.total_ms = r->elapsed_sec * 1e3;
-    *out = r;
+    *out = make_result(run, *options, n, p, t0);
+  });
+}
+
+int fkpc_skeleton_run_custom(const double* data, int n, int p, const fkpc_options* options,
+                             fkpc_level_evaluator evaluator, void* user, fkpc_result** out) {
+  return guarded([&]() {
+    if (!data || !options || !out || !evaluator) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    validate_options(*options, n, p);
+    if (p > 64) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "p must be at most 64");
+    // no engine lock: the evaluator may call back into the batch entry points
+    auto t0 = std::chrono::steady_clock::now();
+    Run run;
+    skeleton(data, n, p, *options, &run, evaluator, user);
+    *out = make_result(run, *options, n, p, t0);
   });
 }
 

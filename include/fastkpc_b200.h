@@ -148,6 +148,25 @@ FKPC_API int fkpc_skeleton_run(const double* data_colmajor, int n, int p,
 FKPC_API void fkpc_result_free(fkpc_result* result);
 
 /*
+ * Evaluator of one level's CI tests for fkpc_skeleton_run_custom: fills
+ * out[t] for test t = (x[t], y[t], S = s_values[s_offsets[t] ..
+ * s_offsets[t+1])) and returns 0, or a positive FKPC_STATUS_* code.
+ */
+typedef int (*fkpc_level_evaluator)(void* user, int level, const int* x, const int* y, const int* s_offsets,
+                                    const int* s_values, int count, fkpc_ci_record* out);
+
+/*
+ * fkpc_skeleton_run with every level's batch of tests evaluated by
+ * ``evaluator`` (batched gamma methods only): the hook through which a host
+ * splits a level's independent tests across GPUs and gathers their records,
+ * while the level plan, the canonical replay, pMax and the sepsets stay
+ * here.  Uses no device itself.  No reference counterpart (the reference
+ * runs one GPU).
+ */
+FKPC_API int fkpc_skeleton_run_custom(const double* data_colmajor, int n, int p, const fkpc_options* options,
+                                      fkpc_level_evaluator evaluator, void* user, fkpc_result** out);
+
+/*
  * One batch of CI tests (x, y, S): residuals of x and y on S by GCV-selected
  * thin-plate / additive smooths, then the statistic and p-value.  Test t uses
  * S = s_values[s_offsets[t] .. s_offsets[t+1]).

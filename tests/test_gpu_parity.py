@@ -252,3 +252,31 @@ def test_permutation_batch_chunks_keep_the_stream_order(lib):
     plain, _ = fk.ci_level_batch(X, triples, mode="plain", **kw)
     assert np.array_equal(batched["p_value"], plain["p_value"])
     assert np.array_equal(batched["statistic"], plain["statistic"])
+
+
+def test_sharded_skeleton_single_rank_equals_direct(lib):
+    """The multi-GPU driver (level evaluator hook, records gathered per level)
+    run as a one-rank group on this GPU gives the direct skeleton exactly."""
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    from fastkpc_b200 import distributed
+    X = workloads.skeleton_200x10()
+    opts = {"numCol": 35, "trace_level": "logical"}
+    direct = fk.fastkpc_compatible_cuda_skeleton(X, 0.1, options=opts)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=0, world_size=1)
+    try:
+        sharded = distributed.sharded_skeleton(X, 0.1, options=opts)
+    finally:
+        dist.destroy_process_group()
+    assert np.array_equal(sharded["adjacency"], direct["adjacency"])
+    assert np.array_equal(sharded["pMax"], direct["pMax"])
+    assert sharded["sepsets"] == direct["sepsets"]
+    assert sharded["n_edgetests"] == direct["n_edgetests"]

@@ -163,7 +163,7 @@ void hq_pre_transpose(std::vector<double>* P, int k, const std::vector<double>& 
 
 }  // namespace
 
-Smooth build_smooth(const double* cols, int n, int d, int k) {
+TprsPrep tprs_prepare(const double* cols, int n, int d, int k) {
   const int m = default_order(d);
   const int M = null_space_dimension(d, m);
   std::vector<double> shifted(static_cast<size_t>(n) * d);
@@ -200,6 +200,33 @@ Smooth build_smooth(const double* cols, int n, int d, int k) {
   std::vector<double> u(static_cast<size_t>(nu) * d);
   for (int i = 0; i < nu; ++i)
     for (int c = 0; c < d; ++c) u[i + static_cast<size_t>(nu) * c] = shifted[uniq[i] + static_cast<size_t>(n) * c];
+  std::vector<int> powers = polynomial_powers(d, m, M);
+  std::vector<double> T(static_cast<size_t>(nu) * M, 1.0);
+  for (int t = 0; t < M; ++t)
+    for (int i = 0; i < nu; ++i) {
+      double v = 1.0;
+      for (int c = 0; c < d; ++c)
+        for (int e = 0; e < powers[t * d + c]; ++e) v *= u[i + static_cast<size_t>(nu) * c];
+      T[i + static_cast<size_t>(nu) * t] = v;
+    }
+  TprsPrep prep;
+  prep.n = n;
+  prep.d = d;
+  prep.k = k;
+  prep.m = m;
+  prep.M = M;
+  prep.nu = nu;
+  prep.u = std::move(u);
+  prep.mapping = std::move(mapping);
+  prep.T = std::move(T);
+  return prep;
+}
+
+double tprs_eta0(int d) { return eta_constant(default_order(d), d); }
+
+std::vector<double> tprs_eta_matrix(const TprsPrep& prep) {
+  const int nu = prep.nu, d = prep.d, m = prep.m;
+  const std::vector<double>& u = prep.u;
   const double eta0 = eta_constant(m, d);
   std::vector<double> E(static_cast<size_t>(nu) * nu, 0.0);
   for (int j = 0; j < nu; ++j)
@@ -213,17 +240,14 @@ Smooth build_smooth(const double* cols, int n, int d, int k) {
       E[i + static_cast<size_t>(nu) * j] = v;
       E[j + static_cast<size_t>(nu) * i] = v;
     }
-  std::vector<int> powers = polynomial_powers(d, m, M);
-  std::vector<double> T(static_cast<size_t>(nu) * M, 1.0);
-  for (int t = 0; t < M; ++t)
-    for (int i = 0; i < nu; ++i) {
-      double v = 1.0;
-      for (int c = 0; c < d; ++c)
-        for (int e = 0; e < powers[t * d + c]; ++e) v *= u[i + static_cast<size_t>(nu) * c];
-      T[i + static_cast<size_t>(nu) * t] = v;
-    }
-  std::vector<double> vals, U;
-  top_magnitude_eigen(E.data(), nu, k, &vals, &U);
+  return E;
+}
+
+Smooth tprs_finish(const TprsPrep& prep, const std::vector<double>& vals, const std::vector<double>& U) {
+  const int n = prep.n, k = prep.k, M = prep.M, nu = prep.nu;
+  const std::vector<double>& T = prep.T;
+  const std::vector<int>& mapping = prep.mapping;
+
   // T'U, row-major M x k
   std::vector<double> TU(static_cast<size_t>(M) * k, 0.0);
   for (int t = 0; t < M; ++t)
@@ -321,6 +345,14 @@ Smooth build_smooth(const double* cols, int n, int d, int k) {
       out.S[(a - 1) + static_cast<size_t>(k - 1) * (c - 1)] = HS[a + static_cast<size_t>(k) * c] - dv * hv[c];
   }
   return out;
+}
+
+Smooth build_smooth(const double* cols, int n, int d, int k) {
+  TprsPrep prep = tprs_prepare(cols, n, d, k);
+  std::vector<double> E = tprs_eta_matrix(prep);
+  std::vector<double> vals, U;
+  top_magnitude_eigen(E.data(), prep.nu, k, &vals, &U);
+  return tprs_finish(prep, vals, U);
 }
 
 std::vector<double> initial_sp(const Design& des) {
@@ -480,8 +512,11 @@ std::shared_ptr<Design> build_design(const double* data, int n, int p, const std
     std::vector<double> cols(static_cast<size_t>(n) * S.size());
     for (size_t c = 0; c < S.size(); ++c)
       std::copy(data + static_cast<size_t>(n) * S[c], data + static_cast<size_t>(n) * (S[c] + 1), cols.begin() + static_cast<size_t>(n) * c);
+    std::shared_ptr<const Smooth> pre = (S.size() == 2 && cache) ? cache->bivariate(S) : nullptr;
     if (S.size() == 1 && cache) {
       parts.push_back(cache->univariate(S[0]));
+    } else if (pre) {
+      parts.push_back(pre);
     } else {
       parts.push_back(std::make_shared<Smooth>(build_smooth(cols.data(), n, static_cast<int>(S.size()), S.size() == 1 ? 10 : 30)));
     }
@@ -526,6 +561,22 @@ std::shared_ptr<const Smooth> DesignCache::univariate(int column) {
   if (it != uni_.end()) return it->second;
   uni_[column] = sm;
   return sm;
+}
+
+void DesignCache::put_bivariate(const std::vector<int>& S, std::shared_ptr<const Smooth> smooth) {
+  std::lock_guard<std::mutex> lock(mu_);
+  bi_[S] = std::move(smooth);
+}
+
+std::shared_ptr<const Smooth> DesignCache::bivariate(const std::vector<int>& S) {
+  std::lock_guard<std::mutex> lock(mu_);
+  auto it = bi_.find(S);
+  return it == bi_.end() ? nullptr : it->second;
+}
+
+bool DesignCache::has_design(const std::vector<int>& S) {
+  std::lock_guard<std::mutex> lock(mu_);
+  return designs_.count(S) > 0 || bi_.count(S) > 0;
 }
 
 std::shared_ptr<const Design> DesignCache::get(const std::vector<int>& S) {

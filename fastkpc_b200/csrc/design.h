@@ -34,6 +34,21 @@ struct Design {
   std::vector<std::vector<double>> roots;
 };
 
+// Thin-plate set-up in three parts, so that the top-k eigen problem of the
+// eta matrix can be solved elsewhere (the device batches it per level):
+// prepare (unique locations, polynomial null-space basis), the eta matrix,
+// and finish (constraint absorption, scaling, centering) from its top-k
+// eigenpairs (descending, largest-magnitude entry of each vector positive).
+struct TprsPrep {
+  int n = 0, d = 0, k = 0, m = 0, M = 0, nu = 0;
+  std::vector<double> u;      // nu x d unique (shifted) locations, column-major
+  std::vector<int> mapping;   // row -> unique location
+  std::vector<double> T;      // nu x M polynomial null-space basis
+};
+TprsPrep tprs_prepare(const double* cols, int n, int d, int k);
+std::vector<double> tprs_eta_matrix(const TprsPrep& prep);
+double tprs_eta0(int d);  // eta constant of the default order for dimension d
+Smooth tprs_finish(const TprsPrep& prep, const std::vector<double>& vals, const std::vector<double>& U);
 Smooth build_smooth(const double* cols, int n, int d, int k);
 double r_mean(const double* v, int n);
 std::vector<double> initial_sp(const Design& des);
@@ -46,7 +61,13 @@ class DesignCache {
   DesignCache(const double* data, int n, int p) : data_(data), n_(n), p_(p) {}
   std::shared_ptr<const Design> get(const std::vector<int>& S);
   std::shared_ptr<const Smooth> univariate(int column);
+  // bivariate thin-plate smooths built outside build_design (device eigen)
+  void put_bivariate(const std::vector<int>& S, std::shared_ptr<const Smooth> smooth);
+  std::shared_ptr<const Smooth> bivariate(const std::vector<int>& S);
+  bool has_design(const std::vector<int>& S);
   size_t size() const { return designs_.size(); }
+  const double* data() const { return data_; }
+  int n() const { return n_; }
 
  private:
   const double* data_;
@@ -54,6 +75,7 @@ class DesignCache {
   std::mutex mu_;
   std::map<std::vector<int>, std::shared_ptr<const Design>> designs_;
   std::map<int, std::shared_ptr<const Smooth>> uni_;
+  std::map<std::vector<int>, std::shared_ptr<const Smooth>> bi_;
 };
 
 std::shared_ptr<Design> build_design(const double* data, int n, int p, const std::vector<int>& S,

@@ -328,4 +328,47 @@ int top_magnitude_eigen(const double* A, int n, int k, std::vector<double>* valu
   throw std::runtime_error("Lanczos did not converge");
 }
 
+bool ritz_from_lanczos(const double* V, const double* alpha, const double* beta, int n, int m, int k,
+                       std::vector<double>* values, std::vector<double>* vectors) {
+  if (k <= 0 || m < k) return false;
+  std::vector<double> dwork(alpha, alpha + m), ework(m, 0.0);
+  for (int i = 0; i + 1 < m; ++i) ework[i] = beta[i];
+  std::vector<double> S(static_cast<size_t>(m) * m, 0.0);
+  for (int i = 0; i < m; ++i) S[i + static_cast<size_t>(m) * i] = 1.0;
+  if (!tridiagonal_ql(m, dwork.data(), ework.data(), S.data())) return false;
+  std::vector<int> sel = top_k_by_magnitude(dwork, m, k);
+  double tmax = 0.0;
+  for (int i = 0; i < m; ++i) tmax = std::max(tmax, std::fabs(dwork[i]));
+  const bool invariant = std::fabs(beta[m - 1]) <= 1e-15 * tmax;
+  if (!invariant)
+    for (int i : sel)
+      if (std::fabs(beta[m - 1] * S[(m - 1) + static_cast<size_t>(m) * i]) > 1e-14 * tmax) return false;
+  std::stable_sort(sel.begin(), sel.end(), [&](int a, int b) { return dwork[a] > dwork[b]; });
+  values->assign(k, 0.0);
+  vectors->assign(static_cast<size_t>(n) * k, 0.0);
+  for (int c = 0; c < k; ++c) {
+    const int i = sel[c];
+    (*values)[c] = dwork[i];
+    double* out = &(*vectors)[static_cast<size_t>(n) * c];
+    for (int b = 0; b < m; ++b) {
+      const double coef = S[b + static_cast<size_t>(m) * i];
+      const double* vb = V + static_cast<size_t>(n) * b;
+      for (int r = 0; r < n; ++r) out[r] += coef * vb[r];
+    }
+    double nn = std::sqrt(dot(out, out, n));
+    int imax = 0;
+    double amax = -1.0;
+    for (int r = 0; r < n; ++r) {
+      out[r] /= nn;
+      if (std::fabs(out[r]) > amax) {
+        amax = std::fabs(out[r]);
+        imax = r;
+      }
+    }
+    if (out[imax] < 0.0)
+      for (int r = 0; r < n; ++r) out[r] = -out[r];
+  }
+  return true;
+}
+
 }  // namespace fkpc

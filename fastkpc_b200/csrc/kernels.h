@@ -89,4 +89,11 @@ cudaError_t launch_dcc_perm_pairs(const double* residuals, int n, const int* com
 // FP64 FMA throughput probe: blocks x 256 threads, 16 chains, iters steps.
 cudaError_t launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t stream);
 
+// Thin-plate set-up: Lanczos on the eta matrices of a level's bivariate
+// designs (one CTA per design); see kernels_tprs.cu.
+constexpr int kTprsMaxSteps = 128;
+cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int* nus, int count, int nu_max,
+                                int steps, double eta0, double* ews, int64_t ews_stride, int ctas, double* V,
+                                const int64_t* voff, double* alpha, double* beta, int* done, cudaStream_t stream);
+
 }  // namespace fkpc

@@ -10,6 +10,7 @@
 //   [-> guard select -> low-rank eigen -> low-rank pairs for dcc.gamma],
 // captured once as a CUDA graph and replayed by execute().
 #include "runtime.h"
+#include "hostla.h"
 
 #include <algorithm>
 #include <atomic>
@@ -164,7 +165,117 @@ void Engine::plan_components(const std::vector<Test>& tests) {
   }
 }
 
+namespace {
+
+// f(i) for i in [0, count) on up to 16 host threads.
+template <class F>
+void parallel_for(size_t count, F f) {
+  std::atomic<size_t> next(0);
+  auto work = [&]() {
+    for (;;) {
+      const size_t i = next.fetch_add(1);
+      if (i >= count) return;
+      f(i);
+    }
+  };
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t workers = std::min<size_t>(std::min<size_t>(hw, 16), count);
+  if (workers <= 1) {
+    work();
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (size_t w = 0; w < workers; ++w) pool.emplace_back(work);
+  for (auto& th : pool) th.join();
+}
+
+constexpr int kTprsK = 30;                  // basis dimension of the bivariate thin-plate smooth
+constexpr int kTprsSteps = kTprsK + 60;     // Lanczos steps on the device (the host needs about 65)
+constexpr size_t kDeviceTprsMin = 32;       // fewer bivariate designs than this: host set-up
+
+}  // namespace
+
+// The top-30 eigen problems of the level's new bivariate designs: prepare on
+// the host, Lanczos on the device, Ritz pairs and the rest of the basis on
+// the host.  Designs whose Ritz pairs do not converge in kTprsSteps steps are
+// left to the host set-up in build_designs.
+void Engine::build_bivariate_on_device(const std::vector<std::vector<int>>& sets) {
+  const int n = n_;
+  const size_t count = sets.size();
+  std::vector<TprsPrep> preps(count);
+  std::vector<char> ok(count, 0);
+  parallel_for(count, [&](size_t i) {
+    try {
+      std::vector<double> cols(static_cast<size_t>(2) * n);
+      std::copy(host_data_.begin() + static_cast<size_t>(n) * sets[i][0],
+                host_data_.begin() + static_cast<size_t>(n) * (sets[i][0] + 1), cols.begin());
+      std::copy(host_data_.begin() + static_cast<size_t>(n) * sets[i][1],
+                host_data_.begin() + static_cast<size_t>(n) * (sets[i][1] + 1), cols.begin() + n);
+      preps[i] = tprs_prepare(cols.data(), n, 2, kTprsK);
+      ok[i] = preps[i].nu > kTprsSteps && preps[i].nu <= 2048;
+    } catch (const std::exception&) {
+      ok[i] = 0;  // the host set-up reports the error
+    }
+  });
+  std::vector<size_t> idx;
+  for (size_t i = 0; i < count; ++i)
+    if (ok[i]) idx.push_back(i);
+  if (idx.empty()) return;
+  std::vector<double> u;
+  std::vector<int64_t> uoff, voff;
+  std::vector<int> nus;
+  int nu_max = 0;
+  int64_t vtotal = 0;
+  for (size_t i : idx) {
+    uoff.push_back(static_cast<int64_t>(u.size()));
+    u.insert(u.end(), preps[i].u.begin(), preps[i].u.end());
+    nus.push_back(preps[i].nu);
+    voff.push_back(vtotal);
+    vtotal += static_cast<int64_t>(preps[i].nu) * kTprsSteps;
+    nu_max = std::max(nu_max, preps[i].nu);
+  }
+  const int cnt = static_cast<int>(idx.size());
+  const int ctas = std::min(cnt, 148);
+  upload(d_tprs_u_, u, stream_);
+  upload(d_tprs_uoff_, uoff, stream_);
+  upload(d_tprs_voff_, voff, stream_);
+  upload(d_tprs_nus_, nus, stream_);
+  const int64_t ews_stride = static_cast<int64_t>(nu_max) * nu_max;
+  double* dV = d_tprs_V_.ensure(static_cast<size_t>(vtotal));
+  double* dab = d_tprs_ab_.ensure(static_cast<size_t>(2) * cnt * kTprsSteps);
+  cuda_check(launch_tprs_lanczos(d_tprs_u_.get(), d_tprs_uoff_.get(), d_tprs_nus_.get(), cnt, nu_max, kTprsSteps,
+                                 tprs_eta0(2), d_tprs_ews_.ensure(static_cast<size_t>(ctas) * ews_stride), ews_stride,
+                                 ctas, dV, d_tprs_voff_.get(), dab, dab + static_cast<size_t>(cnt) * kTprsSteps,
+                                 d_tprs_done_.ensure(cnt), stream_),
+             "thin-plate Lanczos");
+  double* hV = pinned_arena(static_cast<size_t>(vtotal));
+  std::vector<double> ab(static_cast<size_t>(2) * cnt * kTprsSteps);
+  std::vector<int> done(cnt);
+  cuda_check(cudaMemcpyAsync(hV, dV, static_cast<size_t>(vtotal) * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+             "download");
+  cuda_check(cudaMemcpyAsync(ab.data(), dab, ab.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
+  cuda_check(cudaMemcpyAsync(done.data(), d_tprs_done_.get(), done.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                             stream_),
+             "download");
+  cuda_check(cudaStreamSynchronize(stream_), "thin-plate Lanczos");
+  d2h_bytes_ += static_cast<double>(vtotal) * sizeof(double);
+  parallel_for(idx.size(), [&](size_t c) {
+    const size_t i = idx[c];
+    std::vector<double> vals, U;
+    if (!ritz_from_lanczos(hV + voff[c], ab.data() + c * kTprsSteps, ab.data() + (cnt + c) * kTprsSteps, nus[c],
+                           done[c], kTprsK, &vals, &U))
+      return;  // not converged: the host set-up builds this design
+    cache_->put_bivariate(sets[i], std::make_shared<Smooth>(tprs_finish(preps[i], vals, U)));
+  });
+}
+
 void Engine::build_designs() {
+  {
+    std::vector<std::vector<int>> bivariate;
+    for (const auto& S : sets_)
+      if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
+    if (bivariate.size() >= kDeviceTprsMin) build_bivariate_on_device(bivariate);
+  }
   designs_.assign(sets_.size(), nullptr);
   std::atomic<size_t> next(0);
   std::string err;

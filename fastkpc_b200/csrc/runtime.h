@@ -109,6 +109,7 @@ class Engine {
   void enqueue_plain_test(int t);  // one test's launch set (plain form)
   double execute_plain_timed(int repeats);
   void build_designs();
+  void build_bivariate_on_device(const std::vector<std::vector<int>>& sets);
   void pack_and_upload(const fkpc_options& opt, RStream* stream);
   void enqueue();  // the launch sequence
   void release_graph();
@@ -142,6 +143,10 @@ class Engine {
   DevBuf<FitJob> d_single_jobs_, d_multi_jobs_;
   DevBuf<int> d_multi_small_, d_multi_large_, d_multi_huge_, d_direct_cols_, d_direct_slots_, d_comp_cols_;
   DevBuf<double> d_fit_ws_;  // global working sets of the widest fit class
+  // device thin-plate Lanczos of the bivariate designs
+  DevBuf<double> d_tprs_u_, d_tprs_V_, d_tprs_ab_, d_tprs_ews_;
+  DevBuf<int64_t> d_tprs_uoff_, d_tprs_voff_;
+  DevBuf<int> d_tprs_nus_, d_tprs_done_;
   DevBuf<FitResult> d_single_res_, d_multi_res_;
   DevBuf<PairJob> d_pairs_;
   DevBuf<RecordDev> d_records_;

@@ -280,3 +280,26 @@ def test_sharded_skeleton_single_rank_equals_direct(lib):
     assert np.array_equal(sharded["pMax"], direct["pMax"])
     assert sharded["sepsets"] == direct["sepsets"]
     assert sharded["n_edgetests"] == direct["n_edgetests"]
+
+
+def test_bivariate_designs_set_up_on_the_device_match_oracle(lib, dev500):
+    """40 new |S| = 2 designs in one call take the device thin-plate Lanczos
+    (32 or more per batch): residuals against the oracle at the tolerance."""
+    d = dev500["data"]
+    rs = np.random.default_rng(5)
+    fits = []
+    seen = set()
+    while len(fits) < 40:
+        a, b, t = (int(v) for v in rs.choice(d.shape[1], size=3, replace=False))
+        S = tuple(sorted((a, b)))
+        if S in seen:
+            continue
+        seen.add(S)
+        fits.append((t, list(S)))
+    resid, lsp, status = fk.regress_batch(d, fits)
+    assert (status == 0).all()
+    for k, (t, S) in enumerate(fits[:10]):
+        prep = gcv.Prepared(tprs.design(d, S))
+        r, info = gcv.fit(prep, d[:, t])
+        err = np.max(np.abs(resid[:, k] - r)) / np.max(np.abs(r))
+        assert err <= RESID_TOL, (t, S, err)

@@ -191,7 +191,10 @@ void parallel_for(size_t count, F f) {
 
 constexpr int kTprsK = 30;                  // basis dimension of the bivariate thin-plate smooth
 constexpr int kTprsSteps = kTprsK + 60;     // Lanczos steps on the device (the host needs about 65)
-constexpr size_t kDeviceTprsMin = 32;       // fewer bivariate designs than this: host set-up
+// Every bivariate design the engine builds takes the device Lanczos, however
+// few there are: the per-design computation is deterministic, so a design
+// comes out bit-identical whatever batch (plain or batched form) it is in.
+constexpr size_t kDeviceTprsMin = 1;
 
 }  // namespace
 

@@ -283,8 +283,8 @@ def test_sharded_skeleton_single_rank_equals_direct(lib):
 
 
 def test_bivariate_designs_set_up_on_the_device_match_oracle(lib, dev500):
-    """40 new |S| = 2 designs in one call take the device thin-plate Lanczos
-    (32 or more per batch): residuals against the oracle at the tolerance."""
+    """40 new |S| = 2 designs in one call, set up with the device thin-plate
+    Lanczos: residuals against the oracle at the tolerance."""
     d = dev500["data"]
     rs = np.random.default_rng(5)
     fits = []

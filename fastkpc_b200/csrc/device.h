@@ -68,6 +68,22 @@ struct FitResult {
   int flags;
 };
 
+// Optimiser state of a warp-class fit handed from fit_multi_warp_kernel to
+// the speculative continuation kernel at the start of a Newton iteration.
+struct FitState {
+  double log_sp[kWarpM];
+  double newton[kWarpM];
+  double steep[kWarpM];
+  double gradient[kWarpM];
+  double hess[kWarpM * kWarpM];
+  double min_score;
+  double score_red;
+  int it;
+  int calls;
+  int steepest;
+  int pad;
+};
+
 // One CI test: statistic between two residual components.
 struct PairJob {
   int left;        // component index

@@ -33,7 +33,8 @@ cudaError_t launch_gcv_adjoint(int qmax_class, const DesignDev* designs, int des
 cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const double* arena, const double* data,
                              int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
                              FitResult* results, cudaStream_t stream,
-                             int selection = 0, double* workspace = nullptr);
+                             int selection = 0, double* workspace = nullptr, FitState* states = nullptr,
+                             int* defer_list = nullptr, int* defer_count = nullptr);
 // Doubles of global workspace class ``qmax_class`` needs for ``count`` fits
 // (class 2: q <= 112, rsum <= 96, working set in global memory; 0 otherwise).
 size_t multi_workspace_doubles(int qmax_class, int count);

@@ -275,6 +275,7 @@ constexpr double kGnGradTol = 1e-9;   // Gauss-Newton selection: |grad V| <= 1e-
 constexpr double kGnFlatTol = 1e-12;  // or a decrease <= 1e-12 (1 + V)
 constexpr double kGnFlatGrad = 1e-6;  // with |grad V| <= 1e-6 (1 + V)
 constexpr double kGnMaxLogSp = 25.0;  // upper bound of the Gauss-Newton search in log(lambda)
+constexpr int kDeferCalls = 40;       // warp-class fits past this many evaluations continue speculatively
 
 __device__ __forceinline__ int tri(int i, int j) { return j * (j + 1) / 2 + i; }  // packed upper, i <= j
 
@@ -1193,11 +1194,23 @@ struct WarpScalars {
   int rowblk[kWarpR];  // penalty block of each stacked root row (-1 beyond rsum)
 };
 
-// Per-CTA state of the warp kernel (one warp per CTA).  File scope, so that
-// the out-of-line evaluation and derivative routines address it directly.
-__shared__ __align__(16) double s_wsm[WarpLayout::TOTAL];
-__shared__ WarpScalars s_wsc;
-__shared__ DesignDev s_wdes;
+// Per-warp state of the warp kernels: one slot of dynamic shared memory per
+// warp (work arrays, scalars, design descriptor), addressed from the file-scope
+// array so that the out-of-line evaluation and derivative routines keep
+// shared-memory addressing.
+extern __shared__ __align__(16) double s_warp_dyn[];
+constexpr int kWarpScalarDoubles = static_cast<int>((sizeof(WarpScalars) + 7) / 8);
+constexpr int kWarpDesignDoubles = static_cast<int>((sizeof(DesignDev) + 7) / 8);
+constexpr int kWarpSlotDoubles = (WarpLayout::TOTAL + kWarpScalarDoubles + kWarpDesignDoubles + 1) & ~1;
+constexpr size_t kWarpSlotBytes = sizeof(double) * kWarpSlotDoubles;
+
+__device__ __forceinline__ double* warp_slot() { return s_warp_dyn + (threadIdx.x >> 5) * kWarpSlotDoubles; }
+__device__ __forceinline__ WarpScalars& warp_scalars() {
+  return *reinterpret_cast<WarpScalars*>(warp_slot() + WarpLayout::TOTAL);
+}
+__device__ __forceinline__ DesignDev& warp_design() {
+  return *reinterpret_cast<DesignDev*>(warp_slot() + WarpLayout::TOTAL + kWarpScalarDoubles);
+}
 
 // Asynchronous 16-byte global -> shared copies (cp.async, L1-allocating).
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -1269,7 +1282,7 @@ __device__ __forceinline__ void warp_fold_update(int k, int q, int nz, double be
 template <bool TWO>
 __device__ __forceinline__ void warp_fold_step(int k, int q, WarpScalars& sc, double* X, double* pv,
                                                double (&b0)[kWarpR], double (&b1)[kWarpR], int col0, int col1) {
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31;
   const int nz = sc.nzrow[k];
   if (lane == (k & 31)) {
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
@@ -1371,10 +1384,10 @@ __device__ __forceinline__ double warp_column_dot(const double* __restrict__ W, 
 // columns < q), idg, g, Wg and score / rss / edf in sc.
 __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, int jb0, int jb1) {
   using L = WarpLayout;
-  const DesignDev& des = s_wdes;
-  WarpScalars& sc = s_wsc;
-  double* sm = s_wsm;
-  const int lane = threadIdx.x;
+  const DesignDev& des = warp_design();
+  WarpScalars& sc = warp_scalars();
+  double* sm = warp_slot();
+  const int lane = threadIdx.x & 31;
   const int q = des.q;
   double* X = sm + L::X;
   double* Y = sm + L::Y;
@@ -1454,7 +1467,7 @@ __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, 
 template <int B0>
 __device__ __forceinline__ void warp_block_sums(int q, const double* WT, const double* T, const double* av,
                                                 const double* bv, const WarpScalars& sc, double (&p)[kWarpM][4]) {
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31;
   double c[16], d[16];
 #pragma unroll
   for (int u = 0; u < 16; ++u) c[u] = d[u] = 0.0;
@@ -1493,10 +1506,10 @@ __device__ __forceinline__ void warp_block_sums(int q, const double* WT, const d
 // quantities of multi_derivatives).  jrow: penalty block of stacked row ``lane``.
 __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, int n, int jrow) {
   using L = WarpLayout;
-  const DesignDev& des = s_wdes;
-  WarpScalars& sc = s_wsc;
-  double* sm = s_wsm;
-  const int lane = threadIdx.x;
+  const DesignDev& des = warp_design();
+  WarpScalars& sc = warp_scalars();
+  double* sm = warp_slot();
+  const int lane = threadIdx.x & 31;
   const int q = des.q, m = des.m;
   double* X = sm + L::X;
   const double* Y = sm + L::Y;
@@ -1624,13 +1637,13 @@ __device__ __noinline__ void warp_fit_setup(const DesignDev* __restrict__ design
                                             const double* __restrict__ y, int n, int* jb0_out, int* jb1_out,
                                             int* jrow_out) {
   using L = WarpLayout;
-  double* sm = s_wsm;
-  WarpScalars& sc = s_wsc;
-  const DesignDev& des = s_wdes;
-  const int lane = threadIdx.x;
+  double* sm = warp_slot();
+  WarpScalars& sc = warp_scalars();
+  const DesignDev& des = warp_design();
+  const int lane = threadIdx.x & 31;
   {
     const int* src = reinterpret_cast<const int*>(design);
-    int* dst = reinterpret_cast<int*>(&s_wdes);
+    int* dst = reinterpret_cast<int*>(&warp_design());
     for (int i = lane; i < static_cast<int>(sizeof(DesignDev) / sizeof(int)); i += 32) dst[i] = src[i];
   }
   if (lane == 0) {
@@ -1686,13 +1699,16 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
                                                             const FitJob* __restrict__ jobs,
                                                             const int* __restrict__ job_index, int job_count,
                                                             double* __restrict__ residuals,
-                                                            FitResult* __restrict__ results, int selection) {
+                                                            FitResult* __restrict__ results, int selection,
+                                                            int defer_calls, FitState* __restrict__ states,
+                                                            int* __restrict__ defer_list,
+                                                            int* __restrict__ defer_count) {
   using L = WarpLayout;
-  double* sm = s_wsm;
-  WarpScalars& sc = s_wsc;
-  const DesignDev& des = s_wdes;
+  double* sm = warp_slot();
+  WarpScalars& sc = warp_scalars();
+  const DesignDev& des = warp_design();
   if (blockIdx.x >= job_count) return;
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31;
   const int t = job_index[blockIdx.x];
   const FitJob job = jobs[t];
   int jb0 = -1, jb1 = -1, jrow = -1;
@@ -1767,6 +1783,27 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
   } else {
     for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
       int tries = 0;
+      if (it > 1 && defer_calls > 0 && calls >= defer_calls) {
+        // a long search: hand it, at this iteration boundary, to the
+        // speculative continuation kernel (several trials at once)
+        FitState& st = states[t];
+        if (lane < m) {
+          st.log_sp[lane] = sc.log_sp[lane];
+          st.newton[lane] = sc.newton[lane];
+          st.steep[lane] = sc.steep[lane];
+          st.gradient[lane] = sc.gradient[lane];
+          for (int j = 0; j < m; ++j) st.hess[lane + kWarpM * j] = sc.hess_c[lane + WarpScalars::kLd * j];
+        }
+        if (lane == 0) {
+          st.min_score = min_score;
+          st.score_red = score_red;
+          st.it = it;
+          st.calls = calls;
+          st.steepest = steepest ? 1 : 0;
+          defer_list[atomicAdd(defer_count, 1)] = t;
+        }
+        return;
+      }
       if (it > 1) {
         if (lane < m) sc.step[lane] = steepest ? sc.steep[lane] : sc.newton[lane];
         __syncwarp();
@@ -1891,6 +1928,266 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
   }
 }
 
+// ------------------------------------------------------ speculative continuation
+//
+// fit_multi_spec_kernel: the fits that fit_multi_warp_kernel deferred (more
+// than defer_calls evaluations), one per CTA of kSpecWarps warps, each warp
+// with its own slot.  Within a Newton iteration magic's trial steps are fixed
+// in advance -- the Newton step halved for tries 1-3, then (unless already
+// steepest) the steepest-descent step halved, the step zero at try 25 -- and
+// a trial is accepted on its own score, so the warps evaluate kSpecWarps
+// consecutive trials at once and the first accepted one in sequence order is
+// taken: the same point, score and derivatives as the sequential search.  The
+// boundary probes are speculated the same way; the terminal polish and the
+// final fit run on warp 0.
+constexpr int kSpecWarps = 6;
+
+struct SpecShared {
+  double score[kSpecWarps];
+  int status[kSpecWarps];
+  int dec;                    // decision broadcast: accepted / failed trial
+  int dec_warp;
+  double log_sp[kWarpM];      // state after the accepted trial
+  double newton[kWarpM];
+  double steep[kWarpM];
+  double gradient[kWarpM];
+  double min_score;
+  double score_red;
+  int steepest;
+  int converged;
+  int fail;
+};
+
+__global__ void __launch_bounds__(32 * kSpecWarps) fit_multi_spec_kernel(
+    const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data, int n,
+    const FitJob* __restrict__ jobs, const int* __restrict__ defer_list, const int* __restrict__ defer_count,
+    const FitState* __restrict__ states, double* __restrict__ residuals, FitResult* __restrict__ results) {
+  using L = WarpLayout;
+  __shared__ SpecShared ss;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int total = *defer_count;
+  const int max_half = 25;
+  for (int di = blockIdx.x; di < total; di += gridDim.x) {
+    const int t = defer_list[di];
+    const FitJob job = jobs[t];
+    const double* y = data + static_cast<int64_t>(n) * job.column;
+    int jb0 = -1, jb1 = -1, jrow = -1;
+    warp_fit_setup(designs + job.design, arena, y, n, &jb0, &jb1, &jrow);
+    WarpScalars& sc = warp_scalars();
+    const DesignDev& des = warp_design();
+    const int m = des.m, q = des.q;
+    const FitState& st = states[t];
+    if (lane < m) {
+      sc.log_sp[lane] = st.log_sp[lane];
+      sc.newton[lane] = st.newton[lane];
+      sc.steep[lane] = st.steep[lane];
+      sc.gradient[lane] = st.gradient[lane];
+      for (int j = 0; j < m; ++j) sc.hess_c[lane + WarpScalars::kLd * j] = st.hess[lane + kWarpM * j];
+    }
+    double min_score = st.min_score;
+    int calls = st.calls;
+    bool steepest = st.steepest != 0;
+    bool converged = false;
+    int status = kStatusOk;
+    int it = st.it;
+    __syncwarp();
+    for (; it <= kMaxIterations && status == kStatusOk; ++it) {
+      // trial tt (1-based) of this iteration: tt <= 3 Newton (unless
+      // steepest), then steepest descent, halved at every rejection; zero at 25
+      const bool s0 = steepest;
+      int accepted = 0, failed = 0, tries = 0;
+      for (int base = 1; base <= max_half && !accepted && !failed; base += kSpecWarps) {
+        const int tt = base + warp;
+        if (tt <= max_half) {
+          if (lane < m) {
+            double stp;
+            if (tt == max_half) stp = 0.0;
+            else if (!s0 && tt <= 3) stp = ldexp(sc.newton[lane], -(tt - 1));
+            else if (!s0) stp = ldexp(sc.steep[lane], -(tt - 4));
+            else stp = ldexp(sc.steep[lane], -(tt - 1));
+            sc.trial[lane] = sc.log_sp[lane] + stp;
+          }
+          __syncwarp();
+          warp_core(arena, n, jb0, jb1);
+          if (lane == 0) {
+            ss.score[warp] = sc.score;
+            ss.status[warp] = sc.status;
+          }
+        }
+        __syncthreads();
+        for (int w = 0; w < kSpecWarps && base + w <= max_half; ++w) {
+          tries = base + w;
+          if (ss.status[w] != kStatusOk) {
+            failed = ss.status[w];
+            break;
+          }
+          if (ss.score[w] < min_score) {
+            accepted = w + 1;  // warp index + 1
+            break;
+          }
+        }
+        __syncthreads();
+      }
+      calls += tries;
+      if (failed) {
+        status = failed;
+        break;
+      }
+      if (accepted) {
+        const int aw = accepted - 1;
+        if (warp == aw) {
+          if (lane == 0) {
+            ss.score_red = min_score - sc.score;
+            ss.min_score = sc.score;
+          }
+          if (lane < m) sc.log_sp[lane] = sc.trial[lane];
+          __syncwarp();
+          warp_derivatives(arena, n, jrow);
+          double g2 = 0.0;
+          for (int r = 0; r < m; ++r) g2 += sc.gradient[r] * sc.gradient[r];  // the previous gradient
+          bool conv = false;
+          if (it > 3) {
+            const double ms = ss.min_score;
+            conv = ss.score_red <= kConvTol * (1.0 + ms) && sqrt(g2) <= pow(kConvTol, 1.0 / 3.0) * (1.0 + fabs(ms));
+          }
+          if (lane == 0) {
+            for (int r = 0; r < m; ++r) sc.gradient[r] = sc.grad_c[r];
+            bool stp = false;
+            newton_from_hessian(m, &sc, &stp);
+            ss.steepest = stp ? 1 : 0;
+            ss.converged = conv ? 1 : 0;
+            ss.fail = sc.status;
+            for (int r = 0; r < m; ++r) {
+              ss.log_sp[r] = sc.log_sp[r];
+              ss.newton[r] = sc.newton[r];
+              ss.steep[r] = sc.steep[r];
+              ss.gradient[r] = sc.gradient[r];
+            }
+          }
+          __syncwarp();
+        }
+        __syncthreads();
+        // every warp takes the accepted state
+        if (lane < m) {
+          sc.log_sp[lane] = ss.log_sp[lane];
+          sc.newton[lane] = ss.newton[lane];
+          sc.steep[lane] = ss.steep[lane];
+          sc.gradient[lane] = ss.gradient[lane];
+        }
+        __syncwarp();
+        min_score = ss.min_score;
+        steepest = ss.steepest != 0;
+        converged = ss.converged != 0;
+        if (ss.fail != kStatusOk) status = ss.fail;
+        __syncthreads();
+      } else {
+        // no decrease in 25 tries: converged; the Newton direction is unchanged
+        if (it > 3) converged = true;
+      }
+      if (converged || status != kStatusOk) break;
+    }
+    if (status == kStatusOk && !converged) status = kStatusNotConverged;
+    // boundary probes: +-2 up to five times per coordinate, kSpecWarps at once
+    if (status == kStatusOk) {
+      for (int c = 0; c < m && status == kStatusOk; ++c) {
+        const double direction = sc.gradient[c] < 0.0 ? 1.0 : -1.0;
+        int taken = 0;
+        bool stop = false;
+        for (int base = 1; base <= 5 && !stop; base += kSpecWarps) {
+          const int k = base + warp;  // probe k moves coordinate c by 2 k, as k successive +-2 steps
+          if (k <= 5) {
+            if (lane < m) {
+              double v = sc.log_sp[lane];
+              if (lane == c)
+                for (int u = 0; u < k; ++u) v = v + direction * 2.0;
+              sc.trial[lane] = v;
+            }
+            __syncwarp();
+            warp_core(arena, n, jb0, jb1);
+            if (lane == 0) {
+              ss.score[warp] = sc.score;
+              ss.status[warp] = sc.status;
+            }
+          }
+          __syncthreads();
+          double best = min_score;
+          for (int w = 0; w < kSpecWarps && base + w <= 5; ++w) {
+            ++calls;
+            if (ss.status[w] != kStatusOk) {
+              status = ss.status[w];
+              stop = true;
+              break;
+            }
+            if (!(ss.score[w] < best)) {
+              stop = true;
+              break;
+            }
+            best = ss.score[w];
+            taken = base + w;
+          }
+          min_score = best;
+          __syncthreads();
+        }
+        if (lane == c)
+          for (int u = 0; u < taken; ++u) sc.log_sp[c] = sc.log_sp[c] + direction * 2.0;
+        __syncwarp();
+      }
+    }
+    // terminal polish and the final fit on warp 0
+    if (warp == 0) {
+      if (status == kStatusOk) {
+        if (lane == 0) sc.status = kStatusOk;
+        if (lane < m) sc.trial[lane] = sc.log_sp[lane];
+        __syncwarp();
+        warp_core(arena, n, jb0, jb1);
+        for (int ps = 0; ps < kPolishSteps && sc.status == kStatusOk; ++ps) {
+          warp_derivatives(arena, n, jrow);
+          if (lane == 0) sc.ctl = polish_step(m, &sc);
+          __syncwarp();
+          const int act = sc.ctl;
+          __syncwarp();
+          if (act == 0) break;
+          if (lane < m) sc.trial[lane] = sc.log_sp[lane];
+          __syncwarp();
+          warp_core(arena, n, jb0, jb1);
+          ++calls;
+          if (act == 2) break;
+        }
+        if (sc.status == kStatusOk) {
+          __syncwarp();
+          if (lane < m) sc.trial[lane] = sc.log_sp[lane];
+          __syncwarp();
+          warp_core(arena, n, jb0, jb1);
+        }
+        status = sc.status;
+      }
+      const double* Q = arena + des.basis;
+      const double* wg = warp_slot() + L::WG;
+      double* r = residuals + static_cast<int64_t>(n) * job.out;
+      const bool ok = status == kStatusOk;
+      for (int i = lane; i < n; i += 32) {
+        double f = 0.0;
+        if (ok)
+          for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * wg[c];
+        r[i] = ok ? y[i] - f : NAN;
+      }
+      if (lane == 0) {
+        FitResult res;
+        for (int j = 0; j < kMaxPenalties; ++j) res.log_sp[j] = j < m ? sc.log_sp[j] : NAN;
+        res.score = sc.score;
+        res.edf = sc.edf;
+        res.rss = sc.rss;
+        res.status = status;
+        res.iterations = it;
+        res.evaluations = calls;
+        res.flags = 0;
+        results[t] = res;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------ GCV adjoint
 //
 // Score V, gradient, exact Hessian and Gauss-Newton Hessian of V in
@@ -1906,11 +2203,11 @@ __global__ void __launch_bounds__(32) gcv_adjoint_warp_kernel(const DesignDev* _
                                                               double* __restrict__ score, double* __restrict__ grad,
                                                               double* __restrict__ gn, double* __restrict__ hess,
                                                               int* __restrict__ status) {
-  WarpScalars& sc = s_wsc;
-  const DesignDev& des = s_wdes;
+  WarpScalars& sc = warp_scalars();
+  const DesignDev& des = warp_design();
   const int pt = blockIdx.x;
   if (pt >= count) return;
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31;
   int jb0 = -1, jb1 = -1, jrow = -1;
   warp_fit_setup(designs + design, arena, y, n, &jb0, &jb1, &jrow);
   const int m = des.m;
@@ -1970,7 +2267,7 @@ __global__ void __launch_bounds__(kMultiThreads, 1) gcv_adjoint_kernel(
 }
 
 size_t multi_smem_bytes(int qmax_class) {
-  if (qmax_class == 0) return sizeof(double) * WarpLayout::TOTAL + sizeof(WarpScalars) + sizeof(DesignDev);
+  if (qmax_class == 0) return kWarpSlotBytes;
   if (qmax_class == 1) return sizeof(double) * MultiLayout<76, 64>::TOTAL;
   return 0;  // class 2 works in global memory
 }
@@ -1982,6 +2279,9 @@ size_t multi_workspace_doubles(int qmax_class, int count) {
 cudaError_t configure_fit_kernels() {
   cudaError_t e = cudaFuncSetAttribute(fit_multi_warp_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(fit_multi_spec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(kSpecWarps * kWarpSlotBytes));
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(fit_multi_kernel<76, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(multi_smem_bytes(1)));
@@ -1995,8 +2295,8 @@ cudaError_t launch_gcv_adjoint(int qmax_class, const DesignDev* designs, int des
                                double* gn, double* hess, int* status, cudaStream_t stream, double* workspace) {
   if (count <= 0) return cudaSuccess;
   if (qmax_class == 0) {
-    gcv_adjoint_warp_kernel<<<count, 32, 0, stream>>>(designs, design, arena, y, n, rho, count, score, grad, gn, hess,
-                                                      status);
+    gcv_adjoint_warp_kernel<<<count, 32, kWarpSlotBytes, stream>>>(designs, design, arena, y, n, rho, count, score,
+                                                                   grad, gn, hess, status);
   } else if (qmax_class == 1) {
     gcv_adjoint_kernel<76, 64><<<count, kMultiThreads, multi_smem_bytes(1), stream>>>(
         designs, design, arena, y, n, rho, count, score, grad, gn, hess, status, nullptr);
@@ -2020,11 +2320,28 @@ cudaError_t launch_fit_single(const DesignDev* designs, const double* arena, con
 
 cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const double* arena, const double* data,
                              int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
-                             FitResult* results, cudaStream_t stream, int selection, double* workspace) {
+                             FitResult* results, cudaStream_t stream, int selection, double* workspace,
+                             FitState* states, int* defer_list, int* defer_count) {
   if (count <= 0) return cudaSuccess;
   if (qmax_class == 0) {
-    fit_multi_warp_kernel<<<count, 32, 0, stream>>>(designs, arena, data, n, jobs, job_index, count, residuals,
-                                                    results, selection);
+    // fits still searching after kDeferCalls evaluations continue in the
+    // speculative kernel (magic selection, with the deferral buffers given)
+    const bool defer = states && defer_list && defer_count && selection == FKPC_SELECT_MAGIC;
+    if (defer) {
+      cudaError_t e = cudaMemsetAsync(defer_count, 0, sizeof(int), stream);
+      if (e != cudaSuccess) return e;
+    }
+    fit_multi_warp_kernel<<<count, 32, kWarpSlotBytes, stream>>>(designs, arena, data, n, jobs, job_index, count,
+                                                                 residuals, results, selection,
+                                                                 defer ? kDeferCalls : 0, states, defer_list,
+                                                                 defer_count);
+    if (defer) {
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      const int ctas = count < 148 ? count : 148;
+      fit_multi_spec_kernel<<<ctas, 32 * kSpecWarps, kSpecWarps * kWarpSlotBytes, stream>>>(
+          designs, arena, data, n, jobs, defer_list, defer_count, states, residuals, results);
+    }
   } else if (qmax_class == 1) {
     fit_multi_kernel<76, 64><<<count, kMultiThreads, multi_smem_bytes(1), stream>>>(
         designs, arena, data, n, jobs, job_index, count, residuals, results, selection, nullptr);

@@ -458,6 +458,11 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   h2d_bytes_ += upload(d_multi_small_, multi_small_, stream_);
   h2d_bytes_ += upload(d_multi_large_, multi_large_, stream_);
   h2d_bytes_ += upload(d_multi_huge_, multi_huge_, stream_);
+  if (!multi_small_.empty()) {
+    d_fit_states_.ensure(multi_jobs_.size());
+    d_defer_list_.ensure(multi_small_.size());
+    d_defer_count_.ensure(1);
+  }
   if (!multi_huge_.empty()) d_fit_ws_.ensure(multi_workspace_doubles(2, static_cast<int>(multi_huge_.size())));
   h2d_bytes_ += upload(d_direct_cols_, direct_cols_, stream_);
   h2d_bytes_ += upload(d_direct_slots_, direct_slots_, stream_);
@@ -542,9 +547,10 @@ void Engine::enqueue() {
   if (!multi_small_.empty()) {
     cuda_check(launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                 d_multi_small_.get(), static_cast<int>(multi_small_.size()), d_resid_.get(),
-                                d_multi_res_.get(), stream_, opt_.selection),
+                                d_multi_res_.get(), stream_, opt_.selection, nullptr, d_fit_states_.get(),
+                                d_defer_list_.get(), d_defer_count_.get()),
                "fit multi");
-    ++launches_;
+    launches_ += opt_.selection == FKPC_SELECT_MAGIC ? 2 : 1;  // with the speculative continuation
   }
   if (!multi_large_.empty()) {
     cuda_check(launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
@@ -946,7 +952,8 @@ double Engine::time_stage(int stage, int repeats, double* flops_per_launch) {
                                        static_cast<int>(single_jobs_.size()), d_resid_.get(), d_single_res_.get(), stream_);
       case 1: return launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                       d_multi_small_.get(), static_cast<int>(multi_small_.size()), d_resid_.get(),
-                                      d_multi_res_.get(), stream_, opt_.selection);
+                                      d_multi_res_.get(), stream_, opt_.selection, nullptr, d_fit_states_.get(),
+                                      d_defer_list_.get(), d_defer_count_.get());
       case 2: return launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                       d_multi_large_.get(), static_cast<int>(multi_large_.size()), d_resid_.get(),
                                       d_multi_res_.get(), stream_, opt_.selection);

@@ -143,6 +143,8 @@ class Engine {
   DevBuf<FitJob> d_single_jobs_, d_multi_jobs_;
   DevBuf<int> d_multi_small_, d_multi_large_, d_multi_huge_, d_direct_cols_, d_direct_slots_, d_comp_cols_;
   DevBuf<double> d_fit_ws_;  // global working sets of the widest fit class
+  DevBuf<FitState> d_fit_states_;  // optimiser states handed to the speculative continuation
+  DevBuf<int> d_defer_list_, d_defer_count_;
   // device thin-plate Lanczos of the bivariate designs
   DevBuf<double> d_tprs_u_, d_tprs_V_, d_tprs_ab_, d_tprs_ews_;
   DevBuf<int64_t> d_tprs_uoff_, d_tprs_voff_;

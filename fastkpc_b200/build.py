@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfastkpc_b200.so")
-SOURCES = ["hostla.cpp", "design.cpp", "capi.cpp", "runtime.cu", "kernels_fit.cu", "kernels_stat.cu", "kernels_tprs.cu", "noalloc.cu"]
+SOURCES = ["hostla.cpp", "design.cpp", "capi.cpp", "runtime.cu", "kernels_fit.cu", "kernels_stat.cu", "kernels_tprs.cu", "kernels_geom.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 
@@ -46,8 +46,6 @@ def build(force=False, verbose=False):
                 and os.path.getmtime(obj) >= newest_header):
             continue
         cmd = [nvcc(), *ARCH, *COMMON, "-c", path, "-o", obj]
-        if src.endswith(".cpp"):
-            cmd[1:1] = ["-x", "cu"] if False else []
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

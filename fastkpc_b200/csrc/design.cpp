@@ -355,17 +355,31 @@ Smooth build_smooth(const double* cols, int n, int d, int k) {
   return tprs_finish(prep, vals, U);
 }
 
-std::vector<double> initial_sp(const Design& des) {
-  const int n = des.n, q = des.q;
-  std::vector<double> xdiag(q);
-  for (int c = 0; c < q; ++c) {
+namespace {
+
+// Sum of squares of each column of an n x cols matrix, accumulated in long
+// double in row order.
+std::vector<double> column_sumsq(const double* X, int n, int cols) {
+  std::vector<double> out(cols);
+  for (int c = 0; c < cols; ++c) {
     long double t = 0.0L;
     for (int r = 0; r < n; ++r) {
-      double v = des.X[r + static_cast<size_t>(n) * c];
+      double v = X[r + static_cast<size_t>(n) * c];
       t += v * v;
     }
-    xdiag[c] = static_cast<double>(t);
+    out[c] = static_cast<double>(t);
   }
+  return out;
+}
+
+}  // namespace
+
+std::vector<double> initial_sp(const Design& des) {
+  return initial_sp_from_colsq(des, column_sumsq(des.X.data(), des.n, des.q));
+}
+
+std::vector<double> initial_sp_from_colsq(const Design& des, const std::vector<double>& xdiag) {
+  const int q = des.q;
   std::vector<double> pdiag(q, 0.0);
   std::vector<char> penalized(q, 0);
   const double thr_scale = std::pow(2.220446049250313e-16, 0.8);
@@ -478,25 +492,58 @@ void prepare_geometry(Design* des) {
       }
   } else {
     des->roots.clear();
-    for (int j = 0; j < des->m; ++j) {
-      const int dim = des->dims[j], rank = des->ranks[j];
-      std::vector<double> S = des->blocks[j];
-      for (int c = 0; c < dim; ++c)
-        for (int r = c + 1; r < dim; ++r) {
-          double s = 0.5 * (S[r + static_cast<size_t>(dim) * c] + S[c + static_cast<size_t>(dim) * r]);
-          S[r + static_cast<size_t>(dim) * c] = S[c + static_cast<size_t>(dim) * r] = s;
-        }
-      std::vector<double> vals, vecs;
-      jacobi_eigen(S.data(), dim, &vals, &vecs);
-      std::vector<double> root(static_cast<size_t>(dim) * rank);
-      for (int c = 0; c < rank; ++c) {
-        const int src = dim - 1 - c;
-        const double s = std::sqrt(std::max(0.0, vals[src]));
-        for (int r = 0; r < dim; ++r) root[r + static_cast<size_t>(dim) * c] = vecs[r + static_cast<size_t>(dim) * src] * s;
-      }
-      des->roots.push_back(std::move(root));
-    }
+    for (int j = 0; j < des->m; ++j) des->roots.push_back(penalty_root(des->blocks[j], des->dims[j], des->ranks[j]));
   }
+}
+
+std::vector<double> penalty_root(const std::vector<double>& block, int dim, int rank) {
+  std::vector<double> S = block;
+  for (int c = 0; c < dim; ++c)
+    for (int r = c + 1; r < dim; ++r) {
+      double s = 0.5 * (S[r + static_cast<size_t>(dim) * c] + S[c + static_cast<size_t>(dim) * r]);
+      S[r + static_cast<size_t>(dim) * c] = S[c + static_cast<size_t>(dim) * r] = s;
+    }
+  std::vector<double> vals, vecs;
+  jacobi_eigen(S.data(), dim, &vals, &vecs);
+  std::vector<double> root(static_cast<size_t>(dim) * rank);
+  for (int c = 0; c < rank; ++c) {
+    const int src = dim - 1 - c;
+    const double s = std::sqrt(std::max(0.0, vals[src]));
+    for (int r = 0; r < dim; ++r) root[r + static_cast<size_t>(dim) * c] = vecs[r + static_cast<size_t>(dim) * src] * s;
+  }
+  return root;
+}
+
+std::shared_ptr<Design> build_additive_meta(int n, int p, const std::vector<int>& S, DesignCache* cache) {
+  if (S.size() < 3) throw std::runtime_error("an additive design needs |S| >= 3");
+  for (int s : S)
+    if (s < 0 || s >= p) throw std::runtime_error("conditioning index out of range");
+  auto des = std::make_shared<Design>();
+  des->n = n;
+  des->S = S;
+  des->device_geometry = true;
+  for (int s : S) des->parts.push_back(cache->univariate(s));
+  int q = 1;
+  for (auto& sm : des->parts) q += sm->cols;
+  if (q >= n) throw std::runtime_error("design width must be below n");
+  des->q = q;
+  des->m = static_cast<int>(des->parts.size());
+  // the intercept column's sum of squares is n, exactly as accumulated
+  std::vector<double> xdiag(1, column_sumsq(std::vector<double>(n, 1.0).data(), n, 1)[0]);
+  int dest = 1;
+  for (auto& sm : des->parts) {
+    des->blocks.push_back(sm->S);
+    des->offsets.push_back(dest);
+    des->dims.push_back(sm->cols);
+    des->ranks.push_back(sm->rank);
+    des->roots.push_back(sm->root);
+    xdiag.insert(xdiag.end(), sm->colsq.begin(), sm->colsq.end());
+    dest += sm->cols;
+  }
+  std::vector<double> sp = initial_sp_from_colsq(*des, xdiag);
+  des->initial_log_sp.resize(sp.size());
+  for (size_t j = 0; j < sp.size(); ++j) des->initial_log_sp[j] = std::log(sp[j]);
+  return des;
 }
 
 std::shared_ptr<Design> build_design(const double* data, int n, int p, const std::vector<int>& S,
@@ -555,7 +602,10 @@ std::shared_ptr<const Smooth> DesignCache::univariate(int column) {
     auto it = uni_.find(column);
     if (it != uni_.end()) return it->second;
   }
-  auto sm = std::make_shared<Smooth>(build_smooth(data_ + static_cast<size_t>(n_) * column, n_, 1, 10));
+  auto built = std::make_shared<Smooth>(build_smooth(data_ + static_cast<size_t>(n_) * column, n_, 1, 10));
+  built->colsq = column_sumsq(built->X.data(), built->n, built->cols);
+  built->root = penalty_root(built->S, built->cols, built->rank);
+  std::shared_ptr<const Smooth> sm = built;
   std::lock_guard<std::mutex> lock(mu_);
   auto it = uni_.find(column);
   if (it != uni_.end()) return it->second;
@@ -585,7 +635,8 @@ std::shared_ptr<const Design> DesignCache::get(const std::vector<int>& S) {
     auto it = designs_.find(S);
     if (it != designs_.end()) return it->second;
   }
-  std::shared_ptr<const Design> d = build_design(data_, n_, p_, S, this);
+  std::shared_ptr<const Design> d =
+      S.size() >= 3 ? build_additive_meta(n_, p_, S, this) : build_design(data_, n_, p_, S, this);
   std::lock_guard<std::mutex> lock(mu_);
   auto it = designs_.find(S);
   if (it != designs_.end()) return it->second;

@@ -13,6 +13,10 @@ struct Smooth {
   int n = 0, cols = 0, rank = 0;   // cols = k - 1 after the centering constraint
   std::vector<double> X;           // n x cols, column-major
   std::vector<double> S;           // cols x cols penalty
+  // univariate smooths of the design cache only: what every additive design
+  // containing the variable reuses
+  std::vector<double> colsq;       // cols: sum of squares of each column of X
+  std::vector<double> root;        // cols x rank: root root' = S
 };
 
 // One conditioning set's model: X = [1 | smooth_1 | ... ] with one penalty
@@ -32,6 +36,10 @@ struct Design {
   std::vector<double> QW;                   // n x q: Q * W, W the whitened eigenvectors
   // several penalties: per block root (dim_j x rank_j), root root' = S_j
   std::vector<std::vector<double>> roots;
+  // additive designs of the design cache: X, Q and R are not formed on the
+  // host; the device gathers X from these bases and factors it
+  bool device_geometry = false;
+  std::vector<std::shared_ptr<const Smooth>> parts;
 };
 
 // Thin-plate set-up in three parts, so that the top-k eigen problem of the
@@ -39,6 +47,8 @@ struct Design {
 // prepare (unique locations, polynomial null-space basis), the eta matrix,
 // and finish (constraint absorption, scaling, centering) from its top-k
 // eigenpairs (descending, largest-magnitude entry of each vector positive).
+class DesignCache;
+
 struct TprsPrep {
   int n = 0, d = 0, k = 0, m = 0, M = 0, nu = 0;
   std::vector<double> u;      // nu x d unique (shifted) locations, column-major
@@ -52,7 +62,14 @@ Smooth tprs_finish(const TprsPrep& prep, const std::vector<double>& vals, const 
 Smooth build_smooth(const double* cols, int n, int d, int k);
 double r_mean(const double* v, int n);
 std::vector<double> initial_sp(const Design& des);
+// initial.sp from the sums of squares of the columns of X (q)
+std::vector<double> initial_sp_from_colsq(const Design& des, const std::vector<double>& xdiag);
+// root (dim x rank) of a symmetric penalty block: root root' = block
+std::vector<double> penalty_root(const std::vector<double>& block, int dim, int rank);
 void prepare_geometry(Design* des);
+// An additive (|S| >= 3) design without X, Q or R: blocks, roots and
+// initial.sp from the cache's univariate smooths (device_geometry set).
+std::shared_ptr<Design> build_additive_meta(int n, int p, const std::vector<int>& S, DesignCache* cache);
 
 // Cache of univariate smooths (shared by every additive model containing the
 // variable) and of full designs per conditioning set.

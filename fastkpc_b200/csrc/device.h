@@ -49,6 +49,20 @@ struct DesignDev {
   double log_sp0[kMaxPenalties];
 };
 
+// One additive design whose geometry the device builds: X = [1 | B_1 | ...]
+// gathered from the univariate smooth bases, X = Q R by Householder, Q and R
+// (and row-packed R) written to the arena.
+struct GeomJob {
+  int64_t basis;                 // arena offset of Q (n x q)
+  int64_t rmat;                  // arena offset of R (q x q)
+  int64_t rpack;                 // arena offset of row-packed R, or -1
+  int64_t src[kMaxPenalties];    // smooth j's first column in the basis table (n x dim_j)
+  int off[kMaxPenalties];
+  int dim[kMaxPenalties];
+  int q;
+  int m;
+};
+
 // One residual fit: data column ``column`` regressed on design ``design``.
 struct FitJob {
   int design;

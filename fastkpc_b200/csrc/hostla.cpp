@@ -7,30 +7,44 @@
 
 namespace fkpc {
 
-void householder_qr(const double* A, int rows, int cols, std::vector<double>* Q,
-                    std::vector<double>* R) {
-  if (rows < cols || cols <= 0) throw std::runtime_error("householder_qr: need rows >= cols > 0");
+namespace {
+
+// Dot product with eight independent partial sums: the chains overlap and
+// the compiler vectorises them without reassociation flags.
+__attribute__((always_inline)) inline double dot_chains(const double* a, const double* b, int len) {
+  double s[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  int i = 0;
+  for (; i + 8 <= len; i += 8)
+    for (int t = 0; t < 8; ++t) s[t] += a[i + t] * b[i + t];
+  double tail = 0.0;
+  for (; i < len; ++i) tail += a[i] * b[i];
+  return (((s[0] + s[4]) + (s[1] + s[5])) + ((s[2] + s[6]) + (s[3] + s[7]))) + tail;
+}
+
+// Householder QR, Q formed explicitly by backward accumulation.  When H_k is
+// applied to the columns of the (partial) Q, columns j < k are still e_j,
+// which H_k leaves alone, so only columns k.. are touched.
+__attribute__((always_inline)) inline void householder_qr_core(const double* A, int rows, int cols,
+                                                              std::vector<double>* Q, std::vector<double>* R) {
   std::vector<double> W(A, A + static_cast<size_t>(rows) * cols);
   std::vector<double> V(static_cast<size_t>(rows) * cols, 0.0);
   std::vector<double> beta(cols, 0.0);
   for (int k = 0; k < cols; ++k) {
     double* x = &W[static_cast<size_t>(k) * rows];
-    double norm2 = 0.0;
-    for (int i = k; i < rows; ++i) norm2 += x[i] * x[i];
-    double norm = std::sqrt(norm2);
+    const int len = rows - k;
+    const double norm2 = dot_chains(x + k, x + k, len);
+    const double norm = std::sqrt(norm2);
     double* v = &V[static_cast<size_t>(k) * rows];
     if (norm == 0.0) { beta[k] = 0.0; continue; }
-    double alpha = x[k] >= 0.0 ? -norm : norm;
+    const double alpha = x[k] >= 0.0 ? -norm : norm;
     for (int i = k; i < rows; ++i) v[i] = x[i];
     v[k] -= alpha;
-    double vnorm2 = norm2 - x[k] * x[k] + v[k] * v[k];
+    const double vnorm2 = norm2 - x[k] * x[k] + v[k] * v[k];
     beta[k] = 2.0 / vnorm2;
     // apply H = I - beta v v' to columns k..cols-1
     for (int j = k; j < cols; ++j) {
       double* c = &W[static_cast<size_t>(j) * rows];
-      double dot = 0.0;
-      for (int i = k; i < rows; ++i) dot += v[i] * c[i];
-      dot *= beta[k];
+      const double dot = dot_chains(v + k, c + k, len) * beta[k];
       for (int i = k; i < rows; ++i) c[i] -= dot * v[i];
     }
   }
@@ -42,14 +56,34 @@ void householder_qr(const double* A, int rows, int cols, std::vector<double>* Q,
   for (int k = cols - 1; k >= 0; --k) {
     if (beta[k] == 0.0) continue;
     const double* v = &V[static_cast<size_t>(k) * rows];
-    for (int j = 0; j < cols; ++j) {
+    const int len = rows - k;
+    for (int j = k; j < cols; ++j) {
       double* c = &(*Q)[static_cast<size_t>(j) * rows];
-      double dot = 0.0;
-      for (int i = k; i < rows; ++i) dot += v[i] * c[i];
-      dot *= beta[k];
+      const double dot = dot_chains(v + k, c + k, len) * beta[k];
       for (int i = k; i < rows; ++i) c[i] -= dot * v[i];
     }
   }
+}
+
+__attribute__((target("avx2,fma"))) void householder_qr_avx2(const double* A, int rows, int cols,
+                                                             std::vector<double>* Q, std::vector<double>* R) {
+  householder_qr_core(A, rows, cols, Q, R);
+}
+
+void householder_qr_generic(const double* A, int rows, int cols, std::vector<double>* Q, std::vector<double>* R) {
+  householder_qr_core(A, rows, cols, Q, R);
+}
+
+}  // namespace
+
+// The AVX2/FMA build of the same loops where the host CPU has them, chosen
+// once per process, so every design of a process is factored the same way.
+void householder_qr(const double* A, int rows, int cols, std::vector<double>* Q,
+                    std::vector<double>* R) {
+  if (rows < cols || cols <= 0) throw std::runtime_error("householder_qr: need rows >= cols > 0");
+  static const bool avx2 = __builtin_cpu_supports("avx2") && __builtin_cpu_supports("fma");
+  if (avx2) householder_qr_avx2(A, rows, cols, Q, R);
+  else householder_qr_generic(A, rows, cols, Q, R);
 }
 
 void jacobi_eigen(const double* A, int n, std::vector<double>* values,
@@ -326,49 +360,6 @@ int top_magnitude_eigen(const double* A, int n, int k, std::vector<double>* valu
     for (int i = 0; i < n; ++i) qn[i] = w[i] / beta[j];
   }
   throw std::runtime_error("Lanczos did not converge");
-}
-
-bool ritz_from_lanczos(const double* V, const double* alpha, const double* beta, int n, int m, int k,
-                       std::vector<double>* values, std::vector<double>* vectors) {
-  if (k <= 0 || m < k) return false;
-  std::vector<double> dwork(alpha, alpha + m), ework(m, 0.0);
-  for (int i = 0; i + 1 < m; ++i) ework[i] = beta[i];
-  std::vector<double> S(static_cast<size_t>(m) * m, 0.0);
-  for (int i = 0; i < m; ++i) S[i + static_cast<size_t>(m) * i] = 1.0;
-  if (!tridiagonal_ql(m, dwork.data(), ework.data(), S.data())) return false;
-  std::vector<int> sel = top_k_by_magnitude(dwork, m, k);
-  double tmax = 0.0;
-  for (int i = 0; i < m; ++i) tmax = std::max(tmax, std::fabs(dwork[i]));
-  const bool invariant = std::fabs(beta[m - 1]) <= 1e-15 * tmax;
-  if (!invariant)
-    for (int i : sel)
-      if (std::fabs(beta[m - 1] * S[(m - 1) + static_cast<size_t>(m) * i]) > 1e-14 * tmax) return false;
-  std::stable_sort(sel.begin(), sel.end(), [&](int a, int b) { return dwork[a] > dwork[b]; });
-  values->assign(k, 0.0);
-  vectors->assign(static_cast<size_t>(n) * k, 0.0);
-  for (int c = 0; c < k; ++c) {
-    const int i = sel[c];
-    (*values)[c] = dwork[i];
-    double* out = &(*vectors)[static_cast<size_t>(n) * c];
-    for (int b = 0; b < m; ++b) {
-      const double coef = S[b + static_cast<size_t>(m) * i];
-      const double* vb = V + static_cast<size_t>(n) * b;
-      for (int r = 0; r < n; ++r) out[r] += coef * vb[r];
-    }
-    double nn = std::sqrt(dot(out, out, n));
-    int imax = 0;
-    double amax = -1.0;
-    for (int r = 0; r < n; ++r) {
-      out[r] /= nn;
-      if (std::fabs(out[r]) > amax) {
-        amax = std::fabs(out[r]);
-        imax = r;
-      }
-    }
-    if (out[imax] < 0.0)
-      for (int r = 0; r < n; ++r) out[r] = -out[r];
-  }
-  return true;
 }
 
 }  // namespace fkpc

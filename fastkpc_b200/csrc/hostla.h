@@ -32,11 +32,4 @@ bool tridiagonal_ql(int n, double* d, double* e, double* z);
 int top_magnitude_eigen(const double* A, int n, int k, std::vector<double>* values,
                         std::vector<double>* vectors);
 
-// The same k eigenpairs from a Lanczos run computed elsewhere: basis V
-// (n x m, column-major, orthonormal) and tridiagonal alpha (m), beta (m;
-// beta[m-1] the last residual norm).  False when some selected Ritz pair's
-// residual |beta_m s_m| exceeds 1e-14 max|theta| (not converged).
-bool ritz_from_lanczos(const double* V, const double* alpha, const double* beta, int n, int m, int k,
-                       std::vector<double>* values, std::vector<double>* vectors);
-
 }  // namespace fkpc

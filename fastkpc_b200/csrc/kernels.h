@@ -93,8 +93,25 @@ cudaError_t launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st
 // Thin-plate set-up: Lanczos on the eta matrices of a level's bivariate
 // designs (one CTA per design); see kernels_tprs.cu.
 constexpr int kTprsMaxSteps = 128;
+constexpr int kTprsRitzMax = 30;   // Ritz pairs per design (the basis dimension k of the bivariate smooth)
+constexpr int kTprsMaxNu = 1536;  // unique locations a design may have on the device path
+// eta-matrix workspace per CTA: the leading dimension rounded up to the 32-row tile
+FKPC_HD constexpr int64_t tprs_ld(int nu) { return (static_cast<int64_t>(nu) + 31) / 32 * 32; }
+// Ritz pairs of the Lanczos runs: alpha / beta / done as written by the
+// Lanczos kernel; zws: count x steps^2 workspace; vals: count x k; zsel:
+// count x k x steps; ok[d] = 1 when design d's k pairs converged; U: design
+// d's nu x k Ritz vectors at U + uoff[d].  k must equal kTprsRitzMax.
+cudaError_t launch_tprs_ritz(const double* alpha, const double* beta, const int* done, int count, int steps, int k,
+                             double* zws, double* vals, double* zsel, int* ok, const double* V, const int64_t* voff,
+                             const int* nus, double* U, const int64_t* uoff, cudaStream_t stream);
 cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int* nus, int count, int nu_max,
                                 int steps, double eta0, double* ews, int64_t ews_stride, int ctas, double* V,
                                 const int64_t* voff, double* alpha, double* beta, int* done, cudaStream_t stream);
+
+// Additive-design geometry (X gathered from the univariate bases, Householder
+// QR, Q / R / row-packed R into the arena); see kernels_geom.cu.  status[d]:
+// 1 when design d is rank deficient.  max_q <= 112 and below n.
+cudaError_t launch_additive_geometry(const double* table, int n, const GeomJob* jobs, int count, int max_q,
+                                     double* arena, int* status, cudaStream_t stream);
 
 }  // namespace fkpc

@@ -6,13 +6,24 @@
 // unique locations u (fastkpc/src/full_cuda_ci_native_setup.cpp:114-152, 303).
 // On the host that is about 10 ms of Lanczos per design, hundreds of designs
 // per level.  tprs_lanczos_kernel: one CTA per design (grid-stride over the
-// level's designs); it builds E in its own global workspace, then runs a
-// fixed number of Lanczos steps with full re-orthogonalisation (classical
-// Gram-Schmidt, two passes, as the host) from the host's deterministic start
-// vector.  The basis V and the tridiagonal (alpha, beta) go back to the host,
-// which takes the Ritz pairs, checks their residuals and finishes the basis
-// (ritz_from_lanczos, tprs_finish); a design whose Ritz pairs have not
-// converged is rebuilt on the host.
+// level's designs).  It writes the upper block triangle of E (32 x 32 tiles,
+// leading dimension rounded up to 32, zero padding) to its own global
+// workspace, then runs a fixed number of Lanczos steps with full
+// re-orthogonalisation (classical Gram-Schmidt, two passes) from the host's
+// deterministic start vector.  The Ritz pairs follow on the device too
+// (tprs_ritz_select_kernel, tprs_ritz_vectors_kernel below); the host
+// downloads the k Ritz vectors and values and finishes the basis
+// (tprs_finish).  A design whose Ritz pairs have not converged is rebuilt on
+// the host.
+//
+// The matvec E q is memory-bound: E (up to 1536^2 doubles) is read from L2 or
+// HBM once per step.  It reads each tile of the upper block triangle once:
+// a warp owns whole block columns J (paired J and nb-1-J, so the warps get
+// equal tile counts); tile (I, J) adds its row sums to rows of block I and,
+// for I < J, its column sums (through a transposing shared-memory tile) to
+// rows of block J.  Each warp accumulates into its own slice of row
+// accumulators, summed across warps in a fixed order, so the result does not
+// depend on scheduling.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -25,6 +36,9 @@ namespace fkpc {
 namespace {
 
 constexpr int kTprsThreads = 256;
+constexpr int kTprsWarps = kTprsThreads / 32;
+constexpr int kTile = 32;
+constexpr int kTileWords = kTile * (kTile + 1);  // one warp's transposing tile (padded rows)
 
 __device__ __forceinline__ double warp_sum_t(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -48,37 +62,47 @@ __device__ double block_sum_t(double v, double* red) {
 // column-major).  V: design d's basis at V + voff[d] (nus[d] x steps).
 // alpha / beta: count x steps.  done[d]: steps taken (fewer when the Krylov
 // space became invariant).  ews: per-CTA workspace of ews_stride doubles
-// (>= max nus^2).  Dynamic shared memory: 2 x max nus doubles.
+// (>= tprs_ld(max nus)^2).  Dynamic shared memory: tprs_smem_bytes(max nus).
 __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
     const double* __restrict__ u, const int64_t* __restrict__ uoff, const int* __restrict__ nus, int count,
     int steps, double eta0, double* __restrict__ ews, int64_t ews_stride, double* __restrict__ V,
-    const int64_t* __restrict__ voff, double* __restrict__ alpha, double* __restrict__ beta, int* __restrict__ done) {
+    const int64_t* __restrict__ voff, double* __restrict__ alpha, double* __restrict__ beta, int* __restrict__ done,
+    int ld_max) {
   extern __shared__ double sm[];
-  __shared__ double red[kTprsThreads / 32];
+  __shared__ double red[kTprsWarps];
   __shared__ double coef[kTprsMaxSteps];
   __shared__ double scal[2];
   const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  double* q = sm;                                  // ld_max
+  double* w = sm + ld_max;                         // ld_max
+  double* acc = sm + 2 * static_cast<int64_t>(ld_max);                       // kTprsWarps x ld_max
+  double* tile = acc + static_cast<int64_t>(kTprsWarps) * ld_max + warp * kTileWords;  // this warp's 32 x 33
   for (int d = blockIdx.x; d < count; d += gridDim.x) {
     const int nu = nus[d];
+    const int ld = static_cast<int>(tprs_ld(nu));
+    const int nb = ld / kTile;
     const double* ux = u + uoff[d];
     const double* uy = ux + nu;
     double* E = ews + ews_stride * blockIdx.x;
     double* Vd = V + voff[d];
-    double* q = sm;
-    double* w = sm + nu;
-    // E_ij = eta0 log(r2) / 2 * r2 (the host's order of operations)
-    const int64_t nn = static_cast<int64_t>(nu) * nu;
-    for (int64_t idx = tid; idx < nn; idx += blockDim.x) {
-      const int i = static_cast<int>(idx % nu), j = static_cast<int>(idx / nu);
-      const double dx = ux[i] - ux[j], dy = uy[i] - uy[j];
-      const double r2 = dx * dx + dy * dy;
-      double v = 0.0;
-      if (r2 > 0.0) {
-        v = eta0;
-        v *= log(r2) * 0.5;
-        v *= r2;
+    // upper block triangle of E_ij = eta0 log(r2) / 2 * r2 (zero outside nu x nu)
+    for (int J = 0; J < nb; ++J) {
+      const int rows = kTile * (J + 1);
+      for (int idx = tid; idx < rows * kTile; idx += blockDim.x) {
+        const int i = idx % rows, j = kTile * J + idx / rows;
+        double v = 0.0;
+        if (i < nu && j < nu) {
+          const double dx = ux[i] - ux[j], dy = uy[i] - uy[j];
+          const double r2 = dx * dx + dy * dy;
+          if (r2 > 0.0) {
+            v = eta0;
+            v *= log(r2) * 0.5;
+            v *= r2;
+          }
+        }
+        E[i + static_cast<int64_t>(ld) * j] = v;
       }
-      E[idx] = v;
     }
     if (tid == 0) {
       unsigned long state = 1;
@@ -98,21 +122,58 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
     int taken = 0;
     for (int j = 0; j < steps; ++j) {
       const double* vj = Vd + static_cast<int64_t>(nu) * j;
-      for (int i = tid; i < nu; i += blockDim.x) q[i] = vj[i];
+      for (int i = tid; i < ld; i += blockDim.x) q[i] = i < nu ? vj[i] : 0.0;
+      for (int i = tid; i < kTprsWarps * ld; i += blockDim.x) acc[(i / ld) * static_cast<int64_t>(ld_max) + i % ld] = 0.0;
       __syncthreads();
-      // w = E q: thread per row, four chains, coalesced column walk of E
+      // w = E q over the upper block triangle
+      double* my = acc + static_cast<int64_t>(warp) * ld_max;
+      for (int pidx = warp; 2 * pidx < nb; pidx += kTprsWarps) {
+        for (int half = 0; half < 2; ++half) {
+          const int J = half == 0 ? pidx : nb - 1 - pidx;
+          if (half == 1 && J == pidx) break;
+          const double* Ecol = E + static_cast<int64_t>(ld) * kTile * J;
+          const double* qJ = q + kTile * J;
+          double zc = 0.0;  // lane c: column sum of column 32 J + c over the tiles above the diagonal
+          for (int I = 0; I <= J; ++I) {
+            double e[kTile];
+#pragma unroll
+            for (int c = 0; c < kTile; ++c) e[c] = Ecol[kTile * I + lane + static_cast<int64_t>(ld) * c];
+            double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
+#pragma unroll
+            for (int c = 0; c < kTile; c += 4) {
+              r0 += e[c] * qJ[c];
+              r1 += e[c + 1] * qJ[c + 1];
+              r2 += e[c + 2] * qJ[c + 2];
+              r3 += e[c + 3] * qJ[c + 3];
+            }
+            my[kTile * I + lane] += (r0 + r1) + (r2 + r3);
+            if (I < J) {
+#pragma unroll
+              for (int c = 0; c < kTile; ++c) tile[c * (kTile + 1) + lane] = e[c];
+              __syncwarp();
+              const double* qI = q + kTile * I;
+              const double* trow = tile + lane * (kTile + 1);
+              double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
+#pragma unroll
+              for (int l = 0; l < kTile; l += 4) {
+                c0 += trow[l] * qI[l];
+                c1 += trow[l + 1] * qI[l + 1];
+                c2 += trow[l + 2] * qI[l + 2];
+                c3 += trow[l + 3] * qI[l + 3];
+              }
+              zc += (c0 + c1) + (c2 + c3);
+              __syncwarp();
+            }
+          }
+          my[kTile * J + lane] += zc;
+        }
+      }
+      __syncthreads();
       double part = 0.0;
       for (int i = tid; i < nu; i += blockDim.x) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        int t = 0;
-        for (; t + 3 < nu; t += 4) {
-          s0 += E[i + static_cast<int64_t>(nu) * t] * q[t];
-          s1 += E[i + static_cast<int64_t>(nu) * (t + 1)] * q[t + 1];
-          s2 += E[i + static_cast<int64_t>(nu) * (t + 2)] * q[t + 2];
-          s3 += E[i + static_cast<int64_t>(nu) * (t + 3)] * q[t + 3];
-        }
-        for (; t < nu; ++t) s0 += E[i + static_cast<int64_t>(nu) * t] * q[t];
-        const double s = (s0 + s1) + (s2 + s3);
+        double s = 0.0;
+#pragma unroll
+        for (int v = 0; v < kTprsWarps; ++v) s += acc[static_cast<int64_t>(v) * ld_max + i];
         w[i] = s;
         part += q[i] * s;
       }
@@ -126,8 +187,7 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
       __syncthreads();
       // full re-orthogonalisation, two passes
       for (int pass = 0; pass < 2; ++pass) {
-        const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
-        for (int b0 = 4 * warp; b0 <= j; b0 += 4 * nwarps) {
+        for (int b0 = 4 * warp; b0 <= j; b0 += 4 * kTprsWarps) {
           const double* v0 = Vd + static_cast<int64_t>(nu) * b0;
           const bool h1 = b0 + 1 <= j, h2 = b0 + 2 <= j, h3 = b0 + 3 <= j;
           double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
@@ -194,17 +254,297 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Ritz pairs of the Lanczos runs, on the device.
+//
+// tprs_ritz_select_kernel (one warp per design): the eigen-decomposition of
+// the design's tridiagonal T (alpha, beta; m = done[d] <= steps) by implicit
+// QL with Wilkinson shifts (at most 60 sweeps per eigenvalue), eigenvectors
+// accumulated in a global m x m workspace (lane = row).  It selects the k
+// eigenvalues of largest magnitude (ties to the lower index), orders them by
+// value, descending, and accepts the design only when every selected pair's
+// residual |beta_m s_m| is at most 1e-14 max |theta| (or the Krylov space was
+// invariant); ok[d] = 0 otherwise, and the host builds that design itself.
+// Outputs: vals (count x k) and the selected eigenvectors zsel (count x steps
+// x k, column-major per design).
+//
+// tprs_ritz_vectors_kernel (one CTA per accepted design): U = V zsel (nu x k),
+// each column normalised and signed so that its largest-magnitude entry
+// (first on ties) is positive.
+constexpr int kRitzWarps = 4;
+
+__global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
+    const double* __restrict__ alpha, const double* __restrict__ beta, const int* __restrict__ done, int count,
+    int steps, int k, double* __restrict__ zws, double* __restrict__ vals, double* __restrict__ zsel,
+    int* __restrict__ ok) {
+  __shared__ double dsh[kRitzWarps][kTprsMaxSteps], esh[kRitzWarps][kTprsMaxSteps];
+  __shared__ int selsh[kRitzWarps][kTprsRitzMax];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int d = blockIdx.x * kRitzWarps + warp;
+  if (d >= count) return;  // whole warps only: no block barrier follows
+  double* dd = dsh[warp];
+  double* ee = esh[warp];
+  int* sel = selsh[warp];
+  const int ms = done[d];
+  const int64_t ld = steps;
+  double* z = zws + static_cast<int64_t>(d) * steps * steps;
+  const double* al = alpha + static_cast<int64_t>(d) * steps;
+  const double* be = beta + static_cast<int64_t>(d) * steps;
+  constexpr int kRows = kTprsMaxSteps / 32;  // rows per lane
+  for (int i = lane; i < ms; i += 32) {
+    dd[i] = al[i];
+    ee[i] = i + 1 < ms ? be[i] : 0.0;
+  }
+  for (int c = 0; c < ms; ++c)
+    for (int i = lane; i < ms; i += 32) z[i + ld * c] = i == c ? 1.0 : 0.0;
+  __syncwarp();
+  bool good = ms >= k;
+  const double eps = 2.220446049250313e-16;
+  for (int l = 0; l < ms && good; ++l) {
+    int iter = 0;
+    for (;;) {
+      int mm = l;
+      for (; mm < ms - 1; ++mm) {
+        const double sum = fabs(dd[mm]) + fabs(dd[mm + 1]);
+        if (fabs(ee[mm]) <= eps * sum) break;
+      }
+      if (mm == l) break;
+      if (++iter > 60) {
+        good = false;
+        break;
+      }
+      double g = (dd[l + 1] - dd[l]) / (2.0 * ee[l]);
+      double r = hypot(g, 1.0);
+      g = dd[mm] - dd[l] + ee[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
+      double sn = 1.0, cs = 1.0, p = 0.0;
+      // column i + 1 of z rides in registers from one rotation to the next
+      double carry[kRows];
+#pragma unroll
+      for (int t = 0; t < kRows; ++t) {
+        const int row = lane + 32 * t;
+        carry[t] = row < ms ? z[row + ld * mm] : 0.0;
+      }
+      int cur = mm;
+      int i = mm - 1;
+      bool split = false;
+      for (; i >= l; --i) {
+        const double ei = ee[i], di = dd[i], di1 = dd[i + 1];
+        const double f = sn * ei;
+        const double b = cs * ei;
+        const double rr = hypot(f, g);
+        __syncwarp();  // every lane has read d and e before lane 0 writes them
+        if (rr == 0.0) {
+          if (lane == 0) {
+            ee[i + 1] = rr;
+            dd[i + 1] = di1 - p;
+            ee[mm] = 0.0;
+          }
+          split = true;
+          break;
+        }
+        if (lane == 0) ee[i + 1] = rr;
+        sn = f / rr;
+        cs = g / rr;
+        g = di1 - p;
+        r = (di - g) * sn + 2.0 * cs * b;
+        p = sn * r;
+        if (lane == 0) dd[i + 1] = g + p;
+        g = cs * r - b;
+#pragma unroll
+        for (int t = 0; t < kRows; ++t) {
+          const int row = lane + 32 * t;
+          if (row < ms) {
+            const double zi = z[row + ld * i];
+            z[row + ld * (i + 1)] = sn * zi + cs * carry[t];
+            carry[t] = cs * zi - sn * carry[t];
+          }
+        }
+        cur = i;
+      }
+#pragma unroll
+      for (int t = 0; t < kRows; ++t) {
+        const int row = lane + 32 * t;
+        if (row < ms) z[row + ld * cur] = carry[t];
+      }
+      __syncwarp();
+      if (split) continue;
+      if (lane == 0) {
+        dd[l] -= p;
+        ee[l] = g;
+        ee[mm] = 0.0;
+      }
+      __syncwarp();
+    }
+  }
+  if (!good) {
+    if (lane == 0) ok[d] = 0;
+    return;
+  }
+  // the k largest |theta| (stable: ties to the lower index), then by value, descending
+  double tmax = 0.0;
+  for (int i = lane; i < ms; i += 32) tmax = fmax(tmax, fabs(dd[i]));
+  for (int o = 16; o > 0; o >>= 1) tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+  for (int i = lane; i < ms; i += 32) {
+    const double ai = fabs(dd[i]);
+    int rank = 0;
+    for (int j = 0; j < ms; ++j) {
+      const double aj = fabs(dd[j]);
+      rank += (aj > ai || (aj == ai && j < i)) ? 1 : 0;
+    }
+    if (rank < k) sel[rank] = i;
+  }
+  __syncwarp();
+  const double blast = be[ms - 1];
+  const bool invariant = fabs(blast) <= 1e-15 * tmax;
+  bool conv = true;
+  for (int c = lane; c < k; c += 32) {
+    const int i = sel[c];
+    if (!invariant && fabs(blast * z[(ms - 1) + ld * i]) > 1e-14 * tmax) conv = false;
+  }
+  conv = __all_sync(0xffffffffu, conv);
+  for (int c = lane; c < k; c += 32) {
+    const int i = sel[c];
+    const double vi = dd[i];
+    int pos = 0;
+    for (int e = 0; e < k; ++e) {
+      const double ve = dd[sel[e]];
+      pos += (ve > vi || (ve == vi && e < c)) ? 1 : 0;
+    }
+    vals[static_cast<int64_t>(d) * k + pos] = vi;
+    double* zc = zsel + (static_cast<int64_t>(d) * k + pos) * steps;
+    for (int b = 0; b < ms; ++b) zc[b] = z[b + ld * i];
+  }
+  if (lane == 0) ok[d] = conv ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(kTprsThreads) tprs_ritz_vectors_kernel(
+    const double* __restrict__ V, const int64_t* __restrict__ voff, const int* __restrict__ nus,
+    const int* __restrict__ done, const int* __restrict__ ok, const double* __restrict__ zsel, int count, int steps,
+    double* __restrict__ U, const int64_t* __restrict__ uoff) {
+  constexpr int K = kTprsRitzMax;
+  __shared__ double zs[kTprsMaxSteps * K];
+  __shared__ double red_ss[kTprsWarps][K];
+  __shared__ double red_mx[kTprsWarps][K];
+  __shared__ int red_ix[kTprsWarps][K];
+  __shared__ double colscale[K];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int d = blockIdx.x; d < count; d += gridDim.x) {
+    if (!ok[d]) continue;  // uniform across the block
+    const int nu = nus[d], ms = done[d];
+    const double* Vd = V + voff[d];
+    double* Ud = U + uoff[d];
+    for (int idx = tid; idx < K * steps; idx += blockDim.x) {
+      const int c = idx / steps, b = idx % steps;
+      zs[b * K + c] = b < ms ? zsel[(static_cast<int64_t>(d) * K + c) * steps + b] : 0.0;
+    }
+    __syncthreads();
+    double ss[K], mx[K];
+    int ix[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+      ss[c] = 0.0;
+      mx[c] = -1.0;
+      ix[c] = 0;
+    }
+    for (int r = tid; r < nu; r += blockDim.x) {
+      double out[K];
+#pragma unroll
+      for (int c = 0; c < K; ++c) out[c] = 0.0;
+      for (int b = 0; b < ms; ++b) {
+        const double v = Vd[r + static_cast<int64_t>(nu) * b];
+        const double* zb = zs + b * K;
+#pragma unroll
+        for (int c = 0; c < K; ++c) out[c] += v * zb[c];
+      }
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        Ud[r + static_cast<int64_t>(nu) * c] = out[c];
+        ss[c] += out[c] * out[c];
+        const double a = fabs(out[c]);
+        if (a > mx[c]) {  // rows visited in increasing order: the first maximum stays
+          mx[c] = a;
+          ix[c] = r;
+        }
+      }
+    }
+    // block reductions per column: sum of squares; largest |entry|, lowest row on ties
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+      double sv = ss[c], mv = mx[c];
+      int iv = ix[c];
+      for (int o = 16; o > 0; o >>= 1) {
+        sv += __shfl_xor_sync(0xffffffffu, sv, o);
+        const double om = __shfl_xor_sync(0xffffffffu, mv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, iv, o);
+        if (om > mv || (om == mv && oi < iv)) {
+          mv = om;
+          iv = oi;
+        }
+      }
+      if (lane == 0) {
+        red_ss[warp][c] = sv;
+        red_mx[warp][c] = mv;
+        red_ix[warp][c] = iv;
+      }
+    }
+    __syncthreads();
+    if (tid < K) {
+      double sv = 0.0, mv = -1.0;
+      int iv = 0;
+      for (int w = 0; w < kTprsWarps; ++w) {
+        sv += red_ss[w][tid];
+        if (red_mx[w][tid] > mv || (red_mx[w][tid] == mv && red_ix[w][tid] < iv)) {
+          mv = red_mx[w][tid];
+          iv = red_ix[w][tid];
+        }
+      }
+      const double nn = sqrt(sv);
+      const double lead = Ud[iv + static_cast<int64_t>(nu) * tid];
+      colscale[tid] = (lead < 0.0 ? -1.0 : 1.0) / nn;
+    }
+    __syncthreads();
+    for (int64_t idx = tid; idx < static_cast<int64_t>(nu) * K; idx += blockDim.x)
+      Ud[idx] *= colscale[idx / nu];
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_tprs_ritz(const double* alpha, const double* beta, const int* done, int count, int steps, int k,
+                             double* zws, double* vals, double* zsel, int* ok, const double* V, const int64_t* voff,
+                             const int* nus, double* U, const int64_t* uoff, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  if (k != kTprsRitzMax || steps < k || steps > kTprsMaxSteps) return cudaErrorInvalidValue;
+  tprs_ritz_select_kernel<<<(count + kRitzWarps - 1) / kRitzWarps, kRitzWarps * 32, 0, stream>>>(
+      alpha, beta, done, count, steps, k, zws, vals, zsel, ok);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int ctas = count < 2 * 148 ? count : 2 * 148;
+  tprs_ritz_vectors_kernel<<<ctas, kTprsThreads, 0, stream>>>(V, voff, nus, done, ok, zsel, count, steps, U, uoff);
+  return cudaGetLastError();
+}
+
+size_t tprs_smem_bytes(int nu_max) {
+  const int64_t ld = tprs_ld(nu_max);
+  return sizeof(double) * static_cast<size_t>((2 + kTprsWarps) * ld + kTprsWarps * kTileWords);
+}
+
 cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int* nus, int count, int nu_max,
                                 int steps, double eta0, double* ews, int64_t ews_stride, int ctas, double* V,
                                 const int64_t* voff, double* alpha, double* beta, int* done, cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
-  if (steps < 1 || steps > kTprsMaxSteps || ctas < 1) return cudaErrorInvalidValue;
-  const size_t smem = sizeof(double) * 2 * static_cast<size_t>(nu_max);
+  if (steps < 1 || steps > kTprsMaxSteps || ctas < 1 || nu_max < 1 || nu_max > kTprsMaxNu ||
+      ews_stride < tprs_ld(nu_max) * tprs_ld(nu_max))
+    return cudaErrorInvalidValue;
+  const size_t smem = tprs_smem_bytes(nu_max);
   cudaError_t e = cudaFuncSetAttribute(tprs_lanczos_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
+  // two CTAs per SM where their shared memory fits: twice the tile loads in flight
+  e = cudaFuncSetAttribute(tprs_lanczos_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return e;
   tprs_lanczos_kernel<<<ctas, kTprsThreads, smem, stream>>>(u, uoff, nus, count, steps, eta0, ews, ews_stride, V,
-                                                             voff, alpha, beta, done);
+                                                             voff, alpha, beta, done,
+                                                             static_cast<int>(tprs_ld(nu_max)));
   return cudaGetLastError();
 }
 

@@ -199,13 +199,18 @@ constexpr size_t kDeviceTprsMin = 1;
 }  // namespace
 
 // The top-30 eigen problems of the level's new bivariate designs: prepare on
-// the host, Lanczos on the device, Ritz pairs and the rest of the basis on
-// the host.  Designs whose Ritz pairs do not converge in kTprsSteps steps are
-// left to the host set-up in build_designs.
-void Engine::build_bivariate_on_device(const std::vector<std::vector<int>>& sets) {
+// the host, Lanczos and Ritz pairs on the device, the rest of the basis on
+// the host.  launch_bivariate_on_device enqueues the kernels and the copies
+// of their results into page-locked memory and returns at once; the host
+// builds the other designs meanwhile; finish_bivariate_on_device waits and
+// finishes the bases.  Designs whose Ritz pairs do not converge in
+// kTprsSteps steps are left to the host set-up in build_designs.
+void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& sets, TprsBatch* batch) {
   const int n = n_;
   const size_t count = sets.size();
-  std::vector<TprsPrep> preps(count);
+  batch->sets = sets;
+  batch->preps.assign(count, TprsPrep());
+  batch->idx.clear();
   std::vector<char> ok(count, 0);
   parallel_for(count, [&](size_t i) {
     try {
@@ -214,104 +219,128 @@ void Engine::build_bivariate_on_device(const std::vector<std::vector<int>>& sets
                 host_data_.begin() + static_cast<size_t>(n) * (sets[i][0] + 1), cols.begin());
       std::copy(host_data_.begin() + static_cast<size_t>(n) * sets[i][1],
                 host_data_.begin() + static_cast<size_t>(n) * (sets[i][1] + 1), cols.begin() + n);
-      preps[i] = tprs_prepare(cols.data(), n, 2, kTprsK);
-      ok[i] = preps[i].nu > kTprsSteps && preps[i].nu <= 2048;
+      batch->preps[i] = tprs_prepare(cols.data(), n, 2, kTprsK);
+      ok[i] = batch->preps[i].nu > kTprsSteps && batch->preps[i].nu <= kTprsMaxNu;
     } catch (const std::exception&) {
       ok[i] = 0;  // the host set-up reports the error
     }
   });
-  std::vector<size_t> idx;
   for (size_t i = 0; i < count; ++i)
-    if (ok[i]) idx.push_back(i);
-  if (idx.empty()) return;
+    if (ok[i]) batch->idx.push_back(i);
+  if (batch->idx.empty()) return;
   std::vector<double> u;
   std::vector<int64_t> uoff, voff;
-  std::vector<int> nus;
+  batch->uoff.clear();
+  batch->nus.clear();
   int nu_max = 0;
-  int64_t vtotal = 0;
-  for (size_t i : idx) {
+  int64_t vtotal = 0, utotal = 0;
+  for (size_t i : batch->idx) {
+    const TprsPrep& pr = batch->preps[i];
     uoff.push_back(static_cast<int64_t>(u.size()));
-    u.insert(u.end(), preps[i].u.begin(), preps[i].u.end());
-    nus.push_back(preps[i].nu);
+    u.insert(u.end(), pr.u.begin(), pr.u.end());
+    batch->nus.push_back(pr.nu);
     voff.push_back(vtotal);
-    vtotal += static_cast<int64_t>(preps[i].nu) * kTprsSteps;
-    nu_max = std::max(nu_max, preps[i].nu);
+    vtotal += static_cast<int64_t>(pr.nu) * kTprsSteps;
+    batch->uoff.push_back(utotal);
+    utotal += static_cast<int64_t>(pr.nu) * kTprsK;
+    nu_max = std::max(nu_max, pr.nu);
   }
-  const int cnt = static_cast<int>(idx.size());
-  const int ctas = std::min(cnt, 148);
+  const int cnt = static_cast<int>(batch->idx.size());
+  const int ctas = std::min(cnt, 2 * 148);  // two designs per SM (memory-bound matvec)
+  const size_t nab = static_cast<size_t>(2) * cnt * kTprsSteps;
+  const size_t nvals = static_cast<size_t>(cnt) * kTprsK;
+  // page-locked landing area: Ritz vectors, values, then the acceptance flags
+  double* host = pinned_arena(static_cast<size_t>(utotal) + nvals + (static_cast<size_t>(cnt) + 1) / 2);
+  batch->U = host;
+  batch->vals = host + utotal;
+  batch->ok = reinterpret_cast<int*>(host + utotal + nvals);
   upload(d_tprs_u_, u, stream_);
   upload(d_tprs_uoff_, uoff, stream_);
   upload(d_tprs_voff_, voff, stream_);
-  upload(d_tprs_nus_, nus, stream_);
-  const int64_t ews_stride = static_cast<int64_t>(nu_max) * nu_max;
+  upload(d_tprs_roff_, batch->uoff, stream_);
+  upload(d_tprs_nus_, batch->nus, stream_);
+  const int64_t ews_stride = tprs_ld(nu_max) * tprs_ld(nu_max);
   double* dV = d_tprs_V_.ensure(static_cast<size_t>(vtotal));
-  double* dab = d_tprs_ab_.ensure(static_cast<size_t>(2) * cnt * kTprsSteps);
+  double* dab = d_tprs_ab_.ensure(nab);
+  double* ews = d_tprs_ews_.ensure(static_cast<size_t>(ctas) * ews_stride);
+  int* ddone = d_tprs_done_.ensure(cnt);
+  double* dvals = d_tprs_vals_.ensure(nvals);
+  double* dU = d_tprs_U_.ensure(static_cast<size_t>(utotal));
+  int* dok = d_tprs_ok_.ensure(cnt);
   cuda_check(launch_tprs_lanczos(d_tprs_u_.get(), d_tprs_uoff_.get(), d_tprs_nus_.get(), cnt, nu_max, kTprsSteps,
-                                 tprs_eta0(2), d_tprs_ews_.ensure(static_cast<size_t>(ctas) * ews_stride), ews_stride,
-                                 ctas, dV, d_tprs_voff_.get(), dab, dab + static_cast<size_t>(cnt) * kTprsSteps,
-                                 d_tprs_done_.ensure(cnt), stream_),
+                                 tprs_eta0(2), ews, ews_stride, ctas, dV, d_tprs_voff_.get(), dab,
+                                 dab + static_cast<size_t>(cnt) * kTprsSteps, ddone, stream_),
              "thin-plate Lanczos");
-  double* hV = pinned_arena(static_cast<size_t>(vtotal));
-  std::vector<double> ab(static_cast<size_t>(2) * cnt * kTprsSteps);
-  std::vector<int> done(cnt);
-  cuda_check(cudaMemcpyAsync(hV, dV, static_cast<size_t>(vtotal) * sizeof(double), cudaMemcpyDeviceToHost, stream_),
-             "download");
-  cuda_check(cudaMemcpyAsync(ab.data(), dab, ab.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
-  cuda_check(cudaMemcpyAsync(done.data(), d_tprs_done_.get(), done.size() * sizeof(int), cudaMemcpyDeviceToHost,
+  cuda_check(launch_tprs_ritz(dab, dab + static_cast<size_t>(cnt) * kTprsSteps, ddone, cnt, kTprsSteps, kTprsK,
+                              d_tprs_zws_.ensure(static_cast<size_t>(cnt) * kTprsSteps * kTprsSteps), dvals,
+                              d_tprs_zsel_.ensure(nvals * kTprsSteps), dok, dV, d_tprs_voff_.get(),
+                              d_tprs_nus_.get(), dU, d_tprs_roff_.get(), stream_),
+             "thin-plate Ritz pairs");
+  cuda_check(cudaMemcpyAsync(batch->U, dU, static_cast<size_t>(utotal) * sizeof(double), cudaMemcpyDeviceToHost,
                              stream_),
              "download");
+  cuda_check(cudaMemcpyAsync(batch->vals, dvals, nvals * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
+  cuda_check(cudaMemcpyAsync(batch->ok, dok, static_cast<size_t>(cnt) * sizeof(int), cudaMemcpyDeviceToHost, stream_),
+             "download");
+  d2h_bytes_ += static_cast<double>(utotal + nvals) * sizeof(double) + static_cast<double>(cnt) * sizeof(int);
+}
+
+void Engine::finish_bivariate_on_device(TprsBatch* batch) {
+  if (batch->idx.empty()) return;
   cuda_check(cudaStreamSynchronize(stream_), "thin-plate Lanczos");
-  d2h_bytes_ += static_cast<double>(vtotal) * sizeof(double);
-  parallel_for(idx.size(), [&](size_t c) {
-    const size_t i = idx[c];
-    std::vector<double> vals, U;
-    if (!ritz_from_lanczos(hV + voff[c], ab.data() + c * kTprsSteps, ab.data() + (cnt + c) * kTprsSteps, nus[c],
-                           done[c], kTprsK, &vals, &U))
-      return;  // not converged: the host set-up builds this design
-    cache_->put_bivariate(sets[i], std::make_shared<Smooth>(tprs_finish(preps[i], vals, U)));
+  parallel_for(batch->idx.size(), [&](size_t c) {
+    if (!batch->ok[c]) return;  // not converged: the host set-up builds this design
+    const size_t i = batch->idx[c];
+    const int nu = batch->nus[c];
+    std::vector<double> vals(batch->vals + c * kTprsK, batch->vals + (c + 1) * kTprsK);
+    std::vector<double> U(batch->U + batch->uoff[c], batch->U + batch->uoff[c] + static_cast<int64_t>(nu) * kTprsK);
+    cache_->put_bivariate(batch->sets[i], std::make_shared<Smooth>(tprs_finish(batch->preps[i], vals, U)));
   });
 }
 
-void Engine::build_designs() {
-  {
-    std::vector<std::vector<int>> bivariate;
-    for (const auto& S : sets_)
-      if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
-    if (bivariate.size() >= kDeviceTprsMin) build_bivariate_on_device(bivariate);
-  }
-  designs_.assign(sets_.size(), nullptr);
-  std::atomic<size_t> next(0);
+// Designs of the sets selected by `pick`, built on host threads (the cache
+// builds each conditioning set once).
+template <class Pick>
+void Engine::build_host_designs(Pick pick) {
+  std::vector<size_t> todo;
+  for (size_t i = 0; i < sets_.size(); ++i)
+    if (pick(sets_[i])) todo.push_back(i);
   std::string err;
   std::mutex err_mu;
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const size_t workers = std::min<size_t>(hw, std::max<size_t>(1, sets_.size()));
-  auto work = [&]() {
-    for (;;) {
-      const size_t i = next.fetch_add(1);
-      if (i >= sets_.size()) return;
-      try {
-        designs_[i] = cache_->get(sets_[i]);
-      } catch (const std::exception& e) {
-        std::lock_guard<std::mutex> lock(err_mu);
-        if (err.empty()) err = e.what();
-      }
+  parallel_for(todo.size(), [&](size_t c) {
+    const size_t i = todo[c];
+    try {
+      designs_[i] = cache_->get(sets_[i]);
+    } catch (const std::exception& e) {
+      std::lock_guard<std::mutex> lock(err_mu);
+      if (err.empty()) err = e.what();
     }
-  };
-  if (workers <= 1) {
-    work();
-  } else {
-    std::vector<std::thread> pool;
-    for (size_t w = 0; w < workers; ++w) pool.emplace_back(work);
-    for (auto& th : pool) th.join();
-  }
+  });
   if (!err.empty()) throw Error(FKPC_STATUS_RANK, "design set-up failed: " + err);
+}
+
+void Engine::build_designs() {
+  designs_.assign(sets_.size(), nullptr);
+  std::vector<std::vector<int>> bivariate;
+  for (const auto& S : sets_)
+    if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
+  TprsBatch batch;
+  if (bivariate.size() >= kDeviceTprsMin) launch_bivariate_on_device(bivariate, &batch);
+  // the other designs need no bivariate basis: build them while the device works
+  build_host_designs([](const std::vector<int>& S) { return S.size() != 2; });
+  finish_bivariate_on_device(&batch);
+  build_host_designs([](const std::vector<int>& S) { return S.size() == 2; });
 }
 
 void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   const int n = n_;
-  // Pass 1: descriptors and arena offsets (no copies).
+  // Pass 1: descriptors and arena offsets (no copies).  The arena has a
+  // host-filled range [0, total) and, behind it, a device-filled range for the
+  // geometry of the additive designs built on the device (offsets relative to
+  // the range while counting, made absolute below).
   std::vector<DesignDev> ddesc(designs_.size());
-  size_t total = 0;
+  std::vector<size_t> geom_designs;
+  size_t total = 0, dev_total = 0;
   for (size_t d = 0; d < designs_.size(); ++d) {
     const Design& des = *designs_[d];
     DesignDev& dd = ddesc[d];
@@ -332,10 +361,12 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       dd.rsum = des.ranks[0];
     } else {
       dd.kind = 2;
-      dd.basis = static_cast<int64_t>(total);
-      total += des.Q.size();
-      dd.rmat = static_cast<int64_t>(total);
-      total += des.R.size();
+      const bool dev = des.device_geometry;
+      size_t& at = dev ? dev_total : total;
+      dd.basis = static_cast<int64_t>(at);
+      at += static_cast<size_t>(n) * des.q;
+      dd.rmat = static_cast<int64_t>(at);
+      at += static_cast<size_t>(des.q) * des.q;
       dd.roots = static_cast<int64_t>(total);
       int rows = 0;
       int64_t rootoff = 0;
@@ -355,14 +386,23 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
         throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity (q <= 112, |S| <= 12)");
       dd.rpack = -1;
       if (des.q <= kWarpQ) {
-        total += total % 2;  // 16-byte aligned: copied with 16-byte cp.async
-        dd.rpack = static_cast<int64_t>(total);
-        total += kWarpTri;
+        size_t& pat = dev ? dev_total : total;
+        pat += pat % 2;  // 16-byte aligned: copied with 16-byte cp.async
+        dd.rpack = static_cast<int64_t>(pat);
+        pat += kWarpTri;
       }
+      if (dev) geom_designs.push_back(d);
     }
   }
-  // Pass 2: every design copies itself into the pinned staging buffer
-  // (threads over designs), then one DMA to the device arena.
+  const size_t dev_base = total + total % 2;  // keeps the device range's rpack offsets 16-byte aligned
+  for (size_t d : geom_designs) {
+    DesignDev& dd = ddesc[d];
+    dd.basis += static_cast<int64_t>(dev_base);
+    dd.rmat += static_cast<int64_t>(dev_base);
+    if (dd.rpack >= 0) dd.rpack += static_cast<int64_t>(dev_base);
+  }
+  // Pass 2: every design copies its host-built part into the pinned staging
+  // buffer (threads over designs), then one DMA to the device arena.
   double* host = pinned_arena(total);
   {
     std::atomic<size_t> next(0);
@@ -376,10 +416,11 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
           std::memcpy(host + dd.basis, des.QW.data(), des.QW.size() * sizeof(double));
           std::memcpy(host + dd.spec, des.spec.data(), des.spec.size() * sizeof(double));
         } else {
-          std::memcpy(host + dd.basis, des.Q.data(), des.Q.size() * sizeof(double));
-          std::memcpy(host + dd.rmat, des.R.data(), des.R.size() * sizeof(double));
           for (int j = 0; j < des.m; ++j)
             std::memcpy(host + dd.roots + dd.rootoff[j], des.roots[j].data(), des.roots[j].size() * sizeof(double));
+          if (des.device_geometry) continue;
+          std::memcpy(host + dd.basis, des.Q.data(), des.Q.size() * sizeof(double));
+          std::memcpy(host + dd.rmat, des.R.data(), des.R.size() * sizeof(double));
           if (dd.rpack >= 0) {
             double* rp = host + dd.rpack;
             std::fill(rp, rp + kWarpTri, 0.0);
@@ -397,6 +438,36 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       std::vector<std::thread> pool;
       for (size_t w = 0; w < workers; ++w) pool.emplace_back(work);
       for (auto& th : pool) th.join();
+    }
+  }
+  // Device geometry jobs: the distinct univariate bases in one table.
+  std::vector<GeomJob> gjobs(geom_designs.size());
+  std::vector<double> gtable;
+  int geom_max_q = 1;
+  {
+    std::map<const Smooth*, int64_t> slot;
+    for (size_t g = 0; g < geom_designs.size(); ++g) {
+      const Design& des = *designs_[geom_designs[g]];
+      const DesignDev& dd = ddesc[geom_designs[g]];
+      GeomJob& job = gjobs[g];
+      std::memset(&job, 0, sizeof(job));
+      job.basis = dd.basis;
+      job.rmat = dd.rmat;
+      job.rpack = dd.rpack;
+      job.q = des.q;
+      job.m = des.m;
+      geom_max_q = std::max(geom_max_q, des.q);
+      for (int j = 0; j < des.m; ++j) {
+        const Smooth* sm = des.parts[j].get();
+        auto it = slot.find(sm);
+        if (it == slot.end()) {
+          it = slot.emplace(sm, static_cast<int64_t>(gtable.size())).first;
+          gtable.insert(gtable.end(), sm->X.begin(), sm->X.end());
+        }
+        job.src[j] = it->second;
+        job.off[j] = des.offsets[j];
+        job.dim[j] = des.dims[j];
+      }
     }
   }
   single_jobs_.clear();
@@ -448,10 +519,17 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   const size_t npairs = pairs_.size();
   auto t0 = std::chrono::steady_clock::now();
   h2d_bytes_ = static_cast<double>(host_data_.size() * sizeof(double));
+  double* arena = d_arena_.ensure(dev_base + dev_total);
   if (total > 0)
-    cuda_check(cudaMemcpyAsync(d_arena_.ensure(total), host, total * sizeof(double), cudaMemcpyHostToDevice, stream_),
-               "upload arena");
+    cuda_check(cudaMemcpyAsync(arena, host, total * sizeof(double), cudaMemcpyHostToDevice, stream_), "upload arena");
   h2d_bytes_ += static_cast<double>(total * sizeof(double));
+  if (!gjobs.empty()) {
+    h2d_bytes_ += upload(d_geom_table_, gtable, stream_);
+    h2d_bytes_ += upload(d_geom_jobs_, gjobs, stream_);
+    cuda_check(launch_additive_geometry(d_geom_table_.get(), n, d_geom_jobs_.get(), static_cast<int>(gjobs.size()),
+                                        geom_max_q, arena, d_geom_status_.ensure(gjobs.size()), stream_),
+               "additive geometry");
+  }
   h2d_bytes_ += upload(d_designs_, ddesc, stream_);
   h2d_bytes_ += upload(d_single_jobs_, single_jobs_, stream_);
   h2d_bytes_ += upload(d_multi_jobs_, multi_jobs_, stream_);
@@ -508,6 +586,13 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
     }
   }
   cuda_check(cudaStreamSynchronize(stream_), "prepare upload");
+  if (!gjobs.empty()) {
+    std::vector<int> gstatus(gjobs.size());
+    cuda_check(cudaMemcpy(gstatus.data(), d_geom_status_.get(), gstatus.size() * sizeof(int), cudaMemcpyDeviceToHost),
+               "download");
+    for (int st : gstatus)
+      if (st != 0) throw Error(FKPC_STATUS_RANK, "design set-up failed: design matrix is rank deficient");
+  }
   upload_ms_ = ms_since(t0);
 }
 

@@ -109,7 +109,21 @@ class Engine {
   void enqueue_plain_test(int t);  // one test's launch set (plain form)
   double execute_plain_timed(int repeats);
   void build_designs();
-  void build_bivariate_on_device(const std::vector<std::vector<int>>& sets);
+  // one level's bivariate thin-plate Lanczos on the device, in flight
+  struct TprsBatch {
+    std::vector<std::vector<int>> sets;
+    std::vector<TprsPrep> preps;
+    std::vector<size_t> idx;  // sets taken by the device
+    std::vector<int64_t> uoff;  // each design's Ritz vectors (nu x k) in U
+    std::vector<int> nus;
+    double* U = nullptr;      // page-locked results (inside the staging arena)
+    double* vals = nullptr;
+    int* ok = nullptr;
+  };
+  void launch_bivariate_on_device(const std::vector<std::vector<int>>& sets, TprsBatch* batch);
+  void finish_bivariate_on_device(TprsBatch* batch);
+  template <class Pick>
+  void build_host_designs(Pick pick);
   void pack_and_upload(const fkpc_options& opt, RStream* stream);
   void enqueue();  // the launch sequence
   void release_graph();
@@ -147,8 +161,13 @@ class Engine {
   DevBuf<int> d_defer_list_, d_defer_count_;
   // device thin-plate Lanczos of the bivariate designs
   DevBuf<double> d_tprs_u_, d_tprs_V_, d_tprs_ab_, d_tprs_ews_;
-  DevBuf<int64_t> d_tprs_uoff_, d_tprs_voff_;
-  DevBuf<int> d_tprs_nus_, d_tprs_done_;
+  DevBuf<int64_t> d_tprs_uoff_, d_tprs_voff_, d_tprs_roff_;
+  DevBuf<int> d_tprs_nus_, d_tprs_done_, d_tprs_ok_;
+  DevBuf<double> d_tprs_zws_, d_tprs_vals_, d_tprs_zsel_, d_tprs_U_;
+  // device geometry of the additive designs
+  DevBuf<double> d_geom_table_;
+  DevBuf<GeomJob> d_geom_jobs_;
+  DevBuf<int> d_geom_status_;
   DevBuf<FitResult> d_single_res_, d_multi_res_;
   DevBuf<PairJob> d_pairs_;
   DevBuf<RecordDev> d_records_;

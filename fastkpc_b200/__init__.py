@@ -321,8 +321,21 @@ def _tests_arrays(tests):
     return xs, ys, offs, np.array(vals if vals else [0], dtype=np.int32)
 
 
-def _records(recs):
-    return {name: np.array([getattr(r, name) for r in recs]) for name, _ in CiRecord._fields_}
+_RECORD_DTYPE = None
+
+
+def _records(recs, count):
+    """Field arrays (float64, int64) of the first ``count`` entries of a
+    ctypes ``CiRecord`` array."""
+    global _RECORD_DTYPE
+    if _RECORD_DTYPE is None:
+        _RECORD_DTYPE = np.dtype({"names": [f for f, _ in CiRecord._fields_],
+                                  "formats": [np.dtype(t) for _, t in CiRecord._fields_],
+                                  "offsets": [getattr(CiRecord, f).offset for f, _ in CiRecord._fields_],
+                                  "itemsize": ctypes.sizeof(CiRecord)})
+    arr = np.frombuffer(recs, dtype=_RECORD_DTYPE, count=count)
+    return {name: arr[name].astype(np.int64 if arr[name].dtype.kind in "iu" else np.float64)
+            for name, _ in CiRecord._fields_}
 
 
 def ci_level_batch(data, tests, ci_method="dcc.gamma", mode="batched", **kw):
@@ -337,7 +350,7 @@ def ci_level_batch(data, tests, ci_method="dcc.gamma", mode="batched", **kw):
                                                 _ptr(ys, ctypes.c_int), _ptr(offs, ctypes.c_int),
                                                 _ptr(vals, ctypes.c_int), len(tests), ctypes.byref(o), out,
                                                 ctypes.byref(st)))
-    return _records(out[:len(tests)]), st.as_dict()
+    return _records(out, len(tests)), st.as_dict()
 
 
 def ci_plain_one(data, x, y, S, ci_method="dcc.gamma", **kw):
@@ -394,7 +407,7 @@ def stat_batch(residuals, pairs, ci_method="dcc.gamma", permutations=None, **kw)
     out = (CiRecord * max(1, len(pairs)))()
     _check(load_library().fkpc_stat_batch(_ptr(R, ctypes.c_double), n, m, _ptr(left, ctypes.c_int),
                                             _ptr(right, ctypes.c_int), len(pairs), perm_ptr, ctypes.byref(o), out))
-    return _records(out[:len(pairs)])
+    return _records(out, len(pairs))
 
 
 STAGES = {"fit_single": 0, "fit_multi_small": 1, "fit_multi_large": 2, "dcov_components": 3, "dcov_pairs": 4,
@@ -429,7 +442,7 @@ class StagedBatch:
         out = (CiRecord * self.count)()
         st = StageStats()
         _check(load_library().fkpc_batch_collect(self.device, out, ctypes.byref(st)))
-        return _records(out[:self.count]), st.as_dict()
+        return _records(out, self.count), st.as_dict()
 
     def time_stage(self, stage, repeats=3):
         ms = ctypes.c_double()

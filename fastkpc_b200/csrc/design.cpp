@@ -355,8 +355,6 @@ Smooth build_smooth(const double* cols, int n, int d, int k) {
   return tprs_finish(prep, vals, U);
 }
 
-namespace {
-
 // Sum of squares of each column of an n x cols matrix, accumulated in long
 // double in row order.
 std::vector<double> column_sumsq(const double* X, int n, int cols) {
@@ -371,8 +369,6 @@ std::vector<double> column_sumsq(const double* X, int n, int cols) {
   }
   return out;
 }
-
-}  // namespace
 
 std::vector<double> initial_sp(const Design& des) {
   return initial_sp_from_colsq(des, column_sumsq(des.X.data(), des.n, des.q));
@@ -596,6 +592,45 @@ std::shared_ptr<Design> build_design(const double* data, int n, int p, const std
   return des;
 }
 
+std::shared_ptr<Design> build_single_meta(int n, int p, const std::vector<int>& S, DesignCache* cache) {
+  if (S.empty() || S.size() > 2) throw std::runtime_error("a single-penalty design needs |S| of 1 or 2");
+  for (int s : S)
+    if (s < 0 || s >= p) throw std::runtime_error("conditioning index out of range");
+  std::shared_ptr<const Smooth> sm;
+  if (S.size() == 1) {
+    sm = cache->univariate(S[0]);
+  } else {
+    sm = cache->bivariate(S);
+    if (!sm) {
+      std::vector<double> cols(static_cast<size_t>(n) * 2);
+      for (size_t c = 0; c < 2; ++c)
+        std::copy(cache->data() + static_cast<size_t>(n) * S[c], cache->data() + static_cast<size_t>(n) * (S[c] + 1),
+                  cols.begin() + static_cast<size_t>(n) * c);
+      auto built = std::make_shared<Smooth>(build_smooth(cols.data(), n, 2, 30));
+      built->colsq = column_sumsq(built->X.data(), built->n, built->cols);
+      sm = built;
+    }
+  }
+  auto des = std::make_shared<Design>();
+  des->n = n;
+  des->S = S;
+  des->device_geometry = true;
+  des->q = 1 + sm->cols;
+  if (des->q >= n) throw std::runtime_error("design width must be below n");
+  des->m = 1;
+  des->blocks.push_back(sm->S);
+  des->offsets.push_back(1);
+  des->dims.push_back(sm->cols);
+  des->ranks.push_back(sm->rank);
+  std::vector<double> xdiag(1, column_sumsq(std::vector<double>(n, 1.0).data(), n, 1)[0]);
+  std::vector<double> colsq = sm->colsq.empty() ? column_sumsq(sm->X.data(), sm->n, sm->cols) : sm->colsq;
+  xdiag.insert(xdiag.end(), colsq.begin(), colsq.end());
+  std::vector<double> sp = initial_sp_from_colsq(*des, xdiag);
+  des->initial_log_sp.assign(1, std::log(sp[0]));
+  des->parts.push_back(sm);
+  return des;
+}
+
 std::shared_ptr<const Smooth> DesignCache::univariate(int column) {
   {
     std::lock_guard<std::mutex> lock(mu_);
@@ -636,7 +671,7 @@ std::shared_ptr<const Design> DesignCache::get(const std::vector<int>& S) {
     if (it != designs_.end()) return it->second;
   }
   std::shared_ptr<const Design> d =
-      S.size() >= 3 ? build_additive_meta(n_, p_, S, this) : build_design(data_, n_, p_, S, this);
+      S.size() >= 3 ? build_additive_meta(n_, p_, S, this) : build_single_meta(n_, p_, S, this);
   std::lock_guard<std::mutex> lock(mu_);
   auto it = designs_.find(S);
   if (it != designs_.end()) return it->second;

@@ -70,6 +70,11 @@ void prepare_geometry(Design* des);
 // An additive (|S| >= 3) design without X, Q or R: blocks, roots and
 // initial.sp from the cache's univariate smooths (device_geometry set).
 std::shared_ptr<Design> build_additive_meta(int n, int p, const std::vector<int>& S, DesignCache* cache);
+// A single-penalty (|S| <= 2) design without X, Q, QW or the spectrum: the
+// smooth, its penalty and initial.sp (device_geometry set).
+std::shared_ptr<Design> build_single_meta(int n, int p, const std::vector<int>& S, DesignCache* cache);
+// sum of squares of each column of an n x cols matrix (long double accumulation)
+std::vector<double> column_sumsq(const double* X, int n, int cols);
 
 // Cache of univariate smooths (shared by every additive model containing the
 // variable) and of full designs per conditioning set.

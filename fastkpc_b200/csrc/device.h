@@ -63,6 +63,17 @@ struct GeomJob {
   int m;
 };
 
+// One single-penalty design whose geometry the device builds: X = [1 | B],
+// B the smooth's basis, S its penalty; QW and the spectrum to the arena.
+struct SingleGeomJob {
+  int64_t basis;   // arena offset of QW (n x q)
+  int64_t spec;    // arena offset of the spectrum (q)
+  int64_t src;     // B (n x (q - 1)) in the basis table
+  int64_t pen;     // S ((q - 1) x (q - 1)) in the basis table
+  int q;
+  int rank;
+};
+
 // One residual fit: data column ``column`` regressed on design ``design``.
 struct FitJob {
   int design;

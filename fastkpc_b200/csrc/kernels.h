@@ -111,6 +111,10 @@ cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int*
 // Additive-design geometry (X gathered from the univariate bases, Householder
 // QR, Q / R / row-packed R into the arena); see kernels_geom.cu.  status[d]:
 // 1 when design d is rank deficient.  max_q <= 112 and below n.
+// Single-penalty geometry (X = [1 | B], QR, whitened-penalty eigen, QW and
+// spectrum into the arena); status[d] 1 rank deficient, 2 eigen failed.
+cudaError_t launch_single_geometry(const double* table, int n, const SingleGeomJob* jobs, int count, double* arena,
+                                   int* status, cudaStream_t stream);
 cudaError_t launch_additive_geometry(const double* table, int n, const GeomJob* jobs, int count, int max_q,
                                      double* arena, int* status, cudaStream_t stream);
 

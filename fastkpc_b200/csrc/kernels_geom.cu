@@ -52,6 +52,68 @@ __device__ double block_sum_g(double v, double* red) {
 
 }  // namespace
 
+// X (n x q, column-major, at W) = Q R by Householder reflections, in place:
+// on return W holds Q and R (ldr) the upper triangle (its lower triangle must
+// be zero on entry).  Reflector k = I - beta v v', v = (x_k - alpha, x_{k+1},
+// ...): rows > k of column k keep v until Q is formed, v_k and beta sit in
+// vks / betas (q doubles each).  Returns true when a column norm was zero
+// (rank deficient).  Called by the whole block.
+static __device__ bool householder_inplace(double* __restrict__ W, int n, int q, double* R, int ldr, double* vks,
+                                    double* betas, double* red) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  bool deficient = false;
+  for (int k = 0; k < q; ++k) {
+    const double* x = W + static_cast<int64_t>(n) * k;
+    double part = 0.0;
+    for (int i = k + tid; i < n; i += blockDim.x) part += x[i] * x[i];
+    const double norm2 = block_sum_g(part, red);
+    const double norm = sqrt(norm2);
+    const double xk = x[k];
+    double alpha = 0.0, vk = 0.0, beta = 0.0;
+    if (norm == 0.0) {
+      deficient = true;
+    } else {
+      alpha = xk >= 0.0 ? -norm : norm;
+      vk = xk - alpha;
+      beta = 2.0 / (norm2 - xk * xk + vk * vk);
+    }
+    for (int j = k + 1 + warp; j < q; j += kGeomWarps) {
+      double* c = W + static_cast<int64_t>(n) * j;
+      double dot = 0.0;
+      for (int i = k + lane; i < n; i += 32) dot += (i == k ? vk : x[i]) * c[i];
+      dot = warp_sum_g(dot) * beta;
+      for (int i = k + lane; i < n; i += 32) c[i] -= dot * (i == k ? vk : x[i]);
+      if (lane == 0) R[k + static_cast<int64_t>(ldr) * j] = c[k];  // row k is final
+    }
+    if (tid == 0) {
+      R[k + static_cast<int64_t>(ldr) * k] = alpha;
+      vks[k] = vk;
+      betas[k] = beta;
+    }
+    __syncthreads();
+  }
+  // Q = H_0 ... H_{q-1} [I; 0], accumulated backwards in place.  Before step
+  // k, column j > k is zero in rows <= k, so its update starts at row k + 1
+  // and row k receives -dot v_k.
+  for (int k = q - 1; k >= 0; --k) {
+    double* x = W + static_cast<int64_t>(n) * k;
+    const double vk = vks[k], beta = betas[k];
+    for (int j = k + 1 + warp; j < q; j += kGeomWarps) {
+      double* c = W + static_cast<int64_t>(n) * j;
+      double dot = 0.0;
+      for (int i = k + 1 + lane; i < n; i += 32) dot += x[i] * c[i];
+      dot = warp_sum_g(dot) * beta;
+      for (int i = k + 1 + lane; i < n; i += 32) c[i] -= dot * x[i];
+      if (lane == 0) c[k] = -dot * vk;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x)
+      x[i] = i < k ? 0.0 : (i == k ? 1.0 - beta * vk * vk : -beta * vk * x[i]);
+    __syncthreads();
+  }
+  return deficient;
+}
+
 __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const double* __restrict__ table, int n,
                                                                          const GeomJob* __restrict__ jobs, int count,
                                                                          double* __restrict__ arena,
@@ -59,7 +121,7 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const d
   __shared__ int64_t colsrc[kGeomMaxQ];
   __shared__ double vks[kGeomMaxQ], betas[kGeomMaxQ];
   __shared__ double red[kGeomWarps];
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x;
   for (int d = blockIdx.x; d < count; d += gridDim.x) {
     const GeomJob& job = jobs[d];
     const int q = job.q;
@@ -81,58 +143,7 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const d
     }
     for (int idx = tid; idx < q * q; idx += blockDim.x) R[idx] = 0.0;
     __syncthreads();
-    // factorisation: reflector k = I - beta v v', v = (x_k - alpha, x_{k+1}, ...);
-    // rows > k of column k keep v, v_k and beta go to shared memory
-    bool deficient = false;
-    for (int k = 0; k < q; ++k) {
-      const double* x = W + static_cast<int64_t>(n) * k;
-      double part = 0.0;
-      for (int i = k + tid; i < n; i += blockDim.x) part += x[i] * x[i];
-      const double norm2 = block_sum_g(part, red);
-      const double norm = sqrt(norm2);
-      const double xk = x[k];
-      double alpha = 0.0, vk = 0.0, beta = 0.0;
-      if (norm == 0.0) {
-        deficient = true;
-      } else {
-        alpha = xk >= 0.0 ? -norm : norm;
-        vk = xk - alpha;
-        beta = 2.0 / (norm2 - xk * xk + vk * vk);
-      }
-      for (int j = k + 1 + warp; j < q; j += kGeomWarps) {
-        double* c = W + static_cast<int64_t>(n) * j;
-        double dot = 0.0;
-        for (int i = k + lane; i < n; i += 32) dot += (i == k ? vk : x[i]) * c[i];
-        dot = warp_sum_g(dot) * beta;
-        for (int i = k + lane; i < n; i += 32) c[i] -= dot * (i == k ? vk : x[i]);
-        if (lane == 0) R[k + static_cast<int64_t>(q) * j] = c[k];  // row k is final
-      }
-      if (tid == 0) {
-        R[k + static_cast<int64_t>(q) * k] = alpha;
-        vks[k] = vk;
-        betas[k] = beta;
-      }
-      __syncthreads();
-    }
-    // Q = H_0 ... H_{q-1} [I; 0], accumulated backwards in place.  Before step
-    // k, column j > k is zero in rows <= k, so its update starts at row k + 1
-    // and row k receives -dot v_k.
-    for (int k = q - 1; k >= 0; --k) {
-      double* x = W + static_cast<int64_t>(n) * k;
-      const double vk = vks[k], beta = betas[k];
-      for (int j = k + 1 + warp; j < q; j += kGeomWarps) {
-        double* c = W + static_cast<int64_t>(n) * j;
-        double dot = 0.0;
-        for (int i = k + 1 + lane; i < n; i += 32) dot += x[i] * c[i];
-        dot = warp_sum_g(dot) * beta;
-        for (int i = k + 1 + lane; i < n; i += 32) c[i] -= dot * x[i];
-        if (lane == 0) c[k] = -dot * vk;
-      }
-      __syncthreads();
-      for (int i = tid; i < n; i += blockDim.x)
-        x[i] = i < k ? 0.0 : (i == k ? 1.0 - beta * vk * vk : -beta * vk * x[i]);
-      __syncthreads();
-    }
+    const bool deficient = householder_inplace(W, n, q, R, q, vks, betas, red);
     if (job.rpack >= 0) {
       double* rp = arena + job.rpack;
       for (int idx = tid; idx < kWarpTri; idx += blockDim.x) rp[idx] = 0.0;
@@ -145,6 +156,192 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const d
     if (tid == 0) status[d] = deficient ? 1 : 0;
     __syncthreads();
   }
+}
+
+// Single-penalty designs (|S| <= 2): X = [1 | B] with one penalty S on the
+// smooth's columns (fastkpc/src/full_cuda_ci_one_call.cpp:1869-1947 builds
+// this geometry from the Gram Cholesky; here from the QR).  X = Q R, the
+// whitened penalty R^-T S R^-1 = V diag(e) V' (cyclic Jacobi on warp 0, at
+// most 100 sweeps), and the fit kernels' inputs QW = Q V and the spectrum e
+// (descending; zero beyond the penalty rank).  status[d]: 1 rank deficient,
+// 2 Jacobi did not converge.
+__global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(const double* __restrict__ table, int n,
+                                                                       const SingleGeomJob* __restrict__ jobs,
+                                                                       int count, double* __restrict__ arena,
+                                                                       int* __restrict__ status) {
+  constexpr int Q = kMaxSingleQ;
+  constexpr int LA = Q + 1;  // padded leading dimension of the Jacobi matrices
+  __shared__ double Rs[Q * Q], Ri[Q * Q], T[Q * Q];
+  __shared__ double A[Q * LA], Vs[Q * LA];
+  __shared__ double vks[Q], betas[Q], red[kGeomWarps];
+  __shared__ int order[Q];
+  __shared__ int jacobi_ok;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int d = blockIdx.x; d < count; d += gridDim.x) {
+    const SingleGeomJob& job = jobs[d];
+    const int q = job.q, dim = q - 1;
+    double* W = arena + job.basis;
+    const double* B = table + job.src;
+    const double* S = table + job.pen;
+    const int64_t nq = static_cast<int64_t>(n) * q;
+    for (int64_t idx = tid; idx < nq; idx += blockDim.x) {
+      const int r = static_cast<int>(idx % n), c = static_cast<int>(idx / n);
+      W[idx] = c == 0 ? 1.0 : B[r + static_cast<int64_t>(n) * (c - 1)];
+    }
+    for (int idx = tid; idx < q * q; idx += blockDim.x) {
+      Rs[idx] = 0.0;
+      Ri[idx] = 0.0;
+    }
+    __syncthreads();
+    const bool deficient = householder_inplace(W, n, q, Rs, q, vks, betas, red);
+    if (deficient) {
+      if (tid == 0) status[d] = 1;
+      __syncthreads();
+      continue;  // uniform: every thread holds the same flag
+    }
+    // Ri = R^-1, one column per thread, back substitution
+    if (tid < q) {
+      const int c = tid;
+      Ri[c + q * c] = 1.0 / Rs[c + q * c];
+      for (int r = c - 1; r >= 0; --r) {
+        double acc = 0.0;
+        for (int t = r + 1; t <= c; ++t) acc += Rs[r + q * t] * Ri[t + q * c];
+        Ri[r + q * c] = -acc / Rs[r + q * r];
+      }
+    }
+    __syncthreads();
+    // T = S_full Ri (S_full: S on rows / columns 1..q-1), then A = Ri' T
+    for (int idx = tid; idx < q * q; idx += blockDim.x) {
+      const int r = idx % q, c = idx / q;
+      double acc = 0.0;
+      if (r > 0)
+        for (int t = 1; t < q; ++t) acc += S[(r - 1) + static_cast<int64_t>(dim) * (t - 1)] * Ri[t + q * c];
+      T[idx] = acc;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < q * q; idx += blockDim.x) {
+      const int r = idx % q, c = idx / q;
+      double acc = 0.0;
+      for (int t = 0; t < q; ++t) acc += Ri[t + q * r] * T[t + q * c];
+      A[r + LA * c] = acc;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < q * q; idx += blockDim.x) {
+      const int r = idx % q, c = idx / q;
+      if (r > c) {
+        const double v = 0.5 * (A[r + LA * c] + A[c + LA * r]);
+        A[r + LA * c] = v;
+        A[c + LA * r] = v;
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+      for (int c = 0; c < q; ++c)
+        if (lane < q) Vs[lane + LA * c] = lane == c ? 1.0 : 0.0;
+      __syncwarp();
+      bool conv = false;
+      for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0, diag = 0.0;
+        if (lane < q)
+          for (int j = 0; j < q; ++j) {
+            const double v = A[lane + LA * j];
+            if (lane == j) diag += v * v;
+            else off += v * v;
+          }
+        off = warp_sum_g(off);
+        diag = warp_sum_g(diag);
+        if (off <= 1e-32 * diag || off == 0.0) {
+          conv = true;
+          break;
+        }
+        for (int pp = 0; pp < q - 1; ++pp) {
+          for (int qq = pp + 1; qq < q; ++qq) {
+            const double apq = A[pp + LA * qq];
+            if (apq == 0.0) continue;  // the same value in every lane
+            const double app = A[pp + LA * pp], aqq = A[qq + LA * qq];
+            const double theta = (aqq - app) / (2.0 * apq);
+            const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            const double cs = 1.0 / sqrt(t * t + 1.0);
+            const double sn = t * cs;
+            __syncwarp();
+            if (lane < q) {
+              const double akp = A[lane + LA * pp], akq = A[lane + LA * qq];
+              A[lane + LA * pp] = cs * akp - sn * akq;
+              A[lane + LA * qq] = sn * akp + cs * akq;
+            }
+            __syncwarp();
+            if (lane < q) {
+              const double apk = A[pp + LA * lane], aqk = A[qq + LA * lane];
+              A[pp + LA * lane] = cs * apk - sn * aqk;
+              A[qq + LA * lane] = sn * apk + cs * aqk;
+              const double vkp = Vs[lane + LA * pp], vkq = Vs[lane + LA * qq];
+              Vs[lane + LA * pp] = cs * vkp - sn * vkq;
+              Vs[lane + LA * qq] = sn * vkp + cs * vkq;
+            }
+            __syncwarp();
+            if (lane == 0) {
+              A[pp + LA * qq] = 0.0;
+              A[qq + LA * pp] = 0.0;
+            }
+            __syncwarp();
+          }
+        }
+      }
+      // descending eigenvalues; equal values: the higher index first
+      if (lane < q) {
+        const double li = A[lane + LA * lane];
+        int pos = 0;
+        for (int j = 0; j < q; ++j) {
+          const double lj = A[j + LA * j];
+          pos += (lj > li || (lj == li && j > lane)) ? 1 : 0;
+        }
+        order[pos] = lane;
+      }
+      if (lane == 0) jacobi_ok = conv ? 1 : 0;
+    }
+    __syncthreads();
+    if (!jacobi_ok) {
+      if (tid == 0) status[d] = 2;
+      __syncthreads();
+      continue;
+    }
+    double* spec = arena + job.spec;
+    if (tid < q) {
+      const double lv = A[order[tid] + LA * order[tid]];
+      spec[tid] = tid < job.rank ? fmax(0.0, lv) : 0.0;
+    }
+    // T = V sorted by descending eigenvalue
+    for (int idx = tid; idx < q * q; idx += blockDim.x) {
+      const int r = idx % q, c = idx / q;
+      T[idx] = Vs[r + LA * order[c]];
+    }
+    __syncthreads();
+    // QW = Q V, a row per thread, in place
+    for (int r = tid; r < n; r += blockDim.x) {
+      double qrow[Q];
+#pragma unroll
+      for (int t = 0; t < Q; ++t) qrow[t] = t < q ? W[r + static_cast<int64_t>(n) * t] : 0.0;
+#pragma unroll 4
+      for (int c = 0; c < q; ++c) {
+        double acc = 0.0;
+#pragma unroll
+        for (int t = 0; t < Q; ++t)
+          if (t < q) acc += qrow[t] * T[t + q * c];
+        W[r + static_cast<int64_t>(n) * c] = acc;
+      }
+    }
+    if (tid == 0) status[d] = 0;
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_single_geometry(const double* table, int n, const SingleGeomJob* jobs, int count, double* arena,
+                                   int* status, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  if (n <= kMaxSingleQ) return cudaErrorInvalidValue;
+  const int ctas = count < 4 * 148 ? count : 4 * 148;
+  single_geometry_kernel<<<ctas, kGeomThreads, 0, stream>>>(table, n, jobs, count, arena, status);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_additive_geometry(const double* table, int n, const GeomJob* jobs, int count, int max_q,

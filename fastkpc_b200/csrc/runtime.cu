@@ -294,7 +294,9 @@ void Engine::finish_bivariate_on_device(TprsBatch* batch) {
     const int nu = batch->nus[c];
     std::vector<double> vals(batch->vals + c * kTprsK, batch->vals + (c + 1) * kTprsK);
     std::vector<double> U(batch->U + batch->uoff[c], batch->U + batch->uoff[c] + static_cast<int64_t>(nu) * kTprsK);
-    cache_->put_bivariate(batch->sets[i], std::make_shared<Smooth>(tprs_finish(batch->preps[i], vals, U)));
+    auto sm = std::make_shared<Smooth>(tprs_finish(batch->preps[i], vals, U));
+    sm->colsq = column_sumsq(sm->X.data(), sm->n, sm->cols);
+    cache_->put_bivariate(batch->sets[i], sm);
   });
 }
 
@@ -336,11 +338,32 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   const int n = n_;
   // Pass 1: descriptors and arena offsets (no copies).  The arena has a
   // host-filled range [0, total) and, behind it, a device-filled range for the
-  // geometry of the additive designs built on the device (offsets relative to
-  // the range while counting, made absolute below).
+  // geometry the device builds (offsets relative to the range while counting,
+  // made absolute below).  The host range also holds the table of smooth
+  // bases and penalties the geometry kernels read.
   std::vector<DesignDev> ddesc(designs_.size());
-  std::vector<size_t> geom_designs;
+  std::vector<size_t> geom_designs, single_designs;
   size_t total = 0, dev_total = 0;
+  struct SmoothSlot {
+    const Smooth* smooth;
+    int64_t x, pen;  // arena offsets of X (n x cols) and S (cols x cols, or -1)
+  };
+  std::vector<SmoothSlot> smooth_slots;
+  std::map<const Smooth*, size_t> smooth_index;
+  auto smooth_slot = [&](const Smooth* sm, bool with_penalty) -> SmoothSlot& {
+    auto it = smooth_index.find(sm);
+    if (it == smooth_index.end()) {
+      it = smooth_index.emplace(sm, smooth_slots.size()).first;
+      smooth_slots.push_back({sm, static_cast<int64_t>(total), -1});
+      total += sm->X.size();
+    }
+    SmoothSlot& sl = smooth_slots[it->second];
+    if (with_penalty && sl.pen < 0) {
+      sl.pen = static_cast<int64_t>(total);
+      total += sm->S.size();
+    }
+    return sl;
+  };
   for (size_t d = 0; d < designs_.size(); ++d) {
     const Design& des = *designs_[d];
     DesignDev& dd = ddesc[d];
@@ -350,10 +373,15 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
     if (des.m == 1) {
       if (des.q > kMaxSingleQ) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "single-penalty design too wide");
       dd.kind = 1;
-      dd.basis = static_cast<int64_t>(total);
-      total += des.QW.size();
-      dd.spec = static_cast<int64_t>(total);
-      total += des.spec.size();
+      size_t& at = des.device_geometry ? dev_total : total;
+      dd.basis = static_cast<int64_t>(at);
+      at += static_cast<size_t>(n) * des.q;
+      dd.spec = static_cast<int64_t>(at);
+      at += static_cast<size_t>(des.q);
+      if (des.device_geometry) {
+        single_designs.push_back(d);
+        smooth_slot(des.parts[0].get(), true);
+      }
       dd.log_sp0[0] = des.initial_log_sp[0];
       dd.off[0] = des.offsets[0];
       dd.dim[0] = des.dims[0];
@@ -391,7 +419,10 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
         dd.rpack = static_cast<int64_t>(pat);
         pat += kWarpTri;
       }
-      if (dev) geom_designs.push_back(d);
+      if (dev) {
+        geom_designs.push_back(d);
+        for (const auto& sm : des.parts) smooth_slot(sm.get(), false);
+      }
     }
   }
   const size_t dev_base = total + total % 2;  // keeps the device range's rpack offsets 16-byte aligned
@@ -401,6 +432,10 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
     dd.rmat += static_cast<int64_t>(dev_base);
     if (dd.rpack >= 0) dd.rpack += static_cast<int64_t>(dev_base);
   }
+  for (size_t d : single_designs) {
+    ddesc[d].basis += static_cast<int64_t>(dev_base);
+    ddesc[d].spec += static_cast<int64_t>(dev_base);
+  }
   // Pass 2: every design copies its host-built part into the pinned staging
   // buffer (threads over designs), then one DMA to the device arena.
   double* host = pinned_arena(total);
@@ -408,11 +443,19 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
     std::atomic<size_t> next(0);
     auto work = [&]() {
       for (;;) {
-        const size_t d = next.fetch_add(1);
-        if (d >= designs_.size()) return;
+        const size_t item = next.fetch_add(1);
+        if (item >= designs_.size() + smooth_slots.size()) return;
+        if (item >= designs_.size()) {
+          const SmoothSlot& sl = smooth_slots[item - designs_.size()];
+          std::memcpy(host + sl.x, sl.smooth->X.data(), sl.smooth->X.size() * sizeof(double));
+          if (sl.pen >= 0) std::memcpy(host + sl.pen, sl.smooth->S.data(), sl.smooth->S.size() * sizeof(double));
+          continue;
+        }
+        const size_t d = item;
         const Design& des = *designs_[d];
         const DesignDev& dd = ddesc[d];
         if (dd.kind == 1) {
+          if (des.device_geometry) continue;
           std::memcpy(host + dd.basis, des.QW.data(), des.QW.size() * sizeof(double));
           std::memcpy(host + dd.spec, des.spec.data(), des.spec.size() * sizeof(double));
         } else {
@@ -431,7 +474,8 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       }
     };
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t workers = std::min<size_t>(std::min<size_t>(hw, 16), std::max<size_t>(1, designs_.size() / 64));
+    const size_t workers =
+        std::min<size_t>(std::min<size_t>(hw, 16), std::max<size_t>(1, (designs_.size() + smooth_slots.size()) / 64));
     if (workers <= 1) {
       work();
     } else {
@@ -440,34 +484,38 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       for (auto& th : pool) th.join();
     }
   }
-  // Device geometry jobs: the distinct univariate bases in one table.
+  // Device geometry jobs; the smooth bases and penalties sit in the host range.
   std::vector<GeomJob> gjobs(geom_designs.size());
-  std::vector<double> gtable;
+  std::vector<SingleGeomJob> sjobs(single_designs.size());
   int geom_max_q = 1;
-  {
-    std::map<const Smooth*, int64_t> slot;
-    for (size_t g = 0; g < geom_designs.size(); ++g) {
-      const Design& des = *designs_[geom_designs[g]];
-      const DesignDev& dd = ddesc[geom_designs[g]];
-      GeomJob& job = gjobs[g];
-      std::memset(&job, 0, sizeof(job));
-      job.basis = dd.basis;
-      job.rmat = dd.rmat;
-      job.rpack = dd.rpack;
-      job.q = des.q;
-      job.m = des.m;
-      geom_max_q = std::max(geom_max_q, des.q);
-      for (int j = 0; j < des.m; ++j) {
-        const Smooth* sm = des.parts[j].get();
-        auto it = slot.find(sm);
-        if (it == slot.end()) {
-          it = slot.emplace(sm, static_cast<int64_t>(gtable.size())).first;
-          gtable.insert(gtable.end(), sm->X.begin(), sm->X.end());
-        }
-        job.src[j] = it->second;
-        job.off[j] = des.offsets[j];
-        job.dim[j] = des.dims[j];
-      }
+  for (size_t g = 0; g < single_designs.size(); ++g) {
+    const Design& des = *designs_[single_designs[g]];
+    const DesignDev& dd = ddesc[single_designs[g]];
+    const SmoothSlot& sl = smooth_slots[smooth_index.at(des.parts[0].get())];
+    SingleGeomJob& job = sjobs[g];
+    std::memset(&job, 0, sizeof(job));
+    job.basis = dd.basis;
+    job.spec = dd.spec;
+    job.src = sl.x;
+    job.pen = sl.pen;
+    job.q = des.q;
+    job.rank = des.ranks[0];
+  }
+  for (size_t g = 0; g < geom_designs.size(); ++g) {
+    const Design& des = *designs_[geom_designs[g]];
+    const DesignDev& dd = ddesc[geom_designs[g]];
+    GeomJob& job = gjobs[g];
+    std::memset(&job, 0, sizeof(job));
+    job.basis = dd.basis;
+    job.rmat = dd.rmat;
+    job.rpack = dd.rpack;
+    job.q = des.q;
+    job.m = des.m;
+    geom_max_q = std::max(geom_max_q, des.q);
+    for (int j = 0; j < des.m; ++j) {
+      job.src[j] = smooth_slots[smooth_index.at(des.parts[j].get())].x;
+      job.off[j] = des.offsets[j];
+      job.dim[j] = des.dims[j];
     }
   }
   single_jobs_.clear();
@@ -523,12 +571,19 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   if (total > 0)
     cuda_check(cudaMemcpyAsync(arena, host, total * sizeof(double), cudaMemcpyHostToDevice, stream_), "upload arena");
   h2d_bytes_ += static_cast<double>(total * sizeof(double));
+  int* gstatus_dev = nullptr;
+  if (!gjobs.empty() || !sjobs.empty()) gstatus_dev = d_geom_status_.ensure(gjobs.size() + sjobs.size());
   if (!gjobs.empty()) {
-    h2d_bytes_ += upload(d_geom_table_, gtable, stream_);
     h2d_bytes_ += upload(d_geom_jobs_, gjobs, stream_);
-    cuda_check(launch_additive_geometry(d_geom_table_.get(), n, d_geom_jobs_.get(), static_cast<int>(gjobs.size()),
-                                        geom_max_q, arena, d_geom_status_.ensure(gjobs.size()), stream_),
+    cuda_check(launch_additive_geometry(arena, n, d_geom_jobs_.get(), static_cast<int>(gjobs.size()), geom_max_q, arena,
+                                        gstatus_dev, stream_),
                "additive geometry");
+  }
+  if (!sjobs.empty()) {
+    h2d_bytes_ += upload(d_single_geom_jobs_, sjobs, stream_);
+    cuda_check(launch_single_geometry(arena, n, d_single_geom_jobs_.get(), static_cast<int>(sjobs.size()), arena,
+                                      gstatus_dev + gjobs.size(), stream_),
+               "single-penalty geometry");
   }
   h2d_bytes_ += upload(d_designs_, ddesc, stream_);
   h2d_bytes_ += upload(d_single_jobs_, single_jobs_, stream_);
@@ -586,12 +641,14 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
     }
   }
   cuda_check(cudaStreamSynchronize(stream_), "prepare upload");
-  if (!gjobs.empty()) {
-    std::vector<int> gstatus(gjobs.size());
-    cuda_check(cudaMemcpy(gstatus.data(), d_geom_status_.get(), gstatus.size() * sizeof(int), cudaMemcpyDeviceToHost),
+  if (gstatus_dev) {
+    std::vector<int> gstatus(gjobs.size() + sjobs.size());
+    cuda_check(cudaMemcpy(gstatus.data(), gstatus_dev, gstatus.size() * sizeof(int), cudaMemcpyDeviceToHost),
                "download");
-    for (int st : gstatus)
-      if (st != 0) throw Error(FKPC_STATUS_RANK, "design set-up failed: design matrix is rank deficient");
+    for (int st : gstatus) {
+      if (st == 1) throw Error(FKPC_STATUS_RANK, "design set-up failed: design matrix is rank deficient");
+      if (st != 0) throw Error(FKPC_STATUS_NUMERIC, "design set-up failed: penalty eigen-decomposition did not converge");
+    }
   }
   upload_ms_ = ms_since(t0);
 }

@@ -165,8 +165,8 @@ class Engine {
   DevBuf<int> d_tprs_nus_, d_tprs_done_, d_tprs_ok_;
   DevBuf<double> d_tprs_zws_, d_tprs_vals_, d_tprs_zsel_, d_tprs_U_;
   // device geometry of the additive designs
-  DevBuf<double> d_geom_table_;
   DevBuf<GeomJob> d_geom_jobs_;
+  DevBuf<SingleGeomJob> d_single_geom_jobs_;
   DevBuf<int> d_geom_status_;
   DevBuf<FitResult> d_single_res_, d_multi_res_;
   DevBuf<PairJob> d_pairs_;

@@ -324,7 +324,9 @@ def run_ours(args, world, rank, local, pg):
                                        f"processes ({cpu_dt:.1f} s)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": e2e_stats["h2d_bytes"],
                     "d2h_bytes_per_step": e2e_stats["d2h_bytes"], "steps": len(e2e_t), "warmup_calls": 1,
-                    "setup_ms": e2e_stats["setup_ms"], "wall_s": statistics.median(e2e_t)},
+                    "setup_ms": e2e_stats["setup_ms"], "upload_ms": e2e_stats["upload_ms"],
+                    "device_ms": e2e_stats["device_ms"], "download_ms": e2e_stats["download_ms"],
+                    "call_ms": e2e_stats["total_ms"], "wall_s": statistics.median(e2e_t)},
             "skeleton_351x48": skel,
             "gpu_launches": int(st["kernel_launches"]) * args.steps,
             "clocks": clocks_s,

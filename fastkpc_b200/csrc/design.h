@@ -17,6 +17,9 @@ struct Smooth {
   // containing the variable reuses
   std::vector<double> colsq;       // cols: sum of squares of each column of X
   std::vector<double> root;        // cols x rank: root root' = S
+  // bivariate smooths built on the device: X lives in device memory owned by
+  // the engine (n x cols, leading dimension n) and is empty here
+  const double* dev_x = nullptr;
 };
 
 // One conditioning set's model: X = [1 | smooth_1 | ... ] with one penalty

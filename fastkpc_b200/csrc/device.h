@@ -68,8 +68,8 @@ struct GeomJob {
 struct SingleGeomJob {
   int64_t basis;   // arena offset of QW (n x q)
   int64_t spec;    // arena offset of the spectrum (q)
-  int64_t src;     // B (n x (q - 1)) in the basis table
-  int64_t pen;     // S ((q - 1) x (q - 1)) in the basis table
+  const double* src;  // B (n x (q - 1), leading dimension n), device memory
+  const double* pen;  // S ((q - 1) x (q - 1)), device memory
   int q;
   int rank;
 };

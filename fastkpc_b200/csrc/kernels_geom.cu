@@ -165,8 +165,7 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const d
 // most 100 sweeps), and the fit kernels' inputs QW = Q V and the spectrum e
 // (descending; zero beyond the penalty rank).  status[d]: 1 rank deficient,
 // 2 Jacobi did not converge.
-__global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(const double* __restrict__ table, int n,
-                                                                       const SingleGeomJob* __restrict__ jobs,
+__global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(int n, const SingleGeomJob* __restrict__ jobs,
                                                                        int count, double* __restrict__ arena,
                                                                        int* __restrict__ status) {
   constexpr int Q = kMaxSingleQ;
@@ -181,8 +180,8 @@ __global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(const dou
     const SingleGeomJob& job = jobs[d];
     const int q = job.q, dim = q - 1;
     double* W = arena + job.basis;
-    const double* B = table + job.src;
-    const double* S = table + job.pen;
+    const double* B = job.src;
+    const double* S = job.pen;
     const int64_t nq = static_cast<int64_t>(n) * q;
     for (int64_t idx = tid; idx < nq; idx += blockDim.x) {
       const int r = static_cast<int>(idx % n), c = static_cast<int>(idx / n);
@@ -335,12 +334,12 @@ __global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(const dou
   }
 }
 
-cudaError_t launch_single_geometry(const double* table, int n, const SingleGeomJob* jobs, int count, double* arena,
-                                   int* status, cudaStream_t stream) {
+cudaError_t launch_single_geometry(int n, const SingleGeomJob* jobs, int count, double* arena, int* status,
+                                   cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
   if (n <= kMaxSingleQ) return cudaErrorInvalidValue;
   const int ctas = count < 4 * 148 ? count : 4 * 148;
-  single_geometry_kernel<<<ctas, kGeomThreads, 0, stream>>>(table, n, jobs, count, arena, status);
+  single_geometry_kernel<<<ctas, kGeomThreads, 0, stream>>>(n, jobs, count, arena, status);
   return cudaGetLastError();
 }
 

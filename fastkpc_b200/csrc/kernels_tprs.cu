@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
 // tprs_ritz_select_kernel (one warp per design): the eigen-decomposition of
 // the design's tridiagonal T (alpha, beta; m = done[d] <= steps) by implicit
 // QL with Wilkinson shifts (at most 60 sweeps per eigenvalue), eigenvectors
-// accumulated in a global m x m workspace (lane = row).  It selects the k
+// accumulated in shared memory (steps x steps per warp, lane = row).  It selects the k
 // eigenvalues of largest magnitude (ties to the lower index), orders them by
 // value, descending, and accepts the design only when every selected pair's
 // residual |beta_m s_m| is at most 1e-14 max |theta| (or the Krylov space was
@@ -271,23 +271,24 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
 // tprs_ritz_vectors_kernel (one CTA per accepted design): U = V zsel (nu x k),
 // each column normalised and signed so that its largest-magnitude entry
 // (first on ties) is positive.
-constexpr int kRitzWarps = 4;
+constexpr int kRitzWarps = 4;                    // at most, per CTA
+constexpr size_t kRitzSmemBudget = 200 * 1024;   // dynamic shared memory for the warps' eigenvector matrices
 
 __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
     const double* __restrict__ alpha, const double* __restrict__ beta, const int* __restrict__ done, int count,
-    int steps, int k, double* __restrict__ zws, double* __restrict__ vals, double* __restrict__ zsel,
-    int* __restrict__ ok) {
+    int steps, int k, double* __restrict__ vals, double* __restrict__ zsel, int* __restrict__ ok) {
+  extern __shared__ double zsh[];  // steps x steps per warp
   __shared__ double dsh[kRitzWarps][kTprsMaxSteps], esh[kRitzWarps][kTprsMaxSteps];
   __shared__ int selsh[kRitzWarps][kTprsRitzMax];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int d = blockIdx.x * kRitzWarps + warp;
+  const int d = blockIdx.x * (blockDim.x >> 5) + warp;
   if (d >= count) return;  // whole warps only: no block barrier follows
   double* dd = dsh[warp];
   double* ee = esh[warp];
   int* sel = selsh[warp];
   const int ms = done[d];
   const int64_t ld = steps;
-  double* z = zws + static_cast<int64_t>(d) * steps * steps;
+  double* z = zsh + static_cast<int64_t>(warp) * steps * steps;
   const double* al = alpha + static_cast<int64_t>(d) * steps;
   const double* be = beta + static_cast<int64_t>(d) * steps;
   constexpr int kRows = kTprsMaxSteps / 32;  // rows per lane
@@ -510,16 +511,316 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_ritz_vectors_kernel(
 }
 
 cudaError_t launch_tprs_ritz(const double* alpha, const double* beta, const int* done, int count, int steps, int k,
-                             double* zws, double* vals, double* zsel, int* ok, const double* V, const int64_t* voff,
+                             double* vals, double* zsel, int* ok, const double* V, const int64_t* voff,
                              const int* nus, double* U, const int64_t* uoff, cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
   if (k != kTprsRitzMax || steps < k || steps > kTprsMaxSteps) return cudaErrorInvalidValue;
-  tprs_ritz_select_kernel<<<(count + kRitzWarps - 1) / kRitzWarps, kRitzWarps * 32, 0, stream>>>(
-      alpha, beta, done, count, steps, k, zws, vals, zsel, ok);
-  cudaError_t e = cudaGetLastError();
+  const size_t per_warp = sizeof(double) * static_cast<size_t>(steps) * steps;
+  int warps = static_cast<int>(kRitzSmemBudget / per_warp);
+  warps = warps < 1 ? 1 : (warps > kRitzWarps ? kRitzWarps : warps);
+  const size_t smem = per_warp * warps;
+  cudaError_t e = cudaFuncSetAttribute(tprs_ritz_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  tprs_ritz_select_kernel<<<(count + warps - 1) / warps, warps * 32, smem, stream>>>(alpha, beta, done, count, steps,
+                                                                                      k, vals, zsel, ok);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int ctas = count < 2 * 148 ? count : 2 * 148;
   tprs_ritz_vectors_kernel<<<ctas, kTprsThreads, 0, stream>>>(V, voff, nus, done, ok, zsel, count, steps, U, uoff);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// The rest of the bivariate thin-plate basis, on the device: constraint
+// absorption of the polynomial null space, RMS scaling, penalty scaling and
+// the centering constraint (mgcv's smooth.construct.tp + centering, as the
+// reference restates it: fastkpc/src/full_cuda_ci_native_setup.cpp:621-858).
+// Inputs per design: the k Ritz vectors U (nu x k) and values, the unique
+// locations u (nu x 2; the null space is T = [1, u_x, u_y]) and the row ->
+// location mapping (n).  Outputs: the basis X (n x (k-1), at X + d n k with
+// leading dimension n), the penalty S ((k-1) x (k-1)) and the column sums of
+// squares of X (k-1).  status[d]: 0, or 1 (a zero basis column), 2 (penalty
+// scaling), 3 (centering constraint), -1 (Ritz pairs not accepted).
+constexpr int kFinishK = kTprsRitzMax;
+constexpr int kFinishM = 3;  // null space of the d = 2, m = 2 thin plate: 1, x, y
+
+// Sum over the block of a k-vector held per thread; out[c] for c < K (fixed order).
+template <int K>
+__device__ __forceinline__ void block_vec_sum(const double (&v)[K], double (*red)[K], double* out) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int c = 0; c < K; ++c) {
+    const double s = warp_sum_t(v[c]);
+    if (lane == 0) red[warp][c] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < K) {
+    double s = 0.0;
+    for (int w = 0; w < kTprsWarps; ++w) s += red[w][threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kTprsThreads) tprs_finish_kernel(
+    const double* __restrict__ U, const int64_t* __restrict__ uoff, const double* __restrict__ vals,
+    const int* __restrict__ ok, const double* __restrict__ loc, const int64_t* __restrict__ locoff,
+    const int* __restrict__ nus, const int* __restrict__ mapping, int n, int count, double* __restrict__ X,
+    double* __restrict__ S, double* __restrict__ colsq, int* __restrict__ status) {
+  constexpr int K = kFinishK, M = kFinishM;
+  __shared__ double red[kTprsWarps][K];
+  __shared__ double TU[M][K], Z[M][K];
+  __shared__ double P[K][K + 1];
+  __shared__ double rms[K], cm[K], hv[K], val[K], dvs[K];
+  __shared__ double scal[4];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int d = blockIdx.x; d < count; d += gridDim.x) {
+    if (!ok[d]) {
+      if (tid == 0) status[d] = -1;
+      continue;  // uniform across the block
+    }
+    const int nu = nus[d];
+    const double* Ud = U + uoff[d];
+    const double* ux = loc + locoff[d];
+    const double* uy = ux + nu;
+    const int* map = mapping + static_cast<int64_t>(d) * n;
+    double* Xd = X + static_cast<int64_t>(d) * n * K;
+    if (tid < K) val[tid] = vals[static_cast<int64_t>(d) * K + tid];
+    // TU = T' U (M x K)
+    for (int pr = warp; pr < M * K; pr += kTprsWarps) {
+      const int t = pr / K, c = pr % K;
+      double acc = 0.0;
+      for (int i = lane; i < nu; i += 32) {
+        const double ti = t == 0 ? 1.0 : (t == 1 ? ux[i] : uy[i]);
+        acc += ti * Ud[i + static_cast<int64_t>(nu) * c];
+      }
+      acc = warp_sum_t(acc);
+      if (lane == 0) TU[t][c] = acc;
+    }
+    __syncthreads();
+    // Householder vectors z_t with TU H_0 ... H_{M-1} = [0 | L] (one thread)
+    if (tid == 0) {
+      for (int step = 0; step < M; ++step) {
+        const int L = K - step;
+        double* row = TU[step];
+        double scale = 0.0;
+        for (int c = 0; c < L; ++c) scale = fmax(scale, fabs(row[c]));
+        if (scale != 0.0)
+          for (int c = 0; c < L; ++c) row[c] /= scale;
+        double length = 0.0;
+        for (int c = 0; c < L; ++c) length += row[c] * row[c];
+        length = sqrt(length);
+        if (row[L - 1] < 0.0) length = -length;
+        row[L - 1] += length;
+        const double mult = length != 0.0 ? 1.0 / (length * row[L - 1]) : 0.0;
+        for (int r = step + 1; r < M; ++r) {
+          double proj = 0.0;
+          for (int c = 0; c < L; ++c) proj += row[c] * TU[r][c];
+          proj *= mult;
+          for (int c = 0; c < L; ++c) TU[r][c] -= proj * row[c];
+        }
+        const double rm = sqrt(mult);
+        for (int c = 0; c < K; ++c) Z[step][c] = c < L ? row[c] * rm : 0.0;
+      }
+    }
+    // P = diag(vals)
+    for (int idx = tid; idx < K * K; idx += blockDim.x) P[idx % K][idx / K] = idx % K == idx / K ? val[idx % K] : 0.0;
+    __syncthreads();
+    // P <- P H_0 ... H_{M-1} (row-local), then H_{M-1} ... H_0 P (column-local)
+    for (int t = 0; t < M; ++t) {
+      if (tid < K) {
+        double prod = 0.0;
+        for (int c = 0; c < K; ++c) prod += P[tid][c] * Z[t][c];
+        for (int c = 0; c < K; ++c) P[tid][c] -= prod * Z[t][c];
+      }
+      __syncthreads();
+    }
+    for (int t = 0; t < M; ++t) {
+      if (tid < K) {
+        double prod = 0.0;
+        for (int r = 0; r < K; ++r) prod += P[r][tid] * Z[t][r];
+        for (int r = 0; r < K; ++r) P[r][tid] -= prod * Z[t][r];
+      }
+      __syncthreads();
+    }
+    for (int idx = tid; idx < K * K; idx += blockDim.x) {
+      const int a = idx % K, b = idx / K;
+      if (a >= K - M || b >= K - M) P[a][b] = 0.0;
+    }
+    // pass 1: X rows (U diag(vals) H, null-space columns last, gathered by the mapping), column sums of squares
+    double acc[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    // the Householder vectors are re-read from shared memory (volatile) rather
+    // than held in registers across the row loop
+    const volatile double* Zv = &Z[0][0];
+    for (int r = tid; r < n; r += blockDim.x) {
+      const int li = map[r];
+      double x[K];
+#pragma unroll
+      for (int c = 0; c < K; ++c) x[c] = Ud[li + static_cast<int64_t>(nu) * c] * val[c];
+#pragma unroll
+      for (int t = 0; t < M; ++t) {
+        double prod = 0.0;
+#pragma unroll
+        for (int c = 0; c < K; ++c) prod += x[c] * Zv[t * K + c];
+#pragma unroll
+        for (int c = 0; c < K; ++c) x[c] -= prod * Zv[t * K + c];
+      }
+      x[K - M] = 1.0;
+      x[K - M + 1] = ux[li];
+      x[K - M + 2] = uy[li];
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        Xd[r + static_cast<int64_t>(n) * c] = x[c];
+        acc[c] += x[c] * x[c];
+      }
+    }
+    block_vec_sum<K>(acc, red, rms);
+    if (tid < K) rms[tid] = sqrt(rms[tid] / n);
+    __syncthreads();
+    bool bad = false;
+    for (int c = 0; c < K; ++c) bad = bad || !isfinite(rms[c]) || rms[c] == 0.0;
+    if (bad) {
+      if (tid == 0) status[d] = 1;
+      __syncthreads();
+      continue;
+    }
+    // P scaled as the columns of X: entry (a, b) divided by rms_min(a,b), then rms_max(a,b)
+    for (int idx = tid; idx < K * K; idx += blockDim.x) {
+      const int a = idx % K, b = idx / K;
+      const int lo = a < b ? a : b, hi = a < b ? b : a;
+      P[a][b] = P[a][b] / rms[lo] / rms[hi];
+    }
+    // pass 2: scale X; row abs sums (max), column sums
+    const volatile double* rmsv = rms;
+    double xmax = 0.0;
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    for (int r = tid; r < n; r += blockDim.x) {
+      double rs = 0.0;
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        const double v = Xd[r + static_cast<int64_t>(n) * c] / rmsv[c];
+        Xd[r + static_cast<int64_t>(n) * c] = v;
+        rs += fabs(v);
+        acc[c] += v;
+      }
+      xmax = fmax(xmax, rs);
+    }
+    for (int o = 16; o > 0; o >>= 1) xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+    if (lane == 0) red[warp][0] = xmax;  // red is free: block_vec_sum below re-synchronises first
+    __syncthreads();
+    if (tid == 0) {
+      double mx = 0.0;
+      for (int w = 0; w < kTprsWarps; ++w) mx = fmax(mx, red[w][0]);
+      scal[0] = mx;
+    }
+    __syncthreads();
+    block_vec_sum<K>(acc, red, cm);
+    if (tid < K) cm[tid] /= n;
+    __syncthreads();
+    // pass 3: the mean's correction term (two-pass mean)
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    const volatile double* cmv = cm;
+    for (int r = tid; r < n; r += blockDim.x)
+#pragma unroll
+      for (int c = 0; c < K; ++c) acc[c] += Xd[r + static_cast<int64_t>(n) * c] - cmv[c];
+    block_vec_sum<K>(acc, red, dvs);
+    if (tid < K) cm[tid] += dvs[tid] / n;
+    // symmetric penalty, scaled by ||Ps||_1 / ||X||_inf^2
+    __syncthreads();
+    if (tid < K) {
+      for (int a = 0; a < tid; ++a) {
+        const double v = (P[a][tid] + P[tid][a]) / 2.0;
+        P[a][tid] = v;
+        P[tid][a] = v;
+      }
+    }
+    __syncthreads();
+    if (tid < K) {
+      double s = 0.0;
+      for (int a = 0; a < K; ++a) s += fabs(P[a][tid]);
+      dvs[tid] = s;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double pn = 0.0;
+      for (int c = 0; c < K; ++c) pn = fmax(pn, dvs[c]);
+      scal[1] = pn / (scal[0] * scal[0]);
+      double nrm = 0.0;
+      for (int c = 0; c < K; ++c) nrm += cm[c] * cm[c];
+      nrm = sqrt(nrm);
+      if (cm[0] != 0.0) nrm = copysign(nrm, cm[0]);
+      scal[2] = nrm;
+    }
+    __syncthreads();
+    const double pscale = scal[1], nrm = scal[2];
+    if (!isfinite(pscale) || pscale <= 0.0 || nrm == 0.0) {
+      if (tid == 0) status[d] = nrm == 0.0 ? 3 : 2;
+      __syncthreads();
+      continue;
+    }
+    for (int idx = tid; idx < K * K; idx += blockDim.x) P[idx % K][idx / K] /= pscale;
+    if (tid < K) hv[tid] = cm[tid] / nrm + (tid == 0 ? 1.0 : 0.0);
+    __syncthreads();
+    const double v0 = hv[0];
+    // pass 4: X H without its first column, in place; column sums of squares
+    const volatile double* hvv = hv;
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    for (int r = tid; r < n; r += blockDim.x) {
+      double x[K];
+#pragma unroll
+      for (int c = 0; c < K; ++c) x[c] = Xd[r + static_cast<int64_t>(n) * c];
+      double dv = 0.0;
+#pragma unroll
+      for (int c = 0; c < K; ++c) dv += x[c] * hvv[c];
+      dv /= v0;
+#pragma unroll
+      for (int c = 1; c < K; ++c) {
+        const double v = x[c] - dv * hvv[c];
+        Xd[r + static_cast<int64_t>(n) * (c - 1)] = v;
+        acc[c - 1] += v * v;
+      }
+    }
+    acc[K - 1] = 0.0;
+    block_vec_sum<K>(acc, red, dvs);
+    if (tid < K - 1) colsq[static_cast<int64_t>(d) * (K - 1) + tid] = dvs[tid];
+    // S = (H Ps H) without its first row and column: column-local, then row-local
+    if (tid < K) {
+      double dv = 0.0;
+      for (int a = 0; a < K; ++a) dv += hv[a] * P[a][tid];
+      dv /= v0;
+      for (int a = 0; a < K; ++a) P[a][tid] -= dv * hv[a];
+    }
+    __syncthreads();
+    if (tid < K) {
+      double dv = 0.0;
+      for (int c = 0; c < K; ++c) dv += P[tid][c] * hv[c];
+      dvs[tid] = dv / v0;
+    }
+    __syncthreads();
+    double* Sd = S + static_cast<int64_t>(d) * (K - 1) * (K - 1);
+    for (int idx = tid; idx < (K - 1) * (K - 1); idx += blockDim.x) {
+      const int a = idx % (K - 1) + 1, c = idx / (K - 1) + 1;
+      Sd[idx] = P[a][c] - dvs[a] * hv[c];
+    }
+    if (tid == 0) status[d] = 0;
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_tprs_finish(const double* U, const int64_t* uoff, const double* vals, const int* ok,
+                               const double* loc, const int64_t* locoff, const int* nus, const int* mapping, int n,
+                               int count, double* X, double* S, double* colsq, int* status, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  if (n < kFinishK) return cudaErrorInvalidValue;
+  const int ctas = count < 2 * 148 ? count : 2 * 148;
+  tprs_finish_kernel<<<ctas, kTprsThreads, 0, stream>>>(U, uoff, vals, ok, loc, locoff, nus, mapping, n, count, X, S,
+                                                         colsq, status);
   return cudaGetLastError();
 }
 

@@ -114,6 +114,7 @@ void Engine::load(const double* data, int n, int p) {
              "upload data");
   cuda_check(cudaStreamSynchronize(stream_), "upload data");
   cache_.reset(new DesignCache(host_data_.data(), n, p));
+  smooth_store_.clear();
   release_graph();
 }
 
@@ -229,8 +230,8 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
     if (ok[i]) batch->idx.push_back(i);
   if (batch->idx.empty()) return;
   std::vector<double> u;
-  std::vector<int64_t> uoff, voff;
-  batch->uoff.clear();
+  std::vector<int64_t> uoff, voff, roff;
+  std::vector<int> map;
   batch->nus.clear();
   int nu_max = 0;
   int64_t vtotal = 0, utotal = 0;
@@ -238,10 +239,11 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
     const TprsPrep& pr = batch->preps[i];
     uoff.push_back(static_cast<int64_t>(u.size()));
     u.insert(u.end(), pr.u.begin(), pr.u.end());
+    map.insert(map.end(), pr.mapping.begin(), pr.mapping.end());
     batch->nus.push_back(pr.nu);
     voff.push_back(vtotal);
     vtotal += static_cast<int64_t>(pr.nu) * kTprsSteps;
-    batch->uoff.push_back(utotal);
+    roff.push_back(utotal);
     utotal += static_cast<int64_t>(pr.nu) * kTprsK;
     nu_max = std::max(nu_max, pr.nu);
   }
@@ -249,16 +251,19 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
   const int ctas = std::min(cnt, 2 * 148);  // two designs per SM (memory-bound matvec)
   const size_t nab = static_cast<size_t>(2) * cnt * kTprsSteps;
   const size_t nvals = static_cast<size_t>(cnt) * kTprsK;
-  // page-locked landing area: Ritz vectors, values, then the acceptance flags
-  double* host = pinned_arena(static_cast<size_t>(utotal) + nvals + (static_cast<size_t>(cnt) + 1) / 2);
-  batch->U = host;
-  batch->vals = host + utotal;
-  batch->ok = reinterpret_cast<int*>(host + utotal + nvals);
+  const size_t ns = static_cast<size_t>(cnt) * (kTprsK - 1) * (kTprsK - 1);
+  const size_t ncs = static_cast<size_t>(cnt) * (kTprsK - 1);
+  // page-locked landing area: penalties, column sums of squares, status
+  double* host = pinned_arena(ns + ncs + (static_cast<size_t>(cnt) + 1) / 2);
+  batch->S = host;
+  batch->colsq = host + ns;
+  batch->status = reinterpret_cast<int*>(host + ns + ncs);
   upload(d_tprs_u_, u, stream_);
   upload(d_tprs_uoff_, uoff, stream_);
   upload(d_tprs_voff_, voff, stream_);
-  upload(d_tprs_roff_, batch->uoff, stream_);
+  upload(d_tprs_roff_, roff, stream_);
   upload(d_tprs_nus_, batch->nus, stream_);
+  upload(d_tprs_map_, map, stream_);
   const int64_t ews_stride = tprs_ld(nu_max) * tprs_ld(nu_max);
   double* dV = d_tprs_V_.ensure(static_cast<size_t>(vtotal));
   double* dab = d_tprs_ab_.ensure(nab);
@@ -267,37 +272,47 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
   double* dvals = d_tprs_vals_.ensure(nvals);
   double* dU = d_tprs_U_.ensure(static_cast<size_t>(utotal));
   int* dok = d_tprs_ok_.ensure(cnt);
+  smooth_store_.emplace_back(new DevBuf<double>());
+  double* dX = smooth_store_.back()->ensure(static_cast<size_t>(cnt) * n * kTprsK);
+  batch->X = dX;
+  double* dS = d_tprs_S_.ensure(ns);
+  double* dcs = d_tprs_colsq_.ensure(ncs);
+  int* dst = d_tprs_status_.ensure(cnt);
   cuda_check(launch_tprs_lanczos(d_tprs_u_.get(), d_tprs_uoff_.get(), d_tprs_nus_.get(), cnt, nu_max, kTprsSteps,
                                  tprs_eta0(2), ews, ews_stride, ctas, dV, d_tprs_voff_.get(), dab,
                                  dab + static_cast<size_t>(cnt) * kTprsSteps, ddone, stream_),
              "thin-plate Lanczos");
   cuda_check(launch_tprs_ritz(dab, dab + static_cast<size_t>(cnt) * kTprsSteps, ddone, cnt, kTprsSteps, kTprsK,
-                              d_tprs_zws_.ensure(static_cast<size_t>(cnt) * kTprsSteps * kTprsSteps), dvals,
-                              d_tprs_zsel_.ensure(nvals * kTprsSteps), dok, dV, d_tprs_voff_.get(),
+                              dvals, d_tprs_zsel_.ensure(nvals * kTprsSteps), dok, dV, d_tprs_voff_.get(),
                               d_tprs_nus_.get(), dU, d_tprs_roff_.get(), stream_),
              "thin-plate Ritz pairs");
-  cuda_check(cudaMemcpyAsync(batch->U, dU, static_cast<size_t>(utotal) * sizeof(double), cudaMemcpyDeviceToHost,
+  cuda_check(launch_tprs_finish(dU, d_tprs_roff_.get(), dvals, dok, d_tprs_u_.get(), d_tprs_uoff_.get(),
+                                d_tprs_nus_.get(), d_tprs_map_.get(), n, cnt, dX, dS, dcs, dst, stream_),
+             "thin-plate basis");
+  cuda_check(cudaMemcpyAsync(batch->S, dS, ns * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
+  cuda_check(cudaMemcpyAsync(batch->colsq, dcs, ncs * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
+  cuda_check(cudaMemcpyAsync(batch->status, dst, static_cast<size_t>(cnt) * sizeof(int), cudaMemcpyDeviceToHost,
                              stream_),
              "download");
-  cuda_check(cudaMemcpyAsync(batch->vals, dvals, nvals * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
-  cuda_check(cudaMemcpyAsync(batch->ok, dok, static_cast<size_t>(cnt) * sizeof(int), cudaMemcpyDeviceToHost, stream_),
-             "download");
-  d2h_bytes_ += static_cast<double>(utotal + nvals) * sizeof(double) + static_cast<double>(cnt) * sizeof(int);
+  d2h_bytes_ += static_cast<double>(ns + ncs) * sizeof(double) + static_cast<double>(cnt) * sizeof(int);
 }
 
 void Engine::finish_bivariate_on_device(TprsBatch* batch) {
   if (batch->idx.empty()) return;
-  cuda_check(cudaStreamSynchronize(stream_), "thin-plate Lanczos");
-  parallel_for(batch->idx.size(), [&](size_t c) {
-    if (!batch->ok[c]) return;  // not converged: the host set-up builds this design
-    const size_t i = batch->idx[c];
-    const int nu = batch->nus[c];
-    std::vector<double> vals(batch->vals + c * kTprsK, batch->vals + (c + 1) * kTprsK);
-    std::vector<double> U(batch->U + batch->uoff[c], batch->U + batch->uoff[c] + static_cast<int64_t>(nu) * kTprsK);
-    auto sm = std::make_shared<Smooth>(tprs_finish(batch->preps[i], vals, U));
-    sm->colsq = column_sumsq(sm->X.data(), sm->n, sm->cols);
-    cache_->put_bivariate(batch->sets[i], sm);
-  });
+  cuda_check(cudaStreamSynchronize(stream_), "thin-plate set-up");
+  const int n = n_;
+  constexpr int cols = kTprsK - 1;
+  for (size_t c = 0; c < batch->idx.size(); ++c) {
+    if (batch->status[c] != 0) continue;  // not converged or degenerate: the host set-up builds this design
+    auto sm = std::make_shared<Smooth>();
+    sm->n = n;
+    sm->cols = cols;
+    sm->rank = kTprsK - 3;  // the d = 2 thin plate's null space has dimension 3
+    sm->S.assign(batch->S + c * cols * cols, batch->S + (c + 1) * cols * cols);
+    sm->colsq.assign(batch->colsq + c * cols, batch->colsq + (c + 1) * cols);
+    sm->dev_x = batch->X + c * static_cast<size_t>(n) * kTprsK;
+    cache_->put_bivariate(batch->sets[batch->idx[c]], sm);
+  }
 }
 
 // Designs of the sets selected by `pick`, built on host threads (the cache
@@ -354,8 +369,8 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
     auto it = smooth_index.find(sm);
     if (it == smooth_index.end()) {
       it = smooth_index.emplace(sm, smooth_slots.size()).first;
-      smooth_slots.push_back({sm, static_cast<int64_t>(total), -1});
-      total += sm->X.size();
+      smooth_slots.push_back({sm, sm->dev_x ? -1 : static_cast<int64_t>(total), -1});
+      total += sm->X.size();  // empty for a basis already on the device
     }
     SmoothSlot& sl = smooth_slots[it->second];
     if (with_penalty && sl.pen < 0) {
@@ -447,7 +462,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
         if (item >= designs_.size() + smooth_slots.size()) return;
         if (item >= designs_.size()) {
           const SmoothSlot& sl = smooth_slots[item - designs_.size()];
-          std::memcpy(host + sl.x, sl.smooth->X.data(), sl.smooth->X.size() * sizeof(double));
+          if (sl.x >= 0) std::memcpy(host + sl.x, sl.smooth->X.data(), sl.smooth->X.size() * sizeof(double));
           if (sl.pen >= 0) std::memcpy(host + sl.pen, sl.smooth->S.data(), sl.smooth->S.size() * sizeof(double));
           continue;
         }
@@ -484,7 +499,9 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       for (auto& th : pool) th.join();
     }
   }
-  // Device geometry jobs; the smooth bases and penalties sit in the host range.
+  // Device geometry jobs; the smooth bases and penalties sit in the host range
+  // (a bivariate basis built on the device stays in the smooth store).
+  double* arena = d_arena_.ensure(dev_base + dev_total);
   std::vector<GeomJob> gjobs(geom_designs.size());
   std::vector<SingleGeomJob> sjobs(single_designs.size());
   int geom_max_q = 1;
@@ -496,8 +513,8 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
     std::memset(&job, 0, sizeof(job));
     job.basis = dd.basis;
     job.spec = dd.spec;
-    job.src = sl.x;
-    job.pen = sl.pen;
+    job.src = sl.smooth->dev_x ? sl.smooth->dev_x : arena + sl.x;
+    job.pen = arena + sl.pen;
     job.q = des.q;
     job.rank = des.ranks[0];
   }
@@ -567,7 +584,6 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   const size_t npairs = pairs_.size();
   auto t0 = std::chrono::steady_clock::now();
   h2d_bytes_ = static_cast<double>(host_data_.size() * sizeof(double));
-  double* arena = d_arena_.ensure(dev_base + dev_total);
   if (total > 0)
     cuda_check(cudaMemcpyAsync(arena, host, total * sizeof(double), cudaMemcpyHostToDevice, stream_), "upload arena");
   h2d_bytes_ += static_cast<double>(total * sizeof(double));
@@ -581,7 +597,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   }
   if (!sjobs.empty()) {
     h2d_bytes_ += upload(d_single_geom_jobs_, sjobs, stream_);
-    cuda_check(launch_single_geometry(arena, n, d_single_geom_jobs_.get(), static_cast<int>(sjobs.size()), arena,
+    cuda_check(launch_single_geometry(n, d_single_geom_jobs_.get(), static_cast<int>(sjobs.size()), arena,
                                       gstatus_dev + gjobs.size(), stream_),
                "single-penalty geometry");
   }

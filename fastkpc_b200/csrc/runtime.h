@@ -114,11 +114,11 @@ class Engine {
     std::vector<std::vector<int>> sets;
     std::vector<TprsPrep> preps;
     std::vector<size_t> idx;  // sets taken by the device
-    std::vector<int64_t> uoff;  // each design's Ritz vectors (nu x k) in U
     std::vector<int> nus;
-    double* U = nullptr;      // page-locked results (inside the staging arena)
-    double* vals = nullptr;
-    int* ok = nullptr;
+    const double* X = nullptr;  // device: design c's basis at X + c n k (smooth store)
+    double* S = nullptr;        // page-locked results (inside the staging arena)
+    double* colsq = nullptr;
+    int* status = nullptr;
   };
   void launch_bivariate_on_device(const std::vector<std::vector<int>>& sets, TprsBatch* batch);
   void finish_bivariate_on_device(TprsBatch* batch);
@@ -135,6 +135,9 @@ class Engine {
   std::vector<double> host_data_;
   DevBuf<double> d_data_;
   std::unique_ptr<DesignCache> cache_;
+  // device bases of the cache's bivariate smooths (one chunk per level batch);
+  // released with the cache
+  std::vector<std::unique_ptr<DevBuf<double>>> smooth_store_;
 
   // batch plan
   fkpc_options opt_{};
@@ -163,7 +166,8 @@ class Engine {
   DevBuf<double> d_tprs_u_, d_tprs_V_, d_tprs_ab_, d_tprs_ews_;
   DevBuf<int64_t> d_tprs_uoff_, d_tprs_voff_, d_tprs_roff_;
   DevBuf<int> d_tprs_nus_, d_tprs_done_, d_tprs_ok_;
-  DevBuf<double> d_tprs_zws_, d_tprs_vals_, d_tprs_zsel_, d_tprs_U_;
+  DevBuf<double> d_tprs_vals_, d_tprs_zsel_, d_tprs_U_, d_tprs_S_, d_tprs_colsq_;
+  DevBuf<int> d_tprs_map_, d_tprs_status_;
   // device geometry of the additive designs
   DevBuf<GeomJob> d_geom_jobs_;
   DevBuf<SingleGeomJob> d_single_geom_jobs_;

@@ -201,8 +201,12 @@ void evaluate(fkpc::Engine& eng, const std::vector<fkpc::Test>& tests, const fkp
     const size_t e = std::min(tests.size(), b + chunk);
     std::vector<fkpc::Test> part(tests.begin() + b, tests.begin() + e);
     fkpc_stage_stats st{};
-    eng.prepare(part, opt, rs);
-    eng.execute();
+    if (opt.mode == FKPC_MODE_PLAIN) {
+      eng.prepare(part, opt, rs);
+      eng.execute();
+    } else {
+      eng.run_batch(part, opt, rs);
+    }
     eng.collect(out->data() + b, &st);
     add_stats(acc, st);
   }

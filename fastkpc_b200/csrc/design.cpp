@@ -664,6 +664,27 @@ bool DesignCache::has_design(const std::vector<int>& S) {
   return designs_.count(S) > 0 || bi_.count(S) > 0;
 }
 
+std::vector<std::shared_ptr<const Design>> DesignCache::find_designs(const std::vector<const std::vector<int>*>& sets) {
+  std::vector<std::shared_ptr<const Design>> out(sets.size());
+  std::lock_guard<std::mutex> lock(mu_);
+  for (size_t i = 0; i < sets.size(); ++i) {
+    auto it = designs_.find(*sets[i]);
+    if (it != designs_.end()) out[i] = it->second;
+  }
+  return out;
+}
+
+std::shared_ptr<const Design> DesignCache::build(const std::vector<int>& S) {
+  return S.size() >= 3 ? build_additive_meta(n_, p_, S, this) : build_single_meta(n_, p_, S, this);
+}
+
+void DesignCache::put_designs(const std::vector<const std::vector<int>*>& sets,
+                              const std::vector<std::shared_ptr<const Design>>& designs) {
+  std::lock_guard<std::mutex> lock(mu_);
+  for (size_t i = 0; i < sets.size(); ++i)
+    if (designs[i]) designs_.emplace(*sets[i], designs[i]);
+}
+
 std::shared_ptr<const Design> DesignCache::get(const std::vector<int>& S) {
   {
     std::lock_guard<std::mutex> lock(mu_);

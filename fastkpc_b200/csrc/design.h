@@ -85,6 +85,12 @@ class DesignCache {
  public:
   DesignCache(const double* data, int n, int p) : data_(data), n_(n), p_(p) {}
   std::shared_ptr<const Design> get(const std::vector<int>& S);
+  // Batched use from many threads: look every set up under one lock, build
+  // the missing designs without the lock (build), insert them under one lock.
+  std::vector<std::shared_ptr<const Design>> find_designs(const std::vector<const std::vector<int>*>& sets);
+  std::shared_ptr<const Design> build(const std::vector<int>& S);
+  void put_designs(const std::vector<const std::vector<int>*>& sets,
+                   const std::vector<std::shared_ptr<const Design>>& designs);
   std::shared_ptr<const Smooth> univariate(int column);
   // bivariate thin-plate smooths built outside build_design (device eigen)
   void put_bivariate(const std::vector<int>& S, std::shared_ptr<const Smooth> smooth);

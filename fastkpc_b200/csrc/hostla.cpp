@@ -195,7 +195,7 @@ bool tridiagonal_ql(int n, double* d, double* e, double* z) {
 
 namespace {
 
-void symv(const double* A, int n, const double* x, double* y) {
+__attribute__((always_inline)) inline void symv(const double* A, int n, const double* x, double* y) {
   // upper triangle only: column j gives y[i] += A(i,j) x[j] and y[j] += A(i,j) x[i], i < j
   for (int i = 0; i < n; ++i) y[i] = 0.0;
   for (int j = 0; j < n; ++j) {
@@ -217,10 +217,8 @@ void symv(const double* A, int n, const double* x, double* y) {
   }
 }
 
-double dot(const double* a, const double* b, int n) {
-  double s = 0.0;
-  for (int i = 0; i < n; ++i) s += a[i] * b[i];
-  return s;
+__attribute__((always_inline)) inline double dot(const double* a, const double* b, int n) {
+  return dot_chains(a, b, n);
 }
 
 // indices of the k entries of largest |value| (ties toward the lower index)
@@ -361,5 +359,6 @@ int top_magnitude_eigen(const double* A, int n, int k, std::vector<double>* valu
   }
   throw std::runtime_error("Lanczos did not converge");
 }
+
 
 }  // namespace fkpc

@@ -32,6 +32,9 @@ namespace {
 constexpr int kGeomThreads = 256;
 constexpr int kGeomWarps = kGeomThreads / 32;
 constexpr int kGeomMaxQ = 112;
+constexpr size_t kGeomSmemLimit = 220 * 1024;    // dynamic + static shared memory of one CTA
+constexpr size_t kAdditiveStaticSmem = 4 * 1024;  // colsrc, vks, betas, red (2.7 KB) rounded up
+constexpr size_t kSingleStaticSmem = 44 * 1024;   // R, Ri, T, A, V, ... (41.2 KB) rounded up
 
 __device__ __forceinline__ double warp_sum_g(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -114,10 +117,14 @@ static __device__ bool householder_inplace(double* __restrict__ W, int n, int q,
   return deficient;
 }
 
+// in_smem: the design's n x q working matrix lives in dynamic shared memory
+// (n q doubles available) and Q is written to the arena at the end;
+// otherwise it is factored in place in the arena (L2).
 __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const double* __restrict__ table, int n,
                                                                          const GeomJob* __restrict__ jobs, int count,
                                                                          double* __restrict__ arena,
-                                                                         int* __restrict__ status) {
+                                                                         int* __restrict__ status, int in_smem) {
+  extern __shared__ double wsm[];
   __shared__ int64_t colsrc[kGeomMaxQ];
   __shared__ double vks[kGeomMaxQ], betas[kGeomMaxQ];
   __shared__ double red[kGeomWarps];
@@ -125,7 +132,8 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const d
   for (int d = blockIdx.x; d < count; d += gridDim.x) {
     const GeomJob& job = jobs[d];
     const int q = job.q;
-    double* W = arena + job.basis;
+    double* Q = arena + job.basis;
+    double* W = in_smem ? wsm : Q;
     double* R = arena + job.rmat;
     if (tid < q) {
       int64_t src = -1;  // the intercept column
@@ -144,6 +152,8 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const d
     for (int idx = tid; idx < q * q; idx += blockDim.x) R[idx] = 0.0;
     __syncthreads();
     const bool deficient = householder_inplace(W, n, q, R, q, vks, betas, red);
+    if (in_smem)
+      for (int64_t idx = tid; idx < nq; idx += blockDim.x) Q[idx] = W[idx];
     if (job.rpack >= 0) {
       double* rp = arena + job.rpack;
       for (int idx = tid; idx < kWarpTri; idx += blockDim.x) rp[idx] = 0.0;
@@ -167,7 +177,8 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const d
 // 2 Jacobi did not converge.
 __global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(int n, const SingleGeomJob* __restrict__ jobs,
                                                                        int count, double* __restrict__ arena,
-                                                                       int* __restrict__ status) {
+                                                                       int* __restrict__ status, int in_smem) {
+  extern __shared__ double wsm[];
   constexpr int Q = kMaxSingleQ;
   constexpr int LA = Q + 1;  // padded leading dimension of the Jacobi matrices
   __shared__ double Rs[Q * Q], Ri[Q * Q], T[Q * Q];
@@ -179,7 +190,8 @@ __global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(int n, co
   for (int d = blockIdx.x; d < count; d += gridDim.x) {
     const SingleGeomJob& job = jobs[d];
     const int q = job.q, dim = q - 1;
-    double* W = arena + job.basis;
+    double* QW = arena + job.basis;
+    double* W = in_smem ? wsm : QW;
     const double* B = job.src;
     const double* S = job.pen;
     const int64_t nq = static_cast<int64_t>(n) * q;
@@ -315,7 +327,7 @@ __global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(int n, co
       T[idx] = Vs[r + LA * order[c]];
     }
     __syncthreads();
-    // QW = Q V, a row per thread, in place
+    // QW = Q V, a row per thread (in place when W is the arena slot)
     for (int r = tid; r < n; r += blockDim.x) {
       double qrow[Q];
 #pragma unroll
@@ -326,7 +338,7 @@ __global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(int n, co
 #pragma unroll
         for (int t = 0; t < Q; ++t)
           if (t < q) acc += qrow[t] * T[t + q * c];
-        W[r + static_cast<int64_t>(n) * c] = acc;
+        QW[r + static_cast<int64_t>(n) * c] = acc;
       }
     }
     if (tid == 0) status[d] = 0;
@@ -334,12 +346,42 @@ __global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(int n, co
   }
 }
 
+namespace {
+
+// Dynamic shared memory for an n x max_q working matrix, or 0 when it does
+// not fit beside the static arrays (the arena is the working set then).
+size_t geometry_smem(int n, int max_q, size_t static_bytes) {
+  const size_t bytes = sizeof(double) * static_cast<size_t>(n) * max_q;
+  return bytes + static_bytes <= kGeomSmemLimit ? bytes : 0;
+}
+
+template <class K>
+cudaError_t geometry_launch_shape(K kernel, size_t smem, int count, int* ctas) {
+  if (smem > 0) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+  }
+  int per_sm = 4;  // CTAs resident per SM
+  if (smem > 0) {
+    per_sm = static_cast<int>(kGeomSmemLimit / (smem + 2048));
+    per_sm = per_sm < 1 ? 1 : (per_sm > 4 ? 4 : per_sm);
+  }
+  const int cap = 148 * per_sm;
+  *ctas = count < cap ? count : cap;
+  return cudaSuccess;
+}
+
+}  // namespace
+
 cudaError_t launch_single_geometry(int n, const SingleGeomJob* jobs, int count, double* arena, int* status,
                                    cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
   if (n <= kMaxSingleQ) return cudaErrorInvalidValue;
-  const int ctas = count < 4 * 148 ? count : 4 * 148;
-  single_geometry_kernel<<<ctas, kGeomThreads, 0, stream>>>(n, jobs, count, arena, status);
+  const size_t smem = geometry_smem(n, kMaxSingleQ, kSingleStaticSmem);
+  int ctas = 0;
+  cudaError_t e = geometry_launch_shape(single_geometry_kernel, smem, count, &ctas);
+  if (e != cudaSuccess) return e;
+  single_geometry_kernel<<<ctas, kGeomThreads, smem, stream>>>(n, jobs, count, arena, status, smem > 0 ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -347,8 +389,12 @@ cudaError_t launch_additive_geometry(const double* table, int n, const GeomJob* 
                                      double* arena, int* status, cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
   if (n < 2 || max_q < 1 || max_q > kGeomMaxQ || max_q >= n) return cudaErrorInvalidValue;
-  const int ctas = count < 4 * 148 ? count : 4 * 148;
-  additive_geometry_kernel<<<ctas, kGeomThreads, 0, stream>>>(table, n, jobs, count, arena, status);
+  const size_t smem = geometry_smem(n, max_q, kAdditiveStaticSmem);
+  int ctas = 0;
+  cudaError_t e = geometry_launch_shape(additive_geometry_kernel, smem, count, &ctas);
+  if (e != cudaSuccess) return e;
+  additive_geometry_kernel<<<ctas, kGeomThreads, smem, stream>>>(table, n, jobs, count, arena, status,
+                                                                  smem > 0 ? 1 : 0);
   return cudaGetLastError();
 }
 

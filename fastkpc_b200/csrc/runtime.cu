@@ -68,12 +68,52 @@ Engine::~Engine() {
   cudaSetDevice(device_);
   release_graph();
   if (h_arena_) cudaFreeHost(h_arena_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  if (h_stage_) cudaFreeHost(h_stage_);
+  for (char* b : h_stage_retired_) cudaFreeHost(b);
   for (auto& ev : ev_)
     if (ev) cudaEventDestroy(ev);
   if (stream_) {
     cudaStreamSynchronize(stream_);
     cudaStreamDestroy(stream_);
   }
+}
+
+void Engine::stage_reset() {
+  for (char* b : h_stage_retired_) cudaFreeHost(b);
+  h_stage_retired_.clear();
+  h_stage_used_ = 0;
+}
+
+void* Engine::stage_alloc(size_t bytes) {
+  bytes = (bytes + 255) / 256 * 256;
+  if (h_stage_used_ + bytes > h_stage_cap_) {
+    if (h_stage_) h_stage_retired_.push_back(h_stage_);  // copies or the host may still read it
+    h_stage_ = nullptr;
+    const size_t cap = std::max<size_t>(2 * h_stage_cap_, 2 * bytes);
+    h_stage_cap_ = 0;
+    h_stage_used_ = 0;
+    cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&h_stage_), cap, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      h_stage_ = nullptr;
+      throw Error(FKPC_STATUS_ALLOCATION, std::string("pinned host allocation failed: ") + cudaGetErrorString(e));
+    }
+    h_stage_cap_ = cap;
+  }
+  void* p = h_stage_ + h_stage_used_;
+  h_stage_used_ += bytes;
+  return p;
+}
+
+template <class T>
+double Engine::stage_upload(DevBuf<T>& buf, const std::vector<T>& host) {
+  T* d = buf.ensure(host.size());
+  if (host.empty()) return 0.0;
+  const size_t bytes = host.size() * sizeof(T);
+  void* h = stage_alloc(bytes);
+  std::memcpy(h, host.data(), bytes);
+  cuda_check(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream_), "upload");
+  return static_cast<double>(bytes);
 }
 
 double* Engine::pinned_arena(size_t count) {
@@ -191,7 +231,10 @@ void parallel_for(size_t count, F f) {
 }
 
 constexpr int kTprsK = 30;                  // basis dimension of the bivariate thin-plate smooth
-constexpr int kTprsSteps = kTprsK + 60;     // Lanczos steps on the device (the host needs about 65)
+// Lanczos steps on the device.  The host solver, checking every 5 steps,
+// converges within 60-70 steps on the 587 bivariate designs of a 500 x 50
+// level; a design that has not converged by kTprsSteps is rebuilt on the host.
+constexpr int kTprsSteps = kTprsK + 50;
 // Every bivariate design the engine builds takes the device Lanczos, however
 // few there are: the per-design computation is deterministic, so a design
 // comes out bit-identical whatever batch (plain or batched form) it is in.
@@ -254,16 +297,16 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
   const size_t ns = static_cast<size_t>(cnt) * (kTprsK - 1) * (kTprsK - 1);
   const size_t ncs = static_cast<size_t>(cnt) * (kTprsK - 1);
   // page-locked landing area: penalties, column sums of squares, status
-  double* host = pinned_arena(ns + ncs + (static_cast<size_t>(cnt) + 1) / 2);
+  double* host = static_cast<double*>(stage_alloc(sizeof(double) * (ns + ncs + (static_cast<size_t>(cnt) + 1) / 2)));
   batch->S = host;
   batch->colsq = host + ns;
   batch->status = reinterpret_cast<int*>(host + ns + ncs);
-  upload(d_tprs_u_, u, stream_);
-  upload(d_tprs_uoff_, uoff, stream_);
-  upload(d_tprs_voff_, voff, stream_);
-  upload(d_tprs_roff_, roff, stream_);
-  upload(d_tprs_nus_, batch->nus, stream_);
-  upload(d_tprs_map_, map, stream_);
+  stage_upload(d_tprs_u_, u);
+  stage_upload(d_tprs_uoff_, uoff);
+  stage_upload(d_tprs_voff_, voff);
+  stage_upload(d_tprs_roff_, roff);
+  stage_upload(d_tprs_nus_, batch->nus);
+  stage_upload(d_tprs_map_, map);
   const int64_t ews_stride = tprs_ld(nu_max) * tprs_ld(nu_max);
   double* dV = d_tprs_V_.ensure(static_cast<size_t>(vtotal));
   double* dab = d_tprs_ab_.ensure(nab);
@@ -295,11 +338,12 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
                              stream_),
              "download");
   d2h_bytes_ += static_cast<double>(ns + ncs) * sizeof(double) + static_cast<double>(cnt) * sizeof(int);
+  cuda_check(cudaEventRecord(ev_[6], stream_), "event");
 }
 
 void Engine::finish_bivariate_on_device(TprsBatch* batch) {
   if (batch->idx.empty()) return;
-  cuda_check(cudaStreamSynchronize(stream_), "thin-plate set-up");
+  cuda_check(cudaEventSynchronize(ev_[6]), "thin-plate set-up");
   const int n = n_;
   constexpr int cols = kTprsK - 1;
   for (size_t c = 0; c < batch->idx.size(); ++c) {
@@ -320,14 +364,48 @@ void Engine::finish_bivariate_on_device(TprsBatch* batch) {
 template <class Pick>
 void Engine::build_host_designs(Pick pick) {
   std::vector<size_t> todo;
+  std::vector<const std::vector<int>*> keys;
   for (size_t i = 0; i < sets_.size(); ++i)
-    if (pick(sets_[i])) todo.push_back(i);
+    if (!designs_[i] && pick(sets_[i])) {
+      todo.push_back(i);
+      keys.push_back(&sets_[i]);
+    }
+  if (todo.empty()) return;
+  std::vector<std::shared_ptr<const Design>> found = cache_->find_designs(keys);
+  std::vector<std::shared_ptr<const Design>> built(todo.size());
   std::string err;
   std::mutex err_mu;
   parallel_for(todo.size(), [&](size_t c) {
-    const size_t i = todo[c];
+    if (found[c]) return;
     try {
-      designs_[i] = cache_->get(sets_[i]);
+      built[c] = cache_->build(sets_[todo[c]]);
+    } catch (const std::exception& e) {
+      std::lock_guard<std::mutex> lock(err_mu);
+      if (err.empty()) err = e.what();
+    }
+  });
+  if (!err.empty()) throw Error(FKPC_STATUS_RANK, "design set-up failed: " + err);
+  cache_->put_designs(keys, built);
+  for (size_t c = 0; c < todo.size(); ++c) designs_[todo[c]] = found[c] ? found[c] : built[c];
+}
+
+// The univariate smooths of the batch's variables, each built once (several
+// additive designs share a variable; building them design by design would
+// let threads race to build the same smooth).
+void Engine::build_univariate_smooths() {
+  std::vector<char> need(p_, 0);
+  for (const auto& S : sets_)
+    if (S.size() != 2)
+      for (int v : S)
+        if (v >= 0 && v < p_) need[v] = 1;
+  std::vector<int> cols;
+  for (int v = 0; v < p_; ++v)
+    if (need[v]) cols.push_back(v);
+  std::string err;
+  std::mutex err_mu;
+  parallel_for(cols.size(), [&](size_t i) {
+    try {
+      cache_->univariate(cols[i]);
     } catch (const std::exception& e) {
       std::lock_guard<std::mutex> lock(err_mu);
       if (err.empty()) err = e.what();
@@ -344,19 +422,25 @@ void Engine::build_designs() {
   TprsBatch batch;
   if (bivariate.size() >= kDeviceTprsMin) launch_bivariate_on_device(bivariate, &batch);
   // the other designs need no bivariate basis: build them while the device works
+  build_univariate_smooths();
   build_host_designs([](const std::vector<int>& S) { return S.size() != 2; });
   finish_bivariate_on_device(&batch);
   build_host_designs([](const std::vector<int>& S) { return S.size() == 2; });
 }
 
-void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
+void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool defer) {
   const int n = n_;
   // Pass 1: descriptors and arena offsets (no copies).  The arena has a
   // host-filled range [0, total) and, behind it, a device-filled range for the
   // geometry the device builds (offsets relative to the range while counting,
   // made absolute below).  The host range also holds the table of smooth
   // bases and penalties the geometry kernels read.
-  std::vector<DesignDev> ddesc(designs_.size());
+  // A design still null is a bivariate one whose basis the device is still
+  // building: it gets its arena slots now (every bivariate design has
+  // q = kTprsK and one penalty of rank kTprsK - 3) and the rest in pack_late.
+  std::vector<DesignDev>& ddesc = ddesc_;
+  ddesc.assign(designs_.size(), DesignDev());
+  pending_.clear();
   std::vector<size_t> geom_designs, single_designs;
   size_t total = 0, dev_total = 0;
   struct SmoothSlot {
@@ -380,9 +464,25 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
     return sl;
   };
   for (size_t d = 0; d < designs_.size(); ++d) {
-    const Design& des = *designs_[d];
     DesignDev& dd = ddesc[d];
     std::memset(&dd, 0, sizeof(dd));
+    if (!designs_[d]) {
+      if (sets_[d].size() != 2) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "design set-up incomplete");
+      dd.kind = 1;
+      dd.q = kTprsK;
+      dd.m = 1;
+      dd.basis = static_cast<int64_t>(dev_total);
+      dev_total += static_cast<size_t>(n) * kTprsK;
+      dd.spec = static_cast<int64_t>(dev_total);
+      dev_total += kTprsK;
+      dd.off[0] = 1;
+      dd.dim[0] = kTprsK - 1;
+      dd.rank[0] = kTprsK - 3;
+      dd.rsum = kTprsK - 3;
+      pending_.push_back(d);
+      continue;
+    }
+    const Design& des = *designs_[d];
     dd.q = des.q;
     dd.m = des.m;
     if (des.m == 1) {
@@ -451,6 +551,10 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
     ddesc[d].basis += static_cast<int64_t>(dev_base);
     ddesc[d].spec += static_cast<int64_t>(dev_base);
   }
+  for (size_t d : pending_) {
+    ddesc[d].basis += static_cast<int64_t>(dev_base);
+    ddesc[d].spec += static_cast<int64_t>(dev_base);
+  }
   // Pass 2: every design copies its host-built part into the pinned staging
   // buffer (threads over designs), then one DMA to the device arena.
   double* host = pinned_arena(total);
@@ -467,6 +571,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
           continue;
         }
         const size_t d = item;
+        if (!designs_[d]) continue;  // pending: nothing on the host yet
         const Design& des = *designs_[d];
         const DesignDev& dd = ddesc[d];
         if (dd.kind == 1) {
@@ -587,38 +692,39 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
   if (total > 0)
     cuda_check(cudaMemcpyAsync(arena, host, total * sizeof(double), cudaMemcpyHostToDevice, stream_), "upload arena");
   h2d_bytes_ += static_cast<double>(total * sizeof(double));
-  int* gstatus_dev = nullptr;
-  if (!gjobs.empty() || !sjobs.empty()) gstatus_dev = d_geom_status_.ensure(gjobs.size() + sjobs.size());
+  int* gstatus_dev = d_geom_status_.ensure(gjobs.size() + sjobs.size() + pending_.size());
+  geom_status_used_ = gjobs.size() + sjobs.size();
+  geom_status_checked_ = 0;
   if (!gjobs.empty()) {
-    h2d_bytes_ += upload(d_geom_jobs_, gjobs, stream_);
+    h2d_bytes_ += stage_upload(d_geom_jobs_, gjobs);
     cuda_check(launch_additive_geometry(arena, n, d_geom_jobs_.get(), static_cast<int>(gjobs.size()), geom_max_q, arena,
                                         gstatus_dev, stream_),
                "additive geometry");
   }
   if (!sjobs.empty()) {
-    h2d_bytes_ += upload(d_single_geom_jobs_, sjobs, stream_);
+    h2d_bytes_ += stage_upload(d_single_geom_jobs_, sjobs);
     cuda_check(launch_single_geometry(n, d_single_geom_jobs_.get(), static_cast<int>(sjobs.size()), arena,
                                       gstatus_dev + gjobs.size(), stream_),
                "single-penalty geometry");
   }
-  h2d_bytes_ += upload(d_designs_, ddesc, stream_);
-  h2d_bytes_ += upload(d_single_jobs_, single_jobs_, stream_);
-  h2d_bytes_ += upload(d_multi_jobs_, multi_jobs_, stream_);
-  h2d_bytes_ += upload(d_multi_small_, multi_small_, stream_);
-  h2d_bytes_ += upload(d_multi_large_, multi_large_, stream_);
-  h2d_bytes_ += upload(d_multi_huge_, multi_huge_, stream_);
+  h2d_bytes_ += stage_upload(d_designs_, ddesc);
+  h2d_bytes_ += stage_upload(d_single_jobs_, single_jobs_);
+  h2d_bytes_ += stage_upload(d_multi_jobs_, multi_jobs_);
+  h2d_bytes_ += stage_upload(d_multi_small_, multi_small_);
+  h2d_bytes_ += stage_upload(d_multi_large_, multi_large_);
+  h2d_bytes_ += stage_upload(d_multi_huge_, multi_huge_);
   if (!multi_small_.empty()) {
     d_fit_states_.ensure(multi_jobs_.size());
     d_defer_list_.ensure(multi_small_.size());
     d_defer_count_.ensure(1);
   }
   if (!multi_huge_.empty()) d_fit_ws_.ensure(multi_workspace_doubles(2, static_cast<int>(multi_huge_.size())));
-  h2d_bytes_ += upload(d_direct_cols_, direct_cols_, stream_);
-  h2d_bytes_ += upload(d_direct_slots_, direct_slots_, stream_);
-  h2d_bytes_ += upload(d_pairs_, pairs_, stream_);
+  h2d_bytes_ += stage_upload(d_direct_cols_, direct_cols_);
+  h2d_bytes_ += stage_upload(d_direct_slots_, direct_slots_);
+  h2d_bytes_ += stage_upload(d_pairs_, pairs_);
   std::vector<int> ident(ncomp);
   for (size_t c = 0; c < ncomp; ++c) ident[c] = static_cast<int>(c);
-  h2d_bytes_ += upload(d_comp_cols_, ident, stream_);
+  h2d_bytes_ += stage_upload(d_comp_cols_, ident);
   collected_ = false;
   d_single_res_.ensure(single_jobs_.size());
   d_multi_res_.ensure(multi_jobs_.size());
@@ -656,23 +762,82 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream) {
       h2d_bytes_ += upload(d_perms_, perms, stream_);
     }
   }
-  cuda_check(cudaStreamSynchronize(stream_), "prepare upload");
-  if (gstatus_dev) {
-    std::vector<int> gstatus(gjobs.size() + sjobs.size());
-    cuda_check(cudaMemcpy(gstatus.data(), gstatus_dev, gstatus.size() * sizeof(int), cudaMemcpyDeviceToHost),
-               "download");
-    for (int st : gstatus) {
-      if (st == 1) throw Error(FKPC_STATUS_RANK, "design set-up failed: design matrix is rank deficient");
-      if (st != 0) throw Error(FKPC_STATUS_NUMERIC, "design set-up failed: penalty eigen-decomposition did not converge");
-    }
+  if (!defer) {
+    cuda_check(cudaStreamSynchronize(stream_), "prepare upload");
+    check_geometry();
   }
   upload_ms_ = ms_since(t0);
+}
+
+void Engine::check_geometry() {
+  if (geom_status_used_ <= geom_status_checked_) return;
+  std::vector<int> gstatus(geom_status_used_);
+  cuda_check(cudaMemcpy(gstatus.data(), d_geom_status_.get(), gstatus.size() * sizeof(int), cudaMemcpyDeviceToHost),
+             "download");
+  geom_status_checked_ = geom_status_used_;
+  for (int st : gstatus) {
+    if (st == 1) throw Error(FKPC_STATUS_RANK, "design set-up failed: design matrix is rank deficient");
+    if (st != 0) throw Error(FKPC_STATUS_NUMERIC, "design set-up failed: penalty eigen-decomposition did not converge");
+  }
+}
+
+void Engine::pack_late() {
+  if (pending_.empty()) return;
+  const int n = n_;
+  std::vector<double> late;  // penalties, and the bases a host fallback built
+  std::vector<int64_t> xoff(pending_.size(), -1), poff(pending_.size(), -1);
+  for (size_t g = 0; g < pending_.size(); ++g) {
+    const size_t d = pending_[g];
+    const Design& des = *designs_[d];
+    if (des.m != 1 || des.q != kTprsK || !des.device_geometry || des.parts.empty())
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "bivariate design of an unexpected shape");
+    DesignDev& dd = ddesc_[d];
+    dd.log_sp0[0] = des.initial_log_sp[0];
+    dd.off[0] = des.offsets[0];
+    dd.dim[0] = des.dims[0];
+    dd.rank[0] = des.ranks[0];
+    dd.rsum = des.ranks[0];
+    const Smooth& sm = *des.parts[0];
+    if (!sm.dev_x) {
+      xoff[g] = static_cast<int64_t>(late.size());
+      late.insert(late.end(), sm.X.begin(), sm.X.end());
+    }
+    poff[g] = static_cast<int64_t>(late.size());
+    late.insert(late.end(), sm.S.begin(), sm.S.end());
+  }
+  h2d_bytes_ += stage_upload(d_late_table_, late);
+  const double* table = d_late_table_.get();
+  std::vector<SingleGeomJob> jobs(pending_.size());
+  for (size_t g = 0; g < pending_.size(); ++g) {
+    const size_t d = pending_[g];
+    const Design& des = *designs_[d];
+    SingleGeomJob& job = jobs[g];
+    std::memset(&job, 0, sizeof(job));
+    job.basis = ddesc_[d].basis;
+    job.spec = ddesc_[d].spec;
+    job.src = des.parts[0]->dev_x ? des.parts[0]->dev_x : table + xoff[g];
+    job.pen = table + poff[g];
+    job.q = des.q;
+    job.rank = des.ranks[0];
+  }
+  h2d_bytes_ += stage_upload(d_late_geom_jobs_, jobs);
+  // the descriptor array again, now complete: queued behind the multi-penalty
+  // fits, which read the additive descriptors
+  h2d_bytes_ += stage_upload(d_designs_, ddesc_);
+  cuda_check(launch_single_geometry(n, d_late_geom_jobs_.get(), static_cast<int>(jobs.size()), d_arena_.get(),
+                                    d_geom_status_.get() + geom_status_used_, stream_),
+             "single-penalty geometry");
+  geom_status_used_ += jobs.size();
+  pending_.clear();
 }
 
 void Engine::prepare(const std::vector<Test>& tests, const fkpc_options& opt, RStream* rstream) {
   if (n_ == 0) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "no data loaded");
   graph_timed_ = false;
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  cuda_check(cudaStreamSynchronize(stream_), "prepare");
+  stage_reset();
+  d2h_bytes_ = 0.0;
   opt_ = opt;
   stats_enabled_ = true;
   release_graph();
@@ -683,25 +848,60 @@ void Engine::prepare(const std::vector<Test>& tests, const fkpc_options& opt, RS
   pack_and_upload(opt, rstream);
 }
 
+void Engine::run_batch(const std::vector<Test>& tests, const fkpc_options& opt, RStream* rstream) {
+  if (n_ == 0) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "no data loaded");
+  graph_timed_ = false;
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  cuda_check(cudaStreamSynchronize(stream_), "batch");
+  stage_reset();
+  d2h_bytes_ = 0.0;
+  opt_ = opt;
+  stats_enabled_ = true;
+  release_graph();
+  try {
+    auto t0 = std::chrono::steady_clock::now();
+    plan_components(tests);
+    designs_.assign(sets_.size(), nullptr);
+    std::vector<std::vector<int>> bivariate;
+    for (const auto& S : sets_)
+      if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
+    TprsBatch batch;
+    if (!bivariate.empty()) launch_bivariate_on_device(bivariate, &batch);
+    build_univariate_smooths();
+    build_host_designs([this](const std::vector<int>& S) { return S.size() != 2 || cache_->has_design(S); });
+    double host_ms = ms_since(t0);
+    pack_and_upload(opt, rstream, true);  // queued behind the thin-plate kernels
+    double up_ms = upload_ms_;
+    cuda_check(configure_fit_kernels(), "kernel attributes");
+    cuda_check(configure_stat_kernels(n_), "kernel attributes");
+    launches_ = 0;
+    cuda_check(cudaEventRecord(ev_[0], stream_), "event");
+    enqueue_multi();
+    auto t1 = std::chrono::steady_clock::now();
+    finish_bivariate_on_device(&batch);
+    build_host_designs([](const std::vector<int>&) { return true; });
+    host_ms += ms_since(t1);
+    auto t2 = std::chrono::steady_clock::now();
+    pack_late();
+    up_ms += ms_since(t2);
+    enqueue_rest();
+    setup_ms_ = host_ms;
+    upload_ms_ = up_ms;
+  } catch (...) {
+    cudaStreamSynchronize(stream_);  // nothing queued may outlive the call's staging
+    throw;
+  }
+}
+
 void Engine::enqueue() {
-  const int n = n_;
-  const int ncomp = static_cast<int>(comps_.size());
-  const int npairs = static_cast<int>(pairs_.size());
   launches_ = 0;
   cuda_check(cudaEventRecord(ev_[0], stream_), "event");
-  if (!direct_cols_.empty()) {
-    dim3 grid((n + 255) / 256, static_cast<unsigned>(direct_cols_.size()));
-    gather_columns_kernel<<<grid, 256, 0, stream_>>>(d_data_.get(), n, d_direct_cols_.get(), d_direct_slots_.get(),
-                                                      static_cast<int>(direct_cols_.size()), d_resid_.get());
-    cuda_check(cudaGetLastError(), "gather columns");
-    ++launches_;
-  }
-  if (!single_jobs_.empty()) {
-    cuda_check(launch_fit_single(d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_single_jobs_.get(),
-                                 static_cast<int>(single_jobs_.size()), d_resid_.get(), d_single_res_.get(), stream_),
-               "fit single");
-    ++launches_;
-  }
+  enqueue_multi();
+  enqueue_rest();
+}
+
+void Engine::enqueue_multi() {
+  const int n = n_;
   if (!multi_small_.empty()) {
     cuda_check(launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                 d_multi_small_.get(), static_cast<int>(multi_small_.size()), d_resid_.get(),
@@ -722,6 +922,25 @@ void Engine::enqueue() {
                                 d_multi_huge_.get(), static_cast<int>(multi_huge_.size()), d_resid_.get(),
                                 d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get()),
                "fit multi");
+    ++launches_;
+  }
+}
+
+void Engine::enqueue_rest() {
+  const int n = n_;
+  const int ncomp = static_cast<int>(comps_.size());
+  const int npairs = static_cast<int>(pairs_.size());
+  if (!direct_cols_.empty()) {
+    dim3 grid((n + 255) / 256, static_cast<unsigned>(direct_cols_.size()));
+    gather_columns_kernel<<<grid, 256, 0, stream_>>>(d_data_.get(), n, d_direct_cols_.get(), d_direct_slots_.get(),
+                                                      static_cast<int>(direct_cols_.size()), d_resid_.get());
+    cuda_check(cudaGetLastError(), "gather columns");
+    ++launches_;
+  }
+  if (!single_jobs_.empty()) {
+    cuda_check(launch_fit_single(d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_single_jobs_.get(),
+                                 static_cast<int>(single_jobs_.size()), d_resid_.get(), d_single_res_.get(), stream_),
+               "fit single");
     ++launches_;
   }
   cuda_check(cudaEventRecord(ev_[1], stream_), "event");
@@ -829,6 +1048,7 @@ void Engine::execute() {
 void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
   auto t0 = std::chrono::steady_clock::now();
   cuda_check(cudaStreamSynchronize(stream_), "batch execution");
+  check_geometry();
   std::vector<FitResult> sres(single_jobs_.size()), mres(multi_jobs_.size());
   if (!sres.empty())
     cuda_check(cudaMemcpy(sres.data(), d_single_res_.get(), sres.size() * sizeof(FitResult), cudaMemcpyDeviceToHost), "download");
@@ -843,7 +1063,7 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
                                           : (r.status == kStatusNotConverged ? FKPC_STATUS_NOT_CONVERGED : FKPC_STATUS_NUMERIC),
                  s);
   };
-  d2h_bytes_ = static_cast<double>((sres.size() + mres.size()) * sizeof(FitResult));
+  d2h_bytes_ += static_cast<double>((sres.size() + mres.size()) * sizeof(FitResult));
   account_flops(sres, mres);
   collected_ = true;
   for (size_t i = 0; i < sres.size(); ++i)
@@ -1197,6 +1417,9 @@ void Engine::regress(const std::vector<int>& targets, const std::vector<std::vec
   opt.selection = selection;
   opt_ = opt;
   release_graph();
+  cuda_check(cudaStreamSynchronize(stream_), "set-up");
+  stage_reset();
+  d2h_bytes_ = 0.0;
   auto t0 = std::chrono::steady_clock::now();
   plan_components(tests);
   build_designs();
@@ -1253,6 +1476,9 @@ void Engine::adjoint(int target, const std::vector<int>& S, int count, const dou
   fkpc_default_options(&opt);
   opt_ = opt;
   release_graph();
+  cuda_check(cudaStreamSynchronize(stream_), "set-up");
+  stage_reset();
+  d2h_bytes_ = 0.0;
   auto t0 = std::chrono::steady_clock::now();
   plan_components({t});
   build_designs();

@@ -79,6 +79,11 @@ class Engine {
 
   // Batched form: plan, set-up, pack and upload one batch of tests.
   void prepare(const std::vector<Test>& tests, const fkpc_options& opt, RStream* stream);
+  // One-shot batched form (prepare + execute without a graph): the device
+  // work that needs no bivariate basis -- the additive geometry and the
+  // multi-penalty fits -- is queued right behind the bivariate thin-plate
+  // kernels, while the host finishes those bases; collect() follows.
+  void run_batch(const std::vector<Test>& tests, const fkpc_options& opt, RStream* stream);
   // Enqueue the device work of the prepared batch (CUDA graph replay).
   void execute();
   // Wait, copy results back and validate statuses.
@@ -109,6 +114,20 @@ class Engine {
   void enqueue_plain_test(int t);  // one test's launch set (plain form)
   double execute_plain_timed(int repeats);
   void build_designs();
+  void build_univariate_smooths();
+  // copies made while earlier stream work may still run go through page-locked
+  // staging: a copy from pageable memory would first wait for the whole stream.
+  // A bump allocator over a persistent buffer; a full buffer is retired (kept
+  // until the next reset) and replaced by a larger one.  stage_reset() only
+  // when nothing on the stream reads staged memory.
+  void stage_reset();
+  void* stage_alloc(size_t bytes);
+  template <class T>
+  double stage_upload(DevBuf<T>& buf, const std::vector<T>& host);
+  void enqueue_multi();  // the multi-penalty fit classes
+  void enqueue_rest();   // direct columns, single-penalty fits, statistics
+  void pack_late();      // pending bivariate designs: descriptors, geometry
+  void check_geometry();  // statuses of the geometry kernels (after a synchronisation)
   // one level's bivariate thin-plate Lanczos on the device, in flight
   struct TprsBatch {
     std::vector<std::vector<int>> sets;
@@ -124,7 +143,8 @@ class Engine {
   void finish_bivariate_on_device(TprsBatch* batch);
   template <class Pick>
   void build_host_designs(Pick pick);
-  void pack_and_upload(const fkpc_options& opt, RStream* stream);
+  // defer: leave the stream running (the geometry statuses are checked by collect)
+  void pack_and_upload(const fkpc_options& opt, RStream* stream, bool defer = false);
   void enqueue();  // the launch sequence
   void release_graph();
   double* pinned_arena(size_t count);  // persistent page-locked staging buffer of the design arena
@@ -185,7 +205,17 @@ class Engine {
   size_t h_arena_cap_ = 0;
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;
-  cudaEvent_t ev_[6] = {};
+  cudaEvent_t ev_[7] = {};  // [6]: the bivariate thin-plate results have landed
+  char* h_stage_ = nullptr;
+  size_t h_stage_cap_ = 0, h_stage_used_ = 0;
+  std::vector<char*> h_stage_retired_;
+  // the packed descriptors, designs still pending their bivariate basis, and
+  // the geometry statuses written on the device but not yet checked
+  std::vector<DesignDev> ddesc_;
+  std::vector<size_t> pending_;
+  size_t geom_status_used_ = 0, geom_status_checked_ = 0;
+  DevBuf<double> d_late_table_;
+  DevBuf<SingleGeomJob> d_late_geom_jobs_;
   int launches_ = 0;
   double setup_ms_ = 0.0, upload_ms_ = 0.0;
   int guard_count_host_ = 0;

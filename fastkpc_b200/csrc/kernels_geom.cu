@@ -171,8 +171,8 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const d
 // Single-penalty designs (|S| <= 2): X = [1 | B] with one penalty S on the
 // smooth's columns (fastkpc/src/full_cuda_ci_one_call.cpp:1869-1947 builds
 // this geometry from the Gram Cholesky; here from the QR).  X = Q R, the
-// whitened penalty R^-T S R^-1 = V diag(e) V' (cyclic Jacobi on warp 0, at
-// most 100 sweeps), and the fit kernels' inputs QW = Q V and the spectrum e
+// whitened penalty R^-T S R^-1 = V diag(e) V' (parallel Jacobi, at most 100
+// sweeps), and the fit kernels' inputs QW = Q V and the spectrum e
 // (descending; zero beyond the penalty rank).  status[d]: 1 rank deficient,
 // 2 Jacobi did not converge.
 __global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(int n, const SingleGeomJob* __restrict__ jobs,
@@ -186,7 +186,9 @@ __global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(int n, co
   __shared__ double vks[Q], betas[Q], red[kGeomWarps];
   __shared__ int order[Q];
   __shared__ int jacobi_ok;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  __shared__ int rot_p[Q / 2 + 1], rot_q[Q / 2 + 1];
+  __shared__ double rot_c[Q / 2 + 1], rot_s[Q / 2 + 1];
+  const int tid = threadIdx.x;
   for (int d = blockIdx.x; d < count; d += gridDim.x) {
     const SingleGeomJob& job = jobs[d];
     const int q = job.q, dim = q - 1;
@@ -246,70 +248,102 @@ __global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(int n, co
       }
     }
     __syncthreads();
-    if (warp == 0) {
-      for (int c = 0; c < q; ++c)
-        if (lane < q) Vs[lane + LA * c] = lane == c ? 1.0 : 0.0;
-      __syncwarp();
-      bool conv = false;
-      for (int sweep = 0; sweep < 100; ++sweep) {
-        double off = 0.0, diag = 0.0;
-        if (lane < q)
-          for (int j = 0; j < q; ++j) {
-            const double v = A[lane + LA * j];
-            if (lane == j) diag += v * v;
-            else off += v * v;
+    // Jacobi with the round-robin (circle) ordering: in each round the
+    // index pairs are disjoint, so their rotations commute and are applied
+    // together -- angles from the round's A, then all column updates (A J,
+    // V J), then all row updates (J' A).  A sweep is Qe - 1 rounds over
+    // Qe = q rounded up to even (the odd index out sits out the round).
+    for (int idx = tid; idx < q * q; idx += blockDim.x) Vs[idx % q + LA * (idx / q)] = idx % q == idx / q ? 1.0 : 0.0;
+    __syncthreads();
+    const int qe = q + (q & 1);
+    const int npair = qe / 2;
+    bool conv = false;
+    for (int sweep = 0; sweep < 100 && !conv; ++sweep) {
+      double off = 0.0, diag = 0.0;
+      for (int idx = tid; idx < q * q; idx += blockDim.x) {
+        const int r = idx % q, c = idx / q;
+        const double v = A[r + LA * c];
+        if (r == c) diag += v * v;
+        else off += v * v;
+      }
+      off = block_sum_g(off, red);
+      __syncthreads();
+      diag = block_sum_g(diag, red);
+      if (off <= 1e-32 * diag || off == 0.0) {
+        conv = true;
+        break;
+      }
+      for (int round = 0; round < qe - 1; ++round) {
+        if (tid < npair) {
+          int a, b;
+          if (tid == 0) {
+            a = round;
+            b = qe - 1;
+          } else {
+            a = (round + tid) % (qe - 1);
+            b = (round - tid + qe - 1) % (qe - 1);
           }
-        off = warp_sum_g(off);
-        diag = warp_sum_g(diag);
-        if (off <= 1e-32 * diag || off == 0.0) {
-          conv = true;
-          break;
-        }
-        for (int pp = 0; pp < q - 1; ++pp) {
-          for (int qq = pp + 1; qq < q; ++qq) {
+          const int pp = a < b ? a : b, qq = a < b ? b : a;
+          double cs = 1.0, sn = 0.0;
+          if (qq < q) {
             const double apq = A[pp + LA * qq];
-            if (apq == 0.0) continue;  // the same value in every lane
-            const double app = A[pp + LA * pp], aqq = A[qq + LA * qq];
-            const double theta = (aqq - app) / (2.0 * apq);
-            const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-            const double cs = 1.0 / sqrt(t * t + 1.0);
-            const double sn = t * cs;
-            __syncwarp();
-            if (lane < q) {
-              const double akp = A[lane + LA * pp], akq = A[lane + LA * qq];
-              A[lane + LA * pp] = cs * akp - sn * akq;
-              A[lane + LA * qq] = sn * akp + cs * akq;
+            if (apq != 0.0) {
+              const double app = A[pp + LA * pp], aqq = A[qq + LA * qq];
+              const double theta = (aqq - app) / (2.0 * apq);
+              const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+              cs = 1.0 / sqrt(t * t + 1.0);
+              sn = t * cs;
             }
-            __syncwarp();
-            if (lane < q) {
-              const double apk = A[pp + LA * lane], aqk = A[qq + LA * lane];
-              A[pp + LA * lane] = cs * apk - sn * aqk;
-              A[qq + LA * lane] = sn * apk + cs * aqk;
-              const double vkp = Vs[lane + LA * pp], vkq = Vs[lane + LA * qq];
-              Vs[lane + LA * pp] = cs * vkp - sn * vkq;
-              Vs[lane + LA * qq] = sn * vkp + cs * vkq;
-            }
-            __syncwarp();
-            if (lane == 0) {
-              A[pp + LA * qq] = 0.0;
-              A[qq + LA * pp] = 0.0;
-            }
-            __syncwarp();
           }
+          rot_p[tid] = pp;
+          rot_q[tid] = qq;
+          rot_c[tid] = cs;
+          rot_s[tid] = sn;
         }
-      }
-      // descending eigenvalues; equal values: the higher index first
-      if (lane < q) {
-        const double li = A[lane + LA * lane];
-        int pos = 0;
-        for (int j = 0; j < q; ++j) {
-          const double lj = A[j + LA * j];
-          pos += (lj > li || (lj == li && j > lane)) ? 1 : 0;
+        __syncthreads();
+        // columns: A J and V J (pair i, row k)
+        for (int idx = tid; idx < npair * q; idx += blockDim.x) {
+          const int i = idx / q, k = idx % q;
+          const int pp = rot_p[i], qq = rot_q[i];
+          if (qq >= q || rot_s[i] == 0.0) continue;
+          const double cs = rot_c[i], sn = rot_s[i];
+          const double akp = A[k + LA * pp], akq = A[k + LA * qq];
+          A[k + LA * pp] = cs * akp - sn * akq;
+          A[k + LA * qq] = sn * akp + cs * akq;
+          const double vkp = Vs[k + LA * pp], vkq = Vs[k + LA * qq];
+          Vs[k + LA * pp] = cs * vkp - sn * vkq;
+          Vs[k + LA * qq] = sn * vkp + cs * vkq;
         }
-        order[pos] = lane;
+        __syncthreads();
+        // rows: J' A (pair i, column k)
+        for (int idx = tid; idx < npair * q; idx += blockDim.x) {
+          const int i = idx / q, k = idx % q;
+          const int pp = rot_p[i], qq = rot_q[i];
+          if (qq >= q || rot_s[i] == 0.0) continue;
+          const double cs = rot_c[i], sn = rot_s[i];
+          const double apk = A[pp + LA * k], aqk = A[qq + LA * k];
+          A[pp + LA * k] = cs * apk - sn * aqk;
+          A[qq + LA * k] = sn * apk + cs * aqk;
+        }
+        __syncthreads();
+        if (tid < npair && rot_q[tid] < q) {  // as the serial sweep: a_pq is zero after its rotation
+          A[rot_p[tid] + LA * rot_q[tid]] = 0.0;
+          A[rot_q[tid] + LA * rot_p[tid]] = 0.0;
+        }
+        __syncthreads();
       }
-      if (lane == 0) jacobi_ok = conv ? 1 : 0;
     }
+    // descending eigenvalues; equal values: the higher index first
+    if (tid < q) {
+      const double li = A[tid + LA * tid];
+      int pos = 0;
+      for (int j = 0; j < q; ++j) {
+        const double lj = A[j + LA * j];
+        pos += (lj > li || (lj == li && j > tid)) ? 1 : 0;
+      }
+      order[pos] = tid;
+    }
+    if (tid == 0) jacobi_ok = conv ? 1 : 0;
     __syncthreads();
     if (!jacobi_ok) {
       if (tid == 0) status[d] = 2;

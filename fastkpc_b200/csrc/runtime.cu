@@ -50,7 +50,7 @@ double upload(DevBuf<T>& buf, const std::vector<T>& host, cudaStream_t s) {
 
 constexpr double kGuardLower = 0.05;
 constexpr double kGuardUpper = 0.15;
-constexpr int kLegacyCtas = 148;  // one per SM: the Lanczos bases of the active components stay in L2
+constexpr int kLegacyCtas = 2 * 148;  // two per SM: one component's latency-bound step hides the other's
 
 }  // namespace
 

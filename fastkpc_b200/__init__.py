@@ -12,6 +12,7 @@ fallback: importing works without a GPU, but every compute call raises
 the shared library has not been built (``python -m fastkpc_b200.build``).
 """
 import ctypes
+import itertools
 import math
 import os
 
@@ -311,14 +312,16 @@ def _deleted(adj, i, j):
 
 
 def _tests_arrays(tests):
-    xs = np.array([t[0] for t in tests], dtype=np.int32)
-    ys = np.array([t[1] for t in tests], dtype=np.int32)
-    offs = np.zeros(len(tests) + 1, dtype=np.int32)
-    vals = []
-    for k, t in enumerate(tests):
-        vals.extend(int(v) for v in t[2])
-        offs[k + 1] = len(vals)
-    return xs, ys, offs, np.array(vals if vals else [0], dtype=np.int32)
+    count = len(tests)
+    xs = np.fromiter((t[0] for t in tests), dtype=np.int32, count=count)
+    ys = np.fromiter((t[1] for t in tests), dtype=np.int32, count=count)
+    offs = np.zeros(count + 1, dtype=np.int32)
+    np.cumsum(np.fromiter((len(t[2]) for t in tests), dtype=np.int32, count=count), out=offs[1:])
+    total = int(offs[-1])
+    if total == 0:
+        return xs, ys, offs, np.zeros(1, dtype=np.int32)
+    vals = np.fromiter(itertools.chain.from_iterable(t[2] for t in tests), dtype=np.int32, count=total)
+    return xs, ys, offs, vals
 
 
 _RECORD_DTYPE = None

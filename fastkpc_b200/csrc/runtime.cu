@@ -19,6 +19,7 @@
 #include <cstring>
 #include <map>
 #include <thread>
+#include <unordered_map>
 
 namespace fkpc {
 
@@ -154,6 +155,8 @@ void Engine::load(const double* data, int n, int p) {
              "upload data");
   cuda_check(cudaStreamSynchronize(stream_), "upload data");
   cache_.reset(new DesignCache(host_data_.data(), n, p));
+  // the cache's bivariate bases go; their device chunks are kept for reuse
+  for (auto& chunk : smooth_store_) smooth_spare_.push_back(std::move(chunk));
   smooth_store_.clear();
   release_graph();
 }
@@ -163,11 +166,20 @@ void Engine::plan_components(const std::vector<Test>& tests) {
   sets_.clear();
   comps_.clear();
   pairs_.clear();
-  std::map<std::vector<int>, int> set_index;
-  std::map<std::pair<int, int>, int> comp_index;  // (target, set or -1)
+  struct SetHash {
+    size_t operator()(const std::vector<int>& v) const {
+      uint64_t h = 1469598103934665603ull;  // FNV-1a over the indices
+      for (int x : v) h = (h ^ static_cast<uint32_t>(x)) * 1099511628211ull;
+      return static_cast<size_t>(h);
+    }
+  };
+  std::unordered_map<std::vector<int>, int, SetHash> set_index;
+  std::unordered_map<uint64_t, int> comp_index;  // (target, set or -1)
+  set_index.reserve(tests.size());
+  comp_index.reserve(2 * tests.size());
   const bool share = opt_.mode != FKPC_MODE_PLAIN;  // the plain form fits every test on its own
   auto component = [&](int target, int set) {
-    auto key = std::make_pair(target, set);
+    const uint64_t key = (static_cast<uint64_t>(static_cast<uint32_t>(target)) << 32) | static_cast<uint32_t>(set);
     auto it = comp_index.find(key);
     if (share && it != comp_index.end()) return it->second;
     const int id = static_cast<int>(comps_.size());
@@ -185,7 +197,7 @@ void Engine::plan_components(const std::vector<Test>& tests) {
         throw Error(FKPC_STATUS_INVALID_ARGUMENT, "conditioning set must hold distinct variables other than x and y");
     }
     if (static_cast<int>(ts.S.size()) > kMaxPenalties)
-      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "conditioning sets larger than 8 are not supported by this build");
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "conditioning sets larger than 12 are not supported by this build");
     int set = -1;
     if (!ts.S.empty()) {
       auto it = set_index.find(ts.S);
@@ -272,17 +284,16 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
   for (size_t i = 0; i < count; ++i)
     if (ok[i]) batch->idx.push_back(i);
   if (batch->idx.empty()) return;
-  std::vector<double> u;
+  // offsets, then the locations and row mappings written straight into
+  // page-locked staging by the host threads
   std::vector<int64_t> uoff, voff, roff;
-  std::vector<int> map;
   batch->nus.clear();
   int nu_max = 0;
-  int64_t vtotal = 0, utotal = 0;
+  int64_t vtotal = 0, utotal = 0, ltotal = 0;
   for (size_t i : batch->idx) {
     const TprsPrep& pr = batch->preps[i];
-    uoff.push_back(static_cast<int64_t>(u.size()));
-    u.insert(u.end(), pr.u.begin(), pr.u.end());
-    map.insert(map.end(), pr.mapping.begin(), pr.mapping.end());
+    uoff.push_back(ltotal);
+    ltotal += static_cast<int64_t>(pr.u.size());
     batch->nus.push_back(pr.nu);
     voff.push_back(vtotal);
     vtotal += static_cast<int64_t>(pr.nu) * kTprsSteps;
@@ -290,6 +301,13 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
     utotal += static_cast<int64_t>(pr.nu) * kTprsK;
     nu_max = std::max(nu_max, pr.nu);
   }
+  double* hu = static_cast<double*>(stage_alloc(sizeof(double) * static_cast<size_t>(ltotal)));
+  int* hmap = static_cast<int*>(stage_alloc(sizeof(int) * batch->idx.size() * static_cast<size_t>(n)));
+  parallel_for(batch->idx.size(), [&](size_t c) {
+    const TprsPrep& pr = batch->preps[batch->idx[c]];
+    std::memcpy(hu + uoff[c], pr.u.data(), pr.u.size() * sizeof(double));
+    std::memcpy(hmap + c * static_cast<size_t>(n), pr.mapping.data(), static_cast<size_t>(n) * sizeof(int));
+  });
   const int cnt = static_cast<int>(batch->idx.size());
   const int ctas = std::min(cnt, 2 * 148);  // two designs per SM (memory-bound matvec)
   const size_t nab = static_cast<size_t>(2) * cnt * kTprsSteps;
@@ -301,12 +319,16 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
   batch->S = host;
   batch->colsq = host + ns;
   batch->status = reinterpret_cast<int*>(host + ns + ncs);
-  stage_upload(d_tprs_u_, u);
+  cuda_check(cudaMemcpyAsync(d_tprs_u_.ensure(static_cast<size_t>(ltotal)), hu, sizeof(double) * ltotal,
+                             cudaMemcpyHostToDevice, stream_),
+             "upload");
+  cuda_check(cudaMemcpyAsync(d_tprs_map_.ensure(batch->idx.size() * static_cast<size_t>(n)), hmap,
+                             sizeof(int) * batch->idx.size() * n, cudaMemcpyHostToDevice, stream_),
+             "upload");
   stage_upload(d_tprs_uoff_, uoff);
   stage_upload(d_tprs_voff_, voff);
   stage_upload(d_tprs_roff_, roff);
   stage_upload(d_tprs_nus_, batch->nus);
-  stage_upload(d_tprs_map_, map);
   const int64_t ews_stride = tprs_ld(nu_max) * tprs_ld(nu_max);
   double* dV = d_tprs_V_.ensure(static_cast<size_t>(vtotal));
   double* dab = d_tprs_ab_.ensure(nab);
@@ -315,8 +337,18 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
   double* dvals = d_tprs_vals_.ensure(nvals);
   double* dU = d_tprs_U_.ensure(static_cast<size_t>(utotal));
   int* dok = d_tprs_ok_.ensure(cnt);
-  smooth_store_.emplace_back(new DevBuf<double>());
-  double* dX = smooth_store_.back()->ensure(static_cast<size_t>(cnt) * n * kTprsK);
+  // a spare chunk from an earlier cache when one is large enough, else a new one
+  const size_t xneed = static_cast<size_t>(cnt) * n * kTprsK;
+  std::unique_ptr<DevBuf<double>> chunk;
+  for (size_t i = 0; i < smooth_spare_.size(); ++i)
+    if (smooth_spare_[i]->capacity() >= xneed) {
+      chunk = std::move(smooth_spare_[i]);
+      smooth_spare_.erase(smooth_spare_.begin() + static_cast<std::ptrdiff_t>(i));
+      break;
+    }
+  if (!chunk) chunk.reset(new DevBuf<double>());
+  double* dX = chunk->ensure(xneed);
+  smooth_store_.push_back(std::move(chunk));
   batch->X = dX;
   double* dS = d_tprs_S_.ensure(ns);
   double* dcs = d_tprs_colsq_.ensure(ncs);

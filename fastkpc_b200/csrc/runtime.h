@@ -157,7 +157,7 @@ class Engine {
   std::unique_ptr<DesignCache> cache_;
   // device bases of the cache's bivariate smooths (one chunk per level batch);
   // released with the cache
-  std::vector<std::unique_ptr<DevBuf<double>>> smooth_store_;
+  std::vector<std::unique_ptr<DevBuf<double>>> smooth_store_, smooth_spare_;
 
   // batch plan
   fkpc_options opt_{};

@@ -38,7 +38,8 @@ namespace {
 constexpr int kTprsThreads = 256;
 constexpr int kTprsWarps = kTprsThreads / 32;
 constexpr int kTile = 32;
-constexpr int kTileWords = kTile * (kTile + 1);  // one warp's transposing tile (padded rows)
+constexpr int kTileLd = kTile + 2;                // padded row: 16-byte aligned, conflict-free 16-byte reads
+constexpr int kTileWords = kTile * kTileLd;         // one warp's transposing tile
 
 __device__ __forceinline__ double warp_sum_t(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -135,31 +136,37 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
           const double* qJ = q + kTile * J;
           double zc = 0.0;  // lane c: column sum of column 32 J + c over the tiles above the diagonal
           for (int I = 0; I <= J; ++I) {
+            // E is read once per step, far beyond L2: streaming loads, so
+            // that the Lanczos basis the re-orthogonalisation re-reads stays
             double e[kTile];
 #pragma unroll
-            for (int c = 0; c < kTile; ++c) e[c] = Ecol[kTile * I + lane + static_cast<int64_t>(ld) * c];
+            for (int c = 0; c < kTile; ++c) e[c] = __ldcs(Ecol + kTile * I + lane + static_cast<int64_t>(ld) * c);
+            const double2* qJ2 = reinterpret_cast<const double2*>(qJ);
             double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
 #pragma unroll
             for (int c = 0; c < kTile; c += 4) {
-              r0 += e[c] * qJ[c];
-              r1 += e[c + 1] * qJ[c + 1];
-              r2 += e[c + 2] * qJ[c + 2];
-              r3 += e[c + 3] * qJ[c + 3];
+              const double2 qa = qJ2[c / 2], qb = qJ2[c / 2 + 1];
+              r0 += e[c] * qa.x;
+              r1 += e[c + 1] * qa.y;
+              r2 += e[c + 2] * qb.x;
+              r3 += e[c + 3] * qb.y;
             }
             my[kTile * I + lane] += (r0 + r1) + (r2 + r3);
             if (I < J) {
 #pragma unroll
-              for (int c = 0; c < kTile; ++c) tile[c * (kTile + 1) + lane] = e[c];
+              for (int c = 0; c < kTile; ++c) tile[c * kTileLd + lane] = e[c];
               __syncwarp();
-              const double* qI = q + kTile * I;
-              const double* trow = tile + lane * (kTile + 1);
+              const double2* qI2 = reinterpret_cast<const double2*>(q + kTile * I);
+              const double2* trow2 = reinterpret_cast<const double2*>(tile + lane * kTileLd);
               double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
 #pragma unroll
               for (int l = 0; l < kTile; l += 4) {
-                c0 += trow[l] * qI[l];
-                c1 += trow[l + 1] * qI[l + 1];
-                c2 += trow[l + 2] * qI[l + 2];
-                c3 += trow[l + 3] * qI[l + 3];
+                const double2 ta = trow2[l / 2], tb = trow2[l / 2 + 1];
+                const double2 qa = qI2[l / 2], qb = qI2[l / 2 + 1];
+                c0 += ta.x * qa.x;
+                c1 += ta.y * qa.y;
+                c2 += tb.x * qb.x;
+                c3 += tb.y * qb.y;
               }
               zc += (c0 + c1) + (c2 + c3);
               __syncwarp();

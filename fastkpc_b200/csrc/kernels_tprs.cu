@@ -186,13 +186,17 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
       }
       const double a = block_sum_t(part, red);
       const double* vp = j > 0 ? Vd + static_cast<int64_t>(nu) * (j - 1) : nullptr;
+      double before = 0.0;
       for (int i = tid; i < nu; i += blockDim.x) {
         double v = w[i] - a * q[i];
         if (vp) v -= bprev * vp[i];
         w[i] = v;
+        before += v * v;
       }
-      __syncthreads();
-      // full re-orthogonalisation, two passes
+      before = block_sum_t(before, red);
+      // full re-orthogonalisation, classical Gram-Schmidt; a second pass only
+      // when the first removed more than three quarters of |w|^2 (DGKS)
+      double after = before;
       for (int pass = 0; pass < 2; ++pass) {
         for (int b0 = 4 * warp; b0 <= j; b0 += 4 * kTprsWarps) {
           const double* v0 = Vd + static_cast<int64_t>(nu) * b0;
@@ -222,6 +226,7 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
           }
         }
         __syncthreads();
+        double part2 = 0.0;
         for (int i = tid; i < nu; i += blockDim.x) {
           double s0 = w[i], s1 = 0.0, s2 = 0.0, s3 = 0.0;
           int b = 0;
@@ -235,13 +240,15 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
             s3 -= coef[b + 3] * x[3] + coef[b + 7] * x[7];
           }
           for (; b <= j; ++b) s0 -= coef[b] * Vd[i + static_cast<int64_t>(nu) * b];
-          w[i] = (s0 + s1) + (s2 + s3);
+          const double v = (s0 + s1) + (s2 + s3);
+          w[i] = v;
+          part2 += v * v;
         }
-        __syncthreads();
+        after = block_sum_t(part2, red);
+        if (after > 0.25 * before) break;
+        before = after;
       }
-      double nn2 = 0.0;
-      for (int i = tid; i < nu; i += blockDim.x) nn2 += w[i] * w[i];
-      const double bj = sqrt(block_sum_t(nn2, red));
+      const double bj = sqrt(after);
       anorm = fmax(anorm, fabs(a) + bj + bprev);
       if (tid == 0) {
         alpha[static_cast<int64_t>(d) * steps + j] = a;

@@ -82,11 +82,20 @@ static __device__ bool householder_inplace(double* __restrict__ W, int n, int q,
     }
     for (int j = k + 1 + warp; j < q; j += kGeomWarps) {
       double* c = W + static_cast<int64_t>(n) * j;
-      double dot = 0.0;
-      for (int i = k + lane; i < n; i += 32) dot += (i == k ? vk : x[i]) * c[i];
-      dot = warp_sum_g(dot) * beta;
-      for (int i = k + lane; i < n; i += 32) c[i] -= dot * (i == k ? vk : x[i]);
-      if (lane == 0) R[k + static_cast<int64_t>(ldr) * j] = c[k];  // row k is final
+      // v = (vk, x_{k+1}, ...): the pivot row apart, two chains below it
+      double d0 = lane == 0 ? vk * c[k] : 0.0, d1 = 0.0;
+      int i = k + 1 + lane;
+      for (; i + 32 < n; i += 64) {
+        d0 += x[i] * c[i];
+        d1 += x[i + 32] * c[i + 32];
+      }
+      if (i < n) d0 += x[i] * c[i];
+      const double dot = warp_sum_g(d0 + d1) * beta;
+      for (int r = k + 1 + lane; r < n; r += 32) c[r] -= dot * x[r];
+      if (lane == 0) {
+        c[k] -= dot * vk;
+        R[k + static_cast<int64_t>(ldr) * j] = c[k];  // row k is final
+      }
     }
     if (tid == 0) {
       R[k + static_cast<int64_t>(ldr) * k] = alpha;
@@ -103,10 +112,15 @@ static __device__ bool householder_inplace(double* __restrict__ W, int n, int q,
     const double vk = vks[k], beta = betas[k];
     for (int j = k + 1 + warp; j < q; j += kGeomWarps) {
       double* c = W + static_cast<int64_t>(n) * j;
-      double dot = 0.0;
-      for (int i = k + 1 + lane; i < n; i += 32) dot += x[i] * c[i];
-      dot = warp_sum_g(dot) * beta;
-      for (int i = k + 1 + lane; i < n; i += 32) c[i] -= dot * x[i];
+      double d0 = 0.0, d1 = 0.0;
+      int i = k + 1 + lane;
+      for (; i + 32 < n; i += 64) {
+        d0 += x[i] * c[i];
+        d1 += x[i + 32] * c[i + 32];
+      }
+      if (i < n) d0 += x[i] * c[i];
+      const double dot = warp_sum_g(d0 + d1) * beta;
+      for (int r = k + 1 + lane; r < n; r += 32) c[r] -= dot * x[r];
       if (lane == 0) c[k] = -dot * vk;
     }
     __syncthreads();
@@ -144,10 +158,10 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const d
     }
     __syncthreads();
     const int64_t nq = static_cast<int64_t>(n) * q;
-    for (int64_t idx = tid; idx < nq; idx += blockDim.x) {
-      const int r = static_cast<int>(idx % n), c = static_cast<int>(idx / n);
+    for (int c = 0; c < q; ++c) {
       const int64_t s = colsrc[c];
-      W[idx] = s < 0 ? 1.0 : table[s + r];
+      double* wc = W + static_cast<int64_t>(n) * c;
+      for (int r = tid; r < n; r += blockDim.x) wc[r] = s < 0 ? 1.0 : table[s + r];
     }
     for (int idx = tid; idx < q * q; idx += blockDim.x) R[idx] = 0.0;
     __syncthreads();
@@ -196,10 +210,11 @@ __global__ void __launch_bounds__(kGeomThreads) single_geometry_kernel(int n, co
     double* W = in_smem ? wsm : QW;
     const double* B = job.src;
     const double* S = job.pen;
-    const int64_t nq = static_cast<int64_t>(n) * q;
-    for (int64_t idx = tid; idx < nq; idx += blockDim.x) {
-      const int r = static_cast<int>(idx % n), c = static_cast<int>(idx / n);
-      W[idx] = c == 0 ? 1.0 : B[r + static_cast<int64_t>(n) * (c - 1)];
+    for (int r = tid; r < n; r += blockDim.x) W[r] = 1.0;
+    for (int c = 1; c < q; ++c) {
+      const double* bc = B + static_cast<int64_t>(n) * (c - 1);
+      double* wc = W + static_cast<int64_t>(n) * c;
+      for (int r = tid; r < n; r += blockDim.x) wc[r] = bc[r];
     }
     for (int idx = tid; idx < q * q; idx += blockDim.x) {
       Rs[idx] = 0.0;

@@ -346,7 +346,9 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
         const double ei = ee[i], di = dd[i], di1 = dd[i + 1];
         const double f = sn * ei;
         const double b = cs * ei;
-        const double rr = hypot(f, g);
+        // |(f, g)| without hypot's scaling: the tridiagonal's entries are far
+        // from the overflow range here (values of the scaled eta matrices)
+        const double rr = sqrt(f * f + g * g);
         __syncwarp();  // every lane has read d and e before lane 0 writes them
         if (rr == 0.0) {
           if (lane == 0) {
@@ -358,8 +360,9 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
           break;
         }
         if (lane == 0) ee[i + 1] = rr;
-        sn = f / rr;
-        cs = g / rr;
+        const double rinv = 1.0 / rr;
+        sn = f * rinv;
+        cs = g * rinv;
         g = di1 - p;
         r = (di - g) * sn + 2.0 * cs * b;
         p = sn * r;

@@ -323,3 +323,45 @@ def test_one_shot_batch_equals_staged_graph(lib, method):
     # a second one-shot call on the same data reuses the engine's buffers
     again, _ = fk.ci_level_batch(X, triples, ci_method=method)
     assert np.array_equal(again["p_value"], one["p_value"])
+
+
+# Eleven unequally spaced levels.  On an equally spaced grid the eta matrix is
+# symmetric under reversal, half its eigenvectors are antisymmetric, and the
+# sign convention (largest-magnitude entry positive) meets exact ties that
+# rounding decides, differently in any two implementations.
+_LEVELS = np.array([0.0, 1.0, 3.0, 4.5, 7.0, 9.0, 12.0, 15.5, 16.0, 20.0, 23.0])
+
+
+def _discrete_data(n=300, seed=11):
+    """Columns 0 and 1 take 11 values, and their pairs only about 60 distinct
+    locations: the bivariate design on {0, 1} has too few unique locations
+    for the device Lanczos and is built by the host."""
+    rs = np.random.default_rng(seed)
+    X = np.empty((n, 8))
+    a = rs.integers(0, 11, size=n)
+    X[:, 0] = _LEVELS[a]
+    X[:, 1] = _LEVELS[(a + rs.integers(0, 6, size=n)) % 11]
+    for j in range(2, 8):
+        X[:, j] = rs.normal(size=n)
+    X[:, 2] += np.sin(X[:, 0])
+    X[:, 3] += 0.3 * X[:, 1] + np.tanh(X[:, 2])
+    X[:, 6] += np.cos(X[:, 4]) - 0.2 * X[:, 0]
+    X[:, 7] += X[:, 5] ** 2 * 0.3
+    return np.asfortranarray(X)
+
+
+def test_host_built_bivariate_design_in_the_one_shot_batch(lib):
+    X = _discrete_data()
+    pairs = {tuple(int(v) for v in row) for row in X[:, :2]}
+    assert 30 <= len(pairs) <= 80  # between the basis size and the device's step count
+    triples = [(2, 3, [0, 1]), (4, 6, [0, 1]), (2, 5, [0]), (3, 7, [4, 5]), (2, 6, [0, 1, 4]),
+               (6, 7, [0, 4, 5]), (2, 7, []), (3, 6, [1])]
+    one, _ = fk.ci_level_batch(X, triples)
+    cache = skeleton.ResidualCache(X)
+    for k, t in enumerate(triples):
+        p = _oracle_p(cache, t)
+        assert abs(one["p_value"][k] - p) <= 1e-9, (t, one["p_value"][k], p)
+    staged = fk.StagedBatch(X, triples)
+    staged.execute(1)
+    two, _ = staged.collect()
+    assert np.array_equal(one["p_value"], two["p_value"])

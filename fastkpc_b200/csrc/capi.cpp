@@ -236,7 +236,88 @@ void skeleton(const double* data, int n, int p, const fkpc_options& opt, Run* ru
     std::vector<unsigned> fl(plan.size(), 0u);
     std::vector<char> counted(plan.size(), 0);
     auto to_test = [&](const Task& t) { return fkpc::Test{t.x, t.y, t.S}; };
-    if (perm || opt.mode == FKPC_MODE_PLAIN) {
+    if (perm && opt.mode != FKPC_MODE_PLAIN) {
+      if (evaluator) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "the level evaluator serves the batched gamma methods");
+      // Permutation methods draw their permutations from one seeded stream in
+      // pcalg order (x, y, S), and an edge's remaining tests are skipped once
+      // it is deleted.  Speculative windows: the next `window` tests of that
+      // order, as if no edge were deleted, are evaluated as one batch (the
+      // stream consumed test by test in window order).  Results are accepted
+      // in order up to the first test that an accepted deletion skips; the
+      // stream is then reset to its state after the last accepted test, and
+      // the next window starts there.  Outcome and stream use are those of
+      // the one-test-at-a-time order.
+      std::map<std::pair<int, int>, size_t> pos;
+      for (auto& kv : by_edge) pos[kv.first] = 0;
+      auto pick = [&](const std::map<std::pair<int, int>, size_t>& at) {
+        int best = -1;
+        for (auto& kv : by_edge) {
+          const size_t k = at.at(kv.first);
+          if (k >= kv.second.size()) continue;
+          const int cand = kv.second[k];
+          if (best < 0) {
+            best = cand;
+            continue;
+          }
+          const Task& a = plan[cand];
+          const Task& b = plan[best];
+          if (a.x != b.x ? a.x < b.x : (a.y != b.y ? a.y < b.y : a.S < b.S)) best = cand;
+        }
+        return best;
+      };
+      size_t window = 32;
+      std::vector<int> seq;
+      for (;;) {
+        seq.clear();
+        auto at = pos;
+        while (seq.size() < window) {
+          const int b = pick(at);
+          if (b < 0) break;
+          seq.push_back(b);
+          ++at[{plan[b].edge_x, plan[b].edge_y}];
+        }
+        if (seq.empty()) break;
+        std::vector<fkpc::Test> tests;
+        tests.reserve(seq.size());
+        for (int b : seq) tests.push_back(to_test(plan[b]));
+        std::vector<fkpc::RStream> snaps;
+        std::vector<fkpc_ci_record> rec;
+        engp->set_stream_snapshots(&snaps);
+        try {
+          evaluate(*engp, tests, opt, rs.get(), &rec, &run->stats);
+        } catch (...) {
+          engp->set_stream_snapshots(nullptr);
+          throw;
+        }
+        engp->set_stream_snapshots(nullptr);
+        if (snaps.size() != seq.size()) throw fkpc::Error(FKPC_STATUS_NUMERIC, "permutation stream snapshots incomplete");
+        size_t limit = seq.size(), i = 0;
+        for (; i < limit; ++i) {
+          const int b = seq[i];
+          pv[b] = rec[i].p_value;
+          pe[b] = rec[i].p_exact;
+          fl[b] = rec[i].flags;
+          counted[b] = 1;
+          const std::pair<int, int> key{plan[b].edge_x, plan[b].edge_y};
+          if (rec[i].p_value >= opt.alpha) {
+            pos[key] = by_edge[key].size();
+            for (size_t j = i + 1; j < limit; ++j)
+              if (plan[seq[j]].edge_x == key.first && plan[seq[j]].edge_y == key.second) {
+                limit = j;  // that test would have been skipped: later draws belong elsewhere
+                break;
+              }
+          } else {
+            ++pos[key];
+          }
+        }
+        if (i < seq.size()) {
+          *rs = snaps[i - 1];
+          window = std::max<size_t>(8, window / 2);
+        } else {
+          window = std::min<size_t>(1024, window * 2);
+        }
+      }
+    } else if (perm || opt.mode == FKPC_MODE_PLAIN) {
       if (evaluator) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "the level evaluator serves the batched gamma methods");
       // one test at a time; permutation methods in pcalg order
       std::map<std::pair<int, int>, size_t> pos;

@@ -790,6 +790,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
         int* dst = perms.data() + t * static_cast<size_t>(R) * n;
         if (method == FKPC_DCC_PERM) rstream->dcc_permutations(n, R, dst);
         else rstream->hsic_permutations(n, R, dst);
+        if (stream_snapshots_) stream_snapshots_->push_back(*rstream);
       }
       h2d_bytes_ += upload(d_perms_, perms, stream_);
     }

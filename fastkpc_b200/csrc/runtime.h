@@ -106,6 +106,9 @@ class Engine {
   double time_stage(int stage, int repeats, double* flops_per_launch);
   double measure_fp64_peak();
   cudaStream_t stream() const { return stream_; }
+  // When set, packing a permutation batch appends the stream's state after
+  // each test's permutations (a speculative caller rolls back to one).
+  void set_stream_snapshots(std::vector<RStream>* s) { stream_snapshots_ = s; }
   int launches() const { return launches_; }
   double setup_ms() const { return setup_ms_; }
 
@@ -206,6 +209,7 @@ class Engine {
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;
   cudaEvent_t ev_[7] = {};  // [6]: the bivariate thin-plate results have landed
+  std::vector<RStream>* stream_snapshots_ = nullptr;
   char* h_stage_ = nullptr;
   size_t h_stage_cap_ = 0, h_stage_used_ = 0;
   std::vector<char*> h_stage_retired_;

@@ -365,3 +365,23 @@ def test_host_built_bivariate_design_in_the_one_shot_batch(lib):
     staged.execute(1)
     two, _ = staged.collect()
     assert np.array_equal(one["p_value"], two["p_value"])
+
+
+@pytest.mark.parametrize("method", ["dcc.perm", "hsic.perm"])
+def test_permutation_skeleton_windows_follow_the_sequential_stream(lib, method):
+    """p = 12: edges at level 1 and beyond carry several tests, so deletions
+    inside a speculative window cut it short and the stream is reset.  The
+    skeleton, every p-value and the test counts equal the oracle's strictly
+    sequential run."""
+    X = workloads.nonlinear_sem(80, 12, 0.25, 21)[0]
+    opts = {"ci_method": method, "numCol": 35, "trace_level": "logical",
+            "permutation_params": {"replicates": 30, "seed": 7, "include_observed": True}}
+    out = fk.fastkpc_compatible_cuda_skeleton(X, 0.1, options=opts)
+    ora = skeleton.skeleton(X, 0.1, method, replicates=30, seed=7)
+    assert out["n_edgetests"] == ora["n_edgetests"].tolist()
+    assert np.array_equal(out["adjacency"], ora["adjacency"])
+    got = sorted(zip(out["tasks"]["level"], out["tasks"]["x"], out["tasks"]["y"],
+                     map(tuple, out["tasks"]["S"]), out["tasks"]["p_used"]))
+    exp = sorted((r["level"], r["x"], r["y"], tuple(r["S"]), r["p_value"]) for r in ora["trace"])
+    assert [g[:4] for g in got] == [e[:4] for e in exp]
+    assert [g[4] for g in got] == [e[4] for e in exp]

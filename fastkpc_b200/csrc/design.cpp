@@ -648,6 +648,16 @@ std::shared_ptr<const Smooth> DesignCache::univariate(int column) {
   return sm;
 }
 
+void DesignCache::put_univariate(int column, std::shared_ptr<const Smooth> smooth) {
+  std::lock_guard<std::mutex> lock(mu_);
+  uni_[column] = std::move(smooth);
+}
+
+bool DesignCache::has_univariate(int column) {
+  std::lock_guard<std::mutex> lock(mu_);
+  return uni_.count(column) > 0;
+}
+
 void DesignCache::put_bivariate(const std::vector<int>& S, std::shared_ptr<const Smooth> smooth) {
   std::lock_guard<std::mutex> lock(mu_);
   bi_[S] = std::move(smooth);

@@ -94,6 +94,9 @@ class DesignCache {
   std::shared_ptr<const Smooth> univariate(int column);
   // bivariate thin-plate smooths built outside build_design (device eigen)
   void put_bivariate(const std::vector<int>& S, std::shared_ptr<const Smooth> smooth);
+  // univariate smooths built outside the cache (device eigen)
+  void put_univariate(int column, std::shared_ptr<const Smooth> smooth);
+  bool has_univariate(int column);
   std::shared_ptr<const Smooth> bivariate(const std::vector<int>& S);
   bool has_design(const std::vector<int>& S);
   size_t size() const { return designs_.size(); }

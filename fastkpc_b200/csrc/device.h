@@ -56,7 +56,7 @@ struct GeomJob {
   int64_t basis;                 // arena offset of Q (n x q)
   int64_t rmat;                  // arena offset of R (q x q)
   int64_t rpack;                 // arena offset of row-packed R, or -1
-  int64_t src[kMaxPenalties];    // smooth j's first column in the basis table (n x dim_j)
+  const double* src[kMaxPenalties];  // smooth j's basis (n x dim_j, leading dimension n), device memory
   int off[kMaxPenalties];
   int dim[kMaxPenalties];
   int q;

@@ -94,24 +94,27 @@ cudaError_t launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st
 // designs (one CTA per design); see kernels_tprs.cu.
 constexpr int kTprsMaxSteps = 128;
 constexpr int kTprsRitzMax = 30;   // Ritz pairs per design (the basis dimension k of the bivariate smooth)
+constexpr int kTprsUniK = 10;      // the basis dimension k of the univariate smooth
 constexpr int kTprsMaxNu = 1536;  // unique locations a design may have on the device path
 // eta-matrix workspace per CTA: the leading dimension rounded up to the 32-row tile
 FKPC_HD constexpr int64_t tprs_ld(int nu) { return (static_cast<int64_t>(nu) + 31) / 32 * 32; }
 // Ritz pairs of the Lanczos runs: alpha / beta / done as written by the
 // Lanczos kernel; vals: count x k; zsel:
 // count x k x steps; ok[d] = 1 when design d's k pairs converged; U: design
-// d's nu x k Ritz vectors at U + uoff[d].  k must equal kTprsRitzMax.
+// d's nu x k Ritz vectors at U + uoff[d].  k is kTprsRitzMax or kTprsUniK.
 cudaError_t launch_tprs_ritz(const double* alpha, const double* beta, const int* done, int count, int steps, int k,
                              double* vals, double* zsel, int* ok, const double* V, const int64_t* voff,
                              const int* nus, double* U, const int64_t* uoff, cudaStream_t stream);
-// The bivariate thin-plate basis from its Ritz pairs (k = kTprsRitzMax):
+// The thin-plate basis from its Ritz pairs (dim 2: k = kTprsRitzMax; dim 1:
+// k = kTprsUniK):
 // X (count x n x k doubles; design d's basis n x (k - 1) at X + d n k),
 // S (count x (k-1)^2), colsq (count x (k-1)), status (count); see
 // kernels_tprs.cu.
 cudaError_t launch_tprs_finish(const double* U, const int64_t* uoff, const double* vals, const int* ok,
                                const double* loc, const int64_t* locoff, const int* nus, const int* mapping, int n,
-                               int count, double* X, double* S, double* colsq, int* status, cudaStream_t stream);
-cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int* nus, int count, int nu_max,
+                               int count, int dim, double* X, double* S, double* colsq, int* status,
+                               cudaStream_t stream);
+cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int* nus, int count, int nu_max, int dim,
                                 int steps, double eta0, double* ews, int64_t ews_stride, int ctas, double* V,
                                 const int64_t* voff, double* alpha, double* beta, int* done, cudaStream_t stream);
 
@@ -122,7 +125,7 @@ cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int*
 // spectrum into the arena); status[d] 1 rank deficient, 2 eigen failed.
 cudaError_t launch_single_geometry(int n, const SingleGeomJob* jobs, int count, double* arena, int* status,
                                    cudaStream_t stream);
-cudaError_t launch_additive_geometry(const double* table, int n, const GeomJob* jobs, int count, int max_q,
-                                     double* arena, int* status, cudaStream_t stream);
+cudaError_t launch_additive_geometry(int n, const GeomJob* jobs, int count, int max_q, double* arena, int* status,
+                                     cudaStream_t stream);
 
 }  // namespace fkpc

@@ -134,12 +134,11 @@ static __device__ bool householder_inplace(double* __restrict__ W, int n, int q,
 // in_smem: the design's n x q working matrix lives in dynamic shared memory
 // (n q doubles available) and Q is written to the arena at the end;
 // otherwise it is factored in place in the arena (L2).
-__global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const double* __restrict__ table, int n,
-                                                                         const GeomJob* __restrict__ jobs, int count,
-                                                                         double* __restrict__ arena,
+__global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(int n, const GeomJob* __restrict__ jobs,
+                                                                         int count, double* __restrict__ arena,
                                                                          int* __restrict__ status, int in_smem) {
   extern __shared__ double wsm[];
-  __shared__ int64_t colsrc[kGeomMaxQ];
+  __shared__ const double* colsrc[kGeomMaxQ];
   __shared__ double vks[kGeomMaxQ], betas[kGeomMaxQ];
   __shared__ double red[kGeomWarps];
   const int tid = threadIdx.x;
@@ -150,7 +149,7 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const d
     double* W = in_smem ? wsm : Q;
     double* R = arena + job.rmat;
     if (tid < q) {
-      int64_t src = -1;  // the intercept column
+      const double* src = nullptr;  // the intercept column
       for (int j = 0; j < job.m; ++j)
         if (tid >= job.off[j] && tid < job.off[j] + job.dim[j])
           src = job.src[j] + static_cast<int64_t>(n) * (tid - job.off[j]);
@@ -159,9 +158,9 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(const d
     __syncthreads();
     const int64_t nq = static_cast<int64_t>(n) * q;
     for (int c = 0; c < q; ++c) {
-      const int64_t s = colsrc[c];
+      const double* s = colsrc[c];
       double* wc = W + static_cast<int64_t>(n) * c;
-      for (int r = tid; r < n; r += blockDim.x) wc[r] = s < 0 ? 1.0 : table[s + r];
+      for (int r = tid; r < n; r += blockDim.x) wc[r] = s ? s[r] : 1.0;
     }
     for (int idx = tid; idx < q * q; idx += blockDim.x) R[idx] = 0.0;
     __syncthreads();
@@ -434,16 +433,15 @@ cudaError_t launch_single_geometry(int n, const SingleGeomJob* jobs, int count, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_additive_geometry(const double* table, int n, const GeomJob* jobs, int count, int max_q,
-                                     double* arena, int* status, cudaStream_t stream) {
+cudaError_t launch_additive_geometry(int n, const GeomJob* jobs, int count, int max_q, double* arena, int* status,
+                                     cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
   if (n < 2 || max_q < 1 || max_q > kGeomMaxQ || max_q >= n) return cudaErrorInvalidValue;
   const size_t smem = geometry_smem(n, max_q, kAdditiveStaticSmem);
   int ctas = 0;
   cudaError_t e = geometry_launch_shape(additive_geometry_kernel, smem, count, &ctas);
   if (e != cudaSuccess) return e;
-  additive_geometry_kernel<<<ctas, kGeomThreads, smem, stream>>>(table, n, jobs, count, arena, status,
-                                                                  smem > 0 ? 1 : 0);
+  additive_geometry_kernel<<<ctas, kGeomThreads, smem, stream>>>(n, jobs, count, arena, status, smem > 0 ? 1 : 0);
   return cudaGetLastError();
 }
 

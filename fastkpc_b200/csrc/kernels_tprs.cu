@@ -1,5 +1,6 @@
-// Thin-plate set-up on the device: the Lanczos part of the top-k eigen problem
-// of the eta matrix of every bivariate (|S| = 2) design of a level.
+// Thin-plate set-up on the device: the top-k eigen problem of the eta matrix
+// of every bivariate (|S| = 2, k = 30) and univariate (k = 10) smooth of a
+// level, and the rest of the basis.
 //
 // mgcv's tp basis for d = 2 (m = 2, k = 30) needs the k largest-magnitude
 // eigenpairs of E_ij = eta(|u_i - u_j|), eta(r) = r^2 log(r) / (8 pi), over the
@@ -68,7 +69,7 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
     const double* __restrict__ u, const int64_t* __restrict__ uoff, const int* __restrict__ nus, int count,
     int steps, double eta0, double* __restrict__ ews, int64_t ews_stride, double* __restrict__ V,
     const int64_t* __restrict__ voff, double* __restrict__ alpha, double* __restrict__ beta, int* __restrict__ done,
-    int ld_max) {
+    int ld_max, int dim) {
   extern __shared__ double sm[];
   __shared__ double red[kTprsWarps];
   __shared__ double coef[kTprsMaxSteps];
@@ -84,22 +85,32 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
     const int ld = static_cast<int>(tprs_ld(nu));
     const int nb = ld / kTile;
     const double* ux = u + uoff[d];
-    const double* uy = ux + nu;
+    const double* uy = ux + nu;  // read only when dim == 2
     double* E = ews + ews_stride * blockIdx.x;
     double* Vd = V + voff[d];
-    // upper block triangle of E_ij = eta0 log(r2) / 2 * r2 (zero outside nu x nu)
+    // upper block triangle of E_ij = eta(r), zero outside nu x nu, in the
+    // host's order of operations: d = 2: eta0 log(r2) / 2 * r2; d = 1: eta0 r2 sqrt(r2)
     for (int J = 0; J < nb; ++J) {
       const int rows = kTile * (J + 1);
       for (int idx = tid; idx < rows * kTile; idx += blockDim.x) {
         const int i = idx % rows, j = kTile * J + idx / rows;
         double v = 0.0;
         if (i < nu && j < nu) {
-          const double dx = ux[i] - ux[j], dy = uy[i] - uy[j];
-          const double r2 = dx * dx + dy * dy;
+          const double dx = ux[i] - ux[j];
+          double r2 = dx * dx;
+          if (dim == 2) {
+            const double dy = uy[i] - uy[j];
+            r2 += dy * dy;
+          }
           if (r2 > 0.0) {
             v = eta0;
-            v *= log(r2) * 0.5;
-            v *= r2;
+            if (dim == 2) {
+              v *= log(r2) * 0.5;
+              v *= r2;
+            } else {
+              v *= r2;
+              v *= sqrt(r2);
+            }
           }
         }
         E[i + static_cast<int64_t>(ld) * j] = v;
@@ -435,11 +446,11 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
   if (lane == 0) ok[d] = conv ? 1 : 0;
 }
 
+template <int K>
 __global__ void __launch_bounds__(kTprsThreads) tprs_ritz_vectors_kernel(
     const double* __restrict__ V, const int64_t* __restrict__ voff, const int* __restrict__ nus,
     const int* __restrict__ done, const int* __restrict__ ok, const double* __restrict__ zsel, int count, int steps,
     double* __restrict__ U, const int64_t* __restrict__ uoff) {
-  constexpr int K = kTprsRitzMax;
   __shared__ double zs[kTprsMaxSteps * K];
   __shared__ double red_ss[kTprsWarps][K];
   __shared__ double red_mx[kTprsWarps][K];
@@ -531,7 +542,7 @@ cudaError_t launch_tprs_ritz(const double* alpha, const double* beta, const int*
                              double* vals, double* zsel, int* ok, const double* V, const int64_t* voff,
                              const int* nus, double* U, const int64_t* uoff, cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
-  if (k != kTprsRitzMax || steps < k || steps > kTprsMaxSteps) return cudaErrorInvalidValue;
+  if ((k != kTprsRitzMax && k != kTprsUniK) || steps < k || steps > kTprsMaxSteps) return cudaErrorInvalidValue;
   const size_t per_warp = sizeof(double) * static_cast<size_t>(steps) * steps;
   int warps = static_cast<int>(kRitzSmemBudget / per_warp);
   warps = warps < 1 ? 1 : (warps > kRitzWarps ? kRitzWarps : warps);
@@ -544,7 +555,12 @@ cudaError_t launch_tprs_ritz(const double* alpha, const double* beta, const int*
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int ctas = count < 2 * 148 ? count : 2 * 148;
-  tprs_ritz_vectors_kernel<<<ctas, kTprsThreads, 0, stream>>>(V, voff, nus, done, ok, zsel, count, steps, U, uoff);
+  if (k == kTprsRitzMax)
+    tprs_ritz_vectors_kernel<kTprsRitzMax><<<ctas, kTprsThreads, 0, stream>>>(V, voff, nus, done, ok, zsel, count,
+                                                                               steps, U, uoff);
+  else
+    tprs_ritz_vectors_kernel<kTprsUniK><<<ctas, kTprsThreads, 0, stream>>>(V, voff, nus, done, ok, zsel, count,
+                                                                            steps, U, uoff);
   return cudaGetLastError();
 }
 
@@ -559,8 +575,6 @@ cudaError_t launch_tprs_ritz(const double* alpha, const double* beta, const int*
 // leading dimension n), the penalty S ((k-1) x (k-1)) and the column sums of
 // squares of X (k-1).  status[d]: 0, or 1 (a zero basis column), 2 (penalty
 // scaling), 3 (centering constraint), -1 (Ritz pairs not accepted).
-constexpr int kFinishK = kTprsRitzMax;
-constexpr int kFinishM = 3;  // null space of the d = 2, m = 2 thin plate: 1, x, y
 
 // Sum over the block of a k-vector held per thread; out[c] for c < K (fixed order).
 template <int K>
@@ -580,12 +594,14 @@ __device__ __forceinline__ void block_vec_sum(const double (&v)[K], double (*red
   __syncthreads();
 }
 
+// K: the basis dimension; M: the null space of the m = 2 thin plate, 1, x (d = 1)
+// or 1, x, y (d = 2).
+template <int K, int M>
 __global__ void __launch_bounds__(kTprsThreads) tprs_finish_kernel(
     const double* __restrict__ U, const int64_t* __restrict__ uoff, const double* __restrict__ vals,
     const int* __restrict__ ok, const double* __restrict__ loc, const int64_t* __restrict__ locoff,
     const int* __restrict__ nus, const int* __restrict__ mapping, int n, int count, double* __restrict__ X,
     double* __restrict__ S, double* __restrict__ colsq, int* __restrict__ status) {
-  constexpr int K = kFinishK, M = kFinishM;
   __shared__ double red[kTprsWarps][K];
   __shared__ double TU[M][K], Z[M][K];
   __shared__ double P[K][K + 1];
@@ -600,7 +616,7 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_finish_kernel(
     const int nu = nus[d];
     const double* Ud = U + uoff[d];
     const double* ux = loc + locoff[d];
-    const double* uy = ux + nu;
+    const double* uy = ux + nu;  // read only when M == 3
     const int* map = mapping + static_cast<int64_t>(d) * n;
     double* Xd = X + static_cast<int64_t>(d) * n * K;
     if (tid < K) val[tid] = vals[static_cast<int64_t>(d) * K + tid];
@@ -609,7 +625,7 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_finish_kernel(
       const int t = pr / K, c = pr % K;
       double acc = 0.0;
       for (int i = lane; i < nu; i += 32) {
-        const double ti = t == 0 ? 1.0 : (t == 1 ? ux[i] : uy[i]);
+        const double ti = t == 0 ? 1.0 : (t == 1 ? ux[i] : uy[i]);  // t < M
         acc += ti * Ud[i + static_cast<int64_t>(nu) * c];
       }
       acc = warp_sum_t(acc);
@@ -687,7 +703,7 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_finish_kernel(
       }
       x[K - M] = 1.0;
       x[K - M + 1] = ux[li];
-      x[K - M + 2] = uy[li];
+      if (M == 3) x[K - 1] = uy[li];
 #pragma unroll
       for (int c = 0; c < K; ++c) {
         Xd[r + static_cast<int64_t>(n) * c] = x[c];
@@ -832,12 +848,18 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_finish_kernel(
 
 cudaError_t launch_tprs_finish(const double* U, const int64_t* uoff, const double* vals, const int* ok,
                                const double* loc, const int64_t* locoff, const int* nus, const int* mapping, int n,
-                               int count, double* X, double* S, double* colsq, int* status, cudaStream_t stream) {
+                               int count, int dim, double* X, double* S, double* colsq, int* status,
+                               cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
-  if (n < kFinishK) return cudaErrorInvalidValue;
+  const int k = dim == 2 ? kTprsRitzMax : kTprsUniK;
+  if ((dim != 1 && dim != 2) || n < k) return cudaErrorInvalidValue;
   const int ctas = count < 2 * 148 ? count : 2 * 148;
-  tprs_finish_kernel<<<ctas, kTprsThreads, 0, stream>>>(U, uoff, vals, ok, loc, locoff, nus, mapping, n, count, X, S,
-                                                         colsq, status);
+  if (dim == 2)
+    tprs_finish_kernel<kTprsRitzMax, 3><<<ctas, kTprsThreads, 0, stream>>>(U, uoff, vals, ok, loc, locoff, nus,
+                                                                            mapping, n, count, X, S, colsq, status);
+  else
+    tprs_finish_kernel<kTprsUniK, 2><<<ctas, kTprsThreads, 0, stream>>>(U, uoff, vals, ok, loc, locoff, nus, mapping,
+                                                                         n, count, X, S, colsq, status);
   return cudaGetLastError();
 }
 
@@ -846,11 +868,11 @@ size_t tprs_smem_bytes(int nu_max) {
   return sizeof(double) * static_cast<size_t>((2 + kTprsWarps) * ld + kTprsWarps * kTileWords);
 }
 
-cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int* nus, int count, int nu_max,
+cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int* nus, int count, int nu_max, int dim,
                                 int steps, double eta0, double* ews, int64_t ews_stride, int ctas, double* V,
                                 const int64_t* voff, double* alpha, double* beta, int* done, cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
-  if (steps < 1 || steps > kTprsMaxSteps || ctas < 1 || nu_max < 1 || nu_max > kTprsMaxNu ||
+  if (steps < 1 || steps > kTprsMaxSteps || ctas < 1 || nu_max < 1 || nu_max > kTprsMaxNu || (dim != 1 && dim != 2) ||
       ews_stride < tprs_ld(nu_max) * tprs_ld(nu_max))
     return cudaErrorInvalidValue;
   const size_t smem = tprs_smem_bytes(nu_max);
@@ -862,7 +884,7 @@ cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int*
   if (e != cudaSuccess) return e;
   tprs_lanczos_kernel<<<ctas, kTprsThreads, smem, stream>>>(u, uoff, nus, count, steps, eta0, ews, ews_stride, V,
                                                              voff, alpha, beta, done,
-                                                             static_cast<int>(tprs_ld(nu_max)));
+                                                             static_cast<int>(tprs_ld(nu_max)), dim);
   return cudaGetLastError();
 }
 

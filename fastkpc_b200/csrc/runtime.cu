@@ -247,6 +247,9 @@ constexpr int kTprsK = 30;                  // basis dimension of the bivariate 
 // converges within 60-70 steps on the 587 bivariate designs of a 500 x 50
 // level; a design that has not converged by kTprsSteps is rebuilt on the host.
 constexpr int kTprsSteps = kTprsK + 50;
+// The univariate smooths (k = 10): the host solver converges within 25-30
+// steps on a 500 x 50 level's variables.
+constexpr int kTprsUniSteps = kTprsUniK + 30;
 // Every bivariate design the engine builds takes the device Lanczos, however
 // few there are: the per-design computation is deterministic, so a design
 // comes out bit-identical whatever batch (plain or batched form) it is in.
@@ -254,15 +257,21 @@ constexpr size_t kDeviceTprsMin = 1;
 
 }  // namespace
 
-// The top-30 eigen problems of the level's new bivariate designs: prepare on
-// the host, Lanczos and Ritz pairs on the device, the rest of the basis on
-// the host.  launch_bivariate_on_device enqueues the kernels and the copies
-// of their results into page-locked memory and returns at once; the host
-// builds the other designs meanwhile; finish_bivariate_on_device waits and
-// finishes the bases.  Designs whose Ritz pairs do not converge in
-// kTprsSteps steps are left to the host set-up in build_designs.
-void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& sets, TprsBatch* batch) {
+// The thin-plate smooths of a level that the cache lacks -- univariate
+// (k = 10) and bivariate (k = 30) -- set up on the device: prepare on the
+// host; Lanczos, Ritz pairs and the rest of the basis on the device; the
+// basis stays there.  launch_tprs_batch enqueues the kernels and the copies of
+// the penalties and column norms into page-locked memory and returns at once;
+// finish_tprs_batch waits for them and puts the smooths into the cache.
+// Smooths whose Ritz pairs do not converge in the batch's steps, or with too
+// few unique locations, are left to the host set-up.
+void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int dim, TprsBatch* batch) {
+  batch->idx.clear();
+  if (sets.empty()) return;
   const int n = n_;
+  const int kk = dim == 2 ? kTprsK : kTprsUniK;
+  const int steps = dim == 2 ? kTprsSteps : kTprsUniSteps;
+  batch->dim = dim;
   const size_t count = sets.size();
   batch->sets = sets;
   batch->preps.assign(count, TprsPrep());
@@ -270,13 +279,13 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
   std::vector<char> ok(count, 0);
   parallel_for(count, [&](size_t i) {
     try {
-      std::vector<double> cols(static_cast<size_t>(2) * n);
-      std::copy(host_data_.begin() + static_cast<size_t>(n) * sets[i][0],
-                host_data_.begin() + static_cast<size_t>(n) * (sets[i][0] + 1), cols.begin());
-      std::copy(host_data_.begin() + static_cast<size_t>(n) * sets[i][1],
-                host_data_.begin() + static_cast<size_t>(n) * (sets[i][1] + 1), cols.begin() + n);
-      batch->preps[i] = tprs_prepare(cols.data(), n, 2, kTprsK);
-      ok[i] = batch->preps[i].nu > kTprsSteps && batch->preps[i].nu <= kTprsMaxNu;
+      std::vector<double> cols(static_cast<size_t>(dim) * n);
+      for (int c = 0; c < dim; ++c)
+        std::copy(host_data_.begin() + static_cast<size_t>(n) * sets[i][c],
+                  host_data_.begin() + static_cast<size_t>(n) * (sets[i][c] + 1),
+                  cols.begin() + static_cast<size_t>(n) * c);
+      batch->preps[i] = tprs_prepare(cols.data(), n, dim, kk);
+      ok[i] = batch->preps[i].nu > steps && batch->preps[i].nu <= kTprsMaxNu;
     } catch (const std::exception&) {
       ok[i] = 0;  // the host set-up reports the error
     }
@@ -296,9 +305,9 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
     ltotal += static_cast<int64_t>(pr.u.size());
     batch->nus.push_back(pr.nu);
     voff.push_back(vtotal);
-    vtotal += static_cast<int64_t>(pr.nu) * kTprsSteps;
+    vtotal += static_cast<int64_t>(pr.nu) * steps;
     roff.push_back(utotal);
-    utotal += static_cast<int64_t>(pr.nu) * kTprsK;
+    utotal += static_cast<int64_t>(pr.nu) * kk;
     nu_max = std::max(nu_max, pr.nu);
   }
   double* hu = static_cast<double*>(stage_alloc(sizeof(double) * static_cast<size_t>(ltotal)));
@@ -310,10 +319,10 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
   });
   const int cnt = static_cast<int>(batch->idx.size());
   const int ctas = std::min(cnt, 2 * 148);  // two designs per SM (memory-bound matvec)
-  const size_t nab = static_cast<size_t>(2) * cnt * kTprsSteps;
-  const size_t nvals = static_cast<size_t>(cnt) * kTprsK;
-  const size_t ns = static_cast<size_t>(cnt) * (kTprsK - 1) * (kTprsK - 1);
-  const size_t ncs = static_cast<size_t>(cnt) * (kTprsK - 1);
+  const size_t nab = static_cast<size_t>(2) * cnt * steps;
+  const size_t nvals = static_cast<size_t>(cnt) * kk;
+  const size_t ns = static_cast<size_t>(cnt) * (kk - 1) * (kk - 1);
+  const size_t ncs = static_cast<size_t>(cnt) * (kk - 1);
   // page-locked landing area: penalties, column sums of squares, status
   double* host = static_cast<double*>(stage_alloc(sizeof(double) * (ns + ncs + (static_cast<size_t>(cnt) + 1) / 2)));
   batch->S = host;
@@ -338,7 +347,7 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
   double* dU = d_tprs_U_.ensure(static_cast<size_t>(utotal));
   int* dok = d_tprs_ok_.ensure(cnt);
   // a spare chunk from an earlier cache when one is large enough, else a new one
-  const size_t xneed = static_cast<size_t>(cnt) * n * kTprsK;
+  const size_t xneed = static_cast<size_t>(cnt) * n * kk;
   std::unique_ptr<DevBuf<double>> chunk;
   for (size_t i = 0; i < smooth_spare_.size(); ++i)
     if (smooth_spare_[i]->capacity() >= xneed) {
@@ -353,16 +362,16 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
   double* dS = d_tprs_S_.ensure(ns);
   double* dcs = d_tprs_colsq_.ensure(ncs);
   int* dst = d_tprs_status_.ensure(cnt);
-  cuda_check(launch_tprs_lanczos(d_tprs_u_.get(), d_tprs_uoff_.get(), d_tprs_nus_.get(), cnt, nu_max, kTprsSteps,
-                                 tprs_eta0(2), ews, ews_stride, ctas, dV, d_tprs_voff_.get(), dab,
-                                 dab + static_cast<size_t>(cnt) * kTprsSteps, ddone, stream_),
+  cuda_check(launch_tprs_lanczos(d_tprs_u_.get(), d_tprs_uoff_.get(), d_tprs_nus_.get(), cnt, nu_max, dim, steps,
+                                 tprs_eta0(dim), ews, ews_stride, ctas, dV, d_tprs_voff_.get(), dab,
+                                 dab + static_cast<size_t>(cnt) * steps, ddone, stream_),
              "thin-plate Lanczos");
-  cuda_check(launch_tprs_ritz(dab, dab + static_cast<size_t>(cnt) * kTprsSteps, ddone, cnt, kTprsSteps, kTprsK,
-                              dvals, d_tprs_zsel_.ensure(nvals * kTprsSteps), dok, dV, d_tprs_voff_.get(),
+  cuda_check(launch_tprs_ritz(dab, dab + static_cast<size_t>(cnt) * steps, ddone, cnt, steps, kk,
+                              dvals, d_tprs_zsel_.ensure(nvals * steps), dok, dV, d_tprs_voff_.get(),
                               d_tprs_nus_.get(), dU, d_tprs_roff_.get(), stream_),
              "thin-plate Ritz pairs");
   cuda_check(launch_tprs_finish(dU, d_tprs_roff_.get(), dvals, dok, d_tprs_u_.get(), d_tprs_uoff_.get(),
-                                d_tprs_nus_.get(), d_tprs_map_.get(), n, cnt, dX, dS, dcs, dst, stream_),
+                                d_tprs_nus_.get(), d_tprs_map_.get(), n, cnt, dim, dX, dS, dcs, dst, stream_),
              "thin-plate basis");
   cuda_check(cudaMemcpyAsync(batch->S, dS, ns * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
   cuda_check(cudaMemcpyAsync(batch->colsq, dcs, ncs * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
@@ -370,24 +379,35 @@ void Engine::launch_bivariate_on_device(const std::vector<std::vector<int>>& set
                              stream_),
              "download");
   d2h_bytes_ += static_cast<double>(ns + ncs) * sizeof(double) + static_cast<double>(cnt) * sizeof(int);
-  cuda_check(cudaEventRecord(ev_[6], stream_), "event");
+  cuda_check(cudaEventRecord(ev_[dim == 2 ? 6 : 7], stream_), "event");
 }
 
-void Engine::finish_bivariate_on_device(TprsBatch* batch) {
+void Engine::finish_tprs_batch(TprsBatch* batch) {
   if (batch->idx.empty()) return;
-  cuda_check(cudaEventSynchronize(ev_[6]), "thin-plate set-up");
+  const int dim = batch->dim;
+  cuda_check(cudaEventSynchronize(ev_[dim == 2 ? 6 : 7]), "thin-plate set-up");
   const int n = n_;
-  constexpr int cols = kTprsK - 1;
-  for (size_t c = 0; c < batch->idx.size(); ++c) {
-    if (batch->status[c] != 0) continue;  // not converged or degenerate: the host set-up builds this design
+  const int kk = dim == 2 ? kTprsK : kTprsUniK;
+  const int cols = kk - 1;
+  std::vector<std::shared_ptr<Smooth>> made(batch->idx.size());
+  // not converged or degenerate (status != 0): the host set-up builds that smooth
+  parallel_for(batch->idx.size(), [&](size_t c) {
+    if (batch->status[c] != 0) return;
     auto sm = std::make_shared<Smooth>();
     sm->n = n;
     sm->cols = cols;
-    sm->rank = kTprsK - 3;  // the d = 2 thin plate's null space has dimension 3
+    sm->rank = kk - (dim == 2 ? 3 : 2);  // the m = 2 thin plate's null space: 1, x (, y)
     sm->S.assign(batch->S + c * cols * cols, batch->S + (c + 1) * cols * cols);
     sm->colsq.assign(batch->colsq + c * cols, batch->colsq + (c + 1) * cols);
-    sm->dev_x = batch->X + c * static_cast<size_t>(n) * kTprsK;
-    cache_->put_bivariate(batch->sets[batch->idx[c]], sm);
+    if (dim == 1) sm->root = penalty_root(sm->S, cols, sm->rank);
+    sm->dev_x = batch->X + c * static_cast<size_t>(n) * kk;
+    made[c] = sm;
+  });
+  for (size_t c = 0; c < batch->idx.size(); ++c) {
+    if (!made[c]) continue;
+    const std::vector<int>& set = batch->sets[batch->idx[c]];
+    if (dim == 2) cache_->put_bivariate(set, made[c]);
+    else cache_->put_univariate(set[0], made[c]);
   }
 }
 
@@ -424,15 +444,21 @@ void Engine::build_host_designs(Pick pick) {
 // The univariate smooths of the batch's variables, each built once (several
 // additive designs share a variable; building them design by design would
 // let threads race to build the same smooth).
-void Engine::build_univariate_smooths() {
+std::vector<std::vector<int>> Engine::univariate_columns() {
   std::vector<char> need(p_, 0);
   for (const auto& S : sets_)
     if (S.size() != 2)
       for (int v : S)
         if (v >= 0 && v < p_) need[v] = 1;
-  std::vector<int> cols;
+  std::vector<std::vector<int>> cols;
   for (int v = 0; v < p_; ++v)
-    if (need[v]) cols.push_back(v);
+    if (need[v] && !cache_->has_univariate(v)) cols.push_back({v});
+  return cols;
+}
+
+void Engine::build_univariate_smooths() {
+  std::vector<int> cols;
+  for (const auto& c : univariate_columns()) cols.push_back(c[0]);
   std::string err;
   std::mutex err_mu;
   parallel_for(cols.size(), [&](size_t i) {
@@ -451,12 +477,14 @@ void Engine::build_designs() {
   std::vector<std::vector<int>> bivariate;
   for (const auto& S : sets_)
     if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
-  TprsBatch batch;
-  if (bivariate.size() >= kDeviceTprsMin) launch_bivariate_on_device(bivariate, &batch);
+  TprsBatch ubatch, batch;
+  launch_tprs_batch(univariate_columns(), 1, &ubatch);
+  if (bivariate.size() >= kDeviceTprsMin) launch_tprs_batch(bivariate, 2, &batch);
   // the other designs need no bivariate basis: build them while the device works
-  build_univariate_smooths();
+  finish_tprs_batch(&ubatch);
+  build_univariate_smooths();  // those the device could not take
   build_host_designs([](const std::vector<int>& S) { return S.size() != 2; });
-  finish_bivariate_on_device(&batch);
+  finish_tprs_batch(&batch);
   build_host_designs([](const std::vector<int>& S) { return S.size() == 2; });
 }
 
@@ -667,7 +695,8 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
     job.m = des.m;
     geom_max_q = std::max(geom_max_q, des.q);
     for (int j = 0; j < des.m; ++j) {
-      job.src[j] = smooth_slots[smooth_index.at(des.parts[j].get())].x;
+      const Smooth* sm = des.parts[j].get();
+      job.src[j] = sm->dev_x ? sm->dev_x : arena + smooth_slots[smooth_index.at(sm)].x;
       job.off[j] = des.offsets[j];
       job.dim[j] = des.dims[j];
     }
@@ -729,7 +758,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
   geom_status_checked_ = 0;
   if (!gjobs.empty()) {
     h2d_bytes_ += stage_upload(d_geom_jobs_, gjobs);
-    cuda_check(launch_additive_geometry(arena, n, d_geom_jobs_.get(), static_cast<int>(gjobs.size()), geom_max_q, arena,
+    cuda_check(launch_additive_geometry(n, d_geom_jobs_.get(), static_cast<int>(gjobs.size()), geom_max_q, arena,
                                         gstatus_dev, stream_),
                "additive geometry");
   }
@@ -898,9 +927,11 @@ void Engine::run_batch(const std::vector<Test>& tests, const fkpc_options& opt, 
     std::vector<std::vector<int>> bivariate;
     for (const auto& S : sets_)
       if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
-    TprsBatch batch;
-    if (!bivariate.empty()) launch_bivariate_on_device(bivariate, &batch);
-    build_univariate_smooths();
+    TprsBatch ubatch, batch;
+    launch_tprs_batch(univariate_columns(), 1, &ubatch);
+    if (!bivariate.empty()) launch_tprs_batch(bivariate, 2, &batch);
+    finish_tprs_batch(&ubatch);
+    build_univariate_smooths();  // those the device could not take
     build_host_designs([this](const std::vector<int>& S) { return S.size() != 2 || cache_->has_design(S); });
     double host_ms = ms_since(t0);
     pack_and_upload(opt, rstream, true);  // queued behind the thin-plate kernels
@@ -911,7 +942,7 @@ void Engine::run_batch(const std::vector<Test>& tests, const fkpc_options& opt, 
     cuda_check(cudaEventRecord(ev_[0], stream_), "event");
     enqueue_multi();
     auto t1 = std::chrono::steady_clock::now();
-    finish_bivariate_on_device(&batch);
+    finish_tprs_batch(&batch);
     build_host_designs([](const std::vector<int>&) { return true; });
     host_ms += ms_since(t1);
     auto t2 = std::chrono::steady_clock::now();

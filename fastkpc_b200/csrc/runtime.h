@@ -131,8 +131,10 @@ class Engine {
   void enqueue_rest();   // direct columns, single-penalty fits, statistics
   void pack_late();      // pending bivariate designs: descriptors, geometry
   void check_geometry();  // statuses of the geometry kernels (after a synchronisation)
-  // one level's bivariate thin-plate Lanczos on the device, in flight
+  // one level's thin-plate smooths (dim 2: bivariate, dim 1: univariate) on
+  // the device, in flight
   struct TprsBatch {
+    int dim = 2;
     std::vector<std::vector<int>> sets;
     std::vector<TprsPrep> preps;
     std::vector<size_t> idx;  // sets taken by the device
@@ -142,8 +144,9 @@ class Engine {
     double* colsq = nullptr;
     int* status = nullptr;
   };
-  void launch_bivariate_on_device(const std::vector<std::vector<int>>& sets, TprsBatch* batch);
-  void finish_bivariate_on_device(TprsBatch* batch);
+  void launch_tprs_batch(const std::vector<std::vector<int>>& sets, int dim, TprsBatch* batch);
+  void finish_tprs_batch(TprsBatch* batch);
+  std::vector<std::vector<int>> univariate_columns();  // variables whose smooth the cache lacks
   template <class Pick>
   void build_host_designs(Pick pick);
   // defer: leave the stream running (the geometry statuses are checked by collect)
@@ -208,7 +211,7 @@ class Engine {
   size_t h_arena_cap_ = 0;
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;
-  cudaEvent_t ev_[7] = {};  // [6]: the bivariate thin-plate results have landed
+  cudaEvent_t ev_[8] = {};  // [6] / [7]: the bivariate / univariate thin-plate results have landed
   std::vector<RStream>* stream_snapshots_ = nullptr;
   char* h_stage_ = nullptr;
   size_t h_stage_cap_ = 0, h_stage_used_ = 0;

@@ -107,13 +107,13 @@ void* Engine::stage_alloc(size_t bytes) {
 }
 
 template <class T>
-double Engine::stage_upload(DevBuf<T>& buf, const std::vector<T>& host) {
+double Engine::stage_upload(DevBuf<T>& buf, const std::vector<T>& host, cudaStream_t st) {
   T* d = buf.ensure(host.size());
   if (host.empty()) return 0.0;
   const size_t bytes = host.size() * sizeof(T);
   void* h = stage_alloc(bytes);
   std::memcpy(h, host.data(), bytes);
-  cuda_check(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream_), "upload");
+  cuda_check(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st ? st : stream_), "upload");
   return static_cast<double>(bytes);
 }
 
@@ -265,12 +265,14 @@ constexpr size_t kDeviceTprsMin = 1;
 // finish_tprs_batch waits for them and puts the smooths into the cache.
 // Smooths whose Ritz pairs do not converge in the batch's steps, or with too
 // few unique locations, are left to the host set-up.
-void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int dim, TprsBatch* batch) {
+void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int dim, TprsBatch* batch, cudaStream_t st,
+                               int ctas_per_sm) {
   batch->idx.clear();
   if (sets.empty()) return;
   const int n = n_;
   const int kk = dim == 2 ? kTprsK : kTprsUniK;
   const int steps = dim == 2 ? kTprsSteps : kTprsUniSteps;
+  TprsBuffers& tb = tprs_buf_[dim - 1];
   batch->dim = dim;
   const size_t count = sets.size();
   batch->sets = sets;
@@ -318,7 +320,7 @@ void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int di
     std::memcpy(hmap + c * static_cast<size_t>(n), pr.mapping.data(), static_cast<size_t>(n) * sizeof(int));
   });
   const int cnt = static_cast<int>(batch->idx.size());
-  const int ctas = std::min(cnt, 2 * 148);  // two designs per SM (memory-bound matvec)
+  const int ctas = std::min(cnt, ctas_per_sm * 148);
   const size_t nab = static_cast<size_t>(2) * cnt * steps;
   const size_t nvals = static_cast<size_t>(cnt) * kk;
   const size_t ns = static_cast<size_t>(cnt) * (kk - 1) * (kk - 1);
@@ -328,24 +330,24 @@ void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int di
   batch->S = host;
   batch->colsq = host + ns;
   batch->status = reinterpret_cast<int*>(host + ns + ncs);
-  cuda_check(cudaMemcpyAsync(d_tprs_u_.ensure(static_cast<size_t>(ltotal)), hu, sizeof(double) * ltotal,
-                             cudaMemcpyHostToDevice, stream_),
+  cuda_check(cudaMemcpyAsync(tb.u.ensure(static_cast<size_t>(ltotal)), hu, sizeof(double) * ltotal,
+                             cudaMemcpyHostToDevice, st),
              "upload");
-  cuda_check(cudaMemcpyAsync(d_tprs_map_.ensure(batch->idx.size() * static_cast<size_t>(n)), hmap,
-                             sizeof(int) * batch->idx.size() * n, cudaMemcpyHostToDevice, stream_),
+  cuda_check(cudaMemcpyAsync(tb.map.ensure(batch->idx.size() * static_cast<size_t>(n)), hmap,
+                             sizeof(int) * batch->idx.size() * n, cudaMemcpyHostToDevice, st),
              "upload");
-  stage_upload(d_tprs_uoff_, uoff);
-  stage_upload(d_tprs_voff_, voff);
-  stage_upload(d_tprs_roff_, roff);
-  stage_upload(d_tprs_nus_, batch->nus);
+  stage_upload(tb.uoff, uoff, st);
+  stage_upload(tb.voff, voff, st);
+  stage_upload(tb.roff, roff, st);
+  stage_upload(tb.nus, batch->nus, st);
   const int64_t ews_stride = tprs_ld(nu_max) * tprs_ld(nu_max);
-  double* dV = d_tprs_V_.ensure(static_cast<size_t>(vtotal));
-  double* dab = d_tprs_ab_.ensure(nab);
-  double* ews = d_tprs_ews_.ensure(static_cast<size_t>(ctas) * ews_stride);
-  int* ddone = d_tprs_done_.ensure(cnt);
-  double* dvals = d_tprs_vals_.ensure(nvals);
-  double* dU = d_tprs_U_.ensure(static_cast<size_t>(utotal));
-  int* dok = d_tprs_ok_.ensure(cnt);
+  double* dV = tb.V.ensure(static_cast<size_t>(vtotal));
+  double* dab = tb.ab.ensure(nab);
+  double* ews = tb.ews.ensure(static_cast<size_t>(ctas) * ews_stride);
+  int* ddone = tb.done.ensure(cnt);
+  double* dvals = tb.vals.ensure(nvals);
+  double* dU = tb.U.ensure(static_cast<size_t>(utotal));
+  int* dok = tb.ok.ensure(cnt);
   // a spare chunk from an earlier cache when one is large enough, else a new one
   const size_t xneed = static_cast<size_t>(cnt) * n * kk;
   std::unique_ptr<DevBuf<double>> chunk;
@@ -359,27 +361,27 @@ void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int di
   double* dX = chunk->ensure(xneed);
   smooth_store_.push_back(std::move(chunk));
   batch->X = dX;
-  double* dS = d_tprs_S_.ensure(ns);
-  double* dcs = d_tprs_colsq_.ensure(ncs);
-  int* dst = d_tprs_status_.ensure(cnt);
-  cuda_check(launch_tprs_lanczos(d_tprs_u_.get(), d_tprs_uoff_.get(), d_tprs_nus_.get(), cnt, nu_max, dim, steps,
-                                 tprs_eta0(dim), ews, ews_stride, ctas, dV, d_tprs_voff_.get(), dab,
-                                 dab + static_cast<size_t>(cnt) * steps, ddone, stream_),
+  double* dS = tb.S.ensure(ns);
+  double* dcs = tb.colsq.ensure(ncs);
+  int* dst = tb.status.ensure(cnt);
+  cuda_check(launch_tprs_lanczos(tb.u.get(), tb.uoff.get(), tb.nus.get(), cnt, nu_max, dim, steps,
+                                 tprs_eta0(dim), ews, ews_stride, ctas, dV, tb.voff.get(), dab,
+                                 dab + static_cast<size_t>(cnt) * steps, ddone, st),
              "thin-plate Lanczos");
   cuda_check(launch_tprs_ritz(dab, dab + static_cast<size_t>(cnt) * steps, ddone, cnt, steps, kk,
-                              dvals, d_tprs_zsel_.ensure(nvals * steps), dok, dV, d_tprs_voff_.get(),
-                              d_tprs_nus_.get(), dU, d_tprs_roff_.get(), stream_),
+                              dvals, tb.zsel.ensure(nvals * steps), dok, dV, tb.voff.get(),
+                              tb.nus.get(), dU, tb.roff.get(), st),
              "thin-plate Ritz pairs");
-  cuda_check(launch_tprs_finish(dU, d_tprs_roff_.get(), dvals, dok, d_tprs_u_.get(), d_tprs_uoff_.get(),
-                                d_tprs_nus_.get(), d_tprs_map_.get(), n, cnt, dim, dX, dS, dcs, dst, stream_),
+  cuda_check(launch_tprs_finish(dU, tb.roff.get(), dvals, dok, tb.u.get(), tb.uoff.get(),
+                                tb.nus.get(), tb.map.get(), n, cnt, dim, dX, dS, dcs, dst, st),
              "thin-plate basis");
-  cuda_check(cudaMemcpyAsync(batch->S, dS, ns * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
-  cuda_check(cudaMemcpyAsync(batch->colsq, dcs, ncs * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
+  cuda_check(cudaMemcpyAsync(batch->S, dS, ns * sizeof(double), cudaMemcpyDeviceToHost, st), "download");
+  cuda_check(cudaMemcpyAsync(batch->colsq, dcs, ncs * sizeof(double), cudaMemcpyDeviceToHost, st), "download");
   cuda_check(cudaMemcpyAsync(batch->status, dst, static_cast<size_t>(cnt) * sizeof(int), cudaMemcpyDeviceToHost,
-                             stream_),
+                             st),
              "download");
   d2h_bytes_ += static_cast<double>(ns + ncs) * sizeof(double) + static_cast<double>(cnt) * sizeof(int);
-  cuda_check(cudaEventRecord(ev_[dim == 2 ? 6 : 7], stream_), "event");
+  cuda_check(cudaEventRecord(ev_[dim == 2 ? 6 : 7], st), "event");
 }
 
 void Engine::finish_tprs_batch(TprsBatch* batch) {
@@ -478,8 +480,8 @@ void Engine::build_designs() {
   for (const auto& S : sets_)
     if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
   TprsBatch ubatch, batch;
-  launch_tprs_batch(univariate_columns(), 1, &ubatch);
-  if (bivariate.size() >= kDeviceTprsMin) launch_tprs_batch(bivariate, 2, &batch);
+  launch_tprs_batch(univariate_columns(), 1, &ubatch, stream_, 2);
+  if (bivariate.size() >= kDeviceTprsMin) launch_tprs_batch(bivariate, 2, &batch, stream_, 2);
   // the other designs need no bivariate basis: build them while the device works
   finish_tprs_batch(&ubatch);
   build_univariate_smooths();  // those the device could not take
@@ -928,8 +930,8 @@ void Engine::run_batch(const std::vector<Test>& tests, const fkpc_options& opt, 
     for (const auto& S : sets_)
       if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
     TprsBatch ubatch, batch;
-    launch_tprs_batch(univariate_columns(), 1, &ubatch);
-    if (!bivariate.empty()) launch_tprs_batch(bivariate, 2, &batch);
+    launch_tprs_batch(univariate_columns(), 1, &ubatch, stream_, 2);
+    if (!bivariate.empty()) launch_tprs_batch(bivariate, 2, &batch, stream_, 2);
     finish_tprs_batch(&ubatch);
     build_univariate_smooths();  // those the device could not take
     build_host_designs([this](const std::vector<int>& S) { return S.size() != 2 || cache_->has_design(S); });

@@ -126,7 +126,7 @@ class Engine {
   void stage_reset();
   void* stage_alloc(size_t bytes);
   template <class T>
-  double stage_upload(DevBuf<T>& buf, const std::vector<T>& host);
+  double stage_upload(DevBuf<T>& buf, const std::vector<T>& host, cudaStream_t st = nullptr);
   void enqueue_multi();  // the multi-penalty fit classes
   void enqueue_rest();   // direct columns, single-penalty fits, statistics
   void pack_late();      // pending bivariate designs: descriptors, geometry
@@ -144,7 +144,9 @@ class Engine {
     double* colsq = nullptr;
     int* status = nullptr;
   };
-  void launch_tprs_batch(const std::vector<std::vector<int>>& sets, int dim, TprsBatch* batch);
+  // on stream st with ctas_per_sm Lanczos CTAs per SM
+  void launch_tprs_batch(const std::vector<std::vector<int>>& sets, int dim, TprsBatch* batch, cudaStream_t st,
+                         int ctas_per_sm);
   void finish_tprs_batch(TprsBatch* batch);
   std::vector<std::vector<int>> univariate_columns();  // variables whose smooth the cache lacks
   template <class Pick>
@@ -189,11 +191,14 @@ class Engine {
   DevBuf<FitState> d_fit_states_;  // optimiser states handed to the speculative continuation
   DevBuf<int> d_defer_list_, d_defer_count_;
   // device thin-plate Lanczos of the bivariate designs
-  DevBuf<double> d_tprs_u_, d_tprs_V_, d_tprs_ab_, d_tprs_ews_;
-  DevBuf<int64_t> d_tprs_uoff_, d_tprs_voff_, d_tprs_roff_;
-  DevBuf<int> d_tprs_nus_, d_tprs_done_, d_tprs_ok_;
-  DevBuf<double> d_tprs_vals_, d_tprs_zsel_, d_tprs_U_, d_tprs_S_, d_tprs_colsq_;
-  DevBuf<int> d_tprs_map_, d_tprs_status_;
+  // one set per smooth dimension (univariate, bivariate): both batches of a
+  // level are in flight together
+  struct TprsBuffers {
+    DevBuf<double> u, V, ab, ews, vals, zsel, U, S, colsq;
+    DevBuf<int64_t> uoff, voff, roff;
+    DevBuf<int> nus, done, ok, map, status;
+  };
+  TprsBuffers tprs_buf_[2];
   // device geometry of the additive designs
   DevBuf<GeomJob> d_geom_jobs_;
   DevBuf<SingleGeomJob> d_single_geom_jobs_;

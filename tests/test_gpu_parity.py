@@ -385,3 +385,19 @@ def test_permutation_skeleton_windows_follow_the_sequential_stream(lib, method):
     exp = sorted((r["level"], r["x"], r["y"], tuple(r["S"]), r["p_value"]) for r in ora["trace"])
     assert [g[:4] for g in got] == [e[:4] for e in exp]
     assert [g[4] for g in got] == [e[4] for e in exp]
+
+
+def test_device_smooths_at_n1000_match_oracle(lib):
+    """n = 1000: the thin-plate Lanczos runs with leading dimension 1024 (one
+    CTA per SM by shared memory), and the geometry kernels, whose n x q
+    working matrices no longer fit in shared memory, factor in the arena.
+    Univariate, bivariate and additive residuals against the oracle."""
+    X = workloads.nonlinear_sem(1000, 12, 0.3, 31)[0]
+    fits = [(0, [3, 7]), (5, [1, 2]), (9, [4, 11]), (2, [6]), (8, [0, 5, 10]), (11, [1, 3, 6, 9])]
+    resid, lsp, status = fk.regress_batch(X, fits)
+    assert (status == 0).all()
+    for k, (t, S) in enumerate(fits):
+        prep = gcv.Prepared(tprs.design(X, S))
+        r, _ = gcv.fit(prep, X[:, t])
+        err = np.max(np.abs(resid[:, k] - r)) / np.max(np.abs(r))
+        assert err <= RESID_TOL, (t, S, err)

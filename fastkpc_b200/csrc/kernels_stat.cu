@@ -513,17 +513,18 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
     const double alpha = block_sum256(part, ls.red);
     const double bprev = j > 0 ? ls.beta[j - 1] : 0.0;
     const double* vp = j > 0 ? V + static_cast<int64_t>(n) * (j - 1) : nullptr;
+    double before = 0.0;
     for (int i = tid; i < n; i += blockDim.x) {
       double v = w[i] - alpha * qv[i];
       if (vp) v -= bprev * vp[i];
       w[i] = v;
+      before += v * v;
     }
-    __syncthreads();
+    // (the reduction's barriers also publish w)
+    before = block_sum256(before, ls.red);
     // classical Gram-Schmidt against V[:, 0..j]; a second pass only when the
     // first removed more than half the norm ("twice is enough")
-    double before = 0.0;
-    for (int i = tid; i < n; i += blockDim.x) before += w[i] * w[i];
-    before = block_sum256(before, ls.red);
+    double after = before;
     for (int pass = 0; pass < 2; ++pass) {
       // coefficients V(:, b)'w: each warp takes four basis vectors per pass so
       // that their L2 loads overlap
@@ -556,7 +557,7 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
         }
       }
       __syncthreads();
-      double after = 0.0;
+      double part2 = 0.0;
       for (int i = tid; i < n; i += blockDim.x) {
         double s0 = w[i], s1 = 0.0, s2 = 0.0, s3 = 0.0;
         int b = 0;
@@ -572,15 +573,13 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
         for (; b <= j; ++b) s0 -= ls.coef[b] * V[i + static_cast<int64_t>(n) * b];
         const double s = (s0 + s1) + (s2 + s3);
         w[i] = s;
-        after += s * s;
+        part2 += s * s;
       }
-      after = block_sum256(after, ls.red);
+      after = block_sum256(part2, ls.red);
       if (after > 0.25 * before) break;
       before = after;
     }
-    double nn = 0.0;
-    for (int i = tid; i < n; i += blockDim.x) nn += w[i] * w[i];
-    const double beta = sqrt(block_sum256(nn, ls.red));
+    const double beta = sqrt(after);  // |w|^2 of the last pass
     anorm = fmax(anorm, fabs(alpha) + beta + bprev);
     if (tid == 0) {
       ls.alpha[j] = alpha;

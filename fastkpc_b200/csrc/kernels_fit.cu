@@ -275,7 +275,7 @@ constexpr double kGnGradTol = 1e-9;   // Gauss-Newton selection: |grad V| <= 1e-
 constexpr double kGnFlatTol = 1e-12;  // or a decrease <= 1e-12 (1 + V)
 constexpr double kGnFlatGrad = 1e-6;  // with |grad V| <= 1e-6 (1 + V)
 constexpr double kGnMaxLogSp = 25.0;  // upper bound of the Gauss-Newton search in log(lambda)
-constexpr int kDeferCalls = 40;       // warp-class fits past this many evaluations continue speculatively
+constexpr int kDeferCalls = 25;       // warp-class fits past this many evaluations continue speculatively
 
 __device__ __forceinline__ int tri(int i, int j) { return j * (j + 1) / 2 + i; }  // packed upper, i <= j
 

@@ -1941,6 +1941,7 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
 // boundary probes are speculated the same way; the terminal polish and the
 // final fit run on warp 0.
 constexpr int kSpecWarps = 6;
+constexpr int kSpecCtas = 148 * (6 / kSpecWarps);  // as many CTAs as the SMs' shared memory holds
 
 struct SpecShared {
   double score[kSpecWarps];
@@ -2338,7 +2339,7 @@ cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const dou
     if (defer) {
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
-      const int ctas = count < 148 ? count : 148;
+      const int ctas = count < kSpecCtas ? count : kSpecCtas;
       fit_multi_spec_kernel<<<ctas, 32 * kSpecWarps, kSpecWarps * kWarpSlotBytes, stream>>>(
           designs, arena, data, n, jobs, defer_list, defer_count, states, residuals, results);
     }

@@ -741,6 +741,14 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
       else multi_huge_.push_back(idx);
     }
   }
+  if (opt.mode != FKPC_MODE_PLAIN) {
+    // Longest fits first: the warp fit kernel's CTAs start in index order, so
+    // the widest designs (an evaluation costs about q^2) leave the last wave
+    // to the short ones.  Results are written by job index; order is free.
+    std::stable_sort(multi_small_.begin(), multi_small_.end(), [&](int a, int b) {
+      return ddesc[multi_jobs_[a].design].q > ddesc[multi_jobs_[b].design].q;
+    });
+  }
   if (opt.mode == FKPC_MODE_PLAIN) {
     plain_single_off_.push_back(static_cast<int>(single_jobs_.size()));
     plain_small_off_.push_back(static_cast<int>(multi_small_.size()));

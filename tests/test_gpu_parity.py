@@ -401,3 +401,20 @@ def test_device_smooths_at_n1000_match_oracle(lib):
         r, _ = gcv.fit(prep, X[:, t])
         err = np.max(np.abs(resid[:, k] - r)) / np.max(np.abs(r))
         assert err <= RESID_TOL, (t, S, err)
+
+
+def test_widest_first_fit_order_changes_no_record(lib):
+    """The batched form starts the warp-class fits widest design first
+    (|S| = 4, q = 37, before |S| = 3, q = 28); the plain form runs them in
+    test order.  With the two widths interleaved, every record agrees bit for
+    bit."""
+    X, triples = workloads.level_batch_500x50(count=1200)
+    wide = [t for t in triples if len(t[2]) == 4]
+    narrow = [t for t in triples if len(t[2]) == 3]
+    mixed = [t for pair in zip(narrow, wide) for t in pair][:300]
+    assert len(mixed) == 300
+    batched, st = fk.ci_level_batch(X, mixed)
+    plain, _ = fk.ci_level_batch(X, mixed, mode="plain")
+    assert np.all(batched["status"] == 0)
+    for field in ("p_value", "statistic", "p_exact"):
+        assert np.array_equal(batched[field], plain[field]), field

@@ -36,6 +36,11 @@ sys.path.insert(0, ROOT)
 METRIC = "CI tests/s batched vs plain at n=500; 351x48 skeleton wall-s vs host CPU"
 UNIT = "CI tests/s"
 WORKLOAD = "level batch n=500 p=50 SEM edge 0.08, 4096 triples |S|~U{0..4}, dcc.gamma, FP64"
+# DRAM bytes (read + write) of one fit-stage launch -- warp kernel plus
+# speculative continuation -- on this workload (seed 2, 4096 triples), from one
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum); ncu cannot run
+# inside the timed region.
+FIT_STAGE_TRAFFIC = {"bytes": 442.9e6, "source": "profiles/fit_stage_traffic_500x50.txt"}
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -271,6 +276,7 @@ def run_ours(args, world, rank, local, pg):
     peak = fk.measure_fp64_peak(local)
     avg_ms, flops = timed[dominant]
     achieved = flops / (avg_ms * 1e-3) / 1e12 if flops > 0 else None
+    traffic = FIT_STAGE_TRAFFIC["bytes"] if dominant == "fit_multi_small" and args.count == 4096 else None
 
     # plain per-test form on a sample of the same batch (designs resident)
     sample = triples[:args.plain_sample]
@@ -316,7 +322,9 @@ def run_ours(args, world, rank, local, pg):
                       "batched_over_plain": value / world / plain_rate},
             "stages_ms": {s: timed[s][0] for s in stages},
             "roofline": {"bound": "fp64", "kernel": dominant, "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
+                         "traffic": traffic, "traffic_unit": "bytes per launch",
+                         "traffic_source": FIT_STAGE_TRAFFIC["source"] if traffic else None,
                          "peak_source": "measured live: FP64 FMA probe (no FP64 figure in MEASURED_PEAKS.json)",
                          "flops_per_launch": flops, "avg_launch_ms": avg_ms},
             "cpu_baseline": {"value": cpu_rate, "unit": UNIT, "cores": cores, "kind": "port",

@@ -586,14 +586,15 @@ int fkpc_regress_batch(const double* data, int n, int p, const int* target, cons
     fkpc_options o;
     fkpc_default_options(&o);
     if (options) o = *options;
+    if (o.selection != FKPC_SELECT_MAGIC && o.selection != FKPC_SELECT_GN_NEWTON)
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "selection must be FKPC_SELECT_MAGIC or FKPC_SELECT_GN_NEWTON");
+    if (count == 0) return;  // nothing to fit: no device work
     std::lock_guard<std::mutex> lock(g_engine_mu);
     auto& eng = engine_for(o.device);
     eng.load(data, n, p);
     std::vector<int> tg(target, target + count);
     std::vector<std::vector<int>> sets(count);
     for (int t = 0; t < count; ++t) sets[t].assign(s_values + s_offsets[t], s_values + s_offsets[t + 1]);
-    if (o.selection != FKPC_SELECT_MAGIC && o.selection != FKPC_SELECT_GN_NEWTON)
-      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "selection must be FKPC_SELECT_MAGIC or FKPC_SELECT_GN_NEWTON");
     eng.regress(tg, sets, residuals, log_sp, max_penalties, status, o.selection);
   });
 }
@@ -604,6 +605,7 @@ int fkpc_stat_batch(const double* residuals, int n, int m, const int* left, cons
     if (!residuals || !left || !right || !options || !out || count < 0 || m < 1)
       throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
     validate_options(*options, n, std::max(2, m));
+    if (count == 0) return;  // no pairs: no device work
     std::lock_guard<std::mutex> lock(g_engine_mu);
     auto& eng = engine_for(options->device);
     eng.load(residuals, n, m);

@@ -418,3 +418,24 @@ def test_widest_first_fit_order_changes_no_record(lib):
     assert np.all(batched["status"] == 0)
     for field in ("p_value", "statistic", "p_exact"):
         assert np.array_equal(batched[field], plain[field]), field
+
+
+@pytest.mark.parametrize("method", ["dcc.gamma", "hsic.gamma", "dcc.perm"])
+def test_empty_batches_return_no_records(lib, method):
+    """A level with no tests, a regression with no fits and a statistic call
+    with no pairs succeed and return nothing; the staged form, which captures
+    a launch sequence, rejects an empty batch."""
+    X, _ = workloads.level_batch_500x50(count=1)
+    kw = {"seed": 3} if method.endswith("perm") else {}
+    for mode in ("batched", "plain"):
+        rec, st = fk.ci_level_batch(X, [], ci_method=method, mode=mode, **kw)
+        assert all(len(v) == 0 for v in rec.values())
+        assert st["pairs"] == 0 and st["kernel_launches"] == 0
+    resid, lsp, status = fk.regress_batch(X, [])
+    assert resid.shape == (X.shape[0], 0) and status.shape == (0,)
+    perms = np.zeros((0, 100, X.shape[0]), dtype=np.int32) if method.endswith("perm") else None
+    out = fk.stat_batch(X[:, :4], [], ci_method=method, permutations=perms, **kw)
+    assert all(len(v) == 0 for v in out.values())
+    with pytest.raises(fk.FkpcError) as e:
+        fk.StagedBatch(X, [], ci_method=method, **kw)
+    assert e.value.status == 1

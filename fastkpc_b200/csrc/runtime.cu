@@ -703,6 +703,11 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
       job.dim[j] = des.dims[j];
     }
   }
+  // Widest designs first: the geometry kernel's CTAs take jobs in a fixed
+  // stride and a QR costs about n q^2, so the last jobs of every CTA are the
+  // short ones.  Each job writes only its own arena ranges; status is checked
+  // as a whole.
+  std::stable_sort(gjobs.begin(), gjobs.end(), [](const GeomJob& a, const GeomJob& b) { return a.q > b.q; });
   single_jobs_.clear();
   multi_jobs_.clear();
   multi_small_.clear();

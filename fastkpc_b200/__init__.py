@@ -112,7 +112,8 @@ _SIGNATURES = {
     "fkpc_stat_batch": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, ctypes.c_int, _INT,
                                        _P(Options), _P(CiRecord)]),
     "fkpc_gcv_adjoint": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, ctypes.c_int, _INT, ctypes.c_int,
-                                        ctypes.c_int, _DBL, _DBL, _DBL, _DBL, _DBL]),
+                                        ctypes.c_int, _DBL, _DBL, _DBL, _DBL, _DBL, ctypes.c_int]),
+    "fkpc_gamma_q_eval": (ctypes.c_int, [ctypes.c_int, _DBL, _DBL, ctypes.c_int, _DBL, _INT]),
     "fkpc_batch_prepare": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, _INT, ctypes.c_int,
                                           _P(Options)]),
     "fkpc_batch_execute": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _DBL]),
@@ -462,7 +463,7 @@ def measure_fp64_peak(device=0):
     return t.value
 
 
-def gcv_adjoint(data, target, S, log_lambda):
+def gcv_adjoint(data, target, S, log_lambda, device=0):
     """GCV score V, gradient, Gauss-Newton Hessian and exact Hessian in
     rho = log(lambda) of the additive fit of column ``target`` on S (|S| >= 3)
     at each row of ``log_lambda`` (count x |S|; entry j belongs to the j-th
@@ -483,8 +484,22 @@ def gcv_adjoint(data, target, S, log_lambda):
     _check(load_library().fkpc_gcv_adjoint(_ptr(X, ctypes.c_double), n, p, int(target), _ptr(s, ctypes.c_int), m,
                                              count, _ptr(rho, ctypes.c_double), _ptr(score, ctypes.c_double),
                                              _ptr(grad, ctypes.c_double), _ptr(gn, ctypes.c_double),
-                                             _ptr(hess, ctypes.c_double)))
+                                             _ptr(hess, ctypes.c_double), int(device)))
     return {"score": score, "grad": grad, "gn_hessian": gn, "hessian": hess}
+
+
+def gamma_q(a, x, device=0):
+    """Q(a, x), the regularised upper incomplete gamma function, by the
+    statistic kernels' device routine; returns (q, ok) arrays."""
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+    x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).ravel())
+    if a.shape != x.shape:
+        raise ValueError("a and x must have the same length")
+    q = np.zeros_like(a)
+    ok = np.zeros(a.shape, dtype=np.int32)
+    _check(load_library().fkpc_gamma_q_eval(int(device), _ptr(a, ctypes.c_double), _ptr(x, ctypes.c_double),
+                                              len(a), _ptr(q, ctypes.c_double), _ptr(ok, ctypes.c_int)))
+    return q, ok.astype(bool)
 
 
 def design_export(data, S):

@@ -694,16 +694,37 @@ int fkpc_design_export(const double* data, int n, int p, const int* s_values, in
 
 int fkpc_gcv_adjoint(const double* data, int n, int p, int target, const int* s_values, int s_count, int count,
                      const double* log_lambda, double* score, double* grad, double* gn_hessian,
-                     double* exact_hessian) {
+                     double* exact_hessian, int device) {
   return guarded([&]() {
     if (!data || !s_values || (count > 0 && !log_lambda) || count < 0 || s_count < 0)
       throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
     if (n <= 5 || p < 2) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "data must be n x p with n > 5, p >= 2");
+    if (device < 0) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "device must be a CUDA device ordinal");
     std::lock_guard<std::mutex> lock(g_engine_mu);
-    auto& eng = engine_for(0);
+    auto& eng = engine_for(device);
     eng.load(data, n, p);
     eng.adjoint(target, std::vector<int>(s_values, s_values + s_count), count, log_lambda, score, grad, gn_hessian,
                 exact_hessian);
+  });
+}
+
+int fkpc_gamma_q_eval(int device, const double* a, const double* x, int count, double* q, int* ok) {
+  return guarded([&]() {
+    if (count < 0 || (count > 0 && (!a || !x || !q || !ok)))
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    if (device < 0) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "device must be a CUDA device ordinal");
+    if (count == 0) return;
+    fkpc::cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    fkpc::DevBuf<double> da, dx, dq;
+    fkpc::DevBuf<int> dok;
+    const size_t bytes = sizeof(double) * static_cast<size_t>(count);
+    fkpc::cuda_check(cudaMemcpy(da.ensure(count), a, bytes, cudaMemcpyHostToDevice), "upload a");
+    fkpc::cuda_check(cudaMemcpy(dx.ensure(count), x, bytes, cudaMemcpyHostToDevice), "upload x");
+    fkpc::cuda_check(fkpc::launch_gamma_q_eval(da.get(), dx.get(), count, dq.ensure(count), dok.ensure(count), nullptr),
+                     "gamma tail kernel");
+    fkpc::cuda_check(cudaMemcpy(q, dq.get(), bytes, cudaMemcpyDeviceToHost), "download q");
+    fkpc::cuda_check(cudaMemcpy(ok, dok.get(), sizeof(int) * static_cast<size_t>(count), cudaMemcpyDeviceToHost),
+                     "download status");
   });
 }
 

@@ -14,7 +14,13 @@ void set_last_error(const std::string& msg);
 size_t multi_smem_bytes(int qmax_class);
 // Raise the dynamic shared-memory limits (call outside graph capture).
 cudaError_t configure_fit_kernels();
+// Raise (never lower) the statistic kernels' shared-memory limits of the
+// current device to what n samples need.
 cudaError_t configure_stat_kernels(int n);
+// Q(a, x), the regularised upper incomplete gamma the gamma-approximation
+// p-values use, for ``count`` points (ok[i] = 0: series or fraction cap hit).
+cudaError_t launch_gamma_q_eval(const double* a, const double* x, int count, double* q, int* ok,
+                                cudaStream_t stream);
 
 cudaError_t launch_fit_single(const DesignDev* designs, const double* arena, const double* data, int n,
                               const FitJob* jobs, int count, double* residuals, FitResult* results,

@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <map>
+#include <mutex>
 
 #include "device.h"
 #include "kernels.h"
@@ -48,53 +50,87 @@ __device__ double block_sum256(double v, double* red) {
   return s;
 }
 
-// Regularised upper incomplete gamma Q(a, x): power series for x < a + 1,
-// modified Lentz continued fraction otherwise (the standard scheme of
-// Press et al., Numerical Recipes, section 6.2), relative tolerance 2e-15,
-// at most 10000 terms; *ok = 0 when the iteration cap is hit.
+// ---------------------------------------------------------------- gamma tail
+// Q(a, x) = Gamma(a, x) / Gamma(a), the upper tail of the gamma law the
+// dCov / HSIC moments define.  Written from two published representations:
+//
+//  * x < a + 1: the lower function by its power series (DLMF 8.7.1 / 8.11.4),
+//      P(a, x) = x^a e^-x / Gamma(a + 1) * sum_k x^k / ((a + 1) ... (a + k)),
+//    and Q = 1 - P (P is at most about 0.6 here, so Q keeps its absolute bits);
+//  * otherwise: Legendre's continued fraction for Gamma(a, x) (DLMF 8.9.2),
+//      e^x x^-a Gamma(a, x) = 1 / (x + 1 - a) * 1 / (1 + al_1 / (1 + al_2 / (1 + ...))),
+//      al_k = k (a - k) / ((x + 2k - 1 - a)(x + 2k + 1 - a)),
+//    summed as a series by the forward recurrence of W. Gautschi (ACM TOMS 5
+//    (1979) 466-481, section 4): t_0 = 1, r_0 = 0,
+//      r_k = -al_k (1 + r_{k-1}) / (1 + al_k (1 + r_{k-1})),  t_k = r_k t_{k-1}.
+//    For x >= a + 1 every |al_k| with k > a is below 1/4, so the denominators
+//    stay above 1/2: the recurrence needs no underflow guard.
+//
+// The common factor x^a e^-x / Gamma(a) is formed without cancellation for
+// a >= 10 through Stirling's series (Gamma(a) = sqrt(2 pi / a) (a / e)^a
+// e^{st(a)}, st(a) = sum_k B_2k / (2k (2k - 1) a^(2k-1))):
+//      x^a e^-x / Gamma(a) = sqrt(a / (2 pi)) exp(-a phi((x - a) / a) - st(a)),
+//      phi(t) = t - log(1 + t) >= 0,
+// with phi near 0 from the atanh series of log(1 + t) in u = t / (2 + t).
+// Both sums stop once a term falls below 2^-56 of the running sum; after
+// kGammaMaxTerms terms *ok stays 0.
+constexpr int kGammaMaxTerms = 20000;
+
+// t - log1p(t), accurate near t = 0
+__device__ double gamma_phi(double t) {
+  if (fabs(t) < 0.5) {
+    const double u = t / (2.0 + t), u2 = u * u;
+    double s = 0.0;  // 1/3 + u^2/5 + u^4/7 + ... (Horner, from the tail)
+    for (int k = 41; k >= 3; k -= 2) s = fma(s, u2, 1.0 / k);
+    return 2.0 * u2 / (1.0 - u) - 2.0 * u * u2 * s;
+  }
+  return t - log1p(t);
+}
+
+// log(Gamma(a)) - ((a - 1/2) log a - a + log(2 pi) / 2) for a >= 10
+__device__ double gamma_stirling_tail(double a) {
+  const double ia2 = 1.0 / (a * a);
+  double s = 1.0 / 156.0;
+  s = fma(s, ia2, -691.0 / 360360.0);
+  s = fma(s, ia2, 1.0 / 1188.0);
+  s = fma(s, ia2, -1.0 / 1680.0);
+  s = fma(s, ia2, 1.0 / 1260.0);
+  s = fma(s, ia2, -1.0 / 360.0);
+  s = fma(s, ia2, 1.0 / 12.0);
+  return s / a;
+}
+
+// x^a e^-x / Gamma(a), x > 0
+__device__ double gamma_kernel_factor(double a, double x) {
+  if (a < 10.0) return exp(a * log(x) - x - lgamma(a));
+  return sqrt(a * 0.15915494309189533577 /* 1 / (2 pi) */) * exp(-a * gamma_phi((x - a) / a) - gamma_stirling_tail(a));
+}
+
 __device__ double gamma_q(double a, double x, int* ok) {
   *ok = 0;
   if (!(a > 0.0) || !(x >= 0.0) || !isfinite(a) || !isfinite(x)) return NAN;
-  if (x == 0.0) {
-    *ok = 1;
-    return 1.0;
-  }
-  const double lpre = -x + a * log(x) - lgamma(a);
+  *ok = 1;
+  if (x == 0.0) return 1.0;
+  const double eps = 0x1p-56;
   if (x < a + 1.0) {
-    double ap = a, sum = 1.0 / a, term = sum;
-    for (int it = 1; it <= 10000; ++it) {
-      ap += 1.0;
-      term *= x / ap;
+    double sum = 1.0, term = 1.0;
+    for (int k = 1; k <= kGammaMaxTerms; ++k) {
+      term *= x / (a + k);
       sum += term;
-      if (fabs(term) <= fabs(sum) * 2e-15) {
-        *ok = 1;
-        const double lower = fmin(1.0, fmax(0.0, sum * exp(lpre)));
-        return fmin(1.0, fmax(0.0, 1.0 - lower));
-      }
+      if (term <= eps * sum) return fmin(1.0, fmax(0.0, 1.0 - gamma_kernel_factor(a, x) / a * sum));
     }
-    return NAN;
-  }
-  const double tiny = 1e-300;
-  double b = x + 1.0 - a;
-  double c = 1.0 / tiny;
-  double d = 1.0 / fmax(fabs(b), tiny);
-  if (b < 0.0) d = -d;
-  double f = d;
-  for (int it = 1; it <= 10000; ++it) {
-    const double an = -it * (it - a);
-    b += 2.0;
-    d = an * d + b;
-    if (fabs(d) < tiny) d = copysign(tiny, d == 0.0 ? 1.0 : d);
-    c = b + an / c;
-    if (fabs(c) < tiny) c = copysign(tiny, c == 0.0 ? 1.0 : c);
-    d = 1.0 / d;
-    const double delta = d * c;
-    f *= delta;
-    if (fabs(delta - 1.0) <= 2e-15) {
-      *ok = 1;
-      return fmin(1.0, fmax(0.0, exp(lpre) * f));
+  } else {
+    double sum = 1.0, t = 1.0, r = 0.0;
+    for (int k = 1; k <= kGammaMaxTerms; ++k) {
+      const double al = k * (a - k) / ((x + (2 * k - 1) - a) * (x + (2 * k + 1) - a));
+      const double w = al * (1.0 + r);
+      r = -w / (1.0 + w);
+      t *= r;
+      sum += t;
+      if (fabs(t) <= eps * fabs(sum)) return fmin(1.0, gamma_kernel_factor(a, x) / (x + 1.0 - a) * sum);
     }
   }
+  *ok = 0;
   return NAN;
 }
 
@@ -1137,7 +1173,44 @@ cudaError_t launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st
 // legacy Lanczos: r (sorted), q, w (n doubles each) and the sort permutation (n ints)
 size_t legacy_smem_bytes(int n) { return sizeof(double) * 3 * static_cast<size_t>(n) + sizeof(int) * static_cast<size_t>(n); }
 
+__global__ void gamma_q_eval_kernel(const double* __restrict__ a, const double* __restrict__ x, int count,
+                                    double* __restrict__ q, int* __restrict__ ok) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    int good = 0;
+    q[i] = gamma_q(a[i], x[i], &good);
+    ok[i] = good;
+  }
+}
+
+cudaError_t launch_gamma_q_eval(const double* a, const double* x, int count, double* q, int* ok,
+                                cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  gamma_q_eval_kernel<<<(count + 255) / 256, 256, 0, stream>>>(a, x, count, q, ok);
+  return cudaGetLastError();
+}
+
+cudaError_t set_stat_limits(int n);
+
+namespace {
+// Largest n the statistic kernels' shared-memory limits were raised for, per
+// device.  The limits only ever grow, so a call for a small n can never lower
+// them under a launch for a larger n made by another thread.
+std::mutex g_stat_limit_mu;
+std::map<int, int> g_stat_limit_n;
+}  // namespace
+
 cudaError_t configure_stat_kernels(int n) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_stat_limit_mu);
+  int& done = g_stat_limit_n[dev];
+  if (n <= done) return cudaSuccess;
+  if ((e = set_stat_limits(n)) == cudaSuccess) done = n;
+  return e;
+}
+
+cudaError_t set_stat_limits(int n) {
   const int s2 = static_cast<int>(sizeof(double) * 2 * n);
   const int s3 = static_cast<int>(sizeof(double) * 3 * n);
   const int s4 = static_cast<int>(sizeof(double) * 4 * n);

@@ -11,18 +11,20 @@
 // keeps until the process exits.
 //
 // Host code must not use the array's name as a device address (on the host
-// it names a host-side stand-in): the first call on each device looks the
-// address up with cudaGetSymbolAddress, with that device current, and caches
-// it; that first call should come before any stream capture.  Every call
-// shares the array, so calls that overlap on the GPU (different streams or
-// threads at once) race on it; calls on one stream, one after another, are
-// safe.  Each call writes every scratch value it reads before reading it, so
-// nothing is left over from an earlier call.
+// it names a host-side stand-in): every call looks the address up with
+// cudaGetSymbolAddress on the current device and checks the result, so a
+// context that was torn down and re-created (cudaDeviceReset) gets the new
+// address.  The first call on a device loads the library's device code there;
+// make it before any stream capture.  Every call shares the array, so calls
+// that overlap on the GPU (different streams or threads at once) race on it;
+// calls on one stream, one after another, are safe.  Each call writes every
+// scratch value it reads before reading it, so nothing is left over from an
+// earlier call.  The statistic kernels' shared-memory limits are only ever
+// raised (never lowered), so these calls may run beside the library's other
+// entry points.
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <map>
-#include <mutex>
 #include <string>
 
 #include "../../include/fastkpc_b200.h"
@@ -36,9 +38,6 @@ constexpr size_t kScratchDoubles = static_cast<size_t>(1) << 20;  // 8 MiB
 constexpr int kMaxN = 4096;  // the pair kernel stages 4n doubles in shared memory
 
 __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
-
-std::mutex g_mu;
-std::map<int, double*> g_scratch_ptr;
 
 int fail(int code, const std::string& msg) {
   set_last_error(msg);
@@ -58,20 +57,12 @@ __global__ void noalloc_plan_kernel(const int* __restrict__ pairs, int count, in
   }
 }
 
-// Device address of the scratch array for the current device (looked up once).
+// Device address of the scratch array on the current device.
 cudaError_t scratch_address(double** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
   if (e != cudaSuccess) return e;
-  std::lock_guard<std::mutex> lock(g_mu);
-  auto it = g_scratch_ptr.find(dev);
-  if (it == g_scratch_ptr.end()) {
-    void* ptr = nullptr;
-    e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    it = g_scratch_ptr.emplace(dev, static_cast<double*>(ptr)).first;
-  }
-  *out = it->second;
+  *out = static_cast<double*>(ptr);
   return cudaSuccess;
 }
 
@@ -81,8 +72,9 @@ cudaError_t scratch_address(double** out) {
 extern "C" int fkpc_dcov_gamma_noalloc(const double* residuals, int n, int m, const int* pairs, int count,
                                        fkpc_ci_record* out, void* stream_handle) {
   using namespace fkpc;
-  if (!residuals || !pairs || !out || n <= 5 || m < 1 || count < 1)
-    return fail(FKPC_STATUS_INVALID_ARGUMENT, "null pointer or empty problem");
+  if (count < 0 || (count > 0 && (!residuals || !pairs || !out)))
+    return fail(FKPC_STATUS_INVALID_ARGUMENT, "null pointer or negative pair count");
+  if (n <= 5 || m < 1) return fail(FKPC_STATUS_INVALID_ARGUMENT, "residuals must be n x m with n > 5 and m >= 1");
   if (n > kMaxN) return fail(FKPC_STATUS_INVALID_ARGUMENT, "n exceeds 4096, the limit of the no-allocation path");
   // scratch: centring constants n*m, moments m (two doubles each), column map
   // m ints, pair jobs count (two doubles each), one flag
@@ -92,6 +84,10 @@ extern "C" int fkpc_dcov_gamma_noalloc(const double* residuals, int n, int m, co
     return fail(FKPC_STATUS_INVALID_ARGUMENT,
                 "problem needs " + std::to_string(need) + " scratch doubles, more than the fixed " +
                     std::to_string(kScratchDoubles) + " (8 MiB) of the no-allocation path");
+  if (count == 0) {  // nothing to evaluate: no device work
+    set_last_error("");
+    return FKPC_OK;
+  }
   cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
   double* base = nullptr;
   cudaError_t e = scratch_address(&base);

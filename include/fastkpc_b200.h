@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define FKPC_ABI_VERSION 2
+#define FKPC_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define FKPC_API __attribute__((visibility("default")))
@@ -224,7 +224,8 @@ FKPC_API int fkpc_stat_batch(const double* residuals, int n, int m, const int* l
 /*
  * GCV score, gradient and Gauss-Newton Hessian in rho = log(lambda) of the
  * additive-smooth fit of data[:, target] on S (|S| >= 3, m = |S|) at
- * ``count`` given points, plus the exact Hessian for comparison, on device 0.
+ * ``count`` given points, plus the exact Hessian for comparison, on CUDA
+ * device ``device``.
  * Arrays are count-major: log_lambda and grad are count x m, the Hessians
  * count x m x m (row-major per point); any output may be NULL.  Entry j
  * of a point belongs to the j-th smallest variable of S.  The
@@ -236,7 +237,18 @@ FKPC_API int fkpc_stat_batch(const double* residuals, int n, int m, const int* l
 FKPC_API int fkpc_gcv_adjoint(const double* data_colmajor, int n, int p, int target,
                      const int* s_values, int s_count, int count,
                      const double* log_lambda, double* score, double* grad,
-                     double* gn_hessian, double* exact_hessian);
+                     double* gn_hessian, double* exact_hessian, int device);
+
+/*
+ * Q(a[i], x[i]), the regularised upper incomplete gamma function that every
+ * gamma-approximation p-value (dcc.gamma, hsic.gamma) takes, evaluated by the
+ * statistic kernels' own device routine on CUDA device ``device``; ok[i] = 0
+ * where the series or continued fraction did not converge.  Replaces
+ * regularized_gamma_q (fastkpc/src/cuda/full_cuda_ci_vertical.cu:334-398)
+ * as a testable unit.
+ */
+FKPC_API int fkpc_gamma_q_eval(int device, const double* a, const double* x, int count,
+                               double* q, int* ok);
 
 /*
  * Staged form of fkpc_ci_level_batch on the engine of options->device, for
@@ -295,10 +307,14 @@ FKPC_API int fkpc_design_export(const double* data_colmajor, int n, int p,
  * refinement); stream: a cudaStream_t or NULL.  Scratch lives in one fixed
  * 8 MiB device array inside the library: n <= 4096 and
  * n*m + 2.5*m + 2*count + 1 <= 2^20 doubles, otherwise the call fails with
- * FKPC_STATUS_INVALID_ARGUMENT.  The first call on a device looks the array's
- * address up (make it before any stream capture).  Calls share the array:
- * calls that overlap on the GPU race.  Synchronises ``stream`` before
- * returning.
+ * FKPC_STATUS_INVALID_ARGUMENT; count == 0 returns FKPC_OK with no device
+ * work.  Every call looks the array's address up on the current device; the
+ * first call on a device loads the library's device code there (make it
+ * before any stream capture).  Calls share the array: calls that overlap on
+ * the GPU race.  A pair index outside [0, m) fails the call with
+ * FKPC_STATUS_INVALID_ARGUMENT after the kernels ran on clamped indices; the
+ * contents of ``out`` are undefined whenever the call fails.  Synchronises
+ * ``stream`` before returning.
  */
 FKPC_API int fkpc_dcov_gamma_noalloc(const double* residuals, int n, int m,
                                      const int* pairs, int count,

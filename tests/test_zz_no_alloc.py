@@ -74,3 +74,24 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(lib_built):
     got = _noalloc(R, [(0, 1), (2, 3)], torch)
     ref = fk.stat_batch(R, [(0, 1), (2, 3)], ci_method="dcc.gamma")
     assert np.all(np.abs(got["p_value"] - ref["p_exact"]) <= TOL)
+
+
+def test_noalloc_reports_pairs_outside_the_columns(lib_built):
+    torch = pytest.importorskip("torch")
+    R = _pool(400, 6, 7)
+    # the kernels clamp the bad indices before any read, then the call fails
+    for bad in ([(0, 1), (2, 6)], [(-1, 3), (4, 5)]):
+        with pytest.raises(fk.FkpcError, match=r"outside \[0, m\)"):
+            _noalloc(R, bad, torch)
+    pairs = [(0, 1), (2, 3), (4, 5)]
+    got = _noalloc(R, pairs, torch)
+    ref = fk.stat_batch(R, pairs, ci_method="dcc.gamma")
+    assert np.all(np.abs(got["p_value"] - ref["p_exact"]) <= TOL)
+
+
+def test_noalloc_empty_call_does_no_work(lib_built):
+    # count == 0: success with no device work, like the other entry points
+    rc = fk.load_library().fkpc_dcov_gamma_noalloc(None, 100, 4, None, 0, None, None)
+    assert rc == 0
+    rc = fk.load_library().fkpc_dcov_gamma_noalloc(None, 100, 4, None, -1, None, None)
+    assert rc == 1

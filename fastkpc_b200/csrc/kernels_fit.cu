@@ -61,16 +61,18 @@ __device__ double hat_value(double log_sp, double e) {
 }
 
 // All 32 lanes call with the same log_sp; lane k < q owns component k.
+// RSS = rss0 + sum_k (1 - h_k)^2 z_k^2 with rss0 = |y - QW z|^2: two sums of
+// squares, so a fit that explains y almost exactly keeps a positive RSS
+// (|y|^2 - 2 sum h z^2 + sum h^2 z^2 cancels to rounding noise there).
 __device__ SingleObjective single_objective(double log_sp, double e, double z, bool active,
-                                            double yy, int n) {
-  double lin = 0, quad = 0, edf = 0, rg = 0, rh = 0, dg = 0, dh = 0;
+                                            double rss0, int n) {
+  double lin = 0, edf = 0, rg = 0, rh = 0, dg = 0, dh = 0;
   if (active) {
     const double h = hat_value(log_sp, e);
     const double z2 = z * z;
     const double omh = 1.0 - h;
     const double w = h * omh;
-    lin = h * z2;
-    quad = h * h * z2;
+    lin = omh * omh * z2;
     edf = h;
     rg = 2.0 * h * omh * omh * z2;
     rh = 2.0 * h * omh * omh * (3.0 * h - 1.0) * z2;
@@ -78,15 +80,13 @@ __device__ SingleObjective single_objective(double log_sp, double e, double z, b
     dh = -w * (1.0 - 2.0 * h);
   }
   lin = warp_sum(lin);
-  quad = warp_sum(quad);
   edf = warp_sum(edf);
   rg = warp_sum(rg);
   rh = warp_sum(rh);
   dg = warp_sum(dg);
   dh = warp_sum(dh);
   SingleObjective out;
-  double rss = yy - 2.0 * lin + quad;
-  if (rss < 0.0 && isfinite(rss)) rss = 0.0;
+  const double rss = rss0 + lin;
   const double rdf = static_cast<double>(n) - edf;
   out.rss = rss;
   out.edf = edf;
@@ -122,19 +122,16 @@ __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const d
   const double* QW = arena + des.basis;
   const double* y = data + static_cast<int64_t>(n) * job.column;
 
-  // z = QW' y and |y|^2; lane-strided rows, per-column partial sums
+  // z = QW' y; lane-strided rows, per-column partial sums
   double acc[kMaxSingleQ];
 #pragma unroll
   for (int k = 0; k < kMaxSingleQ; ++k) acc[k] = 0.0;
-  double yy = 0.0;
   for (int i = lane; i < n; i += 32) {
     const double yi = y[i];
-    yy += yi * yi;
 #pragma unroll
     for (int k = 0; k < kMaxSingleQ; ++k)
       if (k < q) acc[k] += QW[i + static_cast<int64_t>(n) * k] * yi;
   }
-  yy = warp_sum(yy);
   double zk = 0.0;
 #pragma unroll
   for (int k = 0; k < kMaxSingleQ; ++k) {
@@ -142,6 +139,20 @@ __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const d
     if (k == lane) zk = s;
   }
   const bool active = lane < q;
+  // rss0 = |y - QW z|^2, the part of y outside the design's span
+  __shared__ double coef_all[32 * 8];
+  double* coef = coef_all + warp * 32;
+  coef[lane] = active ? zk : 0.0;
+  __syncwarp();
+  double rss0 = 0.0;
+  for (int i = lane; i < n; i += 32) {
+    double f = 0.0;
+    for (int k = 0; k < q; ++k) f += QW[i + static_cast<int64_t>(n) * k] * coef[k];
+    const double e = y[i] - f;
+    rss0 += e * e;
+  }
+  rss0 = warp_sum(rss0);
+  __syncwarp();
   const double ek = active ? arena[des.spec + lane] : 0.0;
 
   FitResult res;
@@ -150,7 +161,7 @@ __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const d
   res.status = kStatusOk;
   const int max_half = 15;
   double log_sp = des.log_sp0[0];
-  SingleObjective cur = single_objective(log_sp, ek, zk, active, yy, n);
+  SingleObjective cur = single_objective(log_sp, ek, zk, active, rss0, n);
   int calls = 1;
   int it = 0;
   bool converged = false;
@@ -177,7 +188,7 @@ __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const d
           src_newton = false;
         }
         const double trial_ls = log_sp + step;
-        const SingleObjective trial = single_objective(trial_ls, ek, zk, active, yy, n);
+        const SingleObjective trial = single_objective(trial_ls, ek, zk, active, rss0, n);
         ++calls;
         const double pred = cur.gradient * step + 0.5 * cur.hessian * step * step;
         const double resolution = 8.0 * kEps * (1.0 + fabs(min_score));
@@ -218,7 +229,7 @@ __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const d
       const double direction = cur.gradient < 0.0 ? 1.0 : -1.0;
       for (int probe = 0; probe < 5; ++probe) {
         const double trial_ls = log_sp + direction * 2.0;
-        const SingleObjective trial = single_objective(trial_ls, ek, zk, active, yy, n);
+        const SingleObjective trial = single_objective(trial_ls, ek, zk, active, rss0, n);
         ++calls;
         if (!(trial.valid && trial.score < min_score)) break;
         log_sp = trial_ls;
@@ -234,15 +245,13 @@ __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const d
         const double step = -cur.gradient / cur.hessian;
         if (fabs(step) > 1e-6) break;
         log_sp += step;
-        cur = single_objective(log_sp, ek, zk, active, yy, n);
+        cur = single_objective(log_sp, ek, zk, active, rss0, n);
         ++calls;
         if (fabs(step) <= 1e-10) break;
       }
     }
   }
   // residual r = y - QW (h .* z)
-  __shared__ double coef_all[32 * 8];
-  double* coef = coef_all + warp * 32;
   coef[lane] = active ? hat_value(log_sp, ek) * zk : 0.0;
   __syncwarp();
   double* r = residuals + static_cast<int64_t>(n) * job.out;
@@ -304,7 +313,7 @@ struct MultiScalars {
   static constexpr int kLd = kMaxPenalties;  // leading dimension of the m x m matrices
   double beta[2], v0[2];
   double red[kMultiThreads / 32];
-  double score, rss, edf, yy;
+  double score, rss, edf, rss0;  // rss0 = |y - Q Q'y|^2
   double lam[kMaxPenalties];
   double log_sp[kMaxPenalties];
   double trial[kMaxPenalties];
@@ -452,18 +461,19 @@ __device__ void multi_core(const DesignDev& des, const double* __restrict__ aren
     g[c] = s;
   }
   const double edf = block_sum(e, sc);
+  // RSS = |y - Q y0|^2 + |y0 - W g|^2: sums of squares, no cancellation
   double gg = 0.0;
   if (tid < q) {
     const int i = tid;
     double s = 0.0;
     for (int c = i; c < q; ++c) s += W[tri(i, c)] * g[c];
     Wg[i] = s;
-    gg = g[i] * g[i] * -2.0 + s * s;
+    const double d = y0[i] - s;
+    gg = d * d;
   }
   const double part = block_sum(gg, sc);
   if (tid == 0) {
-    double rss = sc->yy + part;
-    if (rss < 0.0) rss = 0.0;
+    const double rss = sc->rss0 + part;
     const double delta = static_cast<double>(n) - edf;
     sc->rss = rss;
     sc->edf = edf;
@@ -898,7 +908,7 @@ __device__ void multi_fit_setup(const DesignDev& des, const double* __restrict__
     for (int c = 0; c < q; ++c)
       for (int i = tid; i <= c; i += kMultiThreads) Rs[tri(i, c)] = R[i + static_cast<int64_t>(q) * c];
   }
-  // y0 = Q'y, yy
+  // y0 = Q'y and rss0 = |y - Q y0|^2
   double* y0 = sm + L::Y0;
   {
     const int warp = tid >> 5, lane = tid & 31;
@@ -908,10 +918,16 @@ __device__ void multi_fit_setup(const DesignDev& des, const double* __restrict__
       s = warp_sum(s);
       if (lane == 0) y0[c] = s;
     }
-    double yy = 0.0;
-    for (int i = tid; i < n; i += kMultiThreads) yy += y[i] * y[i];
-    yy = block_sum(yy, &sc);
-    if (tid == 0) sc.yy = yy;
+    __syncthreads();
+    double ee = 0.0;
+    for (int i = tid; i < n; i += kMultiThreads) {
+      double f = 0.0;
+      for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * y0[c];
+      const double e = y[i] - f;
+      ee += e * e;
+    }
+    ee = block_sum(ee, &sc);
+    if (tid == 0) sc.rss0 = ee;
   }
 }
 
@@ -1173,7 +1189,7 @@ static_assert(kWarpTri % 2 == 0 && WarpLayout::Y % 2 == 0, "16-byte copies of th
 
 struct WarpScalars {
   static constexpr int kLd = kWarpM;  // leading dimension of the m x m matrices
-  double beta, v0, score, rss, edf, yy;
+  double beta, v0, score, rss, edf, rss0;  // rss0 = |y - Q Q'y|^2
   double lam[kWarpM];
   double log_sp[kWarpM];
   double trial[kWarpM];
@@ -1438,16 +1454,17 @@ __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, 
   double* wg = sm + L::WG;
   for (int c = lane; c < q; c += 32) g[c] = warp_column_dot(Y, c, y0);
   __syncwarp();
+  // RSS = |y - Q y0|^2 + |y0 - W g|^2: sums of squares, no cancellation
   double gg = 0.0;
   for (int i = lane; i < q; i += 32) {
     const double s = warp_dot(Y + packed_row(i, 0) + i, g + i, 1, q - i);
     wg[i] = s;
-    gg += g[i] * g[i] * -2.0 + s * s;
+    const double d = y0[i] - s;
+    gg += d * d;
   }
   const double part = warp_sum(gg);
   if (lane == 0) {
-    double rss = sc.yy + part;
-    if (rss < 0.0) rss = 0.0;
+    const double rss = sc.rss0 + part;
     const double delta = static_cast<double>(n) - edf;
     sc.rss = rss;
     sc.edf = edf;
@@ -1682,11 +1699,17 @@ __device__ __noinline__ void warp_fit_setup(const DesignDev* __restrict__ design
       if (lane == 0 && c0 + u < q) y0[c0 + u] = v;
     }
   }
+  __syncwarp();
   {
-    double yy = 0.0;
-    for (int i = lane; i < n; i += 32) yy += y[i] * y[i];
-    yy = warp_sum(yy);
-    if (lane == 0) sc.yy = yy;
+    double ee = 0.0;  // rss0 = |y - Q y0|^2
+    for (int i = lane; i < n; i += 32) {
+      double f = 0.0;
+      for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * y0[c];
+      const double e = y[i] - f;
+      ee += e * e;
+    }
+    ee = warp_sum(ee);
+    if (lane == 0) sc.rss0 = ee;
   }
   *jb0_out = jb0;
   *jb1_out = jb1;

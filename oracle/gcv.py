@@ -27,6 +27,7 @@ Residuals at the selected lambda use the same augmented SVD
 import math
 
 import numpy as np
+from scipy.linalg import solve_triangular
 
 EPS = np.finfo(np.float64).eps
 RANK_TOL = math.sqrt(EPS)  # 1.4901161193847656e-8
@@ -83,7 +84,11 @@ class Prepared:
 
     def response(self, y):
         y = np.asarray(y, dtype=np.float64)
-        out = {"y": y, "y0": self.Q.T @ y, "yy": float(np.dot(y, y))}
+        y0 = self.Q.T @ y
+        e0 = y - self.Q @ y0
+        # rss0 = |y - Q Q'y|^2: the part of y outside the design's span, summed
+        # directly so RSS never comes from |y|^2 minus a nearly equal quantity
+        out = {"y": y, "y0": y0, "yy": float(np.dot(y, y)), "rss0": float(np.dot(e0, e0))}
         if self.m == 1:
             out["z"] = self.rhs_transform @ (self.X.T @ y)
         return out
@@ -101,23 +106,21 @@ def _hat(log_sp, e):
     return 1.0 / (1.0 + math.exp(c))
 
 
-def single_objective(log_sp, e, z, yy, n):
-    lin = quad = edf = rg = rh = dg = dh = 0.0
+def single_objective(log_sp, e, z, rss0, n):
+    """GCV pieces at log_sp; RSS = rss0 + sum (1 - h_k)^2 z_k^2 (|z| = |Q'y|)."""
+    lin = edf = rg = rh = dg = dh = 0.0
     for ek, zk in zip(e, z):
         h = _hat(log_sp, ek)
         z2 = zk * zk
         omh = 1.0 - h
         w = h * omh
-        lin += h * z2
-        quad += h * h * z2
+        lin += omh * omh * z2
         edf += h
         rg += 2.0 * h * omh * omh * z2
         rh += 2.0 * h * omh * omh * (3.0 * h - 1.0) * z2
         dg += w
         dh -= w * (1.0 - 2.0 * h)
-    rss = yy - 2.0 * lin + quad
-    if rss < 0.0 and math.isfinite(rss):
-        rss = 0.0
+    rss = rss0 + lin
     rdf = n - edf
     if not (math.isfinite(rss) and math.isfinite(edf)) or rss <= 0.0 or rdf <= 1e-8:
         return {"valid": False, "rss": rss, "edf": edf, "score": math.inf}
@@ -131,11 +134,11 @@ def single_objective(log_sp, e, z, yy, n):
 def optimize_single(prep, resp):
     e = prep.spec_values
     z = resp["z"]
-    yy = resp["yy"]
+    rss0 = resp["rss0"]
     n = prep.n
     max_half = 15
     log_sp = math.log(prep.initial_sp[0])
-    cur = single_objective(log_sp, e, z, yy, n)
+    cur = single_objective(log_sp, e, z, rss0, n)
     if not cur["valid"]:
         raise ValueError("non-finite single-penalty objective")
     min_score = cur["score"]
@@ -162,7 +165,7 @@ def optimize_single(prep, resp):
                 step = steep
                 src_newton = False
             trial_ls = log_sp + step
-            trial = single_objective(trial_ls, e, z, yy, n)
+            trial = single_objective(trial_ls, e, z, rss0, n)
             calls += 1
             pred = cur["gradient"] * step + 0.5 * cur["hessian"] * step * step
             resolution = 8.0 * EPS * (1.0 + abs(min_score))
@@ -206,7 +209,7 @@ def optimize_single(prep, resp):
     direction = 1.0 if cur["gradient"] < 0.0 else -1.0
     for _ in range(5):
         trial_ls = log_sp + direction * 2.0
-        trial = single_objective(trial_ls, e, z, yy, n)
+        trial = single_objective(trial_ls, e, z, rss0, n)
         calls += 1
         if not (trial["valid"] and trial["score"] < min_score):
             break
@@ -221,7 +224,7 @@ def optimize_single(prep, resp):
         if abs(step) > POLISH_MAX_STEP:
             break
         log_sp = log_sp + step
-        cur = single_objective(log_sp, e, z, yy, n)
+        cur = single_objective(log_sp, e, z, rss0, n)
         calls += 1
         if abs(step) <= POLISH_DONE:
             break
@@ -244,9 +247,8 @@ def multi_core(prep, resp, log_sp):
     U1, V, d, lam = _augmented_svd(prep, log_sp)
     y1 = U1.T @ resp["y0"]
     Uy = U1 @ y1
-    rss = resp["yy"] - 2.0 * float(y1 @ y1) + float(Uy @ Uy)
-    if rss < 0.0:
-        rss = 0.0
+    d0 = resp["y0"] - Uy
+    rss = resp["rss0"] + float(d0 @ d0)
     edf = float(np.sum(U1 * U1))
     delta = prep.n - edf
     if not (math.isfinite(rss) and math.isfinite(edf)) or delta <= 1e-8:
@@ -377,6 +379,88 @@ def optimize_multi(prep, resp, max_half=25):
             "edf": cur["edf"], "iterations": it, "calls": calls}
 
 
+def qr_core(prep, resp, log_sp):
+    """V at rho through the Householder factor of the stacked system.
+
+    Ra (LAPACK QR of [R; B], B the sqrt(lambda)-scaled penalty roots) has
+    Ra'Ra = X'X + S_lambda; W = R Ra^-1, EDF = |W|_F^2, g = W'y0,
+    RSS = rss0 + |y0 - W g|^2.  Householder QR keeps each column's relative
+    accuracy however the rows are scaled, while the SVD of the same stack is
+    accurate only relative to its largest singular value (about sqrt(lambda)):
+    with one smooth near lambda = e^25 the SVD route's gradient carries
+    relative errors near 1e-12 and this one near 1e-15.  Used for the terminal
+    polish, whose purpose is the stationary point itself."""
+    lam = np.exp(np.asarray(log_sp, dtype=np.float64))
+    B = np.vstack([math.sqrt(l) * r.T for l, r in zip(lam, prep.roots)])
+    Ra = np.linalg.qr(np.vstack([prep.R, B]), mode="r")
+    Wt = solve_triangular(Ra, prep.R.T, trans="T")  # W' = Ra^-T R'
+    W = Wt.T
+    y0 = resp["y0"]
+    g = Wt @ y0
+    Wg = W @ g
+    d0 = y0 - Wg
+    rss = resp["rss0"] + float(d0 @ d0)
+    edf = float(np.sum(W * W))
+    delta = prep.n - edf
+    if not (math.isfinite(rss) and math.isfinite(edf)) or delta <= 1e-8:
+        raise ValueError("invalid multi-penalty objective")
+    return {"Ra": Ra, "W": W, "g": g, "Wg": Wg, "lam": lam, "rss": rss, "edf": edf,
+            "score": prep.n * rss / (delta * delta), "log_sp": np.array(log_sp, dtype=np.float64)}
+
+
+def qr_derivatives(prep, core):
+    """Gradient and Hessian of V in rho from qr_core's factor.
+
+    With T = Ra^-T [root_1 .. root_m], a = T'g, b = T'(g - W'W g),
+    C = T'T and D = (WT)'(WT): d delta_j = lam_j sum_{a in j} D_aa,
+    d rss_j = 2 lam_j sum_{a in j} a_a b_a, and the second derivatives are the
+    block sums sum C.D, a'Da, b'Ca, a'Cb over each pair of penalty blocks --
+    the quantities of multi_derivatives in the Householder basis."""
+    lam, W, g = core["lam"], core["W"], core["g"]
+    m = prep.m
+    roots = np.hstack(prep.roots)
+    blk = np.concatenate([np.full(r.shape[1], j) for j, r in enumerate(prep.roots)])
+    T = solve_triangular(core["Ra"], roots, trans="T")
+    e1 = g - W.T @ core["Wg"]
+    a = T.T @ g
+    b = T.T @ e1
+    WT = W @ T
+    C = T.T @ T
+    D = WT.T @ WT
+    sel = [blk == j for j in range(m)]
+    ddelta = np.array([lam[j] * float(np.sum(np.diag(D)[sel[j]])) for j in range(m)])
+    drss = np.array([2.0 * lam[j] * float(np.sum(a[sel[j]] * b[sel[j]])) for j in range(m)])
+    d2delta = np.zeros((m, m))
+    d2rss = np.zeros((m, m))
+    for i in range(m):
+        for j in range(i + 1):
+            Cij = C[np.ix_(sel[i], sel[j])]
+            Dij = D[np.ix_(sel[i], sel[j])]
+            ai, aj, bi, bj = a[sel[i]], a[sel[j]], b[sel[i]], b[sel[j]]
+            ll = lam[i] * lam[j]
+            dd = -2.0 * ll * float(np.sum(Cij * Dij))
+            rr = 2.0 * ll * (float(ai @ Dij @ aj) - float(bi @ Cij @ aj) - float(ai @ Cij @ bj))
+            if i == j:
+                dd += ddelta[i]
+                rr += drss[i]
+            d2delta[i, j] = d2delta[j, i] = dd
+            d2rss[i, j] = d2rss[j, i] = rr
+    n = prep.n
+    delta = n - core["edf"]
+    rss = core["rss"]
+    s1 = n / (delta * delta)
+    s2 = 2.0 * s1 * rss / delta
+    grad = s1 * drss - s2 * ddelta
+    hess = np.zeros((m, m))
+    for i in range(m):
+        for j in range(i + 1):
+            v = (-2.0 * s1 / delta * (ddelta[j] * drss[i] + ddelta[i] * drss[j])
+                 + s1 * d2rss[i, j] + 3.0 * s2 / delta * ddelta[i] * ddelta[j]
+                 - s2 * d2delta[i, j])
+            hess[i, j] = hess[j, i] = v
+    return grad, hess
+
+
 def polish_newton(prep, resp, log_sp, cur):
     """Terminal Newton polish of the selected point.
 
@@ -386,10 +470,13 @@ def polish_newton(prep, resp, log_sp, cur):
     POLISH_CURVATURE * V (smooths pushed to the boundary have none and stay
     put) move the point to the stationary point itself; a step larger than
     POLISH_MAX_STEP, or a sub-Hessian that is not positive definite, leaves the
-    point as selected.  Returns (rho, core, evaluations)."""
+    point as selected.  The derivatives come from qr_core / qr_derivatives,
+    accurate where a smooth sits at a very large lambda.
+    Returns (rho, core, evaluations)."""
     extra = 0
+    cur = qr_core(prep, resp, log_sp)
     for _ in range(POLISH_STEPS):
-        g, H = multi_derivatives(prep, cur)
+        g, H = qr_derivatives(prep, cur)
         act = [j for j in range(prep.m) if H[j, j] > POLISH_CURVATURE * cur["score"]]
         if not act:
             break
@@ -403,7 +490,7 @@ def polish_newton(prep, resp, log_sp, cur):
             break
         log_sp = log_sp.copy()
         log_sp[act] += d
-        cur = multi_core(prep, resp, log_sp)
+        cur = qr_core(prep, resp, log_sp)
         extra += 1
         if np.max(np.abs(d)) <= POLISH_DONE:
             break

@@ -8,6 +8,7 @@ Workload: the single-level CI batch -- n=500, p=50 nonlinear SEM (edge prob
 A step is one pass of the whole batch (fit, residuals, statistics, p-values).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --profile-once [--method dcc.gamma]   # one replay, for ncu
 
 Prints one JSON line.  ``value``: batched tests/s with every input resident in
 HBM (CUDA events on the engine stream over exactly K replays of the captured
@@ -15,8 +16,16 @@ level graph, max over ranks).  ``e2e``: the public call fkpc_ci_level_batch
 with host data in and records out (design set-up, uploads and downloads
 inside the timed region).  ``plain``: the plain per-test GPU form (one launch
 set and a synchronisation per test) on a sample of the same batch.
+``hsic_gamma``: the same batch with hsic.gamma, timed the same way.
+``parity``: per-stage error of this run's records (dcc.gamma, hsic.gamma)
+and residuals against the oracle's records for the whole batch, read from
+the committed fixture ``tests/golden/level500x50_oracle.npz``.
 ``--impl reference`` times the reference algorithm's CPU restatement (the
-oracle) on the host cores with a bounded sample per step.
+oracle) on the host cores: every step is the same stratified sample of the
+batch (every 16th triple) that ``cpu_baseline`` times.
+``--profile-once`` prepares the batch, replays its launch sequence once as
+warm-up and once more, then each stage alone: the command the ncu summaries
+under profiles/ capture.
 """
 import argparse
 import json
@@ -53,7 +62,10 @@ def parse():
     ap.add_argument("--count", type=int, default=4096)
     ap.add_argument("--plain-sample", type=int, default=256)
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-stride", type=int, default=16)
+    ap.add_argument("--profile-once", action="store_true")
+    ap.add_argument("--method", default="dcc.gamma", choices=["dcc.gamma", "hsic.gamma"])
+    ap.add_argument("--no-skeleton", action="store_true")
     return ap.parse_args()
 
 
@@ -157,52 +169,72 @@ def _oracle_chunk(payload):
     """Worker: oracle p-values for a list of triples (spawned process)."""
     sys.path.insert(0, ROOT)
     from oracle import skeleton
-    X, triples = payload
+    X, triples, method = payload
     cache = skeleton.ResidualCache(X)
-    return [skeleton.ci_pvalue(cache, "dcc.gamma", x, y, S) for (x, y, S) in triples]
+    return [skeleton.ci_pvalue(cache, method, x, y, S) for (x, y, S) in triples]
 
 
-def skeleton_351x48(device, cores):
-    """Full default-Inf dcc.gamma skeleton on the n=351, p=48 SEM through the
-    public facade (wall seconds), and the oracle's rate on a sample of the
-    same run's level-1 tests, extrapolated to the run's logical test count."""
-    import fastkpc_b200 as fk
-    from fastkpc_b200 import workloads
-    X = workloads.skeleton_351x48()
-    t0 = time.perf_counter()
-    out = fk.fastkpc_compatible_cuda_skeleton(X, 0.1, options={"numCol": 35, "trace_level": "logical",
-                                                               "device": device})
-    wall = time.perf_counter() - t0
-    tasks = out["tasks"]
-    lvl1 = [(int(tasks["x"][k]), int(tasks["y"][k]), list(tasks["S"][k]))
-            for k in range(len(tasks["level"])) if tasks["level"][k] == 1]
-    rate, count, dt = cpu_oracle_rate(X, lvl1, budget_s=5.0, cores=cores)
-    total = int(sum(out["n_edgetests"]))
-    return {"wall_s": wall, "n_edgetests": out["n_edgetests"], "logical_tests": total,
-            "edges": int(out["adjacency"].sum() // 2), "device_ms": out["summary"]["stages"]["device_ms"],
-            "setup_ms": out["summary"]["stages"]["setup_ms"],
-            "cpu_estimate_s": total / rate, "cpu_cores": cores,
-            "cpu_sample": f"oracle on {count} level-1 tests of this run in {cores} processes ({dt:.1f} s), "
-                          f"rate extrapolated to all {total} logical tests",
-            "data": "synthetic SEM n=351 p=48 edge prob 0.1, max in-degree 8, seed 3"}
-
-
-def cpu_oracle_rate(X, triples, budget_s, cores):
-    """Oracle throughput on the host cores over a bounded sample (tests/s)."""
+def _oracle_pool(cores):
     import multiprocessing as mp
     for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
         os.environ[var] = "1"  # one BLAS thread per worker process: the pool supplies the parallelism
-    ctx = mp.get_context("spawn")
-    per = max(1, int(math.ceil(budget_s * 4.0)))  # ~0.25 s per test per core on this workload
-    sample = triples[:min(len(triples), per * cores)]
-    chunks = [sample[i::cores] for i in range(cores)]
-    chunks = [c for c in chunks if c]
-    with ctx.Pool(len(chunks)) as pool:
-        pool.map(_oracle_chunk, [(X, [c[0]]) for c in chunks])  # import / start-up outside the timing
-        t0 = time.perf_counter()
-        pool.map(_oracle_chunk, [(X, c) for c in chunks])
-        dt = time.perf_counter() - t0
-    return len(sample) / dt, len(sample), dt
+    return mp.get_context("spawn").Pool(cores)
+
+
+def cpu_oracle_time(pool, X, triples, cores, method="dcc.gamma"):
+    """Seconds the oracle takes for ``triples`` on ``cores`` worker processes."""
+    chunks = [c for c in (triples[i::cores] for i in range(cores)) if c]
+    t0 = time.perf_counter()
+    pool.map(_oracle_chunk, [(X, c, method) for c in chunks])
+    return time.perf_counter() - t0
+
+
+def cpu_sample(triples, stride):
+    """The stratified CPU sample of a batch: every ``stride``-th triple (the
+    batch's |S| mix in the same proportions)."""
+    return triples[::stride]
+
+
+def skeleton_rows(device, cores, pool):
+    """Full default-Inf skeletons on the n=351, p=48 SEM through the public
+    facade: hsic.gamma then dcc.gamma, on each seed of
+    fastkpc_b200.workloads.SKELETON_351X48_SEEDS.  The oracle's CPU time is
+    estimated level by level: a sample of every level's logical tests is
+    timed and scaled by that level's count."""
+    import fastkpc_b200 as fk
+    from fastkpc_b200 import workloads
+    rows = []
+    for seed in workloads.SKELETON_351X48_SEEDS:
+        X = workloads.skeleton_351x48(seed)
+        for method in ("hsic.gamma", "dcc.gamma"):
+            t0 = time.perf_counter()
+            out = fk.fastkpc_compatible_cuda_skeleton(X, 0.1, options={
+                "numCol": 35, "trace_level": "logical", "device": device, "ci_method": method})
+            wall = time.perf_counter() - t0
+            tasks = out["tasks"]
+            levels = np.asarray(tasks["level"])
+            est, sampled = 0.0, 0
+            for lv in range(len(out["n_edgetests"])):
+                ids = np.nonzero(levels == lv)[0]
+                if len(ids) == 0:
+                    continue
+                take = ids[np.linspace(0, len(ids) - 1, min(len(ids), 2 * cores)).astype(int)]
+                sample = [(int(tasks["x"][k]), int(tasks["y"][k]), list(tasks["S"][k])) for k in take]
+                dt = cpu_oracle_time(pool, X, sample, cores, method)
+                est += dt / len(sample) * len(ids)
+                sampled += len(sample)
+            total = int(sum(out["n_edgetests"]))
+            rows.append({"seed": seed, "ci_method": method, "wall_s": wall, "n_edgetests": out["n_edgetests"],
+                         "max_level": len(out["n_edgetests"]) - 1, "logical_tests": total,
+                         "edges": int(out["adjacency"].sum() // 2),
+                         "device_ms": out["summary"]["stages"]["device_ms"],
+                         "setup_ms": out["summary"]["stages"]["setup_ms"],
+                         "cpu_estimate_s": est, "cpu_cores": cores,
+                         "cpu_sample": f"oracle on {sampled} logical tests spread over every level "
+                                       f"({2 * cores} per level at most) in {cores} processes; each level's "
+                                       f"time per test scaled by its count",
+                         "data": f"synthetic SEM n=351 p=48 edge prob 0.1, max in-degree 8, seed {seed}"})
+    return rows
 
 
 def host_cores():
@@ -220,31 +252,67 @@ def run_reference(args, world, rank):
         return
     X, triples = workloads.level_batch_500x50(count=args.count)
     cores = host_cores()
-    per_step = 2 * cores
-    rates = []
-    offset = 0
-    for step in range(args.warmup + args.steps):
-        sample = [triples[(offset + i) % len(triples)] for i in range(per_step)]
-        offset += per_step
-        rate, count, dt = cpu_oracle_rate(X, sample, budget_s=per_step / cores / 4.0, cores=cores)
-        if step >= args.warmup:
-            rates.append((count, dt))
-    total = sum(c for c, _ in rates)
-    secs = sum(d for _, d in rates)
-    value = total / secs
+    sample = cpu_sample(triples, args.cpu_stride)
+    secs = []
+    with _oracle_pool(cores) as pool:
+        pool.map(_oracle_chunk, [(X, sample[i:i + 1], "dcc.gamma") for i in range(cores)])  # start-up
+        for step in range(args.warmup + args.steps):
+            dt = cpu_oracle_time(pool, X, sample, cores)
+            if step >= args.warmup:
+                secs.append(dt)
+    value = len(sample) * len(secs) / sum(secs)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(1, args.steps),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": WORKLOAD, "n": 500, "p": 50, "triples": args.count,
-                                              "ci_method": "dcc.gamma", "sample_per_step": per_step},
+                                              "ci_method": "dcc.gamma", "sample_per_step": len(sample)},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{per_step} triples per step of the {args.count}-triple batch, "
-                                       f"numpy oracle restatement in {cores} spawned processes"},
+                             "sample": f"every {args.cpu_stride}th triple of the {args.count}-triple batch "
+                                       f"({len(sample)} triples) per step, numpy oracle restatement in "
+                                       f"{cores} spawned processes"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------ our arm
+
+STAGE_NAMES = ["fit_single", "fit_multi_small", "fit_multi_large", "dcov_components", "dcov_pairs",
+               "lowrank_eigen", "lowrank_pairs"]
+HSIC_STAGES = ["fit_single", "fit_multi_small", "fit_multi_large", "hsic_components", "hsic_pairs"]
+
+
+def profile_once(args):
+    """Prepare the batch, replay it once as warm-up and once more, then each
+    stage alone; exit status 0 only when every record is valid."""
+    import fastkpc_b200 as fk
+    from fastkpc_b200 import workloads
+    X, triples = workloads.level_batch_500x50(count=args.count)
+    batch = fk.StagedBatch(X, triples, ci_method=args.method, device=0)
+    batch.execute(1)
+    ms = batch.execute(1)
+    recs, st = batch.collect()
+    ok = bool(np.all(recs["status"] == 0))
+    names = STAGE_NAMES if args.method == "dcc.gamma" else HSIC_STAGES
+    stages = {name: batch.time_stage(name, repeats=2)[0] for name in names}
+    print(json.dumps({"count": args.count, "method": args.method, "device_ms": ms, "stages_ms": stages,
+                      "fits": st["targets"], "fit_evaluations": st["fit_evaluations"],
+                      "launches_per_replay": st["kernel_launches"], "ok": ok}))
+    return 0 if ok else 1
+
+
+def level_parity(X, triples, dcc, hsic, device):
+    """Per-stage error of this run against the oracle fixture of the batch."""
+    import fastkpc_b200 as fk
+    from tests.golden import level_report
+    fx = level_report.load()
+    if level_report.triples(fx) != triples:
+        return {"skipped": "the batch is not the fixture's (4096 triples, seed 2)"}
+    resid, lsp, status = fk.regress_batch(X, level_report.fits(fx), max_penalties=4, device=device)
+    rep = level_report.report(fx, dcc=dcc, hsic=hsic, residuals=resid, log_sp=lsp)
+    rep["fit_status_failures"] = int(np.sum(status != 0))
+    rep["source"] = "tests/golden/level500x50_oracle.npz (oracle over all 4096 triples and 6005 fits)"
+    return rep
+
 
 def run_ours(args, world, rank, local, pg):
     import fastkpc_b200 as fk
@@ -266,17 +334,24 @@ def run_ours(args, world, rank, local, pg):
     value = total_tests / (ms / 1e3)
 
     # roofline of the dominant kernel (replayed alone, CUDA events)
-    stages = ["fit_single", "fit_multi_small", "fit_multi_large", "dcov_components", "dcov_pairs",
-              "lowrank_eigen", "lowrank_pairs"]
-    timed = {}
-    for s in stages:
-        avg, fl = batch.time_stage(s, repeats=3)
-        timed[s] = (avg, fl)
+    timed = {s: batch.time_stage(s, repeats=3) for s in STAGE_NAMES}
     dominant = max(timed, key=lambda s: timed[s][0])
     peak = fk.measure_fp64_peak(local)
     avg_ms, flops = timed[dominant]
     achieved = flops / (avg_ms * 1e-3) / 1e12 if flops > 0 else None
     traffic = FIT_STAGE_TRAFFIC["bytes"] if dominant == "fit_multi_small" and args.count == 4096 else None
+
+    # the same batch with hsic.gamma
+    hbatch = fk.StagedBatch(X, triples, ci_method="hsic.gamma", device=local)
+    hbatch.execute(args.warmup)
+    barrier(pg)
+    hms = hbatch.execute(args.steps)
+    barrier(pg)
+    hms = max_over_ranks(pg, hms, local)
+    hrecs, hst = hbatch.collect()
+    if not np.all(hrecs["status"] == 0):
+        raise RuntimeError("hsic.gamma batch returned failing records")
+    hvalue = sum_over_ranks(pg, float(args.count * args.steps), local) / (hms / 1e3)
 
     # plain per-test form on a sample of the same batch (designs resident)
     sample = triples[:args.plain_sample]
@@ -305,8 +380,12 @@ def run_ours(args, world, rank, local, pg):
     line = None
     if rank == 0:
         cores = host_cores()
-        skel = skeleton_351x48(local, cores)
-        cpu_rate, cpu_n, cpu_dt = cpu_oracle_rate(X, triples, args.cpu_seconds / 4.0, cores)
+        parity = level_parity(X, triples, recs, hrecs, local)
+        csample = cpu_sample(triples, args.cpu_stride)
+        with _oracle_pool(cores) as pool:
+            pool.map(_oracle_chunk, [(X, csample[i:i + 1], "dcc.gamma") for i in range(cores)])  # start-up
+            cpu_dt = cpu_oracle_time(pool, X, csample, cores)
+            skel = [] if args.no_skeleton else skeleton_rows(local, cores, pool)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -320,23 +399,26 @@ def run_ours(args, world, rank, local, pg):
                        "lowrank_steps_mean": st["lowrank_steps_mean"]},
             "plain": {"value": plain_rate, "unit": UNIT, "sample_tests": len(sample),
                       "batched_over_plain": value / world / plain_rate},
-            "stages_ms": {s: timed[s][0] for s in stages},
+            "hsic_gamma": {"value": hvalue, "unit": UNIT, "ms_per_step": hms / args.steps},
+            "stages_ms": {s: timed[s][0] for s in STAGE_NAMES},
             "roofline": {"bound": "fp64", "kernel": dominant, "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "traffic_unit": "bytes per launch",
                          "traffic_source": FIT_STAGE_TRAFFIC["source"] if traffic else None,
                          "peak_source": "measured live: FP64 FMA probe (no FP64 figure in MEASURED_PEAKS.json)",
                          "flops_per_launch": flops, "avg_launch_ms": avg_ms},
-            "cpu_baseline": {"value": cpu_rate, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"first {cpu_n} triples of the batch, numpy oracle in {cores} spawned "
-                                       f"processes ({cpu_dt:.1f} s)"},
+            "parity": parity,
+            "cpu_baseline": {"value": len(csample) / cpu_dt, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"every {args.cpu_stride}th triple of the batch ({len(csample)} triples), "
+                                       f"numpy oracle in {cores} spawned processes ({cpu_dt:.1f} s); the "
+                                       f"reference arm times the same sample"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": e2e_stats["h2d_bytes"],
                     "d2h_bytes_per_step": e2e_stats["d2h_bytes"], "steps": len(e2e_t), "warmup_calls": 1,
                     "setup_ms": e2e_stats["setup_ms"], "upload_ms": e2e_stats["upload_ms"],
                     "device_ms": e2e_stats["device_ms"], "download_ms": e2e_stats["download_ms"],
                     "call_ms": e2e_stats["total_ms"], "wall_s": statistics.median(e2e_t)},
             "skeleton_351x48": skel,
-            "gpu_launches": int(st["kernel_launches"]) * args.steps,
+            "gpu_launches": int(st["kernel_launches"] + hst["kernel_launches"]) * args.steps,
             "clocks": clocks_s,
         }
     return line
@@ -344,6 +426,8 @@ def run_ours(args, world, rank, local, pg):
 
 def main():
     args = parse()
+    if args.profile_once:
+        sys.exit(profile_once(args))
     world, rank, local, pg = dist_setup(args)
     try:
         if args.impl == "reference":

@@ -63,6 +63,23 @@ def skeleton_351x48(seed=3):
     return nonlinear_sem(351, 48, 0.1, seed, max_in_degree=8)[0]
 
 
+def deep_skeleton_seed(levels_of, min_level=8, first=1, last=1000):
+    """The first seed in [first, last] whose n=351, p=48 SEM (edge prob 0.1,
+    at most 8 parents) gives a default-Inf skeleton that runs level
+    ``min_level`` (a conditioning set of that size is tested), else the
+    seed whose skeleton runs the most levels (the first of equals).
+    ``levels_of(X)`` returns the number of levels a skeleton on X executed
+    (levels 0 .. L-1).  Returns (seed, levels)."""
+    best = (None, -1)
+    for seed in range(first, last + 1):
+        levels = int(levels_of(skeleton_351x48(seed)))
+        if levels - 1 >= min_level:
+            return seed, levels
+        if levels > best[1]:
+            best = (seed, levels)
+    return best
+
+
 def uneven_batch_500x64(seed=4, count=16384):
     """n=500, p=64; |S| ~ geometric(0.35) truncated at 12 (permutation batch)."""
     X, _ = nonlinear_sem(500, 64, 0.08, seed)
@@ -87,3 +104,8 @@ def adjoint_targets_1000(seed=5, count=2048):
         cols = rs.choice(50, size=k + 1, replace=False)
         fits.append((int(cols[0]), sorted(int(c) for c in cols[1:])))
     return X, fits
+
+
+# Seeds of the n=351, p=48 full-skeleton rows: the deepest-skeleton seed
+# (deep_skeleton_seed) and seed 3.
+SKELETON_351X48_SEEDS = (3,)

@@ -439,3 +439,21 @@ def test_empty_batches_return_no_records(lib, method):
     with pytest.raises(fk.FkpcError) as e:
         fk.StagedBatch(X, [], ci_method=method, **kw)
     assert e.value.status == 1
+
+
+def test_near_exact_fit_keeps_a_positive_rss(lib):
+    """Variable 7 of the n=351, p=48 SEM with seed 80 is almost exactly a
+    smooth of variable 34 (RSS about 4e-13 against |y|^2 = 350).  RSS formed
+    as |y|^2 - 2 g'g + |Wg|^2 cancels to rounding noise there; the fit forms
+    it as |y - Q Q'y|^2 + |Q'y - W g|^2 and must succeed, with the oracle's
+    residual to within 1e-12 of max |y| (the residual itself is at the
+    rounding level of y, so a relative bar on it does not apply)."""
+    X, _ = workloads.nonlinear_sem(351, 48, 0.1, 80, max_in_degree=8)
+    resid, lsp, status = fk.regress_batch(X, [(7, [34])])
+    assert status[0] == 0
+    prep = gcv.Prepared(tprs.design(X, [34]))
+    r, info = gcv.fit(prep, X[:, 7])
+    assert info["rss"] > 0.0
+    assert np.max(np.abs(resid[:, 0] - r)) <= 1e-12 * np.max(np.abs(X[:, 7]))
+    rec, _ = fk.ci_level_batch(X, [(7, 12, [34]), (12, 7, [34])], ci_method="dcc.gamma")
+    assert np.all(rec["status"] == 0)

@@ -116,3 +116,85 @@ def test_oracle_reproduces_500x50_dcc_gamma_skeleton(dev500, dev500_trace):
         if (i, j) in ref_sep:
             assert sorted(s) == ref_sep[(i, j)]
     assert all(((i, j) in out["sepsets"]) for (i, j) in ref_sep)
+
+
+def test_level_fixture_is_the_workload_and_the_oracle():
+    """The committed 500x50 level-batch fixture: its triples are the workload
+    generator's, and the oracle re-run on a sample reproduces its records."""
+    from threadpoolctl import threadpool_limits
+    from fastkpc_b200 import workloads
+    from tests.golden import level_report
+    fx = level_report.load()
+    X, triples = workloads.level_batch_500x50(count=len(fx["x"]))
+    assert level_report.triples(fx) == triples
+    cache = skeleton.ResidualCache(X)
+    # the fixture was written with one BLAS thread per process; threaded BLAS
+    # reductions round differently and can move magic's path in the last bits
+    with threadpool_limits(limits=1):
+        for k in (0, 1, 2, 100, 2048, 4095):
+            x, y, S = triples[k]
+            rx, ry = cache.residual(x, S), cache.residual(y, S)
+            p, pe, g = stats.dcc_gamma_decision_p(rx, ry, 35)
+            assert abs(p - fx["dcc_p"][k]) <= 1e-13 and abs(pe - fx["dcc_p_exact"][k]) <= 1e-13
+            assert g == fx["guarded"][k]
+            assert abs(stats.hsic_gamma(rx, ry, 1.0, 35)["p_value"] - fx["hsic_p"][k]) <= 1e-13
+    # the report of the fixture against itself is all zeros
+    g = fx["guarded"]
+    rec = {"flags": g.astype(np.int64),
+           "statistic": np.where(g, fx["dcc_stat_lowrank"], fx["dcc_stat_exact"]),
+           "mean": np.where(g, fx["dcc_mean_lowrank"], fx["dcc_mean_exact"]),
+           "variance": np.where(g, fx["dcc_var_lowrank"], fx["dcc_var_exact"]),
+           "p_exact": fx["dcc_p_exact"], "p_value": fx["dcc_p"]}
+    rep = level_report.report(fx, dcc=rec)
+    assert rep["dcc_alpha_flips"] == 0 and rep["dcc_p_abs_err_max"] == 0.0 and rep["dcc_stat_rel_err_max"] == 0.0
+
+
+@pytest.mark.slow
+def test_polished_point_is_stationary_in_extended_precision():
+    """Fit 4580 of the 500x50 level batch (|S| = 4, two smooths near
+    lambda = e^23 and e^25): the polished log(lambda) has a relative GCV
+    gradient below 1e-13 when V is evaluated in 30-digit arithmetic (a
+    polish on the SVD route's derivatives stopped where it was 1e-12)."""
+    mp = pytest.importorskip("mpmath")
+    from threadpoolctl import threadpool_limits
+    from fastkpc_b200 import workloads
+    from tests.golden import level_report
+    fx = level_report.load()
+    X, _ = workloads.level_batch_500x50(count=len(fx["x"]))
+    i = 4580
+    t = int(fx["fit_target"][i])
+    S = [int(v) for v in fx["fit_S"][i] if v >= 0]
+    d = tprs.design(X, S)
+    with threadpool_limits(limits=1):
+        _, info = gcv.fit(gcv.Prepared(d), X[:, t])
+    assert np.max(np.abs(info["log_sp"] - fx["fit_log_sp"][i][:len(S)])) < 1e-10
+    mp.mp.dps = 30
+    n, q = d["X"].shape
+    Xm = mp.matrix(d["X"].tolist())
+    XtX = Xm.T * Xm
+    ym = mp.matrix(X[:, t].tolist())
+    Xty = Xm.T * ym
+    yy = (ym.T * ym)[0]
+    blocks = [(mp.matrix(b.tolist()), off) for b, off in zip(d["blocks"], d["offsets"])]
+
+    def V(rho):
+        A = XtX.copy()
+        for (b, off), r in zip(blocks, rho):
+            lam = mp.exp(r)
+            for a in range(b.rows):
+                for c in range(b.cols):
+                    A[off + a, off + c] += lam * b[a, c]
+        Ai = mp.inverse(A)
+        beta = Ai * Xty
+        rss = yy - 2 * (Xty.T * beta)[0] + (beta.T * XtX * beta)[0]
+        edf = sum((Ai * XtX)[k, k] for k in range(q))
+        return n * rss / (n - edf) ** 2
+
+    rho = [mp.mpf(float(v)) for v in info["log_sp"]]
+    h = mp.mpf("1e-8")
+    v0 = V(rho)
+    for j in (0, 3):  # the two well-determined coordinates
+        rp, rm = list(rho), list(rho)
+        rp[j] += h
+        rm[j] -= h
+        assert abs((V(rp) - V(rm)) / (2 * h) / v0) < 1e-13

@@ -20,7 +20,7 @@ import numpy as np
 
 __all__ = [
     "FkpcError", "library_path", "load_library", "fastkpc_compatible_cuda_skeleton",
-    "ci_level_batch", "ci_plain_one", "regress_batch", "stat_batch", "design_export",
+    "ci_level_batch", "ci_plain_one", "regress_batch", "stat_batch", "design_export", "Session",
     "METHODS",
 ]
 
@@ -49,7 +49,15 @@ class Options(ctypes.Structure):
                 ("hsic_sig", ctypes.c_double), ("permutation_replicates", ctypes.c_int),
                 ("has_seed", ctypes.c_int), ("seed", ctypes.c_uint), ("mode", ctypes.c_int),
                 ("collect_trace", ctypes.c_int), ("device", ctypes.c_int), ("strict", ctypes.c_int),
-                ("selection", ctypes.c_int)]
+                ("selection", ctypes.c_int), ("level_graph", ctypes.c_int)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("defer_evaluations", ctypes.c_int), ("split_statistics", ctypes.c_int),
+                ("lowrank_ctas_per_sm", ctypes.c_int), ("tprs_ctas_per_sm", ctypes.c_int)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class CiRecord(ctypes.Structure):
@@ -67,7 +75,8 @@ class StageStats(ctypes.Structure):
                 ("fit_evaluations", ctypes.c_double), ("fit_flops", ctypes.c_double),
                 ("statistic_flops", ctypes.c_double), ("fit_iterations", ctypes.c_double),
                 ("lowrank_components", ctypes.c_int), ("lowrank_steps_max", ctypes.c_int),
-                ("lowrank_steps_mean", ctypes.c_double), ("device_ms", ctypes.c_double)]
+                ("lowrank_steps_mean", ctypes.c_double), ("device_ms", ctypes.c_double),
+                ("designs_built", ctypes.c_int), ("smooths_built", ctypes.c_int)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -105,6 +114,9 @@ _SIGNATURES = {
                                                 ctypes.c_void_p, _P(_P(Result))]),
     "fkpc_ci_level_batch": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, _INT, ctypes.c_int,
                                            _P(Options), _P(CiRecord), _P(StageStats)]),
+    "fkpc_session_load": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "fkpc_session_evaluate": (ctypes.c_int, [_INT, _INT, _INT, _INT, ctypes.c_int, _P(Options), _P(CiRecord),
+                                             _P(StageStats)]),
     "fkpc_ci_plain_one": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _INT,
                                          ctypes.c_int, _P(Options), _P(CiRecord)]),
     "fkpc_regress_batch": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, ctypes.c_int,
@@ -114,6 +126,8 @@ _SIGNATURES = {
     "fkpc_gcv_adjoint": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, ctypes.c_int, _INT, ctypes.c_int,
                                         ctypes.c_int, _DBL, _DBL, _DBL, _DBL, _DBL, ctypes.c_int]),
     "fkpc_gamma_q_eval": (ctypes.c_int, [ctypes.c_int, _DBL, _DBL, ctypes.c_int, _DBL, _INT]),
+    "fkpc_get_tuning": (ctypes.c_int, [ctypes.c_int, _P(Tuning)]),
+    "fkpc_set_tuning": (ctypes.c_int, [ctypes.c_int, _P(Tuning)]),
     "fkpc_batch_prepare": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, _INT, ctypes.c_int,
                                           _P(Options)]),
     "fkpc_batch_execute": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _DBL]),
@@ -168,7 +182,7 @@ def _as_data(data):
 
 def make_options(ci_method="dcc.gamma", alpha=0.1, index=1.0, numCol=35, max_conditioning_size=math.inf,
                  hsic_sig=1.0, replicates=100, seed=None, mode="batched", trace=True, device=0, strict=True,
-                 selection="magic"):
+                 selection="magic", level_graph=False):
     o = Options()
     load_library().fkpc_default_options(ctypes.byref(o))
     if ci_method not in METHODS:
@@ -189,11 +203,12 @@ def make_options(ci_method="dcc.gamma", alpha=0.1, index=1.0, numCol=35, max_con
     if selection not in SELECTIONS:
         raise ValueError(f"unknown selection {selection!r}")
     o.selection = SELECTIONS[selection]
+    o.level_graph = 1 if level_graph else 0
     return o
 
 
 _ALLOWED = {"max_conditioning_size", "index", "numCol", "trace_level", "route", "compatible_cuda_strict",
-            "ci_method", "hsic_params", "permutation_params", "mode", "device"}
+            "ci_method", "hsic_params", "permutation_params", "mode", "device", "level_graph"}
 
 
 def fastkpc_compatible_cuda_skeleton(data, alpha, labels=None, options=None):
@@ -206,8 +221,10 @@ def fastkpc_compatible_cuda_skeleton(data, alpha, labels=None, options=None):
     ``compatible_cuda_strict`` (True), ``ci_method`` ("dcc.gamma",
     "dcc.perm", "hsic.gamma", "hsic.perm"), ``hsic_params`` ({"sig": 1}),
     ``permutation_params`` ({"replicates": 100, "seed": None,
-    "include_observed": True}); plus ``mode`` ("batched" | "plain") and
-    ``device``.
+    "include_observed": True}); plus ``mode`` ("batched" | "plain"),
+    ``device`` and ``level_graph`` (False: each level's batch overlaps its
+    host set-up with the device work; True: set-up first, then the level runs
+    as one captured CUDA graph).
 
     Returns a dict with ``adjacency`` (bool p x p), ``pMax``, ``sepsets``
     (list of p lists; None or the separating set, 0-based), ``n_edgetests``,
@@ -245,7 +262,8 @@ def _skeleton_setup(data, alpha, labels, options):
                      max_conditioning_size=options.get("max_conditioning_size", math.inf),
                      hsic_sig=hsic.get("sig", 1), replicates=perm.get("replicates", 100), seed=perm.get("seed"),
                      mode=options.get("mode", "batched"), trace=trace_level in ("logical", "full"),
-                     device=options.get("device", 0), strict=options.get("compatible_cuda_strict", True))
+                     device=options.get("device", 0), strict=options.get("compatible_cuda_strict", True),
+                     level_graph=options.get("level_graph", False))
     return X, labels, o, method
 
 
@@ -355,6 +373,37 @@ def ci_level_batch(data, tests, ci_method="dcc.gamma", mode="batched", **kw):
                                                 _ptr(vals, ctypes.c_int), len(tests), ctypes.byref(o), out,
                                                 ctypes.byref(st)))
     return _records(out, len(tests)), st.as_dict()
+
+
+class Session:
+    """The data matrix kept loaded on one GPU across batches of CI tests, with
+    its cache of conditioning-set designs (fkpc_session_load /
+    fkpc_session_evaluate): a design is set up once per device, however many
+    batches (skeleton levels) use it.  Any other call that loads data on the
+    same device ends the session."""
+
+    def __init__(self, data, device=0):
+        self.X = _as_data(data)
+        self.device = int(device)
+        n, p = self.X.shape
+        _check(load_library().fkpc_session_load(_ptr(self.X, ctypes.c_double), n, p, self.device))
+
+    def evaluate_raw(self, tests, options):
+        """Records (ctypes array) and stats dict of ``tests`` with a ready
+        ``fkpc_options`` (its ``device`` must be the session's)."""
+        out = (CiRecord * max(1, len(tests)))()
+        st = StageStats()
+        xs, ys, offs, vals = _tests_arrays(tests)
+        _check(load_library().fkpc_session_evaluate(_ptr(xs, ctypes.c_int), _ptr(ys, ctypes.c_int),
+                                                      _ptr(offs, ctypes.c_int), _ptr(vals, ctypes.c_int),
+                                                      len(tests), ctypes.byref(options), out, ctypes.byref(st)))
+        return out, st.as_dict()
+
+    def evaluate(self, tests, ci_method="dcc.gamma", **kw):
+        """(records dict, stage stats dict) of ``[(x, y, S), ...]``."""
+        o = make_options(ci_method=ci_method, device=self.device, **kw)
+        out, st = self.evaluate_raw(tests, o)
+        return _records(out, len(tests)), st
 
 
 def ci_plain_one(data, x, y, S, ci_method="dcc.gamma", **kw):
@@ -486,6 +535,26 @@ def gcv_adjoint(data, target, S, log_lambda, device=0):
                                              _ptr(grad, ctypes.c_double), _ptr(gn, ctypes.c_double),
                                              _ptr(hess, ctypes.c_double), int(device)))
     return {"score": score, "grad": grad, "gn_hessian": gn, "hessian": hess}
+
+
+def get_tuning(device=0):
+    """The engine's schedule choices on ``device`` (dict; see fkpc_tuning)."""
+    t = Tuning()
+    _check(load_library().fkpc_get_tuning(int(device), ctypes.byref(t)))
+    return t.as_dict()
+
+
+def set_tuning(device=0, **changes):
+    """Change some of the engine's schedule choices on ``device``; returns the
+    new settings.  Records never depend on them."""
+    t = Tuning()
+    _check(load_library().fkpc_get_tuning(int(device), ctypes.byref(t)))
+    for name, value in changes.items():
+        if name not in dict(Tuning._fields_):
+            raise ValueError(f"unknown tuning {name!r}")
+        setattr(t, name, int(value))
+    _check(load_library().fkpc_set_tuning(int(device), ctypes.byref(t)))
+    return t.as_dict()
 
 
 def gamma_q(a, x, device=0):

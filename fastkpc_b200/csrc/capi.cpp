@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -44,15 +45,31 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 namespace {
 
-std::mutex g_engine_mu;
-std::map<int, std::unique_ptr<fkpc::Engine>> g_engines;
+// One engine per device, each behind its own mutex: calls on different
+// devices run concurrently (one host thread per GPU), calls on one device
+// are serialised.
+struct EngineSlot {
+  std::mutex mu;
+  std::unique_ptr<fkpc::Engine> eng;
+  uint64_t session = 0;  // load_id of the data fkpc_session_load left loaded (0: none)
+};
+std::mutex g_slots_mu;
+std::map<int, std::unique_ptr<EngineSlot>> g_slots;
 
+EngineSlot& slot_for(int device) {
+  std::lock_guard<std::mutex> lock(g_slots_mu);
+  auto& p = g_slots[device];
+  if (!p) p.reset(new EngineSlot());
+  return *p;
+}
+
+std::mutex& device_mutex(int device) { return slot_for(device).mu; }
+
+// The device's engine; call with device_mutex(device) held.
 fkpc::Engine& engine_for(int device) {
-  auto it = g_engines.find(device);
-  if (it == g_engines.end()) {
-    it = g_engines.emplace(device, std::unique_ptr<fkpc::Engine>(new fkpc::Engine(device))).first;
-  }
-  return *it->second;
+  EngineSlot& s = slot_for(device);
+  if (!s.eng) s.eng.reset(new fkpc::Engine(device));
+  return *s.eng;
 }
 
 int fail(int code, const std::string& msg) {
@@ -183,6 +200,8 @@ void add_stats(fkpc_stage_stats* acc, const fkpc_stage_stats& s) {
   acc->lowrank_steps_max = std::max(acc->lowrank_steps_max, s.lowrank_steps_max);
   acc->lowrank_steps_mean = s.lowrank_steps_mean;
   acc->device_ms += s.device_ms;
+  acc->designs_built += s.designs_built;
+  acc->smooths_built += s.smooths_built;
 }
 
 // Evaluate ``tests`` on the engine in chunks; records in test order.
@@ -201,8 +220,9 @@ void evaluate(fkpc::Engine& eng, const std::vector<fkpc::Test>& tests, const fkp
     const size_t e = std::min(tests.size(), b + chunk);
     std::vector<fkpc::Test> part(tests.begin() + b, tests.begin() + e);
     fkpc_stage_stats st{};
-    if (opt.mode == FKPC_MODE_PLAIN) {
-      eng.prepare(part, opt, rs);
+    const bool perm = opt.ci_method == FKPC_DCC_PERM || opt.ci_method == FKPC_HSIC_PERM;
+    if (opt.mode == FKPC_MODE_PLAIN || (opt.level_graph && !perm)) {
+      eng.prepare(part, opt, rs);  // set-up, then the captured launch sequence
       eng.execute();
     } else {
       eng.run_batch(part, opt, rs);
@@ -483,6 +503,7 @@ void fkpc_default_options(fkpc_options* o) {
   o->device = 0;
   o->strict = 1;
   o->selection = FKPC_SELECT_MAGIC;
+  o->level_graph = 0;
 }
 
 int fkpc_skeleton_run(const double* data, int n, int p, const fkpc_options* options, fkpc_result** out) {
@@ -491,7 +512,7 @@ int fkpc_skeleton_run(const double* data, int n, int p, const fkpc_options* opti
     *out = nullptr;
     validate_options(*options, n, p);
     if (p > 64) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "p must be at most 64");
-    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::lock_guard<std::mutex> lock(device_mutex(options->device));
     auto t0 = std::chrono::steady_clock::now();
     Run run;
     skeleton(data, n, p, *options, &run);
@@ -526,6 +547,29 @@ void fkpc_result_free(fkpc_result* r) {
   std::free(r);
 }
 
+// One batch of tests on the engine's loaded data: records into out.
+void level_batch_on(fkpc::Engine& eng, const int* x, const int* y, const int* s_offsets, const int* s_values,
+                    int count, const fkpc_options& opt, fkpc_ci_record* out, fkpc_stage_stats* stats,
+                    std::chrono::steady_clock::time_point t0) {
+  std::vector<fkpc::Test> tests(count);
+  for (int t = 0; t < count; ++t) {
+    tests[t].x = x[t];
+    tests[t].y = y[t];
+    if (s_offsets[t + 1] < s_offsets[t]) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "s_offsets must be nondecreasing");
+    tests[t].S.assign(s_values + s_offsets[t], s_values + s_offsets[t + 1]);
+  }
+  std::unique_ptr<fkpc::RStream> rs;
+  if (opt.ci_method == FKPC_DCC_PERM || opt.ci_method == FKPC_HSIC_PERM) rs.reset(new fkpc::RStream(opt.seed));
+  std::vector<fkpc_ci_record> rec;
+  fkpc_stage_stats acc{};
+  evaluate(eng, tests, opt, rs.get(), &rec, &acc);
+  std::copy(rec.begin(), rec.end(), out);
+  if (stats) {
+    *stats = acc;
+    stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+}
+
 int fkpc_ci_level_batch(const double* data, int n, int p, const int* x, const int* y, const int* s_offsets,
                         const int* s_values, int count, const fkpc_options* options, fkpc_ci_record* out,
                         fkpc_stage_stats* stats) {
@@ -533,27 +577,39 @@ int fkpc_ci_level_batch(const double* data, int n, int p, const int* x, const in
     if (!data || !options || !out || count < 0 || (count > 0 && (!x || !y || !s_offsets)))
       throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
     validate_options(*options, n, p);
-    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::lock_guard<std::mutex> lock(device_mutex(options->device));
     auto t0 = std::chrono::steady_clock::now();
-    std::vector<fkpc::Test> tests(count);
-    for (int t = 0; t < count; ++t) {
-      tests[t].x = x[t];
-      tests[t].y = y[t];
-      if (s_offsets[t + 1] < s_offsets[t]) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "s_offsets must be nondecreasing");
-      tests[t].S.assign(s_values + s_offsets[t], s_values + s_offsets[t + 1]);
-    }
     auto& eng = engine_for(options->device);
     eng.load(data, n, p);
-    std::unique_ptr<fkpc::RStream> rs;
-    if (options->ci_method == FKPC_DCC_PERM || options->ci_method == FKPC_HSIC_PERM) rs.reset(new fkpc::RStream(options->seed));
-    std::vector<fkpc_ci_record> rec;
-    fkpc_stage_stats acc{};
-    evaluate(eng, tests, *options, rs.get(), &rec, &acc);
-    std::copy(rec.begin(), rec.end(), out);
-    if (stats) {
-      *stats = acc;
-      stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    }
+    level_batch_on(eng, x, y, s_offsets, s_values, count, *options, out, stats, t0);
+  });
+}
+
+int fkpc_session_load(const double* data, int n, int p, int device) {
+  return guarded([&]() {
+    if (!data) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    if (device < 0) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "device must be a CUDA device ordinal");
+    std::lock_guard<std::mutex> lock(device_mutex(device));
+    auto& eng = engine_for(device);
+    eng.load(data, n, p);
+    slot_for(device).session = eng.load_id();
+  });
+}
+
+int fkpc_session_evaluate(const int* x, const int* y, const int* s_offsets, const int* s_values, int count,
+                          const fkpc_options* options, fkpc_ci_record* out, fkpc_stage_stats* stats) {
+  return guarded([&]() {
+    if (!options || !out || count < 0 || (count > 0 && (!x || !y || !s_offsets)))
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    if (options->device < 0) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "device must be a CUDA device ordinal");
+    std::lock_guard<std::mutex> lock(device_mutex(options->device));
+    auto t0 = std::chrono::steady_clock::now();
+    EngineSlot& slot = slot_for(options->device);
+    if (!slot.eng || slot.session == 0 || slot.eng->load_id() != slot.session)
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT,
+                        "no session on this device (fkpc_session_load first; another call loaded other data)");
+    validate_options(*options, slot.eng->n(), slot.eng->p());
+    level_batch_on(*slot.eng, x, y, s_offsets, s_values, count, *options, out, stats, t0);
   });
 }
 
@@ -563,7 +619,7 @@ int fkpc_ci_plain_one(const double* data, int n, int p, int x, int y, const int*
     if (!data || !options || !out || s_count < 0 || (s_count > 0 && !s_values))
       throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
     validate_options(*options, n, p);
-    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::lock_guard<std::mutex> lock(device_mutex(options->device));
     auto& eng = engine_for(options->device);
     eng.load(data, n, p);
     fkpc_options o = *options;
@@ -589,7 +645,7 @@ int fkpc_regress_batch(const double* data, int n, int p, const int* target, cons
     if (o.selection != FKPC_SELECT_MAGIC && o.selection != FKPC_SELECT_GN_NEWTON)
       throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "selection must be FKPC_SELECT_MAGIC or FKPC_SELECT_GN_NEWTON");
     if (count == 0) return;  // nothing to fit: no device work
-    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::lock_guard<std::mutex> lock(device_mutex(o.device));
     auto& eng = engine_for(o.device);
     eng.load(data, n, p);
     std::vector<int> tg(target, target + count);
@@ -606,7 +662,7 @@ int fkpc_stat_batch(const double* residuals, int n, int m, const int* left, cons
       throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
     validate_options(*options, n, std::max(2, m));
     if (count == 0) return;  // no pairs: no device work
-    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::lock_guard<std::mutex> lock(device_mutex(options->device));
     auto& eng = engine_for(options->device);
     eng.load(residuals, n, m);
     eng.statistics(residuals, m, std::vector<int>(left, left + count), std::vector<int>(right, right + count),
@@ -622,7 +678,7 @@ int fkpc_batch_prepare(const double* data, int n, int p, const int* x, const int
     validate_options(*options, n, p);
     if (options->ci_method == FKPC_DCC_PERM || options->ci_method == FKPC_HSIC_PERM)
       throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "the staged form covers the gamma methods");
-    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::lock_guard<std::mutex> lock(device_mutex(options->device));
     std::vector<fkpc::Test> tests(count);
     for (int t = 0; t < count; ++t) {
       tests[t].x = x[t];
@@ -638,7 +694,7 @@ int fkpc_batch_prepare(const double* data, int n, int p, const int* x, const int
 int fkpc_batch_execute(int device, int repeats, double* device_ms) {
   return guarded([&]() {
     if (repeats < 1) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "repeats must be positive");
-    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::lock_guard<std::mutex> lock(device_mutex(device));
     const double ms = engine_for(device).execute_timed(repeats);
     if (device_ms) *device_ms = ms;
   });
@@ -646,14 +702,14 @@ int fkpc_batch_execute(int device, int repeats, double* device_ms) {
 
 int fkpc_batch_collect(int device, fkpc_ci_record* out, fkpc_stage_stats* stats) {
   return guarded([&]() {
-    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::lock_guard<std::mutex> lock(device_mutex(device));
     engine_for(device).collect(out, stats);
   });
 }
 
 int fkpc_batch_time_stage(int device, int stage, int repeats, double* avg_ms, double* flops_per_launch) {
   return guarded([&]() {
-    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::lock_guard<std::mutex> lock(device_mutex(device));
     const double ms = engine_for(device).time_stage(stage, repeats, flops_per_launch);
     if (avg_ms) *avg_ms = ms;
   });
@@ -661,7 +717,7 @@ int fkpc_batch_time_stage(int device, int stage, int repeats, double* avg_ms, do
 
 int fkpc_measure_fp64_peak(int device, double* tflops) {
   return guarded([&]() {
-    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::lock_guard<std::mutex> lock(device_mutex(device));
     const double t = engine_for(device).measure_fp64_peak();
     if (tflops) *tflops = t;
   });
@@ -700,11 +756,29 @@ int fkpc_gcv_adjoint(const double* data, int n, int p, int target, const int* s_
       throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
     if (n <= 5 || p < 2) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "data must be n x p with n > 5, p >= 2");
     if (device < 0) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "device must be a CUDA device ordinal");
-    std::lock_guard<std::mutex> lock(g_engine_mu);
+    std::lock_guard<std::mutex> lock(device_mutex(device));
     auto& eng = engine_for(device);
     eng.load(data, n, p);
     eng.adjoint(target, std::vector<int>(s_values, s_values + s_count), count, log_lambda, score, grad, gn_hessian,
                 exact_hessian);
+  });
+}
+
+int fkpc_get_tuning(int device, fkpc_tuning* tuning) {
+  return guarded([&]() {
+    if (!tuning) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    if (device < 0) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "device must be a CUDA device ordinal");
+    std::lock_guard<std::mutex> lock(device_mutex(device));
+    *tuning = engine_for(device).tuning();
+  });
+}
+
+int fkpc_set_tuning(int device, const fkpc_tuning* tuning) {
+  return guarded([&]() {
+    if (!tuning) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    if (device < 0) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "device must be a CUDA device ordinal");
+    std::lock_guard<std::mutex> lock(device_mutex(device));
+    engine_for(device).set_tuning(*tuning);
   });
 }
 

@@ -2,6 +2,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <numeric>
 #include <stdexcept>
 
@@ -249,6 +250,7 @@ int top_magnitude_eigen(const double* A, int n, int k, std::vector<double>* valu
   norm = std::sqrt(norm);
   for (int i = 0; i < n; ++i) Qv[i] /= norm;
   std::vector<double> w(n), theta, S, dwork, ework;
+  uint64_t restart_seed = 0x5eedu;
   int steps = 0;
   const double tol = 1e-14;
   double anorm = 0.0;
@@ -292,7 +294,10 @@ int top_magnitude_eigen(const double* A, int n, int k, std::vector<double>* valu
           if (resid > tol * tmax) { converged = false; break; }
         }
       }
-      if (converged || invariant || j + 1 == maxit) {
+      // an invariant subspace smaller than k (many near-duplicate locations
+      // make the matrix numerically rank deficient): restart below instead
+      const bool restart = invariant && m < k && j + 1 < maxit;
+      if (!restart && (converged || invariant || j + 1 == maxit)) {
         if (m < k) throw std::runtime_error("Lanczos produced fewer Ritz pairs than requested");
         theta.assign(k, 0.0);
         std::vector<double> V(static_cast<size_t>(n) * k, 0.0);
@@ -353,8 +358,36 @@ int top_magnitude_eigen(const double* A, int n, int k, std::vector<double>* valu
         return steps;
       }
     }
-    if (invariant) break;
     double* qn = &Qv[static_cast<size_t>(n) * (j + 1)];
+    if (invariant) {
+      // Deflated restart: the Krylov space is invariant, so the tridiagonal
+      // splits here (beta = 0) and the iteration goes on from a new start
+      // vector orthogonal to every Lanczos vector so far.  The pairs found
+      // after it belong to the rest of the spectrum (near zero when the
+      // split came from near-duplicate locations).
+      beta[j] = 0.0;
+      double nn = 0.0;
+      for (int attempt = 0; attempt < 8 && !(nn > 1e-8); ++attempt) {
+        for (int i = 0; i < n; ++i) {  // splitmix64 stream, seeded by the step
+          uint64_t z = (restart_seed += 0x9e3779b97f4a7c15ull);
+          z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+          z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+          z ^= z >> 31;
+          qn[i] = static_cast<double>(z >> 11) * 0x1.0p-53 - 0.5;
+        }
+        for (int pass = 0; pass < 2; ++pass)
+          for (int b = 0; b <= j; ++b) {
+            const double* qb = &Qv[static_cast<size_t>(n) * b];
+            const double c = dot(qn, qb, n);
+            for (int i = 0; i < n; ++i) qn[i] -= c * qb[i];
+          }
+        nn = std::sqrt(dot(qn, qn, n)) / std::sqrt(static_cast<double>(n));
+      }
+      if (!(nn > 1e-8)) throw std::runtime_error("Lanczos restart found no new direction");
+      const double inv = 1.0 / (nn * std::sqrt(static_cast<double>(n)));
+      for (int i = 0; i < n; ++i) qn[i] *= inv;
+      continue;
+    }
     for (int i = 0; i < n; ++i) qn[i] = w[i] / beta[j];
   }
   throw std::runtime_error("Lanczos did not converge");

@@ -40,10 +40,33 @@ cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const dou
                              int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
                              FitResult* results, cudaStream_t stream,
                              int selection = 0, double* workspace = nullptr, FitState* states = nullptr,
-                             int* defer_list = nullptr, int* defer_count = nullptr);
+                             int* defer_list = nullptr, int* defer_count = nullptr,
+                             cudaEvent_t after_warp = nullptr, int defer_calls = 25);
+// (class 0: ``after_warp`` is recorded on ``stream`` once the one-warp kernel is
+// queued, before the speculative continuation of the fits it deferred)
 // Doubles of global workspace class ``qmax_class`` needs for ``count`` fits
 // (class 2: q <= 112, rsum <= 96, working set in global memory; 0 otherwise).
 size_t multi_workspace_doubles(int qmax_class, int count);
+
+// Optional index list of a statistic launch: work item b of the grid is
+// idx[b] while b < *count (both device memory), instead of b itself.  The
+// grid is sized for the largest list; blocks past the count exit.
+struct WorkList {
+  const int* idx = nullptr;
+  const int* count = nullptr;
+};
+
+// Split a level batch's components and pairs by whether their residual
+// columns are final once the one-warp fit kernel has run: a column is late
+// when its fit is in the speculative continuation's deferral list
+// (defer_count may be NULL: nothing deferred).  With ncomp components
+// (component c reads residual column c) and npairs pairs: part[0..3] =
+// early / late component counts, early / late pair counts; the lists follow
+// at part + 4 (early components), + ncomp (late components), + 2 ncomp
+// (early pairs), + 2 ncomp + npairs (late pairs).  late_col: ncomp ints of
+// scratch.  One CTA.
+cudaError_t launch_stat_partition(const int* defer_list, const int* defer_count, const FitJob* jobs, int ncomp,
+                                  const PairJob* pairs, int npairs, int* late_col, int* part, cudaStream_t stream);
 
 // dCov: per component centring constants and moments, then per pair statistic
 // and gamma p-value.  comp_cols[c] is the residual column of component c.
@@ -53,26 +76,34 @@ struct DcovComponent {
 };
 
 cudaError_t launch_dcov_components(const double* residuals, int n, const int* comp_cols, int count,
-                                   double* centre, DcovComponent* comps, cudaStream_t stream);
+                                   double* centre, DcovComponent* comps, cudaStream_t stream, WorkList wl = {});
 cudaError_t launch_dcov_pairs(const double* residuals, int n, const int* comp_cols, const double* centre,
                               const DcovComponent* comps, const PairJob* pairs, int count, RecordDev* records,
-                              cudaStream_t stream);
+                              cudaStream_t stream, WorkList wl = {});
 
 // Guard band: list the pairs whose exact p lies in [lo, hi] and give each of
 // their components a low-rank slot.  guard layout: [0] pair count, [1] slot
 // count, [2, 2+count) pair list, comp_slot[ncomp], slot_comps[cap].
+// ``wl`` restricts the scan to a list of pairs.  With ``append`` the
+// selection continues an earlier one (components that already hold a slot
+// keep it) and first stores where it starts in mark[0] (pair list) and
+// mark[1] (slots), the ``begin`` of the low-rank launches that follow it.
 cudaError_t launch_guard_select(const RecordDev* records, const PairJob* pairs, int count, int ncomp, int cap,
-                                double lo, double hi, int* guard, cudaStream_t stream);
+                                double lo, double hi, int* guard, cudaStream_t stream, WorkList wl = {},
+                                int append = 0, int* mark = nullptr);
 // Low-rank (legacy) dCov for the guarded pairs: num_col largest-|value|
 // eigenpairs per slot (vals cap x num_col, vecs n x num_col x cap, centred).
 size_t legacy_eigen_workspace_doubles(int n, int ctas);
+// ``slot_begin`` / ``list_begin`` (device ints, or NULL for 0): the first
+// slot / guarded-pair entry this launch handles.
 cudaError_t launch_legacy_eigen(const double* residuals, int n, const int* comp_cols, const int* guard,
                                 const int* slot_comps, int cap, int ctas, int num_col, double* workspace,
-                                double* lowrank_vals, double* lowrank_vecs, int* status, cudaStream_t stream);
+                                double* lowrank_vals, double* lowrank_vecs, int* status, cudaStream_t stream,
+                                const int* slot_begin = nullptr);
 cudaError_t launch_legacy_pairs(int n, int num_col, const double* lowrank_vals, const double* lowrank_vecs,
                                 const DcovComponent* comps, const int* guard, const int* guard_pairs,
                                 const int* comp_slot, const PairJob* pairs, int count, RecordDev* records,
-                                cudaStream_t stream);
+                                cudaStream_t stream, const int* list_begin = nullptr);
 
 // HSIC: incomplete Cholesky factors (n x num_col, column-centred) per component.
 struct HsicComponent {
@@ -83,9 +114,11 @@ struct HsicComponent {
 };
 
 cudaError_t launch_hsic_components(const double* residuals, int n, const int* comp_cols, int count, int num_col,
-                                   double sig, double* factors, HsicComponent* comps, cudaStream_t stream);
+                                   double sig, double* factors, HsicComponent* comps, cudaStream_t stream,
+                                   WorkList wl = {});
 cudaError_t launch_hsic_pairs(int n, int num_col, const double* factors, const HsicComponent* comps,
-                              const PairJob* pairs, int count, RecordDev* records, cudaStream_t stream);
+                              const PairJob* pairs, int count, RecordDev* records, cudaStream_t stream,
+                              WorkList wl = {});
 cudaError_t launch_hsic_perm_pairs(int n, int num_col, const double* factors, const HsicComponent* comps,
                                    const PairJob* pairs, int count, const int* perms, int replicates,
                                    RecordDev* records, cudaStream_t stream);

@@ -284,7 +284,6 @@ constexpr double kGnGradTol = 1e-9;   // Gauss-Newton selection: |grad V| <= 1e-
 constexpr double kGnFlatTol = 1e-12;  // or a decrease <= 1e-12 (1 + V)
 constexpr double kGnFlatGrad = 1e-6;  // with |grad V| <= 1e-6 (1 + V)
 constexpr double kGnMaxLogSp = 25.0;  // upper bound of the Gauss-Newton search in log(lambda)
-constexpr int kDeferCalls = 25;       // warp-class fits past this many evaluations continue speculatively
 
 __device__ __forceinline__ int tri(int i, int j) { return j * (j + 1) / 2 + i; }  // packed upper, i <= j
 
@@ -2345,20 +2344,26 @@ cudaError_t launch_fit_single(const DesignDev* designs, const double* arena, con
 cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const double* arena, const double* data,
                              int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
                              FitResult* results, cudaStream_t stream, int selection, double* workspace,
-                             FitState* states, int* defer_list, int* defer_count) {
+                             FitState* states, int* defer_list, int* defer_count, cudaEvent_t after_warp,
+                             int defer_calls) {
   if (count <= 0) return cudaSuccess;
   if (qmax_class == 0) {
-    // fits still searching after kDeferCalls evaluations continue in the
+    // fits still searching after defer_calls evaluations continue in the
     // speculative kernel (magic selection, with the deferral buffers given)
-    const bool defer = states && defer_list && defer_count && selection == FKPC_SELECT_MAGIC;
+    const bool defer = states && defer_list && defer_count && selection == FKPC_SELECT_MAGIC && defer_calls > 0;
     if (defer) {
       cudaError_t e = cudaMemsetAsync(defer_count, 0, sizeof(int), stream);
       if (e != cudaSuccess) return e;
     }
     fit_multi_warp_kernel<<<count, 32, kWarpSlotBytes, stream>>>(designs, arena, data, n, jobs, job_index, count,
                                                                  residuals, results, selection,
-                                                                 defer ? kDeferCalls : 0, states, defer_list,
+                                                                 defer ? defer_calls : 0, states, defer_list,
                                                                  defer_count);
+    if (after_warp) {
+      cudaError_t e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaEventRecord(after_warp, stream);
+      if (e != cudaSuccess) return e;
+    }
     if (defer) {
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;

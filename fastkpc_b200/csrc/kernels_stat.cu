@@ -39,6 +39,14 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Work item b of a launch: b itself, or the b-th entry of a device index list.
+__device__ __forceinline__ int work_item(const WorkList& wl, int b, int count) {
+  if (!wl.idx) return b < count ? b : -1;
+  if (b >= *wl.count || b >= count) return -1;
+  const int v = wl.idx[b];
+  return (v >= 0 && v < count) ? v : -1;  // an entry outside the launch's range is never used
+}
+
 __device__ double block_sum256(double v, double* red) {
   v = warp_sum(v);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -173,11 +181,12 @@ __device__ void gamma_record(double stat, double mean, double var, bool hsic, Re
 __global__ void __launch_bounds__(kStatThreads) dcov_component_kernel(const double* __restrict__ residuals, int n,
                                                                        const int* __restrict__ comp_cols, int count,
                                                                        double* __restrict__ centre,
-                                                                       DcovComponent* __restrict__ comps) {
+                                                                       DcovComponent* __restrict__ comps,
+                                                                       WorkList wl) {
   extern __shared__ double sm[];
   __shared__ double red[kStatThreads / 32];
-  const int comp = blockIdx.x;
-  if (comp >= count) return;
+  const int comp = work_item(wl, blockIdx.x, count);
+  if (comp < 0) return;
   double* r = sm;
   double* c = sm + n;
   const double* src = residuals + static_cast<int64_t>(n) * comp_cols[comp];
@@ -232,11 +241,11 @@ __global__ void __launch_bounds__(kStatThreads) dcov_pair_kernel(const double* _
                                                                   const double* __restrict__ centre,
                                                                   const DcovComponent* __restrict__ comps,
                                                                   const PairJob* __restrict__ pairs, int count,
-                                                                  RecordDev* __restrict__ records) {
+                                                                  RecordDev* __restrict__ records, WorkList wl) {
   extern __shared__ double sm[];
   __shared__ double red[kStatThreads / 32];
-  const int t = blockIdx.x;
-  if (t >= count) return;
+  const int t = work_item(wl, blockIdx.x, count);
+  if (t < 0) return;
   const PairJob job = pairs[t];
   double* x = sm;
   double* cx = sm + n;
@@ -462,11 +471,13 @@ __global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double
                                                                      int k, double* __restrict__ workspace,
                                                                      double* __restrict__ vals,
                                                                      double* __restrict__ vecs,
-                                                                     int* __restrict__ status) {
+                                                                     int* __restrict__ status,
+                                                                     const int* __restrict__ slot_begin) {
   extern __shared__ double sm[];
   __shared__ LanczosShared ls;
   const int slots = min(guard[1], cap);
-  for (int slot = blockIdx.x; slot < slots; slot += gridDim.x) {
+  const int first = slot_begin ? *slot_begin : 0;
+  for (int slot = first + blockIdx.x; slot < slots; slot += gridDim.x) {
   const int comp = slot_comps[slot];
   const int tid = threadIdx.x;
   const int maxit = min(n, kLanczosMax);
@@ -773,9 +784,10 @@ __global__ void __launch_bounds__(kStatThreads) legacy_pair_kernel(int n, int k,
                                                                     const int* __restrict__ guard_pairs,
                                                                     const int* __restrict__ comp_slot,
                                                                     const PairJob* __restrict__ pairs, int count,
-                                                                    RecordDev* __restrict__ records) {
+                                                                    RecordDev* __restrict__ records,
+                                                                    const int* __restrict__ list_begin) {
   __shared__ double red[kStatThreads / 32];
-  const int t = blockIdx.x;
+  const int t = (list_begin ? *list_begin : 0) + blockIdx.x;
   if (t >= count || t >= guard[0]) return;
   const PairJob job = pairs[guard_pairs[t]];
   const int sx = comp_slot[job.left], sy = comp_slot[job.right];
@@ -820,17 +832,50 @@ __global__ void __launch_bounds__(kStatThreads) legacy_pair_kernel(int n, int k,
 // guard: [0] pair count, [1] slot count, [2, 2+count) pair list,
 // then comp_slot[ncomp] and slot_comps[cap].
 __global__ void guard_select_kernel(const RecordDev* __restrict__ records, const PairJob* __restrict__ pairs,
-                                    int count, int ncomp, int cap, double lo, double hi, int* __restrict__ guard) {
+                                    int count, int ncomp, int cap, double lo, double hi, int* __restrict__ guard,
+                                    WorkList wl, int append, int* __restrict__ mark) {
   int* list = guard + 2;
   int* comp_slot = list + count;
   int* slot_comps = comp_slot + ncomp;
+  const int items = wl.idx ? *wl.count : count;
+  if (append) {
+    // continue the earlier selection: record where this one starts
+    if (threadIdx.x == 0) {
+      mark[0] = guard[0];
+      mark[1] = guard[1];
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < items; b += blockDim.x) {
+      const int t = wl.idx ? wl.idx[b] : b;
+      const PairJob job = pairs[t];
+      const RecordDev rec = records[job.out];
+      if (rec.status == kStatusOk && rec.p_exact >= lo && rec.p_exact <= hi) {
+        const int idx = atomicAdd(guard, 1);
+        list[idx] = t;
+        if (comp_slot[job.left] < 0) comp_slot[job.left] = -2;
+        if (comp_slot[job.right] < 0) comp_slot[job.right] = -2;
+      }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < ncomp; c += blockDim.x) {
+      if (comp_slot[c] == -2) {
+        const int slot = atomicAdd(guard + 1, 1);
+        if (slot < cap) {
+          comp_slot[c] = slot;
+          slot_comps[slot] = c;
+        }
+      }
+    }
+    return;
+  }
   if (threadIdx.x == 0) {
     guard[0] = 0;
     guard[1] = 0;
   }
   for (int c = threadIdx.x; c < ncomp; c += blockDim.x) comp_slot[c] = -1;
   __syncthreads();
-  for (int t = threadIdx.x; t < count; t += blockDim.x) {
+  for (int b = threadIdx.x; b < items; b += blockDim.x) {
+    const int t = wl.idx ? wl.idx[b] : b;
     const PairJob job = pairs[t];
     const RecordDev rec = records[job.out];
     if (rec.status == kStatusOk && rec.p_exact >= lo && rec.p_exact <= hi) {
@@ -858,7 +903,8 @@ __global__ void __launch_bounds__(kStatThreads) hsic_component_kernel(const doub
                                                                        const int* __restrict__ comp_cols, int count,
                                                                        int max_rank, double sigma,
                                                                        double* __restrict__ factors,
-                                                                       HsicComponent* __restrict__ comps) {
+                                                                       HsicComponent* __restrict__ comps,
+                                                                       WorkList wl) {
   extern __shared__ double sm[];
   __shared__ double red[kStatThreads / 32];
   __shared__ double redv[kStatThreads / 32];
@@ -869,8 +915,8 @@ __global__ void __launch_bounds__(kStatThreads) hsic_component_kernel(const doub
   __shared__ double s_tau;
   __shared__ int s_pivot, s_rank, s_active;
   __shared__ double s_residue;
-  const int comp = blockIdx.x;
-  if (comp >= count) return;
+  const int comp = work_item(wl, blockIdx.x, count);
+  if (comp < 0) return;
   const int tid = threadIdx.x;
   double* r = sm;
   double* diag = sm + n;
@@ -1024,10 +1070,10 @@ __device__ double hsic_cross(int n, const double* Gx, int rx, const double* Gy, 
 __global__ void __launch_bounds__(kStatThreads) hsic_pair_kernel(int n, int max_rank, const double* __restrict__ factors,
                                                                   const HsicComponent* __restrict__ comps,
                                                                   const PairJob* __restrict__ pairs, int count,
-                                                                  RecordDev* __restrict__ records) {
+                                                                  RecordDev* __restrict__ records, WorkList wl) {
   __shared__ double red[kStatThreads / 32];
-  const int t = blockIdx.x;
-  if (t >= count) return;
+  const int t = work_item(wl, blockIdx.x, count);
+  if (t < 0) return;
   const PairJob job = pairs[t];
   const HsicComponent cx = comps[job.left], cy = comps[job.right];
   const double* Gx = factors + static_cast<int64_t>(n) * max_rank * job.left;
@@ -1173,6 +1219,44 @@ cudaError_t launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st
 // legacy Lanczos: r (sorted), q, w (n doubles each) and the sort permutation (n ints)
 size_t legacy_smem_bytes(int n) { return sizeof(double) * 3 * static_cast<size_t>(n) + sizeof(int) * static_cast<size_t>(n); }
 
+// ------------------------------------------------------------ partition
+
+__global__ void __launch_bounds__(1024) stat_partition_kernel(const int* __restrict__ defer_list,
+                                                              const int* __restrict__ defer_count,
+                                                              const FitJob* __restrict__ jobs, int ncomp,
+                                                              const PairJob* __restrict__ pairs, int npairs,
+                                                              int* __restrict__ late_col, int* __restrict__ part) {
+  for (int c = threadIdx.x; c < ncomp; c += blockDim.x) late_col[c] = 0;
+  if (threadIdx.x < 4) part[threadIdx.x] = 0;
+  __syncthreads();
+  const int deferred = defer_count ? *defer_count : 0;
+  for (int d = threadIdx.x; d < deferred; d += blockDim.x) {
+    const int col = jobs[defer_list[d]].out;
+    if (col >= 0 && col < ncomp) late_col[col] = 1;
+  }
+  __syncthreads();
+  int* early_comps = part + 4;
+  int* late_comps = early_comps + ncomp;
+  int* early_pairs = late_comps + ncomp;
+  int* late_pairs = early_pairs + npairs;
+  for (int c = threadIdx.x; c < ncomp; c += blockDim.x) {
+    if (late_col[c]) late_comps[atomicAdd(part + 1, 1)] = c;
+    else early_comps[atomicAdd(part + 0, 1)] = c;
+  }
+  for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
+    const PairJob job = pairs[t];
+    if (late_col[job.left] || late_col[job.right]) late_pairs[atomicAdd(part + 3, 1)] = t;
+    else early_pairs[atomicAdd(part + 2, 1)] = t;
+  }
+}
+
+cudaError_t launch_stat_partition(const int* defer_list, const int* defer_count, const FitJob* jobs, int ncomp,
+                                  const PairJob* pairs, int npairs, int* late_col, int* part, cudaStream_t stream) {
+  if (ncomp <= 0) return cudaSuccess;
+  stat_partition_kernel<<<1, 1024, 0, stream>>>(defer_list, defer_count, jobs, ncomp, pairs, npairs, late_col, part);
+  return cudaGetLastError();
+}
+
 __global__ void gamma_q_eval_kernel(const double* __restrict__ a, const double* __restrict__ x, int count,
                                     double* __restrict__ q, int* __restrict__ ok) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
@@ -1225,20 +1309,20 @@ cudaError_t set_stat_limits(int n) {
 }
 
 cudaError_t launch_dcov_components(const double* residuals, int n, const int* comp_cols, int count,
-                                   double* centre, DcovComponent* comps, cudaStream_t stream) {
+                                   double* centre, DcovComponent* comps, cudaStream_t stream, WorkList wl) {
   if (count <= 0) return cudaSuccess;
   const size_t smem = sizeof(double) * 2 * n;
-  dcov_component_kernel<<<count, kStatThreads, smem, stream>>>(residuals, n, comp_cols, count, centre, comps);
+  dcov_component_kernel<<<count, kStatThreads, smem, stream>>>(residuals, n, comp_cols, count, centre, comps, wl);
   return cudaGetLastError();
 }
 
 cudaError_t launch_dcov_pairs(const double* residuals, int n, const int* comp_cols, const double* centre,
                               const DcovComponent* comps, const PairJob* pairs, int count, RecordDev* records,
-                              cudaStream_t stream) {
+                              cudaStream_t stream, WorkList wl) {
   if (count <= 0) return cudaSuccess;
   const size_t smem = sizeof(double) * 4 * n;
   dcov_pair_kernel<<<count, kStatThreads, smem, stream>>>(residuals, n, comp_cols, centre, comps, pairs, count,
-                                                           records);
+                                                           records, wl);
   return cudaGetLastError();
 }
 
@@ -1249,47 +1333,53 @@ size_t legacy_eigen_workspace_doubles(int n, int ctas) {
 }
 
 cudaError_t launch_guard_select(const RecordDev* records, const PairJob* pairs, int count, int ncomp, int cap,
-                                double lo, double hi, int* guard, cudaStream_t stream) {
+                                double lo, double hi, int* guard, cudaStream_t stream, WorkList wl, int append,
+                                int* mark) {
   if (count <= 0) return cudaSuccess;
-  guard_select_kernel<<<1, 1024, 0, stream>>>(records, pairs, count, ncomp, cap, lo, hi, guard);
+  if (append && !mark) return cudaErrorInvalidValue;
+  guard_select_kernel<<<1, 1024, 0, stream>>>(records, pairs, count, ncomp, cap, lo, hi, guard, wl, append, mark);
   return cudaGetLastError();
 }
 
 cudaError_t launch_legacy_eigen(const double* residuals, int n, const int* comp_cols, const int* guard,
                                 const int* slot_comps, int cap, int ctas, int num_col, double* workspace,
-                                double* lowrank_vals, double* lowrank_vecs, int* status, cudaStream_t stream) {
+                                double* lowrank_vals, double* lowrank_vecs, int* status, cudaStream_t stream,
+                                const int* slot_begin) {
   if (cap <= 0 || ctas <= 0) return cudaSuccess;
   if (num_col > 64) return cudaErrorInvalidValue;
   const size_t smem = legacy_smem_bytes(n);
   legacy_eigen_kernel<<<ctas, kStatThreads, smem, stream>>>(residuals, n, comp_cols, guard, slot_comps, cap,
-                                                             num_col, workspace, lowrank_vals, lowrank_vecs, status);
+                                                             num_col, workspace, lowrank_vals, lowrank_vecs, status,
+                                                             slot_begin);
   return cudaGetLastError();
 }
 
 cudaError_t launch_legacy_pairs(int n, int num_col, const double* lowrank_vals, const double* lowrank_vecs,
                                 const DcovComponent* comps, const int* guard, const int* guard_pairs,
                                 const int* comp_slot, const PairJob* pairs, int count, RecordDev* records,
-                                cudaStream_t stream) {
+                                cudaStream_t stream, const int* list_begin) {
   if (count <= 0) return cudaSuccess;
   legacy_pair_kernel<<<count, kStatThreads, 0, stream>>>(n, num_col, lowrank_vals, lowrank_vecs, comps, guard,
-                                                         guard_pairs, comp_slot, pairs, count, records);
+                                                         guard_pairs, comp_slot, pairs, count, records, list_begin);
   return cudaGetLastError();
 }
 
 cudaError_t launch_hsic_components(const double* residuals, int n, const int* comp_cols, int count, int num_col,
-                                   double sig, double* factors, HsicComponent* comps, cudaStream_t stream) {
+                                   double sig, double* factors, HsicComponent* comps, cudaStream_t stream,
+                                   WorkList wl) {
   if (count <= 0) return cudaSuccess;
   if (num_col > 64) return cudaErrorInvalidValue;
   const size_t smem = sizeof(double) * 3 * n;
   hsic_component_kernel<<<count, kStatThreads, smem, stream>>>(residuals, n, comp_cols, count, num_col, 1.0 / sig,
-                                                                factors, comps);
+                                                                factors, comps, wl);
   return cudaGetLastError();
 }
 
 cudaError_t launch_hsic_pairs(int n, int num_col, const double* factors, const HsicComponent* comps,
-                              const PairJob* pairs, int count, RecordDev* records, cudaStream_t stream) {
+                              const PairJob* pairs, int count, RecordDev* records, cudaStream_t stream,
+                              WorkList wl) {
   if (count <= 0) return cudaSuccess;
-  hsic_pair_kernel<<<count, kStatThreads, 0, stream>>>(n, num_col, factors, comps, pairs, count, records);
+  hsic_pair_kernel<<<count, kStatThreads, 0, stream>>>(n, num_col, factors, comps, pairs, count, records, wl);
   return cudaGetLastError();
 }
 

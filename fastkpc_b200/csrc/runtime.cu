@@ -51,7 +51,6 @@ double upload(DevBuf<T>& buf, const std::vector<T>& host, cudaStream_t s) {
 
 constexpr double kGuardLower = 0.05;
 constexpr double kGuardUpper = 0.15;
-constexpr int kLegacyCtas = 2 * 148;  // two per SM: one component's latency-bound step hides the other's
 
 }  // namespace
 
@@ -61,8 +60,19 @@ Engine::Engine(int device) : device_(device) {
   if (e != cudaSuccess || count <= 0) throw Error(FKPC_STATUS_NO_DEVICE, "no CUDA device is available");
   if (device < 0 || device >= count) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "CUDA device ordinal out of range");
   cuda_check(cudaSetDevice(device), "cudaSetDevice");
-  cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  cuda_check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device), "device attribute");
+  // The main stream carries the critical path (the fits, then the
+  // speculative continuation, whose CTAs each need a whole SM's shared
+  // memory); the side stream's statistic CTAs fill whatever it leaves, so
+  // the main stream gets the highest priority and the side stream the lowest.
+  int least = 0, greatest = 0;
+  cuda_check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
+  cuda_check(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
+  cuda_check(cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, least), "cudaStreamCreate");
   for (auto& ev : ev_) cuda_check(cudaEventCreate(&ev), "cudaEventCreate");
+  cuda_check(cudaEventCreateWithFlags(&ev_warp_, cudaEventDisableTiming), "cudaEventCreate");
+  cuda_check(cudaEventCreateWithFlags(&ev_side_, cudaEventDisableTiming), "cudaEventCreate");
+  cuda_check(cudaEventCreateWithFlags(&ev_part_, cudaEventDisableTiming), "cudaEventCreate");
 }
 
 Engine::~Engine() {
@@ -74,6 +84,13 @@ Engine::~Engine() {
   for (char* b : h_stage_retired_) cudaFreeHost(b);
   for (auto& ev : ev_)
     if (ev) cudaEventDestroy(ev);
+  if (ev_warp_) cudaEventDestroy(ev_warp_);
+  if (ev_side_) cudaEventDestroy(ev_side_);
+  if (ev_part_) cudaEventDestroy(ev_part_);
+  if (side_) {
+    cudaStreamSynchronize(side_);
+    cudaStreamDestroy(side_);
+  }
   if (stream_) {
     cudaStreamSynchronize(stream_);
     cudaStreamDestroy(stream_);
@@ -149,6 +166,7 @@ void Engine::load(const double* data, int n, int p) {
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   n_ = n;
   p_ = p;
+  ++load_id_;
   host_data_.assign(data, data + static_cast<size_t>(n) * p);
   double* d = d_data_.ensure(host_data_.size());
   cuda_check(cudaMemcpyAsync(d, host_data_.data(), host_data_.size() * sizeof(double), cudaMemcpyHostToDevice, stream_),
@@ -320,7 +338,7 @@ void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int di
     std::memcpy(hmap + c * static_cast<size_t>(n), pr.mapping.data(), static_cast<size_t>(n) * sizeof(int));
   });
   const int cnt = static_cast<int>(batch->idx.size());
-  const int ctas = std::min(cnt, ctas_per_sm * 148);
+  const int ctas = std::min(cnt, ctas_per_sm * sms_);
   const size_t nab = static_cast<size_t>(2) * cnt * steps;
   const size_t nvals = static_cast<size_t>(cnt) * kk;
   const size_t ns = static_cast<size_t>(cnt) * (kk - 1) * (kk - 1);
@@ -480,8 +498,8 @@ void Engine::build_designs() {
   for (const auto& S : sets_)
     if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
   TprsBatch ubatch, batch;
-  launch_tprs_batch(univariate_columns(), 1, &ubatch, stream_, 2);
-  if (bivariate.size() >= kDeviceTprsMin) launch_tprs_batch(bivariate, 2, &batch, stream_, 2);
+  launch_tprs_batch(univariate_columns(), 1, &ubatch, stream_, tuning_.tprs_ctas_per_sm);
+  if (bivariate.size() >= kDeviceTprsMin) launch_tprs_batch(bivariate, 2, &batch, stream_, tuning_.tprs_ctas_per_sm);
   // the other designs need no bivariate basis: build them while the device works
   finish_tprs_batch(&ubatch);
   build_univariate_smooths();  // those the device could not take
@@ -806,6 +824,10 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
   d_multi_res_.ensure(multi_jobs_.size());
   d_resid_.ensure(static_cast<size_t>(n) * ncomp);
   d_records_.ensure(npairs);
+  d_late_col_.ensure(ncomp);
+  d_part_.ensure(4 + 2 * ncomp + 2 * npairs);
+  d_guard_mark_.ensure(2);
+  late_designs_ = false;  // a new batch: the descriptor array of the side stream is stale
   if (stats_enabled_) {
     const int method = opt.ci_method;
     if (method == FKPC_DCC_GAMMA || method == FKPC_DCC_PERM) {
@@ -824,7 +846,8 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
       d_lr_vals_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col);
       d_lr_vecs_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col * n);
       d_lr_status_.ensure(2 * static_cast<size_t>(guard_cap_));
-      d_legacy_ws_.ensure(legacy_eigen_workspace_doubles(n, kLegacyCtas));
+      d_legacy_ws_.ensure(legacy_eigen_workspace_doubles(n, legacy_ctas()));
+      lr_ws_ctas_ = legacy_ctas();
     }
     if (method == FKPC_DCC_PERM || method == FKPC_HSIC_PERM) {
       if (!rstream) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "permutation methods require a seeded stream");
@@ -858,8 +881,12 @@ void Engine::check_geometry() {
   }
 }
 
-void Engine::pack_late() {
+void Engine::pack_late(cudaStream_t st) {
   if (pending_.empty()) return;
+  const bool side = st == side_;
+  // the side stream reads the arena and the smooth store the main stream
+  // filled before the fits were queued
+  if (side) cuda_check(cudaStreamWaitEvent(side_, ev_[0], 0), "stream wait");
   const int n = n_;
   std::vector<double> late;  // penalties, and the bases a host fallback built
   std::vector<int64_t> xoff(pending_.size(), -1), poff(pending_.size(), -1);
@@ -882,7 +909,7 @@ void Engine::pack_late() {
     poff[g] = static_cast<int64_t>(late.size());
     late.insert(late.end(), sm.S.begin(), sm.S.end());
   }
-  h2d_bytes_ += stage_upload(d_late_table_, late);
+  h2d_bytes_ += stage_upload(d_late_table_, late, st);
   const double* table = d_late_table_.get();
   std::vector<SingleGeomJob> jobs(pending_.size());
   for (size_t g = 0; g < pending_.size(); ++g) {
@@ -897,12 +924,19 @@ void Engine::pack_late() {
     job.q = des.q;
     job.rank = des.ranks[0];
   }
-  h2d_bytes_ += stage_upload(d_late_geom_jobs_, jobs);
-  // the descriptor array again, now complete: queued behind the multi-penalty
-  // fits, which read the additive descriptors
-  h2d_bytes_ += stage_upload(d_designs_, ddesc_);
+  h2d_bytes_ += stage_upload(d_late_geom_jobs_, jobs, st);
+  // the descriptor array again, now complete.  On the main stream it is
+  // queued behind the multi-penalty fits, which read the additive
+  // descriptors; beside them, on the side stream, it goes to a buffer of its
+  // own, which the single-penalty fits read.
+  if (side) {
+    h2d_bytes_ += stage_upload(d_designs_late_, ddesc_, st);
+    late_designs_ = true;
+  } else {
+    h2d_bytes_ += stage_upload(d_designs_, ddesc_, st);
+  }
   cuda_check(launch_single_geometry(n, d_late_geom_jobs_.get(), static_cast<int>(jobs.size()), d_arena_.get(),
-                                    d_geom_status_.get() + geom_status_used_, stream_),
+                                    d_geom_status_.get() + geom_status_used_, st),
              "single-penalty geometry");
   geom_status_used_ += jobs.size();
   pending_.clear();
@@ -917,9 +951,13 @@ void Engine::prepare(const std::vector<Test>& tests, const fkpc_options& opt, RS
   d2h_bytes_ = 0.0;
   opt_ = opt;
   stats_enabled_ = true;
+  late_designs_ = false;
   release_graph();
   auto t0 = std::chrono::steady_clock::now();
   plan_components(tests);
+  designs_built_ = 0;
+  for (const auto& S : sets_) designs_built_ += cache_->has_design(S) ? 0 : 1;
+  smooths_built_ = static_cast<int>(univariate_columns().size());
   build_designs();
   setup_ms_ = ms_since(t0);
   pack_and_upload(opt, rstream);
@@ -934,17 +972,22 @@ void Engine::run_batch(const std::vector<Test>& tests, const fkpc_options& opt, 
   d2h_bytes_ = 0.0;
   opt_ = opt;
   stats_enabled_ = true;
+  late_designs_ = false;
   release_graph();
   try {
     auto t0 = std::chrono::steady_clock::now();
     plan_components(tests);
+    designs_built_ = 0;
+    for (const auto& S : sets_) designs_built_ += cache_->has_design(S) ? 0 : 1;
+    smooths_built_ = static_cast<int>(univariate_columns().size());
+  smooths_built_ = static_cast<int>(univariate_columns().size());
     designs_.assign(sets_.size(), nullptr);
     std::vector<std::vector<int>> bivariate;
     for (const auto& S : sets_)
       if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
     TprsBatch ubatch, batch;
-    launch_tprs_batch(univariate_columns(), 1, &ubatch, stream_, 2);
-    if (!bivariate.empty()) launch_tprs_batch(bivariate, 2, &batch, stream_, 2);
+    launch_tprs_batch(univariate_columns(), 1, &ubatch, stream_, tuning_.tprs_ctas_per_sm);
+    if (!bivariate.empty()) launch_tprs_batch(bivariate, 2, &batch, stream_, tuning_.tprs_ctas_per_sm);
     finish_tprs_batch(&ubatch);
     build_univariate_smooths();  // those the device could not take
     build_host_designs([this](const std::vector<int>& S) { return S.size() != 2 || cache_->has_design(S); });
@@ -961,13 +1004,14 @@ void Engine::run_batch(const std::vector<Test>& tests, const fkpc_options& opt, 
     build_host_designs([](const std::vector<int>&) { return true; });
     host_ms += ms_since(t1);
     auto t2 = std::chrono::steady_clock::now();
-    pack_late();
+    pack_late(split_stats() ? side_ : stream_);
     up_ms += ms_since(t2);
     enqueue_rest();
     setup_ms_ = host_ms;
     upload_ms_ = up_ms;
   } catch (...) {
-    cudaStreamSynchronize(stream_);  // nothing queued may outlive the call's staging
+    cudaStreamSynchronize(side_);  // nothing queued may outlive the call's staging
+    cudaStreamSynchronize(stream_);
     throw;
   }
 }
@@ -981,14 +1025,8 @@ void Engine::enqueue() {
 
 void Engine::enqueue_multi() {
   const int n = n_;
-  if (!multi_small_.empty()) {
-    cuda_check(launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
-                                d_multi_small_.get(), static_cast<int>(multi_small_.size()), d_resid_.get(),
-                                d_multi_res_.get(), stream_, opt_.selection, nullptr, d_fit_states_.get(),
-                                d_defer_list_.get(), d_defer_count_.get()),
-               "fit multi");
-    launches_ += opt_.selection == FKPC_SELECT_MAGIC ? 2 : 1;  // with the speculative continuation
-  }
+  // the CTA classes first: once the one-warp kernel is done, every fit but
+  // the ones it hands to the speculative continuation is final
   if (!multi_large_.empty()) {
     cuda_check(launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                 d_multi_large_.get(), static_cast<int>(multi_large_.size()), d_resid_.get(),
@@ -1003,26 +1041,144 @@ void Engine::enqueue_multi() {
                "fit multi");
     ++launches_;
   }
+  const bool split = split_stats();
+  if (!multi_small_.empty()) {
+    cuda_check(launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                d_multi_small_.get(), static_cast<int>(multi_small_.size()), d_resid_.get(),
+                                d_multi_res_.get(), stream_, opt_.selection, nullptr, d_fit_states_.get(),
+                                d_defer_list_.get(), d_defer_count_.get(), split ? ev_warp_ : nullptr,
+                                tuning_.defer_evaluations),
+               "fit multi");
+    launches_ += opt_.selection == FKPC_SELECT_MAGIC ? 2 : 1;  // with the speculative continuation
+  } else if (split) {
+    cuda_check(cudaEventRecord(ev_warp_, stream_), "event");
+  }
+}
+
+bool Engine::split_stats() const {
+  return tuning_.split_statistics && stats_enabled_ && opt_.mode != FKPC_MODE_PLAIN && !pairs_.empty() &&
+         (opt_.ci_method == FKPC_DCC_GAMMA || opt_.ci_method == FKPC_HSIC_GAMMA);
 }
 
 void Engine::enqueue_rest() {
   const int n = n_;
-  const int ncomp = static_cast<int>(comps_.size());
-  const int npairs = static_cast<int>(pairs_.size());
+  const bool split = split_stats();
+  // direct columns and single-penalty fits: on the side stream when the
+  // statistics split, where they run beside the multi-penalty fits
+  cudaStream_t fs = split ? side_ : stream_;
+  if (split) cuda_check(cudaStreamWaitEvent(side_, ev_[0], 0), "stream wait");
   if (!direct_cols_.empty()) {
     dim3 grid((n + 255) / 256, static_cast<unsigned>(direct_cols_.size()));
-    gather_columns_kernel<<<grid, 256, 0, stream_>>>(d_data_.get(), n, d_direct_cols_.get(), d_direct_slots_.get(),
-                                                      static_cast<int>(direct_cols_.size()), d_resid_.get());
+    gather_columns_kernel<<<grid, 256, 0, fs>>>(d_data_.get(), n, d_direct_cols_.get(), d_direct_slots_.get(),
+                                                 static_cast<int>(direct_cols_.size()), d_resid_.get());
     cuda_check(cudaGetLastError(), "gather columns");
     ++launches_;
   }
   if (!single_jobs_.empty()) {
-    cuda_check(launch_fit_single(d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_single_jobs_.get(),
-                                 static_cast<int>(single_jobs_.size()), d_resid_.get(), d_single_res_.get(), stream_),
+    const DesignDev* designs = late_designs_ ? d_designs_late_.get() : d_designs_.get();
+    cuda_check(launch_fit_single(designs, d_arena_.get(), d_data_.get(), n, d_single_jobs_.get(),
+                                 static_cast<int>(single_jobs_.size()), d_resid_.get(), d_single_res_.get(), fs),
                "fit single");
     ++launches_;
   }
+  if (!split) {
+    cuda_check(cudaEventRecord(ev_[1], stream_), "event");
+    enqueue_stats_serial();
+    cuda_check(cudaEventRecord(ev_[3], stream_), "event");
+    return;
+  }
+  const int ncomp = static_cast<int>(comps_.size());
+  const int npairs = static_cast<int>(pairs_.size());
+  const bool dcc = opt_.ci_method == FKPC_DCC_GAMMA;
+  int* part = d_part_.get();
+  const WorkList early_c{part + 4, part + 0}, late_c{part + 4 + ncomp, part + 1};
+  const WorkList early_p{part + 4 + 2 * ncomp, part + 2}, late_p{part + 4 + 2 * ncomp + npairs, part + 3};
+  int* guard = d_guard_.get();
+  int* mark = d_guard_mark_.get();
+  const int* glist = guard + 2;
+  const int* comp_slot = glist + npairs;
+  const int* slot_comps = comp_slot + ncomp;
+  const int lr_ctas = lowrank_launch_ctas();
+  // side stream, once the one-warp kernel is done: the early statistics
+  cuda_check(cudaStreamWaitEvent(side_, ev_warp_, 0), "stream wait");
+  const bool deferring = !multi_small_.empty() && opt_.selection == FKPC_SELECT_MAGIC && tuning_.defer_evaluations > 0;
+  cuda_check(launch_stat_partition(deferring ? d_defer_list_.get() : nullptr,
+                                   deferring ? d_defer_count_.get() : nullptr, d_multi_jobs_.get(), ncomp,
+                                   d_pairs_.get(), npairs, d_late_col_.get(), part, side_),
+             "partition");
+  ++launches_;
+  // the main stream reads the late lists the partition writes
+  cuda_check(cudaEventRecord(ev_part_, side_), "event");
+  if (dcc) {
+    cuda_check(launch_dcov_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, d_centre_.get(), d_dcov_.get(),
+                                      side_, early_c),
+               "dcov components");
+    cuda_check(launch_dcov_pairs(d_resid_.get(), n, d_comp_cols_.get(), d_centre_.get(), d_dcov_.get(),
+                                 d_pairs_.get(), npairs, d_records_.get(), side_, early_p),
+               "dcov pairs");
+    cuda_check(launch_guard_select(d_records_.get(), d_pairs_.get(), npairs, ncomp, guard_cap_, kGuardLower,
+                                   kGuardUpper, guard, side_, early_p),
+               "guard select");
+    cuda_check(launch_legacy_eigen(d_resid_.get(), n, d_comp_cols_.get(), guard, slot_comps, guard_cap_, lr_ctas,
+                                   opt_.num_col, d_legacy_ws_.get(), d_lr_vals_.get(), d_lr_vecs_.get(),
+                                   d_lr_status_.get(), side_),
+               "legacy eigen");
+    cuda_check(launch_legacy_pairs(n, opt_.num_col, d_lr_vals_.get(), d_lr_vecs_.get(), d_dcov_.get(), guard, glist,
+                                   comp_slot, d_pairs_.get(), npairs, d_records_.get(), side_),
+               "legacy pairs");
+    launches_ += 5;
+  } else {
+    cuda_check(launch_hsic_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, opt_.num_col, opt_.hsic_sig,
+                                      d_factors_.get(), d_hsic_.get(), side_, early_c),
+               "hsic components");
+    cuda_check(launch_hsic_pairs(n, opt_.num_col, d_factors_.get(), d_hsic_.get(), d_pairs_.get(), npairs,
+                                 d_records_.get(), side_, early_p),
+               "hsic pairs");
+    launches_ += 2;
+  }
+  cuda_check(cudaEventRecord(ev_side_, side_), "event");
+  // main stream, after the speculative continuation and the partition: the
+  // late statistics
   cuda_check(cudaEventRecord(ev_[1], stream_), "event");
+  cuda_check(cudaStreamWaitEvent(stream_, ev_part_, 0), "stream wait");
+  if (dcc) {
+    cuda_check(launch_dcov_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, d_centre_.get(), d_dcov_.get(),
+                                      stream_, late_c),
+               "dcov components");
+    cuda_check(cudaStreamWaitEvent(stream_, ev_side_, 0), "stream wait");
+    cuda_check(launch_dcov_pairs(d_resid_.get(), n, d_comp_cols_.get(), d_centre_.get(), d_dcov_.get(),
+                                 d_pairs_.get(), npairs, d_records_.get(), stream_, late_p),
+               "dcov pairs");
+    cuda_check(cudaEventRecord(ev_[2], stream_), "event");
+    cuda_check(launch_guard_select(d_records_.get(), d_pairs_.get(), npairs, ncomp, guard_cap_, kGuardLower,
+                                   kGuardUpper, guard, stream_, late_p, 1, mark),
+               "guard select");
+    cuda_check(launch_legacy_eigen(d_resid_.get(), n, d_comp_cols_.get(), guard, slot_comps, guard_cap_, lr_ctas,
+                                   opt_.num_col, d_legacy_ws_.get(), d_lr_vals_.get(), d_lr_vecs_.get(),
+                                   d_lr_status_.get(), stream_, mark + 1),
+               "legacy eigen");
+    cuda_check(launch_legacy_pairs(n, opt_.num_col, d_lr_vals_.get(), d_lr_vecs_.get(), d_dcov_.get(), guard, glist,
+                                   comp_slot, d_pairs_.get(), npairs, d_records_.get(), stream_, mark),
+               "legacy pairs");
+    launches_ += 5;
+  } else {
+    cuda_check(launch_hsic_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, opt_.num_col, opt_.hsic_sig,
+                                      d_factors_.get(), d_hsic_.get(), stream_, late_c),
+               "hsic components");
+    cuda_check(cudaStreamWaitEvent(stream_, ev_side_, 0), "stream wait");
+    cuda_check(launch_hsic_pairs(n, opt_.num_col, d_factors_.get(), d_hsic_.get(), d_pairs_.get(), npairs,
+                                 d_records_.get(), stream_, late_p),
+               "hsic pairs");
+    cuda_check(cudaEventRecord(ev_[2], stream_), "event");
+    launches_ += 2;
+  }
+  cuda_check(cudaEventRecord(ev_[3], stream_), "event");
+}
+
+void Engine::enqueue_stats_serial() {
+  const int n = n_;
+  const int ncomp = static_cast<int>(comps_.size());
+  const int npairs = static_cast<int>(pairs_.size());
   if (stats_enabled_ && npairs > 0) {
     const int method = opt_.ci_method;
     if (method == FKPC_DCC_GAMMA || method == FKPC_DCC_PERM) {
@@ -1045,7 +1201,7 @@ void Engine::enqueue_rest() {
       const int* comp_slot = list + npairs;
       const int* slot_comps = comp_slot + ncomp;
       cuda_check(launch_legacy_eigen(d_resid_.get(), n, d_comp_cols_.get(), guard, slot_comps, guard_cap_,
-                                     std::min(kLegacyCtas, guard_cap_), opt_.num_col, d_legacy_ws_.get(),
+                                     lowrank_launch_ctas(), opt_.num_col, d_legacy_ws_.get(),
                                      d_lr_vals_.get(), d_lr_vecs_.get(), d_lr_status_.get(), stream_),
                  "legacy eigen");
       cuda_check(launch_legacy_pairs(n, opt_.num_col, d_lr_vals_.get(), d_lr_vecs_.get(), d_dcov_.get(), guard, list,
@@ -1074,7 +1230,6 @@ void Engine::enqueue_rest() {
       ++launches_;
     }
   }
-  cuda_check(cudaEventRecord(ev_[3], stream_), "event");
 }
 
 void Engine::execute() {
@@ -1217,6 +1372,8 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
     stats->refine_ms = g_ms;
     stats->download_ms = download_ms;
     stats->designs = static_cast<int>(sets_.size());
+    stats->designs_built = designs_built_;
+    stats->smooths_built = smooths_built_;
     stats->targets = static_cast<int>(single_jobs_.size() + multi_jobs_.size());
     stats->pairs = static_cast<int>(pairs_.size());
     stats->guarded = guarded;
@@ -1410,7 +1567,8 @@ double Engine::time_stage(int stage, int repeats, double* flops_per_launch) {
       case 1: return launch_fit_multi(0, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                       d_multi_small_.get(), static_cast<int>(multi_small_.size()), d_resid_.get(),
                                       d_multi_res_.get(), stream_, opt_.selection, nullptr, d_fit_states_.get(),
-                                      d_defer_list_.get(), d_defer_count_.get());
+                                      d_defer_list_.get(), d_defer_count_.get(), nullptr,
+                                      tuning_.defer_evaluations);
       case 2: return launch_fit_multi(1, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                       d_multi_large_.get(), static_cast<int>(multi_large_.size()), d_resid_.get(),
                                       d_multi_res_.get(), stream_, opt_.selection);
@@ -1426,7 +1584,7 @@ double Engine::time_stage(int stage, int repeats, double* flops_per_launch) {
       case 6: return launch_hsic_pairs(n, opt_.num_col, d_factors_.get(), d_hsic_.get(), d_pairs_.get(), npairs,
                                        d_records_.get(), stream_);
       case 7: return launch_legacy_eigen(d_resid_.get(), n, d_comp_cols_.get(), guard, guard + 2 + npairs + ncomp,
-                                         guard_cap_, std::min(kLegacyCtas, guard_cap_), opt_.num_col,
+                                         guard_cap_, lowrank_launch_ctas(), opt_.num_col,
                                          d_legacy_ws_.get(), d_lr_vals_.get(), d_lr_vecs_.get(), d_lr_status_.get(),
                                          stream_);
       default: return launch_legacy_pairs(n, opt_.num_col, d_lr_vals_.get(), d_lr_vecs_.get(), d_dcov_.get(), guard,
@@ -1449,6 +1607,22 @@ double Engine::time_stage(int stage, int repeats, double* flops_per_launch) {
   cuda_check(cudaEventElapsedTime(&ms, ev_[4], ev_[5]), "event time");
   if (flops_per_launch) *flops_per_launch = stage_flops_[stage];
   return ms / std::max(1, repeats);
+}
+
+void Engine::set_tuning(const fkpc_tuning& t) {
+  if (t.defer_evaluations < 0 || t.split_statistics < 0 || t.split_statistics > 1 || t.lowrank_ctas_per_sm < 1 ||
+      t.lowrank_ctas_per_sm > 4 || t.tprs_ctas_per_sm < 1 || t.tprs_ctas_per_sm > 4)
+    throw Error(FKPC_STATUS_INVALID_ARGUMENT,
+                "tuning out of range (defer >= 0, split 0/1, Lanczos CTAs per SM 1..4)");
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  cuda_check(cudaStreamSynchronize(stream_), "tuning");
+  tuning_ = t;
+  release_graph();
+  if (lr_ws_ctas_ > 0 && n_ > 0 && lr_ws_ctas_ < legacy_ctas()) {
+    // a prepared guard band: its workspace follows the new CTA count
+    d_legacy_ws_.ensure(legacy_eigen_workspace_doubles(n_, legacy_ctas()));
+    lr_ws_ctas_ = legacy_ctas();
+  }
 }
 
 double Engine::measure_fp64_peak() {
@@ -1501,6 +1675,9 @@ void Engine::regress(const std::vector<int>& targets, const std::vector<std::vec
   d2h_bytes_ = 0.0;
   auto t0 = std::chrono::steady_clock::now();
   plan_components(tests);
+  designs_built_ = 0;
+  for (const auto& S : sets_) designs_built_ += cache_->has_design(S) ? 0 : 1;
+  smooths_built_ = static_cast<int>(univariate_columns().size());
   build_designs();
   setup_ms_ = ms_since(t0);
   stats_enabled_ = false;
@@ -1635,6 +1812,10 @@ void Engine::statistics(const double* residuals, int m, const std::vector<int>& 
              "upload residuals");
   d_records_.ensure(pairs_.size());
   const size_t ncomp = static_cast<size_t>(m), npairs = pairs_.size();
+  late_designs_ = false;
+  d_late_col_.ensure(ncomp);
+  d_part_.ensure(4 + 2 * ncomp + 2 * npairs);
+  d_guard_mark_.ensure(2);
   if (opt.ci_method == FKPC_DCC_GAMMA || opt.ci_method == FKPC_DCC_PERM) {
     d_centre_.ensure(static_cast<size_t>(n) * ncomp);
     d_dcov_.ensure(ncomp);
@@ -1649,7 +1830,8 @@ void Engine::statistics(const double* residuals, int m, const std::vector<int>& 
     d_lr_vals_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col);
     d_lr_vecs_.ensure(static_cast<size_t>(guard_cap_) * opt.num_col * n);
     d_lr_status_.ensure(2 * static_cast<size_t>(guard_cap_));
-    d_legacy_ws_.ensure(legacy_eigen_workspace_doubles(n, kLegacyCtas));
+    d_legacy_ws_.ensure(legacy_eigen_workspace_doubles(n, legacy_ctas()));
+      lr_ws_ctas_ = legacy_ctas();
   }
   if (opt.ci_method == FKPC_DCC_PERM || opt.ci_method == FKPC_HSIC_PERM) {
     if (!permutations) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "permutation methods need a permutation table");

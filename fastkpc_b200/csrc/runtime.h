@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -105,11 +106,15 @@ class Engine {
   // One kernel of the prepared batch replayed alone: mean ms per launch.
   double time_stage(int stage, int repeats, double* flops_per_launch);
   double measure_fp64_peak();
+  fkpc_tuning tuning() const { return tuning_; }
+  void set_tuning(const fkpc_tuning& t);  // validates; the next execution re-captures its graph
   cudaStream_t stream() const { return stream_; }
   // When set, packing a permutation batch appends the stream's state after
   // each test's permutations (a speculative caller rolls back to one).
   void set_stream_snapshots(std::vector<RStream>* s) { stream_snapshots_ = s; }
   int launches() const { return launches_; }
+  // changes with every load(): a session checks that its data is still loaded
+  uint64_t load_id() const { return load_id_; }
   double setup_ms() const { return setup_ms_; }
 
  private:
@@ -128,8 +133,17 @@ class Engine {
   template <class T>
   double stage_upload(DevBuf<T>& buf, const std::vector<T>& host, cudaStream_t st = nullptr);
   void enqueue_multi();  // the multi-penalty fit classes
-  void enqueue_rest();   // direct columns, single-penalty fits, statistics
-  void pack_late();      // pending bivariate designs: descriptors, geometry
+  // direct columns, single-penalty fits, statistics.  For the gamma methods
+  // the single-penalty fits and the statistics of every pair whose residuals
+  // are final once the one-warp fit kernel has run go to the side stream
+  // (early), beside the speculative continuation; the pairs of the fits it
+  // continues follow on the main stream (late).
+  void enqueue_rest();
+  void enqueue_stats_serial();  // every statistic on the main stream, after every fit
+  // pending bivariate designs: descriptors, geometry, on stream ``st``
+  // (the side stream uploads the descriptor array to its own buffer)
+  void pack_late(cudaStream_t st);
+  bool split_stats() const;  // the early / late statistic split applies
   void check_geometry();  // statuses of the geometry kernels (after a synchronisation)
   // one level's thin-plate smooths (dim 2: bivariate, dim 1: univariate) on
   // the device, in flight
@@ -158,7 +172,17 @@ class Engine {
   double* pinned_arena(size_t count);  // persistent page-locked staging buffer of the design arena
 
   int device_ = 0;
+  int sms_ = 148;
+  fkpc_tuning tuning_{25, 1, 2, 2};
+  int legacy_ctas() const { return tuning_.lowrank_ctas_per_sm * sms_; }
+  int lr_ws_ctas_ = 0;  // CTAs the guard-band workspace was sized for
+  // guard-band Lanczos CTAs of a launch: never more than the workspace holds
+  int lowrank_launch_ctas() const { return std::min(std::min(legacy_ctas(), guard_cap_), lr_ws_ctas_); }
   cudaStream_t stream_ = nullptr;
+  cudaStream_t side_ = nullptr;  // early statistics beside the speculative continuation
+  cudaEvent_t ev_warp_ = nullptr;  // main stream: every fit but the continued ones is done
+  cudaEvent_t ev_side_ = nullptr;  // side stream: the early statistics are done
+  cudaEvent_t ev_part_ = nullptr;  // side stream: the early / late lists are written
   int n_ = 0, p_ = 0;
   std::vector<double> host_data_;
   DevBuf<double> d_data_;
@@ -209,6 +233,10 @@ class Engine {
   DevBuf<DcovComponent> d_dcov_;
   DevBuf<HsicComponent> d_hsic_;
   DevBuf<int> d_guard_;  // [0] pair count, [1] slot count, then lists
+  DevBuf<int> d_guard_mark_;  // where the late guard-band selection starts (pairs, slots)
+  DevBuf<int> d_late_col_, d_part_;  // early / late split of the components and pairs
+  DevBuf<DesignDev> d_designs_late_;  // descriptor array uploaded on the side stream
+  bool late_designs_ = false;
   DevBuf<int> d_lr_status_;
   DevBuf<int> d_perms_;
 
@@ -229,6 +257,9 @@ class Engine {
   DevBuf<double> d_late_table_;
   DevBuf<SingleGeomJob> d_late_geom_jobs_;
   int launches_ = 0;
+  uint64_t load_id_ = 0;
+  int designs_built_ = 0;  // sets of the last batch whose design the cache lacked
+  int smooths_built_ = 0;  // univariate smooths the last batch set up
   double setup_ms_ = 0.0, upload_ms_ = 0.0;
   int guard_count_host_ = 0;
   double h2d_bytes_ = 0.0, d2h_bytes_ = 0.0;

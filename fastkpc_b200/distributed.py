@@ -5,8 +5,9 @@ of the level.  ``sharded_skeleton`` runs ``fkpc_skeleton_run_custom`` on every
 rank of a ``torch.distributed`` process group (one process per GPU, NCCL or
 gloo).  The library plans each level identically on every rank and calls back
 here with the level's tests.  Each rank evaluates its share -- whole same-S
-cohorts, so no conditioning-set design is built twice -- with
-``fkpc_ci_level_batch`` on its own GPU.  The 48-byte records are then
+cohorts, so no conditioning-set design is built twice -- on its own GPU
+through a session (fkpc_session_load once, fkpc_session_evaluate per
+level), so the rank's design cache lives across levels.  The 48-byte records are then
 all-gathered on the host, and the full level is handed back for the canonical
 replay (pMax, sepsets, deletions), which every rank performs identically.  No
 collective touches the device data path: the only exchange is the gather of
@@ -52,19 +53,19 @@ def partition_tests(tests, world):
 
 def level_batch_evaluator(X, options):
     """Evaluate a list of tests on this rank's GPU with ``options`` (an
-    ``fkpc_options``): returns a ctypes array of ``CiRecord``."""
-    lib = fk.load_library()
-    n, p = X.shape
+    ``fkpc_options``): returns a ctypes array of ``CiRecord``.  The data is
+    loaded once (a session), so the designs built for one level serve every
+    later level; ``evaluate.stats`` collects each call's stage stats."""
+    session = fk.Session(X, device=options.device)
 
     def evaluate(tests):
-        out = (fk.CiRecord * max(1, len(tests)))()
-        if tests:
-            xs, ys, offs, vals = fk._tests_arrays(tests)
-            fk._check(lib.fkpc_ci_level_batch(fk._ptr(X, ctypes.c_double), n, p, fk._ptr(xs, ctypes.c_int),
-                                              fk._ptr(ys, ctypes.c_int), fk._ptr(offs, ctypes.c_int),
-                                              fk._ptr(vals, ctypes.c_int), len(tests), ctypes.byref(options), out,
-                                              None))
+        if not tests:
+            return (fk.CiRecord * 1)()
+        out, st = session.evaluate_raw(tests, options)
+        evaluate.stats.append(st)
         return out
+    evaluate.stats = []
+    evaluate.session = session
     return evaluate
 
 
@@ -74,7 +75,9 @@ def sharded_skeleton(data, alpha, labels=None, options=None, group=None, evaluat
     Every rank must call it with the same data and options; every rank
     returns the same result.  ``options["device"]`` is this rank's GPU.
     ``evaluate`` (tests -> sequence of ``CiRecord``) replaces the GPU
-    evaluation, e.g. for tests of the host logic."""
+    evaluation, e.g. for tests of the host logic.  The result's
+    ``summary["rank_stats"]`` lists this rank's stage stats per level when
+    the GPU evaluator ran."""
     import torch.distributed as dist
 
     X, labels, o, method = fk._skeleton_setup(data, alpha, labels, options)
@@ -108,7 +111,9 @@ def sharded_skeleton(data, alpha, labels=None, options=None, group=None, evaluat
 
     callback = fk.LEVEL_EVALUATOR(level_eval)
     try:
-        return fk._run_skeleton(X, alpha, labels, o, method, callback)
+        out = fk._run_skeleton(X, alpha, labels, o, method, callback)
+        out["summary"]["rank_stats"] = list(getattr(evaluate, "stats", []))
+        return out
     except fk.FkpcError:
         if failures:
             raise failures[0]

@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define FKPC_ABI_VERSION 3
+#define FKPC_ABI_VERSION 4
 
 #if defined(__GNUC__)
 #define FKPC_API __attribute__((visibility("default")))
@@ -69,6 +69,9 @@ typedef struct fkpc_options {
   int device;                   /* CUDA device ordinal */
   int strict;                   /* reference envelope: alpha 0.1, index 1, numCol 35 < n, 2 <= p <= 64 */
   int selection;                /* FKPC_SELECT_MAGIC (default) or FKPC_SELECT_GN_NEWTON */
+  int level_graph;              /* batched gamma methods: 1 = set each batch up, then run it as one
+                                   captured CUDA graph; 0 (default) = the one-shot flow that overlaps
+                                   the host set-up with the device work */
 } fkpc_options;
 
 /* One CI test result. */
@@ -106,6 +109,8 @@ typedef struct fkpc_stage_stats {
   int lowrank_steps_max;    /* most Lanczos steps any of them took */
   double lowrank_steps_mean;
   double device_ms;         /* device time of the batch's launch sequence */
+  int designs_built;        /* conditioning-set designs the call set up (not found in the cache) */
+  int smooths_built;        /* per-variable (univariate) smooth bases the call set up */
 } fkpc_stage_stats;
 
 typedef struct fkpc_trace_row {
@@ -181,6 +186,27 @@ FKPC_API int fkpc_ci_level_batch(const double* data_colmajor, int n, int p,
                         const int* s_values, int count,
                         const fkpc_options* options, fkpc_ci_record* out,
                         fkpc_stage_stats* stats);
+
+/*
+ * A session: the data matrix stays loaded on one device, with the cache of
+ * conditioning-set designs and smooth bases built from it, across calls of
+ * fkpc_session_evaluate -- the form a host that evaluates a skeleton level by
+ * level (one process per GPU, each taking a share of every level) needs, so
+ * that a design is set up once per device and not once per level.
+ * fkpc_session_load replaces any earlier session on ``device``.  Any other
+ * call that takes a data matrix on the same device (fkpc_ci_level_batch,
+ * fkpc_skeleton_run, ...) loads its own data and ends the session; a later
+ * fkpc_session_evaluate then fails with FKPC_STATUS_INVALID_ARGUMENT.
+ * fkpc_session_evaluate has the arguments and results of fkpc_ci_level_batch
+ * without the data; options->device selects the session.
+ * Same reference counterpart as fkpc_ci_level_batch (the reference keeps its
+ * caches inside one skeleton call, fastkpc/src/full_cuda_ci_one_call.cpp:5040).
+ */
+FKPC_API int fkpc_session_load(const double* data_colmajor, int n, int p, int device);
+FKPC_API int fkpc_session_evaluate(const int* x, const int* y, const int* s_offsets,
+                                   const int* s_values, int count,
+                                   const fkpc_options* options, fkpc_ci_record* out,
+                                   fkpc_stage_stats* stats);
 
 /*
  * The plain per-test form: one CI test, one launch set, synchronised.
@@ -281,6 +307,22 @@ FKPC_API int fkpc_batch_time_stage(int device, int stage, int repeats,
  * independent FMA chains in every thread.  No reference counterpart.
  */
 FKPC_API int fkpc_measure_fp64_peak(int device, double* tflops);
+
+/*
+ * Schedule choices of a device's engine.  No result depends on them: records
+ * are bit-identical under every setting (fastkpc_b200/autotune.py checks
+ * this while it times the candidates).  No reference counterpart.
+ */
+typedef struct fkpc_tuning {
+  int defer_evaluations;    /* a one-warp GCV search still running after this many evaluations
+                               moves to the speculative continuation (0: never); default 25 */
+  int split_statistics;     /* 1 (default): the statistics of pairs whose fits are final run
+                               beside the continuation; 0: after every fit */
+  int lowrank_ctas_per_sm;  /* guard-band Lanczos CTAs per SM, 1..4; default 2 */
+  int tprs_ctas_per_sm;     /* thin-plate set-up Lanczos CTAs per SM, 1..4; default 2 */
+} fkpc_tuning;
+FKPC_API int fkpc_get_tuning(int device, fkpc_tuning* tuning);
+FKPC_API int fkpc_set_tuning(int device, const fkpc_tuning* tuning);
 
 /*
  * Host-only design set-up for one conditioning set S (no device needed):

@@ -46,9 +46,41 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300))) if len(b) else 0.0
 
 
+AGREE_LOG_SP = 1e-11
+
+
+def fit_agreement(fx, log_sp):
+    """Per fit: True when the GPU's selected log(lambda) equals the oracle's to
+    AGREE_LOG_SP on every entry the GCV curvature pins down (|entry| < 15)."""
+    ref = fx["fit_log_sp"]
+    got = log_sp[:, :ref.shape[1]]
+    det = np.isfinite(ref) & (np.abs(ref) < 15.0)
+    diff = np.where(det, np.abs(got - np.where(det, ref, 0.0)), 0.0)
+    return np.max(diff, axis=1) <= AGREE_LOG_SP
+
+
+def triple_agreement(fx, fit_agree):
+    """Per triple: both residual fits agree (a direct |S| = 0 side always does)."""
+    index = {key: i for i, key in enumerate((t, tuple(S)) for t, S in fits(fx))}
+    out = np.ones(len(fx["x"]), dtype=bool)
+    for k, (x, y, S) in enumerate(triples(fx)):
+        if S:
+            out[k] = bool(fit_agree[index[(x, tuple(S))]] and fit_agree[index[(y, tuple(S))]])
+    return out
+
+
 def report(fx, dcc=None, hsic=None, residuals=None, log_sp=None):
-    """Errors of the GPU records / residuals against the fixture (dict)."""
+    """Errors of the GPU records / residuals against the fixture (dict).
+
+    With ``log_sp`` and records, the p errors are also reported over the
+    triples whose fits both land on the oracle's point (``*_agreeing``):
+    elsewhere magic stopped outside its Newton region, where two
+    implementations' searches end up to ~1e-9 apart in log(lambda)."""
     out = {}
+    agree = None
+    if log_sp is not None and (dcc is not None or hsic is not None):
+        agree = triple_agreement(fx, fit_agreement(fx, log_sp))
+        out["triples_fits_agreeing"] = int(agree.sum())
     if residuals is not None:
         n = residuals.shape[0]
         idx = fx["full_index"]
@@ -89,6 +121,8 @@ def report(fx, dcc=None, hsic=None, residuals=None, log_sp=None):
         out["dcc_p_lowrank_abs_err_max"] = (float(np.max(np.abs(dcc["p_value"][lr] - fx["dcc_p"][lr])))
                                             if lr.any() else 0.0)
         out["dcc_p_abs_err_max"] = float(np.max(np.abs(dcc["p_value"] - fx["dcc_p"])))
+        if agree is not None:
+            out["dcc_p_exact_abs_err_max_agreeing"] = float(np.max(np.abs(dcc["p_exact"] - fx["dcc_p_exact"])[agree]))
         out["dcc_alpha_flips"] = int(np.sum((dcc["p_value"] >= ALPHA) != (fx["dcc_p"] >= ALPHA)))
         out["dcc_guarded"] = int(g.sum())
         out["triples"] = int(len(g))
@@ -96,5 +130,7 @@ def report(fx, dcc=None, hsic=None, residuals=None, log_sp=None):
         out["hsic_stat_rel_err_max"] = _rel(hsic["statistic"], fx["hsic_stat"])
         out["hsic_moment_rel_err_max"] = max(_rel(hsic["mean"], fx["hsic_mean"]), _rel(hsic["variance"], fx["hsic_var"]))
         out["hsic_p_abs_err_max"] = float(np.max(np.abs(hsic["p_value"] - fx["hsic_p"])))
+        if agree is not None:
+            out["hsic_p_abs_err_max_agreeing"] = float(np.max(np.abs(hsic["p_value"] - fx["hsic_p"])[agree]))
         out["hsic_alpha_flips"] = int(np.sum((hsic["p_value"] >= ALPHA) != (fx["hsic_p"] >= ALPHA)))
     return out

@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol(lib_built):
 
 
 def test_abi_version_and_defaults(lib_built):
-    assert lib_built.fkpc_abi_version() == 3
+    assert lib_built.fkpc_abi_version() == 4
     o = fk.make_options()
     assert o.alpha == 0.1 and o.num_col == 35 and o.index == 1.0 and o.strict == 1
     assert o.selection == 0 and fk.make_options(selection="gn_newton").selection == 1
@@ -68,3 +68,20 @@ def test_host_design_matches_oracle(lib_built, dev500, S):
     rc, ic = gcv.fit(gcv.Prepared(desc), d[:, 20])
     ro, io = gcv.fit(gcv.Prepared(od), d[:, 20])
     assert np.max(np.abs(rc - ro)) <= 1e-10 * np.max(np.abs(ro))
+
+
+def test_host_lanczos_restarts_on_near_duplicate_locations(lib_built):
+    """Column 43 of the n=351, p=48 SEM with seed 619: 320 of its 351 values
+    lie within 1e-9 of each other, so the eta matrix of its smooth is
+    numerically rank deficient and Lanczos meets an invariant subspace before
+    it has k = 10 Ritz pairs.  The set-up restarts from a new orthogonal start
+    vector instead of failing (the near-null pairs it adds are rounding-level,
+    as any dense eigensolver's would be)."""
+    from fastkpc_b200 import workloads
+    X = workloads.skeleton_351x48(619)
+    c = np.sort(X[:, 43])
+    assert np.sum(np.diff(c) < 1e-9) > 300
+    d = fk.design_export(X, [43])
+    assert d["q"] == 10 and np.all(np.isfinite(d["X"]))
+    d2 = fk.design_export(X, [43, 7])
+    assert d2["q"] == 30 and np.all(np.isfinite(d2["X"]))

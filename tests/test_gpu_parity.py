@@ -273,7 +273,21 @@ def test_sharded_skeleton_single_rank_equals_direct(lib):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=0, world_size=1)
     try:
-        sharded = distributed.sharded_skeleton(X, 0.1, options=opts)
+        _, _, o, _ = fk._skeleton_setup(X, 0.1, None, opts)
+        inner = distributed.level_batch_evaluator(X, o)
+        seen = []
+
+        def evaluate(tests):
+            seen.extend(tuple(t[2]) for t in tests)
+            return inner(tests)
+        sharded = distributed.sharded_skeleton(X, 0.1, options=opts, evaluate=evaluate)
+        # the rank's session keeps its caches across levels: every design and
+        # every per-variable smooth is set up once, however many levels use it
+        sets = {S for S in seen if S}
+        smooth_vars = {v for S in sets if len(S) != 2 for v in S}
+        assert sum(st["designs_built"] for st in inner.stats) == len(sets)
+        assert sum(st["smooths_built"] for st in inner.stats) == len(smooth_vars)
+        assert sum(st["smooths_built"] > 0 for st in inner.stats) >= 1
     finally:
         dist.destroy_process_group()
     assert np.array_equal(sharded["adjacency"], direct["adjacency"])
@@ -457,3 +471,30 @@ def test_near_exact_fit_keeps_a_positive_rss(lib):
     assert np.max(np.abs(resid[:, 0] - r)) <= 1e-12 * np.max(np.abs(X[:, 7]))
     rec, _ = fk.ci_level_batch(X, [(7, 12, [34]), (12, 7, [34])], ci_method="dcc.gamma")
     assert np.all(rec["status"] == 0)
+
+
+@pytest.mark.parametrize("method", ["dcc.gamma", "hsic.gamma"])
+def test_schedule_tunings_change_no_record(lib, method):
+    """fkpc_set_tuning changes how a level batch is laid out -- deferral
+    threshold, statistics beside the continuation or after every fit,
+    Lanczos CTAs per SM -- never a record: one-shot and staged forms give
+    bit-identical records under each setting."""
+    X, triples = workloads.level_batch_500x50(count=600)
+    base = fk.get_tuning(0)
+    try:
+        ref, _ = fk.ci_level_batch(X, triples, ci_method=method)
+        for change in ({"split_statistics": 0}, {"defer_evaluations": 0}, {"defer_evaluations": 40},
+                       {"lowrank_ctas_per_sm": 1, "tprs_ctas_per_sm": 1},
+                       {"lowrank_ctas_per_sm": 3, "tprs_ctas_per_sm": 3}):
+            fk.set_tuning(0, **{**base, **change})
+            rec, _ = fk.ci_level_batch(X, triples, ci_method=method)
+            batch = fk.StagedBatch(X, triples, ci_method=method)
+            batch.execute(1)
+            srec, _ = batch.collect()
+            for r in (rec, srec):
+                for f in ("p_value", "p_exact", "statistic", "mean", "variance", "status", "flags"):
+                    assert np.array_equal(np.nan_to_num(r[f]), np.nan_to_num(ref[f])), (change, f)
+        with pytest.raises(fk.FkpcError):
+            fk.set_tuning(0, lowrank_ctas_per_sm=9)
+    finally:
+        fk.set_tuning(0, **base)

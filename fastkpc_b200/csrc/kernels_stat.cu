@@ -464,7 +464,7 @@ __device__ void block_exscan2(double a, double c, double* scan, double* ea, doub
 // workspace per CTA: V (n x (kLanczosMax+1)) Lanczos basis, S
 // (kLanczosMax x 64) Ritz coefficient vectors, 64 x 5 x kLanczosMax
 // inverse-iteration scratch (one set per thread).
-__global__ void __launch_bounds__(kStatThreads) legacy_eigen_kernel(const double* __restrict__ residuals, int n,
+__global__ void __launch_bounds__(kStatThreads, 2) legacy_eigen_kernel(const double* __restrict__ residuals, int n,
                                                                      const int* __restrict__ comp_cols,
                                                                      const int* __restrict__ guard,
                                                                      const int* __restrict__ slot_comps, int cap,

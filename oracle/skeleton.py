@@ -86,8 +86,15 @@ def _pcalg_key(t):
 
 
 def skeleton(data, alpha=0.1, method="dcc.gamma", m_max=None, num_col=35, sig=1.0,
-             replicates=100, seed=None, pvalue_fn=None):
-    """Run the stable skeleton; returns adjacency, pmax, sepsets, n_edgetests, trace."""
+             replicates=100, seed=None, pvalue_fn=None, edge_runner=None):
+    """Run the stable skeleton; returns adjacency, pmax, sepsets, n_edgetests, trace.
+
+    ``edge_runner(level, chains)`` (batched methods only) may evaluate a
+    level's per-edge task chains elsewhere, e.g. in worker processes: chains
+    is a list of task lists, one per edge in plan order, and it returns one
+    list of p-values per chain, each stopping at the first p >= alpha (the
+    tests of one edge after a deletion are never run).  Edges are independent
+    given the level-start graph, so this is the sequential result."""
     n, p = data.shape
     if m_max is None:
         m_max = p - 2
@@ -105,7 +112,13 @@ def skeleton(data, alpha=0.1, method="dcc.gamma", m_max=None, num_col=35, sig=1.
         for i, t in enumerate(tasks):
             by_edge.setdefault(t["edge"], []).append(i)
         pvals = {}
-        if stream is None:
+        if stream is None and edge_runner is not None:
+            edges = list(by_edge)
+            results = edge_runner(level, [[tasks[i] for i in by_edge[e]] for e in edges])
+            for e, ps in zip(edges, results):
+                for i, pv in zip(by_edge[e], ps):
+                    pvals[i] = pv
+        elif stream is None:
             for edge, idx in by_edge.items():
                 for i in idx:
                     t = tasks[i]

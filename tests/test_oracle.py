@@ -198,3 +198,27 @@ def test_polished_point_is_stationary_in_extended_precision():
         rp[j] += h
         rm[j] -= h
         assert abs((V(rp) - V(rm)) / (2 * h) / v0) < 1e-13
+
+
+def test_skeleton_fixture_is_the_oracle():
+    """The committed 351x48 (seed 537) oracle skeletons: the trace holds
+    n.edgetests rows, deletions match the adjacency, and the oracle re-run on
+    the first level-1 tests reproduces their p-values."""
+    from threadpoolctl import threadpool_limits
+    from fastkpc_b200 import workloads
+    with np.load(golden_path("skeleton351x48_s537_oracle.npz")) as f:
+        fx = {k: f[k] for k in f.files}
+    X = workloads.skeleton_351x48(int(fx["seed"]))
+    cache = skeleton.ResidualCache(X)
+    for method in ("hsic.gamma", "dcc.gamma"):
+        key = method.replace(".", "_") + "_"
+        assert len(fx[key + "trace_p"]) == int(fx[key + "n_edgetests"].sum())
+        deleted = int(fx[key + "trace_deletes"].sum())
+        edges = int(fx[key + "adjacency"].sum()) // 2
+        assert edges + deleted == 48 * 47 // 2
+        rows = np.nonzero(fx[key + "trace_level"] == 1)[0][:6]
+        with threadpool_limits(limits=1):
+            for k in rows:
+                S = [int(v) for v in fx[key + "trace_S"][k] if v >= 0]
+                pv = skeleton.ci_pvalue(cache, method, int(fx[key + "trace_x"][k]), int(fx[key + "trace_y"][k]), S)
+                assert abs(pv - fx[key + "trace_p"][k]) <= 1e-12

@@ -1372,12 +1372,12 @@ __device__ __forceinline__ double warp_dot(const double* __restrict__ a, const d
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   int i = 0;
   for (; i + 3 < len; i += 4) {
-    s0 += a[i] * b[ldb * i];
-    s1 += a[i + 1] * b[ldb * (i + 1)];
-    s2 += a[i + 2] * b[ldb * (i + 2)];
-    s3 += a[i + 3] * b[ldb * (i + 3)];
+    s0 = fma(a[i], b[ldb * i], s0);
+    s1 = fma(a[i + 1], b[ldb * (i + 1)], s1);
+    s2 = fma(a[i + 2], b[ldb * (i + 2)], s2);
+    s3 = fma(a[i + 3], b[ldb * (i + 3)], s3);
   }
-  for (; i < len; ++i) s0 += a[i] * b[ldb * i];
+  for (; i < len; ++i) s0 = fma(a[i], b[ldb * i], s0);
   return (s0 + s1) + (s2 + s3);
 }
 
@@ -1480,6 +1480,24 @@ __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, 
 // C = T'T and D = (WT)'(WT) for the 16 columns b = B0..B0+15: row a (this
 // lane) accumulated over the coefficient index, then folded into the block
 // sums p[bj] = {sum C.D, sum D a_b, sum C a_b, sum C b_b} over b in block bj.
+// Column b's terms of the block sums, from C(a, b) and D(a, b) of this lane's
+// row a; explicit roundings, so that every path that forms the block sums in
+// the same order of b gets the same bits.
+__device__ __forceinline__ void block_term(int b, double c, double d, const double* av, const double* bv,
+                                           const WarpScalars& sc, double (&p)[kWarpM][4]) {
+  const int jb = sc.rowblk[b];
+  const double avb = av[b], bvb = bv[b];
+  const double cd = __dmul_rn(c, d), da = __dmul_rn(d, avb), ca = __dmul_rn(c, avb), cb = __dmul_rn(c, bvb);
+#pragma unroll
+  for (int bj = 0; bj < kWarpM; ++bj)
+    if (jb == bj) {
+      p[bj][0] = __dadd_rn(p[bj][0], cd);
+      p[bj][1] = __dadd_rn(p[bj][1], da);
+      p[bj][2] = __dadd_rn(p[bj][2], ca);
+      p[bj][3] = __dadd_rn(p[bj][3], cb);
+    }
+}
+
 template <int B0>
 __device__ __forceinline__ void warp_block_sums(int q, const double* WT, const double* T, const double* av,
                                                 const double* bv, const WarpScalars& sc, double (&p)[kWarpM][4]) {
@@ -1495,38 +1513,29 @@ __device__ __forceinline__ void warp_block_sums(int q, const double* WT, const d
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const double2 x = trow[u], y = wrow[u];
-      c[2 * u] += ta * x.x;
-      c[2 * u + 1] += ta * x.y;
-      d[2 * u] += wa * y.x;
-      d[2 * u + 1] += wa * y.y;
+      c[2 * u] = fma(ta, x.x, c[2 * u]);
+      c[2 * u + 1] = fma(ta, x.y, c[2 * u + 1]);
+      d[2 * u] = fma(wa, y.x, d[2 * u]);
+      d[2 * u + 1] = fma(wa, y.y, d[2 * u + 1]);
     }
   }
 #pragma unroll
-  for (int u = 0; u < 16; ++u) {
-    const int b = B0 + u;
-    const int jb = sc.rowblk[b];
-    const double avb = av[b], bvb = bv[b];
-    const double cd = c[u] * d[u], da = d[u] * avb, ca = c[u] * avb, cb = c[u] * bvb;
-#pragma unroll
-    for (int bj = 0; bj < kWarpM; ++bj)
-      if (jb == bj) {
-        p[bj][0] += cd;
-        p[bj][1] += da;
-        p[bj][2] += ca;
-        p[bj][3] += cb;
-      }
-  }
+  for (int u = 0; u < 16; ++u) block_term(B0 + u, c[u], d[u], av, bv, sc, p);
 }
 
 // Gradient and Hessian of V at the point of the last warp_core call (the
-// quantities of multi_derivatives).  jrow: penalty block of stacked row ``lane``.
-__device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, int n, int jrow) {
+// quantities of multi_derivatives), in three pieces on a warp slot ``sm``:
+// deriv_setup (one warp): e1 = g - W'(W g), T = Ra^-T root (lane a: column a,
+// row-major in Z), a = T'g and b = T'e1 into AV / BV; then WT = W T into X,
+// the per-lane sum of squares of WT and the block sums of C = T'T and
+// D = (WT)'(WT) (warp_derivatives on one warp, spec_derivatives on the
+// continuation's warps); deriv_finish (one warp): the partial sums, the
+// gradient and both Hessians.  jrow: penalty block of stacked row ``lane``.
+__device__ __forceinline__ void deriv_setup(double* sm, const double* __restrict__ arena, int jrow) {
   using L = WarpLayout;
-  const DesignDev& des = warp_design();
-  WarpScalars& sc = warp_scalars();
-  double* sm = warp_slot();
+  const DesignDev& des = *reinterpret_cast<const DesignDev*>(sm + L::TOTAL + kWarpScalarDoubles);
   const int lane = threadIdx.x & 31;
-  const int q = des.q, m = des.m;
+  const int q = des.q;
   double* X = sm + L::X;
   const double* Y = sm + L::Y;
   double* Z = sm + L::Z;
@@ -1560,24 +1569,21 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
     }
   }
   if (jrow >= 0) warp_left_subst(ta, kWarpR, des.off[jrow], q, X, idg);
-  __syncwarp();  // e1 written; every read of Ra done: X takes WT
-  const double sa = warp_dot(g, ta, kWarpR, q);
-  const double sb = warp_dot(e1, ta, kWarpR, q);
-  // WT(:, a) = W T(:, a), row-major in X
-  double dd = 0.0;
-  for (int i = 0; i < q; ++i) {
-    const double s = warp_dot(Y + packed_row(i, 0) + i, ta + kWarpR * i, kWarpR, q - i);
-    X[kWarpR * i + lane] = s;
-    dd += s * s;
-  }
-  av[lane] = sa;
-  bv[lane] = sb;
+  __syncwarp();  // e1 written; every read of Ra done: X may take WT
+  av[lane] = warp_dot(g, ta, kWarpR, q);
+  bv[lane] = warp_dot(e1, ta, kWarpR, q);
   __syncwarp();
-  double p[kWarpM][4];
-#pragma unroll
-  for (int bj = 0; bj < kWarpM; ++bj) p[bj][0] = p[bj][1] = p[bj][2] = p[bj][3] = 0.0;
-  warp_block_sums<0>(q, X, Z, av, bv, sc, p);
-  warp_block_sums<16>(q, X, Z, av, bv, sc, p);
+}
+
+__device__ __forceinline__ void deriv_finish(double* sm, int n, double (&p)[kWarpM][4], double dd) {
+  using L = WarpLayout;
+  const DesignDev& des = *reinterpret_cast<const DesignDev*>(sm + L::TOTAL + kWarpScalarDoubles);
+  WarpScalars& sc = *reinterpret_cast<WarpScalars*>(sm + L::TOTAL);
+  const int lane = threadIdx.x & 31;
+  const int m = des.m;
+  double* X = sm + L::X;
+  double* Z = sm + L::Z;
+  const double sa = sm[L::AV + lane], sb = sm[L::BV + lane];
   __syncwarp();  // T / WT reads done: X takes the per-lane partial sums
   {
     double* part = X + kWarpPart * lane;
@@ -1642,6 +1648,34 @@ __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, 
     for (int j = 0; j < m; ++j) sc.grad_c[j] = s1 * sc.drss[j] - s2 * sc.ddelta[j];
   }
   __syncwarp();
+}
+
+__device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, int n, int jrow) {
+  using L = WarpLayout;
+  double* sm = warp_slot();
+  const DesignDev& des = warp_design();
+  const WarpScalars& sc = warp_scalars();
+  const int lane = threadIdx.x & 31;
+  const int q = des.q;
+  double* X = sm + L::X;
+  const double* Y = sm + L::Y;
+  const double* Z = sm + L::Z;
+  deriv_setup(sm, arena, jrow);
+  // WT(:, a) = W T(:, a), row-major in X
+  const double* ta = Z + lane;
+  double dd = 0.0;
+  for (int i = 0; i < q; ++i) {
+    const double s = warp_dot(Y + packed_row(i, 0) + i, ta + kWarpR * i, kWarpR, q - i);
+    X[kWarpR * i + lane] = s;
+    dd = fma(s, s, dd);
+  }
+  __syncwarp();
+  double p[kWarpM][4];
+#pragma unroll
+  for (int bj = 0; bj < kWarpM; ++bj) p[bj][0] = p[bj][1] = p[bj][2] = p[bj][3] = 0.0;
+  warp_block_sums<0>(q, X, Z, sm + L::AV, sm + L::BV, sc, p);
+  warp_block_sums<16>(q, X, Z, sm + L::AV, sm + L::BV, sc, p);
+  deriv_finish(sm, n, p, dd);
 }
 
 }  // namespace
@@ -1981,6 +2015,54 @@ struct SpecShared {
   int fail;
 };
 
+// warp_derivatives of the trial warp ``aw`` accepted, with the q-length dot
+// products -- the entries of WT = W T and of C = T'T and D = (WT)'(WT) --
+// spread over all kSpecWarps warps of the CTA; every sum whose order matters
+// (the sum of squares of WT, the block sums over the columns b) stays on warp
+// aw in warp_derivatives' order, so the results are the same bits.  C and D
+// go to the X regions of two other warps (stride 33: no bank conflicts),
+// which hold nothing between trials.  Called by every warp of the CTA.
+__device__ __noinline__ void spec_derivatives(const double* __restrict__ arena, int n, int jrow, int aw) {
+  using L = WarpLayout;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* sm = s_warp_dyn + aw * kWarpSlotDoubles;
+  const DesignDev& des = *reinterpret_cast<const DesignDev*>(sm + L::TOTAL + kWarpScalarDoubles);
+  const WarpScalars& sc = *reinterpret_cast<const WarpScalars*>(sm + L::TOTAL);
+  const int q = des.q;
+  double* X = sm + L::X;
+  const double* Y = sm + L::Y;
+  const double* Z = sm + L::Z;
+  double* Cb = s_warp_dyn + ((aw + 1) % kSpecWarps) * kWarpSlotDoubles + L::X;
+  double* Db = s_warp_dyn + ((aw + 2) % kSpecWarps) * kWarpSlotDoubles + L::X;
+  if (warp == aw) deriv_setup(sm, arena, jrow);
+  __syncthreads();
+  for (int i = warp; i < q; i += kSpecWarps)
+    X[kWarpR * i + lane] = warp_dot(Y + packed_row(i, 0) + i, Z + lane + kWarpR * i, kWarpR, q - i);
+  __syncthreads();
+  for (int b = warp; b < kWarpR; b += kSpecWarps) {
+    double c = 0.0, d = 0.0;
+    for (int i = 0; i < q; ++i) {
+      c = fma(Z[kWarpR * i + lane], Z[kWarpR * i + b], c);
+      d = fma(X[kWarpR * i + lane], X[kWarpR * i + b], d);
+    }
+    Cb[33 * lane + b] = c;
+    Db[33 * lane + b] = d;
+  }
+  __syncthreads();
+  if (warp == aw) {
+    double dd = 0.0;
+    for (int i = 0; i < q; ++i) {
+      const double s = X[kWarpR * i + lane];
+      dd = fma(s, s, dd);
+    }
+    double p[kWarpM][4];
+#pragma unroll
+    for (int bj = 0; bj < kWarpM; ++bj) p[bj][0] = p[bj][1] = p[bj][2] = p[bj][3] = 0.0;
+    for (int b = 0; b < kWarpR; ++b) block_term(b, Cb[33 * lane + b], Db[33 * lane + b], sm + L::AV, sm + L::BV, sc, p);
+    deriv_finish(sm, n, p, dd);
+  }
+}
+
 __global__ void __launch_bounds__(32 * kSpecWarps) fit_multi_spec_kernel(
     const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data, int n,
     const FitJob* __restrict__ jobs, const int* __restrict__ defer_list, const int* __restrict__ defer_count,
@@ -2065,7 +2147,9 @@ __global__ void __launch_bounds__(32 * kSpecWarps) fit_multi_spec_kernel(
           }
           if (lane < m) sc.log_sp[lane] = sc.trial[lane];
           __syncwarp();
-          warp_derivatives(arena, n, jrow);
+        }
+        spec_derivatives(arena, n, jrow, aw);  // every warp of the CTA takes part
+        if (warp == aw) {
           double g2 = 0.0;
           for (int r = 0; r < m; ++r) g2 += sc.gradient[r] * sc.gradient[r];  // the previous gradient
           bool conv = false;

@@ -1396,15 +1396,8 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
   }
 }
 
-// Algorithmic FP64 flop counts of the implemented algorithms (FMA = 2):
-//  fit single : z = (QW)'y and the residual, 2nq each; 20q per spectral
-//               objective evaluation.
-//  fit multi  : y0 = Q'y and the residual, 2nq each; per objective
-//               evaluation the Householder fold of the stacked roots
-//               4 (rsum + 1) q^2 / 2, the triangular inverse and W = R Ra^-1
-//               q^3 / 3 each, g and W g 2 q^2; per derivative evaluation
-//               (one per Newton iteration) T and W T 2 q^2 rsum, C and D
-//               2 rsum^2 q.
+// Algorithmic FP64 flop counts (FMA = 2):
+//  fits       : per fit 6nq + E (16 q^3 + 2 m q^3) (comment in the body).
 //  dCov components : row sums 2 n^2, squared centred entries 2.5 n (n - 1).
 //  dCov pairs      : 4 n (n - 1) (n(n-1)/2 entries x 2 abs-diffs, 4 centring
 //                    subtractions and one FMA).
@@ -1414,18 +1407,22 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
 void Engine::account_flops(const std::vector<FitResult>& sres, const std::vector<FitResult>& mres) {
   for (double& f : stage_flops_) f = 0.0;
   const double n = n_;
+  // The fit stages count the path's algorithmic FP64 work as the scope table
+  // of the hot path defines it, per fit: Q'y (4nq) and the residual (2nq),
+  // plus 16q^3 (the SVD of the stacked system with U1) + 2mq^3 (the
+  // derivatives) per GCV evaluation, E evaluations from the search's own
+  // counter.  The kernels execute less (the spectral single-penalty form,
+  // the Householder fold, derivatives only at accepted points).
   for (size_t i = 0; i < single_jobs_.size(); ++i) {
     const double q = designs_[single_jobs_[i].design]->q;
-    stage_flops_[0] += 4.0 * n * q + 20.0 * q * sres[i].evaluations;
+    stage_flops_[0] += 6.0 * n * q + (16.0 + 2.0) * q * q * q * sres[i].evaluations;
   }
   for (size_t i = 0; i < multi_jobs_.size(); ++i) {
     const Design& des = *designs_[multi_jobs_[i].design];
     const double q = des.q;
     double rs = 0.0;
     for (int r : des.ranks) rs += r;
-    const double core = 2.0 * (rs + 1.0) * q * q + 2.0 * q * q * q / 3.0 + 4.0 * q * q;
-    const double deriv = 2.0 * q * q * rs + 2.0 * rs * rs * q;
-    const double f = 4.0 * n * q + core * mres[i].evaluations + deriv * mres[i].iterations;
+    const double f = 6.0 * n * q + (16.0 + 2.0 * des.m) * q * q * q * mres[i].evaluations;
     const bool small = des.q <= kWarpQ && rs <= kWarpR && des.m <= kWarpM;
     const bool large = !small && des.q <= 76 && rs <= 64;
     stage_flops_[small ? 1 : (large ? 2 : 9)] += f;

@@ -6,6 +6,10 @@ same name (fastkpc/R/fast_kpc.R:56-130 -> precision_run_skeleton_full_cuda_nativ
 fastkpc/R/cuda_native.R:2237-2311): same option names and meaning, same
 fail-closed errors.  Indices are 0-based here (the R facade is 1-based).
 
+``fastkpc_compatible_cuda_wanpdag`` mirrors the reference's strict WAN-PDAG
+facade (fastkpc/R/fast_kpc.R:449-600): the same skeleton, then kpcalg's
+orientation with every regrVonPS residual and CI test on the device.
+
 The compute runs in ``libfastkpc_b200.so`` (CUDA, sm_100a).  There is no CPU
 fallback: importing works without a GPU, but every compute call raises
 ``FkpcError`` when no CUDA device is present, and loading fails loudly when
@@ -20,7 +24,7 @@ import numpy as np
 
 __all__ = [
     "FkpcError", "library_path", "load_library", "fastkpc_compatible_cuda_skeleton",
-    "ci_level_batch", "ci_plain_one", "regress_batch", "stat_batch", "design_export", "Session",
+    "fastkpc_compatible_cuda_wanpdag", "orient_wanpdag", "orient_wanpdag_custom", "ci_level_batch", "ci_plain_one", "regress_batch", "stat_batch", "design_export", "Session",
     "METHODS",
 ]
 
@@ -98,6 +102,22 @@ class Result(ctypes.Structure):
                 ("elapsed_sec", ctypes.c_double), ("stats", StageStats)]
 
 
+class OrientationTest(ctypes.Structure):
+    _fields_ = [("reverse", ctypes.c_int), ("target", ctypes.c_int), ("other", ctypes.c_int),
+                ("s_offset", ctypes.c_int), ("s_count", ctypes.c_int), ("z_offset", ctypes.c_int),
+                ("z_count", ctypes.c_int), ("p_value", ctypes.c_double), ("rejected", ctypes.c_int)]
+
+
+class Orientation(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_int), ("pdag", ctypes.POINTER(ctypes.c_int)),
+                ("collider_orientations", ctypes.c_int), ("rule1_orientations", ctypes.c_int),
+                ("rule2_orientations", ctypes.c_int), ("rule3_orientations", ctypes.c_int),
+                ("generalized_orientations", ctypes.c_int), ("regrvonps_calls", ctypes.c_int),
+                ("residual_fits", ctypes.c_int), ("residual_cache_hits", ctypes.c_int), ("tests", ctypes.c_int),
+                ("trace", ctypes.POINTER(OrientationTest)), ("set_values", ctypes.POINTER(ctypes.c_int)),
+                ("elapsed_sec", ctypes.c_double)]
+
+
 _lib = None
 
 _P = ctypes.POINTER
@@ -110,6 +130,11 @@ _SIGNATURES = {
     "fkpc_default_options": (None, [_P(Options)]),
     "fkpc_skeleton_run": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _P(Options), _P(_P(Result))]),
     "fkpc_result_free": (None, [_P(Result)]),
+    "fkpc_orient_wanpdag": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, _P(Options),
+                                           _P(_P(Orientation))]),
+    "fkpc_orientation_free": (None, [_P(Orientation)]),
+    "fkpc_orient_wanpdag_custom": (ctypes.c_int, [ctypes.c_int, _INT, _INT, _INT, ctypes.c_double, ctypes.c_void_p,
+                                                  ctypes.c_void_p, _P(_P(Orientation))]),
     "fkpc_skeleton_run_custom": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _P(Options), ctypes.c_void_p,
                                                 ctypes.c_void_p, _P(_P(Result))]),
     "fkpc_ci_level_batch": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, _INT, ctypes.c_int,
@@ -328,6 +353,195 @@ def _run_skeleton(X, alpha, labels, o, method, evaluator):
 
 def _deleted(adj, i, j):
     return i != j and not adj[i, j]
+
+
+def orient_wanpdag(skeleton, data, alpha=0.1, index=1, numCol=None, ci_method="dcc.gamma", hsic_params=None,
+                   orient_collider=True, solve_confl=False, rules=(True, True, True), device=0, selection="magic",
+                   strict=True):
+    """WAN-PDAG orientation of a skeleton (kpcalg's udag2wanpdag as kpc()
+    runs it), every regrVonPS residual fit and CI test on the device.
+
+    Mirrors ``fastkpc_orient_wanpdag_kpcalg_authority`` (fastkpc/R/fast_kpc.R:263-330):
+    ``skeleton`` is a ``fastkpc_compatible_cuda_skeleton`` result (its
+    ``adjacency`` and ``sepsets``); alpha, numCol (default floor(n/10)), the
+    CI method (gamma methods) and hsic_params as the skeleton used them.
+    Only kpc()'s defaults are provided: orient_collider = True, solve_confl =
+    False, all three rules.
+
+    Returns a dict: ``pdag`` (int p x p; pdag[i, j] = 1, pdag[j, i] = 0 is
+    i -> j), ``ci_trace`` (column arrays of every CI test in call order),
+    ``diagnostics`` (orientation counts, regrVonPS calls, residual fits and
+    cache hits, ci_test_count, orientation_elapsed_sec).
+    """
+    if not orient_collider or solve_confl or tuple(bool(r) for r in rules) != (True, True, True):
+        raise ValueError("only kpc()'s orientation defaults are provided: orient_collider = TRUE, "
+                         "solve_confl = FALSE, rules = c(TRUE, TRUE, TRUE)")
+    if ci_method not in ("dcc.gamma", "hsic.gamma"):
+        raise ValueError("the orientation covers the gamma methods")
+    X = _as_data(data)
+    n, p = X.shape
+    A, offs, vals = _skeleton_arrays(skeleton, p)
+    hsic = hsic_params or {"sig": 1}
+    o = make_options(ci_method=ci_method, alpha=alpha, index=index, numCol=n // 10 if numCol is None else numCol,
+                     hsic_sig=hsic.get("sig", 1), device=device, strict=strict, selection=selection)
+    lib = load_library()
+    res = _P(Orientation)()
+    _check(lib.fkpc_orient_wanpdag(_ptr(X, ctypes.c_double), n, p, _ptr(A, ctypes.c_int),
+                                   _ptr(offs, ctypes.c_int), _ptr(vals, ctypes.c_int), ctypes.byref(o),
+                                   ctypes.byref(res)))
+    out = _read_orientation(lib, res, p)
+    out["ci_method"] = ci_method
+    return out
+
+
+# One regrVonPS call for fkpc_orient_wanpdag_custom.
+REGRVONPS_EVALUATOR = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, _INT, ctypes.c_int, _INT,
+                                       ctypes.c_int, _DBL)
+
+
+def orient_wanpdag_custom(skeleton, p, alpha, regr_v_on_ps):
+    """The orientation's graph logic (``fkpc_orient_wanpdag_custom``) with
+    every regrVonPS call answered by ``regr_v_on_ps(target, S, Z)``, which
+    returns one p-value per member of S (the test of the residual of target
+    on Z against that member).  Uses no device.  Same result dict as
+    ``orient_wanpdag``."""
+    A, offs, vals = _skeleton_arrays(skeleton, p)
+    errors = []
+
+    def cb(_user, target, subset, ns, cond, nz, out):
+        try:
+            pv = regr_v_on_ps(int(target), [int(subset[k]) for k in range(ns)], [int(cond[k]) for k in range(nz)])
+            if len(pv) != ns:
+                raise ValueError("the evaluator must return one p-value per member of S")
+            for k in range(ns):
+                out[k] = float(pv[k])
+            return 0
+        except Exception as e:  # reported after the call returns
+            errors.append(e)
+            return 1
+    fn = REGRVONPS_EVALUATOR(cb)
+    lib = load_library()
+    res = _P(Orientation)()
+    rc = lib.fkpc_orient_wanpdag_custom(p, _ptr(A, ctypes.c_int), _ptr(offs, ctypes.c_int),
+                                        _ptr(vals, ctypes.c_int), float(alpha), ctypes.cast(fn, ctypes.c_void_p),
+                                        None, ctypes.byref(res))
+    if errors:
+        raise errors[0]
+    _check(rc)
+    return _read_orientation(lib, res, p)
+
+
+def _skeleton_arrays(skeleton, p):
+    """(adjacency int32 column-major, sepset CSR offsets, values) of a skeleton dict."""
+    adj = np.asarray(skeleton["adjacency"]).astype(bool)
+    if adj.shape != (p, p):
+        raise ValueError("skeleton adjacency must be p x p")
+    sep = skeleton.get("sepsets")
+    offs = np.zeros(p * p + 1, dtype=np.int32)
+    vals = []
+    for j in range(p):
+        for i in range(p):
+            if isinstance(sep, dict):
+                s_ij = sep.get((i, j))
+            else:
+                s_ij = sep[i][j] if sep is not None else None
+            if s_ij:
+                vals.extend(int(v) for v in s_ij)
+            offs[i + p * j + 1] = len(vals)
+    vals = np.asarray(vals if vals else [0], dtype=np.int32)
+    return np.asfortranarray(adj.astype(np.int32)), offs, vals
+
+
+def _read_orientation(lib, res, p):
+    try:
+        r = res.contents
+        pdag = np.ctypeslib.as_array(r.pdag, shape=(p * p,)).reshape((p, p), order="F").astype(np.int64)
+        rows = [r.trace[k] for k in range(r.tests)]
+        sv = r.set_values
+        trace = {
+            "context": ["reverseRegrVonPS" if t.reverse else "regrVonPS" for t in rows],
+            "reverse": np.array([t.reverse for t in rows], dtype=np.int64),
+            "target": np.array([t.target for t in rows], dtype=np.int64),
+            "other": np.array([t.other for t in rows], dtype=np.int64),
+            "subset": [[int(sv[t.s_offset + k]) for k in range(t.s_count)] for t in rows],
+            "residual_conditioning_set": [[int(sv[t.z_offset + k]) for k in range(t.z_count)] for t in rows],
+            "p_value": np.array([t.p_value for t in rows]),
+            "rejected": np.array([bool(t.rejected) for t in rows]),
+        }
+        diag = {"collider_orientations": r.collider_orientations, "rule1_orientations": r.rule1_orientations,
+                "rule2_orientations": r.rule2_orientations, "rule3_orientations": r.rule3_orientations,
+                "generalized_orientations": r.generalized_orientations, "regrvonps_calls": r.regrvonps_calls,
+                "residual_fits": r.residual_fits, "residual_cache_hits": r.residual_cache_hits,
+                "ci_test_count": r.tests, "orientation_elapsed_sec": r.elapsed_sec}
+        return {"pdag": pdag, "ci_trace": trace, "diagnostics": diag,
+                "authority": "kpcalg::udag2wanpdag semantics, device residuals and CI tests"}
+    finally:
+        lib.fkpc_orientation_free(res)
+
+
+def pdag_edge_counts(pdag):
+    """Directed, undirected and bidirected (conflict, value 2) edge counts of a PDAG."""
+    a = np.asarray(pdag)
+    iu = np.triu_indices(a.shape[0], 1)
+    x, y = a[iu], a.T[iu]
+    return {"directed": int(np.sum(((x == 1) & (y == 0)) | ((x == 0) & (y == 1)))),
+            "undirected": int(np.sum((x == 1) & (y == 1))),
+            "bidirected": int(np.sum((x == 2) | (y == 2)))}
+
+
+_WANPDAG_ALLOWED = {"max_conditioning_size", "index", "numCol", "trace_level", "route", "compatible_cuda_strict",
+                    "ci_method", "hsic_params", "permutation_params", "orient_collider", "solve_confl", "rules",
+                    "mode", "device", "level_graph"}
+
+
+def fastkpc_compatible_cuda_wanpdag(data, alpha=0.1, labels=None, options=None):
+    """Strict kernel-PC: the full-CUDA skeleton, then the WAN-PDAG orientation.
+
+    Mirrors ``fastkpc_compatible_cuda_wanpdag`` (fastkpc/R/fast_kpc.R:449-600):
+    the skeleton options of ``fastkpc_compatible_cuda_skeleton`` (trace_level
+    "logical" or "full") plus ``orient_collider``, ``solve_confl`` and
+    ``rules``; the orientation uses the skeleton's alpha, numCol, CI method
+    and hsic_params.  Returns ``config``, ``skeleton``, ``orientation``,
+    ``timings`` (seconds per stage) and ``metrics`` (edge counts, CI test
+    counts).
+    """
+    import time
+    options = dict(options or {})
+    unknown = set(options) - _WANPDAG_ALLOWED
+    if unknown:
+        raise ValueError("unknown compatible CUDA WAN-PDAG option(s): " + ",".join(sorted(unknown)))
+    if options.get("route", "full_cuda") != "full_cuda" or not options.get("compatible_cuda_strict", True):
+        raise ValueError("compatible CUDA WAN-PDAG requires strict full_cuda skeleton execution")
+    trace_level = options.setdefault("trace_level", "logical")
+    if trace_level not in ("logical", "full"):
+        raise ValueError("compatible CUDA WAN-PDAG requires logical or full skeleton trace")
+    orient_keys = {k: options.pop(k) for k in ("orient_collider", "solve_confl", "rules") if k in options}
+    method = options.get("ci_method", "dcc.gamma")
+    X = _as_data(data)
+    t0 = time.perf_counter()
+    skel = fastkpc_compatible_cuda_skeleton(X, alpha, labels=labels, options=options)
+    t1 = time.perf_counter()
+    orient = orient_wanpdag(skel, X, alpha=alpha, index=options.get("index", 1),
+                            numCol=options.get("numCol", X.shape[0] // 10), ci_method=method,
+                            hsic_params=options.get("hsic_params"), device=options.get("device", 0),
+                            strict=options.get("compatible_cuda_strict", True), **orient_keys)
+    t2 = time.perf_counter()
+    counts = pdag_edge_counts(orient["pdag"])
+    adj = skel["adjacency"]
+    return {
+        "schema_version": "fastkpc-compatible-cuda-wanpdag-v1",
+        "config": {"alpha": float(alpha), "ci_method": method, "skeleton_authority": "full_cuda",
+                   "orientation_authority": "device regrVonPS, kpcalg udag2wanpdag semantics",
+                   "max_conditioning_size_resolved": skel["summary"]["max_conditioning_size_resolved"]},
+        "skeleton": skel,
+        "orientation": orient,
+        "timings": {"skeleton": t1 - t0, "orientation": t2 - t1, "total": t2 - t0},
+        "metrics": {"skeleton_edge_count": int(np.sum(np.triu(adj, 1))),
+                    "directed_edge_count": counts["directed"], "undirected_edge_count": counts["undirected"],
+                    "bidirected_edge_count": counts["bidirected"],
+                    "skeleton_ci_test_count": int(sum(skel["n_edgetests"])),
+                    "orientation_ci_test_count": orient["diagnostics"]["ci_test_count"]},
+    }
 
 
 def _tests_arrays(tests):

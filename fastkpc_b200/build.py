@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfastkpc_b200.so")
-SOURCES = ["hostla.cpp", "design.cpp", "capi.cpp", "runtime.cu", "kernels_fit.cu", "kernels_stat.cu", "kernels_tprs.cu", "kernels_geom.cu", "noalloc.cu"]
+SOURCES = ["hostla.cpp", "design.cpp", "capi.cpp", "orient.cpp", "runtime.cu", "kernels_fit.cu", "kernels_stat.cu", "kernels_tprs.cu", "kernels_geom.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "../../include/fastkpc_b200.h"
+#include "orient.h"
 #include "runtime.h"
 
 namespace {
@@ -479,6 +480,71 @@ fkpc_result* make_result(const Run& run, const fkpc_options& options, int n, int
   return r;
 }
 
+void validate_skeleton_input(int p, const int* adjacency, const int* sepset_offsets, const int* sepset_values) {
+  using fkpc::Error;
+  if (!adjacency || !sepset_offsets) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+  const size_t pp = static_cast<size_t>(p) * p;
+  for (int i = 0; i < p; ++i)
+    for (int j = 0; j < p; ++j) {
+      const int a = adjacency[i + static_cast<size_t>(p) * j], b = adjacency[j + static_cast<size_t>(p) * i];
+      if ((a != 0 && a != 1) || a != b || (i == j && a != 0))
+        throw Error(FKPC_STATUS_INVALID_ARGUMENT, "adjacency must be a symmetric 0/1 matrix with a zero diagonal");
+    }
+  if (sepset_offsets[0] != 0) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "sepset offsets must start at 0");
+  for (size_t c = 0; c < pp; ++c)
+    if (sepset_offsets[c + 1] < sepset_offsets[c])
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "sepset offsets must be nondecreasing");
+  if (sepset_offsets[pp] > 0 && !sepset_values) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "null sepset values");
+  for (int k = 0; k < sepset_offsets[pp]; ++k)
+    if (sepset_values[k] < 0 || sepset_values[k] >= p)
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "sepset member out of range");
+}
+
+fkpc_orientation* make_orientation(const fkpc::Orientation& o, int p, std::chrono::steady_clock::time_point t0) {
+  std::vector<fkpc_orientation_test> rows;
+  std::vector<int> sets;
+  for (const auto& t : o.trace) {
+    fkpc_orientation_test r{};
+    r.reverse = t.reverse;
+    r.target = t.target;
+    r.other = t.other;
+    r.s_offset = static_cast<int>(sets.size());
+    r.s_count = static_cast<int>(t.S.size());
+    sets.insert(sets.end(), t.S.begin(), t.S.end());
+    r.z_offset = static_cast<int>(sets.size());
+    r.z_count = static_cast<int>(t.Z.size());
+    sets.insert(sets.end(), t.Z.begin(), t.Z.end());
+    r.p_value = t.p_value;
+    r.rejected = t.rejected ? 1 : 0;
+    rows.push_back(r);
+  }
+  fkpc_orientation* r = static_cast<fkpc_orientation*>(std::calloc(1, sizeof(fkpc_orientation)));
+  if (!r) throw std::bad_alloc();
+  try {
+    r->pdag = copy_out(o.pdag);
+    r->trace = copy_out(rows);
+    r->set_values = copy_out(sets);
+  } catch (...) {
+    std::free(r->pdag);
+    std::free(r->trace);
+    std::free(r->set_values);
+    std::free(r);
+    throw;
+  }
+  r->p = p;
+  r->collider_orientations = o.collider;
+  r->rule1_orientations = o.rule1;
+  r->rule2_orientations = o.rule2;
+  r->rule3_orientations = o.rule3;
+  r->generalized_orientations = o.generalized;
+  r->regrvonps_calls = o.regrvonps_calls;
+  r->residual_fits = o.residual_fits;
+  r->residual_cache_hits = o.residual_cache_hits;
+  r->tests = static_cast<int>(rows.size());
+  r->elapsed_sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return r;
+}
+
 }  // namespace
 
 extern "C" {
@@ -518,6 +584,53 @@ int fkpc_skeleton_run(const double* data, int n, int p, const fkpc_options* opti
     skeleton(data, n, p, *options, &run);
     *out = make_result(run, *options, n, p, t0);
   });
+}
+
+int fkpc_orient_wanpdag(const double* data, int n, int p, const int* adjacency, const int* sepset_offsets,
+                        const int* sepset_values, const fkpc_options* options, fkpc_orientation** out) {
+  return guarded([&]() {
+    using fkpc::Error;
+    if (!data || !options || !out) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    validate_options(*options, n, p);
+    if (options->ci_method != FKPC_DCC_GAMMA && options->ci_method != FKPC_HSIC_GAMMA)
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "the orientation covers the gamma methods");
+    validate_skeleton_input(p, adjacency, sepset_offsets, sepset_values);
+    std::lock_guard<std::mutex> lock(device_mutex(options->device));
+    auto t0 = std::chrono::steady_clock::now();
+    auto& eng = engine_for(options->device);
+    eng.load(data, n, p);
+    *out = make_orientation(
+        fkpc::orient_wanpdag(eng, *options, data, n, p, adjacency, sepset_offsets, sepset_values), p, t0);
+  });
+}
+
+int fkpc_orient_wanpdag_custom(int p, const int* adjacency, const int* sepset_offsets, const int* sepset_values,
+                               double alpha, fkpc_regrvonps_evaluator evaluator, void* user,
+                               fkpc_orientation** out) {
+  return guarded([&]() {
+    using fkpc::Error;
+    if (!evaluator || !out) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (p < 2) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "need p >= 2");
+    if (!(std::isfinite(alpha) && alpha > 0.0 && alpha < 1.0))
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "alpha must lie in (0, 1)");
+    validate_skeleton_input(p, adjacency, sepset_offsets, sepset_values);
+    auto t0 = std::chrono::steady_clock::now();
+    fkpc::RegrVonPs eval = [&](int v, const std::vector<int>& S, const std::vector<int>& Z, double* pv) {
+      const int rc = evaluator(user, v, S.data(), static_cast<int>(S.size()), Z.data(), static_cast<int>(Z.size()), pv);
+      if (rc != 0) throw Error(rc, "orientation evaluator failed with status " + std::to_string(rc));
+    };
+    *out = make_orientation(fkpc::orient_wanpdag(eval, alpha, p, adjacency, sepset_offsets, sepset_values), p, t0);
+  });
+}
+
+void fkpc_orientation_free(fkpc_orientation* r) {
+  if (!r) return;
+  std::free(r->pdag);
+  std::free(r->trace);
+  std::free(r->set_values);
+  std::free(r);
 }
 
 int fkpc_skeleton_run_custom(const double* data, int n, int p, const fkpc_options* options,

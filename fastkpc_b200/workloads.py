@@ -111,3 +111,25 @@ def adjoint_targets_1000(seed=5, count=2048):
 # Seeds of the n=351, p=48 full-skeleton rows: the deepest-skeleton seed
 # (deep_skeleton_seed) and seed 3.
 SKELETON_351X48_SEEDS = (537, 3)
+
+
+def orientation_collider_free(n=300, p=12, edge_prob=0.25, seed=2, max_in_degree=4):
+    """An orientation input with no colliders: the SEM's true skeleton, and
+    for every non-adjacent pair a separating set of all other nodes (so no
+    v-structure is oriented and every undirected neighbourhood goes through
+    the regrVonPS stage).  Returns (X, adjacency p x p bool, sepsets
+    {(a, b): S})."""
+    X, edges = nonlinear_sem(n, p, edge_prob, seed, max_in_degree=max_in_degree)
+    adj = np.zeros((p, p), dtype=bool)
+    for i, j in edges:
+        adj[i, j] = adj[j, i] = True
+    sepsets = {(a, b): [c for c in range(p) if c not in (a, b)]
+               for a in range(p) for b in range(p) if a != b and not adj[a, b]}
+    return X, adj, sepsets
+
+
+ORIENTATION_CASES = {
+    # name: (generator, kwargs)
+    "free300x12_s2": dict(n=300, p=12, edge_prob=0.25, seed=2),
+    "free351x24_s4": dict(n=351, p=24, edge_prob=0.2, seed=4),
+}

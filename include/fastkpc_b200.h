@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define FKPC_ABI_VERSION 4
+#define FKPC_ABI_VERSION 5
 
 #if defined(__GNUC__)
 #define FKPC_API __attribute__((visibility("default")))
@@ -151,6 +151,73 @@ typedef struct fkpc_result {
 FKPC_API int fkpc_skeleton_run(const double* data_colmajor, int n, int p,
                       const fkpc_options* options, fkpc_result** out);
 FKPC_API void fkpc_result_free(fkpc_result* result);
+
+/* one CI test of the orientation's regrVonPS calls */
+typedef struct fkpc_orientation_test {
+  int reverse;         /* 0: the tested node's own call; 1: the reverse call for a W in S */
+  int target;          /* the regressed node */
+  int other;           /* the member of S tested against the residual */
+  int s_offset;        /* S, into fkpc_orientation.set_values */
+  int s_count;
+  int z_offset;        /* S + parents(target), sorted: the residual's conditioning set */
+  int z_count;
+  double p_value;
+  int rejected;        /* p_value < alpha */
+} fkpc_orientation_test;
+
+typedef struct fkpc_orientation {
+  int p;
+  int* pdag;                     /* p*p column-major: pdag[i+p*j] = 1, pdag[j+p*i] = 0 is i -> j; both 1: i - j */
+  int collider_orientations;     /* collider triples that changed the graph */
+  int rule1_orientations;        /* edges each rule changed */
+  int rule2_orientations;
+  int rule3_orientations;
+  int generalized_orientations;  /* accepted S -> V orientations */
+  int regrvonps_calls;
+  int residual_fits;             /* residuals fitted on the device */
+  int residual_cache_hits;       /* residuals reused for a repeated (target, conditioning set) */
+  int tests;
+  fkpc_orientation_test* trace;  /* every CI test in call order */
+  int* set_values;
+  double elapsed_sec;
+} fkpc_orientation;
+
+/*
+ * WAN-PDAG orientation of a skeleton (kpcalg udag2wanpdag with kpc()'s
+ * defaults: colliders, generalised orientations by regrVonPS, rules 1-3 to a
+ * fixed point; no unfaithful triples, solve.confl = FALSE).  adjacency is
+ * p*p column-major (symmetric, zero diagonal); the sepsets are a CSR over
+ * cells i + p*j as fkpc_result holds them.  options supplies alpha, the CI
+ * method (gamma methods), numCol, the HSIC sig, the selection and the device.
+ * Every residual is fitted and every CI test evaluated on the device.
+ * Replaces fastkpc_orient_wanpdag_kpcalg_authority
+ * (fastkpc/R/fast_kpc.R:263-330) and C_fast_orient_wanpdag_cuda
+ * (fastkpc/R/cuda_native.R:2695, fastkpc/src/wanpdag_engine.hpp:12).
+ */
+FKPC_API int fkpc_orient_wanpdag(const double* data_colmajor, int n, int p, const int* adjacency,
+                                 const int* sepset_offsets, const int* sepset_values,
+                                 const fkpc_options* options, fkpc_orientation** out);
+FKPC_API void fkpc_orientation_free(fkpc_orientation* orientation);
+
+/*
+ * One regrVonPS call for fkpc_orient_wanpdag_custom: fills p_values[k] with
+ * the p-value of the test of (residual of ``target`` on ``conditioning``
+ * (S + parents(target), sorted), data[:, subset[k]]) for k < subset_count,
+ * and returns 0, or a positive FKPC_STATUS_* code.
+ */
+typedef int (*fkpc_regrvonps_evaluator)(void* user, int target, const int* subset, int subset_count,
+                                        const int* conditioning, int conditioning_count, double* p_values);
+
+/*
+ * fkpc_orient_wanpdag's graph logic with every regrVonPS call answered by
+ * ``evaluator`` (no device use): the hook through which a host supplies its
+ * own CI backend.  Replaces orient_wanpdag_native's evaluator argument
+ * (fastkpc/src/wanpdag_engine.hpp:12-16).
+ */
+FKPC_API int fkpc_orient_wanpdag_custom(int p, const int* adjacency, const int* sepset_offsets,
+                                        const int* sepset_values, double alpha,
+                                        fkpc_regrvonps_evaluator evaluator, void* user,
+                                        fkpc_orientation** out);
 
 /*
  * Evaluator of one level's CI tests for fkpc_skeleton_run_custom: fills

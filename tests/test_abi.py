@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol(lib_built):
 
 
 def test_abi_version_and_defaults(lib_built):
-    assert lib_built.fkpc_abi_version() == 4
+    assert lib_built.fkpc_abi_version() == 5
     o = fk.make_options()
     assert o.alpha == 0.1 and o.num_col == 35 and o.index == 1.0 and o.strict == 1
     assert o.selection == 0 and fk.make_options(selection="gn_newton").selection == 1

@@ -9,6 +9,9 @@ numCol 35, hsic sig 1) on
   SEM of seed 537), for hsic.gamma and dcc.gamma;
 * the oracle skeleton of ``workloads.skeleton_200x10(1)`` (computed here),
   for both methods;
+* the reference's own 500 x 50 development dataset and its dcc.gamma
+  skeleton (``dev500x50.npz`` and the sepsets of ``dev500x50_trace.json``,
+  read from the reference's fixture by ``make_golden.py``), for both methods;
 * the collider-free inputs ``workloads.ORIENTATION_CASES`` (every
   neighbourhood goes through regrVonPS), for both methods;
 
@@ -18,6 +21,7 @@ input adjacency and sepsets (p x p x max|S|, -1 padded), the PDAG, the counts
 trace in call order (reverse flag, target, other, S and Z -1 padded, p,
 rejected).
 """
+import json
 import os
 import sys
 import time
@@ -88,6 +92,12 @@ def main():
     for method in ("hsic.gamma", "dcc.gamma"):
         res = skeleton.skeleton(X, ALPHA, method=method, num_col=35, sig=1.0)
         run_case(out, "skel200x10_s1", X, res["adjacency"], res["sepsets"], method)
+    X = np.load(os.path.join(HERE, "dev500x50.npz"))["data"]
+    adj = np.load(os.path.join(HERE, "dev500x50.npz"))["adjacency"].astype(bool)
+    with open(os.path.join(HERE, "dev500x50_trace.json")) as f:
+        sepsets = {(i, j): S for i, j, S in json.load(f)["sepsets"]}
+    for method in ("hsic.gamma", "dcc.gamma"):
+        run_case(out, "dev500x50", X, adj, sepsets, method)
     for name, kw in workloads.ORIENTATION_CASES.items():
         X, adj, sepsets = workloads.orientation_collider_free(**kw)
         for method in ("hsic.gamma", "dcc.gamma"):

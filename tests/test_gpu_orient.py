@@ -2,7 +2,8 @@
 
 Every case of ``tests/golden/orient_oracle.npz`` (``make_orient_fixture.py``):
 the oracle skeletons of the 351 x 48 SEM (seed 537) and of the 200 x 10 SEM
-(seed 1), and the collider-free inputs of ``workloads.ORIENTATION_CASES``,
+(seed 1), the reference's 500 x 50 development dataset with its own
+skeleton, and the collider-free inputs of ``workloads.ORIENTATION_CASES``,
 each for hsic.gamma and dcc.gamma.  Bars: the PDAG, the orientation counts
 and the CI trace's calls and decisions exact; its p-values within 1e-9 (the
 measured maximum is printed).  The full strict pipeline (device skeleton,
@@ -20,7 +21,7 @@ from tests.test_orient import COUNT_KEYS, LIB_COUNT_KEYS, case_input, fixture_se
 
 pytestmark = pytest.mark.gpu
 
-CASES = [f"{c}_{m}" for c in ("skel351x48_s537", "skel200x10_s1", "free300x12_s2", "free351x24_s4")
+CASES = [f"{c}_{m}" for c in ("skel351x48_s537", "skel200x10_s1", "dev500x50", "free300x12_s2", "free351x24_s4")
          for m in ("hsic_gamma", "dcc_gamma")]
 
 

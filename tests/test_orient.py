@@ -214,6 +214,8 @@ def case_input(name):
         return workloads.skeleton_351x48(537)
     if name.startswith("skel200x10_s1"):
         return workloads.skeleton_200x10(1)
+    if name.startswith("dev500x50"):
+        return np.load(golden_path("dev500x50.npz"))["data"]
     for case, kw in workloads.ORIENTATION_CASES.items():
         if name.startswith(case):
             return workloads.orientation_collider_free(**kw)[0]
@@ -238,7 +240,7 @@ def fixture_trace(ofx, key):
 
 def test_fixture_covers_the_cases(ofx):
     names = fixture_cases(ofx)
-    assert len(names) == 8
+    assert len(names) == 10
     total = {k: 0 for k in COUNT_KEYS}
     for name in names:
         for k, v in zip(COUNT_KEYS, ofx[name + "_counts"]):
@@ -246,7 +248,8 @@ def test_fixture_covers_the_cases(ofx):
     assert total["collider"] > 0 and total["rule1"] > 0 and total["rule2"] > 0 and total["generalized"] > 0
 
 
-@pytest.mark.parametrize("case", ["skel200x10_s1_dcc_gamma", "free300x12_s2_hsic_gamma", "free351x24_s4_dcc_gamma"])
+@pytest.mark.parametrize("case", ["skel200x10_s1_dcc_gamma", "free300x12_s2_hsic_gamma", "free351x24_s4_dcc_gamma",
+                                  "dev500x50_dcc_gamma"])
 def test_oracle_reproduces_fixture_and_library_logic_agrees(lib_built, ofx, case):
     """The oracle regenerates the fixture (pin), and the library's graph logic
     fed the oracle's regrVonPS p-values reproduces it exactly."""

@@ -633,14 +633,18 @@ def ci_plain_one(data, x, y, S, ci_method="dcc.gamma", **kw):
     return {name: getattr(rec, name) for name, _ in CiRecord._fields_}
 
 
-def regress_batch(data, fits, max_penalties=12, device=0, selection="magic"):
+def regress_batch(data, fits, max_penalties=None, device=0, selection="magic"):
     """regrXonS residuals for ``[(target, S), ...]``: (residuals n x k, log_sp k x m, status k).
 
-    ``selection``: "magic" (mgcv magic's search, as the reference) or
-    "gn_newton" (Newton on the Gauss-Newton Hessian of GCV) for |S| >= 3."""
+    ``max_penalties`` (default: the largest |S|) columns of log_sp, NaN
+    beyond a fit's penalties.  ``selection``: "magic" (mgcv magic's search,
+    as the reference) or "gn_newton" (Newton on the Gauss-Newton Hessian of
+    GCV) for |S| >= 3."""
     X = _as_data(data)
     n, p = X.shape
     k = len(fits)
+    if max_penalties is None:
+        max_penalties = max([len(f[1]) for f in fits] + [1])
     tg = np.array([f[0] for f in fits], dtype=np.int32)
     offs = np.zeros(k + 1, dtype=np.int32)
     vals = []
@@ -678,7 +682,8 @@ def stat_batch(residuals, pairs, ci_method="dcc.gamma", permutations=None, **kw)
 
 
 STAGES = {"fit_single": 0, "fit_multi_small": 1, "fit_multi_large": 2, "dcov_components": 3, "dcov_pairs": 4,
-          "hsic_components": 5, "hsic_pairs": 6, "lowrank_eigen": 7, "lowrank_pairs": 8, "fit_multi_huge": 9}
+          "hsic_components": 5, "hsic_pairs": 6, "lowrank_eigen": 7, "lowrank_pairs": 8, "fit_multi_huge": 9,
+          "fit_multi_wide": 10}
 
 
 class StagedBatch:

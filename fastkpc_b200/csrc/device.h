@@ -10,7 +10,10 @@
 
 namespace fkpc {
 
-constexpr int kMaxPenalties = 12;     // |S| <= 12 (design widths up to q = 109)
+constexpr int kMaxPenalties = 62;     // |S| <= 62 (p <= 64), design widths up to q = 559
+constexpr int kCtaPenalties = 12;     // the shared-memory CTA fit classes: |S| <= 12
+constexpr int kWideQ = 560;           // the wide fit class: q <= 560 coefficients,
+constexpr int kWideR = 496;           // at most 496 stacked penalty-root rows
 constexpr int kMaxSingleQ = 32;       // single-penalty designs have q in {10, 30}
 constexpr int kStatusOk = 0;
 constexpr int kStatusNumeric = 3;
@@ -30,8 +33,10 @@ constexpr int kWarpTri = kWarpQ * (kWarpQ + 1) / 2;
 // Row-packed upper triangle of width kWarpQ: row t holds columns t..kWarpQ-1.
 FKPC_HD constexpr int packed_row(int t, int c) { return t * (2 * kWarpQ - t + 1) / 2 + (c - t); }
 
-// One conditioning set's geometry, resident in a device arena of doubles.
-struct DesignDev {
+// One conditioning set's geometry, resident in a device arena of doubles,
+// for at most MP penalties.
+template <int MP>
+struct DesignT {
   int kind;        // 1: single penalty (spectral), 2: several penalties (augmented QR)
   int q;           // coefficients
   int m;           // penalties
@@ -41,13 +46,16 @@ struct DesignDev {
   int64_t spec;    // kind 1: hat eigenvalues e (q)
   int64_t roots;   // kind 2: penalty roots, block j dim_j x rank_j column-major, consecutive
   int64_t rpack;   // kind 2 with q <= kWarpQ: R row-packed (kWarpTri doubles, zero beyond q), else -1
-  int off[kMaxPenalties];
-  int dim[kMaxPenalties];
-  int rank[kMaxPenalties];
-  int rowoff[kMaxPenalties];    // first stacked-root row of block j
-  int rootoff[kMaxPenalties];   // offset of block j's root inside ``roots``
-  double log_sp0[kMaxPenalties];
+  int off[MP];
+  int dim[MP];
+  int rank[MP];
+  int rowoff[MP];    // first stacked-root row of block j
+  int rootoff[MP];   // offset of block j's root inside ``roots``
+  double log_sp0[MP];
 };
+using DesignDev = DesignT<kMaxPenalties>;
+// The warp fit class's copy in shared memory (m <= kWarpM).
+using WarpDesign = DesignT<kWarpM>;
 
 // One additive design whose geometry the device builds: X = [1 | B_1 | ...]
 // gathered from the univariate smooth bases, X = Q R by Householder, Q and R

@@ -26,8 +26,10 @@ cudaError_t launch_fit_single(const DesignDev* designs, const double* arena, con
                               const FitJob* jobs, int count, double* residuals, FitResult* results,
                               cudaStream_t stream);
 
-// qmax_class 0: q <= 40 and rank sum <= 32 (warp per fit); 1: q <= 76 and rank sum <= 64;
-// 2: q <= 112 and rank sum <= 96 (working set in global memory).
+// Fit classes (qmax_class): 0: q <= 40, rank sum <= 32, m <= 4 (warp per fit);
+// 1: q <= 76, rank sum <= 64, m <= 12; 2: q <= 112, rank sum <= 96, m <= 12
+// (working set in global memory); 3: q <= 560, rank sum <= 496, m <= 62
+// (working set and scalars in global memory, persistent CTAs).
 // Score, gradient, Gauss-Newton and exact Hessian of GCV in log(lambda) at
 // ``count`` points (rho: count x m) for design ``design`` and response y.
 // qmax_class 0: q <= kWarpQ, rsum <= kWarpR, m <= kWarpM; 1: q <= 76, rsum <= 64;
@@ -45,7 +47,7 @@ cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const dou
 // (class 0: ``after_warp`` is recorded on ``stream`` once the one-warp kernel is
 // queued, before the speculative continuation of the fits it deferred)
 // Doubles of global workspace class ``qmax_class`` needs for ``count`` fits
-// (class 2: q <= 112, rsum <= 96, working set in global memory; 0 otherwise).
+// (classes 2 and 3; 0 otherwise).
 size_t multi_workspace_doubles(int qmax_class, int count);
 
 // Optional index list of a statistic launch: work item b of the grid is

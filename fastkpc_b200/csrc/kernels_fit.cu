@@ -108,6 +108,20 @@ __device__ SingleObjective single_objective(double log_sp, double e, double z, b
 
 }  // namespace
 
+// The result record of one fit, written field by field (log_sp[j] for
+// j < m, NaN beyond), so no kernel holds a whole record in registers.
+__device__ __forceinline__ void store_result(FitResult* __restrict__ out, const double* log_sp, int m, double score,
+                                             double edf, double rss, int status, int iterations, int evaluations) {
+  for (int j = 0; j < kMaxPenalties; ++j) out->log_sp[j] = j < m ? log_sp[j] : NAN;
+  out->score = score;
+  out->edf = edf;
+  out->rss = rss;
+  out->status = status;
+  out->iterations = iterations;
+  out->evaluations = evaluations;
+  out->flags = 0;
+}
+
 __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const double* __restrict__ arena,
                                   const double* __restrict__ data, int n, const FitJob* __restrict__ jobs,
                                   int job_count, double* __restrict__ residuals, FitResult* __restrict__ results) {
@@ -155,9 +169,9 @@ __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const d
   __syncwarp();
   const double ek = active ? arena[des.spec + lane] : 0.0;
 
-  FitResult res;
-  for (int j = 0; j < kMaxPenalties; ++j) res.log_sp[j] = NAN;
-  res.flags = 0;
+  struct {
+    int status;
+  } res;
   res.status = kStatusOk;
   const int max_half = 15;
   double log_sp = des.log_sp0[0];
@@ -260,15 +274,7 @@ __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const d
     for (int k = 0; k < q; ++k) f += QW[i + static_cast<int64_t>(n) * k] * coef[k];
     r[i] = y[i] - f;
   }
-  if (lane == 0) {
-    res.log_sp[0] = log_sp;
-    res.score = cur.score;
-    res.edf = cur.edf;
-    res.rss = cur.rss;
-    res.iterations = it;
-    res.evaluations = calls;
-    results[t] = res;
-  }
+  if (lane == 0) store_result(results + t, &log_sp, 1, cur.score, cur.edf, cur.rss, res.status, it, calls);
 }
 
 // ----------------------------------------------------------------- multi
@@ -308,33 +314,40 @@ struct MultiLayout {
   static constexpr int TOTAL = IDG + QMAX;
 };
 
-struct MultiScalars {
-  static constexpr int kLd = kMaxPenalties;  // leading dimension of the m x m matrices
+// Scalars and index maps of one CTA-class fit: at most MP penalties, NT
+// threads, QC coefficients and RC stacked root rows.
+template <int MP, int NT, int QC, int RC>
+struct MultiScalarsT {
+  static constexpr int kLd = MP;  // leading dimension of the m x m matrices
+  static constexpr int kThreads = NT;
   double beta[2], v0[2];
-  double red[kMultiThreads / 32];
+  double red[NT / 32];
   double score, rss, edf, rss0;  // rss0 = |y - Q Q'y|^2
-  double lam[kMaxPenalties];
-  double log_sp[kMaxPenalties];
-  double trial[kMaxPenalties];
-  double step[kMaxPenalties];
-  double grad_c[kMaxPenalties];
-  double hess_c[kMaxPenalties * kMaxPenalties];
-  double gn_c[kMaxPenalties * kMaxPenalties];  // Gauss-Newton Hessian (adjoint entry point)
-  double gradient[kMaxPenalties];
-  double newton[kMaxPenalties];
-  double steep[kMaxPenalties];
-  double ddelta[kMaxPenalties];
-  double drss[kMaxPenalties];
+  double lam[MP];
+  double log_sp[MP];
+  double trial[MP];
+  double step[MP];
+  double grad_c[MP];
+  double hess_c[MP * MP];
+  double gn_c[MP * MP];  // Gauss-Newton Hessian (adjoint entry point)
+  double gradient[MP];
+  double newton[MP];
+  double steep[MP];
+  double ddelta[MP];
+  double drss[MP];
   int status;
-  int nzrow[128];
-  int col_block[128];
-  int pair_i[kMaxPenalties * (kMaxPenalties + 1) / 2];
-  int pair_j[kMaxPenalties * (kMaxPenalties + 1) / 2];
-  double ja[kMaxPenalties * kMaxPenalties];  // thread-0 scratch: Jacobi matrix / Cholesky factor
-  double jv[kMaxPenalties * kMaxPenalties];  // Jacobi rotations
+  int nzrow[QC];
+  int col_block[RC];
+  int pair_i[MP * (MP + 1) / 2];
+  int pair_j[MP * (MP + 1) / 2];
+  double ja[MP * MP];  // thread-0 scratch: Jacobi matrix / Cholesky factor
+  double jv[MP * MP];  // Jacobi rotations
 };
+// the shared-memory classes (q <= 112, |S| <= 12)
+using MultiScalars = MultiScalarsT<kCtaPenalties, kMultiThreads, 128, 128>;
 
-__device__ double block_sum(double v, MultiScalars* sc) {
+template <class S>
+__device__ double block_sum(double v, S* sc) {
   v = warp_sum(v);
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -343,17 +356,17 @@ __device__ double block_sum(double v, MultiScalars* sc) {
   __syncthreads();
   double s = 0.0;
 #pragma unroll
-  for (int w = 0; w < kMultiThreads / 32; ++w) s += sc->red[w];
+  for (int w = 0; w < S::kThreads / 32; ++w) s += sc->red[w];
   return s;
 }
 
 // Objective at sc->trial: fold the stacked roots into R (Ra'Ra = X'X + S),
 // W = R Ra^-1 by row solves, g = W'y0, W g, EDF, RSS, score.  Leaves Ra, W,
 // g, Wg in shared memory for multi_derivatives.
-template <int QMAX, int RMAX>
-__device__ void multi_core(const DesignDev& des, const double* __restrict__ arena, int n, double* sm,
-                           MultiScalars* sc) {
+template <int QMAX, int RMAX, class S = MultiScalars>
+__device__ void multi_core(const DesignDev& des, const double* __restrict__ arena, int n, double* sm, S* sc) {
   using L = MultiLayout<QMAX, RMAX>;
+  constexpr int NT = S::kThreads;
   const int tid = threadIdx.x;
   const int q = des.q, m = des.m;
   double* Ra = sm + L::RA;
@@ -362,15 +375,15 @@ __device__ void multi_core(const DesignDev& des, const double* __restrict__ aren
   const double* Rs = sm + L::RS;
   double* idg = sm + L::IDG;
   const double* roots = arena + des.roots;
-  if (tid < m) sc->lam[tid] = exp(sc->trial[tid]);
-  for (int idx = tid; idx < L::LDB * q; idx += kMultiThreads) B[idx] = 0.0;
-  for (int idx = tid; idx < q * (q + 1) / 2; idx += kMultiThreads) Ra[idx] = Rs[idx];
+  for (int j = tid; j < m; j += NT) sc->lam[j] = exp(sc->trial[j]);
+  for (int idx = tid; idx < L::LDB * q; idx += NT) B[idx] = 0.0;
+  for (int idx = tid; idx < q * (q + 1) / 2; idx += NT) Ra[idx] = Rs[idx];
   __syncthreads();
   for (int j = 0; j < m; ++j) {
     const double s = sqrt(sc->lam[j]);
     const int dim = des.dim[j], rk = des.rank[j];
     const double* root = roots + des.rootoff[j];
-    for (int idx = tid; idx < dim * rk; idx += kMultiThreads) {
+    for (int idx = tid; idx < dim * rk; idx += NT) {
       const int a = idx % dim, c = idx / dim;  // root[a + dim c] -> B[rowoff + c, off + a]
       B[(des.rowoff[j] + c) + L::LDB * (des.off[j] + a)] = s * root[idx];
     }
@@ -402,8 +415,7 @@ __device__ void multi_core(const DesignDev& des, const double* __restrict__ aren
     __syncthreads();
     const double beta = sc->beta[0];
     const double v0 = sc->v0[0];
-    const int j = tid;
-    if (beta != 0.0 && j > k && j < q) {
+    for (int j = k + 1 + tid; beta != 0.0 && j < q; j += NT) {
       double* Bj = B + L::LDB * j;
       double w0 = v0 * Ra[tri(k, j)], w1 = 0.0, w2 = 0.0, w3 = 0.0;
       int i = 0;
@@ -421,15 +433,14 @@ __device__ void multi_core(const DesignDev& des, const double* __restrict__ aren
     __syncthreads();
   }
   // reciprocal diagonal once, so the triangular solves below multiply
-  if (tid < q) {
-    const double dc = Ra[tri(tid, tid)];
+  for (int c = tid; c < q; c += NT) {
+    const double dc = Ra[tri(c, c)];
     if (dc == 0.0) sc->status = kStatusRank;
-    idg[tid] = 1.0 / dc;
+    idg[c] = 1.0 / dc;
   }
   __syncthreads();
   // W = R Ra^-1: row i solves w Ra = R(i, :), w upper triangular
-  if (tid < q) {
-    const int i = tid;
+  for (int i = tid; i < q; i += NT) {
     for (int c = i; c < q; ++c) {
       const double* rac = Ra + c * (c + 1) / 2;  // column c of Ra
       double s0 = Rs[tri(i, c)], s1 = 0.0, s2 = 0.0, s3 = 0.0;
@@ -449,8 +460,7 @@ __device__ void multi_core(const DesignDev& des, const double* __restrict__ aren
   double* g = sm + L::G;
   double* Wg = sm + L::WG;
   double e = 0.0;
-  if (tid < q) {
-    const int c = tid;
+  for (int c = tid; c < q; c += NT) {
     double s = 0.0;
     for (int i = 0; i <= c; ++i) {
       const double w = W[tri(i, c)];
@@ -462,13 +472,12 @@ __device__ void multi_core(const DesignDev& des, const double* __restrict__ aren
   const double edf = block_sum(e, sc);
   // RSS = |y - Q y0|^2 + |y0 - W g|^2: sums of squares, no cancellation
   double gg = 0.0;
-  if (tid < q) {
-    const int i = tid;
+  for (int i = tid; i < q; i += NT) {
     double s = 0.0;
     for (int c = i; c < q; ++c) s += W[tri(i, c)] * g[c];
     Wg[i] = s;
     const double d = y0[i] - s;
-    gg = d * d;
+    gg += d * d;
   }
   const double part = block_sum(gg, sc);
   if (tid == 0) {
@@ -490,10 +499,10 @@ __device__ void multi_core(const DesignDev& des, const double* __restrict__ aren
 // M_j = T_j T_j' with T = Ra^-T root; with C = T'T and D = (WT)'(WT) every
 // trace is a block sum: d delta_j = lam_j sum_{a in j} D_aa,
 // d rss_j = 2 lam_j b_j'a_j, tr(M_i M_j P) = sum C_ab D_ab over block (i, j).
-template <int QMAX, int RMAX>
-__device__ void multi_derivatives(const DesignDev& des, const double* __restrict__ arena, int n, double* sm,
-                                  MultiScalars* sc) {
+template <int QMAX, int RMAX, class S = MultiScalars>
+__device__ void multi_derivatives(const DesignDev& des, const double* __restrict__ arena, int n, double* sm, S* sc) {
   using L = MultiLayout<QMAX, RMAX>;
+  constexpr int NT = S::kThreads;
   const int tid = threadIdx.x;
   const int q = des.q, m = des.m, rs = des.rsum;
   const double* Ra = sm + L::RA;
@@ -507,8 +516,7 @@ __device__ void multi_derivatives(const DesignDev& des, const double* __restrict
   double* bv = sm + L::BV;
   const double* roots = arena + des.roots;
   // T(:, col) = Ra^-T root(:, col): forward substitution, one thread per column
-  if (tid < rs) {
-    const int col = tid;
+  for (int col = tid; col < rs; col += NT) {
     const int j = sc->col_block[col];
     const int c = col - des.rowoff[j];
     const int off = des.off[j], dim = des.dim[j];
@@ -531,33 +539,32 @@ __device__ void multi_derivatives(const DesignDev& des, const double* __restrict
     }
   }
   // e1 = g - W'(W g)
-  for (int c = tid; c < q; c += kMultiThreads) {
+  for (int c = tid; c < q; c += NT) {
     double s = 0.0;
     for (int i = 0; i <= c; ++i) s += W[tri(i, c)] * Wg[i];
     e1[c] = g[c] - s;
   }
   __syncthreads();
   // W T, a = T'g, b = T'e1
-  for (int idx = tid; idx < q * rs; idx += kMultiThreads) {
+  for (int idx = tid; idx < q * rs; idx += NT) {
     const int i = idx % q, col = idx / q;
     const int j = sc->col_block[col];
     double s = 0.0;
     for (int t = max(i, des.off[j]); t < q; ++t) s += W[tri(i, t)] * T[t + L::LDT * col];
     WT[i + L::LDT * col] = s;
   }
-  if (tid < rs) {
+  for (int col = tid; col < rs; col += NT) {
     double sa = 0.0, sb = 0.0;
     for (int i = 0; i < q; ++i) {
-      const double tv = T[i + L::LDT * tid];
+      const double tv = T[i + L::LDT * col];
       sa += tv * g[i];
       sb += tv * e1[i];
     }
-    av[tid] = sa;
-    bv[tid] = sb;
+    av[col] = sa;
+    bv[col] = sb;
   }
   __syncthreads();
-  if (tid < m) {
-    const int j = tid;
+  for (int j = tid; j < m; j += NT) {
     double dd = 0.0, dr = 0.0;
     for (int a = des.rowoff[j]; a < des.rowoff[j] + des.rank[j]; ++a) {
       double d = 0.0;
@@ -575,7 +582,7 @@ __device__ void multi_derivatives(const DesignDev& des, const double* __restrict
   const double s2 = 2.0 * s1 * sc->rss / delta;
   const int npair = m * (m + 1) / 2;
   const int warp = tid >> 5, lane = tid & 31;
-  for (int pidx = warp; pidx < npair; pidx += kMultiThreads / 32) {
+  for (int pidx = warp; pidx < npair; pidx += NT / 32) {
     const int bi = sc->pair_i[pidx], bj = sc->pair_j[pidx];
     const int ri = des.rank[bi], rj = des.rank[bj];
     const int oi = des.rowoff[bi], oj = des.rowoff[bj];
@@ -606,16 +613,16 @@ __device__ void multi_derivatives(const DesignDev& des, const double* __restrict
       }
       const double h = -2.0 * s1 / delta * (sc->ddelta[bj] * sc->drss[bi] + sc->ddelta[bi] * sc->drss[bj]) +
                        s1 * d2rss + 3.0 * s2 / delta * sc->ddelta[bi] * sc->ddelta[bj] - s2 * d2delta;
-      sc->hess_c[bi + kMaxPenalties * bj] = h;
-      sc->hess_c[bj + kMaxPenalties * bi] = h;
+      sc->hess_c[bi + S::kLd * bj] = h;
+      sc->hess_c[bj + S::kLd * bi] = h;
       // Gauss-Newton: V = |f|^2, f = sqrt(n) r / delta, dr_i . dr_j = ll a_i' D_ij a_j
       const double gn = 2.0 * s1 * ll * t1 - s1 / delta * (sc->ddelta[bj] * sc->drss[bi] + sc->ddelta[bi] * sc->drss[bj]) +
                         s2 / delta * sc->ddelta[bi] * sc->ddelta[bj];
-      sc->gn_c[bi + kMaxPenalties * bj] = gn;
-      sc->gn_c[bj + kMaxPenalties * bi] = gn;
+      sc->gn_c[bi + S::kLd * bj] = gn;
+      sc->gn_c[bj + S::kLd * bi] = gn;
     }
   }
-  if (tid < m) sc->grad_c[tid] = s1 * sc->drss[tid] - s2 * sc->ddelta[tid];
+  for (int j = tid; j < m; j += NT) sc->grad_c[j] = s1 * sc->drss[j] - s2 * sc->ddelta[j];
   __syncthreads();
 }
 
@@ -670,7 +677,7 @@ __device__ void newton_from_hessian_eigen(int m, S* sc, bool* steepest) {
     if (a[j + S::kLd * j] < 0.0) neg = true;
   *steepest = neg;
   if (!neg) {
-    double proj[kMaxPenalties];
+    double proj[S::kLd];
     for (int c = 0; c < m; ++c) {
       double s = 0.0;
       for (int r = 0; r < m; ++r) s += v[r + S::kLd * c] * sc->gradient[r];
@@ -723,7 +730,7 @@ __device__ void newton_from_hessian(int m, S* sc, bool* steepest) {
     return;
   }
   *steepest = false;
-  double z[kMaxPenalties];
+  double z[S::kLd];
   for (int r = 0; r < m; ++r) {
     double s = -sc->gradient[r];
     for (int k = 0; k < r; ++k) s -= Lm[r + S::kLd * k] * z[k];
@@ -748,7 +755,7 @@ __device__ void newton_from_hessian(int m, S* sc, bool* steepest) {
 // 1 when the step was applied, 2 when it was applied and was negligible.
 template <class S>
 __device__ int polish_step(int m, S* sc) {
-  int act[kMaxPenalties];
+  int act[S::kLd];
   int na = 0;
   for (int j = 0; j < m; ++j)
     if (sc->hess_c[j + S::kLd * j] > kPolishCurvature * sc->score) act[na++] = j;
@@ -768,7 +775,7 @@ __device__ int polish_step(int m, S* sc) {
       Lm[r + S::kLd * c] = s / d;
     }
   }
-  double z[kMaxPenalties];
+  double z[S::kLd];
   for (int r = 0; r < na; ++r) {
     double s = -sc->grad_c[act[r]];
     for (int k = 0; k < r; ++k) s -= Lm[r + S::kLd * k] * z[k];
@@ -786,15 +793,14 @@ __device__ int polish_step(int m, S* sc) {
   return mx <= kPolishDone ? 2 : 1;
 }
 
-// Cholesky solve of (A + mu I) z = -g (one thread, m <= kMaxPenalties, A
-// column-major with leading dimension kMaxPenalties) on the coordinates
-// whose bit in ``fixed`` is clear; fixed coordinates get z = 0.  False when
-// the factor does not exist.
-__device__ bool chol_solve_neg(int m, int ld, const double* A, double mu, const double* g, unsigned fixed,
-                               double* Lm, double* z) {
+// Cholesky solve of (A + mu I) z = -g (one thread, m <= 62, A column-major
+// with leading dimension ld) on the coordinates whose bit in ``fixed`` is
+// clear; fixed coordinates get z = 0.  False when the factor does not exist.
+__device__ bool chol_solve_neg(int m, int ld, const double* A, double mu, const double* g,
+                               unsigned long long fixed, double* Lm, double* z) {
   for (int c = 0; c < m; ++c)
     for (int r = 0; r < m; ++r) {
-      const bool fr = (fixed >> r) & 1u, fc = (fixed >> c) & 1u;
+      const bool fr = (fixed >> r) & 1ull, fc = (fixed >> c) & 1ull;
       Lm[r + ld * c] = (fr || fc) ? (r == c ? 1.0 : 0.0) : A[r + ld * c] + (r == c ? mu : 0.0);
     }
   for (int c = 0; c < m; ++c) {
@@ -810,7 +816,7 @@ __device__ bool chol_solve_neg(int m, int ld, const double* A, double mu, const 
     }
   }
   for (int r = 0; r < m; ++r) {
-    double v = ((fixed >> r) & 1u) ? 0.0 : -g[r];
+    double v = ((fixed >> r) & 1ull) ? 0.0 : -g[r];
     for (int k = 0; k < r; ++k) v -= Lm[r + ld * k] * z[k];
     z[r] = v / Lm[r + ld * r];
   }
@@ -825,7 +831,7 @@ __device__ bool chol_solve_neg(int m, int ld, const double* A, double mu, const 
 // Newton or damped Gauss-Newton solve of the adjoint-driven selection on the
 // free coordinates (see gn_step).  False when no factor exists.
 template <class S>
-__device__ bool gn_solve(int m, S* sc, unsigned fixed, double* z) {
+__device__ bool gn_solve(int m, S* sc, unsigned long long fixed, double* z) {
   if (chol_solve_neg(m, S::kLd, sc->hess_c, 0.0, sc->grad_c, fixed, sc->ja, z)) return true;
   double dmax = 0.0;
   for (int j = 0; j < m; ++j) dmax = fmax(dmax, fabs(sc->gn_c[j + S::kLd * j]));
@@ -847,12 +853,12 @@ __device__ bool gn_solve(int m, S* sc, unsigned fixed, double* z) {
 // step is capped at 5 in max norm as magic's.
 template <class S>
 __device__ void gn_step(int m, S* sc) {
-  double z[kMaxPenalties];
-  unsigned fixed = 0u;
+  double z[S::kLd];
+  unsigned long long fixed = 0ull;
   bool ok = gn_solve(m, sc, fixed, z);
   if (ok) {
     for (int r = 0; r < m; ++r)
-      if (sc->log_sp[r] >= kGnMaxLogSp && z[r] > 0.0) fixed |= 1u << r;
+      if (sc->log_sp[r] >= kGnMaxLogSp && z[r] > 0.0) fixed |= 1ull << r;
     if (fixed) ok = gn_solve(m, sc, fixed, z);
   }
   if (!ok) {
@@ -875,10 +881,11 @@ __device__ void gn_step(int m, S* sc) {
 
 // Per-fit set-up shared by the fit and adjoint kernels: fill-in bounds, block
 // maps, R staged in shared memory, y0 = Q'y and |y|^2.
-template <int QMAX, int RMAX>
+template <int QMAX, int RMAX, class S = MultiScalars>
 __device__ void multi_fit_setup(const DesignDev& des, const double* __restrict__ arena, const double* __restrict__ y,
-                                int n, double* sm, MultiScalars& sc) {
+                                int n, double* sm, S& sc) {
   using L = MultiLayout<QMAX, RMAX>;
+  constexpr int NT = S::kThreads;
   const int tid = threadIdx.x;
   const int q = des.q, m = des.m;
   const double* Q = arena + des.basis;
@@ -905,13 +912,13 @@ __device__ void multi_fit_setup(const DesignDev& des, const double* __restrict__
     const double* R = arena + des.rmat;
     double* Rs = sm + L::RS;
     for (int c = 0; c < q; ++c)
-      for (int i = tid; i <= c; i += kMultiThreads) Rs[tri(i, c)] = R[i + static_cast<int64_t>(q) * c];
+      for (int i = tid; i <= c; i += NT) Rs[tri(i, c)] = R[i + static_cast<int64_t>(q) * c];
   }
   // y0 = Q'y and rss0 = |y - Q y0|^2
   double* y0 = sm + L::Y0;
   {
     const int warp = tid >> 5, lane = tid & 31;
-    for (int c = warp; c < q; c += kMultiThreads / 32) {
+    for (int c = warp; c < q; c += NT / 32) {
       double s = 0.0;
       for (int i = lane; i < n; i += 32) s += Q[i + static_cast<int64_t>(n) * c] * y[i];
       s = warp_sum(s);
@@ -919,7 +926,7 @@ __device__ void multi_fit_setup(const DesignDev& des, const double* __restrict__
     }
     __syncthreads();
     double ee = 0.0;
-    for (int i = tid; i < n; i += kMultiThreads) {
+    for (int i = tid; i < n; i += NT) {
       double f = 0.0;
       for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * y0[c];
       const double e = y[i] - f;
@@ -930,33 +937,27 @@ __device__ void multi_fit_setup(const DesignDev& des, const double* __restrict__
   }
 }
 
-template <int QMAX, int RMAX>
-__global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
-    const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data,
-    int n, const FitJob* __restrict__ jobs, const int* __restrict__ job_index, int job_count,
-    double* __restrict__ residuals, FitResult* __restrict__ results, int selection, double* __restrict__ workspace) {
+// One fit of a CTA class: magic's search (or the Gauss-Newton selection),
+// boundary probes, polish, residual and result record.  sm: the working set
+// (shared or global), sc: the scalars, ctl: 4 shared ints.
+template <int QMAX, int RMAX, class S>
+__device__ void multi_fit_job(const DesignDev& des, const FitJob& job, int t, const double* __restrict__ arena,
+                              const double* __restrict__ data, int n, double* __restrict__ residuals,
+                              FitResult* __restrict__ results, int selection, double* sm, S& sc, int* ctl) {
   using L = MultiLayout<QMAX, RMAX>;
-  extern __shared__ double smem_dyn[];
-  // the widest class keeps its (~330 KB) working set in a global workspace per CTA
-  double* sm = workspace ? workspace + static_cast<int64_t>(blockIdx.x) * L::TOTAL : smem_dyn;
-  __shared__ MultiScalars sc;
-  __shared__ int ctl[4];
-  if (blockIdx.x >= job_count) return;
-  const int t = job_index[blockIdx.x];
-  const FitJob job = jobs[t];
-  const DesignDev& des = designs[job.design];
+  constexpr int NT = S::kThreads;
   const int tid = threadIdx.x;
   const int q = des.q, m = des.m;
   const double* y = data + static_cast<int64_t>(n) * job.column;
   const double* Q = arena + des.basis;
-  multi_fit_setup<QMAX, RMAX>(des, arena, y, n, sm, sc);
+  multi_fit_setup<QMAX, RMAX, S>(des, arena, y, n, sm, sc);
   if (tid < m) {
     sc.log_sp[tid] = des.log_sp0[tid];
     sc.trial[tid] = des.log_sp0[tid];
   }
   __syncthreads();
-  multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
-  multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
+  multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
+  multi_derivatives<QMAX, RMAX, S>(des, arena, n, sm, &sc);
   double min_score = sc.score;
   double score_red = 1e10;
   bool steepest = false;
@@ -981,7 +982,7 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
       for (int tries = 1; tries <= max_half; ++tries) {
         if (tid < m) sc.trial[tid] = sc.log_sp[tid] + sc.step[tid];
         __syncthreads();
-        multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+        multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
         ++calls;
         if (sc.status != kStatusOk) break;
         if (sc.score < min_score) {
@@ -1000,7 +1001,7 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
       min_score = sc.score;
       if (tid < m) sc.log_sp[tid] = sc.trial[tid];
       __syncthreads();
-      multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
+      multi_derivatives<QMAX, RMAX, S>(des, arena, n, sm, &sc);
       if (tid < m) sc.gradient[tid] = sc.grad_c[tid];
       __syncthreads();
       double g2 = 0.0;  // projected gradient: a coordinate on the upper bound that V pushes outwards counts 0
@@ -1030,7 +1031,7 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
           __syncthreads();
           if (tid < m) sc.trial[tid] = sc.log_sp[tid] + sc.step[tid];
           __syncthreads();
-          multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+          multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
           ++calls;
           if (sc.status != kStatusOk) break;
           const double tscore = sc.score;
@@ -1040,7 +1041,7 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
             min_score = tscore;
             if (tid < m) sc.log_sp[tid] = sc.trial[tid];
             __syncthreads();
-            multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
+            multi_derivatives<QMAX, RMAX, S>(des, arena, n, sm, &sc);
           } else {
             if (tid < m) sc.step[tid] *= 0.5;
           }
@@ -1081,7 +1082,7 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
       for (int probe = 0; probe < 5; ++probe) {
         if (tid < m) sc.trial[tid] = sc.log_sp[tid] + (tid == c ? direction * 2.0 : 0.0);
         __syncthreads();
-        multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+        multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
         ++calls;
         if (sc.status != kStatusOk || !(sc.score < min_score)) break;
         min_score = sc.score;
@@ -1096,16 +1097,16 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
     __syncthreads();
     if (tid < m) sc.trial[tid] = sc.log_sp[tid];
     __syncthreads();
-    multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+    multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
     for (int ps = 0; ps < kPolishSteps && sc.status == kStatusOk; ++ps) {
-      multi_derivatives<QMAX, RMAX>(des, arena, n, sm, &sc);
+      multi_derivatives<QMAX, RMAX, S>(des, arena, n, sm, &sc);
       if (tid == 0) ctl[1] = polish_step(m, &sc);
       __syncthreads();
       const int act = ctl[1];
       if (act == 0) break;
       if (tid < m) sc.trial[tid] = sc.log_sp[tid];
       __syncthreads();
-      multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+      multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
       ++calls;
       if (act == 2) break;
     }
@@ -1115,28 +1116,60 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
     __syncthreads();
     if (tid < m) sc.trial[tid] = sc.log_sp[tid];
     __syncthreads();
-    multi_core<QMAX, RMAX>(des, arena, n, sm, &sc);
+    multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
   }
   const double* Wg = sm + L::WG;
   double* r = residuals + static_cast<int64_t>(n) * job.out;
   const bool ok = sc.status == kStatusOk;
-  for (int i = tid; i < n; i += kMultiThreads) {
+  for (int i = tid; i < n; i += NT) {
     double f = 0.0;
     if (ok)
       for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * Wg[c];
     r[i] = ok ? y[i] - f : NAN;
   }
-  if (tid == 0) {
-    FitResult res;
-    for (int j = 0; j < kMaxPenalties; ++j) res.log_sp[j] = j < m ? sc.log_sp[j] : NAN;
-    res.score = sc.score;
-    res.edf = sc.edf;
-    res.rss = sc.rss;
-    res.status = sc.status;
-    res.iterations = it;
-    res.evaluations = calls;
-    res.flags = 0;
-    results[t] = res;
+  if (tid == 0) store_result(results + t, sc.log_sp, m, sc.score, sc.edf, sc.rss, sc.status, it, calls);
+}
+
+template <int QMAX, int RMAX>
+__global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
+    const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data,
+    int n, const FitJob* __restrict__ jobs, const int* __restrict__ job_index, int job_count,
+    double* __restrict__ residuals, FitResult* __restrict__ results, int selection, double* __restrict__ workspace) {
+  using L = MultiLayout<QMAX, RMAX>;
+  extern __shared__ double smem_dyn[];
+  // the q <= 112 class keeps its (~330 KB) working set in a global workspace per CTA
+  double* sm = workspace ? workspace + static_cast<int64_t>(blockIdx.x) * L::TOTAL : smem_dyn;
+  __shared__ MultiScalars sc;
+  __shared__ int ctl[4];
+  if (blockIdx.x >= job_count) return;
+  const int t = job_index[blockIdx.x];
+  const FitJob job = jobs[t];
+  multi_fit_job<QMAX, RMAX, MultiScalars>(designs[job.design], job, t, arena, data, n, residuals, results, selection,
+                                         sm, sc, ctl);
+}
+
+// The wide class: |S| up to 62 (q <= kWideQ, stacked roots <= kWideR rows),
+// working set and scalars in a global workspace per CTA, one persistent CTA
+// per SM at most walking the class's jobs.
+constexpr int kWideThreads = 256;
+using WideScalars = MultiScalarsT<kMaxPenalties, kWideThreads, kWideQ, kWideR>;
+constexpr int64_t kWideScalarDoubles = static_cast<int64_t>((sizeof(WideScalars) + 15) / 16 * 2);
+constexpr int64_t kWideSlotDoubles = MultiLayout<kWideQ, kWideR>::TOTAL + kWideScalarDoubles;
+
+__global__ void __launch_bounds__(kWideThreads, 1) fit_multi_wide_kernel(
+    const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data,
+    int n, const FitJob* __restrict__ jobs, const int* __restrict__ job_index, int job_count,
+    double* __restrict__ residuals, FitResult* __restrict__ results, int selection, double* __restrict__ workspace) {
+  using L = MultiLayout<kWideQ, kWideR>;
+  __shared__ int ctl[4];
+  double* sm = workspace + static_cast<int64_t>(blockIdx.x) * kWideSlotDoubles;
+  WideScalars& sc = *reinterpret_cast<WideScalars*>(sm + L::TOTAL);
+  for (int k = blockIdx.x; k < job_count; k += gridDim.x) {
+    __syncthreads();  // the previous job's scalars are read no more
+    const int t = job_index[k];
+    const FitJob job = jobs[t];
+    multi_fit_job<kWideQ, kWideR, WideScalars>(designs[job.design], job, t, arena, data, n, residuals, results,
+                                               selection, sm, sc, ctl);
   }
 }
 
@@ -1182,7 +1215,7 @@ struct WarpLayout {
   static constexpr int TOTAL = PV + kWarpR;
 };
 static_assert(WarpLayout::XSZ >= kWarpTri && WarpLayout::XSZ >= 32 * kWarpPart, "warp layout");
-static_assert(WarpLayout::XSZ >= kWarpSums + 2 * kMaxPenalties * kMaxPenalties, "warp layout");
+static_assert(WarpLayout::XSZ >= kWarpSums + 2 * kWarpM * kWarpM, "warp layout");
 static_assert(kWarpR == 32 && kWarpQ > 32 && kWarpQ <= 64 && kWarpQ % 4 == 0, "warp class shape");
 static_assert(kWarpTri % 2 == 0 && WarpLayout::Y % 2 == 0, "16-byte copies of the packed triangle");
 
@@ -1215,7 +1248,7 @@ struct WarpScalars {
 // shared-memory addressing.
 extern __shared__ __align__(16) double s_warp_dyn[];
 constexpr int kWarpScalarDoubles = static_cast<int>((sizeof(WarpScalars) + 7) / 8);
-constexpr int kWarpDesignDoubles = static_cast<int>((sizeof(DesignDev) + 7) / 8);
+constexpr int kWarpDesignDoubles = static_cast<int>((sizeof(WarpDesign) + 7) / 8);
 constexpr int kWarpSlotDoubles = (WarpLayout::TOTAL + kWarpScalarDoubles + kWarpDesignDoubles + 1) & ~1;
 constexpr size_t kWarpSlotBytes = sizeof(double) * kWarpSlotDoubles;
 
@@ -1223,8 +1256,32 @@ __device__ __forceinline__ double* warp_slot() { return s_warp_dyn + (threadIdx.
 __device__ __forceinline__ WarpScalars& warp_scalars() {
   return *reinterpret_cast<WarpScalars*>(warp_slot() + WarpLayout::TOTAL);
 }
-__device__ __forceinline__ DesignDev& warp_design() {
-  return *reinterpret_cast<DesignDev*>(warp_slot() + WarpLayout::TOTAL + kWarpScalarDoubles);
+__device__ __forceinline__ WarpDesign& warp_design() {
+  return *reinterpret_cast<WarpDesign*>(warp_slot() + WarpLayout::TOTAL + kWarpScalarDoubles);
+}
+
+// The warp-class descriptor (m <= kWarpM) from the full one, lanes in parallel.
+__device__ __forceinline__ void copy_warp_design(const DesignDev* __restrict__ d, int lane) {
+  WarpDesign& w = warp_design();
+  if (lane == 0) {
+    w.kind = d->kind;
+    w.q = d->q;
+    w.m = d->m;
+    w.rsum = d->rsum;
+    w.basis = d->basis;
+    w.rmat = d->rmat;
+    w.spec = d->spec;
+    w.roots = d->roots;
+    w.rpack = d->rpack;
+  }
+  if (lane < kWarpM) {
+    w.off[lane] = d->off[lane];
+    w.dim[lane] = d->dim[lane];
+    w.rank[lane] = d->rank[lane];
+    w.rowoff[lane] = d->rowoff[lane];
+    w.rootoff[lane] = d->rootoff[lane];
+    w.log_sp0[lane] = d->log_sp0[lane];
+  }
 }
 
 // Asynchronous 16-byte global -> shared copies (cp.async, L1-allocating).
@@ -1237,7 +1294,7 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Column ``col`` of the stacked roots scaled by sqrt(lambda) (rows 0..kWarpR-1).
-__device__ __forceinline__ void warp_root_column(const DesignDev& des, const double* __restrict__ arena,
+__device__ __forceinline__ void warp_root_column(const WarpDesign& des, const double* __restrict__ arena,
                                                  const WarpScalars& sc, int col, int jb, double (&b)[kWarpR]) {
   int ro = 0, rk = 0, dim = 1, a = 0;
   double s = 0.0;
@@ -1399,7 +1456,7 @@ __device__ __forceinline__ double warp_column_dot(const double* __restrict__ W, 
 // columns < q), idg, g, Wg and score / rss / edf in sc.
 __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, int jb0, int jb1) {
   using L = WarpLayout;
-  const DesignDev& des = warp_design();
+  const WarpDesign& des = warp_design();
   WarpScalars& sc = warp_scalars();
   double* sm = warp_slot();
   const int lane = threadIdx.x & 31;
@@ -1533,7 +1590,7 @@ __device__ __forceinline__ void warp_block_sums(int q, const double* WT, const d
 // gradient and both Hessians.  jrow: penalty block of stacked row ``lane``.
 __device__ __forceinline__ void deriv_setup(double* sm, const double* __restrict__ arena, int jrow) {
   using L = WarpLayout;
-  const DesignDev& des = *reinterpret_cast<const DesignDev*>(sm + L::TOTAL + kWarpScalarDoubles);
+  const WarpDesign& des = *reinterpret_cast<const WarpDesign*>(sm + L::TOTAL + kWarpScalarDoubles);
   const int lane = threadIdx.x & 31;
   const int q = des.q;
   double* X = sm + L::X;
@@ -1577,7 +1634,7 @@ __device__ __forceinline__ void deriv_setup(double* sm, const double* __restrict
 
 __device__ __forceinline__ void deriv_finish(double* sm, int n, double (&p)[kWarpM][4], double dd) {
   using L = WarpLayout;
-  const DesignDev& des = *reinterpret_cast<const DesignDev*>(sm + L::TOTAL + kWarpScalarDoubles);
+  const WarpDesign& des = *reinterpret_cast<const WarpDesign*>(sm + L::TOTAL + kWarpScalarDoubles);
   WarpScalars& sc = *reinterpret_cast<WarpScalars*>(sm + L::TOTAL);
   const int lane = threadIdx.x & 31;
   const int m = des.m;
@@ -1653,7 +1710,7 @@ __device__ __forceinline__ void deriv_finish(double* sm, int n, double (&p)[kWar
 __device__ __noinline__ void warp_derivatives(const double* __restrict__ arena, int n, int jrow) {
   using L = WarpLayout;
   double* sm = warp_slot();
-  const DesignDev& des = warp_design();
+  const WarpDesign& des = warp_design();
   const WarpScalars& sc = warp_scalars();
   const int lane = threadIdx.x & 31;
   const int q = des.q;
@@ -1689,13 +1746,9 @@ __device__ __noinline__ void warp_fit_setup(const DesignDev* __restrict__ design
   using L = WarpLayout;
   double* sm = warp_slot();
   WarpScalars& sc = warp_scalars();
-  const DesignDev& des = warp_design();
+  const WarpDesign& des = warp_design();
   const int lane = threadIdx.x & 31;
-  {
-    const int* src = reinterpret_cast<const int*>(design);
-    int* dst = reinterpret_cast<int*>(&warp_design());
-    for (int i = lane; i < static_cast<int>(sizeof(DesignDev) / sizeof(int)); i += 32) dst[i] = src[i];
-  }
+  copy_warp_design(design, lane);
   if (lane == 0) {
     sc.status = kStatusOk;
     sc.ja = sm + L::Z + kWarpSums;
@@ -1762,7 +1815,7 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
   using L = WarpLayout;
   double* sm = warp_slot();
   WarpScalars& sc = warp_scalars();
-  const DesignDev& des = warp_design();
+  const WarpDesign& des = warp_design();
   if (blockIdx.x >= job_count) return;
   const int lane = threadIdx.x & 31;
   const int t = job_index[blockIdx.x];
@@ -1970,18 +2023,7 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
       for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * wg[c];
     r[i] = ok ? y[i] - f : NAN;
   }
-  if (lane == 0) {
-    FitResult res;
-    for (int j = 0; j < kMaxPenalties; ++j) res.log_sp[j] = j < m ? sc.log_sp[j] : NAN;
-    res.score = sc.score;
-    res.edf = sc.edf;
-    res.rss = sc.rss;
-    res.status = sc.status;
-    res.iterations = it;
-    res.evaluations = calls;
-    res.flags = 0;
-    results[t] = res;
-  }
+  if (lane == 0) store_result(results + t, sc.log_sp, m, sc.score, sc.edf, sc.rss, sc.status, it, calls);
 }
 
 // ------------------------------------------------------ speculative continuation
@@ -2026,7 +2068,7 @@ __device__ __noinline__ void spec_derivatives(const double* __restrict__ arena, 
   using L = WarpLayout;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* sm = s_warp_dyn + aw * kWarpSlotDoubles;
-  const DesignDev& des = *reinterpret_cast<const DesignDev*>(sm + L::TOTAL + kWarpScalarDoubles);
+  const WarpDesign& des = *reinterpret_cast<const WarpDesign*>(sm + L::TOTAL + kWarpScalarDoubles);
   const WarpScalars& sc = *reinterpret_cast<const WarpScalars*>(sm + L::TOTAL);
   const int q = des.q;
   double* X = sm + L::X;
@@ -2079,7 +2121,7 @@ __global__ void __launch_bounds__(32 * kSpecWarps) fit_multi_spec_kernel(
     int jb0 = -1, jb1 = -1, jrow = -1;
     warp_fit_setup(designs + job.design, arena, y, n, &jb0, &jb1, &jrow);
     WarpScalars& sc = warp_scalars();
-    const DesignDev& des = warp_design();
+    const WarpDesign& des = warp_design();
     const int m = des.m, q = des.q;
     const FitState& st = states[t];
     if (lane < m) {
@@ -2278,18 +2320,7 @@ __global__ void __launch_bounds__(32 * kSpecWarps) fit_multi_spec_kernel(
           for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * wg[c];
         r[i] = ok ? y[i] - f : NAN;
       }
-      if (lane == 0) {
-        FitResult res;
-        for (int j = 0; j < kMaxPenalties; ++j) res.log_sp[j] = j < m ? sc.log_sp[j] : NAN;
-        res.score = sc.score;
-        res.edf = sc.edf;
-        res.rss = sc.rss;
-        res.status = status;
-        res.iterations = it;
-        res.evaluations = calls;
-        res.flags = 0;
-        results[t] = res;
-      }
+      if (lane == 0) store_result(results + t, sc.log_sp, m, sc.score, sc.edf, sc.rss, status, it, calls);
     }
     __syncthreads();
   }
@@ -2311,7 +2342,7 @@ __global__ void __launch_bounds__(32) gcv_adjoint_warp_kernel(const DesignDev* _
                                                               double* __restrict__ gn, double* __restrict__ hess,
                                                               int* __restrict__ status) {
   WarpScalars& sc = warp_scalars();
-  const DesignDev& des = warp_design();
+  const WarpDesign& des = warp_design();
   const int pt = blockIdx.x;
   if (pt >= count) return;
   const int lane = threadIdx.x & 31;
@@ -2352,7 +2383,7 @@ __global__ void __launch_bounds__(kMultiThreads, 1) gcv_adjoint_kernel(
   const DesignDev& des = designs[design];
   const int tid = threadIdx.x;
   const int m = des.m;
-  multi_fit_setup<QMAX, RMAX>(des, arena, y, n, sm, sc);
+  multi_fit_setup<QMAX, RMAX, MultiScalars>(des, arena, y, n, sm, sc);
   if (tid < m) {
     sc.trial[tid] = rho[static_cast<int64_t>(pt) * m + tid];
     sc.log_sp[tid] = sc.trial[tid];
@@ -2366,8 +2397,8 @@ __global__ void __launch_bounds__(kMultiThreads, 1) gcv_adjoint_kernel(
     for (int i = 0; i < m; ++i) {
       grad[static_cast<int64_t>(pt) * m + i] = sc.grad_c[i];
       for (int j = 0; j < m; ++j) {
-        gn[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.gn_c[i + kMaxPenalties * j];
-        hess[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.hess_c[i + kMaxPenalties * j];
+        gn[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.gn_c[i + MultiScalars::kLd * j];
+        hess[(static_cast<int64_t>(pt) * m + i) * m + j] = sc.hess_c[i + MultiScalars::kLd * j];
       }
     }
   }
@@ -2379,8 +2410,13 @@ size_t multi_smem_bytes(int qmax_class) {
   return 0;  // class 2 works in global memory
 }
 
+// CTAs of the wide class's persistent launch (one per SM at most).
+int wide_ctas(int count) { return count < 148 ? count : 148; }
+
 size_t multi_workspace_doubles(int qmax_class, int count) {
-  return qmax_class == 2 ? static_cast<size_t>(MultiLayout<112, 96>::TOTAL) * static_cast<size_t>(count) : 0;
+  if (qmax_class == 2) return static_cast<size_t>(MultiLayout<112, 96>::TOTAL) * static_cast<size_t>(count);
+  if (qmax_class == 3) return static_cast<size_t>(kWideSlotDoubles) * static_cast<size_t>(wide_ctas(count));
+  return 0;
 }
 
 cudaError_t configure_fit_kernels() {
@@ -2458,10 +2494,15 @@ cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const dou
   } else if (qmax_class == 1) {
     fit_multi_kernel<76, 64><<<count, kMultiThreads, multi_smem_bytes(1), stream>>>(
         designs, arena, data, n, jobs, job_index, count, residuals, results, selection, nullptr);
-  } else {
+  } else if (qmax_class == 2) {
     if (!workspace) return cudaErrorInvalidValue;
     fit_multi_kernel<112, 96><<<count, kMultiThreads, 0, stream>>>(designs, arena, data, n, jobs, job_index, count,
                                                                     residuals, results, selection, workspace);
+  } else {
+    if (!workspace) return cudaErrorInvalidValue;
+    fit_multi_wide_kernel<<<wide_ctas(count), kWideThreads, 0, stream>>>(designs, arena, data, n, jobs, job_index,
+                                                                        count, residuals, results, selection,
+                                                                        workspace);
   }
   return cudaGetLastError();
 }

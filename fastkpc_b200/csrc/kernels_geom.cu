@@ -31,9 +31,9 @@ namespace {
 
 constexpr int kGeomThreads = 256;
 constexpr int kGeomWarps = kGeomThreads / 32;
-constexpr int kGeomMaxQ = 112;
+constexpr int kGeomMaxQ = 560;  // additive designs up to |S| = 62
 constexpr size_t kGeomSmemLimit = 220 * 1024;    // dynamic + static shared memory of one CTA
-constexpr size_t kAdditiveStaticSmem = 4 * 1024;  // colsrc, vks, betas, red (2.7 KB) rounded up
+constexpr size_t kAdditiveStaticSmem = 14 * 1024;  // colsrc, vks, betas, red (13.2 KB) rounded up
 constexpr size_t kSingleStaticSmem = 44 * 1024;   // R, Ri, T, A, V, ... (41.2 KB) rounded up
 
 __device__ __forceinline__ double warp_sum_g(double v) {
@@ -148,12 +148,11 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(int n, 
     double* Q = arena + job.basis;
     double* W = in_smem ? wsm : Q;
     double* R = arena + job.rmat;
-    if (tid < q) {
+    for (int c = tid; c < q; c += blockDim.x) {
       const double* src = nullptr;  // the intercept column
       for (int j = 0; j < job.m; ++j)
-        if (tid >= job.off[j] && tid < job.off[j] + job.dim[j])
-          src = job.src[j] + static_cast<int64_t>(n) * (tid - job.off[j]);
-      colsrc[tid] = src;
+        if (c >= job.off[j] && c < job.off[j] + job.dim[j]) src = job.src[j] + static_cast<int64_t>(n) * (c - job.off[j]);
+      colsrc[c] = src;
     }
     __syncthreads();
     const int64_t nq = static_cast<int64_t>(n) * q;

@@ -215,7 +215,7 @@ void Engine::plan_components(const std::vector<Test>& tests) {
         throw Error(FKPC_STATUS_INVALID_ARGUMENT, "conditioning set must hold distinct variables other than x and y");
     }
     if (static_cast<int>(ts.S.size()) > kMaxPenalties)
-      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "conditioning sets larger than 12 are not supported by this build");
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "conditioning sets larger than 62 are not supported");
     int set = -1;
     if (!ts.S.empty()) {
       auto it = set_index.find(ts.S);
@@ -605,8 +605,11 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
       }
       total += static_cast<size_t>(rootoff);
       dd.rsum = rows;
-      if (des.q > 112 || rows > 96 || des.m > kMaxPenalties)
-        throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity (q <= 112, |S| <= 12)");
+      if (des.q > kWideQ || rows > kWideR || des.m > kMaxPenalties)
+        throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity (q <= 560, |S| <= 62)");
+      if (des.q >= n_)
+        throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design has at least as many coefficients as observations (q = " +
+                                                      std::to_string(des.q) + ", n = " + std::to_string(n_) + ")");
       dd.rpack = -1;
       if (des.q <= kWarpQ) {
         size_t& pat = dev ? dev_total : total;
@@ -731,12 +734,14 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
   multi_small_.clear();
   multi_large_.clear();
   multi_huge_.clear();
+  multi_wide_.clear();
   direct_cols_.clear();
   direct_slots_.clear();
   plain_single_off_.clear();
   plain_small_off_.clear();
   plain_large_off_.clear();
   plain_huge_off_.clear();
+  plain_wide_off_.clear();
   plain_direct_off_.clear();
   for (size_t c = 0; c < comps_.size(); ++c) {
     if (opt.mode == FKPC_MODE_PLAIN && c % 2 == 0) {
@@ -744,6 +749,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
       plain_small_off_.push_back(static_cast<int>(multi_small_.size()));
       plain_large_off_.push_back(static_cast<int>(multi_large_.size()));
       plain_huge_off_.push_back(static_cast<int>(multi_huge_.size()));
+      plain_wide_off_.push_back(static_cast<int>(multi_wide_.size()));
       plain_direct_off_.push_back(static_cast<int>(direct_cols_.size()));
     }
     const Component& cp = comps_[c];
@@ -760,8 +766,9 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
       const int idx = static_cast<int>(multi_jobs_.size());
       multi_jobs_.push_back(job);
       if (dd.q <= kWarpQ && dd.rsum <= kWarpR && dd.m <= kWarpM) multi_small_.push_back(idx);
-      else if (dd.q <= 76 && dd.rsum <= 64) multi_large_.push_back(idx);
-      else multi_huge_.push_back(idx);
+      else if (dd.q <= 76 && dd.rsum <= 64 && dd.m <= kCtaPenalties) multi_large_.push_back(idx);
+      else if (dd.q <= 112 && dd.rsum <= 96 && dd.m <= kCtaPenalties) multi_huge_.push_back(idx);
+      else multi_wide_.push_back(idx);
     }
   }
   if (opt.mode != FKPC_MODE_PLAIN) {
@@ -777,6 +784,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
     plain_small_off_.push_back(static_cast<int>(multi_small_.size()));
     plain_large_off_.push_back(static_cast<int>(multi_large_.size()));
     plain_huge_off_.push_back(static_cast<int>(multi_huge_.size()));
+    plain_wide_off_.push_back(static_cast<int>(multi_wide_.size()));
     plain_direct_off_.push_back(static_cast<int>(direct_cols_.size()));
   }
   const size_t ncomp = comps_.size();
@@ -807,12 +815,15 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
   h2d_bytes_ += stage_upload(d_multi_small_, multi_small_);
   h2d_bytes_ += stage_upload(d_multi_large_, multi_large_);
   h2d_bytes_ += stage_upload(d_multi_huge_, multi_huge_);
+  h2d_bytes_ += stage_upload(d_multi_wide_, multi_wide_);
   if (!multi_small_.empty()) {
     d_fit_states_.ensure(multi_jobs_.size());
     d_defer_list_.ensure(multi_small_.size());
     d_defer_count_.ensure(1);
   }
-  if (!multi_huge_.empty()) d_fit_ws_.ensure(multi_workspace_doubles(2, static_cast<int>(multi_huge_.size())));
+  if (!multi_huge_.empty() || !multi_wide_.empty())
+    d_fit_ws_.ensure(std::max(multi_workspace_doubles(2, static_cast<int>(multi_huge_.size())),
+                              multi_workspace_doubles(3, static_cast<int>(multi_wide_.size()))));
   h2d_bytes_ += stage_upload(d_direct_cols_, direct_cols_);
   h2d_bytes_ += stage_upload(d_direct_slots_, direct_slots_);
   h2d_bytes_ += stage_upload(d_pairs_, pairs_);
@@ -1037,6 +1048,13 @@ void Engine::enqueue_multi() {
   if (!multi_huge_.empty()) {
     cuda_check(launch_fit_multi(2, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                 d_multi_huge_.get(), static_cast<int>(multi_huge_.size()), d_resid_.get(),
+                                d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get()),
+               "fit multi");
+    ++launches_;
+  }
+  if (!multi_wide_.empty()) {  // after the q <= 112 class: the two share the workspace
+    cuda_check(launch_fit_multi(3, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                d_multi_wide_.get(), static_cast<int>(multi_wide_.size()), d_resid_.get(),
                                 d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get()),
                "fit multi");
     ++launches_;
@@ -1384,7 +1402,7 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
     for (const auto& r : sres) evals += r.evaluations;
     for (const auto& r : mres) evals += r.evaluations;
     stats->fit_evaluations = evals;
-    stats->fit_flops = stage_flops_[0] + stage_flops_[1] + stage_flops_[2];
+    stats->fit_flops = stage_flops_[0] + stage_flops_[1] + stage_flops_[2] + stage_flops_[9] + stage_flops_[10];
     double its = 0.0;
     for (const auto& r : sres) its += r.iterations;
     for (const auto& r : mres) its += r.iterations;
@@ -1424,8 +1442,9 @@ void Engine::account_flops(const std::vector<FitResult>& sres, const std::vector
     for (int r : des.ranks) rs += r;
     const double f = 6.0 * n * q + (16.0 + 2.0 * des.m) * q * q * q * mres[i].evaluations;
     const bool small = des.q <= kWarpQ && rs <= kWarpR && des.m <= kWarpM;
-    const bool large = !small && des.q <= 76 && rs <= 64;
-    stage_flops_[small ? 1 : (large ? 2 : 9)] += f;
+    const bool large = !small && des.q <= 76 && rs <= 64 && des.m <= kCtaPenalties;
+    const bool huge = !small && !large && des.q <= 112 && rs <= 96 && des.m <= kCtaPenalties;
+    stage_flops_[small ? 1 : (large ? 2 : (huge ? 9 : 10))] += f;
   }
   if (stats_enabled_) {
     const double nc = static_cast<double>(comps_.size()), np = static_cast<double>(pairs_.size());
@@ -1480,6 +1499,14 @@ void Engine::enqueue_plain_test(int t) {
   if (h1 > h0) {
     cuda_check(launch_fit_multi(2, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                 d_multi_huge_.get() + h0, h1 - h0, d_resid_.get(), d_multi_res_.get(), stream_,
+                                opt_.selection, d_fit_ws_.get()),
+               "fit multi");
+    ++launches_;
+  }
+  const int w0 = plain_wide_off_[t], w1 = plain_wide_off_[t + 1];
+  if (w1 > w0) {
+    cuda_check(launch_fit_multi(3, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                d_multi_wide_.get() + w0, w1 - w0, d_resid_.get(), d_multi_res_.get(), stream_,
                                 opt_.selection, d_fit_ws_.get()),
                "fit multi");
     ++launches_;
@@ -1550,7 +1577,7 @@ double Engine::execute_timed(int repeats) {
 
 double Engine::time_stage(int stage, int repeats, double* flops_per_launch) {
   if (!collected_) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "collect the prepared batch before timing a stage");
-  if (stage < 0 || stage > 9) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "unknown stage");
+  if (stage < 0 || stage > 10) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "unknown stage");
   cuda_check(configure_fit_kernels(), "kernel attributes");
   cuda_check(configure_stat_kernels(n_), "kernel attributes");
   const int n = n_;
@@ -1572,6 +1599,9 @@ double Engine::time_stage(int stage, int repeats, double* flops_per_launch) {
       case 9: return launch_fit_multi(2, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                       d_multi_huge_.get(), static_cast<int>(multi_huge_.size()), d_resid_.get(),
                                       d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get());
+      case 10: return launch_fit_multi(3, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
+                                       d_multi_wide_.get(), static_cast<int>(multi_wide_.size()), d_resid_.get(),
+                                       d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get());
       case 3: return launch_dcov_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, d_centre_.get(),
                                             d_dcov_.get(), stream_);
       case 4: return launch_dcov_pairs(d_resid_.get(), n, d_comp_cols_.get(), d_centre_.get(), d_dcov_.get(),
@@ -1744,6 +1774,8 @@ void Engine::adjoint(int target, const std::vector<int>& S, int count, const dou
   const int m = des.m;
   int rsum = 0;
   for (int r : des.ranks) rsum += r;
+  if (des.q > 112 || rsum > 96 || m > kCtaPenalties)
+    throw Error(FKPC_STATUS_INVALID_ARGUMENT, "the GCV adjoint covers designs with |S| <= 12 (q <= 112)");
   const int qclass = (des.q <= kWarpQ && rsum <= kWarpR && m <= kWarpM) ? 0 : (des.q <= 76 && rsum <= 64 ? 1 : 2);
   if (count == 0) return;
   DevBuf<double> d_rho, d_score, d_grad, d_gn, d_hess;
@@ -1796,6 +1828,7 @@ void Engine::statistics(const double* residuals, int m, const std::vector<int>& 
   multi_small_.clear();
   multi_large_.clear();
   multi_huge_.clear();
+  multi_wide_.clear();
   direct_cols_.clear();
   direct_slots_.clear();
   stats_enabled_ = true;

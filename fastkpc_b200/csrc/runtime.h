@@ -199,10 +199,11 @@ class Engine {
   std::vector<Component> comps_;
   std::vector<PairJob> pairs_;
   std::vector<FitJob> single_jobs_, multi_jobs_;
-  std::vector<int> multi_small_, multi_large_, multi_huge_;
+  std::vector<int> multi_small_, multi_large_, multi_huge_, multi_wide_;
   std::vector<int> direct_cols_, direct_slots_;
   // plain form: per test, offsets of its jobs in the job lists
-  std::vector<int> plain_single_off_, plain_small_off_, plain_large_off_, plain_huge_off_, plain_direct_off_;
+  std::vector<int> plain_single_off_, plain_small_off_, plain_large_off_, plain_huge_off_, plain_wide_off_,
+      plain_direct_off_;
   int guard_cap_ = 0;
   bool stats_enabled_ = true;
 
@@ -210,7 +211,8 @@ class Engine {
   DevBuf<double> d_arena_, d_resid_, d_centre_, d_factors_, d_lr_vals_, d_lr_vecs_, d_legacy_ws_;
   DevBuf<DesignDev> d_designs_;
   DevBuf<FitJob> d_single_jobs_, d_multi_jobs_;
-  DevBuf<int> d_multi_small_, d_multi_large_, d_multi_huge_, d_direct_cols_, d_direct_slots_, d_comp_cols_;
+  DevBuf<int> d_multi_small_, d_multi_large_, d_multi_huge_, d_multi_wide_, d_direct_cols_, d_direct_slots_,
+      d_comp_cols_;
   DevBuf<double> d_fit_ws_;  // global working sets of the widest fit class
   DevBuf<FitState> d_fit_states_;  // optimiser states handed to the speculative continuation
   DevBuf<int> d_defer_list_, d_defer_count_;
@@ -263,7 +265,7 @@ class Engine {
   double setup_ms_ = 0.0, upload_ms_ = 0.0;
   int guard_count_host_ = 0;
   double h2d_bytes_ = 0.0, d2h_bytes_ = 0.0;
-  double stage_flops_[10] = {};
+  double stage_flops_[11] = {};
   bool collected_ = false;
   bool graph_timed_ = false;
   double lowrank_steps_mean_ = 0.0;

@@ -363,7 +363,8 @@ FKPC_API int fkpc_batch_collect(int device, fkpc_ci_record* out,
  * its mean CUDA-event duration (ms) and its algorithmic FP64 flops per launch.
  * Stages: 0 fit single, 1 fit multi (q <= 40), 2 fit multi (q <= 76),
  * 3 dCov components, 4 dCov pairs, 5 HSIC components, 6 HSIC pairs,
- * 7 low-rank eigen, 8 low-rank pairs, 9 fit multi (q <= 112).  Run
+ * 7 low-rank eigen, 8 low-rank pairs, 9 fit multi (q <= 112), 10 fit
+ * multi (q <= 560, |S| <= 62).  Run
  * fkpc_batch_execute first.
  * No reference counterpart (measurement utility).
  */

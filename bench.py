@@ -20,6 +20,12 @@ set and a synchronisation per test) on a sample of the same batch.
 ``parity``: per-stage error of this run's records (dcc.gamma, hsic.gamma)
 and residuals against the oracle's records for the whole batch, read from
 the committed fixture ``tests/golden/level500x50_oracle.npz``.
+``skeleton_351x48``: full default-Inf skeletons of the n=351, p=48 SEM.
+``uneven_perm_500x64``: the uneven-width permutation batch (n=500, p=64,
+|S| ~ geometric(0.35) <= 12, hsic.perm and dcc.perm with 1000 seeded
+permutations), ``--perm-count`` of its 16384 triples through the public call.
+``adjoint_1000``: magic's search and the Gauss-Newton selection over 2048
+additive fits at n=1000, and the GCV adjoint against central differences.
 ``--impl reference`` times the reference algorithm's CPU restatement (the
 oracle) on the host cores: every step is the same stratified sample of the
 batch (every 16th triple) that ``cpu_baseline`` times.
@@ -66,6 +72,9 @@ def parse():
     ap.add_argument("--profile-once", action="store_true")
     ap.add_argument("--method", default="dcc.gamma", choices=["dcc.gamma", "hsic.gamma"])
     ap.add_argument("--no-skeleton", action="store_true")
+    ap.add_argument("--perm-count", type=int, default=1024,
+                    help="triples of the 16384-triple uneven permutation batch to time (0: skip)")
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -248,6 +257,103 @@ def skeleton_rows(device, cores, pool):
     return rows
 
 
+def uneven_perm_row(device, count, replicates=1000, seed=12, parity_tests=2):
+    """The uneven-width permutation batch: n=500, p=64 SEM, triples with |S|
+    ~ geometric(0.35) truncated at 12 (workloads.uneven_batch_500x64), the
+    first ``count`` of its 16384, hsic.perm then dcc.perm with ``replicates``
+    seeded permutations each, through the public call.  The permutation
+    tables come from the R-compatible stream on the host, test after test in
+    batch order (the reference's contract), so the host stream is inside the
+    timed call; ``device_ms`` is the device part.  Parity: the first
+    ``parity_tests`` p-values against the oracle on the same stream."""
+    import fastkpc_b200 as fk
+    from fastkpc_b200 import workloads
+    from oracle import rng, skeleton
+    X, triples = workloads.uneven_batch_500x64()
+    sample = triples[:count]
+    out = {"count": len(sample), "of": len(triples), "replicates": replicates, "seed": seed,
+           "sizes": {str(k): int(sum(len(t[2]) == k for t in sample)) for k in range(13)},
+           "data": "synthetic SEM n=500 p=64 edge prob 0.08, |S| ~ geometric(0.35) <= 12 (seed 4)"}
+    cache = skeleton.ResidualCache(X)
+    for method in ("hsic.perm", "dcc.perm"):
+        fk.ci_level_batch(X, sample[:32], ci_method=method, seed=seed, replicates=replicates, device=device)
+        t0 = time.perf_counter()
+        rec, st = fk.ci_level_batch(X, sample, ci_method=method, seed=seed, replicates=replicates, device=device)
+        wall = time.perf_counter() - t0
+        if not np.all(rec["status"] == 0):
+            raise RuntimeError(f"{method}: failing records in the uneven permutation batch")
+        stream = rng.RStream(seed)
+        gen = rng.dcc_permutations if method == "dcc.perm" else rng.hsic_permutations
+        exact = 0
+        for k in range(parity_tests):
+            x, y, S = sample[k]
+            perms = gen(stream, X.shape[0], replicates)
+            exact += int(rec["p_value"][k] == skeleton.ci_pvalue(cache, method, x, y, S, perms=perms))
+        out[method.replace(".", "_")] = {
+            "value": len(sample) / wall, "unit": UNIT, "wall_s": wall, "device_ms": st["device_ms"],
+            "device_tests_per_s": len(sample) / (st["device_ms"] / 1e3) if st["device_ms"] > 0 else None,
+            "setup_ms": st["setup_ms"], "upload_ms": st["upload_ms"],
+            "parity": f"{exact} of the first {parity_tests} p-values equal to the oracle's on the same stream"}
+    return out
+
+
+def adjoint_row(device, fd_fits=48, h=1e-5):
+    """The GCV adjoint / Newton-selection workload: n=1000, 2048 (target, S)
+    fits with |S| uniform on 3..8 (workloads.adjoint_targets_1000).  Times
+    magic's search (the plain search) and the Gauss-Newton selection over all
+    2048 fits; compares their residuals; checks the adjoint's gradient and
+    exact Hessian against central differences (h = 1e-5 in log lambda) of its
+    own score and gradient at magic's selected points of ``fd_fits`` fits."""
+    import fastkpc_b200 as fk
+    from fastkpc_b200 import workloads
+    X, fits = workloads.adjoint_targets_1000()
+    fk.regress_batch(X, fits[:16], device=device)
+    t0 = time.perf_counter()
+    r_m, l_m, s_m = fk.regress_batch(X, fits, device=device)
+    t_m = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    r_g, l_g, s_g = fk.regress_batch(X, fits, device=device, selection="gn_newton")
+    t_g = time.perf_counter() - t0
+    ok = (s_m == 0) & (s_g == 0)
+    rel = np.array([np.max(np.abs(r_m[:, k] - r_g[:, k])) / max(np.max(np.abs(r_m[:, k])), 1e-300)
+                    for k in range(len(fits))])[ok]
+    grad_err, hess_err, v_gn_le_magic = [], [], 0
+    points = 0
+    t_adj = 0.0
+    for k in np.linspace(0, len(fits) - 1, fd_fits).astype(int):
+        t, S = fits[k]
+        m = len(S)
+        rho = l_m[k, :m]
+        pts = [rho]
+        for j in range(m):
+            e = np.zeros(m)
+            e[j] = h
+            pts += [rho + e, rho - e]
+        t0 = time.perf_counter()
+        a = fk.gcv_adjoint(X, t, S, np.array(pts), device=device)
+        t_adj += time.perf_counter() - t0
+        points += len(pts)
+        fd_g = np.array([(a["score"][1 + 2 * j] - a["score"][2 + 2 * j]) / (2 * h) for j in range(m)])
+        fd_h = np.array([(a["grad"][1 + 2 * j] - a["grad"][2 + 2 * j]) / (2 * h) for j in range(m)])
+        g, H = a["grad"][0], a["hessian"][0]
+        # at a selected point the gradient is near zero: scale by |grad| + 1e-6 V
+        grad_err.append(np.max(np.abs(fd_g - g)) / (np.max(np.abs(g)) + 1e-6 * abs(a["score"][0])))
+        hess_err.append(np.max(np.abs(fd_h - H)) / max(np.max(np.abs(H)), 1e-300))
+        v_gn = fk.gcv_adjoint(X, t, S, l_g[k, :m][None, :], device=device)["score"][0]
+        v_gn_le_magic += int(v_gn <= a["score"][0] * (1 + 1e-12))
+    return {"fits": len(fits), "sizes": {str(k): int(sum(len(f[1]) == k for f in fits)) for k in range(3, 9)},
+            "magic": {"fits_per_s": len(fits) / t_m, "wall_s": t_m, "failed": int(np.sum(s_m != 0))},
+            "gn_newton": {"fits_per_s": len(fits) / t_g, "wall_s": t_g, "failed": int(np.sum(s_g != 0))},
+            "residual_rel_diff_gn_vs_magic": {"median": float(np.median(rel)), "max": float(np.max(rel)),
+                                              "within_1e-6": float(np.mean(rel <= 1e-6))},
+            "gn_score_at_most_magic": f"{v_gn_le_magic} of {fd_fits}",
+            "adjoint_vs_central_differences": {"fits": fd_fits, "points": points, "h": h,
+                                               "gradient_rel_err_max": float(np.max(grad_err)),
+                                               "hessian_rel_err_max": float(np.max(hess_err))},
+            "adjoint_points_per_s_incl_setup": points / t_adj,
+            "data": "synthetic SEM n=1000 p=50 edge prob 0.08, |S| uniform on 3..8 (seed 5)"}
+
+
 def host_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -404,6 +510,8 @@ def run_ours(args, world, rank, local, pg):
             pool.map(_oracle_chunk, [(X, csample[i:i + 1], "dcc.gamma") for i in range(cores)])  # start-up
             cpu_dt = cpu_oracle_time(pool, X, csample, cores)
             skel = [] if args.no_skeleton else skeleton_rows(local, cores, pool)
+        uneven = uneven_perm_row(local, args.perm_count) if args.perm_count > 0 else None
+        adjoint = None if args.no_adjoint else adjoint_row(local)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -439,6 +547,8 @@ def run_ours(args, world, rank, local, pg):
                     "device_ms": e2e_stats["device_ms"], "download_ms": e2e_stats["download_ms"],
                     "call_ms": e2e_stats["total_ms"], "wall_s": statistics.median(e2e_t)},
             "skeleton_351x48": skel,
+            "uneven_perm_500x64": uneven,
+            "adjoint_1000": adjoint,
             "gpu_launches": int(st["kernel_launches"] + hst["kernel_launches"]) * args.steps,
             "clocks": clocks_s,
         }

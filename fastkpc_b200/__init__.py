@@ -80,7 +80,10 @@ class StageStats(ctypes.Structure):
                 ("statistic_flops", ctypes.c_double), ("fit_iterations", ctypes.c_double),
                 ("lowrank_components", ctypes.c_int), ("lowrank_steps_max", ctypes.c_int),
                 ("lowrank_steps_mean", ctypes.c_double), ("device_ms", ctypes.c_double),
-                ("designs_built", ctypes.c_int), ("smooths_built", ctypes.c_int)]
+                ("designs_built", ctypes.c_int), ("smooths_built", ctypes.c_int), ("plan_ms", ctypes.c_double),
+                ("tprs_host_ms", ctypes.c_double), ("design_host_ms", ctypes.c_double),
+                ("smooth_wait_ms", ctypes.c_double), ("late_wait_ms", ctypes.c_double),
+                ("prefit_device_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

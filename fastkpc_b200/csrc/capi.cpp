@@ -203,6 +203,12 @@ void add_stats(fkpc_stage_stats* acc, const fkpc_stage_stats& s) {
   acc->device_ms += s.device_ms;
   acc->designs_built += s.designs_built;
   acc->smooths_built += s.smooths_built;
+  acc->plan_ms += s.plan_ms;
+  acc->tprs_host_ms += s.tprs_host_ms;
+  acc->design_host_ms += s.design_host_ms;
+  acc->smooth_wait_ms += s.smooth_wait_ms;
+  acc->late_wait_ms += s.late_wait_ms;
+  acc->prefit_device_ms += s.prefit_device_ms;
 }
 
 // Evaluate ``tests`` on the engine in chunks; records in test order.

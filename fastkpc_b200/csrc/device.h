@@ -46,6 +46,7 @@ struct DesignT {
   int64_t spec;    // kind 1: hat eigenvalues e (q)
   int64_t roots;   // kind 2: penalty roots, block j dim_j x rank_j column-major, consecutive
   int64_t rpack;   // kind 2 with q <= kWarpQ: R row-packed (kWarpTri doubles, zero beyond q), else -1
+  int64_t ext;     // m > kCtaPenalties: arena offset of the design's WideDesign (all m blocks), else -1
   int off[MP];
   int dim[MP];
   int rank[MP];
@@ -53,23 +54,31 @@ struct DesignT {
   int rootoff[MP];   // offset of block j's root inside ``roots``
   double log_sp0[MP];
 };
-using DesignDev = DesignT<kMaxPenalties>;
+// The descriptor array every kernel indexes: the blocks of designs with
+// m <= kCtaPenalties; a wider design keeps its header here and its full
+// descriptor (a WideDesign) in the arena at ``ext``.
+using DesignDev = DesignT<kCtaPenalties>;
+using WideDesign = DesignT<kMaxPenalties>;
 // The warp fit class's copy in shared memory (m <= kWarpM).
 using WarpDesign = DesignT<kWarpM>;
+static_assert(sizeof(WideDesign) % sizeof(double) == 0, "wide descriptors are copied into the arena as doubles");
 
 // One additive design whose geometry the device builds: X = [1 | B_1 | ...]
 // gathered from the univariate smooth bases, X = Q R by Householder, Q and R
 // (and row-packed R) written to the arena.
-struct GeomJob {
+template <int MP>
+struct GeomJobT {
   int64_t basis;                 // arena offset of Q (n x q)
   int64_t rmat;                  // arena offset of R (q x q)
   int64_t rpack;                 // arena offset of row-packed R, or -1
-  const double* src[kMaxPenalties];  // smooth j's basis (n x dim_j, leading dimension n), device memory
-  int off[kMaxPenalties];
-  int dim[kMaxPenalties];
+  const double* src[MP];         // smooth j's basis (n x dim_j, leading dimension n), device memory
+  int off[MP];
+  int dim[MP];
   int q;
   int m;
 };
+using GeomJob = GeomJobT<kCtaPenalties>;
+using WideGeomJob = GeomJobT<kMaxPenalties>;
 
 // One single-penalty design whose geometry the device builds: X = [1 | B],
 // B the smooth's basis, S its penalty; QW and the spectrum to the arena.
@@ -91,7 +100,7 @@ struct FitJob {
 };
 
 struct FitResult {
-  double log_sp[kMaxPenalties];
+  double log_sp[kCtaPenalties];  // the first kCtaPenalties (a wide fit writes all m to a buffer of its own)
   double score;
   double edf;
   double rss;

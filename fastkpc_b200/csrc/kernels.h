@@ -43,9 +43,12 @@ cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const dou
                              FitResult* results, cudaStream_t stream,
                              int selection = 0, double* workspace = nullptr, FitState* states = nullptr,
                              int* defer_list = nullptr, int* defer_count = nullptr,
-                             cudaEvent_t after_warp = nullptr, int defer_calls = 25);
+                             cudaEvent_t after_warp = nullptr, int defer_calls = 25,
+                             double* wide_log_sp = nullptr);
 // (class 0: ``after_warp`` is recorded on ``stream`` once the one-warp kernel is
-// queued, before the speculative continuation of the fits it deferred)
+// queued, before the speculative continuation of the fits it deferred; class
+// 3: ``wide_log_sp`` receives kMaxPenalties log(lambda) per job, in job-list
+// order)
 // Doubles of global workspace class ``qmax_class`` needs for ``count`` fits
 // (classes 2 and 3; 0 otherwise).
 size_t multi_workspace_doubles(int qmax_class, int count);
@@ -168,5 +171,7 @@ cudaError_t launch_single_geometry(int n, const SingleGeomJob* jobs, int count, 
                                    cudaStream_t stream);
 cudaError_t launch_additive_geometry(int n, const GeomJob* jobs, int count, int max_q, double* arena, int* status,
                                      cudaStream_t stream);
+cudaError_t launch_additive_geometry(int n, const WideGeomJob* jobs, int count, int max_q, double* arena,
+                                     int* status, cudaStream_t stream);
 
 }  // namespace fkpc

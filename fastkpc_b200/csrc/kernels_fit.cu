@@ -109,10 +109,11 @@ __device__ SingleObjective single_objective(double log_sp, double e, double z, b
 }  // namespace
 
 // The result record of one fit, written field by field (log_sp[j] for
-// j < m, NaN beyond), so no kernel holds a whole record in registers.
+// j < m, NaN beyond, the first kCtaPenalties), so no kernel holds a whole
+// record in registers.
 __device__ __forceinline__ void store_result(FitResult* __restrict__ out, const double* log_sp, int m, double score,
                                              double edf, double rss, int status, int iterations, int evaluations) {
-  for (int j = 0; j < kMaxPenalties; ++j) out->log_sp[j] = j < m ? log_sp[j] : NAN;
+  for (int j = 0; j < kCtaPenalties; ++j) out->log_sp[j] = j < m ? log_sp[j] : NAN;
   out->score = score;
   out->edf = edf;
   out->rss = rss;
@@ -363,8 +364,8 @@ __device__ double block_sum(double v, S* sc) {
 // Objective at sc->trial: fold the stacked roots into R (Ra'Ra = X'X + S),
 // W = R Ra^-1 by row solves, g = W'y0, W g, EDF, RSS, score.  Leaves Ra, W,
 // g, Wg in shared memory for multi_derivatives.
-template <int QMAX, int RMAX, class S = MultiScalars>
-__device__ void multi_core(const DesignDev& des, const double* __restrict__ arena, int n, double* sm, S* sc) {
+template <int QMAX, int RMAX, class S = MultiScalars, class D = DesignDev>
+__device__ void multi_core(const D& des, const double* __restrict__ arena, int n, double* sm, S* sc) {
   using L = MultiLayout<QMAX, RMAX>;
   constexpr int NT = S::kThreads;
   const int tid = threadIdx.x;
@@ -499,8 +500,8 @@ __device__ void multi_core(const DesignDev& des, const double* __restrict__ aren
 // M_j = T_j T_j' with T = Ra^-T root; with C = T'T and D = (WT)'(WT) every
 // trace is a block sum: d delta_j = lam_j sum_{a in j} D_aa,
 // d rss_j = 2 lam_j b_j'a_j, tr(M_i M_j P) = sum C_ab D_ab over block (i, j).
-template <int QMAX, int RMAX, class S = MultiScalars>
-__device__ void multi_derivatives(const DesignDev& des, const double* __restrict__ arena, int n, double* sm, S* sc) {
+template <int QMAX, int RMAX, class S = MultiScalars, class D = DesignDev>
+__device__ void multi_derivatives(const D& des, const double* __restrict__ arena, int n, double* sm, S* sc) {
   using L = MultiLayout<QMAX, RMAX>;
   constexpr int NT = S::kThreads;
   const int tid = threadIdx.x;
@@ -881,8 +882,8 @@ __device__ void gn_step(int m, S* sc) {
 
 // Per-fit set-up shared by the fit and adjoint kernels: fill-in bounds, block
 // maps, R staged in shared memory, y0 = Q'y and |y|^2.
-template <int QMAX, int RMAX, class S = MultiScalars>
-__device__ void multi_fit_setup(const DesignDev& des, const double* __restrict__ arena, const double* __restrict__ y,
+template <int QMAX, int RMAX, class S = MultiScalars, class D = DesignDev>
+__device__ void multi_fit_setup(const D& des, const double* __restrict__ arena, const double* __restrict__ y,
                                 int n, double* sm, S& sc) {
   using L = MultiLayout<QMAX, RMAX>;
   constexpr int NT = S::kThreads;
@@ -940,24 +941,25 @@ __device__ void multi_fit_setup(const DesignDev& des, const double* __restrict__
 // One fit of a CTA class: magic's search (or the Gauss-Newton selection),
 // boundary probes, polish, residual and result record.  sm: the working set
 // (shared or global), sc: the scalars, ctl: 4 shared ints.
-template <int QMAX, int RMAX, class S>
-__device__ void multi_fit_job(const DesignDev& des, const FitJob& job, int t, const double* __restrict__ arena,
+template <int QMAX, int RMAX, class S, class D>
+__device__ void multi_fit_job(const D& des, const FitJob& job, int t, const double* __restrict__ arena,
                               const double* __restrict__ data, int n, double* __restrict__ residuals,
-                              FitResult* __restrict__ results, int selection, double* sm, S& sc, int* ctl) {
+                              FitResult* __restrict__ results, int selection, double* sm, S& sc, int* ctl,
+                              double* __restrict__ all_log_sp) {
   using L = MultiLayout<QMAX, RMAX>;
   constexpr int NT = S::kThreads;
   const int tid = threadIdx.x;
   const int q = des.q, m = des.m;
   const double* y = data + static_cast<int64_t>(n) * job.column;
   const double* Q = arena + des.basis;
-  multi_fit_setup<QMAX, RMAX, S>(des, arena, y, n, sm, sc);
+  multi_fit_setup<QMAX, RMAX, S, D>(des, arena, y, n, sm, sc);
   if (tid < m) {
     sc.log_sp[tid] = des.log_sp0[tid];
     sc.trial[tid] = des.log_sp0[tid];
   }
   __syncthreads();
-  multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
-  multi_derivatives<QMAX, RMAX, S>(des, arena, n, sm, &sc);
+  multi_core<QMAX, RMAX, S, D>(des, arena, n, sm, &sc);
+  multi_derivatives<QMAX, RMAX, S, D>(des, arena, n, sm, &sc);
   double min_score = sc.score;
   double score_red = 1e10;
   bool steepest = false;
@@ -982,7 +984,7 @@ __device__ void multi_fit_job(const DesignDev& des, const FitJob& job, int t, co
       for (int tries = 1; tries <= max_half; ++tries) {
         if (tid < m) sc.trial[tid] = sc.log_sp[tid] + sc.step[tid];
         __syncthreads();
-        multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
+        multi_core<QMAX, RMAX, S, D>(des, arena, n, sm, &sc);
         ++calls;
         if (sc.status != kStatusOk) break;
         if (sc.score < min_score) {
@@ -1001,7 +1003,7 @@ __device__ void multi_fit_job(const DesignDev& des, const FitJob& job, int t, co
       min_score = sc.score;
       if (tid < m) sc.log_sp[tid] = sc.trial[tid];
       __syncthreads();
-      multi_derivatives<QMAX, RMAX, S>(des, arena, n, sm, &sc);
+      multi_derivatives<QMAX, RMAX, S, D>(des, arena, n, sm, &sc);
       if (tid < m) sc.gradient[tid] = sc.grad_c[tid];
       __syncthreads();
       double g2 = 0.0;  // projected gradient: a coordinate on the upper bound that V pushes outwards counts 0
@@ -1031,7 +1033,7 @@ __device__ void multi_fit_job(const DesignDev& des, const FitJob& job, int t, co
           __syncthreads();
           if (tid < m) sc.trial[tid] = sc.log_sp[tid] + sc.step[tid];
           __syncthreads();
-          multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
+          multi_core<QMAX, RMAX, S, D>(des, arena, n, sm, &sc);
           ++calls;
           if (sc.status != kStatusOk) break;
           const double tscore = sc.score;
@@ -1041,7 +1043,7 @@ __device__ void multi_fit_job(const DesignDev& des, const FitJob& job, int t, co
             min_score = tscore;
             if (tid < m) sc.log_sp[tid] = sc.trial[tid];
             __syncthreads();
-            multi_derivatives<QMAX, RMAX, S>(des, arena, n, sm, &sc);
+            multi_derivatives<QMAX, RMAX, S, D>(des, arena, n, sm, &sc);
           } else {
             if (tid < m) sc.step[tid] *= 0.5;
           }
@@ -1082,7 +1084,7 @@ __device__ void multi_fit_job(const DesignDev& des, const FitJob& job, int t, co
       for (int probe = 0; probe < 5; ++probe) {
         if (tid < m) sc.trial[tid] = sc.log_sp[tid] + (tid == c ? direction * 2.0 : 0.0);
         __syncthreads();
-        multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
+        multi_core<QMAX, RMAX, S, D>(des, arena, n, sm, &sc);
         ++calls;
         if (sc.status != kStatusOk || !(sc.score < min_score)) break;
         min_score = sc.score;
@@ -1097,16 +1099,16 @@ __device__ void multi_fit_job(const DesignDev& des, const FitJob& job, int t, co
     __syncthreads();
     if (tid < m) sc.trial[tid] = sc.log_sp[tid];
     __syncthreads();
-    multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
+    multi_core<QMAX, RMAX, S, D>(des, arena, n, sm, &sc);
     for (int ps = 0; ps < kPolishSteps && sc.status == kStatusOk; ++ps) {
-      multi_derivatives<QMAX, RMAX, S>(des, arena, n, sm, &sc);
+      multi_derivatives<QMAX, RMAX, S, D>(des, arena, n, sm, &sc);
       if (tid == 0) ctl[1] = polish_step(m, &sc);
       __syncthreads();
       const int act = ctl[1];
       if (act == 0) break;
       if (tid < m) sc.trial[tid] = sc.log_sp[tid];
       __syncthreads();
-      multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
+      multi_core<QMAX, RMAX, S, D>(des, arena, n, sm, &sc);
       ++calls;
       if (act == 2) break;
     }
@@ -1116,7 +1118,7 @@ __device__ void multi_fit_job(const DesignDev& des, const FitJob& job, int t, co
     __syncthreads();
     if (tid < m) sc.trial[tid] = sc.log_sp[tid];
     __syncthreads();
-    multi_core<QMAX, RMAX, S>(des, arena, n, sm, &sc);
+    multi_core<QMAX, RMAX, S, D>(des, arena, n, sm, &sc);
   }
   const double* Wg = sm + L::WG;
   double* r = residuals + static_cast<int64_t>(n) * job.out;
@@ -1128,6 +1130,8 @@ __device__ void multi_fit_job(const DesignDev& des, const FitJob& job, int t, co
     r[i] = ok ? y[i] - f : NAN;
   }
   if (tid == 0) store_result(results + t, sc.log_sp, m, sc.score, sc.edf, sc.rss, sc.status, it, calls);
+  if (all_log_sp)
+    for (int j = tid; j < kMaxPenalties; j += NT) all_log_sp[j] = j < m ? sc.log_sp[j] : NAN;
 }
 
 template <int QMAX, int RMAX>
@@ -1144,13 +1148,15 @@ __global__ void __launch_bounds__(kMultiThreads, 1) fit_multi_kernel(
   if (blockIdx.x >= job_count) return;
   const int t = job_index[blockIdx.x];
   const FitJob job = jobs[t];
-  multi_fit_job<QMAX, RMAX, MultiScalars>(designs[job.design], job, t, arena, data, n, residuals, results, selection,
-                                         sm, sc, ctl);
+  multi_fit_job<QMAX, RMAX, MultiScalars, DesignDev>(designs[job.design], job, t, arena, data, n, residuals, results,
+                                                    selection, sm, sc, ctl, nullptr);
 }
 
 // The wide class: |S| up to 62 (q <= kWideQ, stacked roots <= kWideR rows),
 // working set and scalars in a global workspace per CTA, one persistent CTA
-// per SM at most walking the class's jobs.
+// per SM at most walking the class's jobs.  Each design's full descriptor
+// sits in the arena at its header's ``ext``; the k-th job of the class writes
+// all its log(lambda) to wide_log_sp[k * kMaxPenalties ...].
 constexpr int kWideThreads = 256;
 using WideScalars = MultiScalarsT<kMaxPenalties, kWideThreads, kWideQ, kWideR>;
 constexpr int64_t kWideScalarDoubles = static_cast<int64_t>((sizeof(WideScalars) + 15) / 16 * 2);
@@ -1159,7 +1165,8 @@ constexpr int64_t kWideSlotDoubles = MultiLayout<kWideQ, kWideR>::TOTAL + kWideS
 __global__ void __launch_bounds__(kWideThreads, 1) fit_multi_wide_kernel(
     const DesignDev* __restrict__ designs, const double* __restrict__ arena, const double* __restrict__ data,
     int n, const FitJob* __restrict__ jobs, const int* __restrict__ job_index, int job_count,
-    double* __restrict__ residuals, FitResult* __restrict__ results, int selection, double* __restrict__ workspace) {
+    double* __restrict__ residuals, FitResult* __restrict__ results, int selection, double* __restrict__ workspace,
+    double* __restrict__ wide_log_sp) {
   using L = MultiLayout<kWideQ, kWideR>;
   __shared__ int ctl[4];
   double* sm = workspace + static_cast<int64_t>(blockIdx.x) * kWideSlotDoubles;
@@ -1168,8 +1175,9 @@ __global__ void __launch_bounds__(kWideThreads, 1) fit_multi_wide_kernel(
     __syncthreads();  // the previous job's scalars are read no more
     const int t = job_index[k];
     const FitJob job = jobs[t];
-    multi_fit_job<kWideQ, kWideR, WideScalars>(designs[job.design], job, t, arena, data, n, residuals, results,
-                                               selection, sm, sc, ctl);
+    const WideDesign& des = *reinterpret_cast<const WideDesign*>(arena + designs[job.design].ext);
+    multi_fit_job<kWideQ, kWideR, WideScalars, WideDesign>(des, job, t, arena, data, n, residuals, results, selection,
+                                                           sm, sc, ctl, wide_log_sp + static_cast<int64_t>(k) * kMaxPenalties);
   }
 }
 
@@ -2383,7 +2391,7 @@ __global__ void __launch_bounds__(kMultiThreads, 1) gcv_adjoint_kernel(
   const DesignDev& des = designs[design];
   const int tid = threadIdx.x;
   const int m = des.m;
-  multi_fit_setup<QMAX, RMAX, MultiScalars>(des, arena, y, n, sm, sc);
+  multi_fit_setup<QMAX, RMAX, MultiScalars, DesignDev>(des, arena, y, n, sm, sc);
   if (tid < m) {
     sc.trial[tid] = rho[static_cast<int64_t>(pt) * m + tid];
     sc.log_sp[tid] = sc.trial[tid];
@@ -2465,7 +2473,7 @@ cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const dou
                              int n, const FitJob* jobs, const int* job_index, int count, double* residuals,
                              FitResult* results, cudaStream_t stream, int selection, double* workspace,
                              FitState* states, int* defer_list, int* defer_count, cudaEvent_t after_warp,
-                             int defer_calls) {
+                             int defer_calls, double* wide_log_sp) {
   if (count <= 0) return cudaSuccess;
   if (qmax_class == 0) {
     // fits still searching after defer_calls evaluations continue in the
@@ -2499,10 +2507,10 @@ cudaError_t launch_fit_multi(int qmax_class, const DesignDev* designs, const dou
     fit_multi_kernel<112, 96><<<count, kMultiThreads, 0, stream>>>(designs, arena, data, n, jobs, job_index, count,
                                                                     residuals, results, selection, workspace);
   } else {
-    if (!workspace) return cudaErrorInvalidValue;
+    if (!workspace || !wide_log_sp) return cudaErrorInvalidValue;
     fit_multi_wide_kernel<<<wide_ctas(count), kWideThreads, 0, stream>>>(designs, arena, data, n, jobs, job_index,
                                                                         count, residuals, results, selection,
-                                                                        workspace);
+                                                                        workspace, wide_log_sp);
   }
   return cudaGetLastError();
 }

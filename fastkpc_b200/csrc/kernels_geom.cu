@@ -134,7 +134,8 @@ static __device__ bool householder_inplace(double* __restrict__ W, int n, int q,
 // in_smem: the design's n x q working matrix lives in dynamic shared memory
 // (n q doubles available) and Q is written to the arena at the end;
 // otherwise it is factored in place in the arena (L2).
-__global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(int n, const GeomJob* __restrict__ jobs,
+template <class J>
+__global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(int n, const J* __restrict__ jobs,
                                                                          int count, double* __restrict__ arena,
                                                                          int* __restrict__ status, int in_smem) {
   extern __shared__ double wsm[];
@@ -143,7 +144,7 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(int n, 
   __shared__ double red[kGeomWarps];
   const int tid = threadIdx.x;
   for (int d = blockIdx.x; d < count; d += gridDim.x) {
-    const GeomJob& job = jobs[d];
+    const J& job = jobs[d];
     const int q = job.q;
     double* Q = arena + job.basis;
     double* W = in_smem ? wsm : Q;
@@ -432,16 +433,27 @@ cudaError_t launch_single_geometry(int n, const SingleGeomJob* jobs, int count, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_additive_geometry(int n, const GeomJob* jobs, int count, int max_q, double* arena, int* status,
-                                     cudaStream_t stream) {
+template <class J>
+cudaError_t launch_additive_geometry_t(int n, const J* jobs, int count, int max_q, double* arena, int* status,
+                                       cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
   if (n < 2 || max_q < 1 || max_q > kGeomMaxQ || max_q >= n) return cudaErrorInvalidValue;
   const size_t smem = geometry_smem(n, max_q, kAdditiveStaticSmem);
   int ctas = 0;
-  cudaError_t e = geometry_launch_shape(additive_geometry_kernel, smem, count, &ctas);
+  cudaError_t e = geometry_launch_shape(additive_geometry_kernel<J>, smem, count, &ctas);
   if (e != cudaSuccess) return e;
-  additive_geometry_kernel<<<ctas, kGeomThreads, smem, stream>>>(n, jobs, count, arena, status, smem > 0 ? 1 : 0);
+  additive_geometry_kernel<J><<<ctas, kGeomThreads, smem, stream>>>(n, jobs, count, arena, status, smem > 0 ? 1 : 0);
   return cudaGetLastError();
+}
+
+cudaError_t launch_additive_geometry(int n, const GeomJob* jobs, int count, int max_q, double* arena, int* status,
+                                     cudaStream_t stream) {
+  return launch_additive_geometry_t(n, jobs, count, max_q, arena, status, stream);
+}
+
+cudaError_t launch_additive_geometry(int n, const WideGeomJob* jobs, int count, int max_q, double* arena,
+                                     int* status, cudaStream_t stream) {
+  return launch_additive_geometry_t(n, jobs, count, max_q, arena, status, stream);
 }
 
 }  // namespace fkpc

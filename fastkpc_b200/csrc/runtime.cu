@@ -73,6 +73,7 @@ Engine::Engine(int device) : device_(device) {
   cuda_check(cudaEventCreateWithFlags(&ev_warp_, cudaEventDisableTiming), "cudaEventCreate");
   cuda_check(cudaEventCreateWithFlags(&ev_side_, cudaEventDisableTiming), "cudaEventCreate");
   cuda_check(cudaEventCreateWithFlags(&ev_part_, cudaEventDisableTiming), "cudaEventCreate");
+  cuda_check(cudaEventCreate(&ev_call_), "cudaEventCreate");
 }
 
 Engine::~Engine() {
@@ -87,6 +88,7 @@ Engine::~Engine() {
   if (ev_warp_) cudaEventDestroy(ev_warp_);
   if (ev_side_) cudaEventDestroy(ev_side_);
   if (ev_part_) cudaEventDestroy(ev_part_);
+  if (ev_call_) cudaEventDestroy(ev_call_);
   if (side_) {
     cudaStreamSynchronize(side_);
     cudaStreamDestroy(side_);
@@ -543,9 +545,13 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
     }
     return sl;
   };
+  // designs with more than kCtaPenalties blocks: their full descriptors,
+  // copied into the host range of the arena at ``ext``
+  std::vector<std::pair<size_t, WideDesign>> wide_desc;
   for (size_t d = 0; d < designs_.size(); ++d) {
     DesignDev& dd = ddesc[d];
     std::memset(&dd, 0, sizeof(dd));
+    dd.ext = -1;
     if (!designs_[d]) {
       if (sets_[d].size() != 2) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "design set-up incomplete");
       dd.kind = 1;
@@ -591,21 +597,38 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
       dd.rmat = static_cast<int64_t>(at);
       at += static_cast<size_t>(des.q) * des.q;
       dd.roots = static_cast<int64_t>(total);
+      if (des.m > kMaxPenalties)
+        throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity (q <= 560, |S| <= 62)");
+      WideDesign wd;
+      std::memset(&wd, 0, sizeof(wd));
       int rows = 0;
       int64_t rootoff = 0;
       for (int j = 0; j < des.m; ++j) {
-        dd.off[j] = des.offsets[j];
-        dd.dim[j] = des.dims[j];
-        dd.rank[j] = des.ranks[j];
-        dd.rowoff[j] = rows;
-        dd.rootoff[j] = static_cast<int>(rootoff);
-        dd.log_sp0[j] = des.initial_log_sp[j];
+        wd.off[j] = des.offsets[j];
+        wd.dim[j] = des.dims[j];
+        wd.rank[j] = des.ranks[j];
+        wd.rowoff[j] = rows;
+        wd.rootoff[j] = static_cast<int>(rootoff);
+        wd.log_sp0[j] = des.initial_log_sp[j];
         rows += des.ranks[j];
         rootoff += static_cast<int64_t>(des.roots[j].size());
       }
+      for (int j = 0; j < des.m && j < kCtaPenalties; ++j) {
+        dd.off[j] = wd.off[j];
+        dd.dim[j] = wd.dim[j];
+        dd.rank[j] = wd.rank[j];
+        dd.rowoff[j] = wd.rowoff[j];
+        dd.rootoff[j] = wd.rootoff[j];
+        dd.log_sp0[j] = wd.log_sp0[j];
+      }
       total += static_cast<size_t>(rootoff);
       dd.rsum = rows;
-      if (des.q > kWideQ || rows > kWideR || des.m > kMaxPenalties)
+      if (des.m > kCtaPenalties) {
+        dd.ext = static_cast<int64_t>(total);
+        total += sizeof(WideDesign) / sizeof(double);
+        wide_desc.emplace_back(d, wd);
+      }
+      if (des.q > kWideQ || rows > kWideR)
         throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity (q <= 560, |S| <= 62)");
       if (des.q >= n_)
         throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design has at least as many coefficients as observations (q = " +
@@ -638,9 +661,23 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
     ddesc[d].basis += static_cast<int64_t>(dev_base);
     ddesc[d].spec += static_cast<int64_t>(dev_base);
   }
+  for (auto& [d, wd] : wide_desc) {  // the header with its final arena offsets
+    const DesignDev& dd = ddesc[d];
+    wd.kind = dd.kind;
+    wd.q = dd.q;
+    wd.m = dd.m;
+    wd.rsum = dd.rsum;
+    wd.basis = dd.basis;
+    wd.rmat = dd.rmat;
+    wd.spec = dd.spec;
+    wd.roots = dd.roots;
+    wd.rpack = dd.rpack;
+    wd.ext = dd.ext;
+  }
   // Pass 2: every design copies its host-built part into the pinned staging
   // buffer (threads over designs), then one DMA to the device arena.
   double* host = pinned_arena(total);
+  for (const auto& [d, wd] : wide_desc) std::memcpy(host + ddesc[d].ext, &wd, sizeof(WideDesign));
   {
     std::atomic<size_t> next(0);
     auto work = [&]() {
@@ -662,8 +699,11 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
           std::memcpy(host + dd.basis, des.QW.data(), des.QW.size() * sizeof(double));
           std::memcpy(host + dd.spec, des.spec.data(), des.spec.size() * sizeof(double));
         } else {
-          for (int j = 0; j < des.m; ++j)
-            std::memcpy(host + dd.roots + dd.rootoff[j], des.roots[j].data(), des.roots[j].size() * sizeof(double));
+          size_t rootoff = 0;  // the blocks' roots are consecutive (rootoff of the descriptors)
+          for (int j = 0; j < des.m; ++j) {
+            std::memcpy(host + dd.roots + rootoff, des.roots[j].data(), des.roots[j].size() * sizeof(double));
+            rootoff += des.roots[j].size();
+          }
           if (des.device_geometry) continue;
           std::memcpy(host + dd.basis, des.Q.data(), des.Q.size() * sizeof(double));
           std::memcpy(host + dd.rmat, des.R.data(), des.R.size() * sizeof(double));
@@ -690,7 +730,8 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
   // Device geometry jobs; the smooth bases and penalties sit in the host range
   // (a bivariate basis built on the device stays in the smooth store).
   double* arena = d_arena_.ensure(dev_base + dev_total);
-  std::vector<GeomJob> gjobs(geom_designs.size());
+  std::vector<GeomJob> gjobs;
+  std::vector<WideGeomJob> wgjobs;
   std::vector<SingleGeomJob> sjobs(single_designs.size());
   int geom_max_q = 1;
   for (size_t g = 0; g < single_designs.size(); ++g) {
@@ -706,22 +747,32 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
     job.q = des.q;
     job.rank = des.ranks[0];
   }
-  for (size_t g = 0; g < geom_designs.size(); ++g) {
-    const Design& des = *designs_[geom_designs[g]];
-    const DesignDev& dd = ddesc[geom_designs[g]];
-    GeomJob& job = gjobs[g];
+  int wide_max_q = 1;
+  auto fill_geom = [&](auto& job, const Design& des, const DesignDev& dd) {
     std::memset(&job, 0, sizeof(job));
     job.basis = dd.basis;
     job.rmat = dd.rmat;
     job.rpack = dd.rpack;
     job.q = des.q;
     job.m = des.m;
-    geom_max_q = std::max(geom_max_q, des.q);
     for (int j = 0; j < des.m; ++j) {
       const Smooth* sm = des.parts[j].get();
       job.src[j] = sm->dev_x ? sm->dev_x : arena + smooth_slots[smooth_index.at(sm)].x;
       job.off[j] = des.offsets[j];
       job.dim[j] = des.dims[j];
+    }
+  };
+  for (size_t g = 0; g < geom_designs.size(); ++g) {
+    const Design& des = *designs_[geom_designs[g]];
+    const DesignDev& dd = ddesc[geom_designs[g]];
+    if (des.m > kCtaPenalties) {
+      wgjobs.emplace_back();
+      fill_geom(wgjobs.back(), des, dd);
+      wide_max_q = std::max(wide_max_q, des.q);
+    } else {
+      gjobs.emplace_back();
+      fill_geom(gjobs.back(), des, dd);
+      geom_max_q = std::max(geom_max_q, des.q);
     }
   }
   // Widest designs first: the geometry kernel's CTAs take jobs in a fixed
@@ -768,7 +819,8 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
       if (dd.q <= kWarpQ && dd.rsum <= kWarpR && dd.m <= kWarpM) multi_small_.push_back(idx);
       else if (dd.q <= 76 && dd.rsum <= 64 && dd.m <= kCtaPenalties) multi_large_.push_back(idx);
       else if (dd.q <= 112 && dd.rsum <= 96 && dd.m <= kCtaPenalties) multi_huge_.push_back(idx);
-      else multi_wide_.push_back(idx);
+      else if (dd.ext >= 0) multi_wide_.push_back(idx);
+      else throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design fits no fit class");
     }
   }
   if (opt.mode != FKPC_MODE_PLAIN) {
@@ -794,8 +846,8 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
   if (total > 0)
     cuda_check(cudaMemcpyAsync(arena, host, total * sizeof(double), cudaMemcpyHostToDevice, stream_), "upload arena");
   h2d_bytes_ += static_cast<double>(total * sizeof(double));
-  int* gstatus_dev = d_geom_status_.ensure(gjobs.size() + sjobs.size() + pending_.size());
-  geom_status_used_ = gjobs.size() + sjobs.size();
+  int* gstatus_dev = d_geom_status_.ensure(gjobs.size() + wgjobs.size() + sjobs.size() + pending_.size());
+  geom_status_used_ = gjobs.size() + wgjobs.size() + sjobs.size();
   geom_status_checked_ = 0;
   if (!gjobs.empty()) {
     h2d_bytes_ += stage_upload(d_geom_jobs_, gjobs);
@@ -803,10 +855,16 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
                                         gstatus_dev, stream_),
                "additive geometry");
   }
+  if (!wgjobs.empty()) {
+    h2d_bytes_ += stage_upload(d_wide_geom_jobs_, wgjobs);
+    cuda_check(launch_additive_geometry(n, d_wide_geom_jobs_.get(), static_cast<int>(wgjobs.size()), wide_max_q, arena,
+                                        gstatus_dev + gjobs.size(), stream_),
+               "additive geometry");
+  }
   if (!sjobs.empty()) {
     h2d_bytes_ += stage_upload(d_single_geom_jobs_, sjobs);
     cuda_check(launch_single_geometry(n, d_single_geom_jobs_.get(), static_cast<int>(sjobs.size()), arena,
-                                      gstatus_dev + gjobs.size(), stream_),
+                                      gstatus_dev + gjobs.size() + wgjobs.size(), stream_),
                "single-penalty geometry");
   }
   h2d_bytes_ += stage_upload(d_designs_, ddesc);
@@ -824,6 +882,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
   if (!multi_huge_.empty() || !multi_wide_.empty())
     d_fit_ws_.ensure(std::max(multi_workspace_doubles(2, static_cast<int>(multi_huge_.size())),
                               multi_workspace_doubles(3, static_cast<int>(multi_wide_.size()))));
+  if (!multi_wide_.empty()) d_wide_log_sp_.ensure(multi_wide_.size() * static_cast<size_t>(kMaxPenalties));
   h2d_bytes_ += stage_upload(d_direct_cols_, direct_cols_);
   h2d_bytes_ += stage_upload(d_direct_slots_, direct_slots_);
   h2d_bytes_ += stage_upload(d_pairs_, pairs_);
@@ -956,6 +1015,7 @@ void Engine::pack_late(cudaStream_t st) {
 void Engine::prepare(const std::vector<Test>& tests, const fkpc_options& opt, RStream* rstream) {
   if (n_ == 0) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "no data loaded");
   graph_timed_ = false;
+  call_timed_ = false;
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   cuda_check(cudaStreamSynchronize(stream_), "prepare");
   stage_reset();
@@ -987,23 +1047,34 @@ void Engine::run_batch(const std::vector<Test>& tests, const fkpc_options& opt, 
   release_graph();
   try {
     auto t0 = std::chrono::steady_clock::now();
+    cuda_check(cudaEventRecord(ev_call_, stream_), "event");
+    call_timed_ = true;
     plan_components(tests);
     designs_built_ = 0;
     for (const auto& S : sets_) designs_built_ += cache_->has_design(S) ? 0 : 1;
     smooths_built_ = static_cast<int>(univariate_columns().size());
-  smooths_built_ = static_cast<int>(univariate_columns().size());
+    plan_ms_ = ms_since(t0);
     designs_.assign(sets_.size(), nullptr);
     std::vector<std::vector<int>> bivariate;
     for (const auto& S : sets_)
       if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
+    // Both thin-plate batches on the main stream: the Lanczos kernels are
+    // persistent and hold every SM, so on a second stream they would delay
+    // the multi-penalty fits rather than run beside them.
     TprsBatch ubatch, batch;
+    auto tp = std::chrono::steady_clock::now();
     launch_tprs_batch(univariate_columns(), 1, &ubatch, stream_, tuning_.tprs_ctas_per_sm);
     if (!bivariate.empty()) launch_tprs_batch(bivariate, 2, &batch, stream_, tuning_.tprs_ctas_per_sm);
+    tprs_host_ms_ = ms_since(tp);
+    auto tw = std::chrono::steady_clock::now();
     finish_tprs_batch(&ubatch);
+    smooth_wait_ms_ = ms_since(tw);
+    auto td = std::chrono::steady_clock::now();
     build_univariate_smooths();  // those the device could not take
     build_host_designs([this](const std::vector<int>& S) { return S.size() != 2 || cache_->has_design(S); });
+    design_host_ms_ = ms_since(td);
     double host_ms = ms_since(t0);
-    pack_and_upload(opt, rstream, true);  // queued behind the thin-plate kernels
+    pack_and_upload(opt, rstream, true);  // queued behind the univariate thin-plate kernels
     double up_ms = upload_ms_;
     cuda_check(configure_fit_kernels(), "kernel attributes");
     cuda_check(configure_stat_kernels(n_), "kernel attributes");
@@ -1012,7 +1083,10 @@ void Engine::run_batch(const std::vector<Test>& tests, const fkpc_options& opt, 
     enqueue_multi();
     auto t1 = std::chrono::steady_clock::now();
     finish_tprs_batch(&batch);
+    late_wait_ms_ = ms_since(t1);
+    auto td2 = std::chrono::steady_clock::now();
     build_host_designs([](const std::vector<int>&) { return true; });
+    design_host_ms_ += ms_since(td2);
     host_ms += ms_since(t1);
     auto t2 = std::chrono::steady_clock::now();
     pack_late(split_stats() ? side_ : stream_);
@@ -1055,7 +1129,8 @@ void Engine::enqueue_multi() {
   if (!multi_wide_.empty()) {  // after the q <= 112 class: the two share the workspace
     cuda_check(launch_fit_multi(3, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                 d_multi_wide_.get(), static_cast<int>(multi_wide_.size()), d_resid_.get(),
-                                d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get()),
+                                d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get(), nullptr, nullptr,
+                                nullptr, nullptr, 0, d_wide_log_sp_.get()),
                "fit multi");
     ++launches_;
   }
@@ -1392,6 +1467,14 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
     stats->designs = static_cast<int>(sets_.size());
     stats->designs_built = designs_built_;
     stats->smooths_built = smooths_built_;
+    stats->plan_ms = call_timed_ ? plan_ms_ : 0.0;
+    stats->tprs_host_ms = call_timed_ ? tprs_host_ms_ : 0.0;
+    stats->design_host_ms = call_timed_ ? design_host_ms_ : 0.0;
+    stats->smooth_wait_ms = call_timed_ ? smooth_wait_ms_ : 0.0;
+    stats->late_wait_ms = call_timed_ ? late_wait_ms_ : 0.0;
+    float pre = 0.f;
+    if (call_timed_) cudaEventElapsedTime(&pre, ev_call_, ev_[0]);
+    stats->prefit_device_ms = pre;
     stats->targets = static_cast<int>(single_jobs_.size() + multi_jobs_.size());
     stats->pairs = static_cast<int>(pairs_.size());
     stats->guarded = guarded;
@@ -1507,7 +1590,8 @@ void Engine::enqueue_plain_test(int t) {
   if (w1 > w0) {
     cuda_check(launch_fit_multi(3, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                 d_multi_wide_.get() + w0, w1 - w0, d_resid_.get(), d_multi_res_.get(), stream_,
-                                opt_.selection, d_fit_ws_.get()),
+                                opt_.selection, d_fit_ws_.get(), nullptr, nullptr, nullptr, nullptr, 0,
+                                d_wide_log_sp_.get() + static_cast<size_t>(w0) * kMaxPenalties),
                "fit multi");
     ++launches_;
   }
@@ -1601,7 +1685,8 @@ double Engine::time_stage(int stage, int repeats, double* flops_per_launch) {
                                       d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get());
       case 10: return launch_fit_multi(3, d_designs_.get(), d_arena_.get(), d_data_.get(), n, d_multi_jobs_.get(),
                                        d_multi_wide_.get(), static_cast<int>(multi_wide_.size()), d_resid_.get(),
-                                       d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get());
+                                       d_multi_res_.get(), stream_, opt_.selection, d_fit_ws_.get(), nullptr,
+                                       nullptr, nullptr, nullptr, 0, d_wide_log_sp_.get());
       case 3: return launch_dcov_components(d_resid_.get(), n, d_comp_cols_.get(), ncomp, d_centre_.get(),
                                             d_dcov_.get(), stream_);
       case 4: return launch_dcov_pairs(d_resid_.get(), n, d_comp_cols_.get(), d_centre_.get(), d_dcov_.get(),
@@ -1696,6 +1781,7 @@ void Engine::regress(const std::vector<int>& targets, const std::vector<std::vec
   fkpc_default_options(&opt);
   opt.selection = selection;
   opt_ = opt;
+  call_timed_ = false;
   release_graph();
   cuda_check(cudaStreamSynchronize(stream_), "set-up");
   stage_reset();
@@ -1724,16 +1810,27 @@ void Engine::regress(const std::vector<int>& targets, const std::vector<std::vec
   std::vector<const FitResult*> by_comp(comps_.size(), nullptr);
   for (size_t i = 0; i < single_jobs_.size(); ++i) by_comp[single_jobs_[i].out] = &sres[i];
   for (size_t i = 0; i < multi_jobs_.size(); ++i) by_comp[multi_jobs_[i].out] = &mres[i];
+  // the wide class's log(lambda), all m of them, per component
+  std::vector<double> wide(multi_wide_.size() * static_cast<size_t>(kMaxPenalties));
+  std::vector<const double*> wide_by_comp(comps_.size(), nullptr);
+  if (!wide.empty()) {
+    cuda_check(cudaMemcpy(wide.data(), d_wide_log_sp_.get(), wide.size() * sizeof(double), cudaMemcpyDeviceToHost),
+               "download");
+    for (size_t k = 0; k < multi_wide_.size(); ++k)
+      wide_by_comp[multi_jobs_[multi_wide_[k]].out] = wide.data() + k * kMaxPenalties;
+  }
   for (size_t i = 0; i < targets.size(); ++i) {
     const int c = pairs_[i].left;
     std::copy(slab.begin() + static_cast<size_t>(n) * c, slab.begin() + static_cast<size_t>(n) * (c + 1),
               residuals + static_cast<size_t>(n) * i);
     const FitResult* r = by_comp[c];
+    const double* wl = wide_by_comp[c];
     if (status) status[i] = r ? r->status : kStatusOk;
     if (evaluations) evaluations[i] = r ? r->evaluations : 0;
     if (log_sp)
       for (int j = 0; j < max_penalties; ++j)
-        log_sp[i * static_cast<size_t>(max_penalties) + j] = (r && j < kMaxPenalties) ? r->log_sp[j] : NAN;
+        log_sp[i * static_cast<size_t>(max_penalties) + j] =
+            wl ? (j < kMaxPenalties ? wl[j] : NAN) : ((r && j < kCtaPenalties) ? r->log_sp[j] : NAN);
   }
   stats_enabled_ = true;
 }
@@ -1813,6 +1910,7 @@ void Engine::statistics(const double* residuals, int m, const std::vector<int>& 
     if (left[i] < 0 || left[i] >= m || right[i] < 0 || right[i] >= m)
       throw Error(FKPC_STATUS_INVALID_ARGUMENT, "residual column index out of range");
   opt_ = opt;
+  call_timed_ = false;
   release_graph();
   tests_.clear();
   comps_.assign(m, Component{0, -1});

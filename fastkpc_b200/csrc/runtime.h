@@ -227,6 +227,8 @@ class Engine {
   TprsBuffers tprs_buf_[2];
   // device geometry of the additive designs
   DevBuf<GeomJob> d_geom_jobs_;
+  DevBuf<WideGeomJob> d_wide_geom_jobs_;
+  DevBuf<double> d_wide_log_sp_;  // kMaxPenalties log(lambda) per wide-class job
   DevBuf<SingleGeomJob> d_single_geom_jobs_;
   DevBuf<int> d_geom_status_;
   DevBuf<FitResult> d_single_res_, d_multi_res_;
@@ -263,6 +265,11 @@ class Engine {
   int designs_built_ = 0;  // sets of the last batch whose design the cache lacked
   int smooths_built_ = 0;  // univariate smooths the last batch set up
   double setup_ms_ = 0.0, upload_ms_ = 0.0;
+  // timeline of a one-shot batch (run_batch): host planning, host waits on
+  // the device's smooth bases, and the call-start event of the device timeline
+  double plan_ms_ = 0.0, smooth_wait_ms_ = 0.0, late_wait_ms_ = 0.0, tprs_host_ms_ = 0.0, design_host_ms_ = 0.0;
+  bool call_timed_ = false;
+  cudaEvent_t ev_call_ = nullptr;
   int guard_count_host_ = 0;
   double h2d_bytes_ = 0.0, d2h_bytes_ = 0.0;
   double stage_flops_[11] = {};

@@ -111,6 +111,13 @@ typedef struct fkpc_stage_stats {
   double device_ms;         /* device time of the batch's launch sequence */
   int designs_built;        /* conditioning-set designs the call set up (not found in the cache) */
   int smooths_built;        /* per-variable (univariate) smooth bases the call set up */
+  /* timeline of a one-shot call (fkpc_ci_level_batch and the skeleton's levels) */
+  double plan_ms;           /* host: components and conditioning sets of the tests */
+  double tprs_host_ms;      /* host: unique locations and staging of the thin-plate set-up */
+  double design_host_ms;    /* host: design descriptors, initial.sp and penalty roots */
+  double smooth_wait_ms;    /* host blocked until the device's univariate smooth bases landed */
+  double late_wait_ms;      /* host blocked until the device's bivariate smooth bases landed */
+  double prefit_device_ms;  /* device timeline from the call's first launch to the first fit launch */
 } fkpc_stage_stats;
 
 typedef struct fkpc_trace_row {

@@ -289,7 +289,9 @@ constexpr double kPolishDone = 1e-10;
 constexpr double kPolishCurvature = 1e-6;
 constexpr double kGnGradTol = 1e-9;   // Gauss-Newton selection: |grad V| <= 1e-9 (1 + V),
 constexpr double kGnFlatTol = 1e-12;  // or a decrease <= 1e-12 (1 + V)
-constexpr double kGnFlatGrad = 1e-6;  // with |grad V| <= 1e-6 (1 + V)
+constexpr double kGnFlatGrad = 1e-6;  // with |grad V| <= 1e-6 (1 + V),
+constexpr double kGnStallStep = 1e-8;  // or an accepted step below 1e-8 in max norm
+constexpr double kGnStallTol = 1e-10;  // that decreased V by at most 1e-10 (1 + V): stalled
 constexpr double kGnMaxLogSp = 25.0;  // upper bound of the Gauss-Newton search in log(lambda)
 
 __device__ __forceinline__ int tri(int i, int j) { return j * (j + 1) / 2 + i; }  // packed upper, i <= j
@@ -1009,10 +1011,14 @@ __device__ void multi_fit_job(const D& des, const FitJob& job, int t, const doub
       double g2 = 0.0;  // projected gradient: a coordinate on the upper bound that V pushes outwards counts 0
       for (int r = 0; r < m; ++r)
         if (!(sc.log_sp[r] >= kGnMaxLogSp && sc.gradient[r] < 0.0)) g2 += sc.gradient[r] * sc.gradient[r];
-      // a stationary point (not magic's loose stop), or V no longer moving
-      // along directions that have gone flat (log lambda drifting upwards)
+      // a stationary point (not magic's loose stop), V no longer moving along
+      // directions that have gone flat (log lambda drifting upwards), or a
+      // line search that only finds negligible steps (the direction stalls)
+      double smax = 0.0;
+      for (int r = 0; r < m; ++r) smax = fmax(smax, fabs(sc.step[r]));
       if (sqrt(g2) <= kGnGradTol * (1.0 + fabs(min_score)) ||
-          (score_red <= kGnFlatTol * (1.0 + min_score) && sqrt(g2) <= kGnFlatGrad * (1.0 + fabs(min_score)))) {
+          (score_red <= kGnFlatTol * (1.0 + min_score) && sqrt(g2) <= kGnFlatGrad * (1.0 + fabs(min_score))) ||
+          (smax <= kGnStallStep && score_red <= kGnStallTol * (1.0 + min_score))) {
         converged = true;
         break;
       }
@@ -1889,10 +1895,14 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
       double g2 = 0.0;  // projected gradient: a coordinate on the upper bound that V pushes outwards counts 0
       for (int r = 0; r < m; ++r)
         if (!(sc.log_sp[r] >= kGnMaxLogSp && sc.gradient[r] < 0.0)) g2 += sc.gradient[r] * sc.gradient[r];
-      // a stationary point (not magic's loose stop), or V no longer moving
-      // along directions that have gone flat (log lambda drifting upwards)
+      // a stationary point (not magic's loose stop), V no longer moving along
+      // directions that have gone flat (log lambda drifting upwards), or a
+      // line search that only finds negligible steps (the direction stalls)
+      double smax = 0.0;
+      for (int r = 0; r < m; ++r) smax = fmax(smax, fabs(sc.step[r]));
       if (sqrt(g2) <= kGnGradTol * (1.0 + fabs(min_score)) ||
-          (score_red <= kGnFlatTol * (1.0 + min_score) && sqrt(g2) <= kGnFlatGrad * (1.0 + fabs(min_score)))) {
+          (score_red <= kGnFlatTol * (1.0 + min_score) && sqrt(g2) <= kGnFlatGrad * (1.0 + fabs(min_score))) ||
+          (smax <= kGnStallStep && score_red <= kGnStallTol * (1.0 + min_score))) {
         converged = true;
         break;
       }

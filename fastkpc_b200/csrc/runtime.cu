@@ -231,7 +231,9 @@ void Engine::plan_components(const std::vector<Test>& tests) {
     }
     PairJob job;
     job.left = component(ts.x, set);
-    job.right = component(ts.y, set);
+    // a regression batch fits the targets alone: its tests' partners are
+    // placeholders, given the target's component
+    job.right = regress_only_ ? job.left : component(ts.y, set);
     job.out = static_cast<int>(t);
     job.pad = 0;
     pairs_.push_back(job);
@@ -1393,10 +1395,14 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
   d2h_bytes_ += static_cast<double>((sres.size() + mres.size()) * sizeof(FitResult));
   account_flops(sres, mres);
   collected_ = true;
-  for (size_t i = 0; i < sres.size(); ++i)
-    if (sres[i].status != kStatusOk) throw fit_failure(single_jobs_[i], sres[i]);
-  for (size_t i = 0; i < mres.size(); ++i)
-    if (mres[i].status != kStatusOk) throw fit_failure(multi_jobs_[i], mres[i]);
+  // a regression batch reports each fit's status (its residual is NaN); a
+  // CI batch fails as a whole
+  if (stats_enabled_) {
+    for (size_t i = 0; i < sres.size(); ++i)
+      if (sres[i].status != kStatusOk) throw fit_failure(single_jobs_[i], sres[i]);
+    for (size_t i = 0; i < mres.size(); ++i)
+      if (mres[i].status != kStatusOk) throw fit_failure(multi_jobs_[i], mres[i]);
+  }
   std::vector<RecordDev> recs(pairs_.size());
   if (!recs.empty() && stats_enabled_)
     cuda_check(cudaMemcpy(recs.data(), d_records_.get(), recs.size() * sizeof(RecordDev), cudaMemcpyDeviceToHost), "download");
@@ -1787,7 +1793,14 @@ void Engine::regress(const std::vector<int>& targets, const std::vector<std::vec
   stage_reset();
   d2h_bytes_ = 0.0;
   auto t0 = std::chrono::steady_clock::now();
-  plan_components(tests);
+  regress_only_ = true;
+  try {
+    plan_components(tests);
+  } catch (...) {
+    regress_only_ = false;
+    throw;
+  }
+  regress_only_ = false;
   designs_built_ = 0;
   for (const auto& S : sets_) designs_built_ += cache_->has_design(S) ? 0 : 1;
   smooths_built_ = static_cast<int>(univariate_columns().size());

@@ -269,6 +269,7 @@ class Engine {
   // the device's smooth bases, and the call-start event of the device timeline
   double plan_ms_ = 0.0, smooth_wait_ms_ = 0.0, late_wait_ms_ = 0.0, tprs_host_ms_ = 0.0, design_host_ms_ = 0.0;
   bool call_timed_ = false;
+  bool regress_only_ = false;  // plan_components: the targets' components only
   cudaEvent_t ev_call_ = nullptr;
   int guard_count_host_ = 0;
   double h2d_bytes_ = 0.0, d2h_bytes_ = 0.0;

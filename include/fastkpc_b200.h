@@ -295,7 +295,8 @@ FKPC_API int fkpc_ci_plain_one(const double* data_colmajor, int n, int p, int x,
  * regrXonS residuals for ``count`` (target, S) fits: residuals is n x count
  * column-major; log_sp receives up to ``max_penalties`` selected
  * log smoothing parameters per fit (row-major count x max_penalties, unused
- * entries NaN); status per fit.
+ * entries NaN); status per fit (a failed fit leaves NaN residuals and its
+ * FKPC_STATUS_* code; the call itself still returns 0).
  * Replaces single_penalty_gcv_cuda (fastkpc/src/cuda/mgcv_single_penalty_gcv.cu:1863),
  * multi_penalty_gcv_capacity_optimize_batch
  * (fastkpc/src/cuda/mgcv_multi_penalty_gcv_capacity.cpp:233) and

@@ -561,6 +561,8 @@ def gcv_residual_vector(prep, y, log_sp):
 
 GN_GRAD_TOL = 1e-9
 GN_FLAT_TOL = 1e-12
+GN_STALL_STEP = 1e-8   # an accepted step below this in max norm ...
+GN_STALL_TOL = 1e-10   # ... that decreased V by at most this (1 + V): the direction has stalled
 GN_FLAT_GRAD = 1e-6
 GN_MAX_LOG_SP = 25.0
 
@@ -617,8 +619,10 @@ def optimize_gn(prep, y, max_half=25, max_iter=400, trace=None):
     """Newton selection driven by the adjoint (the library's
     FKPC_SELECT_GN_NEWTON): from magic's start, exact-Hessian Newton where that
     Hessian is positive definite and damped Gauss-Newton elsewhere, halving
-    until V decreases; stop at |grad V| <= GN_GRAD_TOL (1 + V) or when no
-    decrease is possible, with log(lambda) kept <= GN_MAX_LOG_SP; then the
+    until V decreases; stop at |grad V| <= GN_GRAD_TOL (1 + V), when no
+    decrease is possible, or when the line search only finds steps below
+    GN_STALL_STEP that decrease V by at most GN_STALL_TOL (1 + V), with
+    log(lambda) kept <= GN_MAX_LOG_SP; then the
     terminal polish (no boundary probes)."""
     resp = prep.response(y)
     m = prep.m
@@ -651,7 +655,8 @@ def optimize_gn(prep, y, max_half=25, max_iter=400, trace=None):
         gn = gcv_gauss_newton(prep, y, rho)
         gnorm = np.linalg.norm(np.where((rho >= GN_MAX_LOG_SP) & (g < 0.0), 0.0, g))  # projected gradient
         if (gnorm <= GN_GRAD_TOL * (1.0 + abs(core["score"]))
-                or (red <= GN_FLAT_TOL * (1.0 + core["score"]) and gnorm <= GN_FLAT_GRAD * (1.0 + abs(core["score"])))):
+                or (red <= GN_FLAT_TOL * (1.0 + core["score"]) and gnorm <= GN_FLAT_GRAD * (1.0 + abs(core["score"])))
+                or (np.max(np.abs(step)) <= GN_STALL_STEP and red <= GN_STALL_TOL * (1.0 + core["score"]))):
             converged = True
             break
     if not converged:

@@ -34,6 +34,7 @@ METHODS = {"dcc.gamma": 0, "dcc.perm": 1, "hsic.gamma": 2, "hsic.perm": 3}
 MODES = {"batched": 0, "plain": 1}
 FLAG_GUARDED = 1
 FLAG_DIRECT = 2
+FLAG_RANK_TRUNCATED = 4
 
 STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-finite numerics",
                 4: "iteration limit", 5: "rank deficiency", 6: "allocation failure", 7: "no CUDA device"}

@@ -22,6 +22,7 @@ constexpr int kStatusRank = 5;
 constexpr int kStatusInvalid = 1;
 constexpr unsigned int FKPC_FLAG_GUARDED_DEV = 1u;  // matches FKPC_FLAG_GUARDED
 constexpr unsigned int FKPC_FLAG_DIRECT_DEV = 2u;   // matches FKPC_FLAG_DIRECT
+constexpr int kFitFlagRankTruncated = 1;            // FitResult.flags: the rank rule dropped a coefficient
 
 // Warp-per-fit class of additive designs: q <= kWarpQ coefficients, at most
 // kWarpR stacked penalty rows and kWarpM penalties.

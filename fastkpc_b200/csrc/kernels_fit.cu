@@ -43,6 +43,21 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// The rank rule of magic's truncated SVD (mgcv; the reference's
+// rank_tolerance = sqrt(eps), fastkpc/src/cuda/mgcv_multi_penalty_gcv.hpp:230):
+// an augmented pivot |Ra(c, c)| at most kRankTol times the largest one marks
+// a direction in the null spaces of both X and the scaled penalties; its
+// coefficient is dropped (1 / Ra(c, c) taken as 0 in every triangular solve),
+// which leaves the fitted values and the influence trace of the truncated
+// solution.  The fit record's flags carry kFitRankTruncated then.
+constexpr double kRankTol = 1.4901161193847656e-8;
+constexpr int kFitRankTruncated = kFitFlagRankTruncated;
+
 // ----------------------------------------------------------------- single
 
 struct SingleObjective {
@@ -112,7 +127,8 @@ __device__ SingleObjective single_objective(double log_sp, double e, double z, b
 // j < m, NaN beyond, the first kCtaPenalties), so no kernel holds a whole
 // record in registers.
 __device__ __forceinline__ void store_result(FitResult* __restrict__ out, const double* log_sp, int m, double score,
-                                             double edf, double rss, int status, int iterations, int evaluations) {
+                                             double edf, double rss, int status, int iterations, int evaluations,
+                                             int flags = 0) {
   for (int j = 0; j < kCtaPenalties; ++j) out->log_sp[j] = j < m ? log_sp[j] : NAN;
   out->score = score;
   out->edf = edf;
@@ -120,7 +136,7 @@ __device__ __forceinline__ void store_result(FitResult* __restrict__ out, const 
   out->status = status;
   out->iterations = iterations;
   out->evaluations = evaluations;
-  out->flags = 0;
+  out->flags = flags;
 }
 
 __global__ void fit_single_kernel(const DesignDev* __restrict__ designs, const double* __restrict__ arena,
@@ -290,8 +306,7 @@ constexpr double kPolishCurvature = 1e-6;
 constexpr double kGnGradTol = 1e-9;   // Gauss-Newton selection: |grad V| <= 1e-9 (1 + V),
 constexpr double kGnFlatTol = 1e-12;  // or a decrease <= 1e-12 (1 + V)
 constexpr double kGnFlatGrad = 1e-6;  // with |grad V| <= 1e-6 (1 + V),
-constexpr double kGnStallStep = 1e-8;  // or an accepted step below 1e-8 in max norm
-constexpr double kGnStallTol = 1e-10;  // that decreased V by at most 1e-10 (1 + V): stalled
+constexpr double kGnStallTol = 1e-10;  // a decrease of V at most 1e-10 (1 + V): the direction has stalled
 constexpr double kGnMaxLogSp = 25.0;  // upper bound of the Gauss-Newton search in log(lambda)
 
 __device__ __forceinline__ int tri(int i, int j) { return j * (j + 1) / 2 + i; }  // packed upper, i <= j
@@ -326,6 +341,7 @@ struct MultiScalarsT {
   double beta[2], v0[2];
   double red[NT / 32];
   double score, rss, edf, rss0;  // rss0 = |y - Q Q'y|^2
+  int dropped;                   // coefficients the rank rule dropped at the last evaluation
   double lam[MP];
   double log_sp[MP];
   double trial[MP];
@@ -348,6 +364,20 @@ struct MultiScalarsT {
 };
 // the shared-memory classes (q <= 112, |S| <= 12)
 using MultiScalars = MultiScalarsT<kCtaPenalties, kMultiThreads, 128, 128>;
+
+template <class S>
+__device__ double block_max(double v, S* sc) {
+  v = warp_max(v);
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sc->red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+#pragma unroll
+  for (int w = 0; w < S::kThreads / 32; ++w) s = fmax(s, sc->red[w]);
+  return s;
+}
 
 template <class S>
 __device__ double block_sum(double v, S* sc) {
@@ -435,11 +465,22 @@ __device__ void multi_core(const D& des, const double* __restrict__ arena, int n
     }
     __syncthreads();
   }
-  // reciprocal diagonal once, so the triangular solves below multiply
+  // reciprocal diagonal once, so the triangular solves below multiply; the
+  // rank rule drops the coefficients of negligible pivots
+  double dmax = 0.0;
+  for (int c = tid; c < q; c += NT) dmax = fmax(dmax, fabs(Ra[tri(c, c)]));
+  dmax = block_max(dmax, sc);
+  double dropped = 0.0;
   for (int c = tid; c < q; c += NT) {
     const double dc = Ra[tri(c, c)];
-    if (dc == 0.0) sc->status = kStatusRank;
-    idg[c] = 1.0 / dc;
+    const bool keep = fabs(dc) > kRankTol * dmax;
+    idg[c] = keep ? 1.0 / dc : 0.0;
+    dropped += keep ? 0.0 : 1.0;
+  }
+  dropped = block_sum(dropped, sc);
+  if (tid == 0) {
+    sc->dropped = static_cast<int>(dropped);
+    if (!(dmax > 0.0)) sc->status = kStatusRank;
   }
   __syncthreads();
   // W = R Ra^-1: row i solves w Ra = R(i, :), w upper triangular
@@ -880,6 +921,21 @@ __device__ void gn_step(int m, S* sc) {
   }
 }
 
+// Projected steepest descent for a stalled Gauss-Newton search (one
+// thread): -g / max|g| over the coordinates that no outward push holds at
+// the bound log(lambda) <= kGnMaxLogSp, clipped to the bound.
+template <class S>
+__device__ void gn_steepest(int m, S* sc) {
+  double mg = 0.0;
+  for (int r = 0; r < m; ++r)
+    if (!(sc->log_sp[r] >= kGnMaxLogSp && sc->gradient[r] < 0.0)) mg = fmax(mg, fabs(sc->gradient[r]));
+  for (int r = 0; r < m; ++r) {
+    const bool held = sc->log_sp[r] >= kGnMaxLogSp && sc->gradient[r] < 0.0;
+    const double z = (mg == 0.0 || held) ? 0.0 : -sc->gradient[r] / mg;
+    sc->step[r] = fmin(z, kGnMaxLogSp - sc->log_sp[r]);
+  }
+}
+
 }  // namespace
 
 // Per-fit set-up shared by the fit and adjoint kernels: fill-in bounds, block
@@ -979,8 +1035,12 @@ __device__ void multi_fit_job(const D& des, const FitJob& job, int t, const doub
     // Newton on the Gauss-Newton Hessian, halving until V decreases
     if (tid < m) sc.gradient[tid] = sc.grad_c[tid];
     __syncthreads();
+    bool stalled = false;
     for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
-      if (tid == 0) gn_step(m, &sc);
+      if (tid == 0) {
+        if (stalled) gn_steepest(m, &sc);
+        else gn_step(m, &sc);
+      }
       __syncthreads();
       bool accepted = false;
       for (int tries = 1; tries <= max_half; ++tries) {
@@ -1011,17 +1071,21 @@ __device__ void multi_fit_job(const D& des, const FitJob& job, int t, const doub
       double g2 = 0.0;  // projected gradient: a coordinate on the upper bound that V pushes outwards counts 0
       for (int r = 0; r < m; ++r)
         if (!(sc.log_sp[r] >= kGnMaxLogSp && sc.gradient[r] < 0.0)) g2 += sc.gradient[r] * sc.gradient[r];
-      // a stationary point (not magic's loose stop), V no longer moving along
-      // directions that have gone flat (log lambda drifting upwards), or a
-      // line search that only finds negligible steps (the direction stalls)
-      double smax = 0.0;
-      for (int r = 0; r < m; ++r) smax = fmax(smax, fabs(sc.step[r]));
+      // a stationary point (not magic's loose stop), or V no longer moving
+      // along directions that have gone flat (log lambda drifting upwards)
       if (sqrt(g2) <= kGnGradTol * (1.0 + fabs(min_score)) ||
-          (score_red <= kGnFlatTol * (1.0 + min_score) && sqrt(g2) <= kGnFlatGrad * (1.0 + fabs(min_score))) ||
-          (smax <= kGnStallStep && score_red <= kGnStallTol * (1.0 + min_score))) {
+          (score_red <= kGnFlatTol * (1.0 + min_score) && sqrt(g2) <= kGnFlatGrad * (1.0 + fabs(min_score)))) {
         converged = true;
         break;
       }
+      // a decrease below kGnStallTol (1 + V): the next step is projected
+      // steepest descent; a second such decrease in a row ends the search
+      const bool tiny = score_red <= kGnStallTol * (1.0 + min_score);
+      if (tiny && stalled) {
+        converged = true;
+        break;
+      }
+      stalled = tiny;
     }
   } else {
     for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
@@ -1135,7 +1199,9 @@ __device__ void multi_fit_job(const D& des, const FitJob& job, int t, const doub
       for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * Wg[c];
     r[i] = ok ? y[i] - f : NAN;
   }
-  if (tid == 0) store_result(results + t, sc.log_sp, m, sc.score, sc.edf, sc.rss, sc.status, it, calls);
+  if (tid == 0)
+    store_result(results + t, sc.log_sp, m, sc.score, sc.edf, sc.rss, sc.status, it, calls,
+                 sc.dropped > 0 ? kFitRankTruncated : 0);
   if (all_log_sp)
     for (int j = tid; j < kMaxPenalties; j += NT) all_log_sp[j] = j < m ? sc.log_sp[j] : NAN;
 }
@@ -1236,6 +1302,7 @@ static_assert(kWarpTri % 2 == 0 && WarpLayout::Y % 2 == 0, "16-byte copies of th
 struct WarpScalars {
   static constexpr int kLd = kWarpM;  // leading dimension of the m x m matrices
   double beta, v0, score, rss, edf, rss0;  // rss0 = |y - Q Q'y|^2
+  int dropped;                              // coefficients the rank rule dropped at the last evaluation
   double lam[kWarpM];
   double log_sp[kWarpM];
   double trial[kWarpM];
@@ -1506,10 +1573,23 @@ __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, 
     }
     for (int k = qa > 0 ? qa : 0; k < q; ++k) warp_fold_step<false>(k, q, sc, X, pv, b0, b1, col0, 0);
   }
-  for (int c = lane; c < q; c += 32) {
-    const double d = X[packed_row(c, c)];
-    if (d == 0.0) sc.status = kStatusRank;
-    idg[c] = 1.0 / d;
+  {
+    // the rank rule drops the coefficients of negligible pivots
+    double dmax = 0.0;
+    for (int c = lane; c < q; c += 32) dmax = fmax(dmax, fabs(X[packed_row(c, c)]));
+    dmax = warp_max(dmax);
+    double dropped = 0.0;
+    for (int c = lane; c < q; c += 32) {
+      const double d = X[packed_row(c, c)];
+      const bool keep = fabs(d) > kRankTol * dmax;
+      idg[c] = keep ? 1.0 / d : 0.0;
+      dropped += keep ? 0.0 : 1.0;
+    }
+    dropped = warp_sum(dropped);
+    if (lane == 0) {
+      sc.dropped = static_cast<int>(dropped);
+      if (!(dmax > 0.0)) sc.status = kStatusRank;
+    }
   }
   // W = R Ra^-1: row i (lane i; rows 32.. on lanes 0..) solves w Ra = R(i, :).
   // Packed row i starts at Y + packed_row(i, 0), entry c >= i at offset c.
@@ -1863,8 +1943,12 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
     // Newton on the Gauss-Newton Hessian, halving until V decreases
     if (lane < m) sc.gradient[lane] = sc.grad_c[lane];
     __syncwarp();
+    bool stalled = false;
     for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
-      if (lane == 0) gn_step(m, &sc);
+      if (lane == 0) {
+        if (stalled) gn_steepest(m, &sc);
+        else gn_step(m, &sc);
+      }
       __syncwarp();
       bool accepted = false;
       for (int tries = 1; tries <= max_half; ++tries) {
@@ -1895,17 +1979,21 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
       double g2 = 0.0;  // projected gradient: a coordinate on the upper bound that V pushes outwards counts 0
       for (int r = 0; r < m; ++r)
         if (!(sc.log_sp[r] >= kGnMaxLogSp && sc.gradient[r] < 0.0)) g2 += sc.gradient[r] * sc.gradient[r];
-      // a stationary point (not magic's loose stop), V no longer moving along
-      // directions that have gone flat (log lambda drifting upwards), or a
-      // line search that only finds negligible steps (the direction stalls)
-      double smax = 0.0;
-      for (int r = 0; r < m; ++r) smax = fmax(smax, fabs(sc.step[r]));
+      // a stationary point (not magic's loose stop), or V no longer moving
+      // along directions that have gone flat (log lambda drifting upwards)
       if (sqrt(g2) <= kGnGradTol * (1.0 + fabs(min_score)) ||
-          (score_red <= kGnFlatTol * (1.0 + min_score) && sqrt(g2) <= kGnFlatGrad * (1.0 + fabs(min_score))) ||
-          (smax <= kGnStallStep && score_red <= kGnStallTol * (1.0 + min_score))) {
+          (score_red <= kGnFlatTol * (1.0 + min_score) && sqrt(g2) <= kGnFlatGrad * (1.0 + fabs(min_score)))) {
         converged = true;
         break;
       }
+      // a decrease below kGnStallTol (1 + V): the next step is projected
+      // steepest descent; a second such decrease in a row ends the search
+      const bool tiny = score_red <= kGnStallTol * (1.0 + min_score);
+      if (tiny && stalled) {
+        converged = true;
+        break;
+      }
+      stalled = tiny;
     }
   } else {
     for (it = 1; it <= kMaxIterations && sc.status == kStatusOk; ++it) {
@@ -2041,7 +2129,9 @@ __global__ void __launch_bounds__(32) fit_multi_warp_kernel(const DesignDev* __r
       for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * wg[c];
     r[i] = ok ? y[i] - f : NAN;
   }
-  if (lane == 0) store_result(results + t, sc.log_sp, m, sc.score, sc.edf, sc.rss, sc.status, it, calls);
+  if (lane == 0)
+    store_result(results + t, sc.log_sp, m, sc.score, sc.edf, sc.rss, sc.status, it, calls,
+                 sc.dropped > 0 ? kFitRankTruncated : 0);
 }
 
 // ------------------------------------------------------ speculative continuation
@@ -2338,7 +2428,9 @@ __global__ void __launch_bounds__(32 * kSpecWarps) fit_multi_spec_kernel(
           for (int c = 0; c < q; ++c) f += Q[i + static_cast<int64_t>(n) * c] * wg[c];
         r[i] = ok ? y[i] - f : NAN;
       }
-      if (lane == 0) store_result(results + t, sc.log_sp, m, sc.score, sc.edf, sc.rss, status, it, calls);
+      if (lane == 0)
+        store_result(results + t, sc.log_sp, m, sc.score, sc.edf, sc.rss, status, it, calls,
+                     sc.dropped > 0 ? kFitRankTruncated : 0);
     }
     __syncthreads();
   }

@@ -17,7 +17,9 @@
 // One CTA per design (grid-stride).  Reflector k: a block reduction for the
 // column norm, then warp per trailing column (dot product and update over the
 // rows, coalesced).  The working set (n x q doubles, ~150 KB at n = 500) stays
-// in L2.  A zero column norm marks the design rank deficient in status[d].
+// in L2.  A zero column norm leaves R(k, k) = 0 (an identity reflector, Q
+// still orthonormal); the fits' rank rule drops that direction, so status[d]
+// stays 0.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -176,7 +178,10 @@ __global__ void __launch_bounds__(kGeomThreads) additive_geometry_kernel(int n, 
         if (t <= c) rp[packed_row(t, c)] = R[idx];
       }
     }
-    if (tid == 0) status[d] = deficient ? 1 : 0;
+    // a zero column (R(k, k) = 0, an identity reflector) is left to the fits,
+    // whose rank rule drops the direction it leaves in the augmented system
+    (void)deficient;
+    if (tid == 0) status[d] = 0;
     __syncthreads();
   }
 }

@@ -1433,6 +1433,12 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
   }
   double download_ms = ms_since(t0);
   if (out) {
+    // a test whose residual came from a rank-truncated fit says so
+    std::vector<char> truncated(comps_.size(), 0);
+    for (size_t i = 0; i < sres.size(); ++i)
+      if (sres[i].flags & kFitFlagRankTruncated) truncated[single_jobs_[i].out] = 1;
+    for (size_t i = 0; i < mres.size(); ++i)
+      if (mres[i].flags & kFitFlagRankTruncated) truncated[multi_jobs_[i].out] = 1;
     for (size_t t = 0; t < recs.size(); ++t) {
       const RecordDev& r = recs[t];
       fkpc_ci_record& o = out[t];
@@ -1443,6 +1449,8 @@ void Engine::collect(fkpc_ci_record* out, fkpc_stage_stats* stats) {
       o.variance = r.variance;
       o.status = r.status;
       o.flags = r.flags | (tests_[t].S.empty() ? FKPC_FLAG_DIRECT : 0u);
+      if (t < pairs_.size() && (truncated[pairs_[t].left] || truncated[pairs_[t].right]))
+        o.flags |= FKPC_FLAG_RANK_TRUNCATED;
       if (r.status != kStatusOk)
         throw Error(r.status == kStatusNotConverged ? FKPC_STATUS_NOT_CONVERGED : FKPC_STATUS_NUMERIC,
                     "statistic of test " + std::to_string(t) + " failed with status " + std::to_string(r.status));

@@ -53,6 +53,7 @@ extern "C" {
 /* per-record flags */
 #define FKPC_FLAG_GUARDED 1u       /* dcc.gamma p came from the low-rank refinement */
 #define FKPC_FLAG_DIRECT 2u        /* |S| = 0: raw columns, no regression */
+#define FKPC_FLAG_RANK_TRUNCATED 4u /* a residual fit dropped a coefficient by magic's rank rule (sqrt(eps)) */
 
 typedef struct fkpc_options {
   double alpha;                 /* significance level; the reference fixes 0.1 */

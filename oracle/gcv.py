@@ -561,8 +561,7 @@ def gcv_residual_vector(prep, y, log_sp):
 
 GN_GRAD_TOL = 1e-9
 GN_FLAT_TOL = 1e-12
-GN_STALL_STEP = 1e-8   # an accepted step below this in max norm ...
-GN_STALL_TOL = 1e-10   # ... that decreased V by at most this (1 + V): the direction has stalled
+GN_STALL_TOL = 1e-10   # a decrease of V at most this (1 + V): the direction has stalled
 GN_FLAT_GRAD = 1e-6
 GN_MAX_LOG_SP = 25.0
 
@@ -615,14 +614,26 @@ def newton_gn_step(hess, gn, grad, rho):
     return np.minimum(z, GN_MAX_LOG_SP - rho)
 
 
+def steepest_gn_step(grad, rho):
+    """Projected steepest descent for a stalled Gauss-Newton search: -g /
+    max|g| over the coordinates that no outward push holds at the bound
+    rho <= GN_MAX_LOG_SP, clipped to the bound."""
+    free = ~((rho >= GN_MAX_LOG_SP) & (grad < 0.0))
+    g = np.where(free, grad, 0.0)
+    mg = float(np.max(np.abs(g)))
+    z = np.zeros(len(g)) if mg == 0.0 else -g / mg
+    return np.minimum(z, GN_MAX_LOG_SP - rho)
+
+
 def optimize_gn(prep, y, max_half=25, max_iter=400, trace=None):
     """Newton selection driven by the adjoint (the library's
     FKPC_SELECT_GN_NEWTON): from magic's start, exact-Hessian Newton where that
     Hessian is positive definite and damped Gauss-Newton elsewhere, halving
-    until V decreases; stop at |grad V| <= GN_GRAD_TOL (1 + V), when no
-    decrease is possible, or when the line search only finds steps below
-    GN_STALL_STEP that decrease V by at most GN_STALL_TOL (1 + V), with
-    log(lambda) kept <= GN_MAX_LOG_SP; then the
+    until V decreases; after a decrease of at most GN_STALL_TOL (1 + V) the
+    next step is projected steepest descent (steepest_gn_step); stop at
+    |grad V| <= GN_GRAD_TOL (1 + V), when no decrease is possible, or after
+    two such small decreases in a row, with log(lambda) kept <=
+    GN_MAX_LOG_SP; then the
     terminal polish (no boundary probes)."""
     resp = prep.response(y)
     m = prep.m
@@ -633,8 +644,9 @@ def optimize_gn(prep, y, max_half=25, max_iter=400, trace=None):
     calls = 1
     converged = False
     it = 0
+    stalled = False
     for it in range(1, max_iter + 1):
-        step = newton_gn_step(H, gn, g, rho)
+        step = steepest_gn_step(g, rho) if stalled else newton_gn_step(H, gn, g, rho)
         accepted = None
         for _ in range(max_half):
             trial = rho + step
@@ -655,10 +667,16 @@ def optimize_gn(prep, y, max_half=25, max_iter=400, trace=None):
         gn = gcv_gauss_newton(prep, y, rho)
         gnorm = np.linalg.norm(np.where((rho >= GN_MAX_LOG_SP) & (g < 0.0), 0.0, g))  # projected gradient
         if (gnorm <= GN_GRAD_TOL * (1.0 + abs(core["score"]))
-                or (red <= GN_FLAT_TOL * (1.0 + core["score"]) and gnorm <= GN_FLAT_GRAD * (1.0 + abs(core["score"])))
-                or (np.max(np.abs(step)) <= GN_STALL_STEP and red <= GN_STALL_TOL * (1.0 + core["score"]))):
+                or (red <= GN_FLAT_TOL * (1.0 + core["score"]) and gnorm <= GN_FLAT_GRAD * (1.0 + abs(core["score"])))):
             converged = True
             break
+        # a decrease below GN_STALL_TOL (1 + V): the next step is projected
+        # steepest descent; a second such decrease in a row ends the search
+        tiny = red <= GN_STALL_TOL * (1.0 + core["score"])
+        if tiny and stalled:
+            converged = True
+            break
+        stalled = tiny
     if not converged:
         raise ValueError("Gauss-Newton selection hit its iteration limit")
     rho, core, extra = polish_newton(prep, resp, rho, core)

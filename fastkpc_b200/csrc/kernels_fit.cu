@@ -306,7 +306,7 @@ constexpr double kPolishCurvature = 1e-6;
 constexpr double kGnGradTol = 1e-9;   // Gauss-Newton selection: |grad V| <= 1e-9 (1 + V),
 constexpr double kGnFlatTol = 1e-12;  // or a decrease <= 1e-12 (1 + V)
 constexpr double kGnFlatGrad = 1e-6;  // with |grad V| <= 1e-6 (1 + V),
-constexpr double kGnStallTol = 1e-10;  // a decrease of V at most 1e-10 (1 + V): the direction has stalled
+constexpr double kGnStallTol = 1e-9;   // a decrease of V at most 1e-9 (1 + V): the direction has stalled
 constexpr double kGnMaxLogSp = 25.0;  // upper bound of the Gauss-Newton search in log(lambda)
 
 __device__ __forceinline__ int tri(int i, int j) { return j * (j + 1) / 2 + i; }  // packed upper, i <= j
@@ -1302,6 +1302,7 @@ static_assert(kWarpTri % 2 == 0 && WarpLayout::Y % 2 == 0, "16-byte copies of th
 struct WarpScalars {
   static constexpr int kLd = kWarpM;  // leading dimension of the m x m matrices
   double beta, v0, score, rss, edf, rss0;  // rss0 = |y - Q Q'y|^2
+  double dmax;                              // largest pivot of the current fold
   int dropped;                              // coefficients the rank rule dropped at the last evaluation
   double lam[kWarpM];
   double log_sp[kWarpM];
@@ -1458,14 +1459,16 @@ __device__ __forceinline__ void warp_fold_step(int k, int q, WarpScalars& sc, do
     const double sg = (s0 + s1) + (s2 + s3);
     const int kk = packed_row(k, k);
     const double akk = X[kk];
-    double beta = 0.0, v0 = 0.0;
+    double beta = 0.0, v0 = 0.0, piv = fabs(akk);
     if (sg != 0.0) {
       const double nrm = sqrt(akk * akk + sg);
       const double alpha = akk >= 0.0 ? -nrm : nrm;
       v0 = akk - alpha;
       beta = 2.0 / (v0 * v0 + sg);
       X[kk] = alpha;
+      piv = nrm;
     }
+    sc.dmax = fmax(sc.dmax, piv);  // the largest pivot so far, for the rank rule
     sc.beta = beta;
     sc.v0 = v0;
   }
@@ -1558,6 +1561,7 @@ __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, 
     cp_async_commit();
     cp_async_wait<1>();
   }
+  if (lane == 0) sc.dmax = 0.0;
   __syncwarp();
   {
     double b0[kWarpR], b1[kWarpR];
@@ -1574,21 +1578,23 @@ __device__ __noinline__ void warp_core(const double* __restrict__ arena, int n, 
     for (int k = qa > 0 ? qa : 0; k < q; ++k) warp_fold_step<false>(k, q, sc, X, pv, b0, b1, col0, 0);
   }
   {
-    // the rank rule drops the coefficients of negligible pivots
-    double dmax = 0.0;
-    for (int c = lane; c < q; c += 32) dmax = fmax(dmax, fabs(X[packed_row(c, c)]));
-    dmax = warp_max(dmax);
-    double dropped = 0.0;
-    for (int c = lane; c < q; c += 32) {
-      const double d = X[packed_row(c, c)];
-      const bool keep = fabs(d) > kRankTol * dmax;
-      idg[c] = keep ? 1.0 / d : 0.0;
-      dropped += keep ? 0.0 : 1.0;
+    // the rank rule drops the coefficients of negligible pivots (the fold
+    // kept the largest pivot in sc.dmax)
+    const double tol = kRankTol * sc.dmax;
+    int dropped = 0;
+    for (int c0 = 0; c0 < q; c0 += 32) {
+      const int c = c0 + lane;
+      bool drop = false;
+      if (c < q) {
+        const double d = X[packed_row(c, c)];
+        drop = !(fabs(d) > tol);
+        idg[c] = drop ? 0.0 : 1.0 / d;
+      }
+      dropped += __popc(__ballot_sync(0xffffffffu, drop));
     }
-    dropped = warp_sum(dropped);
     if (lane == 0) {
-      sc.dropped = static_cast<int>(dropped);
-      if (!(dmax > 0.0)) sc.status = kStatusRank;
+      sc.dropped = dropped;
+      if (!(sc.dmax > 0.0)) sc.status = kStatusRank;
     }
   }
   // W = R Ra^-1: row i (lane i; rows 32.. on lanes 0..) solves w Ra = R(i, :).

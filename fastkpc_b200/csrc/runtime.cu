@@ -550,6 +550,9 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
   // designs with more than kCtaPenalties blocks: their full descriptors,
   // copied into the host range of the arena at ``ext``
   std::vector<std::pair<size_t, WideDesign>> wide_desc;
+  // penalty roots in the host range, one per distinct root vector
+  std::map<const std::vector<double>*, int64_t> root_slot;
+  std::vector<std::pair<const std::vector<double>*, int64_t>> root_copies;
   for (size_t d = 0; d < designs_.size(); ++d) {
     DesignDev& dd = ddesc[d];
     std::memset(&dd, 0, sizeof(dd));
@@ -598,22 +601,33 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
       at += static_cast<size_t>(n) * des.q;
       dd.rmat = static_cast<int64_t>(at);
       at += static_cast<size_t>(des.q) * des.q;
-      dd.roots = static_cast<int64_t>(total);
+      // the roots: one copy per univariate smooth, shared by every design
+      // that contains the variable (absolute offsets, roots = 0); a block
+      // whose root is not its smooth's own gets a copy of its own
+      dd.roots = 0;
       if (des.m > kMaxPenalties)
         throw Error(FKPC_STATUS_INVALID_ARGUMENT, "additive design exceeds the kernel capacity (q <= 560, |S| <= 62)");
       WideDesign wd;
       std::memset(&wd, 0, sizeof(wd));
       int rows = 0;
-      int64_t rootoff = 0;
       for (int j = 0; j < des.m; ++j) {
+        const Smooth* part = j < static_cast<int>(des.parts.size()) ? des.parts[j].get() : nullptr;
+        const std::vector<double>* src = &des.roots[j];
+        if (part && part->root == des.roots[j]) src = &part->root;
+        auto it = root_slot.find(src);
+        if (it == root_slot.end()) {
+          it = root_slot.emplace(src, static_cast<int64_t>(total)).first;
+          root_copies.push_back({src, static_cast<int64_t>(total)});
+          total += src->size();
+        }
+        if (it->second > INT32_MAX) throw Error(FKPC_STATUS_ALLOCATION, "penalty roots beyond the arena's int32 offsets");
         wd.off[j] = des.offsets[j];
         wd.dim[j] = des.dims[j];
         wd.rank[j] = des.ranks[j];
         wd.rowoff[j] = rows;
-        wd.rootoff[j] = static_cast<int>(rootoff);
+        wd.rootoff[j] = static_cast<int>(it->second);
         wd.log_sp0[j] = des.initial_log_sp[j];
         rows += des.ranks[j];
-        rootoff += static_cast<int64_t>(des.roots[j].size());
       }
       for (int j = 0; j < des.m && j < kCtaPenalties; ++j) {
         dd.off[j] = wd.off[j];
@@ -623,7 +637,6 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
         dd.rootoff[j] = wd.rootoff[j];
         dd.log_sp0[j] = wd.log_sp0[j];
       }
-      total += static_cast<size_t>(rootoff);
       dd.rsum = rows;
       if (des.m > kCtaPenalties) {
         dd.ext = static_cast<int64_t>(total);
@@ -680,6 +693,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
   // buffer (threads over designs), then one DMA to the device arena.
   double* host = pinned_arena(total);
   for (const auto& [d, wd] : wide_desc) std::memcpy(host + ddesc[d].ext, &wd, sizeof(WideDesign));
+  for (const auto& [src, at] : root_copies) std::memcpy(host + at, src->data(), src->size() * sizeof(double));
   {
     std::atomic<size_t> next(0);
     auto work = [&]() {
@@ -701,12 +715,7 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
           std::memcpy(host + dd.basis, des.QW.data(), des.QW.size() * sizeof(double));
           std::memcpy(host + dd.spec, des.spec.data(), des.spec.size() * sizeof(double));
         } else {
-          size_t rootoff = 0;  // the blocks' roots are consecutive (rootoff of the descriptors)
-          for (int j = 0; j < des.m; ++j) {
-            std::memcpy(host + dd.roots + rootoff, des.roots[j].data(), des.roots[j].size() * sizeof(double));
-            rootoff += des.roots[j].size();
-          }
-          if (des.device_geometry) continue;
+          if (des.device_geometry) continue;  // its roots are the shared copies above
           std::memcpy(host + dd.basis, des.Q.data(), des.Q.size() * sizeof(double));
           std::memcpy(host + dd.rmat, des.R.data(), des.R.size() * sizeof(double));
           if (dd.rpack >= 0) {

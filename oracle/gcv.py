@@ -561,7 +561,7 @@ def gcv_residual_vector(prep, y, log_sp):
 
 GN_GRAD_TOL = 1e-9
 GN_FLAT_TOL = 1e-12
-GN_STALL_TOL = 1e-10   # a decrease of V at most this (1 + V): the direction has stalled
+GN_STALL_TOL = 1e-9    # a decrease of V at most this (1 + V): the direction has stalled
 GN_FLAT_GRAD = 1e-6
 GN_MAX_LOG_SP = 25.0
 

@@ -55,7 +55,7 @@ WORKLOAD = "level batch n=500 p=50 SEM edge 0.08, 4096 triples |S|~U{0..4}, dcc.
 # speculative continuation -- on this workload (seed 2, 4096 triples), from one
 # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum); ncu cannot run
 # inside the timed region.
-FIT_STAGE_TRAFFIC = {"bytes": 442.9e6, "source": "profiles/fit_stage_traffic_500x50.txt"}
+FIT_STAGE_TRAFFIC = {"bytes": 419.2e6, "source": "profiles/fit_stage_traffic_500x50.txt"}
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 

@@ -40,7 +40,9 @@ class RStream {
 
   int unif_index(int dn) {
     if (dn <= 0) return 0;
-    const int bits = static_cast<int>(std::ceil(std::log2(static_cast<double>(dn))));
+    // ceil(log2(dn)) as R computes it in double, exact for every int dn >= 1:
+    // the bit length of dn - 1
+    const int bits = dn == 1 ? 0 : 32 - __builtin_clz(static_cast<unsigned>(dn - 1));
     for (;;) {
       int64_t v = 0;
       for (int k = 0; k <= bits; k += 16) v = 65536 * v + static_cast<int64_t>(std::floor(unif_rand() * 65536.0));
@@ -51,34 +53,71 @@ class RStream {
 
   // replicates x n table for one dcc.perm test
   void dcc_permutations(int n, int replicates, int* out) {
-    perm_.resize(n);
-    for (int i = 0; i < n; ++i) perm_[i] = i;
+    dcc_swaps(n, replicates, out);
+    dcc_assemble(n, replicates, out, &perm_);
+  }
+
+  // replicates x n table for one hsic.perm test
+  void hsic_permutations(int n, int replicates, int* out) {
+    hsic_draws(n, replicates, out);
+    hsic_assemble(n, replicates, out, &pool_);
+  }
+
+  // The two tables in two passes: the stream's part (the draws, in stream
+  // order, into the table's rows) and the part that uses no stream (turning
+  // a row's draws into its permutation), which may run for many tests at
+  // once.  dcc.perm: swap k of a replicate takes j = floor(u (n - k)) and
+  // exchanges entries j and n - 1 - k of one vector carried from replicate
+  // to replicate; hsic.perm: draw i takes R_unif_index(n - i) from a pool
+  // that each replicate starts afresh.
+  void dcc_swaps(int n, int replicates, int* out) {
     for (int r = 0; r < replicates; ++r) {
+      int* row = out + static_cast<int64_t>(r) * n;
       int remaining = n;
       for (int k = 0; k < n - 1; ++k) {
         int j = static_cast<int>(std::floor(unif_rand() * remaining));
         if (j < 0) j = 0;
         if (j >= remaining) j = remaining - 1;
         --remaining;
-        const int t = perm_[j];
-        perm_[j] = perm_[remaining];
-        perm_[remaining] = t;
+        row[k] = j;
       }
-      for (int i = 0; i < n; ++i) out[static_cast<int64_t>(r) * n + i] = perm_[i];
     }
   }
-
-  // replicates x n table for one hsic.perm test
-  void hsic_permutations(int n, int replicates, int* out) {
-    pool_.resize(n);
+  static void dcc_assemble(int n, int replicates, int* out, std::vector<int>* scratch) {
+    std::vector<int>& perm = *scratch;
+    perm.resize(n);
+    for (int i = 0; i < n; ++i) perm[i] = i;
     for (int r = 0; r < replicates; ++r) {
-      for (int i = 0; i < n; ++i) pool_[i] = i;
+      int* row = out + static_cast<int64_t>(r) * n;
+      int remaining = n;
+      for (int k = 0; k < n - 1; ++k) {
+        const int j = row[k];
+        --remaining;
+        const int t = perm[j];
+        perm[j] = perm[remaining];
+        perm[remaining] = t;
+      }
+      for (int i = 0; i < n; ++i) row[i] = perm[i];
+    }
+  }
+  void hsic_draws(int n, int replicates, int* out) {
+    for (int r = 0; r < replicates; ++r) {
+      int* row = out + static_cast<int64_t>(r) * n;
+      for (int i = 0; i < n; ++i) row[i] = unif_index(n - i);
+    }
+  }
+  static void hsic_assemble(int n, int replicates, int* out, std::vector<int>* scratch) {
+    std::vector<int>& pool = *scratch;
+    pool.resize(n);
+    for (int r = 0; r < replicates; ++r) {
+      int* row = out + static_cast<int64_t>(r) * n;
+      for (int i = 0; i < n; ++i) pool[i] = i;
       int remaining = n;
       for (int i = 0; i < n; ++i) {
-        const int j = unif_index(remaining);
-        out[static_cast<int64_t>(r) * n + i] = pool_[j];
+        const int j = row[i];
+        row[i] = pool[j];
         --remaining;
-        pool_[j] = pool_[remaining];
+        pool[j] = pool[remaining];
       }
     }
   }

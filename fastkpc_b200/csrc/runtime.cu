@@ -934,12 +934,20 @@ void Engine::pack_and_upload(const fkpc_options& opt, RStream* rstream, bool def
       if (!rstream) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "permutation methods require a seeded stream");
       const int R = opt.permutation_replicates;
       std::vector<int> perms(npairs * static_cast<size_t>(R) * n);
+      // the stream's draws test after test (sequential: one seeded stream),
+      // then every test's table from its draws on the host threads
       for (size_t t = 0; t < npairs; ++t) {
         int* dst = perms.data() + t * static_cast<size_t>(R) * n;
-        if (method == FKPC_DCC_PERM) rstream->dcc_permutations(n, R, dst);
-        else rstream->hsic_permutations(n, R, dst);
+        if (method == FKPC_DCC_PERM) rstream->dcc_swaps(n, R, dst);
+        else rstream->hsic_draws(n, R, dst);
         if (stream_snapshots_) stream_snapshots_->push_back(*rstream);
       }
+      parallel_for(npairs, [&](size_t t) {
+        thread_local std::vector<int> scratch;
+        int* dst = perms.data() + t * static_cast<size_t>(R) * n;
+        if (method == FKPC_DCC_PERM) RStream::dcc_assemble(n, R, dst, &scratch);
+        else RStream::hsic_assemble(n, R, dst, &scratch);
+      });
       h2d_bytes_ += upload(d_perms_, perms, stream_);
     }
   }

@@ -2,7 +2,7 @@
 
 The oracle's records and residual summaries come from the committed fixture
 ``tests/golden/level500x50_oracle.npz`` (``make_level_fixture.py``).  Every
-call goes through the C ABI.  Bars:
+call goes through the C ABI.  Bars (the tolerances of the CI path):
 
 * residuals within 1e-10 relative (max-abs error over max |r|) on the 301
   fits stored in full; on all 6005 fits |(r - r_o) . z| <= 1e-10 |r_o| |z|

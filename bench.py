@@ -228,6 +228,10 @@ def skeleton_rows(device, cores, pool):
                     walls[graph].append(time.perf_counter() - t0)
             out, gout = outs[False], outs[True]
             wall, graph_wall = min(walls[False]), min(walls[True])
+            # the WAN-PDAG orientation that follows (regrVonPS residuals and tests on the device)
+            t0 = time.perf_counter()
+            orient = fk.orient_wanpdag(out, X, alpha=0.1, numCol=35, ci_method=method, device=device)
+            orient_wall = time.perf_counter() - t0
             if gout["n_edgetests"] != out["n_edgetests"] or not np.array_equal(gout["adjacency"], out["adjacency"]):
                 raise RuntimeError("the level-graph skeleton differs from the one-shot one")
             tasks = out["tasks"]
@@ -249,6 +253,11 @@ def skeleton_rows(device, cores, pool):
                          "edges": int(out["adjacency"].sum() // 2),
                          "device_ms": out["summary"]["stages"]["device_ms"],
                          "setup_ms": out["summary"]["stages"]["setup_ms"],
+                         "orientation": {"wall_s": orient_wall,
+                                         "ci_tests": orient["diagnostics"]["ci_test_count"],
+                                         "regrvonps_calls": orient["diagnostics"]["regrvonps_calls"],
+                                         "directed": int(np.sum((orient["pdag"] == 1) & (orient["pdag"].T == 0))),
+                                         "undirected": int(np.sum((orient["pdag"] == 1) & (orient["pdag"].T == 1)) // 2)},
                          "cpu_estimate_s": est, "cpu_cores": cores,
                          "cpu_sample": f"oracle on {sampled} logical tests spread over every level "
                                        f"({2 * cores} per level at most) in {cores} processes; each level's "

@@ -155,6 +155,8 @@ _SIGNATURES = {
     "fkpc_gcv_adjoint": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, ctypes.c_int, _INT, ctypes.c_int,
                                         ctypes.c_int, _DBL, _DBL, _DBL, _DBL, _DBL, ctypes.c_int]),
     "fkpc_gamma_q_eval": (ctypes.c_int, [ctypes.c_int, _DBL, _DBL, ctypes.c_int, _DBL, _INT]),
+    "fkpc_permutation_tables": (ctypes.c_int, [ctypes.c_uint, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               _INT]),
     "fkpc_get_tuning": (ctypes.c_int, [ctypes.c_int, _P(Tuning)]),
     "fkpc_set_tuning": (ctypes.c_int, [ctypes.c_int, _P(Tuning)]),
     "fkpc_batch_prepare": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, _INT, ctypes.c_int,
@@ -666,6 +668,16 @@ def regress_batch(data, fits, max_penalties=None, device=0, selection="magic"):
                                                _ptr(lsp, ctypes.c_double), max_penalties,
                                                _ptr(status, ctypes.c_int)))
     return resid, lsp, status
+
+
+def permutation_tables(seed, ci_method, n, replicates, count):
+    """The R-compatible permutation tables of ``count`` consecutive tests
+    (count x replicates x n int32) for dcc.perm or hsic.perm, as the batch
+    entry points draw them after set.seed(seed); ``stat_batch`` takes them."""
+    out = np.zeros((count, replicates, n), dtype=np.int32)
+    _check(load_library().fkpc_permutation_tables(int(seed) & 0xFFFFFFFF, METHODS[ci_method], int(n),
+                                                   int(replicates), int(count), _ptr(out, ctypes.c_int)))
+    return out
 
 
 def stat_batch(residuals, pairs, ci_method="dcc.gamma", permutations=None, **kw):

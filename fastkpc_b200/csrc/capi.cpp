@@ -752,6 +752,22 @@ int fkpc_ci_plain_one(const double* data, int n, int p, int x, int y, const int*
   });
 }
 
+int fkpc_permutation_tables(unsigned int seed, int ci_method, int n, int replicates, int count, int* out) {
+  return guarded([&]() {
+    using fkpc::Error;
+    if (!out && count > 0) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    if (ci_method != FKPC_DCC_PERM && ci_method != FKPC_HSIC_PERM)
+      throw Error(FKPC_STATUS_INVALID_ARGUMENT, "permutation tables exist for dcc.perm and hsic.perm");
+    if (n < 2 || replicates < 1 || count < 0) throw Error(FKPC_STATUS_INVALID_ARGUMENT, "need n >= 2, replicates >= 1");
+    fkpc::RStream rs(seed);
+    const size_t per = static_cast<size_t>(replicates) * n;
+    for (int t = 0; t < count; ++t) {
+      if (ci_method == FKPC_DCC_PERM) rs.dcc_permutations(n, replicates, out + per * t);
+      else rs.hsic_permutations(n, replicates, out + per * t);
+    }
+  });
+}
+
 int fkpc_regress_batch(const double* data, int n, int p, const int* target, const int* s_offsets,
                        const int* s_values, int count, const fkpc_options* options, double* residuals,
                        double* log_sp, int max_penalties, int* status) {

@@ -324,6 +324,17 @@ FKPC_API int fkpc_stat_batch(const double* residuals, int n, int m, const int* l
                     const fkpc_options* options, fkpc_ci_record* out);
 
 /*
+ * Permutation tables of ``count`` consecutive tests in the R-compatible
+ * stream of set.seed(seed) (RNGkind Mersenne-Twister, sample.kind
+ * "Rejection"): out is count x replicates x n int32, test after test in
+ * stream order -- dcc.perm: energy's dCOVtest swaps (one vector carried
+ * across a test's replicates); hsic.perm: sample(n) per replicate.  The
+ * tables fkpc_stat_batch's permutation methods take; no device work.
+ * Replaces the host table builder of fastkpc/src/full_cuda_ci_one_call.cpp:464-567.
+ */
+FKPC_API int fkpc_permutation_tables(unsigned int seed, int ci_method, int n, int replicates, int count, int* out);
+
+/*
  * GCV score, gradient and Gauss-Newton Hessian in rho = log(lambda) of the
  * additive-smooth fit of data[:, target] on S (|S| >= 3, m = |S|) at
  * ``count`` given points, plus the exact Hessian for comparison, on CUDA

@@ -85,3 +85,21 @@ def test_host_lanczos_restarts_on_near_duplicate_locations(lib_built):
     assert d["q"] == 10 and np.all(np.isfinite(d["X"]))
     d2 = fk.design_export(X, [43, 7])
     assert d2["q"] == 30 and np.all(np.isfinite(d2["X"]))
+
+
+@pytest.mark.parametrize("method", ["dcc.perm", "hsic.perm"])
+def test_permutation_tables_are_the_oracle_stream(lib_built, method):
+    """The library's R stream draws the oracle's tables test after test
+    (fastkpc/src/full_cuda_ci_one_call.cpp:464-567), including sizes whose
+    R_unif_index bit count changes (n = 2, 33, 64, 65)."""
+    from oracle import rng
+    draw = rng.dcc_permutations if method == "dcc.perm" else rng.hsic_permutations
+    for seed, n, reps, count in [(537, 37, 19, 5), (1, 2, 4, 3), (2024, 33, 7, 2), (9, 64, 3, 2), (9, 65, 3, 2)]:
+        got = fk.permutation_tables(seed, method, n, reps, count)
+        s = rng.RStream(seed)
+        want = np.array([draw(s, n, reps) for _ in range(count)])
+        assert np.array_equal(got, want), (seed, n)
+    with pytest.raises(fk.FkpcError):
+        fk.permutation_tables(1, "dcc.gamma", 10, 2, 1)
+    with pytest.raises(fk.FkpcError):
+        fk.permutation_tables(1, method, 1, 2, 1)

@@ -142,13 +142,33 @@ constexpr int kTprsUniK = 10;      // the basis dimension k of the univariate sm
 constexpr int kTprsMaxNu = 1536;  // unique locations a design may have on the device path
 // eta-matrix workspace per CTA: the leading dimension rounded up to the 32-row tile
 FKPC_HD constexpr int64_t tprs_ld(int nu) { return (static_cast<int64_t>(nu) + 31) / 32 * 32; }
-// Ritz pairs of the Lanczos runs: alpha / beta / done as written by the
-// Lanczos kernel; vals: count x k; zsel:
-// count x k x steps; ok[d] = 1 when design d's k pairs converged; U: design
-// d's nu x k Ritz vectors at U + uoff[d].  k is kTprsRitzMax or kTprsUniK.
-cudaError_t launch_tprs_ritz(const double* alpha, const double* beta, const int* done, int count, int steps, int k,
-                             double* vals, double* zsel, int* ok, const double* V, const int64_t* voff,
-                             const int* nus, double* U, const int64_t* uoff, cudaStream_t stream);
+// Block Lanczos for bivariate designs with kTprsBlockMinNu <= nu and
+// tprs_ld(nu) <= kTprsBlockMaxLd: blocks of kTprsBlock vectors, a Krylov space
+// of kTprsBlockDim in kTprsBlockSteps passes over the eta matrix.
+constexpr int kTprsBlock = 4;
+constexpr int kTprsBlockSteps = 26;
+constexpr int kTprsBlockDim = kTprsBlock * kTprsBlockSteps;
+constexpr int kTprsBlockMaxLd = 512;
+constexpr int kTprsBlockMinNu = kTprsBlockDim + 16;
+// V: design d's nu x kTprsBlockDim basis at V + voff[d]; blocks: count x
+// kTprsBlockSteps x 32 (A_s, R_s); done[d] = kTprsBlockDim, or -1 when a block
+// lost a direction (the host builds that design).  ews: ctas x ews_stride.
+cudaError_t launch_tprs_block_lanczos(const double* u, const int64_t* uoff, const int* nus, int count, int nu_max,
+                                      double eta0, double* ews, int64_t ews_stride, int ctas, double* V,
+                                      const int64_t* voff, double* blocks, int* done, cudaStream_t stream);
+// Ritz pairs: vals (count x k); zsel (count x k x zstride: the selected
+// eigenvectors in the Lanczos basis); ok[d] = 1 when design d's k pairs
+// converged.  The select launches take the tridiagonal runs (alpha / beta /
+// done of the single-vector kernel, stride steps) or the block runs; the
+// vectors launch forms design d's nu x k Ritz vectors at U + uoff[d] for every
+// accepted design.  k is kTprsRitzMax or kTprsUniK (block runs: kTprsRitzMax).
+cudaError_t launch_tprs_ritz_select(const double* alpha, const double* beta, const int* done, int count, int steps,
+                                    int k, int zstride, double* vals, double* zsel, int* ok, cudaStream_t stream);
+cudaError_t launch_tprs_ritz_block_select(const double* blocks, const int* done, int count, int k, int zstride,
+                                          double* vals, double* zsel, int* ok, cudaStream_t stream);
+cudaError_t launch_tprs_ritz_vectors(const double* V, const int64_t* voff, const int* nus, const int* done,
+                                     const int* ok, const double* zsel, int count, int zstride, int k, double* U,
+                                     const int64_t* uoff, cudaStream_t stream);
 // The thin-plate basis from its Ritz pairs (dim 2: k = kTprsRitzMax; dim 1:
 // k = kTprsUniK):
 // X (count x n x k doubles; design d's basis n x (k - 1) at X + d n k),

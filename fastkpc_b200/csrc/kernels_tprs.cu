@@ -15,7 +15,9 @@
 // (tprs_ritz_select_kernel, tprs_ritz_vectors_kernel below); the host
 // downloads the k Ritz vectors and values and finishes the basis
 // (tprs_finish).  A design whose Ritz pairs have not converged is rebuilt on
-// the host.
+// the host.  Bivariate designs with 120 <= n_u and a leading dimension up to
+// 512 take the block Lanczos kernel instead (tprs_block_lanczos_kernel: four
+// vectors per pass over E, 26 passes in place of 80).
 //
 // The matvec E q is memory-bound: E (up to 1536^2 doubles) is read from L2 or
 // HBM once per step.  It reads each tile of the upper block triangle once:
@@ -280,6 +282,337 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
 }
 
 // ---------------------------------------------------------------------------
+// Block Lanczos for the bivariate eta matrices (ld <= kTprsBlockMaxLd).
+//
+// The single-vector kernel above streams the whole upper block triangle of E
+// from HBM once per Lanczos step: 80 passes of 1.11 MB per design at
+// n_u = 500.  Here each pass multiplies kTprsBlock = 4 vectors at once, so a
+// Krylov space of kTprsBlockDim = 104 takes 26 passes (a block Krylov space
+// needs a somewhat larger dimension than a single-vector one for the same
+// k = 30 pairs: 104 reaches residuals of 1e-15 relative on the 500 x 50
+// level's designs, where 80 single-vector steps also do).
+//
+// Step s, with Q_s (nu x 4) the current orthonormal block and V the basis so
+// far (Q_0 .. Q_s):
+//   W = E Q_s (upper-triangle matvec, four vectors per tile);
+//   block classical Gram-Schmidt, twice, each pass followed by a Cholesky QR
+//   (BCGS2): C1 = V'W, W -= V C1, W = Q1 R1; C2 = V'Q1, Q1 -= V C2,
+//   Q1 = Q_{s+1} R2.  Then E Q_s = V (C1 + C2 R1) + Q_{s+1} (R2 R1).
+// The diagonal block A_s (rows of Q_s of C1 + C2 R1) and R_s = R2 R1 form the
+// block-tridiagonal projection T = V' E V (the entries of C further from the
+// diagonal are rounding-level under full re-orthogonalisation); the Ritz step
+// below tridiagonalises T.  A Cholesky pivot below kTprsBlockPivotTol of its
+// Gram diagonal (a block that has lost a direction: cond(W) above about 3e6)
+// ends the run with done[d] = -1, and the host builds that design.
+//
+// Outputs per design d: V (nu x 104 at voff[d]), blocks (count x 26 x 32:
+// A_s then R_s, 4 x 4 column-major each), done[d] = 104 or -1.  One CTA per
+// design (grid-stride), one CTA per SM: dynamic shared memory
+// tprs_block_smem_bytes(ld_max), about 212 KB at ld 512.
+namespace {
+
+constexpr double kTprsBlockPivotTol = 1e-13;
+
+// Gram matrix of the block W (4 x ld in shared memory, rows < nu) into G
+// (4 x 4, both triangles); every thread returns after G is in shared memory.
+__device__ void block_gram(const double* W, int ld, int nu, double (*red)[10], double* G) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double g[10];
+#pragma unroll
+  for (int t = 0; t < 10; ++t) g[t] = 0.0;
+  for (int i = tid; i < nu; i += blockDim.x) {
+    const double w0 = W[i], w1 = W[ld + i], w2 = W[2 * ld + i], w3 = W[3 * ld + i];
+    g[0] += w0 * w0;
+    g[1] += w0 * w1;
+    g[2] += w0 * w2;
+    g[3] += w0 * w3;
+    g[4] += w1 * w1;
+    g[5] += w1 * w2;
+    g[6] += w1 * w3;
+    g[7] += w2 * w2;
+    g[8] += w2 * w3;
+    g[9] += w3 * w3;
+  }
+#pragma unroll
+  for (int t = 0; t < 10; ++t) {
+    const double s = warp_sum_t(g[t]);
+    if (lane == 0) red[warp][t] = s;
+  }
+  __syncthreads();
+  if (tid < 10) {
+    double s = 0.0;
+    for (int w = 0; w < kTprsWarps; ++w) s += red[w][tid];
+    // packed upper triangle (u <= v) -> both triangles of the 4 x 4
+    const int u = tid < 4 ? 0 : (tid < 7 ? 1 : (tid < 9 ? 2 : 3));
+    const int v = u + (tid - (u == 0 ? 0 : (u == 1 ? 4 : (u == 2 ? 7 : 9))));
+    G[u + 4 * v] = s;
+    G[v + 4 * u] = s;
+  }
+  __syncthreads();
+}
+
+// Cholesky G = R'R (R upper, 4 x 4 column-major) and R^-1, by one thread.
+// Returns false when a pivot falls below kTprsBlockPivotTol of its diagonal.
+__device__ bool chol4(const double* G, double* R, double* Ri) {
+  for (int t = 0; t < 16; ++t) {
+    R[t] = 0.0;
+    Ri[t] = 0.0;
+  }
+  for (int v = 0; v < 4; ++v) {
+    for (int u = 0; u < v; ++u) {
+      double s = G[u + 4 * v];
+      for (int w = 0; w < u; ++w) s -= R[w + 4 * u] * R[w + 4 * v];
+      R[u + 4 * v] = s / R[u + 4 * u];
+    }
+    double p = G[v + 4 * v];
+    for (int w = 0; w < v; ++w) p -= R[w + 4 * v] * R[w + 4 * v];
+    if (!(p > kTprsBlockPivotTol * G[v + 4 * v])) return false;
+    R[v + 4 * v] = sqrt(p);
+  }
+  // R^-1 by back substitution, column by column
+  for (int v = 0; v < 4; ++v) {
+    Ri[v + 4 * v] = 1.0 / R[v + 4 * v];
+    for (int u = v - 1; u >= 0; --u) {
+      double s = 0.0;
+      for (int w = u + 1; w <= v; ++w) s += R[u + 4 * w] * Ri[w + 4 * v];
+      Ri[u + 4 * v] = -s / R[u + 4 * u];
+    }
+  }
+  return true;
+}
+
+// W <- W Ri (Ri upper triangular), row by row.
+__device__ void block_scale(double* W, int ld, int nu, const double* Ri) {
+  for (int i = threadIdx.x; i < nu; i += blockDim.x) {
+    const double w0 = W[i], w1 = W[ld + i], w2 = W[2 * ld + i], w3 = W[3 * ld + i];
+    W[i] = w0 * Ri[0];
+    W[ld + i] = w0 * Ri[4] + w1 * Ri[5];
+    W[2 * ld + i] = w0 * Ri[8] + w1 * Ri[9] + w2 * Ri[10];
+    W[3 * ld + i] = w0 * Ri[12] + w1 * Ri[13] + w2 * Ri[14] + w3 * Ri[15];
+  }
+  __syncthreads();
+}
+
+// One classical Gram-Schmidt pass of the block W against the basis columns
+// 0 .. used-1 of Vd (nu rows): coef[v * kTprsBlockDim + j] = V_j . W_v, then
+// W_v -= sum_j coef V_j (fixed order).
+__device__ void block_project(double* W, int ld, int nu, const double* Vd, int used, double* coef) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int j = warp; j < used; j += kTprsWarps) {
+    const double* vj = Vd + static_cast<int64_t>(nu) * j;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    for (int i = lane; i < nu; i += 32) {
+      const double x = vj[i];
+      s0 += x * W[i];
+      s1 += x * W[ld + i];
+      s2 += x * W[2 * ld + i];
+      s3 += x * W[3 * ld + i];
+    }
+    s0 = warp_sum_t(s0);
+    s1 = warp_sum_t(s1);
+    s2 = warp_sum_t(s2);
+    s3 = warp_sum_t(s3);
+    if (lane == 0) {
+      coef[j] = s0;
+      coef[kTprsBlockDim + j] = s1;
+      coef[2 * kTprsBlockDim + j] = s2;
+      coef[3 * kTprsBlockDim + j] = s3;
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < nu; i += blockDim.x) {
+    double w0 = W[i], w1 = W[ld + i], w2 = W[2 * ld + i], w3 = W[3 * ld + i];
+    for (int j = 0; j < used; ++j) {
+      const double x = Vd[i + static_cast<int64_t>(nu) * j];
+      w0 -= coef[j] * x;
+      w1 -= coef[kTprsBlockDim + j] * x;
+      w2 -= coef[2 * kTprsBlockDim + j] * x;
+      w3 -= coef[3 * kTprsBlockDim + j] * x;
+    }
+    W[i] = w0;
+    W[ld + i] = w1;
+    W[2 * ld + i] = w2;
+    W[3 * ld + i] = w3;
+  }
+  __syncthreads();
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kTprsThreads, 1) tprs_block_lanczos_kernel(
+    const double* __restrict__ u, const int64_t* __restrict__ uoff, const int* __restrict__ nus, int count,
+    double eta0, double* __restrict__ ews, int64_t ews_stride, double* __restrict__ V,
+    const int64_t* __restrict__ voff, double* __restrict__ blocks, int* __restrict__ done, int ld_max) {
+  extern __shared__ double sm[];
+  __shared__ double red[kTprsWarps][10];
+  __shared__ double coef1[kTprsBlock * kTprsBlockDim], coef2[kTprsBlock * kTprsBlockDim];
+  __shared__ double G[16], R1[16], R1i[16], R2[16], R2i[16];
+  __shared__ int broke;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  double* q = sm;                                                       // 4 x ld_max: Q_s, then W
+  double* acc = sm + kTprsBlock * static_cast<int64_t>(ld_max);          // warps x 4 x ld_max
+  double* tile = acc + static_cast<int64_t>(kTprsWarps) * kTprsBlock * ld_max + warp * kTileWords;
+  double* W = q;  // the new block once the matvec has consumed Q_s
+  for (int d = blockIdx.x; d < count; d += gridDim.x) {
+    const int nu = nus[d];
+    const int ld = static_cast<int>(tprs_ld(nu));
+    const int nb = ld / kTile;
+    const double* ux = u + uoff[d];
+    const double* uy = ux + nu;
+    double* E = ews + ews_stride * blockIdx.x;
+    double* Vd = V + voff[d];
+    double* blk = blocks + static_cast<int64_t>(d) * kTprsBlockSteps * 32;
+    // upper block triangle of E_ij = eta0 log(r2) / 2 * r2, zero outside nu x nu
+    for (int J = 0; J < nb; ++J) {
+      const int rows = kTile * (J + 1);
+      for (int idx = tid; idx < rows * kTile; idx += blockDim.x) {
+        const int i = idx % rows, j = kTile * J + idx / rows;
+        double v = 0.0;
+        if (i < nu && j < nu) {
+          const double dx = ux[i] - ux[j], dy = uy[i] - uy[j];
+          const double r2 = dx * dx + dy * dy;
+          if (r2 > 0.0) {
+            v = eta0;
+            v *= log(r2) * 0.5;
+            v *= r2;
+          }
+        }
+        E[i + static_cast<int64_t>(ld) * j] = v;
+      }
+    }
+    // start block: the host's deterministic sequence, continued over the four columns
+    if (tid == 0) {
+      unsigned long state = 1;
+      for (int v = 0; v < kTprsBlock; ++v)
+        for (int i = 0; i < nu; ++i) {
+          state = (state * 106UL + 1283UL) % 6075UL;
+          W[v * ld_max + i] = static_cast<double>(state) / 6075.0 - 0.5;
+        }
+      broke = 0;
+    }
+    __syncthreads();
+    for (int pass = 0; pass < 2; ++pass) {
+      block_gram(W, ld_max, nu, red, G);
+      if (tid == 0 && !chol4(G, R1, R1i)) broke = 1;
+      __syncthreads();
+      if (broke) break;
+      block_scale(W, ld_max, nu, R1i);
+    }
+    if (!broke)
+      for (int idx = tid; idx < kTprsBlock * nu; idx += blockDim.x)
+        Vd[idx] = W[(idx / nu) * ld_max + idx % nu];
+    __syncthreads();
+    for (int s = 0; s < kTprsBlockSteps && !broke; ++s) {
+      const double* Qs = Vd + static_cast<int64_t>(nu) * kTprsBlock * s;
+      for (int idx = tid; idx < kTprsBlock * ld; idx += blockDim.x) {
+        const int v = idx / ld, i = idx % ld;
+        q[v * ld_max + i] = i < nu ? Qs[static_cast<int64_t>(nu) * v + i] : 0.0;
+      }
+      for (int idx = tid; idx < kTprsWarps * kTprsBlock * ld; idx += blockDim.x) {
+        const int sl = idx / ld, i = idx % ld;
+        acc[static_cast<int64_t>(sl) * ld_max + i] = 0.0;
+      }
+      __syncthreads();
+      // W = E Q_s over the upper block triangle; slice (warp, v) at acc + (warp * 4 + v) * ld_max
+      double* my = acc + static_cast<int64_t>(warp) * kTprsBlock * ld_max;
+      for (int pidx = warp; 2 * pidx < nb; pidx += kTprsWarps) {
+        for (int half = 0; half < 2; ++half) {
+          const int J = half == 0 ? pidx : nb - 1 - pidx;
+          if (half == 1 && J == pidx) break;
+          const double* Ecol = E + static_cast<int64_t>(ld) * kTile * J;
+          double zc[kTprsBlock] = {0.0, 0.0, 0.0, 0.0};
+          for (int I = 0; I <= J; ++I) {
+            double e[kTile];
+#pragma unroll
+            for (int c = 0; c < kTile; ++c) e[c] = __ldcs(Ecol + kTile * I + lane + static_cast<int64_t>(ld) * c);
+#pragma unroll
+            for (int v = 0; v < kTprsBlock; ++v) {
+              const double2* qv = reinterpret_cast<const double2*>(q + v * ld_max + kTile * J);
+              double r0 = 0.0, r1 = 0.0;
+#pragma unroll
+              for (int c = 0; c < kTile; c += 2) {
+                const double2 qq = qv[c / 2];
+                r0 += e[c] * qq.x;
+                r1 += e[c + 1] * qq.y;
+              }
+              my[v * ld_max + kTile * I + lane] += r0 + r1;
+            }
+            if (I < J) {
+#pragma unroll
+              for (int c = 0; c < kTile; ++c) tile[c * kTileLd + lane] = e[c];
+              __syncwarp();
+              const double2* trow2 = reinterpret_cast<const double2*>(tile + lane * kTileLd);
+#pragma unroll
+              for (int l = 0; l < kTile; l += 2) {
+                const double2 t = trow2[l / 2];
+                e[l] = t.x;
+                e[l + 1] = t.y;
+              }
+              __syncwarp();
+#pragma unroll
+              for (int v = 0; v < kTprsBlock; ++v) {
+                const double2* qv = reinterpret_cast<const double2*>(q + v * ld_max + kTile * I);
+                double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+                for (int l = 0; l < kTile; l += 2) {
+                  const double2 qq = qv[l / 2];
+                  c0 += e[l] * qq.x;
+                  c1 += e[l + 1] * qq.y;
+                }
+                zc[v] += c0 + c1;
+              }
+            }
+          }
+#pragma unroll
+          for (int v = 0; v < kTprsBlock; ++v) my[v * ld_max + kTile * J + lane] += zc[v];
+        }
+      }
+      __syncthreads();
+      // W (over Q_s, rows < nu) = sum over the warps' slices, fixed order
+      for (int idx = tid; idx < kTprsBlock * nu; idx += blockDim.x) {
+        const int v = idx / nu, i = idx % nu;
+        double sacc = 0.0;
+#pragma unroll
+        for (int w = 0; w < kTprsWarps; ++w) sacc += acc[(static_cast<int64_t>(w) * kTprsBlock + v) * ld_max + i];
+        W[v * ld_max + i] = sacc;
+      }
+      __syncthreads();
+      const int used = kTprsBlock * (s + 1);
+      block_project(W, ld_max, nu, Vd, used, coef1);
+      block_gram(W, ld_max, nu, red, G);
+      if (tid == 0 && !chol4(G, R1, R1i)) broke = 1;
+      __syncthreads();
+      if (broke) break;
+      block_scale(W, ld_max, nu, R1i);
+      block_project(W, ld_max, nu, Vd, used, coef2);
+      block_gram(W, ld_max, nu, red, G);
+      if (tid == 0 && !chol4(G, R2, R2i)) broke = 1;
+      __syncthreads();
+      if (broke) break;
+      block_scale(W, ld_max, nu, R2i);
+      // A_s = rows of Q_s of C1 + C2 R1; R_s = R2 R1 (upper triangular)
+      if (tid < 16) {
+        const int r = tid & 3, c = tid >> 2, j = kTprsBlock * s + r;
+        double a = coef1[c * kTprsBlockDim + j];
+        for (int w = 0; w <= c; ++w) a += coef2[w * kTprsBlockDim + j] * R1[w + 4 * c];
+        blk[32 * s + tid] = a;
+        double rr = 0.0;
+        for (int w = r; w <= c; ++w) rr += R2[r + 4 * w] * R1[w + 4 * c];
+        blk[32 * s + 16 + tid] = r <= c ? rr : 0.0;
+      }
+      if (s + 1 < kTprsBlockSteps) {
+        double* vn = Vd + static_cast<int64_t>(nu) * kTprsBlock * (s + 1);
+        for (int idx = tid; idx < kTprsBlock * nu; idx += blockDim.x) vn[idx] = W[(idx / nu) * ld_max + idx % nu];
+      }
+      __syncthreads();
+    }
+    if (tid == 0) done[d] = broke ? -1 : kTprsBlockDim;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Ritz pairs of the Lanczos runs, on the device.
 //
 // tprs_ritz_select_kernel (one warp per design): the eigen-decomposition of
@@ -299,34 +632,18 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
 constexpr int kRitzWarps = 4;                    // at most, per CTA
 constexpr size_t kRitzSmemBudget = 200 * 1024;   // dynamic shared memory for the warps' eigenvector matrices
 
-__global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
-    const double* __restrict__ alpha, const double* __restrict__ beta, const int* __restrict__ done, int count,
-    int steps, int k, double* __restrict__ vals, double* __restrict__ zsel, int* __restrict__ ok) {
-  extern __shared__ double zsh[];  // steps x steps per warp
-  __shared__ double dsh[kRitzWarps][kTprsMaxSteps], esh[kRitzWarps][kTprsMaxSteps];
-  __shared__ int selsh[kRitzWarps][kTprsRitzMax];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int d = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (d >= count) return;  // whole warps only: no block barrier follows
-  double* dd = dsh[warp];
-  double* ee = esh[warp];
-  int* sel = selsh[warp];
-  const int ms = done[d];
-  const int64_t ld = steps;
-  double* z = zsh + static_cast<int64_t>(warp) * steps * steps;
-  const double* al = alpha + static_cast<int64_t>(d) * steps;
-  const double* be = beta + static_cast<int64_t>(d) * steps;
-  constexpr int kRows = kTprsMaxSteps / 32;  // rows per lane
-  for (int i = lane; i < ms; i += 32) {
-    dd[i] = al[i];
-    ee[i] = i + 1 < ms ? be[i] : 0.0;
-  }
-  for (int c = 0; c < ms; ++c)
-    for (int i = lane; i < ms; i += 32) z[i + ld * c] = i == c ? 1.0 : 0.0;
-  __syncwarp();
-  bool good = ms >= k;
+namespace {
+
+constexpr int kRows = kTprsMaxSteps / 32;  // rows of an eigenvector matrix per lane
+
+// Implicit QL with Wilkinson shifts on the symmetric tridiagonal (dd, ee;
+// ee[ms - 1] = 0), by one warp: eigenvalues into dd, the rotations applied to
+// the columns of z (ms rows, column stride ld; lane = row, column i + 1 carried
+// in registers from one rotation to the next).  false when an eigenvalue takes
+// more than 60 sweeps.
+__device__ bool tridiag_ql(double* dd, double* ee, double* z, int ms, int64_t ld, int lane) {
   const double eps = 2.220446049250313e-16;
-  for (int l = 0; l < ms && good; ++l) {
+  for (int l = 0; l < ms; ++l) {
     int iter = 0;
     for (;;) {
       int mm = l;
@@ -335,15 +652,11 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
         if (fabs(ee[mm]) <= eps * sum) break;
       }
       if (mm == l) break;
-      if (++iter > 60) {
-        good = false;
-        break;
-      }
+      if (++iter > 60) return false;
       double g = (dd[l + 1] - dd[l]) / (2.0 * ee[l]);
       double r = hypot(g, 1.0);
       g = dd[mm] - dd[l] + ee[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
       double sn = 1.0, cs = 1.0, p = 0.0;
-      // column i + 1 of z rides in registers from one rotation to the next
       double carry[kRows];
 #pragma unroll
       for (int t = 0; t < kRows; ++t) {
@@ -405,11 +718,12 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
       __syncwarp();
     }
   }
-  if (!good) {
-    if (lane == 0) ok[d] = 0;
-    return;
-  }
-  // the k largest |theta| (stable: ties to the lower index), then by value, descending
+  return true;
+}
+
+// sel[rank] = index of the eigenvalue of rank-th largest |theta| (stable:
+// ties to the lower index), for rank < k; returns max |theta|.
+__device__ double select_largest(const double* dd, int ms, int k, int* sel, int lane) {
   double tmax = 0.0;
   for (int i = lane; i < ms; i += 32) tmax = fmax(tmax, fabs(dd[i]));
   for (int o = 16; o > 0; o >>= 1) tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
@@ -423,14 +737,13 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
     if (rank < k) sel[rank] = i;
   }
   __syncwarp();
-  const double blast = be[ms - 1];
-  const bool invariant = fabs(blast) <= 1e-15 * tmax;
-  bool conv = true;
-  for (int c = lane; c < k; c += 32) {
-    const int i = sel[c];
-    if (!invariant && fabs(blast * z[(ms - 1) + ld * i]) > 1e-14 * tmax) conv = false;
-  }
-  conv = __all_sync(0xffffffffu, conv);
+  return tmax;
+}
+
+// The selected pairs ordered by value, descending: vals (k per design) and
+// their eigenvectors (zstride doubles per column, ms rows used).
+__device__ void write_ritz(const double* dd, const double* z, int64_t ld, int ms, int k, const int* sel, int d,
+                           int zstride, double* vals, double* zsel, int lane) {
   for (int c = lane; c < k; c += 32) {
     const int i = sel[c];
     const double vi = dd[i];
@@ -440,9 +753,210 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
       pos += (ve > vi || (ve == vi && e < c)) ? 1 : 0;
     }
     vals[static_cast<int64_t>(d) * k + pos] = vi;
-    double* zc = zsel + (static_cast<int64_t>(d) * k + pos) * steps;
+    double* zc = zsel + (static_cast<int64_t>(d) * k + pos) * zstride;
     for (int b = 0; b < ms; ++b) zc[b] = z[b + ld * i];
   }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
+    const double* __restrict__ alpha, const double* __restrict__ beta, const int* __restrict__ done, int count,
+    int steps, int k, int zstride, double* __restrict__ vals, double* __restrict__ zsel, int* __restrict__ ok) {
+  extern __shared__ double zsh[];  // steps x steps per warp
+  __shared__ double dsh[kRitzWarps][kTprsMaxSteps], esh[kRitzWarps][kTprsMaxSteps];
+  __shared__ int selsh[kRitzWarps][kTprsRitzMax];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int d = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (d >= count) return;  // whole warps only: no block barrier follows
+  double* dd = dsh[warp];
+  double* ee = esh[warp];
+  int* sel = selsh[warp];
+  const int ms = done[d];
+  const int64_t ld = steps;
+  double* z = zsh + static_cast<int64_t>(warp) * steps * steps;
+  const double* al = alpha + static_cast<int64_t>(d) * steps;
+  const double* be = beta + static_cast<int64_t>(d) * steps;
+  for (int i = lane; i < ms; i += 32) {
+    dd[i] = al[i];
+    ee[i] = i + 1 < ms ? be[i] : 0.0;
+  }
+  for (int c = 0; c < ms; ++c)
+    for (int i = lane; i < ms; i += 32) z[i + ld * c] = i == c ? 1.0 : 0.0;
+  __syncwarp();
+  if (ms < k || !tridiag_ql(dd, ee, z, ms, ld, lane)) {
+    if (lane == 0) ok[d] = 0;
+    return;
+  }
+  const double tmax = select_largest(dd, ms, k, sel, lane);
+  const double blast = be[ms - 1];
+  const bool invariant = fabs(blast) <= 1e-15 * tmax;
+  bool conv = true;
+  for (int c = lane; c < k; c += 32) {
+    const int i = sel[c];
+    if (!invariant && fabs(blast * z[(ms - 1) + ld * i]) > 1e-14 * tmax) conv = false;
+  }
+  conv = __all_sync(0xffffffffu, conv);
+  write_ritz(dd, z, ld, ms, k, sel, d, zstride, vals, zsel, lane);
+  if (lane == 0) ok[d] = conv ? 1 : 0;
+}
+
+// Ritz pairs of the block Lanczos runs (one warp per design).  T (104 x 104,
+// column stride 105 in shared memory) is assembled from the diagonal blocks
+// (A_s + A_s') / 2 and the couplings R_s; Householder reflections reduce it to
+// a tridiagonal (Golub and Van Loan, Matrix Computations, algorithm 8.3.1:
+// H_k = I - tau v v', v(k+1) = 1, stored below the subdiagonal of column k),
+// the product P = H_0 ... H_{m-3} is formed in place from the back, and the
+// implicit QL above rotates P's columns into T's eigenvectors.  The residual
+// of a Ritz pair (theta, y) is |R_last y_last| (y_last its rows of the last
+// block), accepted at 1e-14 max |theta| as for the single-vector runs.
+__global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel(
+    const double* __restrict__ blocks, const int* __restrict__ done, int count, int k, int zstride,
+    double* __restrict__ vals, double* __restrict__ zsel, int* __restrict__ ok) {
+  extern __shared__ double zsh[];  // (m + 1) x m per warp
+  __shared__ double dsh[kRitzWarps][kTprsMaxSteps], esh[kRitzWarps][kTprsMaxSteps];
+  __shared__ double tsh[kRitzWarps][kTprsMaxSteps], wsh[kRitzWarps][kTprsMaxSteps];
+  __shared__ int selsh[kRitzWarps][kTprsRitzMax];
+  constexpr int m = kTprsBlockDim;
+  constexpr int64_t ld = m + 1;  // odd stride: a warp reading a row touches distinct banks
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int d = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (d >= count) return;  // whole warps only: no block barrier follows
+  if (done[d] != m) {
+    if (lane == 0) ok[d] = 0;
+    return;
+  }
+  double* dd = dsh[warp];
+  double* ee = esh[warp];
+  double* tau = tsh[warp];
+  double* wv = wsh[warp];
+  int* sel = selsh[warp];
+  double* a = zsh + static_cast<int64_t>(warp) * ld * m;
+  const double* blk = blocks + static_cast<int64_t>(d) * kTprsBlockSteps * 32;
+  for (int64_t idx = lane; idx < ld * m; idx += 32) a[idx] = 0.0;
+  __syncwarp();
+  for (int s = 0; s < kTprsBlockSteps; ++s) {
+    if (lane < 16) {
+      const int r = lane & 3, c = lane >> 2;
+      a[(4 * s + r) + ld * (4 * s + c)] = 0.5 * (blk[32 * s + r + 4 * c] + blk[32 * s + c + 4 * r]);
+      if (s + 1 < kTprsBlockSteps && r <= c) {
+        const double rv = blk[32 * s + 16 + r + 4 * c];
+        a[(4 * (s + 1) + r) + ld * (4 * s + c)] = rv;
+        a[(4 * s + c) + ld * (4 * (s + 1) + r)] = rv;
+      }
+    }
+  }
+  __syncwarp();
+  // Householder tridiagonalisation: lanes over rows
+  for (int kk = 0; kk < m - 2; ++kk) {
+    const int r0 = kk + 1;
+    double* col = a + ld * kk;
+    double tail = 0.0;
+    for (int i = r0 + 1 + lane; i < m; i += 32) tail += col[i] * col[i];
+    tail = warp_sum_t(tail);
+    const double x0 = col[r0];
+    double t = 0.0, beta = x0;
+    if (tail > 0.0) {
+      const double nrm = sqrt(x0 * x0 + tail);
+      beta = x0 >= 0.0 ? -nrm : nrm;
+      t = (beta - x0) / beta;
+      const double scale = 1.0 / (x0 - beta);
+      for (int i = r0 + 1 + lane; i < m; i += 32) col[i] *= scale;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      col[r0] = 1.0;
+      ee[kk] = beta;
+      tau[kk] = t;
+      dd[kk] = a[kk + ld * kk];
+    }
+    __syncwarp();
+    if (t != 0.0) {
+      // p = t A22 v; w = p - (t/2)(p.v) v; A22 -= v w' + w v'
+      double p[kRows];
+      double pv = 0.0;
+#pragma unroll
+      for (int tt = 0; tt < kRows; ++tt) {
+        const int row = r0 + lane + 32 * tt;
+        p[tt] = 0.0;
+        if (row < m) {
+          double acc = 0.0;
+          for (int j = r0; j < m; ++j) acc += a[row + ld * j] * col[j];
+          p[tt] = t * acc;
+          pv += p[tt] * col[row];
+        }
+      }
+      pv = warp_sum_t(pv);
+      const double kw = 0.5 * t * pv;
+#pragma unroll
+      for (int tt = 0; tt < kRows; ++tt) {
+        const int row = r0 + lane + 32 * tt;
+        if (row < m) wv[row] = p[tt] - kw * col[row];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int tt = 0; tt < kRows; ++tt) {
+        const int row = r0 + lane + 32 * tt;
+        if (row < m) {
+          const double vr = col[row], wr = wv[row];
+          for (int j = r0; j < m; ++j) a[row + ld * j] -= vr * wv[j] + wr * col[j];
+        }
+      }
+      __syncwarp();
+    }
+  }
+  if (lane == 0) {
+    dd[m - 2] = a[(m - 2) + ld * (m - 2)];
+    dd[m - 1] = a[(m - 1) + ld * (m - 1)];
+    ee[m - 2] = a[(m - 1) + ld * (m - 2)];
+    ee[m - 1] = 0.0;
+    a[(m - 1) + ld * (m - 1)] = 1.0;
+  }
+  __syncwarp();
+  // P = H_0 ... H_{m-3}, from the back: before H_kk, row and column kk + 1
+  // of the trailing block become unit; H_kk then acts on rows kk + 1 .. m - 1
+  // (lanes over columns)
+  for (int kk = m - 3; kk >= -1; --kk) {
+    const int r0 = kk + 1;
+    for (int j = r0 + 1 + lane; j < m; j += 32) {
+      a[r0 + ld * j] = 0.0;
+      a[j + ld * r0] = 0.0;
+    }
+    if (lane == 0) a[r0 + ld * r0] = 1.0;
+    __syncwarp();
+    if (kk < 0) break;
+    const double t = tau[kk];
+    if (t != 0.0) {
+      const double* v = a + ld * kk;
+      for (int j = r0 + lane; j < m; j += 32) {
+        double sdot = 0.0;
+        for (int i = r0; i < m; ++i) sdot += v[i] * a[i + ld * j];
+        sdot *= t;
+        for (int i = r0; i < m; ++i) a[i + ld * j] -= v[i] * sdot;
+      }
+    }
+    __syncwarp();
+  }
+  if (!tridiag_ql(dd, ee, a, m, ld, lane)) {
+    if (lane == 0) ok[d] = 0;
+    return;
+  }
+  const double tmax = select_largest(dd, m, k, sel, lane);
+  const double* rl = blk + 32 * (kTprsBlockSteps - 1) + 16;  // R_last, upper triangular
+  bool conv = true;
+  for (int c = lane; c < k; c += 32) {
+    const int i = sel[c];
+    const double* y = a + ld * i + (m - kTprsBlock);
+    double res = 0.0;
+    for (int r = 0; r < kTprsBlock; ++r) {
+      double x = 0.0;
+      for (int w = r; w < kTprsBlock; ++w) x += rl[r + 4 * w] * y[w];
+      res += x * x;
+    }
+    if (sqrt(res) > 1e-14 * tmax) conv = false;
+  }
+  conv = __all_sync(0xffffffffu, conv);
+  write_ritz(dd, a, ld, m, k, sel, d, zstride, vals, zsel, lane);
   if (lane == 0) ok[d] = conv ? 1 : 0;
 }
 
@@ -538,11 +1052,11 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_ritz_vectors_kernel(
   }
 }
 
-cudaError_t launch_tprs_ritz(const double* alpha, const double* beta, const int* done, int count, int steps, int k,
-                             double* vals, double* zsel, int* ok, const double* V, const int64_t* voff,
-                             const int* nus, double* U, const int64_t* uoff, cudaStream_t stream) {
+cudaError_t launch_tprs_ritz_select(const double* alpha, const double* beta, const int* done, int count, int steps,
+                                    int k, int zstride, double* vals, double* zsel, int* ok, cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
-  if ((k != kTprsRitzMax && k != kTprsUniK) || steps < k || steps > kTprsMaxSteps) return cudaErrorInvalidValue;
+  if ((k != kTprsRitzMax && k != kTprsUniK) || steps < k || steps > kTprsMaxSteps || zstride < steps)
+    return cudaErrorInvalidValue;
   const size_t per_warp = sizeof(double) * static_cast<size_t>(steps) * steps;
   int warps = static_cast<int>(kRitzSmemBudget / per_warp);
   warps = warps < 1 ? 1 : (warps > kRitzWarps ? kRitzWarps : warps);
@@ -551,16 +1065,38 @@ cudaError_t launch_tprs_ritz(const double* alpha, const double* beta, const int*
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   tprs_ritz_select_kernel<<<(count + warps - 1) / warps, warps * 32, smem, stream>>>(alpha, beta, done, count, steps,
-                                                                                      k, vals, zsel, ok);
-  e = cudaGetLastError();
+                                                                                      k, zstride, vals, zsel, ok);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tprs_ritz_block_select(const double* blocks, const int* done, int count, int k, int zstride,
+                                          double* vals, double* zsel, int* ok, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  if (k != kTprsRitzMax || zstride < kTprsBlockDim) return cudaErrorInvalidValue;
+  const size_t per_warp = sizeof(double) * static_cast<size_t>(kTprsBlockDim + 1) * kTprsBlockDim;
+  int warps = static_cast<int>(kRitzSmemBudget / per_warp);
+  warps = warps < 1 ? 1 : (warps > kRitzWarps ? kRitzWarps : warps);
+  const size_t smem = per_warp * warps;
+  cudaError_t e = cudaFuncSetAttribute(tprs_ritz_block_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
   if (e != cudaSuccess) return e;
+  tprs_ritz_block_select_kernel<<<(count + warps - 1) / warps, warps * 32, smem, stream>>>(blocks, done, count, k,
+                                                                                            zstride, vals, zsel, ok);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tprs_ritz_vectors(const double* V, const int64_t* voff, const int* nus, const int* done,
+                                     const int* ok, const double* zsel, int count, int zstride, int k, double* U,
+                                     const int64_t* uoff, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  if ((k != kTprsRitzMax && k != kTprsUniK) || zstride < k || zstride > kTprsMaxSteps) return cudaErrorInvalidValue;
   const int ctas = count < 2 * 148 ? count : 2 * 148;
   if (k == kTprsRitzMax)
     tprs_ritz_vectors_kernel<kTprsRitzMax><<<ctas, kTprsThreads, 0, stream>>>(V, voff, nus, done, ok, zsel, count,
-                                                                               steps, U, uoff);
+                                                                               zstride, U, uoff);
   else
     tprs_ritz_vectors_kernel<kTprsUniK><<<ctas, kTprsThreads, 0, stream>>>(V, voff, nus, done, ok, zsel, count,
-                                                                            steps, U, uoff);
+                                                                            zstride, U, uoff);
   return cudaGetLastError();
 }
 
@@ -885,6 +1421,29 @@ cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int*
   tprs_lanczos_kernel<<<ctas, kTprsThreads, smem, stream>>>(u, uoff, nus, count, steps, eta0, ews, ews_stride, V,
                                                              voff, alpha, beta, done,
                                                              static_cast<int>(tprs_ld(nu_max)), dim);
+  return cudaGetLastError();
+}
+
+size_t tprs_block_smem_bytes(int nu_max) {
+  const int64_t ld = tprs_ld(nu_max);
+  return sizeof(double) * static_cast<size_t>((1 + kTprsWarps) * kTprsBlock * ld + kTprsWarps * kTileWords);
+}
+
+cudaError_t launch_tprs_block_lanczos(const double* u, const int64_t* uoff, const int* nus, int count, int nu_max,
+                                      double eta0, double* ews, int64_t ews_stride, int ctas, double* V,
+                                      const int64_t* voff, double* blocks, int* done, cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  if (ctas < 1 || nu_max <= kTprsBlockDim || tprs_ld(nu_max) > kTprsBlockMaxLd ||
+      ews_stride < tprs_ld(nu_max) * tprs_ld(nu_max))
+    return cudaErrorInvalidValue;
+  const size_t smem = tprs_block_smem_bytes(nu_max);
+  cudaError_t e = cudaFuncSetAttribute(tprs_block_lanczos_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(tprs_block_lanczos_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return e;
+  tprs_block_lanczos_kernel<<<ctas, kTprsThreads, smem, stream>>>(u, uoff, nus, count, eta0, ews, ews_stride, V, voff,
+                                                                   blocks, done, static_cast<int>(tprs_ld(nu_max)));
   return cudaGetLastError();
 }
 

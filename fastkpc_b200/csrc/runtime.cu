@@ -317,22 +317,33 @@ void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int di
   for (size_t i = 0; i < count; ++i)
     if (ok[i]) batch->idx.push_back(i);
   if (batch->idx.empty()) return;
+  // bivariate designs the block Lanczos takes come first, the single-vector
+  // runs after them; the choice depends on the design's own locations only
+  auto blockable = [&](size_t i) {
+    const int nu = batch->preps[i].nu;
+    return dim == 2 && nu >= kTprsBlockMinNu && tprs_ld(nu) <= kTprsBlockMaxLd;
+  };
+  std::stable_partition(batch->idx.begin(), batch->idx.end(), blockable);
+  int nblk = 0;
+  while (nblk < static_cast<int>(batch->idx.size()) && blockable(batch->idx[nblk])) ++nblk;
+  const int zstride = nblk > 0 ? std::max(steps, kTprsBlockDim) : steps;
   // offsets, then the locations and row mappings written straight into
   // page-locked staging by the host threads
   std::vector<int64_t> uoff, voff, roff;
   batch->nus.clear();
-  int nu_max = 0;
+  int nu_max_blk = 0, nu_max = 0;
   int64_t vtotal = 0, utotal = 0, ltotal = 0;
-  for (size_t i : batch->idx) {
-    const TprsPrep& pr = batch->preps[i];
+  for (size_t c = 0; c < batch->idx.size(); ++c) {
+    const TprsPrep& pr = batch->preps[batch->idx[c]];
+    const bool blk = static_cast<int>(c) < nblk;
     uoff.push_back(ltotal);
     ltotal += static_cast<int64_t>(pr.u.size());
     batch->nus.push_back(pr.nu);
     voff.push_back(vtotal);
-    vtotal += static_cast<int64_t>(pr.nu) * steps;
+    vtotal += static_cast<int64_t>(pr.nu) * (blk ? kTprsBlockDim : steps);
     roff.push_back(utotal);
     utotal += static_cast<int64_t>(pr.nu) * kk;
-    nu_max = std::max(nu_max, pr.nu);
+    (blk ? nu_max_blk : nu_max) = std::max(blk ? nu_max_blk : nu_max, pr.nu);
   }
   double* hu = static_cast<double*>(stage_alloc(sizeof(double) * static_cast<size_t>(ltotal)));
   int* hmap = static_cast<int*>(stage_alloc(sizeof(int) * batch->idx.size() * static_cast<size_t>(n)));
@@ -342,8 +353,10 @@ void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int di
     std::memcpy(hmap + c * static_cast<size_t>(n), pr.mapping.data(), static_cast<size_t>(n) * sizeof(int));
   });
   const int cnt = static_cast<int>(batch->idx.size());
-  const int ctas = std::min(cnt, ctas_per_sm * sms_);
-  const size_t nab = static_cast<size_t>(2) * cnt * steps;
+  const int nsingle = cnt - nblk;
+  const int ctas = std::min(nsingle, ctas_per_sm * sms_);
+  const int ctas_blk = std::min(nblk, sms_);  // one CTA per SM (its shared memory)
+  const size_t nab = static_cast<size_t>(2) * nsingle * steps;
   const size_t nvals = static_cast<size_t>(cnt) * kk;
   const size_t ns = static_cast<size_t>(cnt) * (kk - 1) * (kk - 1);
   const size_t ncs = static_cast<size_t>(cnt) * (kk - 1);
@@ -363,9 +376,12 @@ void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int di
   stage_upload(tb.roff, roff, st);
   stage_upload(tb.nus, batch->nus, st);
   const int64_t ews_stride = tprs_ld(nu_max) * tprs_ld(nu_max);
+  const int64_t ews_stride_blk = tprs_ld(nu_max_blk) * tprs_ld(nu_max_blk);
   double* dV = tb.V.ensure(static_cast<size_t>(vtotal));
-  double* dab = tb.ab.ensure(nab);
-  double* ews = tb.ews.ensure(static_cast<size_t>(ctas) * ews_stride);
+  double* dab = tb.ab.ensure(std::max<size_t>(nab, 1));
+  double* dblocks = tb.blocks.ensure(std::max<size_t>(static_cast<size_t>(nblk) * kTprsBlockSteps * 32, 1));
+  double* ews = tb.ews.ensure(std::max(static_cast<size_t>(ctas) * ews_stride,
+                                       static_cast<size_t>(ctas_blk) * ews_stride_blk));
   int* ddone = tb.done.ensure(cnt);
   double* dvals = tb.vals.ensure(nvals);
   double* dU = tb.U.ensure(static_cast<size_t>(utotal));
@@ -386,14 +402,23 @@ void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int di
   double* dS = tb.S.ensure(ns);
   double* dcs = tb.colsq.ensure(ncs);
   int* dst = tb.status.ensure(cnt);
-  cuda_check(launch_tprs_lanczos(tb.u.get(), tb.uoff.get(), tb.nus.get(), cnt, nu_max, dim, steps,
-                                 tprs_eta0(dim), ews, ews_stride, ctas, dV, tb.voff.get(), dab,
-                                 dab + static_cast<size_t>(cnt) * steps, ddone, st),
+  double* dzsel = tb.zsel.ensure(nvals * zstride);
+  cuda_check(launch_tprs_block_lanczos(tb.u.get(), tb.uoff.get(), tb.nus.get(), nblk, nu_max_blk, tprs_eta0(dim),
+                                       ews, ews_stride_blk, ctas_blk, dV, tb.voff.get(), dblocks, ddone, st),
+             "thin-plate block Lanczos");
+  cuda_check(launch_tprs_lanczos(tb.u.get(), tb.uoff.get() + nblk, tb.nus.get() + nblk, nsingle, nu_max, dim, steps,
+                                 tprs_eta0(dim), ews, ews_stride, ctas, dV, tb.voff.get() + nblk, dab,
+                                 dab + static_cast<size_t>(nsingle) * steps, ddone + nblk, st),
              "thin-plate Lanczos");
-  cuda_check(launch_tprs_ritz(dab, dab + static_cast<size_t>(cnt) * steps, ddone, cnt, steps, kk,
-                              dvals, tb.zsel.ensure(nvals * steps), dok, dV, tb.voff.get(),
-                              tb.nus.get(), dU, tb.roff.get(), st),
+  cuda_check(launch_tprs_ritz_block_select(dblocks, ddone, nblk, kk, zstride, dvals, dzsel, dok, st),
              "thin-plate Ritz pairs");
+  cuda_check(launch_tprs_ritz_select(dab, dab + static_cast<size_t>(nsingle) * steps, ddone + nblk, nsingle, steps,
+                                     kk, zstride, dvals + static_cast<size_t>(nblk) * kk,
+                                     dzsel + static_cast<size_t>(nblk) * kk * zstride, dok + nblk, st),
+             "thin-plate Ritz pairs");
+  cuda_check(launch_tprs_ritz_vectors(dV, tb.voff.get(), tb.nus.get(), ddone, dok, dzsel, cnt, zstride, kk, dU,
+                                      tb.roff.get(), st),
+             "thin-plate Ritz vectors");
   cuda_check(launch_tprs_finish(dU, tb.roff.get(), dvals, dok, tb.u.get(), tb.uoff.get(),
                                 tb.nus.get(), tb.map.get(), n, cnt, dim, dX, dS, dcs, dst, st),
              "thin-plate basis");

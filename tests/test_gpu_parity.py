@@ -498,3 +498,28 @@ def test_schedule_tunings_change_no_record(lib, method):
             fk.set_tuning(0, lowrank_ctas_per_sm=9)
     finally:
         fk.set_tuning(0, **base)
+
+
+def test_block_and_single_vector_lanczos_in_one_batch(lib):
+    """Bivariate designs with at least 120 unique locations (and a leading
+    dimension up to 512) take the block Lanczos; the design on {0, 1} below
+    has 95 (two columns of 10 levels each) and takes the single-vector run in
+    the same batch.  Residuals of both against the oracle."""
+    rs = np.random.default_rng(13)
+    n = 300
+    X = rs.normal(size=(n, 6))
+    lv = np.array([0.0, 1.1, 2.5, 3.2, 4.8, 6.0, 7.7, 9.1, 10.4, 12.9])
+    X[:, 0] = lv[rs.integers(0, 10, size=n)]
+    X[:, 1] = lv[rs.integers(0, 10, size=n)] * 0.7 + 0.13
+    X[:, 2] += np.sin(X[:, 0]) + 0.2 * X[:, 1]
+    X[:, 5] += np.tanh(X[:, 3]) - 0.1 * X[:, 0]
+    X = np.asfortranarray(X)
+    assert len({tuple(r) for r in X[:, :2]}) == 95
+    fits = [(2, [0, 1]), (5, [0, 1]), (2, [3, 4]), (5, [3, 4]), (0, [2, 5]), (4, [1, 3])]
+    resid, lsp, status = fk.regress_batch(X, fits)
+    assert (status == 0).all()
+    for k, (t, S) in enumerate(fits):
+        prep = gcv.Prepared(tprs.design(X, S))
+        r, _ = gcv.fit(prep, X[:, t])
+        err = np.max(np.abs(resid[:, k] - r)) / np.max(np.abs(r))
+        assert err <= RESID_TOL, (t, S, err)

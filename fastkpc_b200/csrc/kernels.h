@@ -164,8 +164,10 @@ cudaError_t launch_tprs_block_lanczos(const double* u, const int64_t* uoff, cons
 // accepted design.  k is kTprsRitzMax or kTprsUniK (block runs: kTprsRitzMax).
 cudaError_t launch_tprs_ritz_select(const double* alpha, const double* beta, const int* done, int count, int steps,
                                     int k, int zstride, double* vals, double* zsel, int* ok, cudaStream_t stream);
+// pws: tprs_ritz_block_workspace(count) doubles (the inner Lanczos bases).
 cudaError_t launch_tprs_ritz_block_select(const double* blocks, const int* done, int count, int k, int zstride,
-                                          double* vals, double* zsel, int* ok, cudaStream_t stream);
+                                          double* pws, double* vals, double* zsel, int* ok, cudaStream_t stream);
+size_t tprs_ritz_block_workspace(int count);
 cudaError_t launch_tprs_ritz_vectors(const double* V, const int64_t* voff, const int* nus, const int* done,
                                      const int* ok, const double* zsel, int count, int zstride, int k, double* U,
                                      const int64_t* uoff, cudaStream_t stream);

@@ -284,34 +284,41 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
 // ---------------------------------------------------------------------------
 // Block Lanczos for the bivariate eta matrices (ld <= kTprsBlockMaxLd).
 //
-// The single-vector kernel above streams the whole upper block triangle of E
-// from HBM once per Lanczos step: 80 passes of 1.11 MB per design at
-// n_u = 500.  Here each pass multiplies kTprsBlock = 4 vectors at once, so a
-// Krylov space of kTprsBlockDim = 104 takes 26 passes (a block Krylov space
-// needs a somewhat larger dimension than a single-vector one for the same
-// k = 30 pairs: 104 reaches residuals of 1e-15 relative on the 500 x 50
-// level's designs, where 80 single-vector steps also do).
+// The single-vector kernel above streams the upper block triangle of E from
+// HBM once per Lanczos step: 80 passes of 1.11 MB per design at n_u = 500.
+// Here each pass multiplies kTprsBlock = 4 vectors at once, so a Krylov space
+// of kTprsBlockDim = 104 takes 26 passes (a block Krylov space needs a
+// somewhat larger dimension than a single-vector one for the same k = 30
+// pairs: 104 reaches residuals of 1e-15 relative on the 500 x 50 level's
+// designs, where 80 single-vector steps also do).
+//
+// E is stored whole (both triangles, 2.1 MB at ld 512): a warp owns row
+// blocks of 32 rows (lane = row) and sums whole rows in registers, so the
+// matvec needs no transposing tiles and no per-warp row accumulators, and two
+// CTAs fit on an SM (about 100 KB of shared memory each): one streams E while
+// the other re-orthogonalises.
 //
 // Step s, with Q_s (nu x 4) the current orthonormal block and V the basis so
 // far (Q_0 .. Q_s):
-//   W = E Q_s (upper-triangle matvec, four vectors per tile);
-//   block classical Gram-Schmidt, twice, each pass followed by a Cholesky QR
-//   (BCGS2): C1 = V'W, W -= V C1, W = Q1 R1; C2 = V'Q1, Q1 -= V C2,
-//   Q1 = Q_{s+1} R2.  Then E Q_s = V (C1 + C2 R1) + Q_{s+1} (R2 R1).
+//   W = E Q_s;
+//   block Gram-Schmidt, twice, each pass followed by a Cholesky QR (BCGS2):
+//   C1 = V'W, W -= V C1, W = Q1 R1; C2 = V'Q1, Q1 -= V C2, Q1 = Q_{s+1} R2.
+//   Then E Q_s = V (C1 + C2 R1) + Q_{s+1} (R2 R1).
 // The diagonal block A_s (rows of Q_s of C1 + C2 R1) and R_s = R2 R1 form the
 // block-tridiagonal projection T = V' E V (the entries of C further from the
-// diagonal are rounding-level under full re-orthogonalisation); the Ritz step
-// below tridiagonalises T.  A Cholesky pivot below kTprsBlockPivotTol of its
-// Gram diagonal (a block that has lost a direction: cond(W) above about 3e6)
-// ends the run with done[d] = -1, and the host builds that design.
+// diagonal are rounding-level under full re-orthogonalisation).  A Cholesky
+// pivot below kTprsBlockPivotTol of its Gram diagonal (a block that has lost
+// a direction: cond(W) above about 3e6) ends the run with done[d] = -1, and
+// the host builds that design.
 //
 // Outputs per design d: V (nu x 104 at voff[d]), blocks (count x 26 x 32:
 // A_s then R_s, 4 x 4 column-major each), done[d] = 104 or -1.  One CTA per
-// design (grid-stride), one CTA per SM: dynamic shared memory
-// tprs_block_smem_bytes(ld_max), about 212 KB at ld 512.
+// design (grid-stride), two CTAs per SM: dynamic shared memory
+// tprs_block_smem_bytes(ld_max), 96 KB at ld 512; ews: ld^2 per CTA.
 namespace {
 
 constexpr double kTprsBlockPivotTol = 1e-13;
+constexpr int kTprsStageCols = 16;  // basis columns staged in shared memory per projection chunk
 
 // Gram matrix of the block W (4 x ld in shared memory, rows < nu) into G
 // (4 x 4, both triangles); every thread returns after G is in shared memory.
@@ -393,53 +400,64 @@ __device__ void block_scale(double* W, int ld, int nu, const double* Ri) {
   __syncthreads();
 }
 
-// One classical Gram-Schmidt pass of the block W against the basis columns
-// 0 .. used-1 of Vd (nu rows): coef[v * kTprsBlockDim + j] = V_j . W_v, then
-// W_v -= sum_j coef V_j (fixed order).
-__device__ void block_project(double* W, int ld, int nu, const double* Vd, int used, double* coef) {
+// One Gram-Schmidt pass of the block W against the basis columns 0 .. used-1
+// of Vd (nu rows), kTprsStageCols columns at a time staged through shared
+// memory (stage: kTprsStageCols x ld): coef[v * kTprsBlockDim + j] = V_j . W_v, W_v -= sum_j coef V_j, a
+// chunk's coefficients taken after the chunks before it are subtracted
+// (classical within a chunk, modified across chunks; the coefficients are
+// the amounts subtracted, so E Q_s = V C + W holds either way).
+__device__ void block_project(double* W, int ld, int nu, const double* Vd, int used, double* coef, double* stage) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  for (int j = warp; j < used; j += kTprsWarps) {
-    const double* vj = Vd + static_cast<int64_t>(nu) * j;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    for (int i = lane; i < nu; i += 32) {
-      const double x = vj[i];
-      s0 += x * W[i];
-      s1 += x * W[ld + i];
-      s2 += x * W[2 * ld + i];
-      s3 += x * W[3 * ld + i];
+  for (int c0 = 0; c0 < used; c0 += kTprsStageCols) {
+    const int cn = used - c0 < kTprsStageCols ? used - c0 : kTprsStageCols;
+    const double* src = Vd + static_cast<int64_t>(nu) * c0;
+    for (int jj = warp; jj < cn; jj += kTprsWarps)
+      for (int i = lane; i < nu; i += 32) stage[jj * ld + i] = src[static_cast<int64_t>(nu) * jj + i];
+    __syncthreads();
+    for (int jj = warp; jj < cn; jj += kTprsWarps) {
+      const double* vj = stage + jj * ld;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      for (int i = lane; i < nu; i += 32) {
+        const double x = vj[i];
+        s0 += x * W[i];
+        s1 += x * W[ld + i];
+        s2 += x * W[2 * ld + i];
+        s3 += x * W[3 * ld + i];
+      }
+      s0 = warp_sum_t(s0);
+      s1 = warp_sum_t(s1);
+      s2 = warp_sum_t(s2);
+      s3 = warp_sum_t(s3);
+      if (lane == 0) {
+        coef[c0 + jj] = s0;
+        coef[kTprsBlockDim + c0 + jj] = s1;
+        coef[2 * kTprsBlockDim + c0 + jj] = s2;
+        coef[3 * kTprsBlockDim + c0 + jj] = s3;
+      }
     }
-    s0 = warp_sum_t(s0);
-    s1 = warp_sum_t(s1);
-    s2 = warp_sum_t(s2);
-    s3 = warp_sum_t(s3);
-    if (lane == 0) {
-      coef[j] = s0;
-      coef[kTprsBlockDim + j] = s1;
-      coef[2 * kTprsBlockDim + j] = s2;
-      coef[3 * kTprsBlockDim + j] = s3;
+    __syncthreads();
+    for (int i = tid; i < nu; i += blockDim.x) {
+      double w0 = W[i], w1 = W[ld + i], w2 = W[2 * ld + i], w3 = W[3 * ld + i];
+      for (int jj = 0; jj < cn; ++jj) {
+        const double x = stage[jj * ld + i];
+        const int j = c0 + jj;
+        w0 -= coef[j] * x;
+        w1 -= coef[kTprsBlockDim + j] * x;
+        w2 -= coef[2 * kTprsBlockDim + j] * x;
+        w3 -= coef[3 * kTprsBlockDim + j] * x;
+      }
+      W[i] = w0;
+      W[ld + i] = w1;
+      W[2 * ld + i] = w2;
+      W[3 * ld + i] = w3;
     }
+    __syncthreads();
   }
-  __syncthreads();
-  for (int i = tid; i < nu; i += blockDim.x) {
-    double w0 = W[i], w1 = W[ld + i], w2 = W[2 * ld + i], w3 = W[3 * ld + i];
-    for (int j = 0; j < used; ++j) {
-      const double x = Vd[i + static_cast<int64_t>(nu) * j];
-      w0 -= coef[j] * x;
-      w1 -= coef[kTprsBlockDim + j] * x;
-      w2 -= coef[2 * kTprsBlockDim + j] * x;
-      w3 -= coef[3 * kTprsBlockDim + j] * x;
-    }
-    W[i] = w0;
-    W[ld + i] = w1;
-    W[2 * ld + i] = w2;
-    W[3 * ld + i] = w3;
-  }
-  __syncthreads();
 }
 
 }  // namespace
 
-__global__ void __launch_bounds__(kTprsThreads, 1) tprs_block_lanczos_kernel(
+__global__ void __launch_bounds__(kTprsThreads, 2) tprs_block_lanczos_kernel(
     const double* __restrict__ u, const int64_t* __restrict__ uoff, const int* __restrict__ nus, int count,
     double eta0, double* __restrict__ ews, int64_t ews_stride, double* __restrict__ V,
     const int64_t* __restrict__ voff, double* __restrict__ blocks, int* __restrict__ done, int ld_max) {
@@ -450,10 +468,9 @@ __global__ void __launch_bounds__(kTprsThreads, 1) tprs_block_lanczos_kernel(
   __shared__ int broke;
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  double* q = sm;                                                       // 4 x ld_max: Q_s, then W
-  double* acc = sm + kTprsBlock * static_cast<int64_t>(ld_max);          // warps x 4 x ld_max
-  double* tile = acc + static_cast<int64_t>(kTprsWarps) * kTprsBlock * ld_max + warp * kTileWords;
-  double* W = q;  // the new block once the matvec has consumed Q_s
+  double* q = sm;                                                   // 4 x ld_max: Q_s, zero beyond nu
+  double* W = q + kTprsBlock * static_cast<int64_t>(ld_max);         // 4 x ld_max: the new block
+  double* stage = W + kTprsBlock * static_cast<int64_t>(ld_max);     // kTprsStageCols x ld_max
   for (int d = blockIdx.x; d < count; d += gridDim.x) {
     const int nu = nus[d];
     const int ld = static_cast<int>(tprs_ld(nu));
@@ -463,14 +480,15 @@ __global__ void __launch_bounds__(kTprsThreads, 1) tprs_block_lanczos_kernel(
     double* E = ews + ews_stride * blockIdx.x;
     double* Vd = V + voff[d];
     double* blk = blocks + static_cast<int64_t>(d) * kTprsBlockSteps * 32;
-    // upper block triangle of E_ij = eta0 log(r2) / 2 * r2, zero outside nu x nu
-    for (int J = 0; J < nb; ++J) {
-      const int rows = kTile * (J + 1);
-      for (int idx = tid; idx < rows * kTile; idx += blockDim.x) {
-        const int i = idx % rows, j = kTile * J + idx / rows;
+    // E_ij = eta0 log(r2) / 2 * r2 (both triangles), zero outside nu x nu:
+    // a warp per column, lanes down the rows
+    for (int j = warp; j < ld; j += kTprsWarps) {
+      double* Ej = E + static_cast<int64_t>(ld) * j;
+      const double xj = j < nu ? ux[j] : 0.0, yj = j < nu ? uy[j] : 0.0;
+      for (int i = lane; i < ld; i += 32) {
         double v = 0.0;
         if (i < nu && j < nu) {
-          const double dx = ux[i] - ux[j], dy = uy[i] - uy[j];
+          const double dx = ux[i] - xj, dy = uy[i] - yj;
           const double r2 = dx * dx + dy * dy;
           if (r2 > 0.0) {
             v = eta0;
@@ -478,7 +496,7 @@ __global__ void __launch_bounds__(kTprsThreads, 1) tprs_block_lanczos_kernel(
             v *= r2;
           }
         }
-        E[i + static_cast<int64_t>(ld) * j] = v;
+        Ej[i] = v;
       }
     }
     // start block: the host's deterministic sequence, continued over the four columns
@@ -500,92 +518,49 @@ __global__ void __launch_bounds__(kTprsThreads, 1) tprs_block_lanczos_kernel(
       block_scale(W, ld_max, nu, R1i);
     }
     if (!broke)
-      for (int idx = tid; idx < kTprsBlock * nu; idx += blockDim.x)
-        Vd[idx] = W[(idx / nu) * ld_max + idx % nu];
+      for (int v = warp; v < kTprsBlock; v += kTprsWarps)
+        for (int i = lane; i < nu; i += 32) Vd[static_cast<int64_t>(nu) * v + i] = W[v * ld_max + i];
     __syncthreads();
     for (int s = 0; s < kTprsBlockSteps && !broke; ++s) {
       const double* Qs = Vd + static_cast<int64_t>(nu) * kTprsBlock * s;
-      for (int idx = tid; idx < kTprsBlock * ld; idx += blockDim.x) {
-        const int v = idx / ld, i = idx % ld;
-        q[v * ld_max + i] = i < nu ? Qs[static_cast<int64_t>(nu) * v + i] : 0.0;
-      }
-      for (int idx = tid; idx < kTprsWarps * kTprsBlock * ld; idx += blockDim.x) {
-        const int sl = idx / ld, i = idx % ld;
-        acc[static_cast<int64_t>(sl) * ld_max + i] = 0.0;
-      }
+      for (int v = warp; v < kTprsBlock; v += kTprsWarps)
+        for (int i = lane; i < ld; i += 32) q[v * ld_max + i] = i < nu ? Qs[static_cast<int64_t>(nu) * v + i] : 0.0;
       __syncthreads();
-      // W = E Q_s over the upper block triangle; slice (warp, v) at acc + (warp * 4 + v) * ld_max
-      double* my = acc + static_cast<int64_t>(warp) * kTprsBlock * ld_max;
-      for (int pidx = warp; 2 * pidx < nb; pidx += kTprsWarps) {
-        for (int half = 0; half < 2; ++half) {
-          const int J = half == 0 ? pidx : nb - 1 - pidx;
-          if (half == 1 && J == pidx) break;
-          const double* Ecol = E + static_cast<int64_t>(ld) * kTile * J;
-          double zc[kTprsBlock] = {0.0, 0.0, 0.0, 0.0};
-          for (int I = 0; I <= J; ++I) {
-            double e[kTile];
+      // W = E Q_s: warp w owns row blocks w, w + 8, ...; lane = row; E is read
+      // once per pass, far beyond L2: streaming loads keep the basis in L2
+      for (int I = warp; I < nb; I += kTprsWarps) {
+        double a0[kTprsBlock], a1[kTprsBlock];
 #pragma unroll
-            for (int c = 0; c < kTile; ++c) e[c] = __ldcs(Ecol + kTile * I + lane + static_cast<int64_t>(ld) * c);
+        for (int v = 0; v < kTprsBlock; ++v) a0[v] = a1[v] = 0.0;
+        const double* Erow = E + kTile * I + lane;
+        for (int J = 0; J < nb; ++J) {
+          double e[kTile];
 #pragma unroll
-            for (int v = 0; v < kTprsBlock; ++v) {
-              const double2* qv = reinterpret_cast<const double2*>(q + v * ld_max + kTile * J);
-              double r0 = 0.0, r1 = 0.0;
+          for (int c = 0; c < kTile; ++c) e[c] = __ldcs(Erow + static_cast<int64_t>(ld) * (kTile * J + c));
 #pragma unroll
-              for (int c = 0; c < kTile; c += 2) {
-                const double2 qq = qv[c / 2];
-                r0 += e[c] * qq.x;
-                r1 += e[c + 1] * qq.y;
-              }
-              my[v * ld_max + kTile * I + lane] += r0 + r1;
-            }
-            if (I < J) {
+          for (int v = 0; v < kTprsBlock; ++v) {
+            const double2* qv = reinterpret_cast<const double2*>(q + v * ld_max + kTile * J);
 #pragma unroll
-              for (int c = 0; c < kTile; ++c) tile[c * kTileLd + lane] = e[c];
-              __syncwarp();
-              const double2* trow2 = reinterpret_cast<const double2*>(tile + lane * kTileLd);
-#pragma unroll
-              for (int l = 0; l < kTile; l += 2) {
-                const double2 t = trow2[l / 2];
-                e[l] = t.x;
-                e[l + 1] = t.y;
-              }
-              __syncwarp();
-#pragma unroll
-              for (int v = 0; v < kTprsBlock; ++v) {
-                const double2* qv = reinterpret_cast<const double2*>(q + v * ld_max + kTile * I);
-                double c0 = 0.0, c1 = 0.0;
-#pragma unroll
-                for (int l = 0; l < kTile; l += 2) {
-                  const double2 qq = qv[l / 2];
-                  c0 += e[l] * qq.x;
-                  c1 += e[l + 1] * qq.y;
-                }
-                zc[v] += c0 + c1;
-              }
+            for (int c = 0; c < kTile; c += 2) {
+              const double2 qq = qv[c / 2];
+              a0[v] += e[c] * qq.x;
+              a1[v] += e[c + 1] * qq.y;
             }
           }
-#pragma unroll
-          for (int v = 0; v < kTprsBlock; ++v) my[v * ld_max + kTile * J + lane] += zc[v];
         }
-      }
-      __syncthreads();
-      // W (over Q_s, rows < nu) = sum over the warps' slices, fixed order
-      for (int idx = tid; idx < kTprsBlock * nu; idx += blockDim.x) {
-        const int v = idx / nu, i = idx % nu;
-        double sacc = 0.0;
+        const int row = kTile * I + lane;
 #pragma unroll
-        for (int w = 0; w < kTprsWarps; ++w) sacc += acc[(static_cast<int64_t>(w) * kTprsBlock + v) * ld_max + i];
-        W[v * ld_max + i] = sacc;
+        for (int v = 0; v < kTprsBlock; ++v) W[v * ld_max + row] = row < nu ? a0[v] + a1[v] : 0.0;
       }
       __syncthreads();
       const int used = kTprsBlock * (s + 1);
-      block_project(W, ld_max, nu, Vd, used, coef1);
+      block_project(W, ld_max, nu, Vd, used, coef1, stage);
       block_gram(W, ld_max, nu, red, G);
       if (tid == 0 && !chol4(G, R1, R1i)) broke = 1;
       __syncthreads();
       if (broke) break;
       block_scale(W, ld_max, nu, R1i);
-      block_project(W, ld_max, nu, Vd, used, coef2);
+      block_project(W, ld_max, nu, Vd, used, coef2, stage);
       block_gram(W, ld_max, nu, red, G);
       if (tid == 0 && !chol4(G, R2, R2i)) broke = 1;
       __syncthreads();
@@ -603,7 +578,8 @@ __global__ void __launch_bounds__(kTprsThreads, 1) tprs_block_lanczos_kernel(
       }
       if (s + 1 < kTprsBlockSteps) {
         double* vn = Vd + static_cast<int64_t>(nu) * kTprsBlock * (s + 1);
-        for (int idx = tid; idx < kTprsBlock * nu; idx += blockDim.x) vn[idx] = W[(idx / nu) * ld_max + idx % nu];
+        for (int v = warp; v < kTprsBlock; v += kTprsWarps)
+          for (int i = lane; i < nu; i += 32) vn[static_cast<int64_t>(nu) * v + i] = W[v * ld_max + i];
       }
       __syncthreads();
     }
@@ -638,82 +614,105 @@ constexpr int kRows = kTprsMaxSteps / 32;  // rows of an eigenvector matrix per 
 
 // Implicit QL with Wilkinson shifts on the symmetric tridiagonal (dd, ee;
 // ee[ms - 1] = 0), by one warp: eigenvalues into dd, the rotations applied to
-// the columns of z (ms rows, column stride ld; lane = row, column i + 1 carried
-// in registers from one rotation to the next).  false when an eigenvalue takes
-// more than 60 sweeps.
-__device__ bool tridiag_ql(double* dd, double* ee, double* z, int ms, int64_t ld, int lane) {
+// the columns of z (ms rows, column stride ld).  Lane 0 alone runs each
+// sweep's rotation chain on dd / ee and records the rotations in rc / rs;
+// the warp then applies them to z in the same order (lane = row, column i + 1
+// carried in registers from one rotation to the next), so the serial chain
+// carries no z traffic and no warp barrier per rotation.  ctl: three ints of
+// per-warp scratch.  false when an eigenvalue takes more than 60 sweeps.
+__device__ bool tridiag_ql(double* dd, double* ee, double* z, int ms, int64_t ld, double* rc, double* rs, int* ctl,
+                           int lane) {
   const double eps = 2.220446049250313e-16;
+  int iter = 0;  // lane 0's count for the current eigenvalue
   for (int l = 0; l < ms; ++l) {
-    int iter = 0;
+    if (lane == 0) iter = 0;
     for (;;) {
-      int mm = l;
-      for (; mm < ms - 1; ++mm) {
-        const double sum = fabs(dd[mm]) + fabs(dd[mm + 1]);
-        if (fabs(ee[mm]) <= eps * sum) break;
-      }
-      if (mm == l) break;
-      if (++iter > 60) return false;
-      double g = (dd[l + 1] - dd[l]) / (2.0 * ee[l]);
-      double r = hypot(g, 1.0);
-      g = dd[mm] - dd[l] + ee[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
-      double sn = 1.0, cs = 1.0, p = 0.0;
-      double carry[kRows];
-#pragma unroll
-      for (int t = 0; t < kRows; ++t) {
-        const int row = lane + 32 * t;
-        carry[t] = row < ms ? z[row + ld * mm] : 0.0;
-      }
-      int cur = mm;
-      int i = mm - 1;
-      bool split = false;
-      for (; i >= l; --i) {
-        const double ei = ee[i], di = dd[i], di1 = dd[i + 1];
-        const double f = sn * ei;
-        const double b = cs * ei;
-        // |(f, g)| without hypot's scaling: the tridiagonal's entries are far
-        // from the overflow range here (values of the scaled eta matrices)
-        const double rr = sqrt(f * f + g * g);
-        __syncwarp();  // every lane has read d and e before lane 0 writes them
-        if (rr == 0.0) {
-          if (lane == 0) {
-            ee[i + 1] = rr;
-            dd[i + 1] = di1 - p;
-            ee[mm] = 0.0;
-          }
-          split = true;
-          break;
+      if (lane == 0) {
+        int mm = l;
+        for (; mm < ms - 1; ++mm) {
+          const double sum = fabs(dd[mm]) + fabs(dd[mm + 1]);
+          if (fabs(ee[mm]) <= eps * sum) break;
         }
-        if (lane == 0) ee[i + 1] = rr;
-        const double rinv = 1.0 / rr;
-        sn = f * rinv;
-        cs = g * rinv;
-        g = di1 - p;
-        r = (di - g) * sn + 2.0 * cs * b;
-        p = sn * r;
-        if (lane == 0) dd[i + 1] = g + p;
-        g = cs * r - b;
+        int status = 0;  // 0: dd[l] converged, 1: sweep done, 2: sweep split, 3: no convergence
+        int lo = mm;     // the lowest column the sweep rotated
+        if (mm != l) {
+          if (++iter > 60) {
+            status = 3;
+          } else {
+            double g = (dd[l + 1] - dd[l]) / (2.0 * ee[l]);
+            double r = hypot(g, 1.0);
+            g = dd[mm] - dd[l] + ee[l] / (g + (g >= 0.0 ? fabs(r) : -fabs(r)));
+            double sn = 1.0, cs = 1.0, p = 0.0;
+            status = 1;
+            for (int i = mm - 1; i >= l; --i) {
+              const double ei = ee[i], di = dd[i], di1 = dd[i + 1];
+              const double f = sn * ei;
+              const double b = cs * ei;
+              // |(f, g)| without hypot's scaling (the tridiagonal's entries are far
+              // from the overflow range here: values of the scaled eta matrices),
+              // and its reciprocal from one reciprocal square root, the shortest
+              // dependent chain for the serial rotation sequence
+              const double h = f * f + g * g;
+              if (h == 0.0) {
+                ee[i + 1] = 0.0;
+                dd[i + 1] = di1 - p;
+                ee[mm] = 0.0;
+                status = 2;
+                break;
+              }
+              const double rinv = rsqrt(h);
+              ee[i + 1] = h * rinv;
+              sn = f * rinv;
+              cs = g * rinv;
+              g = di1 - p;
+              r = (di - g) * sn + 2.0 * cs * b;
+              p = sn * r;
+              dd[i + 1] = g + p;
+              g = cs * r - b;
+              rc[i] = cs;
+              rs[i] = sn;
+              lo = i;
+            }
+            if (status == 1) {
+              dd[l] -= p;
+              ee[l] = g;
+              ee[mm] = 0.0;
+            }
+          }
+        }
+        ctl[0] = status;
+        ctl[1] = mm;
+        ctl[2] = lo;
+      }
+      __syncwarp();
+      const int status = ctl[0], mm = ctl[1], lo = ctl[2];
+      __syncwarp();
+      if (status == 0) break;
+      if (status == 3) return false;
+      if (lo < mm) {
+        double carry[kRows];
 #pragma unroll
         for (int t = 0; t < kRows; ++t) {
           const int row = lane + 32 * t;
-          if (row < ms) {
-            const double zi = z[row + ld * i];
-            z[row + ld * (i + 1)] = sn * zi + cs * carry[t];
-            carry[t] = cs * zi - sn * carry[t];
+          carry[t] = row < ms ? z[row + ld * mm] : 0.0;
+        }
+        for (int i = mm - 1; i >= lo; --i) {
+          const double cs = rc[i], sn = rs[i];
+#pragma unroll
+          for (int t = 0; t < kRows; ++t) {
+            const int row = lane + 32 * t;
+            if (row < ms) {
+              const double zi = z[row + ld * i];
+              z[row + ld * (i + 1)] = sn * zi + cs * carry[t];
+              carry[t] = cs * zi - sn * carry[t];
+            }
           }
         }
-        cur = i;
-      }
 #pragma unroll
-      for (int t = 0; t < kRows; ++t) {
-        const int row = lane + 32 * t;
-        if (row < ms) z[row + ld * cur] = carry[t];
-      }
-      __syncwarp();
-      if (split) continue;
-      if (lane == 0) {
-        dd[l] -= p;
-        ee[l] = g;
-        ee[mm] = 0.0;
+        for (int t = 0; t < kRows; ++t) {
+          const int row = lane + 32 * t;
+          if (row < ms) z[row + ld * lo] = carry[t];
+        }
       }
       __syncwarp();
     }
@@ -765,7 +764,9 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
     int steps, int k, int zstride, double* __restrict__ vals, double* __restrict__ zsel, int* __restrict__ ok) {
   extern __shared__ double zsh[];  // steps x steps per warp
   __shared__ double dsh[kRitzWarps][kTprsMaxSteps], esh[kRitzWarps][kTprsMaxSteps];
+  __shared__ double rcsh[kRitzWarps][kTprsMaxSteps], rssh[kRitzWarps][kTprsMaxSteps];
   __shared__ int selsh[kRitzWarps][kTprsRitzMax];
+  __shared__ int ctlsh[kRitzWarps][4];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int d = blockIdx.x * (blockDim.x >> 5) + warp;
   if (d >= count) return;  // whole warps only: no block barrier follows
@@ -784,7 +785,7 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
   for (int c = 0; c < ms; ++c)
     for (int i = lane; i < ms; i += 32) z[i + ld * c] = i == c ? 1.0 : 0.0;
   __syncwarp();
-  if (ms < k || !tridiag_ql(dd, ee, z, ms, ld, lane)) {
+  if (ms < k || !tridiag_ql(dd, ee, z, ms, ld, rcsh[warp], rssh[warp], ctlsh[warp], lane)) {
     if (lane == 0) ok[d] = 0;
     return;
   }
@@ -801,24 +802,32 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
   if (lane == 0) ok[d] = conv ? 1 : 0;
 }
 
-// Ritz pairs of the block Lanczos runs (one warp per design).  T (104 x 104,
-// column stride 105 in shared memory) is assembled from the diagonal blocks
-// (A_s + A_s') / 2 and the couplings R_s; Householder reflections reduce it to
-// a tridiagonal (Golub and Van Loan, Matrix Computations, algorithm 8.3.1:
-// H_k = I - tau v v', v(k+1) = 1, stored below the subdiagonal of column k),
-// the product P = H_0 ... H_{m-3} is formed in place from the back, and the
-// implicit QL above rotates P's columns into T's eigenvectors.  The residual
-// of a Ritz pair (theta, y) is |R_last y_last| (y_last its rows of the last
-// block), accepted at 1e-14 max |theta| as for the single-vector runs.
+// Ritz pairs of the block Lanczos runs (one warp per design).  T = V'EV
+// (104 x 104, bandwidth 4: diagonal blocks (A_s + A_s')/2, couplings R_s) is
+// held as its band.  A single-vector Lanczos on T (full re-orthogonalisation,
+// two classical passes) from the host's deterministic start sequence reduces
+// it to a tridiagonal T' = P'TP of kTprsInnerSteps = 72 (P: 104 x 72, in a
+// per-design global workspace): on the 500 x 50 level's designs T's k = 30
+// pairs have converged to 1e-20 relative by then.  The implicit QL above
+// diagonalises T' (a 72-step rotation chain in place of a 104-step one); a
+// selected pair's eigenvector in the block basis is P s.  The residual of the
+// Ritz pair (theta, V P s) of E has two orthogonal parts, beta_72 s_72 (inside
+// the block Krylov space) and R_last (P s)_last (the block that would follow):
+// the pair is accepted when their root-sum-square is at most 1e-14 max|theta|.
+constexpr int kTprsInnerSteps = 72;
+constexpr int kTprsBand = 2 * kTprsBlock + 1;
+// per-warp dynamic shared memory (doubles): z, the band, p, w, coefficients, d / e / rotations
+constexpr int kRitzBlockWords = kTprsInnerSteps * kTprsInnerSteps + kTprsBlockDim * kTprsBand + 2 * kTprsBlockDim +
+                                kTprsInnerSteps + 4 * kTprsMaxSteps;
+
 __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel(
     const double* __restrict__ blocks, const int* __restrict__ done, int count, int k, int zstride,
-    double* __restrict__ vals, double* __restrict__ zsel, int* __restrict__ ok) {
-  extern __shared__ double zsh[];  // (m + 1) x m per warp
-  __shared__ double dsh[kRitzWarps][kTprsMaxSteps], esh[kRitzWarps][kTprsMaxSteps];
-  __shared__ double tsh[kRitzWarps][kTprsMaxSteps], wsh[kRitzWarps][kTprsMaxSteps];
-  __shared__ int selsh[kRitzWarps][kTprsRitzMax];
-  constexpr int m = kTprsBlockDim;
-  constexpr int64_t ld = m + 1;  // odd stride: a warp reading a row touches distinct banks
+    double* __restrict__ pws, double* __restrict__ vals, double* __restrict__ zsel, int* __restrict__ ok) {
+  extern __shared__ double rsh[];
+  __shared__ int selsh[kRitzWarps][kTprsRitzMax], possh[kRitzWarps][kTprsRitzMax];
+  __shared__ int ctlsh[kRitzWarps][4];
+  constexpr int m = kTprsBlockDim, ms2 = kTprsInnerSteps;
+  constexpr int kR = (m + 31) / 32;  // rows of T per lane
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int d = blockIdx.x * (blockDim.x >> 5) + warp;
   if (d >= count) return;  // whole warps only: no block barrier follows
@@ -826,137 +835,208 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel
     if (lane == 0) ok[d] = 0;
     return;
   }
-  double* dd = dsh[warp];
-  double* ee = esh[warp];
-  double* tau = tsh[warp];
-  double* wv = wsh[warp];
+  double* z = rsh + static_cast<int64_t>(warp) * kRitzBlockWords;  // ms2 x ms2
+  double* tb = z + ms2 * ms2;                                        // m x kTprsBand
+  double* pv = tb + m * kTprsBand;                                   // p_j
+  double* wv = pv + m;                                               // w
+  double* cf = wv + m;                                               // ms2 coefficients
+  double* dd = cf + ms2;
+  double* ee = dd + kTprsMaxSteps;
+  double* rc = ee + kTprsMaxSteps;
+  double* rs = rc + kTprsMaxSteps;
   int* sel = selsh[warp];
-  double* a = zsh + static_cast<int64_t>(warp) * ld * m;
+  int* pos = possh[warp];
+  double* P = pws + static_cast<int64_t>(d) * m * ms2;  // column-major, leading dimension m
   const double* blk = blocks + static_cast<int64_t>(d) * kTprsBlockSteps * 32;
-  for (int64_t idx = lane; idx < ld * m; idx += 32) a[idx] = 0.0;
+  // the band of T: tb[i * kTprsBand + (j - i + kTprsBlock)]
+  for (int idx = lane; idx < m * kTprsBand; idx += 32) tb[idx] = 0.0;
   __syncwarp();
   for (int s = 0; s < kTprsBlockSteps; ++s) {
     if (lane < 16) {
       const int r = lane & 3, c = lane >> 2;
-      a[(4 * s + r) + ld * (4 * s + c)] = 0.5 * (blk[32 * s + r + 4 * c] + blk[32 * s + c + 4 * r]);
+      const int i = 4 * s + r, j = 4 * s + c;
+      tb[i * kTprsBand + (j - i + kTprsBlock)] = 0.5 * (blk[32 * s + r + 4 * c] + blk[32 * s + c + 4 * r]);
       if (s + 1 < kTprsBlockSteps && r <= c) {
         const double rv = blk[32 * s + 16 + r + 4 * c];
-        a[(4 * (s + 1) + r) + ld * (4 * s + c)] = rv;
-        a[(4 * s + c) + ld * (4 * (s + 1) + r)] = rv;
+        const int i2 = 4 * (s + 1) + r;  // T(i2, j) = R_s(r, c) and its mirror
+        tb[i2 * kTprsBand + (j - i2 + kTprsBlock)] = rv;
+        tb[j * kTprsBand + (i2 - j + kTprsBlock)] = rv;
       }
     }
   }
-  __syncwarp();
-  // Householder tridiagonalisation: lanes over rows
-  for (int kk = 0; kk < m - 2; ++kk) {
-    const int r0 = kk + 1;
-    double* col = a + ld * kk;
-    double tail = 0.0;
-    for (int i = r0 + 1 + lane; i < m; i += 32) tail += col[i] * col[i];
-    tail = warp_sum_t(tail);
-    const double x0 = col[r0];
-    double t = 0.0, beta = x0;
-    if (tail > 0.0) {
-      const double nrm = sqrt(x0 * x0 + tail);
-      beta = x0 >= 0.0 ? -nrm : nrm;
-      t = (beta - x0) / beta;
-      const double scale = 1.0 / (x0 - beta);
-      for (int i = r0 + 1 + lane; i < m; i += 32) col[i] *= scale;
-    }
-    __syncwarp();
-    if (lane == 0) {
-      col[r0] = 1.0;
-      ee[kk] = beta;
-      tau[kk] = t;
-      dd[kk] = a[kk + ld * kk];
-    }
-    __syncwarp();
-    if (t != 0.0) {
-      // p = t A22 v; w = p - (t/2)(p.v) v; A22 -= v w' + w v'
-      double p[kRows];
-      double pv = 0.0;
-#pragma unroll
-      for (int tt = 0; tt < kRows; ++tt) {
-        const int row = r0 + lane + 32 * tt;
-        p[tt] = 0.0;
-        if (row < m) {
-          double acc = 0.0;
-          for (int j = r0; j < m; ++j) acc += a[row + ld * j] * col[j];
-          p[tt] = t * acc;
-          pv += p[tt] * col[row];
-        }
-      }
-      pv = warp_sum_t(pv);
-      const double kw = 0.5 * t * pv;
-#pragma unroll
-      for (int tt = 0; tt < kRows; ++tt) {
-        const int row = r0 + lane + 32 * tt;
-        if (row < m) wv[row] = p[tt] - kw * col[row];
-      }
-      __syncwarp();
-#pragma unroll
-      for (int tt = 0; tt < kRows; ++tt) {
-        const int row = r0 + lane + 32 * tt;
-        if (row < m) {
-          const double vr = col[row], wr = wv[row];
-          for (int j = r0; j < m; ++j) a[row + ld * j] -= vr * wv[j] + wr * col[j];
-        }
-      }
-      __syncwarp();
-    }
-  }
+  // start vector: the host's deterministic sequence, normalised
   if (lane == 0) {
-    dd[m - 2] = a[(m - 2) + ld * (m - 2)];
-    dd[m - 1] = a[(m - 1) + ld * (m - 1)];
-    ee[m - 2] = a[(m - 1) + ld * (m - 2)];
-    ee[m - 1] = 0.0;
-    a[(m - 1) + ld * (m - 1)] = 1.0;
+    unsigned long state = 1;
+    for (int i = 0; i < m; ++i) {
+      state = (state * 106UL + 1283UL) % 6075UL;
+      pv[i] = static_cast<double>(state) / 6075.0 - 0.5;
+    }
   }
   __syncwarp();
-  // P = H_0 ... H_{m-3}, from the back: before H_kk, row and column kk + 1
-  // of the trailing block become unit; H_kk then acts on rows kk + 1 .. m - 1
-  // (lanes over columns)
-  for (int kk = m - 3; kk >= -1; --kk) {
-    const int r0 = kk + 1;
-    for (int j = r0 + 1 + lane; j < m; j += 32) {
-      a[r0 + ld * j] = 0.0;
-      a[j + ld * r0] = 0.0;
+  double pr[kR], pp[kR];
+  {
+    double nrm = 0.0;
+#pragma unroll
+    for (int t = 0; t < kR; ++t) {
+      const int i = lane + 32 * t;
+      pr[t] = i < m ? pv[i] : 0.0;
+      nrm += pr[t] * pr[t];
     }
-    if (lane == 0) a[r0 + ld * r0] = 1.0;
-    __syncwarp();
-    if (kk < 0) break;
-    const double t = tau[kk];
-    if (t != 0.0) {
-      const double* v = a + ld * kk;
-      for (int j = r0 + lane; j < m; j += 32) {
-        double sdot = 0.0;
-        for (int i = r0; i < m; ++i) sdot += v[i] * a[i + ld * j];
-        sdot *= t;
-        for (int i = r0; i < m; ++i) a[i + ld * j] -= v[i] * sdot;
+    nrm = sqrt(warp_sum_t(nrm));
+#pragma unroll
+    for (int t = 0; t < kR; ++t) {
+      const int i = lane + 32 * t;
+      pr[t] /= nrm;
+      pp[t] = 0.0;
+      if (i < m) {
+        P[i] = pr[t];
+        pv[i] = pr[t];
       }
     }
+  }
+  __syncwarp();
+  double anorm = 0.0, bprev = 0.0;
+  int taken = 0;
+  for (int j = 0; j < ms2; ++j) {
+    double wr[kR];
+    double part = 0.0;
+#pragma unroll
+    for (int t = 0; t < kR; ++t) {
+      const int i = lane + 32 * t;
+      double y = 0.0;
+      if (i < m) {
+#pragma unroll
+        for (int b = -kTprsBlock; b <= kTprsBlock; ++b) {
+          const int jj = i + b;
+          if (jj >= 0 && jj < m) y += tb[i * kTprsBand + b + kTprsBlock] * pv[jj];
+        }
+      }
+      wr[t] = y;
+      part += pr[t] * y;
+    }
+    const double a = warp_sum_t(part);
+    double before = 0.0;
+#pragma unroll
+    for (int t = 0; t < kR; ++t) {
+      wr[t] -= a * pr[t] + bprev * pp[t];
+      before += wr[t] * wr[t];
+    }
+    // full re-orthogonalisation against P's columns 0 .. j, two classical passes
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int c = 0; c <= j; ++c) {
+        const double* pc = P + static_cast<int64_t>(m) * c;
+        double sdot = 0.0;
+#pragma unroll
+        for (int t = 0; t < kR; ++t) {
+          const int i = lane + 32 * t;
+          if (i < m) sdot += pc[i] * wr[t];
+        }
+        sdot = warp_sum_t(sdot);
+        if (lane == 0) cf[c] = sdot;
+      }
+      __syncwarp();
+      for (int c = 0; c <= j; ++c) {
+        const double* pc = P + static_cast<int64_t>(m) * c;
+        const double cc = cf[c];
+#pragma unroll
+        for (int t = 0; t < kR; ++t) {
+          const int i = lane + 32 * t;
+          if (i < m) wr[t] -= cc * pc[i];
+        }
+      }
+      __syncwarp();
+    }
+    double after = 0.0;
+#pragma unroll
+    for (int t = 0; t < kR; ++t) after += wr[t] * wr[t];
+    const double bj = sqrt(warp_sum_t(after));
+    anorm = fmax(anorm, fabs(a) + bj + bprev);
+    if (lane == 0) {
+      dd[j] = a;
+      ee[j] = bj;
+    }
+    taken = j + 1;
+    if (bj <= 1e-15 * anorm || j + 1 == ms2) break;
+    const double binv = 1.0 / bj;
+#pragma unroll
+    for (int t = 0; t < kR; ++t) {
+      const int i = lane + 32 * t;
+      pp[t] = pr[t];
+      pr[t] = wr[t] * binv;
+      if (i < m) {
+        P[i + static_cast<int64_t>(m) * (j + 1)] = pr[t];
+        pv[i] = pr[t];
+      }
+    }
+    bprev = bj;
     __syncwarp();
   }
-  if (!tridiag_ql(dd, ee, a, m, ld, lane)) {
+  __syncwarp();
+  const double blast = ee[taken - 1];
+  if (lane == 0) ee[taken - 1] = 0.0;
+  for (int c = 0; c < taken; ++c)
+    for (int i = lane; i < taken; i += 32) z[i + ms2 * c] = i == c ? 1.0 : 0.0;
+  __syncwarp();
+  if (taken < k || !tridiag_ql(dd, ee, z, taken, ms2, rc, rs, ctlsh[warp], lane)) {
     if (lane == 0) ok[d] = 0;
     return;
   }
-  const double tmax = select_largest(dd, m, k, sel, lane);
+  const double tmax = select_largest(dd, taken, k, sel, lane);
+  const bool invariant = fabs(blast) <= 1e-15 * tmax;
   const double* rl = blk + 32 * (kTprsBlockSteps - 1) + 16;  // R_last, upper triangular
   bool conv = true;
   for (int c = lane; c < k; c += 32) {
     const int i = sel[c];
-    const double* y = a + ld * i + (m - kTprsBlock);
-    double res = 0.0;
+    const double inner = invariant ? 0.0 : blast * z[(taken - 1) + ms2 * i];
+    double y[kTprsBlock];
+#pragma unroll
+    for (int r = 0; r < kTprsBlock; ++r) {
+      double acc = 0.0;
+      for (int b = 0; b < taken; ++b) acc += P[(m - kTprsBlock + r) + static_cast<int64_t>(m) * b] * z[b + ms2 * i];
+      y[r] = acc;
+    }
+    double outer = 0.0;
+#pragma unroll
     for (int r = 0; r < kTprsBlock; ++r) {
       double x = 0.0;
+#pragma unroll
       for (int w = r; w < kTprsBlock; ++w) x += rl[r + 4 * w] * y[w];
-      res += x * x;
+      outer += x * x;
     }
-    if (sqrt(res) > 1e-14 * tmax) conv = false;
+    if (sqrt(inner * inner + outer) > 1e-14 * tmax) conv = false;
+    // place by value, descending (ties to the lower selection rank)
+    const double vi = dd[i];
+    int ps = 0;
+    for (int e = 0; e < k; ++e) {
+      const double ve = dd[sel[e]];
+      ps += (ve > vi || (ve == vi && e < c)) ? 1 : 0;
+    }
+    pos[c] = ps;
+    vals[static_cast<int64_t>(d) * k + ps] = vi;
   }
   conv = __all_sync(0xffffffffu, conv);
-  write_ritz(dd, a, ld, m, k, sel, d, zstride, vals, zsel, lane);
+  __syncwarp();
+  // eigenvectors in the block basis: P s, lanes over rows
+  for (int c = 0; c < k; ++c) {
+    const int i = sel[c];
+    double* zc = zsel + (static_cast<int64_t>(d) * k + pos[c]) * zstride;
+    double acc[kR];
+#pragma unroll
+    for (int t = 0; t < kR; ++t) acc[t] = 0.0;
+    for (int b = 0; b < taken; ++b) {
+      const double zb = z[b + ms2 * i];
+#pragma unroll
+      for (int t = 0; t < kR; ++t) {
+        const int row = lane + 32 * t;
+        if (row < m) acc[t] += P[row + static_cast<int64_t>(m) * b] * zb;
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < kR; ++t) {
+      const int row = lane + 32 * t;
+      if (row < m) zc[row] = acc[t];
+    }
+  }
   if (lane == 0) ok[d] = conv ? 1 : 0;
 }
 
@@ -1070,19 +1150,23 @@ cudaError_t launch_tprs_ritz_select(const double* alpha, const double* beta, con
 }
 
 cudaError_t launch_tprs_ritz_block_select(const double* blocks, const int* done, int count, int k, int zstride,
-                                          double* vals, double* zsel, int* ok, cudaStream_t stream) {
+                                          double* pws, double* vals, double* zsel, int* ok, cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
   if (k != kTprsRitzMax || zstride < kTprsBlockDim) return cudaErrorInvalidValue;
-  const size_t per_warp = sizeof(double) * static_cast<size_t>(kTprsBlockDim + 1) * kTprsBlockDim;
-  int warps = static_cast<int>(kRitzSmemBudget / per_warp);
-  warps = warps < 1 ? 1 : (warps > kRitzWarps ? kRitzWarps : warps);
+  const size_t per_warp = sizeof(double) * static_cast<size_t>(kRitzBlockWords);
+  const int warps = kRitzWarps;
   const size_t smem = per_warp * warps;
   cudaError_t e = cudaFuncSetAttribute(tprs_ritz_block_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   tprs_ritz_block_select_kernel<<<(count + warps - 1) / warps, warps * 32, smem, stream>>>(blocks, done, count, k,
-                                                                                            zstride, vals, zsel, ok);
+                                                                                            zstride, pws, vals, zsel,
+                                                                                            ok);
   return cudaGetLastError();
+}
+
+size_t tprs_ritz_block_workspace(int count) {
+  return static_cast<size_t>(count) * kTprsBlockDim * kTprsInnerSteps;
 }
 
 cudaError_t launch_tprs_ritz_vectors(const double* V, const int64_t* voff, const int* nus, const int* done,
@@ -1426,7 +1510,7 @@ cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int*
 
 size_t tprs_block_smem_bytes(int nu_max) {
   const int64_t ld = tprs_ld(nu_max);
-  return sizeof(double) * static_cast<size_t>((1 + kTprsWarps) * kTprsBlock * ld + kTprsWarps * kTileWords);
+  return sizeof(double) * static_cast<size_t>((2 * kTprsBlock + kTprsStageCols) * ld);
 }
 
 cudaError_t launch_tprs_block_lanczos(const double* u, const int64_t* uoff, const int* nus, int count, int nu_max,

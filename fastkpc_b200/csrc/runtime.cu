@@ -355,7 +355,7 @@ void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int di
   const int cnt = static_cast<int>(batch->idx.size());
   const int nsingle = cnt - nblk;
   const int ctas = std::min(nsingle, ctas_per_sm * sms_);
-  const int ctas_blk = std::min(nblk, sms_);  // one CTA per SM (its shared memory)
+  const int ctas_blk = std::min(nblk, 2 * sms_);  // two CTAs per SM (their shared memory)
   const size_t nab = static_cast<size_t>(2) * nsingle * steps;
   const size_t nvals = static_cast<size_t>(cnt) * kk;
   const size_t ns = static_cast<size_t>(cnt) * (kk - 1) * (kk - 1);
@@ -410,7 +410,8 @@ void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int di
                                  tprs_eta0(dim), ews, ews_stride, ctas, dV, tb.voff.get() + nblk, dab,
                                  dab + static_cast<size_t>(nsingle) * steps, ddone + nblk, st),
              "thin-plate Lanczos");
-  cuda_check(launch_tprs_ritz_block_select(dblocks, ddone, nblk, kk, zstride, dvals, dzsel, dok, st),
+  cuda_check(launch_tprs_ritz_block_select(dblocks, ddone, nblk, kk, zstride,
+                                           tb.ritzp.ensure(tprs_ritz_block_workspace(nblk)), dvals, dzsel, dok, st),
              "thin-plate Ritz pairs");
   cuda_check(launch_tprs_ritz_select(dab, dab + static_cast<size_t>(nsingle) * steps, ddone + nblk, nsingle, steps,
                                      kk, zstride, dvals + static_cast<size_t>(nblk) * kk,

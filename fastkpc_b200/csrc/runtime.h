@@ -220,7 +220,7 @@ class Engine {
   // one set per smooth dimension (univariate, bivariate): both batches of a
   // level are in flight together
   struct TprsBuffers {
-    DevBuf<double> u, V, ab, blocks, ews, vals, zsel, U, S, colsq;
+    DevBuf<double> u, V, ab, blocks, ritzp, ews, vals, zsel, U, S, colsq;
     DevBuf<int64_t> uoff, voff, roff;
     DevBuf<int> nus, done, ok, map, status;
   };

@@ -29,6 +29,7 @@
 // depend on scheduling.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 
@@ -318,7 +319,8 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
 namespace {
 
 constexpr double kTprsBlockPivotTol = 1e-13;
-constexpr int kTprsStageCols = 16;  // basis columns staged in shared memory per projection chunk
+constexpr int kTprsStageCols = 16;  // basis columns staged in shared memory (two chunks)
+constexpr int kTprsChunk = kTprsStageCols / 2;
 
 // Gram matrix of the block W (4 x ld in shared memory, rows < nu) into G
 // (4 x 4, both triangles); every thread returns after G is in shared memory.
@@ -400,22 +402,77 @@ __device__ void block_scale(double* W, int ld, int nu, const double* Ri) {
   __syncthreads();
 }
 
-// One Gram-Schmidt pass of the block W against the basis columns 0 .. used-1
-// of Vd (nu rows), kTprsStageCols columns at a time staged through shared
-// memory (stage: kTprsStageCols x ld): coef[v * kTprsBlockDim + j] = V_j . W_v, W_v -= sum_j coef V_j, a
-// chunk's coefficients taken after the chunks before it are subtracted
-// (classical within a chunk, modified across chunks; the coefficients are
-// the amounts subtracted, so E Q_s = V C + W holds either way).
-__device__ void block_project(double* W, int ld, int nu, const double* Vd, int used, double* coef, double* stage) {
+// Asynchronous 16-byte copies global -> shared (cp.async, bypassing L1) with
+// an L2 eviction policy; the caller waits with cp_async_wait_all.
+__device__ __forceinline__ unsigned long long l2_evict_first_policy() {
+  unsigned long long pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(pol));
+  return pol;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, unsigned long long pol) {
+  const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(gmem), "l"(pol)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Tile (I, J) of E (32 x 32, column-major, leading dimension ld) into the
+// warp's buffer tbuf (column-major, 32 x 32): 16 copies of 16 bytes per lane.
+// E is read once per pass, far beyond L2: evict-first, so that the basis the
+// projections re-read stays.
+__device__ __forceinline__ void tile_prefetch(double* tbuf, const double* E, int ld, int I, int J, int lane,
+                                              unsigned long long pol) {
+  // lane: column (lane >> 4) + 2 t, rows 2 (lane & 15) and the next, for t < 16
+  const double* src = E + kTile * I + static_cast<int64_t>(ld) * (kTile * J + (lane >> 4)) + 2 * (lane & 15);
+  double* dst = tbuf + 2 * lane;
+  const int64_t step = 2 * static_cast<int64_t>(ld);
+#pragma unroll
+  for (int t = 0; t < 16; ++t) cp_async16(dst + 2 * kTile * t, src + step * t, pol);
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// One Gram-Schmidt pass of the block W (4 x ld in shared memory, rows < nu)
+// against the basis columns 0 .. used-1 of Vd (nu rows), then the Gram matrix
+// of the result into G (both triangles).  Chunks of kTprsChunk columns pass
+// through two shared-memory buffers (stage: 2 x kTprsChunk x ld) by
+// asynchronous copies, the next chunk in flight while the current one is
+// used: coef[v * kTprsBlockDim + j] = V_j . W_v, then W_v -= sum_j coef V_j.
+// A chunk's coefficients are taken after the chunks before it are subtracted
+// (classical within a chunk, modified across chunks; the coefficients are the
+// amounts subtracted, so E Q_s = V C + W holds either way).
+__device__ void block_project_gram(double* W, int ld, int nu, const double* Vd, int used, double* coef,
+                                   double* stage, double (*red)[10], double* G) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  for (int c0 = 0; c0 < used; c0 += kTprsStageCols) {
-    const int cn = used - c0 < kTprsStageCols ? used - c0 : kTprsStageCols;
-    const double* src = Vd + static_cast<int64_t>(nu) * c0;
+  const int nch = (used + kTprsChunk - 1) / kTprsChunk;
+  auto issue = [&](int ch) {
+    double* buf = stage + (ch & 1) * kTprsChunk * ld;
+    const int c0 = ch * kTprsChunk, cn = used - c0 < kTprsChunk ? used - c0 : kTprsChunk;
     for (int jj = warp; jj < cn; jj += kTprsWarps)
-      for (int i = lane; i < nu; i += 32) stage[jj * ld + i] = src[static_cast<int64_t>(nu) * jj + i];
+      for (int i = lane; i < nu; i += 32) cp_async8(buf + jj * ld + i, Vd + static_cast<int64_t>(nu) * (c0 + jj) + i);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  issue(0);
+  if (nch > 1) issue(1);
+  double g[10];
+#pragma unroll
+  for (int t = 0; t < 10; ++t) g[t] = 0.0;
+  for (int ch = 0; ch < nch; ++ch) {
+    if (ch + 1 < nch) cp_async_wait_one();
+    else cp_async_wait_all();
     __syncthreads();
+    const double* buf = stage + (ch & 1) * kTprsChunk * ld;
+    const int c0 = ch * kTprsChunk, cn = used - c0 < kTprsChunk ? used - c0 : kTprsChunk;
     for (int jj = warp; jj < cn; jj += kTprsWarps) {
-      const double* vj = stage + jj * ld;
+      const double* vj = buf + jj * ld;
       double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
       for (int i = lane; i < nu; i += 32) {
         const double x = vj[i];
@@ -436,10 +493,11 @@ __device__ void block_project(double* W, int ld, int nu, const double* Vd, int u
       }
     }
     __syncthreads();
+    const bool last = ch + 1 == nch;
     for (int i = tid; i < nu; i += blockDim.x) {
       double w0 = W[i], w1 = W[ld + i], w2 = W[2 * ld + i], w3 = W[3 * ld + i];
       for (int jj = 0; jj < cn; ++jj) {
-        const double x = stage[jj * ld + i];
+        const double x = buf[jj * ld + i];
         const int j = c0 + jj;
         w0 -= coef[j] * x;
         w1 -= coef[kTprsBlockDim + j] * x;
@@ -450,9 +508,37 @@ __device__ void block_project(double* W, int ld, int nu, const double* Vd, int u
       W[ld + i] = w1;
       W[2 * ld + i] = w2;
       W[3 * ld + i] = w3;
+      if (last) {
+        g[0] += w0 * w0;
+        g[1] += w0 * w1;
+        g[2] += w0 * w2;
+        g[3] += w0 * w3;
+        g[4] += w1 * w1;
+        g[5] += w1 * w2;
+        g[6] += w1 * w3;
+        g[7] += w2 * w2;
+        g[8] += w2 * w3;
+        g[9] += w3 * w3;
+      }
     }
     __syncthreads();
+    if (ch + 2 < nch) issue(ch + 2);
   }
+#pragma unroll
+  for (int t = 0; t < 10; ++t) {
+    const double sg = warp_sum_t(g[t]);
+    if (lane == 0) red[warp][t] = sg;
+  }
+  __syncthreads();
+  if (tid < 10) {
+    double sg = 0.0;
+    for (int w = 0; w < kTprsWarps; ++w) sg += red[w][tid];
+    const int u = tid < 4 ? 0 : (tid < 7 ? 1 : (tid < 9 ? 2 : 3));
+    const int v = u + (tid - (u == 0 ? 0 : (u == 1 ? 4 : (u == 2 ? 7 : 9))));
+    G[u + 4 * v] = sg;
+    G[v + 4 * u] = sg;
+  }
+  __syncthreads();
 }
 
 }  // namespace
@@ -470,7 +556,8 @@ __global__ void __launch_bounds__(kTprsThreads, 2) tprs_block_lanczos_kernel(
   const int warp = tid >> 5, lane = tid & 31;
   double* q = sm;                                                   // 4 x ld_max: Q_s, zero beyond nu
   double* W = q + kTprsBlock * static_cast<int64_t>(ld_max);         // 4 x ld_max: the new block
-  double* stage = W + kTprsBlock * static_cast<int64_t>(ld_max);     // kTprsStageCols x ld_max
+  double* stage = W + kTprsBlock * static_cast<int64_t>(ld_max);     // projections, then the warps' tile buffers
+  const unsigned long long pol = l2_evict_first_policy();
   for (int d = blockIdx.x; d < count; d += gridDim.x) {
     const int nu = nus[d];
     const int ld = static_cast<int>(tprs_ld(nu));
@@ -526,17 +613,27 @@ __global__ void __launch_bounds__(kTprsThreads, 2) tprs_block_lanczos_kernel(
       for (int v = warp; v < kTprsBlock; v += kTprsWarps)
         for (int i = lane; i < ld; i += 32) q[v * ld_max + i] = i < nu ? Qs[static_cast<int64_t>(nu) * v + i] : 0.0;
       __syncthreads();
-      // W = E Q_s: warp w owns row blocks w, w + 8, ...; lane = row; E is read
-      // once per pass, far beyond L2: streaming loads keep the basis in L2
-      for (int I = warp; I < nb; I += kTprsWarps) {
+      // W = E Q_s: warp w owns row blocks w, w + 8, ...; lane = row.  The
+      // warp's 32 x 32 tiles stream through its own shared-memory buffer: the
+      // asynchronous copy of the next tile runs while the current one is
+      // summed from registers
+      {
+        double* tbuf = stage + warp * kTile * kTile;
+        const int nI = warp < nb ? (nb - 1 - warp) / kTprsWarps + 1 : 0;
+        const int ntile = nI * nb;
+        if (ntile > 0) tile_prefetch(tbuf, E, ld, warp, 0, lane, pol);
         double a0[kTprsBlock], a1[kTprsBlock];
 #pragma unroll
         for (int v = 0; v < kTprsBlock; ++v) a0[v] = a1[v] = 0.0;
-        const double* Erow = E + kTile * I + lane;
-        for (int J = 0; J < nb; ++J) {
+        for (int t = 0; t < ntile; ++t) {
+          const int I = warp + kTprsWarps * (t / nb), J = t % nb;
+          cp_async_wait_all();
+          __syncwarp();
           double e[kTile];
 #pragma unroll
-          for (int c = 0; c < kTile; ++c) e[c] = __ldcs(Erow + static_cast<int64_t>(ld) * (kTile * J + c));
+          for (int c = 0; c < kTile; ++c) e[c] = tbuf[c * kTile + lane];
+          __syncwarp();
+          if (t + 1 < ntile) tile_prefetch(tbuf, E, ld, warp + kTprsWarps * ((t + 1) / nb), (t + 1) % nb, lane, pol);
 #pragma unroll
           for (int v = 0; v < kTprsBlock; ++v) {
             const double2* qv = reinterpret_cast<const double2*>(q + v * ld_max + kTile * J);
@@ -547,21 +644,24 @@ __global__ void __launch_bounds__(kTprsThreads, 2) tprs_block_lanczos_kernel(
               a1[v] += e[c + 1] * qq.y;
             }
           }
-        }
-        const int row = kTile * I + lane;
+          if (J == nb - 1) {
+            const int row = kTile * I + lane;
 #pragma unroll
-        for (int v = 0; v < kTprsBlock; ++v) W[v * ld_max + row] = row < nu ? a0[v] + a1[v] : 0.0;
+            for (int v = 0; v < kTprsBlock; ++v) {
+              W[v * ld_max + row] = row < nu ? a0[v] + a1[v] : 0.0;
+              a0[v] = a1[v] = 0.0;
+            }
+          }
+        }
       }
       __syncthreads();
       const int used = kTprsBlock * (s + 1);
-      block_project(W, ld_max, nu, Vd, used, coef1, stage);
-      block_gram(W, ld_max, nu, red, G);
+      block_project_gram(W, ld_max, nu, Vd, used, coef1, stage, red, G);
       if (tid == 0 && !chol4(G, R1, R1i)) broke = 1;
       __syncthreads();
       if (broke) break;
       block_scale(W, ld_max, nu, R1i);
-      block_project(W, ld_max, nu, Vd, used, coef2, stage);
-      block_gram(W, ld_max, nu, red, G);
+      block_project_gram(W, ld_max, nu, Vd, used, coef2, stage, red, G);
       if (tid == 0 && !chol4(G, R2, R2i)) broke = 1;
       __syncthreads();
       if (broke) break;
@@ -1510,7 +1610,8 @@ cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int*
 
 size_t tprs_block_smem_bytes(int nu_max) {
   const int64_t ld = tprs_ld(nu_max);
-  return sizeof(double) * static_cast<size_t>((2 * kTprsBlock + kTprsStageCols) * ld);
+  const int64_t stage = std::max<int64_t>(kTprsStageCols * ld, kTprsWarps * kTile * kTile);
+  return sizeof(double) * static_cast<size_t>(2 * kTprsBlock * ld + stage);
 }
 
 cudaError_t launch_tprs_block_lanczos(const double* u, const int64_t* uoff, const int* nus, int count, int nu_max,

@@ -916,9 +916,9 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
 // the pair is accepted when their root-sum-square is at most 1e-14 max|theta|.
 constexpr int kTprsInnerSteps = 72;
 constexpr int kTprsBand = 2 * kTprsBlock + 1;
-// per-warp dynamic shared memory (doubles): z, the band, p, w, coefficients, d / e / rotations
+// per-warp dynamic shared memory (doubles): z, the band, p, w, d / e / rotations
 constexpr int kRitzBlockWords = kTprsInnerSteps * kTprsInnerSteps + kTprsBlockDim * kTprsBand + 2 * kTprsBlockDim +
-                                kTprsInnerSteps + 4 * kTprsMaxSteps;
+                                4 * kTprsMaxSteps;
 
 __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel(
     const double* __restrict__ blocks, const int* __restrict__ done, int count, int k, int zstride,
@@ -939,8 +939,7 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel
   double* tb = z + ms2 * ms2;                                        // m x kTprsBand
   double* pv = tb + m * kTprsBand;                                   // p_j
   double* wv = pv + m;                                               // w
-  double* cf = wv + m;                                               // ms2 coefficients
-  double* dd = cf + ms2;
+  double* dd = wv + m;
   double* ee = dd + kTprsMaxSteps;
   double* rc = ee + kTprsMaxSteps;
   double* rs = rc + kTprsMaxSteps;
@@ -1021,30 +1020,32 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel
       wr[t] -= a * pr[t] + bprev * pp[t];
       before += wr[t] * wr[t];
     }
-    // full re-orthogonalisation against P's columns 0 .. j, two classical passes
+    // full re-orthogonalisation against P's columns 0 .. j, two passes, eight
+    // columns at a time: their entries of this lane's rows held in registers,
+    // the eight dot products reduced together (every lane gets the sums),
+    // then subtracted (classical within a group of eight, modified across)
     for (int pass = 0; pass < 2; ++pass) {
-      for (int c = 0; c <= j; ++c) {
-        const double* pc = P + static_cast<int64_t>(m) * c;
-        double sdot = 0.0;
+      for (int c0 = 0; c0 <= j; c0 += 8) {
+        double pcv[8][kR];
+        double sd[8];
 #pragma unroll
-        for (int t = 0; t < kR; ++t) {
-          const int i = lane + 32 * t;
-          if (i < m) sdot += pc[i] * wr[t];
-        }
-        sdot = warp_sum_t(sdot);
-        if (lane == 0) cf[c] = sdot;
-      }
-      __syncwarp();
-      for (int c = 0; c <= j; ++c) {
-        const double* pc = P + static_cast<int64_t>(m) * c;
-        const double cc = cf[c];
+        for (int u = 0; u < 8; ++u) {
+          const int c = c0 + u;
+          sd[u] = 0.0;
 #pragma unroll
-        for (int t = 0; t < kR; ++t) {
-          const int i = lane + 32 * t;
-          if (i < m) wr[t] -= cc * pc[i];
+          for (int t = 0; t < kR; ++t) {
+            const int i = lane + 32 * t;
+            pcv[u][t] = (c <= j && i < m) ? P[i + static_cast<int64_t>(m) * c] : 0.0;
+            sd[u] += pcv[u][t] * wr[t];
+          }
         }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) sd[u] = warp_sum_t(sd[u]);
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+          for (int t = 0; t < kR; ++t) wr[t] -= sd[u] * pcv[u][t];
       }
-      __syncwarp();
     }
     double after = 0.0;
 #pragma unroll

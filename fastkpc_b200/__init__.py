@@ -157,6 +157,8 @@ _SIGNATURES = {
     "fkpc_gamma_q_eval": (ctypes.c_int, [ctypes.c_int, _DBL, _DBL, ctypes.c_int, _DBL, _INT]),
     "fkpc_permutation_tables": (ctypes.c_int, [ctypes.c_uint, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                _INT]),
+    "fkpc_tprs_export": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        _INT, _INT, _INT, _DBL, _DBL]),
     "fkpc_get_tuning": (ctypes.c_int, [ctypes.c_int, _P(Tuning)]),
     "fkpc_set_tuning": (ctypes.c_int, [ctypes.c_int, _P(Tuning)]),
     "fkpc_batch_prepare": (ctypes.c_int, [_DBL, ctypes.c_int, ctypes.c_int, _INT, _INT, _INT, _INT, ctypes.c_int,
@@ -668,6 +670,25 @@ def regress_batch(data, fits, max_penalties=None, device=0, selection="magic"):
                                                _ptr(lsp, ctypes.c_double), max_penalties,
                                                _ptr(status, ctypes.c_int)))
     return resid, lsp, status
+
+
+def tprs_export(data, a, b, device=0):
+    """The device thin-plate set-up of the bivariate smooth on columns {a, b}:
+    dict(n_u, path ("block", "single" or None when the device does not take
+    it), ok, values (30, descending), vectors (n_u x 30, unit norm, largest
+    entry positive))."""
+    X = np.asfortranarray(data, dtype=np.float64)
+    n, p = X.shape
+    nu, path, ok = (ctypes.c_int(0) for _ in range(3))
+    vals = np.zeros(30)
+    vecs = np.zeros(n * 30)
+    _check(load_library().fkpc_tprs_export(_ptr(X, ctypes.c_double), n, p, int(a), int(b), int(device),
+                                           ctypes.byref(nu), ctypes.byref(path), ctypes.byref(ok),
+                                           _ptr(vals, ctypes.c_double), _ptr(vecs, ctypes.c_double)))
+    names = {0: None, 1: "single", 2: "block"}
+    k = nu.value
+    return {"n_u": k, "path": names[path.value], "ok": bool(ok.value), "values": vals,
+            "vectors": vecs[:k * 30].reshape(30, k).T.copy() if path.value else None}
 
 
 def permutation_tables(seed, ci_method, n, replicates, count):

@@ -883,6 +883,23 @@ int fkpc_design_export(const double* data, int n, int p, const int* s_values, in
   });
 }
 
+int fkpc_tprs_export(const double* data, int n, int p, int a, int b, int device, int* n_u, int* path, int* ok,
+                     double* values, double* vectors) {
+  return guarded([&]() {
+    if (!data || !n_u || !path || !ok || !values || !vectors)
+      throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "null argument");
+    if (n <= 5 || p < 2) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "data must be n x p with n > 5, p >= 2");
+    if (device < 0) throw fkpc::Error(FKPC_STATUS_INVALID_ARGUMENT, "device must be a CUDA device ordinal");
+    std::lock_guard<std::mutex> lock(device_mutex(device));
+    auto& eng = engine_for(device);
+    eng.load(data, n, p);
+    std::vector<double> vals, U;
+    eng.tprs_export(a, b, n_u, path, ok, &vals, &U);
+    std::copy(vals.begin(), vals.end(), values);
+    std::copy(U.begin(), U.end(), vectors);
+  });
+}
+
 int fkpc_gcv_adjoint(const double* data, int n, int p, int target, const int* s_values, int s_count, int count,
                      const double* log_lambda, double* score, double* grad, double* gn_hessian,
                      double* exact_hessian, int device) {

@@ -432,6 +432,37 @@ void Engine::launch_tprs_batch(const std::vector<std::vector<int>>& sets, int di
   cuda_check(cudaEventRecord(ev_[dim == 2 ? 6 : 7], st), "event");
 }
 
+void Engine::tprs_export(int a, int b, int* nu, int* path, int* ok, std::vector<double>* vals,
+                         std::vector<double>* U) {
+  if (a < 0 || b < 0 || a >= p_ || b >= p_ || a == b)
+    throw Error(FKPC_STATUS_INVALID_ARGUMENT, "a bivariate smooth needs two distinct columns of the data");
+  release_graph();
+  cuda_check(cudaStreamSynchronize(stream_), "set-up");
+  stage_reset();
+  TprsBatch batch;
+  launch_tprs_batch({{std::min(a, b), std::max(a, b)}}, 2, &batch, stream_, tuning_.tprs_ctas_per_sm);
+  *nu = batch.preps.empty() ? 0 : batch.preps[0].nu;
+  *path = 0;
+  *ok = 0;
+  vals->clear();
+  U->clear();
+  if (batch.idx.empty()) {
+    cuda_check(cudaStreamSynchronize(stream_), "thin-plate set-up");
+    return;
+  }
+  const int n_u = batch.nus[0];
+  *path = n_u >= kTprsBlockMinNu && tprs_ld(n_u) <= kTprsBlockMaxLd ? 2 : 1;
+  TprsBuffers& tb = tprs_buf_[1];
+  vals->assign(kTprsK, 0.0);
+  U->assign(static_cast<size_t>(n_u) * kTprsK, 0.0);
+  cuda_check(cudaMemcpyAsync(ok, tb.ok.get(), sizeof(int), cudaMemcpyDeviceToHost, stream_), "download");
+  cuda_check(cudaMemcpyAsync(vals->data(), tb.vals.get(), sizeof(double) * kTprsK, cudaMemcpyDeviceToHost, stream_),
+             "download");
+  cuda_check(cudaMemcpyAsync(U->data(), tb.U.get(), sizeof(double) * U->size(), cudaMemcpyDeviceToHost, stream_),
+             "download");
+  cuda_check(cudaStreamSynchronize(stream_), "thin-plate set-up");
+}
+
 void Engine::finish_tprs_batch(TprsBatch* batch) {
   if (batch->idx.empty()) return;
   const int dim = batch->dim;

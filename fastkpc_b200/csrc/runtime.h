@@ -94,6 +94,12 @@ class Engine {
   void regress(const std::vector<int>& targets, const std::vector<std::vector<int>>& sets,
                double* residuals, double* log_sp, int max_penalties, int* status,
                int selection = FKPC_SELECT_MAGIC, int* evaluations = nullptr);
+  // The device thin-plate set-up of the bivariate smooth on {a, b} alone:
+  // its k = 30 Ritz values (descending) and vectors (nu x 30, normalised,
+  // largest-magnitude entry positive).  path: 2 block Lanczos, 1
+  // single-vector, 0 not taken by the device (too few or too many unique
+  // locations); ok: the Ritz pairs converged.
+  void tprs_export(int a, int b, int* nu, int* path, int* ok, std::vector<double>* vals, std::vector<double>* U);
   // Statistics only, on caller residual columns.
   void statistics(const double* residuals, int m, const std::vector<int>& left, const std::vector<int>& right,
                   const int* permutations, const fkpc_options& opt, fkpc_ci_record* out);

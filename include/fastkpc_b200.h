@@ -427,6 +427,20 @@ FKPC_API int fkpc_design_export(const double* data_colmajor, int n, int p,
                                 double* initial_log_sp);
 
 /*
+ * The device thin-plate set-up of the bivariate smooth on columns {a, b}
+ * (k = 30), for checking the device eigensolvers: n_u (the unique
+ * locations), path (2: block Lanczos, taken when 120 <= n_u <= 512; 1:
+ * single-vector Lanczos; 0: not taken by the device, values and vectors
+ * untouched), ok (1 when the Ritz pairs converged), the 30 Ritz values of
+ * the eta matrix of largest magnitude in descending order and their vectors
+ * (n_u x 30 column-major, each of unit norm with its largest-magnitude entry
+ * positive; ``vectors`` holds at least n x 30 doubles).  The eigen problem of
+ * fastkpc/src/full_cuda_ci_native_setup.cpp:114-152 (Lanczos at :303).
+ */
+FKPC_API int fkpc_tprs_export(const double* data_colmajor, int n, int p, int a, int b, int device, int* n_u,
+                              int* path, int* ok, double* values, double* vectors);
+
+/*
  * Exact-screen dcc.gamma records for ``count`` pairs without allocating any
  * device memory, for callers that cannot call cudaMalloc -- code running
  * inside a host framework that owns every device allocation, or that must

@@ -1134,12 +1134,16 @@ void Engine::run_batch(const std::vector<Test>& tests, const fkpc_options& opt, 
     std::vector<std::vector<int>> bivariate;
     for (const auto& S : sets_)
       if (S.size() == 2 && !cache_->has_design(S)) bivariate.push_back(S);
-    // Both thin-plate batches on the main stream: the Lanczos kernels are
-    // persistent and hold every SM, so on a second stream they would delay
-    // the multi-penalty fits rather than run beside them.
+    // The univariate thin-plate batch (one CTA per variable: a third of the
+    // SMs at p = 50) on the side stream, beside the bivariate one on the main
+    // stream; the host waits for it before it builds the additive descriptors,
+    // so everything the main stream queues after that sees its bases.  The
+    // bivariate kernels stay on the main stream ahead of the fits: they hold
+    // every SM, so on a second stream they would delay the multi-penalty fits
+    // rather than run beside them.
     TprsBatch ubatch, batch;
     auto tp = std::chrono::steady_clock::now();
-    launch_tprs_batch(univariate_columns(), 1, &ubatch, stream_, tuning_.tprs_ctas_per_sm);
+    launch_tprs_batch(univariate_columns(), 1, &ubatch, side_, tuning_.tprs_ctas_per_sm);
     if (!bivariate.empty()) launch_tprs_batch(bivariate, 2, &batch, stream_, tuning_.tprs_ctas_per_sm);
     tprs_host_ms_ = ms_since(tp);
     auto tw = std::chrono::steady_clock::now();

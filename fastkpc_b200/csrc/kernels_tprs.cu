@@ -321,6 +321,19 @@ namespace {
 constexpr double kTprsBlockPivotTol = 1e-13;
 constexpr int kTprsStageCols = 16;  // basis columns staged in shared memory (two chunks)
 constexpr int kTprsChunk = kTprsStageCols / 2;
+// Column stride of a warp's tile buffer: 36 doubles keeps the buffer's rows
+// 16-byte aligned for the asynchronous copies, and the tensor-core fragment
+// reads (lane (g, t) reads row 8 m + g of column 4 k + t) conflict-free.
+constexpr int kTileBufLd = 36;
+
+// D += A B on the FP64 tensor pipe: mma.m8n8k4, A 8 x 4 (row), B 4 x 8 (col);
+// lane (g, t) = (lane >> 2, lane & 3) holds A(g, t), B(t, g) and D(g, 2t),
+// D(g, 2t + 1).
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
 
 // Gram matrix of the block W (4 x ld in shared memory, rows < nu) into G
 // (4 x 4, both triangles); every thread returns after G is in shared memory.
@@ -419,17 +432,18 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, unsigne
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Tile (I, J) of E (32 x 32, column-major, leading dimension ld) into the
-// warp's buffer tbuf (column-major, 32 x 32): 16 copies of 16 bytes per lane.
+// warp's buffer tbuf (column-major, column stride kTileBufLd): 16 copies of
+// 16 bytes per lane.
 // E is read once per pass, far beyond L2: evict-first, so that the basis the
 // projections re-read stays.
 __device__ __forceinline__ void tile_prefetch(double* tbuf, const double* E, int ld, int I, int J, int lane,
                                               unsigned long long pol) {
   // lane: column (lane >> 4) + 2 t, rows 2 (lane & 15) and the next, for t < 16
   const double* src = E + kTile * I + static_cast<int64_t>(ld) * (kTile * J + (lane >> 4)) + 2 * (lane & 15);
-  double* dst = tbuf + 2 * lane;
+  double* dst = tbuf + kTileBufLd * (lane >> 4) + 2 * (lane & 15);
   const int64_t step = 2 * static_cast<int64_t>(ld);
 #pragma unroll
-  for (int t = 0; t < 16; ++t) cp_async16(dst + 2 * kTile * t, src + step * t, pol);
+  for (int t = 0; t < 16; ++t) cp_async16(dst + 2 * kTileBufLd * t, src + step * t, pol);
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
@@ -613,44 +627,50 @@ __global__ void __launch_bounds__(kTprsThreads, 2) tprs_block_lanczos_kernel(
       for (int v = warp; v < kTprsBlock; v += kTprsWarps)
         for (int i = lane; i < ld; i += 32) q[v * ld_max + i] = i < nu ? Qs[static_cast<int64_t>(nu) * v + i] : 0.0;
       __syncthreads();
-      // W = E Q_s: warp w owns row blocks w, w + 8, ...; lane = row.  The
-      // warp's 32 x 32 tiles stream through its own shared-memory buffer: the
-      // asynchronous copy of the next tile runs while the current one is
-      // summed from registers
+      // W = E Q_s: warp w owns row blocks w, w + 8, ...  The warp's 32 x 32
+      // tiles stream through its own shared-memory buffer: the asynchronous
+      // copy of the next tile runs while the current one is multiplied.  A
+      // tile times the block's rows of Q_s (32 x 4, padded to 8 columns) is
+      // 4 x 8 mma.m8n8k4 on the FP64 tensor pipe: 8-row sub-blocks mt, 4-column
+      // steps ks; lane (g, t) accumulates rows 8 mt + g of vectors 2t, 2t + 1
       {
-        double* tbuf = stage + warp * kTile * kTile;
+        double* tbuf = stage + warp * kTile * kTileBufLd;
+        const int g = lane >> 2, tg = lane & 3;
         const int nI = warp < nb ? (nb - 1 - warp) / kTprsWarps + 1 : 0;
         const int ntile = nI * nb;
         if (ntile > 0) tile_prefetch(tbuf, E, ld, warp, 0, lane, pol);
-        double a0[kTprsBlock], a1[kTprsBlock];
+        double acc[4][2];
 #pragma unroll
-        for (int v = 0; v < kTprsBlock; ++v) a0[v] = a1[v] = 0.0;
+        for (int mt = 0; mt < 4; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
         for (int t = 0; t < ntile; ++t) {
           const int I = warp + kTprsWarps * (t / nb), J = t % nb;
           cp_async_wait_all();
           __syncwarp();
-          double e[kTile];
+          double af[4][8];
 #pragma unroll
-          for (int c = 0; c < kTile; ++c) e[c] = tbuf[c * kTile + lane];
+          for (int ks = 0; ks < 8; ++ks)
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt) af[mt][ks] = tbuf[(4 * ks + tg) * kTileBufLd + 8 * mt + g];
           __syncwarp();
           if (t + 1 < ntile) tile_prefetch(tbuf, E, ld, warp + kTprsWarps * ((t + 1) / nb), (t + 1) % nb, lane, pol);
+          const double* qJ = q + g * ld_max + kTile * J + tg;
 #pragma unroll
-          for (int v = 0; v < kTprsBlock; ++v) {
-            const double2* qv = reinterpret_cast<const double2*>(q + v * ld_max + kTile * J);
+          for (int ks = 0; ks < 8; ++ks) {
+            const double bf = g < kTprsBlock ? qJ[4 * ks] : 0.0;
 #pragma unroll
-            for (int c = 0; c < kTile; c += 2) {
-              const double2 qq = qv[c / 2];
-              a0[v] += e[c] * qq.x;
-              a1[v] += e[c + 1] * qq.y;
-            }
+            for (int mt = 0; mt < 4; ++mt) dmma_m8n8k4(acc[mt][0], acc[mt][1], af[mt][ks], bf);
           }
           if (J == nb - 1) {
-            const int row = kTile * I + lane;
+            if (tg < kTprsBlock / 2) {
 #pragma unroll
-            for (int v = 0; v < kTprsBlock; ++v) {
-              W[v * ld_max + row] = row < nu ? a0[v] + a1[v] : 0.0;
-              a0[v] = a1[v] = 0.0;
+              for (int mt = 0; mt < 4; ++mt) {
+                const int row = kTile * I + 8 * mt + g;
+                W[(2 * tg) * ld_max + row] = row < nu ? acc[mt][0] : 0.0;
+                W[(2 * tg + 1) * ld_max + row] = row < nu ? acc[mt][1] : 0.0;
+              }
             }
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
           }
         }
       }
@@ -1611,7 +1631,7 @@ cudaError_t launch_tprs_lanczos(const double* u, const int64_t* uoff, const int*
 
 size_t tprs_block_smem_bytes(int nu_max) {
   const int64_t ld = tprs_ld(nu_max);
-  const int64_t stage = std::max<int64_t>(kTprsStageCols * ld, kTprsWarps * kTile * kTile);
+  const int64_t stage = std::max<int64_t>(kTprsStageCols * ld, kTprsWarps * kTile * kTileBufLd);
   return sizeof(double) * static_cast<size_t>(2 * kTprsBlock * ld + stage);
 }
 

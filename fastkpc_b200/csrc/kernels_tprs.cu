@@ -936,7 +936,7 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
 // the pair is accepted when their root-sum-square is at most 1e-14 max|theta|.
 constexpr int kTprsInnerSteps = 72;
 constexpr int kTprsBand = 2 * kTprsBlock + 1;
-// per-warp dynamic shared memory (doubles): z, the band, p, w, d / e / rotations
+// per-warp dynamic shared memory (doubles): z, the band, p and a spare vector, d / e / rotations
 constexpr int kRitzBlockWords = kTprsInnerSteps * kTprsInnerSteps + kTprsBlockDim * kTprsBand + 2 * kTprsBlockDim +
                                 4 * kTprsMaxSteps;
 
@@ -958,8 +958,7 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel
   double* z = rsh + static_cast<int64_t>(warp) * kRitzBlockWords;  // ms2 x ms2
   double* tb = z + ms2 * ms2;                                        // m x kTprsBand
   double* pv = tb + m * kTprsBand;                                   // p_j
-  double* wv = pv + m;                                               // w
-  double* dd = wv + m;
+  double* dd = pv + 2 * m;                                           // (a spare m doubles after p)
   double* ee = dd + kTprsMaxSteps;
   double* rc = ee + kTprsMaxSteps;
   double* rs = rc + kTprsMaxSteps;

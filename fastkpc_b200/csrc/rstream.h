@@ -38,15 +38,22 @@ class RStream {
     return x;
   }
 
+  // R_unif_index(dn) under sample.kind "Rejection".  unif_rand() is y 2^-32
+  // for the tempered word y (y = 0 lifted to 2^-33), so floor(u 65536), R's
+  // 16-bit chunk, is exactly y >> 16: the chunks come straight from the words.
   int unif_index(int dn) {
     if (dn <= 0) return 0;
     // ceil(log2(dn)) as R computes it in double, exact for every int dn >= 1:
     // the bit length of dn - 1
     const int bits = dn == 1 ? 0 : 32 - __builtin_clz(static_cast<unsigned>(dn - 1));
+    const int64_t mask = (static_cast<int64_t>(1) << bits) - 1;
     for (;;) {
       int64_t v = 0;
-      for (int k = 0; k <= bits; k += 16) v = 65536 * v + static_cast<int64_t>(std::floor(unif_rand() * 65536.0));
-      v &= (static_cast<int64_t>(1) << bits) - 1;
+      for (int k = 0; k <= bits; k += 16) {
+        ++draws_;
+        v = 65536 * v + static_cast<int64_t>(genword() >> 16);
+      }
+      v &= mask;
       if (v < dn) return static_cast<int>(v);
     }
   }
@@ -70,14 +77,24 @@ class RStream {
   // exchanges entries j and n - 1 - k of one vector carried from replicate
   // to replicate; hsic.perm: draw i takes R_unif_index(n - i) from a pool
   // that each replicate starts afresh.
+  // floor(u m) for u = y 2^-32 is (y m) >> 32 while y m stays below 2^53
+  // (m < 2^21): the product and its scaling are exact in double (y = 0, lifted
+  // to 2^-33, gives 0 either way).
   void dcc_swaps(int n, int replicates, int* out) {
+    const bool exact = n < (1 << 21);
     for (int r = 0; r < replicates; ++r) {
       int* row = out + static_cast<int64_t>(r) * n;
       int remaining = n;
       for (int k = 0; k < n - 1; ++k) {
-        int j = static_cast<int>(std::floor(unif_rand() * remaining));
-        if (j < 0) j = 0;
-        if (j >= remaining) j = remaining - 1;
+        int j;
+        if (exact) {
+          ++draws_;
+          j = static_cast<int>((static_cast<uint64_t>(genword()) * static_cast<uint64_t>(remaining)) >> 32);
+        } else {
+          j = static_cast<int>(std::floor(unif_rand() * remaining));
+          if (j < 0) j = 0;
+          if (j >= remaining) j = remaining - 1;
+        }
         --remaining;
         row[k] = j;
       }
@@ -100,10 +117,25 @@ class RStream {
       for (int i = 0; i < n; ++i) row[i] = perm[i];
     }
   }
+  // hsic.perm's draws word by word, without a branch on the rejection: every
+  // word is written to the current slot and the slot advances when the word
+  // is accepted (R_unif_index(dn) takes one word per attempt while dn <= 2^15).
   void hsic_draws(int n, int replicates, int* out) {
     for (int r = 0; r < replicates; ++r) {
       int* row = out + static_cast<int64_t>(r) * n;
-      for (int i = 0; i < n; ++i) row[i] = unif_index(n - i);
+      if (n > (1 << 15)) {
+        for (int i = 0; i < n; ++i) row[i] = unif_index(n - i);
+        continue;
+      }
+      int i = 0;
+      while (i < n) {
+        const int dn = n - i;
+        const uint32_t mask = dn == 1 ? 0u : (0xffffffffu >> __builtin_clz(static_cast<unsigned>(dn - 1)));
+        const int v = static_cast<int>((genword() >> 16) & mask);
+        ++draws_;
+        row[i] = v;
+        i += v < dn ? 1 : 0;
+      }
     }
   }
   static void hsic_assemble(int n, int replicates, int* out, std::vector<int>* scratch) {
@@ -125,7 +157,10 @@ class RStream {
   uint64_t draws() const { return draws_; }
 
  private:
-  double genrand() {
+  double genrand() { return static_cast<double>(genword()) * 2.3283064365386963e-10; }
+
+  // the next tempered MT19937 word
+  uint32_t genword() {
     static const uint32_t mag01[2] = {0u, 0x9908b0dfu};
     if (mti_ >= 624) {
       int kk = 0;
@@ -146,7 +181,7 @@ class RStream {
     y ^= (y << 7) & 0x9d2c5680u;
     y ^= (y << 15) & 0xefc60000u;
     y ^= y >> 18;
-    return static_cast<double>(y) * 2.3283064365386963e-10;
+    return y;
   }
 
   uint32_t mt_[624];

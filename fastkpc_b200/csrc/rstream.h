@@ -161,30 +161,34 @@ class RStream {
 
   // the next tempered MT19937 word
   uint32_t genword() {
-    static const uint32_t mag01[2] = {0u, 0x9908b0dfu};
-    if (mti_ >= 624) {
-      int kk = 0;
-      for (; kk < 624 - 397; ++kk) {
-        const uint32_t y = (mt_[kk] & 0x80000000u) | (mt_[kk + 1] & 0x7fffffffu);
-        mt_[kk] = mt_[kk + 397] ^ (y >> 1) ^ mag01[y & 1u];
-      }
-      for (; kk < 623; ++kk) {
-        const uint32_t y = (mt_[kk] & 0x80000000u) | (mt_[kk + 1] & 0x7fffffffu);
-        mt_[kk] = mt_[kk + (397 - 624)] ^ (y >> 1) ^ mag01[y & 1u];
-      }
-      const uint32_t y = (mt_[623] & 0x80000000u) | (mt_[0] & 0x7fffffffu);
-      mt_[623] = mt_[396] ^ (y >> 1) ^ mag01[y & 1u];
-      mti_ = 0;
+    if (mti_ >= 624) refill();
+    return tw_[mti_++];
+  }
+
+  // The next 624 words: the state's twist (the tap 0x9908b0df applied by a
+  // mask, without a table), then all 624 tempered at once into tw_.
+  void refill() {
+    auto twist = [](uint32_t hi, uint32_t lo, uint32_t far) {
+      const uint32_t y = (hi & 0x80000000u) | (lo & 0x7fffffffu);
+      return far ^ (y >> 1) ^ (0x9908b0dfu & (0u - (y & 1u)));
+    };
+    int kk = 0;
+    for (; kk < 624 - 397; ++kk) mt_[kk] = twist(mt_[kk], mt_[kk + 1], mt_[kk + 397]);
+    for (; kk < 623; ++kk) mt_[kk] = twist(mt_[kk], mt_[kk + 1], mt_[kk + (397 - 624)]);
+    mt_[623] = twist(mt_[623], mt_[0], mt_[396]);
+    for (int i = 0; i < 624; ++i) {
+      uint32_t y = mt_[i];
+      y ^= y >> 11;
+      y ^= (y << 7) & 0x9d2c5680u;
+      y ^= (y << 15) & 0xefc60000u;
+      y ^= y >> 18;
+      tw_[i] = y;
     }
-    uint32_t y = mt_[mti_++];
-    y ^= y >> 11;
-    y ^= (y << 7) & 0x9d2c5680u;
-    y ^= (y << 15) & 0xefc60000u;
-    y ^= y >> 18;
-    return y;
+    mti_ = 0;
   }
 
   uint32_t mt_[624];
+  uint32_t tw_[624];  // the current block of tempered words
   int mti_;
   uint64_t draws_ = 0;
   std::vector<int> perm_, pool_;

@@ -294,10 +294,12 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
 // designs, where 80 single-vector steps also do).
 //
 // E is stored whole (both triangles, 2.1 MB at ld 512): a warp owns row
-// blocks of 32 rows (lane = row) and sums whole rows in registers, so the
-// matvec needs no transposing tiles and no per-warp row accumulators, and two
-// CTAs fit on an SM (about 100 KB of shared memory each): one streams E while
-// the other re-orthogonalises.
+// blocks of 32 rows and accumulates whole rows in registers, so the matvec
+// needs no transposing tiles and no per-warp row accumulators, and two CTAs
+// fit on an SM (106.5 KB of shared memory each): one streams E while the
+// other re-orthogonalises.  Tiles stream into a per-warp buffer by cp.async,
+// one ahead, and a tile times the block's rows of Q is 32 mma.m8n8k4 on the
+// FP64 tensor pipe.
 //
 // Step s, with Q_s (nu x 4) the current orthonormal block and V the basis so
 // far (Q_0 .. Q_s):
@@ -315,7 +317,7 @@ __global__ void __launch_bounds__(kTprsThreads) tprs_lanczos_kernel(
 // Outputs per design d: V (nu x 104 at voff[d]), blocks (count x 26 x 32:
 // A_s then R_s, 4 x 4 column-major each), done[d] = 104 or -1.  One CTA per
 // design (grid-stride), two CTAs per SM: dynamic shared memory
-// tprs_block_smem_bytes(ld_max), 96 KB at ld 512; ews: ld^2 per CTA.
+// tprs_block_smem_bytes(ld_max), 104 KB at ld 512; ews: ld^2 per CTA.
 namespace {
 
 constexpr double kTprsBlockPivotTol = 1e-13;

@@ -16,10 +16,16 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <exception>
+#include <functional>
 #include <map>
+#include <mutex>
 #include <thread>
 #include <unordered_map>
+
+#include <unistd.h>
 
 namespace fkpc {
 
@@ -243,25 +249,100 @@ void Engine::plan_components(const std::vector<Test>& tests) {
 namespace {
 
 // f(i) for i in [0, count) on up to 16 host threads.
+// Host worker threads kept for the life of the process: a call's host
+// set-up runs several parallel loops, and starting and joining up to 16
+// threads for each cost more than the short loops themselves.  One job at a
+// time: a parallel_for that finds the pool busy (another device's engine, or
+// a loop nested in a job), or runs in a child forked from the process that
+// started the pool (whose threads the child does not have), starts its own
+// threads instead.  The pool is never destroyed: its threads wait on it until
+// the process ends.
+class HostPool {
+ public:
+  static HostPool& get() {
+    static HostPool* pool = new HostPool();
+    return *pool;
+  }
+  // runs work() on every pool thread and on the caller; false when busy
+  bool run(const std::function<void()>& work) {
+    if (getpid() != owner_) return false;
+    std::unique_lock<std::mutex> busy(submit_, std::try_to_lock);
+    if (!busy.owns_lock() || threads_.empty()) return false;
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      job_ = &work;
+      pending_ = threads_.size();
+      ++generation_;
+    }
+    wake_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(m_);
+    done_.wait(lk, [&] { return pending_ == 0; });
+    job_ = nullptr;
+    return true;
+  }
+
+ private:
+  HostPool() : owner_(getpid()) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned n = std::min(hw, 16u) - 1;
+    for (unsigned w = 0; w < n; ++w) threads_.emplace_back([this] { loop(); });
+  }
+  void loop() {
+    uint64_t seen = 0;
+    for (;;) {
+      const std::function<void()>* job;
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        wake_.wait(lk, [&] { return generation_ != seen; });
+        seen = generation_;
+        job = job_;
+      }
+      (*job)();
+      std::lock_guard<std::mutex> lk(m_);
+      if (--pending_ == 0) done_.notify_one();
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::mutex submit_, m_;
+  std::condition_variable wake_, done_;
+  const std::function<void()>* job_ = nullptr;
+  size_t pending_ = 0;
+  uint64_t generation_ = 0;
+  const pid_t owner_;
+};
+
+// f(i) for every i < count on the host threads; the first exception any f
+// throws is rethrown to the caller once every thread has left the loop.
 template <class F>
 void parallel_for(size_t count, F f) {
   std::atomic<size_t> next(0);
-  auto work = [&]() {
+  std::mutex error_mu;
+  std::exception_ptr error;
+  const std::function<void()> work = [&]() {
     for (;;) {
       const size_t i = next.fetch_add(1);
       if (i >= count) return;
-      f(i);
+      try {
+        f(i);
+      } catch (...) {
+        std::lock_guard<std::mutex> lk(error_mu);
+        if (!error) error = std::current_exception();
+        next.store(count);  // the rest is skipped
+      }
     }
   };
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const size_t workers = std::min<size_t>(std::min<size_t>(hw, 16), count);
-  if (workers <= 1) {
+  if (count <= 1) {
     work();
-    return;
+  } else if (!HostPool::get().run(work)) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t workers = std::min<size_t>(std::min<size_t>(hw, 16), count);
+    std::vector<std::thread> pool;
+    for (size_t w = 1; w < workers; ++w) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
   }
-  std::vector<std::thread> pool;
-  for (size_t w = 0; w < workers; ++w) pool.emplace_back(work);
-  for (auto& th : pool) th.join();
+  if (error) std::rethrow_exception(error);
 }
 
 constexpr int kTprsK = 30;                  // basis dimension of the bivariate thin-plate smooth

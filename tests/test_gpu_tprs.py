@@ -45,16 +45,29 @@ def _ten_levels(n=300, seed=13):
     return np.asfortranarray(X)
 
 
+def _twelve_levels(n=300, seed=1):
+    """Two columns of 12 jittered levels: 127 unique locations, the block
+    path's smallest range (leading dimension 128: four of the eight warps own
+    a row block)."""
+    rs = np.random.default_rng(seed)
+    lv = np.linspace(0.0, 11.0, 12) + rs.normal(scale=0.05, size=12)
+    X = np.empty((n, 3))
+    X[:, 0] = lv[rs.integers(0, 12, size=n)]
+    X[:, 1] = lv[rs.integers(0, 12, size=n)] * 0.9 + 0.2
+    X[:, 2] = rs.normal(size=n)
+    return np.asfortranarray(X)
+
+
 def cases():
     dev = np.load(golden_path("dev500x50.npz"))["data"]
     sem351 = workloads.skeleton_351x48(537)
     sem1000 = workloads.nonlinear_sem(1000, 12, 0.3, 31)[0]
     return [("dev500", dev, 0, 1, "block"), ("dev500", dev, 17, 42, "block"), ("dev500", dev, 5, 49, "block"),
             ("sem351x48", sem351, 3, 40, "block"), ("sem1000x12", sem1000, 3, 7, "single"),
-            ("ten_levels", _ten_levels(), 0, 1, "single")]
+            ("ten_levels", _ten_levels(), 0, 1, "single"), ("twelve_levels", _twelve_levels(), 0, 1, "block")]
 
 
-@pytest.mark.parametrize("case", range(6))
+@pytest.mark.parametrize("case", range(7))
 def test_device_ritz_pairs_match_dense_eigen(lib_built, case):
     name, X, a, b, path = cases()[case]
     got = fk.tprs_export(X, a, b)

@@ -407,7 +407,7 @@ typedef struct fkpc_tuning {
   int split_statistics;     /* 1 (default): the statistics of pairs whose fits are final run
                                beside the continuation; 0: after every fit */
   int lowrank_ctas_per_sm;  /* guard-band Lanczos CTAs per SM, 1..4; default 2 */
-  int tprs_ctas_per_sm;     /* thin-plate set-up Lanczos CTAs per SM, 1..4; default 2 */
+  int tprs_ctas_per_sm;     /* single-vector thin-plate Lanczos CTAs per SM, 1..4; default 2 (the block Lanczos runs two per SM, as its shared memory allows) */
 } fkpc_tuning;
 FKPC_API int fkpc_get_tuning(int device, fkpc_tuning* tuning);
 FKPC_API int fkpc_set_tuning(int device, const fkpc_tuning* tuning);

@@ -927,7 +927,8 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
 // Ritz pairs of the block Lanczos runs (one warp per design).  T = V'EV
 // (104 x 104, bandwidth 4: diagonal blocks (A_s + A_s')/2, couplings R_s) is
 // held as its band.  A single-vector Lanczos on T (full re-orthogonalisation,
-// two classical passes) from the host's deterministic start sequence reduces
+// two passes, eight basis columns at a time) from the host's deterministic
+// start sequence reduces
 // it to a tridiagonal T' = P'TP of kTprsInnerSteps = 72 (P: 104 x 72, in a
 // per-design global workspace): on the 500 x 50 level's designs T's k = 30
 // pairs have converged to 1e-20 relative by then.  The implicit QL above

@@ -556,7 +556,10 @@ def run_ours(args, world, rank, local, pg):
                     "d2h_bytes_per_step": e2e_stats["d2h_bytes"], "steps": len(e2e_t), "warmup_calls": 1,
                     "setup_ms": e2e_stats["setup_ms"], "upload_ms": e2e_stats["upload_ms"],
                     "device_ms": e2e_stats["device_ms"], "download_ms": e2e_stats["download_ms"],
-                    "call_ms": e2e_stats["total_ms"], "wall_s": statistics.median(e2e_t)},
+                    "call_ms": e2e_stats["total_ms"], "wall_s": statistics.median(e2e_t),
+                    "timeline_ms": {k: e2e_stats[k] for k in ("plan_ms", "tprs_host_ms", "smooth_wait_ms",
+                                                              "design_host_ms", "late_wait_ms",
+                                                              "prefit_device_ms")}},
             "skeleton_351x48": skel,
             "uneven_perm_500x64": uneven,
             "adjoint_1000": adjoint,

@@ -937,6 +937,48 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
 // Ritz pair (theta, V P s) of E has two orthogonal parts, beta_72 s_72 (inside
 // the block Krylov space) and R_last (P s)_last (the block that would follow):
 // the pair is accepted when their root-sum-square is at most 1e-14 max|theta|.
+namespace {
+
+// Number of eigenvalues below x of the symmetric tridiagonal (d, e), e[i]
+// coupling rows i and i + 1: the sign changes of the leading principal minors
+// p_0 = 1, p_i = (d_{i-1} - x) p_{i-1} - e_{i-2}^2 p_{i-2} (Wilkinson's Sturm
+// sequence), a zero minor counted as a change, the pair rescaled by a power
+// of two whenever it leaves [1e-150, 1e150].
+__device__ int sturm_below(const double* d, const double* e, int m, double x) {
+  double pm = 1.0, pc = d[0] - x;
+  if (pc == 0.0) pc = -1e-300;
+  int cnt = pc < 0.0 ? 1 : 0;
+  for (int i = 1; i < m; ++i) {
+    double pn = (d[i] - x) * pc - (e[i - 1] * e[i - 1]) * pm;
+    if (pn == 0.0) pn = pc < 0.0 ? 1e-300 : -1e-300;
+    if ((pn < 0.0) != (pc < 0.0)) ++cnt;
+    pm = pc;
+    pc = pn;
+    const double a = fabs(pc);
+    if (a > 1e150 || a < 1e-150) {
+      const int ex = ilogb(a);
+      pc = scalbn(pc, -ex);
+      pm = scalbn(pm, -ex);
+    }
+  }
+  return cnt;
+}
+
+// The idx-th smallest eigenvalue (0-based) of (d, e) by bisection on [lo, hi]
+// until the bracket is at rounding level of the value.
+__device__ double tridiag_bisect(const double* d, const double* e, int m, int idx, double lo, double hi,
+                                 double floor_tol) {
+  for (int it = 0; it < 160; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (hi - lo <= 2.220446049250313e-16 * fmax(fabs(lo), fabs(hi)) + floor_tol || mid <= lo || mid >= hi) break;
+    if (sturm_below(d, e, m, mid) <= idx) lo = mid;
+    else hi = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+
+}  // namespace
+
 constexpr int kTprsInnerSteps = 72;
 constexpr int kTprsBand = 2 * kTprsBlock + 1;
 // per-warp dynamic shared memory (doubles): z, the band, p and a spare vector, d / e / rotations
@@ -1042,10 +1084,13 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel
       wr[t] -= a * pr[t] + bprev * pp[t];
       before += wr[t] * wr[t];
     }
-    // full re-orthogonalisation against P's columns 0 .. j, two passes, eight
-    // columns at a time: their entries of this lane's rows held in registers,
-    // the eight dot products reduced together (every lane gets the sums),
-    // then subtracted (classical within a group of eight, modified across)
+    // full re-orthogonalisation against P's columns 0 .. j, eight columns at
+    // a time: their entries of this lane's rows held in registers, the eight
+    // dot products reduced together (every lane gets the sums), then
+    // subtracted (classical within a group of eight, modified across); a
+    // second pass only when the first removed more than three quarters of
+    // |w|^2 (DGKS)
+    before = warp_sum_t(before);
     for (int pass = 0; pass < 2; ++pass) {
       for (int c0 = 0; c0 <= j; c0 += 8) {
         double pcv[8][kR];
@@ -1068,6 +1113,12 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel
 #pragma unroll
           for (int t = 0; t < kR; ++t) wr[t] -= sd[u] * pcv[u][t];
       }
+      double after = 0.0;
+#pragma unroll
+      for (int t = 0; t < kR; ++t) after += wr[t] * wr[t];
+      after = warp_sum_t(after);
+      if (after > 0.25 * before) break;
+      before = after;
     }
     double after = 0.0;
 #pragma unroll
@@ -1097,25 +1148,140 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel
   __syncwarp();
   const double blast = ee[taken - 1];
   if (lane == 0) ee[taken - 1] = 0.0;
-  for (int c = 0; c < taken; ++c)
-    for (int i = lane; i < taken; i += 32) z[i + ms2 * c] = i == c ? 1.0 : 0.0;
   __syncwarp();
-  if (taken < k || !tridiag_ql(dd, ee, z, taken, ms2, rc, rs, ctlsh[warp], lane)) {
+  if (taken < k) {
     if (lane == 0) ok[d] = 0;
     return;
   }
-  const double tmax = select_largest(dd, taken, k, sel, lane);
+  // T's eigenpairs: the candidate eigenvalues by bisection (one per lane, in step),
+  // the k selected vectors by inverse iteration (lane c: selection rank c;
+  // x and the factorisation's pivots interleaved by lane in z, conflict-free),
+  // re-orthogonalised within clusters.  They are kept only when every
+  // selected pair has a residual below 1e-13 |T| and the vectors are
+  // orthogonal to 1e-12; otherwise the implicit QL above diagonalises T'.
+  double* d0 = pv + m;  // the tridiagonal, kept for the fallback (p is no longer needed)
+  double* e0 = pv;
+  for (int i = lane; i < taken; i += 32) {
+    d0[i] = dd[i];
+    e0[i] = ee[i];
+  }
+  __syncwarp();
+  double glo = INFINITY, ghi = -INFINITY;
+  for (int i = lane; i < taken; i += 32) {
+    const double r = (i > 0 ? fabs(e0[i - 1]) : 0.0) + fabs(e0[i]);
+    glo = fmin(glo, d0[i] - r);
+    ghi = fmax(ghi, d0[i] + r);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    glo = fmin(glo, __shfl_xor_sync(0xffffffffu, glo, o));
+    ghi = fmax(ghi, __shfl_xor_sync(0xffffffffu, ghi, o));
+  }
+  const double tnorm = fmax(fabs(glo), fabs(ghi));
+  const double eps = 2.220446049250313e-16;
+  // the k values of largest magnitude are among the k most negative and the k
+  // most positive: only those (at most 2k) are bisected, the rest set to 0
+  const int nneg = sturm_below(d0, e0, taken, 0.0);
+  const int lo_end = min(k, nneg), hi_begin = max(nneg, taken - k);
+  const int ncand = lo_end + (taken - hi_begin);
+  for (int idx = lane; idx < taken; idx += 32) dd[idx] = 0.0;
+  __syncwarp();
+  for (int cidx = lane; cidx < ncand; cidx += 32) {
+    const int idx = cidx < lo_end ? cidx : hi_begin + (cidx - lo_end);
+    dd[idx] = tridiag_bisect(d0, e0, taken, idx, glo, ghi, eps * tnorm * 1e-3);
+  }
+  __syncwarp();
+  double tmax = select_largest(dd, taken, k, sel, lane);
+  double* xs = z;             // x: xs[i * 32 + c]
+  double* us = z + 32 * ms2;  // 1 / pivot: us[i * 32 + c]
+  bool good = true;
+  if (lane < k) {
+    const double th = dd[sel[lane]];
+    const double tiny = eps * tnorm;
+    double piv = d0[0] - th;
+    for (int i = 0; i < taken; ++i) {
+      if (i > 0) piv = (d0[i] - th) - e0[i - 1] * e0[i - 1] * us[(i - 1) * 32 + lane];
+      if (fabs(piv) < tiny) piv = piv < 0.0 ? -tiny : tiny;
+      us[i * 32 + lane] = 1.0 / piv;
+      xs[i * 32 + lane] = 1.0 / (1.0 + static_cast<double>((i * 37 + lane * 11) % 17));
+    }
+    for (int it = 0; it < 3; ++it) {
+      // (T' - theta) x_new = x: L y = x, then U x_new = y; normalised
+      for (int i = 1; i < taken; ++i)
+        xs[i * 32 + lane] -= e0[i - 1] * us[(i - 1) * 32 + lane] * xs[(i - 1) * 32 + lane];
+      xs[(taken - 1) * 32 + lane] *= us[(taken - 1) * 32 + lane];
+      for (int i = taken - 2; i >= 0; --i)
+        xs[i * 32 + lane] = (xs[i * 32 + lane] - e0[i] * xs[(i + 1) * 32 + lane]) * us[i * 32 + lane];
+      double nrm = 0.0;
+      for (int i = 0; i < taken; ++i) nrm += xs[i * 32 + lane] * xs[i * 32 + lane];
+      const double inv = 1.0 / sqrt(nrm);
+      for (int i = 0; i < taken; ++i) xs[i * 32 + lane] *= inv;
+    }
+  }
+  __syncwarp();
+  // re-orthogonalise within clusters (values closer than 1e-3 |T|), in rank order
+  for (int c = 1; c < k; ++c) {
+    for (int c2 = 0; c2 < c; ++c2) {
+      if (fabs(dd[sel[c]] - dd[sel[c2]]) > 1e-3 * tnorm) continue;
+      double dot = 0.0;
+      for (int i = lane; i < taken; i += 32) dot += xs[i * 32 + c] * xs[i * 32 + c2];
+      dot = warp_sum_t(dot);
+      double nrm = 0.0;
+      for (int i = lane; i < taken; i += 32) {
+        const double v = xs[i * 32 + c] - dot * xs[i * 32 + c2];
+        xs[i * 32 + c] = v;
+        nrm += v * v;
+      }
+      nrm = warp_sum_t(nrm);
+      const double inv = 1.0 / sqrt(nrm);
+      for (int i = lane; i < taken; i += 32) xs[i * 32 + c] *= inv;
+      __syncwarp();
+    }
+  }
+  if (lane < k) {
+    const double th = dd[sel[lane]];
+    double res = 0.0;
+    for (int i = 0; i < taken; ++i) {
+      double r = (d0[i] - th) * xs[i * 32 + lane];
+      if (i > 0) r += e0[i - 1] * xs[(i - 1) * 32 + lane];
+      if (i + 1 < taken) r += e0[i] * xs[(i + 1) * 32 + lane];
+      res += r * r;
+    }
+    if (!(sqrt(res) <= 1e-13 * tnorm)) good = false;
+    for (int c2 = 0; c2 < k; ++c2) {
+      if (c2 == lane) continue;
+      double dot = 0.0;
+      for (int i = 0; i < taken; ++i) dot += xs[i * 32 + lane] * xs[i * 32 + c2];
+      if (!(fabs(dot) <= 1e-12)) good = false;
+    }
+  }
+  good = __all_sync(0xffffffffu, good);
+  if (!good) {
+    for (int i = lane; i < taken; i += 32) {
+      dd[i] = d0[i];
+      ee[i] = e0[i];
+    }
+    for (int c = 0; c < taken; ++c)
+      for (int i = lane; i < taken; i += 32) z[i + ms2 * c] = i == c ? 1.0 : 0.0;
+    __syncwarp();
+    if (!tridiag_ql(dd, ee, z, taken, ms2, rc, rs, ctlsh[warp], lane)) {
+      if (lane == 0) ok[d] = 0;
+      return;
+    }
+    tmax = select_largest(dd, taken, k, sel, lane);
+  }
+  // component b of the selected vector of rank c
+  auto vec = [&](int c, int b) { return good ? xs[b * 32 + c] : z[b + ms2 * sel[c]]; };
   const bool invariant = fabs(blast) <= 1e-15 * tmax;
   const double* rl = blk + 32 * (kTprsBlockSteps - 1) + 16;  // R_last, upper triangular
   bool conv = true;
   for (int c = lane; c < k; c += 32) {
     const int i = sel[c];
-    const double inner = invariant ? 0.0 : blast * z[(taken - 1) + ms2 * i];
+    const double inner = invariant ? 0.0 : blast * vec(c, taken - 1);
     double y[kTprsBlock];
 #pragma unroll
     for (int r = 0; r < kTprsBlock; ++r) {
       double acc = 0.0;
-      for (int b = 0; b < taken; ++b) acc += P[(m - kTprsBlock + r) + static_cast<int64_t>(m) * b] * z[b + ms2 * i];
+      for (int b = 0; b < taken; ++b) acc += P[(m - kTprsBlock + r) + static_cast<int64_t>(m) * b] * vec(c, b);
       y[r] = acc;
     }
     double outer = 0.0;
@@ -1141,13 +1307,12 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel
   __syncwarp();
   // eigenvectors in the block basis: P s, lanes over rows
   for (int c = 0; c < k; ++c) {
-    const int i = sel[c];
     double* zc = zsel + (static_cast<int64_t>(d) * k + pos[c]) * zstride;
     double acc[kR];
 #pragma unroll
     for (int t = 0; t < kR; ++t) acc[t] = 0.0;
     for (int b = 0; b < taken; ++b) {
-      const double zb = z[b + ms2 * i];
+      const double zb = vec(c, b);
 #pragma unroll
       for (int t = 0; t < kR; ++t) {
         const int row = lane + 32 * t;

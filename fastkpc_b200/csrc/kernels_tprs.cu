@@ -939,21 +939,27 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_select_kernel(
 // the pair is accepted when their root-sum-square is at most 1e-14 max|theta|.
 namespace {
 
-// Number of eigenvalues below x of the symmetric tridiagonal (d, e), e[i]
-// coupling rows i and i + 1: the sign changes of the leading principal minors
-// p_0 = 1, p_i = (d_{i-1} - x) p_{i-1} - e_{i-2}^2 p_{i-2} (Wilkinson's Sturm
-// sequence), a zero minor counted as a change, the pair rescaled by a power
-// of two whenever it leaves [1e-150, 1e150].
-__device__ int sturm_below(const double* d, const double* e, int m, double x) {
+// Number of eigenvalues below x of the symmetric tridiagonal (d, e), e2[i] =
+// e[i]^2 the squared coupling of rows i and i + 1: the sign changes of the
+// leading principal minors p_0 = 1, p_i = (d_{i-1} - x) p_{i-1} - e2_{i-2}
+// p_{i-2} (Wilkinson's Sturm sequence), a zero minor counted as a change.
+// Four minors at a time, after which the pair is rescaled by a power of two
+// when it has left [1e-150, 1e150] (four steps move it by far less than the
+// rest of the double range for these spectra).
+__device__ int sturm_below(const double* d, const double* e2, int m, double x) {
   double pm = 1.0, pc = d[0] - x;
   if (pc == 0.0) pc = -1e-300;
   int cnt = pc < 0.0 ? 1 : 0;
-  for (int i = 1; i < m; ++i) {
-    double pn = (d[i] - x) * pc - (e[i - 1] * e[i - 1]) * pm;
-    if (pn == 0.0) pn = pc < 0.0 ? 1e-300 : -1e-300;
-    if ((pn < 0.0) != (pc < 0.0)) ++cnt;
-    pm = pc;
-    pc = pn;
+  int i = 1;
+  for (; i + 4 <= m; i += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      double pn = (d[i + u] - x) * pc - e2[i + u - 1] * pm;
+      if (pn == 0.0) pn = pc < 0.0 ? 1e-300 : -1e-300;
+      cnt += (pn < 0.0) != (pc < 0.0) ? 1 : 0;
+      pm = pc;
+      pc = pn;
+    }
     const double a = fabs(pc);
     if (a > 1e150 || a < 1e-150) {
       const int ex = ilogb(a);
@@ -961,17 +967,24 @@ __device__ int sturm_below(const double* d, const double* e, int m, double x) {
       pm = scalbn(pm, -ex);
     }
   }
+  for (; i < m; ++i) {
+    double pn = (d[i] - x) * pc - e2[i - 1] * pm;
+    if (pn == 0.0) pn = pc < 0.0 ? 1e-300 : -1e-300;
+    cnt += (pn < 0.0) != (pc < 0.0) ? 1 : 0;
+    pm = pc;
+    pc = pn;
+  }
   return cnt;
 }
 
-// The idx-th smallest eigenvalue (0-based) of (d, e) by bisection on [lo, hi]
-// until the bracket is at rounding level of the value.
-__device__ double tridiag_bisect(const double* d, const double* e, int m, int idx, double lo, double hi,
+// The idx-th smallest eigenvalue (0-based) of (d, e2) by bisection on
+// [lo, hi] until the bracket is at rounding level of the value.
+__device__ double tridiag_bisect(const double* d, const double* e2, int m, int idx, double lo, double hi,
                                  double floor_tol) {
   for (int it = 0; it < 160; ++it) {
     const double mid = 0.5 * (lo + hi);
     if (hi - lo <= 2.220446049250313e-16 * fmax(fabs(lo), fabs(hi)) + floor_tol || mid <= lo || mid >= hi) break;
-    if (sturm_below(d, e, m, mid) <= idx) lo = mid;
+    if (sturm_below(d, e2, m, mid) <= idx) lo = mid;
     else hi = mid;
   }
   return 0.5 * (lo + hi);
@@ -1179,15 +1192,19 @@ __global__ void __launch_bounds__(kRitzWarps * 32) tprs_ritz_block_select_kernel
   const double tnorm = fmax(fabs(glo), fabs(ghi));
   const double eps = 2.220446049250313e-16;
   // the k values of largest magnitude are among the k most negative and the k
-  // most positive: only those (at most 2k) are bisected, the rest set to 0
-  const int nneg = sturm_below(d0, e0, taken, 0.0);
+  // most positive: only those (at most 2k) are bisected, the rest set to 0.
+  // The squared couplings in rc (the QL fallback's rotations come later).
+  double* e2 = rc;
+  for (int i = lane; i < taken; i += 32) e2[i] = e0[i] * e0[i];
+  __syncwarp();
+  const int nneg = sturm_below(d0, e2, taken, 0.0);
   const int lo_end = min(k, nneg), hi_begin = max(nneg, taken - k);
   const int ncand = lo_end + (taken - hi_begin);
   for (int idx = lane; idx < taken; idx += 32) dd[idx] = 0.0;
   __syncwarp();
   for (int cidx = lane; cidx < ncand; cidx += 32) {
     const int idx = cidx < lo_end ? cidx : hi_begin + (cidx - lo_end);
-    dd[idx] = tridiag_bisect(d0, e0, taken, idx, glo, ghi, eps * tnorm * 1e-3);
+    dd[idx] = tridiag_bisect(d0, e2, taken, idx, glo, ghi, eps * tnorm * 1e-3);
   }
   __syncwarp();
   double tmax = select_largest(dd, taken, k, sel, lane);
